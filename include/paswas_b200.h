@@ -1,0 +1,148 @@
+/*
+ * paswas_b200.h -- C ABI of the B200 Smith-Waterman engine (libpaswas_b200.so).
+ *
+ * Drop-in for the device side of pyPaSWAS's CUDA backend
+ * (pyPaSWAS/Core/SmithWatermanCuda.py).  Plain pointers and sizes only; every
+ * call returns a status code (PW_OK == 0, negative on error) and never aborts.
+ * A human-readable message for the last failure is available from
+ * pw_last_error().  One engine per host thread; calls on one engine are
+ * serialised on its own CUDA stream.
+ *
+ * Host arrays are borrowed for the duration of a call.  Device memory is owned
+ * by the engine.  Results stay valid until the next pw_align() or pw_destroy().
+ */
+#ifndef PASWAS_B200_H
+#define PASWAS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes; the Python layer maps them onto the reference's exceptions
+ * (pyPaSWAS/Core/Exceptions.py): ARG -> InvalidOptionException,
+ * DEVICE -> HardwareException, KERNEL/NOMEM/CAPACITY -> CudaException. */
+#define PW_OK 0
+#define PW_ERR_ARG (-1)
+#define PW_ERR_DEVICE (-2)
+#define PW_ERR_KERNEL (-3)
+#define PW_ERR_NOMEM (-4)
+#define PW_ERR_CAPACITY (-5)
+#define PW_ERR_STATE (-6)
+
+/* pw_align() flags */
+#define PW_FLAG_SCORE_ONLY 1u /* pair maxima only: no starting points, no walk */
+#define PW_FLAG_PLAIN 2u      /* one pair per kernel launch (the unbatched form) */
+
+typedef struct pw_engine pw_engine;
+
+/* One alignment produced by the walk of SmithWaterman._print_alignments
+ * (pyPaSWAS/Core/SmithWaterman.py:703-838).  Coordinates follow the
+ * reference: s_* are query (x axis) positions, t_* target (y axis) positions,
+ * both inclusive and 0-based.  The three alignment strings of the hit are
+ * n_cols bytes each at strbuf + str_offset (sequence_match), + n_cols
+ * (alignment), + 2 * n_cols (target_match). */
+typedef struct {
+    int32_t query;      /* index into the query list given to pw_set_queries */
+    int32_t target;     /* index into the target list given to pw_set_targets */
+    int32_t s_start, s_end, t_start, t_end;
+    float score;        /* starting-point score (fp32, as the reference) */
+    int32_t matches, mismatches;
+    int32_t n_cols;
+    int64_t str_offset;
+} pw_hit;
+
+typedef struct {
+    int64_t pairs;          /* query x target pairs aligned */
+    int64_t cells;          /* sum of len(q) * len(t) over the pairs */
+    int64_t traced_pairs;   /* pairs whose maximum reached the minimum score */
+    int64_t starting_points;
+    int64_t hits;           /* hits kept by the walk (before the Python filter) */
+    int64_t string_bytes;   /* bytes needed for all hit strings (3 * n_cols summed) */
+    int32_t kernel_launches;
+    int32_t truncated;      /* 1 when the starting-point cap cut the walk short */
+    double score_ms, trace_ms, walk_ms; /* device time of the three phases */
+} pw_run_info;
+
+/* Creates an engine on CUDA device `device`.
+ * Replaces SmithWatermanCuda._initialize_device (SmithWatermanCuda.py:46-62). */
+int pw_create(int device, pw_engine** out);
+
+/* Releases all device memory of the engine (SmithWatermanCuda._clear_memory,
+ * SmithWatermanCuda.py:69-94, plus the context pop of __del__, :40-43). */
+void pw_destroy(pw_engine* e);
+
+/* Message of the last failure on this engine ("" when none). */
+const char* pw_last_error(pw_engine* e);
+
+/* Free device memory in bytes (SmithWatermanCuda._device_global_mem_size,
+ * SmithWatermanCuda.py:64-66). */
+int pw_device_free_memory(pw_engine* e, int64_t* free_bytes, int64_t* total_bytes);
+
+/* Scoring model and kernel constants.  Replaces the template substitution of
+ * PaSWAS.Code.set_score_code (pyPaSWAS/Core/PaSWAS.py:55-72) and the per-shape
+ * recompile of SmithWatermanCuda._compile_code (SmithWatermanCuda.py:170-174):
+ * the engine takes these at run time.
+ *   matrix        dim * dim substitution scores, row = query residue,
+ *                 column = target residue, both minus char_offset
+ *                 (default_score.cu:23, default_main.cu:234)
+ *   gap, ext      gapScore / gapExtension; affine != 0 selects
+ *                 calculateScoreAffineGap (SmithWaterman.py:149)
+ *   lower_limit   LOWER_LIMIT_SCORE, minimum_score MINIMUM_SCORE, both fp32
+ *                 as compiled (default_score.cu, default_main.cu:596,609)
+ *   host_minimum  settings.minimum_score as the Python float the host walk
+ *                 compares against (SmithWaterman.py:758)
+ *   highest, filter_factor   give maxPossibleScore per pair,
+ *                 fp32(highest * min(len_q, len_t) * filter_factor) evaluated
+ *                 in double (SmithWatermanCuda.py:269-275)
+ * Gap penalties must be <= 0. */
+int pw_set_scoring(pw_engine* e, const float* matrix, int dim, int char_offset, float gap, float ext, int affine,
+                   float lower_limit, float minimum_score, double host_minimum, double highest,
+                   double filter_factor);
+
+/* Query sequences (the x axis; records_seqs of SmithWaterman.align_sequences,
+ * SmithWaterman.py:441).  residues: all sequences concatenated, upper-cased,
+ * unpadded; offsets: n + 1 entries.  id_keys: one int per record, equal for
+ * records whose ids are equal (same-id pairs are skipped,
+ * SmithWaterman.py:752-755).  Replaces the query half of copy_sequences
+ * (SmithWatermanCuda.py:176-184). */
+int pw_set_queries(pw_engine* e, const uint8_t* residues, const int64_t* offsets, int32_t n,
+                   const int32_t* id_keys);
+
+/* Target sequences (the y axis), same conventions; they stay resident on the
+ * device until replaced.  Replaces set_targets + the target half of
+ * copy_sequences (SmithWaterman.py:370-414, SmithWatermanCuda.py:176-184). */
+int pw_set_targets(pw_engine* e, const uint8_t* residues, const int64_t* offsets, int32_t n,
+                   const int32_t* id_keys);
+
+/* Aligns every query against every target: score sweep, starting-point
+ * collection and the traceback walk.  Replaces SmithWaterman._calculate_score,
+ * _traceback_host and the walk of _print_alignments (SmithWaterman.py:592-841)
+ * with the kernel calls of SmithWatermanCuda._execute_calculate_score_kernel /
+ * _execute_traceback_kernel (SmithWatermanCuda.py:191-259).
+ * start_cap < 0: no cap; otherwise at most start_cap starting points are
+ * walked, chosen in emission order (SmithWaterman.py:683-685). */
+int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_info* info);
+
+/* Pair maxima (the last block of the maxima chain, default_main.cu:591),
+ * row-major [n_queries][n_targets]. */
+int pw_get_pair_max(pw_engine* e, float* out, int64_t n);
+
+/* Hits of the last pw_align in the order the reference appends them to its
+ * HitList: ascending score, then the pinned emission order of their starting
+ * points.  strbuf receives the alignment strings (info->string_bytes). */
+int pw_get_hits(pw_engine* e, pw_hit* hits, int64_t max_hits, char* strbuf, int64_t strbuf_bytes);
+
+/* Starting points of the last pw_align (StartingPoint layout of
+ * default_main.cu:66-76, 36 bytes each) in emission order; `sequence` and
+ * `target` are query / target list indices. */
+int pw_get_starting_points(pw_engine* e, void* out36, int64_t max_points, int64_t* n_points);
+
+/* Number of this library's kernels launched by the last pw_align. */
+int pw_last_launch_count(pw_engine* e, int64_t* n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,217 @@
+"""ctypes binding of libpaswas_b200.so (include/paswas_b200.h).
+
+The library is built in-tree by ``pypaswas_b200.build`` (nvcc, sm_100a).  There
+is no CPU fallback: when the library or a CUDA device is missing, loading or
+creating an engine raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from .exceptions import CudaException, HardwareException, InvalidOptionException
+
+PACKAGE_DIR = os.path.dirname(os.path.abspath(__file__))
+LIBRARY_PATH = os.path.join(PACKAGE_DIR, "libpaswas_b200.so")
+
+PW_OK = 0
+PW_ERR_ARG = -1
+PW_ERR_DEVICE = -2
+PW_ERR_KERNEL = -3
+PW_ERR_NOMEM = -4
+PW_ERR_CAPACITY = -5
+PW_ERR_STATE = -6
+
+PW_FLAG_SCORE_ONLY = 1
+PW_FLAG_PLAIN = 2
+
+# symbols the header declares, checked by the CPU test-suite
+EXPORTED_SYMBOLS = (
+    "pw_create", "pw_destroy", "pw_last_error", "pw_device_free_memory", "pw_set_scoring",
+    "pw_set_queries", "pw_set_targets", "pw_align", "pw_get_pair_max", "pw_get_hits",
+    "pw_get_starting_points", "pw_last_launch_count",
+)
+
+
+class PwHit(ctypes.Structure):
+    _fields_ = [("query", ctypes.c_int32), ("target", ctypes.c_int32), ("s_start", ctypes.c_int32),
+                ("s_end", ctypes.c_int32), ("t_start", ctypes.c_int32), ("t_end", ctypes.c_int32),
+                ("score", ctypes.c_float), ("matches", ctypes.c_int32), ("mismatches", ctypes.c_int32),
+                ("n_cols", ctypes.c_int32), ("str_offset", ctypes.c_int64)]
+
+
+HIT_DTYPE = np.dtype([("query", "<i4"), ("target", "<i4"), ("s_start", "<i4"), ("s_end", "<i4"),
+                      ("t_start", "<i4"), ("t_end", "<i4"), ("score", "<f4"), ("matches", "<i4"),
+                      ("mismatches", "<i4"), ("n_cols", "<i4"), ("str_offset", "<i8")])
+assert HIT_DTYPE.itemsize == ctypes.sizeof(PwHit)
+
+START_DTYPE = np.dtype([("sequence", "<u4"), ("target", "<u4"), ("block_x", "<u4"), ("block_y", "<u4"),
+                        ("value_x", "<u4"), ("value_y", "<u4"), ("score", "<f4"), ("max_score", "<f4"),
+                        ("pos_score", "<f4")])
+
+
+class PwRunInfo(ctypes.Structure):
+    _fields_ = [("pairs", ctypes.c_int64), ("cells", ctypes.c_int64), ("traced_pairs", ctypes.c_int64),
+                ("starting_points", ctypes.c_int64), ("hits", ctypes.c_int64), ("string_bytes", ctypes.c_int64),
+                ("kernel_launches", ctypes.c_int32), ("truncated", ctypes.c_int32), ("score_ms", ctypes.c_double),
+                ("trace_ms", ctypes.c_double), ("walk_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+def bind(lib):
+    """Declares the argument and result types of every exported function."""
+    P, I32, I64, U32, F, D = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_uint32, ctypes.c_float, \
+        ctypes.c_double
+    sig = {
+        "pw_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+        "pw_destroy": (None, [P]),
+        "pw_last_error": (ctypes.c_char_p, [P]),
+        "pw_device_free_memory": (ctypes.c_int, [P, ctypes.POINTER(I64), ctypes.POINTER(I64)]),
+        "pw_set_scoring": (ctypes.c_int, [P, P, ctypes.c_int, ctypes.c_int, F, F, ctypes.c_int, F, F, D, D, D]),
+        "pw_set_queries": (ctypes.c_int, [P, P, P, I32, P]),
+        "pw_set_targets": (ctypes.c_int, [P, P, P, I32, P]),
+        "pw_align": (ctypes.c_int, [P, U32, I64, ctypes.POINTER(PwRunInfo)]),
+        "pw_get_pair_max": (ctypes.c_int, [P, P, I64]),
+        "pw_get_hits": (ctypes.c_int, [P, P, I64, P, I64]),
+        "pw_get_starting_points": (ctypes.c_int, [P, P, I64, ctypes.POINTER(I64)]),
+        "pw_last_launch_count": (ctypes.c_int, [P, ctypes.POINTER(I64)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+_lib = None
+
+
+def load_library():
+    """Loads the in-tree engine library; raises HardwareException when absent."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBRARY_PATH):
+            raise HardwareException("libpaswas_b200.so is not built (run pypaswas_b200.build.build())")
+        _lib = bind(ctypes.CDLL(LIBRARY_PATH))
+    return _lib
+
+
+def _check(lib, handle, rc, what):
+    if rc == PW_OK:
+        return
+    msg = lib.pw_last_error(handle) if handle else None
+    msg = "%s failed (%d): %s" % (what, rc, msg.decode() if msg else "")
+    if rc == PW_ERR_ARG:
+        raise InvalidOptionException(msg)
+    if rc == PW_ERR_DEVICE:
+        raise HardwareException(msg)
+    raise CudaException(msg)
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None and a.size else ctypes.c_void_p(0)
+
+
+def pack_sequences(seqs):
+    """Concatenates byte strings; returns (residues uint8, offsets int64)."""
+    lens = np.fromiter((len(s) for s in seqs), dtype=np.int64, count=len(seqs))
+    off = np.zeros(len(seqs) + 1, dtype=np.int64)
+    np.cumsum(lens, out=off[1:])
+    buf = np.frombuffer(b"".join(seqs), dtype=np.uint8) if len(seqs) else np.zeros(0, np.uint8)
+    return np.ascontiguousarray(buf), off
+
+
+class Engine(object):
+    """One device engine (one CUDA stream).  Thin, stateful wrapper of the C ABI."""
+
+    def __init__(self, device=0, lib=None):
+        self.lib = lib if lib is not None else load_library()
+        h = ctypes.c_void_p()
+        rc = self.lib.pw_create(int(device), ctypes.byref(h))
+        if rc != PW_OK:
+            raise HardwareException("Failed to initialize device %d (status %d)" % (device, rc))
+        self.handle = h
+        self.n_queries = 0
+        self.n_targets = 0
+        self.last_info = None
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.pw_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def free_memory(self):
+        f, t = ctypes.c_int64(), ctypes.c_int64()
+        _check(self.lib, self.handle, self.lib.pw_device_free_memory(self.handle, ctypes.byref(f), ctypes.byref(t)),
+               "pw_device_free_memory")
+        return f.value, t.value
+
+    def set_scoring(self, matrix, char_offset, gap, ext, affine, lower_limit, minimum_score, host_minimum,
+                    highest, filter_factor):
+        m = np.ascontiguousarray(matrix, dtype=np.float32)
+        self._matrix = m
+        rc = self.lib.pw_set_scoring(self.handle, _ptr(m), int(m.shape[0]), int(char_offset), float(gap), float(ext),
+                                     int(bool(affine)), float(lower_limit), float(minimum_score), float(host_minimum),
+                                     float(highest), float(filter_factor))
+        _check(self.lib, self.handle, rc, "pw_set_scoring")
+
+    def set_queries(self, seqs, id_keys):
+        buf, off = pack_sequences(seqs)
+        keys = np.ascontiguousarray(id_keys, dtype=np.int32)
+        _check(self.lib, self.handle,
+               self.lib.pw_set_queries(self.handle, _ptr(buf), _ptr(off), len(seqs), _ptr(keys)), "pw_set_queries")
+        self.n_queries = len(seqs)
+
+    def set_targets(self, seqs, id_keys):
+        buf, off = pack_sequences(seqs)
+        keys = np.ascontiguousarray(id_keys, dtype=np.int32)
+        _check(self.lib, self.handle,
+               self.lib.pw_set_targets(self.handle, _ptr(buf), _ptr(off), len(seqs), _ptr(keys)), "pw_set_targets")
+        self.n_targets = len(seqs)
+
+    def align(self, score_only=False, plain=False, start_cap=-1):
+        info = PwRunInfo()
+        flags = (PW_FLAG_SCORE_ONLY if score_only else 0) | (PW_FLAG_PLAIN if plain else 0)
+        rc = self.lib.pw_align(self.handle, flags, int(start_cap), ctypes.byref(info))
+        _check(self.lib, self.handle, rc, "pw_align")
+        self.last_info = info
+        return info
+
+    def pair_max(self):
+        out = np.zeros((self.n_queries, self.n_targets), dtype=np.float32)
+        _check(self.lib, self.handle, self.lib.pw_get_pair_max(self.handle, _ptr(out), out.size), "pw_get_pair_max")
+        return out
+
+    def hits(self):
+        """Returns (structured array of hits in HitList order, string bytes)."""
+        n = int(self.last_info.hits) if self.last_info is not None else 0
+        nb = int(self.last_info.string_bytes) if self.last_info is not None else 0
+        hits = np.zeros(n, dtype=HIT_DTYPE)
+        strbuf = np.zeros(max(nb, 1), dtype=np.uint8)
+        _check(self.lib, self.handle, self.lib.pw_get_hits(self.handle, _ptr(hits), n, _ptr(strbuf), nb),
+               "pw_get_hits")
+        return hits, strbuf[:nb].tobytes()
+
+    def starting_points(self):
+        n = ctypes.c_int64()
+        _check(self.lib, self.handle, self.lib.pw_get_starting_points(self.handle, None, 0, ctypes.byref(n)),
+               "pw_get_starting_points")
+        out = np.zeros(n.value, dtype=START_DTYPE)
+        _check(self.lib, self.handle,
+               self.lib.pw_get_starting_points(self.handle, _ptr(out), n.value, ctypes.byref(n)),
+               "pw_get_starting_points")
+        return out
+
+    def launch_count(self):
+        n = ctypes.c_int64()
+        _check(self.lib, self.handle, self.lib.pw_last_launch_count(self.handle, ctypes.byref(n)),
+               "pw_last_launch_count")
+        return n.value

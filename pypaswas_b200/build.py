@@ -1,0 +1,40 @@
+"""Builds libpaswas_b200.so in-tree with nvcc for sm_100a (B200).
+
+Usage: python -m pypaswas_b200.build [--force]
+"""
+import os
+import subprocess
+import sys
+
+PACKAGE_DIR = os.path.dirname(os.path.abspath(__file__))
+REPO_DIR = os.path.dirname(PACKAGE_DIR)
+CSRC = os.path.join(PACKAGE_DIR, "csrc")
+SOURCES = [os.path.join(CSRC, "engine.cu")]
+DEPENDS = SOURCES + [os.path.join(CSRC, f) for f in ("pw_device.cuh", "pw_kernels.cuh")] + [
+    os.path.join(REPO_DIR, "include", "paswas_b200.h")]
+LIBRARY = os.path.join(PACKAGE_DIR, "libpaswas_b200.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17", "-lineinfo",
+              "-Xcompiler", "-fPIC", "-shared", "-Xptxas", "-O3"]
+
+
+def up_to_date():
+    if not os.path.exists(LIBRARY):
+        return False
+    t = os.path.getmtime(LIBRARY)
+    return all(os.path.getmtime(p) <= t for p in DEPENDS if os.path.exists(p))
+
+
+def build(force=False, verbose=False):
+    """Compiles the engine if any source changed; returns the library path."""
+    if not force and up_to_date():
+        return LIBRARY
+    tmp = LIBRARY + ".tmp"
+    cmd = [NVCC] + NVCC_FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-o", tmp] + SOURCES
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, LIBRARY)
+    return LIBRARY
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))

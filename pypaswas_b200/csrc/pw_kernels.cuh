@@ -1,0 +1,746 @@
+// pw_kernels.cuh -- the engine's kernels.
+//
+//   score_kernel     pair maxima (calculateScore / calculateScoreAffineGap,
+//                    default_main.cu:130-303 / 317-561, max chain :169-180,297)
+//   dir_kernel       the same sweep again for pairs whose maximum reached
+//                    MINIMUM_SCORE, writing one code byte per cell (direction,
+//                    stop flag, candidate flag) and the pair's candidate list
+//   collect_kernel   starting points (traceback / tracebackAffineGap,
+//                    default_main.cu:566-714 / 802-909): a candidate is a start
+//                    unless another candidate's marking chain reaches it
+//   walk_kernel      the host walk of SmithWaterman._print_alignments
+//                    (SmithWaterman.py:699-838), one thread per pair
+//   ops_kernel       writes the column operations of every kept hit
+#pragma once
+#include "pw_device.cuh"
+
+namespace pw {
+
+// ------------------------------------------------------------------ profile
+// Strip profile: for strip rows [y0, y0+S) and compact query residue a,
+// word (g, a) packs the scores of rows y0+4g .. y0+4g+3 (int8 each; rows past
+// the target end get the padding score).  fp32 path: one float4 per (g, a).
+template <typename T, int S>
+__device__ __forceinline__ void build_profile(void* prof, const int8_t* cmat_i8, const float* cmat_f,
+                                              const uint8_t* tres, int y0, int lt, int alpha1, int dim,
+                                              int lane) {
+    const int n = (S / 4) * alpha1;
+    for (int idx = lane; idx < n; idx += kWarp) {
+        const int g = idx / alpha1, a = idx % alpha1;
+        if constexpr (sizeof(T) == 4 && T(0.5f) == T(0)) {  // int path
+            uint32_t w = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int y = y0 + 4 * g + k;
+                const int8_t s = y < lt ? cmat_i8[a * dim + tres[y]] : (int8_t)-128;
+                w |= (uint32_t)(uint8_t)s << (8 * k);
+            }
+            ((uint32_t*)prof)[idx] = w;
+        } else {
+            float4 w;
+            float* wp = &w.x;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int y = y0 + 4 * g + k;
+                wp[k] = y < lt ? cmat_f[a * dim + tres[y]] : -1.0e30f;
+            }
+            ((float4*)prof)[idx] = w;
+        }
+    }
+}
+
+template <typename T>
+struct Prof4 {
+    T s[4];
+};
+
+template <typename T>
+__device__ __forceinline__ Prof4<T> load_prof(const void* prof, int g, int alpha1, int a) {
+    Prof4<T> p;
+    if constexpr (T(0.5f) == T(0)) {
+        const uint32_t w = ((const uint32_t*)prof)[g * alpha1 + a];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) p.s[k] = sext_byte(w, k);
+    } else {
+        const float4 w = ((const float4*)prof)[g * alpha1 + a];
+        p.s[0] = w.x;
+        p.s[1] = w.y;
+        p.s[2] = w.z;
+        p.s[3] = w.w;
+    }
+    return p;
+}
+
+template <typename T>
+__device__ __forceinline__ T relu_addmax(T a, T b, T c) {  // max(a + b, c, 0)
+    if constexpr (T(0.5f) == T(0))
+        return addmax_relu(a, b, c);
+    else
+        return fmaxf(fmaxf(a + b, c), 0.0f);
+}
+
+template <typename T>
+__device__ __forceinline__ T negT() {
+    if constexpr (T(0.5f) == T(0))
+        return (T)kNeg;
+    else
+        return (T)-1.0e10f;
+}
+
+// Boundary element handed from one strip to the next (row y0 + S - 1).
+template <typename T>
+struct Bnd {
+    T m, i, b, pad;
+};
+
+// Per-lane context of one (query, target) pair.
+struct LaneCtx {
+    const uint8_t* qc;  // compact query codes, padded to a multiple of 4 with the pad code
+    int lq, lq4;        // length and length rounded up to 4
+    int lt;
+    int y0;
+    bool has_up, has_down;
+};
+
+// ------------------------------------------------------------ score sweeps
+template <typename T, int S, bool AFFINE>
+__device__ __forceinline__ void sweep_score(const LaneCtx& c, const void* prof, int alpha1, T gap, T ext, T ge,
+                                            Bnd<T>* bnd, T& mx) {
+    if constexpr (!AFFINE) {
+        T H[S];
+#pragma unroll
+        for (int r = 0; r < S; ++r) H[r] = 0;
+        T hb_prev = 0;
+        for (int x4 = 0; x4 < c.lq4; x4 += 4) {
+            const uint32_t cw = *(const uint32_t*)(c.qc + x4);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int x = x4 + j;
+                const int a = (cw >> (8 * j)) & 0xff;
+                T up = c.has_up ? bnd[(int64_t)x * kWarp].m : T(0);
+                T diag = hb_prev;
+                hb_prev = up;
+#pragma unroll
+                for (int g = 0; g < S / 4; ++g) {
+                    const Prof4<T> p = load_prof<T>(prof, g, alpha1, a);
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const int r = 4 * g + k;
+                        const T left = H[r];
+                        T h = addmax(left, gap, diag + p.s[k]);
+                        h = relu_addmax(up, gap, h);
+                        diag = left;
+                        H[r] = h;
+                        up = h;
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < S; r += 2) mx = max3(mx, H[r], H[r + 1]);
+                if (c.has_down) bnd[(int64_t)x * kWarp].m = H[S - 1];
+            }
+        }
+    } else {
+        T Ml[S], Jl[S], Bl[S];
+        const T neg = negT<T>();
+#pragma unroll
+        for (int r = 0; r < S; ++r) {
+            Ml[r] = 0;
+            Jl[r] = neg;
+            Bl[r] = 0;
+        }
+        T bb_prev = 0;
+        for (int x4 = 0; x4 < c.lq4; x4 += 4) {
+            const uint32_t cw = *(const uint32_t*)(c.qc + x4);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int x = x4 + j;
+                const int a = (cw >> (8 * j)) & 0xff;
+                T mup = 0, iup = neg, bup = 0;
+                if (c.has_up) {
+                    const Bnd<T> b = bnd[(int64_t)x * kWarp];
+                    mup = b.m;
+                    iup = b.i;
+                    bup = b.b;
+                }
+                T bdiag = bb_prev;
+                bb_prev = bup;
+#pragma unroll
+                for (int g = 0; g < S / 4; ++g) {
+                    const Prof4<T> p = load_prof<T>(prof, g, alpha1, a);
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const int r = 4 * g + k;
+                        const T m = relu_addmax(bdiag, p.s[k], neg);
+                        const T i = addmax(iup, ext, mup + ge);
+                        const T jj = addmax(Jl[r], ext, Ml[r] + ge);
+                        const T b = max3(m, i, jj);
+                        bdiag = Bl[r];
+                        Ml[r] = m;
+                        Jl[r] = jj;
+                        Bl[r] = b;
+                        mup = m;
+                        iup = i;
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < S; r += 2) mx = max3(mx, Bl[r], Bl[r + 1]);
+                if (c.has_down) {
+                    Bnd<T> b;
+                    b.m = mup;
+                    b.i = iup;
+                    b.b = Bl[S - 1];
+                    b.pad = 0;
+                    bnd[(int64_t)x * kWarp] = b;
+                }
+            }
+        }
+    }
+}
+
+// --------------------------------------------------------- direction sweeps
+// Same recurrence as sweep_score; additionally classifies every cell like the
+// reference and records starting-point candidates.
+//   linear (default_main.cu:259-271): direction LEFT if H == left+gap, else UP
+//     if H == up+gap, else UPPER_LEFT; NO when H == 0.  Stop flag: UPPER_LEFT
+//     with a zero diagonal predecessor inside the matrix (:632-659).
+//     Candidate: UPPER_LEFT and H >= threshold (:609).
+//   affine (:467-526): best B = max(M, I, J); source MAIN if B == M, else I if
+//     B == I, else J; NO when B == 0.  Stop flag: MAIN with M(x-1, y-1) == 0
+//     inside the matrix (:724-751).  Candidate: MAIN and M >= threshold (:850).
+template <typename T, int S, bool AFFINE>
+__device__ __forceinline__ void sweep_dirs(const LaneCtx& c, const void* prof, int alpha1, T gap, T ext, T ge,
+                                           Bnd<T>* bnd, uint8_t* codes, int lane, int xmax4, T thr, Cand* cand,
+                                           int cand_cap, int& n_cand) {
+    uint4* out = (uint4*)codes;
+    if constexpr (!AFFINE) {
+        T H[S];
+#pragma unroll
+        for (int r = 0; r < S; ++r) H[r] = 0;
+        T hb_prev = 0;
+        for (int x4 = 0; x4 < c.lq4; x4 += 4) {
+            const uint32_t cw = *(const uint32_t*)(c.qc + x4);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int x = x4 + j;
+                const int a = (cw >> (8 * j)) & 0xff;
+                const bool xin = x > 0;
+                T up = c.has_up ? bnd[(int64_t)x * kWarp].m : T(0);
+                T diag = hb_prev;
+                hb_prev = up;
+                uint32_t words[S / 4];
+#pragma unroll
+                for (int g = 0; g < S / 4; ++g) {
+                    const Prof4<T> p = load_prof<T>(prof, g, alpha1, a);
+                    uint32_t w = 0;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const int r = 4 * g + k;
+                        const T left = H[r];
+                        const T ls = left + gap, us = up + gap, ds = diag + p.s[k];
+                        T h = addmax(left, gap, ds);
+                        h = relu_addmax(up, gap, h);
+                        uint32_t code = h == ls ? kLeft : (h == us ? kUp : kUL);
+                        code = h > T(0) ? code : kNo;
+                        const bool ul = code == kUL;
+                        const bool yin = (r > 0) || c.has_up;
+                        const bool stop = ul && xin && yin && diag == T(0);
+                        const bool cnd = ul && h >= thr;
+                        code |= stop ? kStopFlag : 0u;
+                        if (cnd) {
+                            const int y = c.y0 + r;
+                            if (x < c.lq && y < c.lt) {
+                                code |= kCand;
+                                if (n_cand < cand_cap) {
+                                    Cand cc;
+                                    cc.x = x;
+                                    cc.y = y;
+                                    cc.score_i = (int32_t)h;
+                                    cc.score_f = (float)h;
+                                    cand[n_cand] = cc;
+                                }
+                                ++n_cand;
+                            }
+                        }
+                        w |= code << (8 * k);
+                        diag = left;
+                        H[r] = h;
+                        up = h;
+                    }
+                    words[g] = w;
+                }
+#pragma unroll
+                for (int q = 0; q < S / 16; ++q)
+                    out[((int64_t)x * (S / 16) + q) * kWarp + lane] =
+                        make_uint4(words[4 * q], words[4 * q + 1], words[4 * q + 2], words[4 * q + 3]);
+                if (c.has_down) bnd[(int64_t)x * kWarp].m = H[S - 1];
+            }
+        }
+    } else {
+        T Ml[S], Jl[S], Bl[S];
+        const T neg = negT<T>();
+#pragma unroll
+        for (int r = 0; r < S; ++r) {
+            Ml[r] = 0;
+            Jl[r] = neg;
+            Bl[r] = 0;
+        }
+        T bb_prev = 0, bm_prev = 0;
+        for (int x4 = 0; x4 < c.lq4; x4 += 4) {
+            const uint32_t cw = *(const uint32_t*)(c.qc + x4);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int x = x4 + j;
+                const int a = (cw >> (8 * j)) & 0xff;
+                const bool xin = x > 0;
+                T mup = 0, iup = neg, bup = 0;
+                if (c.has_up) {
+                    const Bnd<T> b = bnd[(int64_t)x * kWarp];
+                    mup = b.m;
+                    iup = b.i;
+                    bup = b.b;
+                }
+                T bdiag = bb_prev, mdiag = bm_prev;
+                bb_prev = bup;
+                bm_prev = mup;
+                uint32_t words[S / 4];
+#pragma unroll
+                for (int g = 0; g < S / 4; ++g) {
+                    const Prof4<T> p = load_prof<T>(prof, g, alpha1, a);
+                    uint32_t w = 0;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const int r = 4 * g + k;
+                        const T m = relu_addmax(bdiag, p.s[k], neg);
+                        const T i = addmax(iup, ext, mup + ge);
+                        const T jj = addmax(Jl[r], ext, Ml[r] + ge);
+                        const T b = max3(m, i, jj);
+                        uint32_t code = b == m ? kUL : (b == i ? kUp : kLeft);
+                        code = b > T(0) ? code : kNo;
+                        const bool main_src = code == kUL;
+                        const bool yin = (r > 0) || c.has_up;
+                        const bool stop = main_src && xin && yin && mdiag == T(0);
+                        const bool cnd = main_src && m >= thr;
+                        code |= stop ? kStopFlag : 0u;
+                        if (cnd) {
+                            const int y = c.y0 + r;
+                            if (x < c.lq && y < c.lt) {
+                                code |= kCand;
+                                if (n_cand < cand_cap) {
+                                    Cand cc;
+                                    cc.x = x;
+                                    cc.y = y;
+                                    cc.score_i = (int32_t)m;
+                                    cc.score_f = (float)m;
+                                    cand[n_cand] = cc;
+                                }
+                                ++n_cand;
+                            }
+                        }
+                        w |= code << (8 * k);
+                        bdiag = Bl[r];
+                        mdiag = Ml[r];
+                        Ml[r] = m;
+                        Jl[r] = jj;
+                        Bl[r] = b;
+                        mup = m;
+                        iup = i;
+                    }
+                    words[g] = w;
+                }
+#pragma unroll
+                for (int q = 0; q < S / 16; ++q)
+                    out[((int64_t)x * (S / 16) + q) * kWarp + lane] =
+                        make_uint4(words[4 * q], words[4 * q + 1], words[4 * q + 2], words[4 * q + 3]);
+                if (c.has_down) {
+                    Bnd<T> b;
+                    b.m = mup;
+                    b.i = iup;
+                    b.b = Bl[S - 1];
+                    b.pad = 0;
+                    bnd[(int64_t)x * kWarp] = b;
+                }
+            }
+        }
+    }
+    (void)xmax4;
+}
+
+// Sequences on the device.
+struct SeqSet {
+    const uint8_t* codes;    // query: compact codes / target: matrix residue index
+    const int64_t* code_off; // 16-byte aligned offsets into codes
+    const uint8_t* raw;      // upper-cased residues as given
+    const int64_t* raw_off;
+    const int32_t* len;
+    const int32_t* key;      // id equality key
+};
+
+struct KernelArgs {
+    const WorkItem* items;
+    int n_items;
+    int* item_counter;
+    SeqSet q, t;
+    const int32_t* q_order;  // sorted position -> query index
+    const int8_t* cmat_i8;   // [(alpha+1) * dim]
+    const float* cmat_f;
+    ScoreParams P;
+    float* pair_max;         // [nq * nt]
+    int nt;
+    void* bnd_pool;
+    int64_t bnd_slot_elems;  // elements per warp slot (xmax4 * 32)
+    // phase 2
+    uint8_t* codes;
+    PairMeta* metas;
+    Cand* cands;
+    const int32_t* cand_base;  // per pair slot: first candidate
+    const int32_t* cand_cap;   // per pair slot: capacity
+    unsigned long long* launches;  // diagnostic counter (unused on device)
+};
+
+template <typename T>
+__device__ __forceinline__ T from_f(float v) {
+    if constexpr (T(0.5f) == T(0))
+        return (T)v;
+    else
+        return v;
+}
+
+// Persistent kernel over work items: one warp per item, dynamic scheduling.
+// PHASE 1 writes pair maxima; PHASE 2 writes cell codes and candidates.
+template <typename T, int S, bool AFFINE, bool MULTI, int PHASE>
+__global__ void __launch_bounds__(128) sweep_kernel(KernelArgs A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int alpha1 = A.P.alpha + 1;
+    const int prof_bytes = (S / 4) * alpha1 * (int)(T(0.5f) == T(0) ? 4 : 16);
+    void* prof = smem + wib * ((prof_bytes + 15) & ~15);
+    const int64_t warp_global = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
+    Bnd<T>* bnd_slot = MULTI ? (Bnd<T>*)A.bnd_pool + warp_global * A.bnd_slot_elems + lane : nullptr;
+    const T gap = A.P.is_float ? from_f<T>(A.P.gap_f) : (T)A.P.gap_i;
+    const T ext = A.P.is_float ? from_f<T>(A.P.ext_f) : (T)A.P.ext_i;
+    const T ge = A.P.is_float ? from_f<T>(A.P.ge_f) : (T)A.P.ge_i;
+
+    for (;;) {
+        int it = 0;
+        if (lane == 0) it = atomicAdd(A.item_counter, 1);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it >= A.n_items) break;
+        const WorkItem W = A.items[it];
+        const int t = W.target;
+        const int lt = A.t.len[t];
+        const bool active = lane < W.lanes;
+        const int q = active ? A.q_order[W.first + lane] : 0;
+        LaneCtx c;
+        c.qc = A.q.codes + A.q.code_off[q];
+        c.lq = active ? A.q.len[q] : 0;
+        c.lq4 = (c.lq + 3) & ~3;
+        c.lt = lt;
+        const uint8_t* tres = A.t.codes + A.t.code_off[t];
+        const int nstrips = MULTI ? (lt + S - 1) / S : 1;
+        T mx = 0;
+        // phase 2 per-pair state
+        T thr = 0;
+        int n_cand = 0;
+        Cand* cand = nullptr;
+        int cap = 0;
+        int64_t pslot = W.pair_base + lane;
+        if (PHASE == 2 && active) {
+            const float maxf = A.pair_max[(int64_t)q * A.nt + t];
+            const int mn = c.lq < lt ? c.lq : lt;
+            // maxPossibleScore, SmithWatermanCuda.py:269-275 (double, stored as fp32)
+            const float pos = (float)(A.P.highest * (double)mn * A.P.filter_factor);
+            const float llm = __fmul_rn(A.P.lower_limit, maxf);
+            const float thf = fmaxf(llm, pos);
+            if constexpr (T(0.5f) == T(0)) {
+                float tc = ceilf(thf);
+                tc = fminf(fmaxf(tc, -1.0e9f), 1.0e9f);
+                thr = (T)tc;
+            } else {
+                thr = thf;
+            }
+            cand = A.cands + A.cand_base[pslot];
+            cap = A.cand_cap[pslot];
+            PairMeta& pm = A.metas[pslot];
+            pm.query = q;
+            pm.target = t;
+            pm.item = W.index;
+            pm.lane = lane;
+            pm.thr_f = thf;
+            pm.thr_i = (int32_t)(T(0.5f) == T(0) ? (float)thr : 0.0f);
+            pm.max_f = maxf;
+        }
+        const int xmax4 = (W.xmax + 3) & ~3;
+        for (int s = 0; s < nstrips; ++s) {
+            c.y0 = s * S;
+            c.has_up = s > 0;
+            c.has_down = s + 1 < nstrips;
+            __syncwarp();
+            build_profile<T, S>(prof, A.cmat_i8, A.cmat_f, tres, c.y0, lt, alpha1, A.P.dim, lane);
+            __syncwarp();
+            if (active) {
+                if (PHASE == 1) {
+                    sweep_score<T, S, AFFINE>(c, prof, alpha1, gap, ext, ge, bnd_slot, mx);
+                } else {
+                    uint8_t* codes = A.codes + W.dir_base + (int64_t)s * xmax4 * S * kWarp;
+                    sweep_dirs<T, S, AFFINE>(c, prof, alpha1, gap, ext, ge, bnd_slot, codes, lane, xmax4, thr,
+                                             cand, cap, n_cand);
+                }
+            }
+        }
+        if (active) {
+            if (PHASE == 1)
+                A.pair_max[(int64_t)q * A.nt + t] = (float)mx;
+            else
+                A.metas[pslot].n_cand = n_cand;
+        }
+    }
+}
+
+// ------------------------------------------------------------ traceback side
+struct TraceArgs {
+    const PairMeta* metas;
+    int n_pairs;
+    const WorkItem* items;
+    uint8_t* codes;
+    Cand* cands;
+    const int32_t* cand_base;
+    int32_t* n_starts;       // per pair: starting points (after collect)
+    SeqSet q, t;
+    ScoreParams P;
+    const uint8_t* allowed;  // per candidate slot: walk this start (start cap); null = all
+    DevHit* hits;
+    int* hit_count;
+    int max_hits;
+    char* ops;
+};
+
+struct PairView {
+    uint8_t* base;
+    int S, lane, xmax4, lq, lt;
+    __device__ __forceinline__ uint8_t& at(int x, int y) const {
+        return base[cell_offset_rt(S, x, y, lane, xmax4)];
+    }
+};
+
+__device__ __forceinline__ PairView pair_view(const TraceArgs& A, const PairMeta& pm) {
+    PairView v;
+    const WorkItem W = A.items[pm.item];
+    v.base = A.codes + W.dir_base;
+    v.S = W.S;
+    v.lane = pm.lane;
+    v.xmax4 = (W.xmax + 3) & ~3;
+    v.lq = A.q.len[pm.query];
+    v.lt = A.t.len[pm.target];
+    return v;
+}
+
+// Emission rank of a starting point inside its pair: the reference's reverse
+// sweep emits by block anti-diagonal descending, block x descending, cell
+// anti-diagonal descending inside the 8x8 block, then linear thread index
+// (thread y ascending).  Smaller key = emitted earlier.
+__host__ __device__ __forceinline__ uint64_t emission_key(int x, int y) {
+    const uint32_t bx = (uint32_t)x >> 3, by = (uint32_t)y >> 3;
+    const uint32_t d = bx + by, i = (x & 7) + (y & 7), ty = y & 7;
+    // descending fields are stored complemented
+    return ((uint64_t)(0xFFFFFu - d) << 40) | ((uint64_t)(0xFFFFFu - bx) << 20) |
+           ((uint64_t)(15u - i) << 4) | ty;
+}
+
+template <bool AFFINE>
+__global__ void collect_kernel(TraceArgs A) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= A.n_pairs) return;
+    const PairMeta pm = A.metas[p];
+    Cand* cl = A.cands + A.cand_base[p];
+    const int n = pm.n_cand;
+    PairView v = pair_view(A, pm);
+    // marking chains: the nearest candidate up a candidate's chain is covered
+    for (int k = 0; k < n; ++k) {
+        int x = cl[k].x - 1, y = cl[k].y - 1;
+        while (x >= 0 && y >= 0) {
+            uint8_t& cd = v.at(x, y);
+            const int d = cd & 3;
+            if (cd & kCand) {
+                cd |= kCovered;
+                break;
+            }
+            if (AFFINE) {
+                if (d != kUL) break;
+                --x;
+                --y;
+            } else {
+                if (d == kNo) break;
+                if (d == kUL) {
+                    --x;
+                    --y;
+                } else if (d == kUp) {
+                    --y;
+                } else {
+                    --x;
+                }
+            }
+        }
+    }
+    // keep uncovered candidates, then order them for the walk: ascending score,
+    // then emission order (SmithWaterman.py:699 is a stable sort)
+    int m = 0;
+    for (int k = 0; k < n; ++k) {
+        const Cand cc = cl[k];
+        if (!(v.at(cc.x, cc.y) & kCovered)) cl[m++] = cc;
+    }
+    for (int k = 1; k < m; ++k) {
+        const Cand key = cl[k];
+        const uint64_t ek = emission_key(key.x, key.y);
+        int j = k - 1;
+        while (j >= 0) {
+            const Cand o = cl[j];
+            const bool after = o.score_f > key.score_f ||
+                               (o.score_f == key.score_f && emission_key(o.x, o.y) > ek);
+            if (!after) break;
+            cl[j + 1] = o;
+            --j;
+        }
+        cl[j + 1] = key;
+    }
+    A.n_starts[p] = m;
+}
+
+// Affine stop rule: a MAIN cell with a zero diagonal predecessor becomes STOP
+// only if it is marked, i.e. a candidate lies on its diagonal run of MAIN cells
+// (itself or further down-right).
+__device__ __forceinline__ bool run_has_candidate(const PairView& v, int x, int y) {
+    while (x < v.lq && y < v.lt) {
+        const uint8_t cd = v.at(x, y);
+        if (cd & kCand) return true;
+        if ((cd & 3) != kUL) return false;
+        ++x;
+        ++y;
+    }
+    return false;
+}
+
+constexpr int kStopDir = 64, kInAlignment = 96;
+
+template <bool AFFINE>
+__device__ __forceinline__ int walk_direction(const PairView& v, int x, int y) {
+    const uint8_t cd = v.at(x, y);
+    if (cd & kVisited) return kInAlignment;
+    const int d = cd & 3;
+    if (d == kUL && (cd & kStopFlag)) {
+        if (!AFFINE || run_has_candidate(v, x, y)) return kStopDir;
+    }
+    return d;  // 0: never written in the reference's zero-copy buffer
+}
+
+__device__ __forceinline__ bool same_residue(uint8_t a, uint8_t b) {
+    // str.lower() equality of single characters (SmithWaterman.py:771)
+    const bool la = (a >= 'A' && a <= 'Z') || (a >= 'a' && a <= 'z');
+    return la ? ((a | 0x20) == (b | 0x20)) : a == b;
+}
+
+template <bool AFFINE>
+__global__ void walk_kernel(TraceArgs A) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= A.n_pairs) return;
+    const PairMeta pm = A.metas[p];
+    const Cand* cl = A.cands + A.cand_base[p];
+    const int m = A.n_starts[p];
+    PairView v = pair_view(A, pm);
+    const uint8_t* qs = A.q.raw + A.q.raw_off[pm.query];
+    const uint8_t* ts = A.t.raw + A.t.raw_off[pm.target];
+    const bool same_id = A.q.key[pm.query] == A.t.key[pm.target];
+    for (int k = 0; k < m; ++k) {
+        if (A.allowed && !A.allowed[A.cand_base[p] + k]) continue;
+        const Cand st = cl[k];
+        int x = st.x, y = st.y;
+        int dir = walk_direction<AFFINE>(v, x, y);
+        bool show = true;
+        if (same_id) {  // SmithWaterman.py:752-755
+            dir = kStopDir;
+            show = false;
+        }
+        if ((double)st.score_f < A.P.host_minimum) show = false;  // :758-759
+        int s_start = x + 1, t_start = y + 1, ncols = 0, mt = 0, mm = 0;
+        while (show && x >= 0 && y >= 0 && dir != kStopDir && dir != 32) {  // :761
+            dir = walk_direction<AFFINE>(v, x, y);
+            v.at(x, y) |= kVisited;
+            if (dir == kInAlignment) {
+                show = false;
+            } else if (dir == kUL || dir == kStopDir) {
+                if (same_residue(ts[y], qs[x]))
+                    ++mt;
+                else
+                    ++mm;
+                --s_start;
+                --t_start;
+                ++ncols;
+                if (dir == kUL) {
+                    --x;
+                    --y;
+                }
+            } else if (dir == kLeft) {
+                --s_start;
+                ++ncols;
+                --x;
+            } else if (dir == kUp) {
+                --t_start;
+                ++ncols;
+                --y;
+            } else {
+                x = -1;
+            }
+        }
+        if (show) {
+            const int h = atomicAdd(A.hit_count, 1);
+            if (h < A.max_hits) {
+                DevHit o;
+                o.pair = p;
+                o.query = pm.query;
+                o.target = pm.target;
+                o.s_start = s_start;
+                o.s_end = st.x;
+                o.t_start = t_start;
+                o.t_end = st.y;
+                o.score = st.score_f;
+                o.matches = mt;
+                o.mismatches = mm;
+                o.n_cols = ncols;
+                o.end_x = st.x;
+                o.end_y = st.y;
+                o.ops_offset = -1;
+                A.hits[h] = o;
+            }
+        }
+    }
+}
+
+// Column operations of each hit, in alignment order: 'M' both residues,
+// 'I' query residue against a gap, 'D' target residue against a gap.
+__global__ void ops_kernel(TraceArgs A, const DevHit* hits, int n_hits) {
+    const int h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= n_hits) return;
+    const DevHit H = hits[h];
+    const PairMeta pm = A.metas[H.pair];
+    PairView v = pair_view(A, pm);
+    int x = H.end_x, y = H.end_y;
+    char* o = A.ops + H.ops_offset;
+    for (int k = 0; k < H.n_cols; ++k) {
+        const int d = v.at(x, y) & 3;
+        char op;
+        if (d == kLeft) {
+            op = 'I';
+            --x;
+        } else if (d == kUp) {
+            op = 'D';
+            --y;
+        } else {
+            op = 'M';
+            --x;
+            --y;
+        }
+        o[H.n_cols - 1 - k] = op;
+    }
+}
+
+}  // namespace pw

@@ -1,0 +1,88 @@
+"""Engine (CUDA, through the C ABI) against the CPU oracle on seeded cases.
+
+Bit-exact: pair maxima, every hit's coordinates, score, match counts and the
+three alignment strings, in HitList order."""
+import numpy as np
+import pytest
+
+import cases
+from engine_helpers import run_engine
+
+pytestmark = pytest.mark.gpu
+
+KINDS = ["dna", "protein", "dna_ambiguous", "dna_float"]
+
+
+def _oracle(oracle_mod, queries, targets, score, settings, q_keys=None, t_keys=None):
+    p = cases.oracle_params(oracle_mod, score)
+    pos = cases.pos_scores(score, settings, queries, targets)
+    return oracle_mod.run(p, queries, targets, pos, float(settings.minimum_score), q_keys, t_keys)
+
+
+@pytest.mark.parametrize("seed", range(24))
+def test_random_cases_bit_exact(engine_lib, oracle_mod, seed):
+    kind = KINDS[seed % len(KINDS)]
+    queries, targets, score, st = cases.make_case(1000 + seed, kind)
+    o = _oracle(oracle_mod, queries, targets, score, st)
+    pm, hits, info, launches = run_engine(engine_lib, queries, targets, score, st)
+    assert launches > 0
+    np.testing.assert_array_equal(pm, o["pair_max"])
+    assert hits == o["hits"]
+
+
+def test_same_id_pairs_are_skipped(engine_lib, oracle_mod):
+    queries, targets, score, st = cases.make_case(77, "dna")
+    q_keys = np.arange(len(queries))
+    t_keys = np.array([0] + [len(queries) + i for i in range(1, len(targets))])  # target 0 shares query 0's id
+    o = _oracle(oracle_mod, queries, targets, score, st, q_keys, t_keys)
+    pm, hits, _, _ = run_engine(engine_lib, queries, targets, score, st, q_keys, t_keys)
+    assert hits == o["hits"]
+    assert not any(h["query"] == 0 and h["target"] == 0 for h in hits)
+
+
+def test_score_only_matches_full_run(engine_lib, oracle_mod):
+    queries, targets, score, st = cases.make_case(5, "protein")
+    pm, hits, info, _ = run_engine(engine_lib, queries, targets, score, st, score_only=True)
+    assert hits == []
+    np.testing.assert_array_equal(pm, oracle_mod.pair_max(cases.oracle_params(oracle_mod, score), queries, targets))
+
+
+def test_run_is_deterministic(engine_lib):
+    queries, targets, score, st = cases.make_case(11, "dna")
+    a = run_engine(engine_lib, queries, targets, score, st)
+    b = run_engine(engine_lib, queries, targets, score, st)
+    np.testing.assert_array_equal(a[0], b[0])
+    assert a[1] == b[1]
+
+
+def test_edge_lengths(engine_lib, oracle_mod):
+    # single residues, lengths around strip and lane-group boundaries
+    rng = np.random.default_rng(3)
+    lens_q = [1, 2, 3, 4, 5, 7, 8, 9, 15, 16, 17, 31, 32, 33, 63, 64, 65]
+    lens_t = [1, 4, 16, 17, 32, 33, 64, 65, 97]
+    q = ["".join("ACGT"[i] for i in rng.integers(0, 4, n)) for n in lens_q]
+    t = ["".join("ACGT"[i] for i in rng.integers(0, 4, n)) for n in lens_t]
+    t[3] = q[-1][:17]
+    for aff in ("0", "-1"):
+        st = cases.Settings(minimum_score="2", lower_limit_score="0.5", gap_extension=aff)
+        from pypaswas_b200 import scores
+        score = scores.make_score(st)
+        o = _oracle(oracle_mod, q, t, score, st)
+        pm, hits, _, _ = run_engine(engine_lib, q, t, score, st)
+        np.testing.assert_array_equal(pm, o["pair_max"])
+        assert hits == o["hits"]
+
+
+def test_many_pairs_pair_max(engine_lib, oracle_mod):
+    # 600 x 40 pairs: several warps per target and all strip classes
+    rng = np.random.default_rng(9)
+    q = ["".join("ACGT"[i] for i in rng.integers(0, 4, int(rng.integers(1, 160)))) for _ in range(600)]
+    t = ["".join("ACGT"[i] for i in rng.integers(0, 4, int(rng.integers(1, 120)))) for _ in range(40)]
+    for aff in ("0", "-1"):
+        st = cases.Settings(minimum_score="9", gap_extension=aff)
+        from pypaswas_b200 import scores
+        score = scores.make_score(st)
+        o = _oracle(oracle_mod, q, t, score, st)
+        pm, hits, _, _ = run_engine(engine_lib, q, t, score, st)
+        np.testing.assert_array_equal(pm, o["pair_max"])
+        assert hits == o["hits"]
