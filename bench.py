@@ -1,0 +1,340 @@
+#!/usr/bin/env python
+"""GCUPS of the Smith-Waterman hot path on B200.
+
+Workload (the configuration the metric is quoted on): protein, affine gap,
+batched uneven lengths -- 200 queries (log-normal, median 350 aa, 100-1000)
+against 2,000 targets (50-2,000 aa), BLOSUM62, gap open -11 / extension -1,
+10% of pairs sharing a planted 150-aa domain at 40% identity: 400,000 pairs,
+all-vs-all, full path (score sweep, starting points, traceback walk, hits).
+Synthetic, seeded (pypaswas_b200.workloads.config2).
+
+One "step" = one pw_align over all 400,000 pairs with the sequences resident
+in HBM.  `e2e` repeats the step through the public driver
+(SmithWatermanB200.align_sequences) from host sequence records, host<->device
+copies and Hit construction included.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun (N > 1) every rank aligns its own replica of the workload
+(pairs are independent; no collective on the data path): weak scaling.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+import numpy as np  # noqa: E402
+
+# algorithmic operations per cell (add and max counted separately) of the
+# recurrences: linear/affine, score only / with direction classification
+OPS_PER_CELL = {("linear", "score"): 5, ("linear", "dirs"): 8, ("affine", "score"): 10, ("affine", "dirs"): 14}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), \
+        int(os.environ.get("LOCAL_RANK", "0"))
+
+
+class ClockSampler(object):
+    """nvidia-smi clock / throttle samples while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.QUERY,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def load_traffic():
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+    try:
+        with open(os.path.join(REPO, "profiles", "traffic.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def engine_for(workload, device):
+    from pypaswas_b200 import _native, scores
+    from pypaswas_b200.smith_waterman import configure_engine, id_keys
+    score = scores.make_score(workload.settings)
+    e = _native.Engine(device)
+    configure_engine(e, score, workload.settings)
+    qk, tk = id_keys([i for i, _ in workload.queries], [i for i, _ in workload.targets])
+    e.set_queries([s for _, s in workload.queries], qk)
+    e.set_targets([s for _, s in workload.targets], tk)
+    return e, score
+
+
+def cpu_baseline(workload, score, seconds, processes=1):
+    """The oracle (CPU restatement of the reference path) on a bounded sample of
+    the workload: queries x targets taken evenly from the length-sorted lists,
+    grown until the estimated run time reaches `seconds`."""
+    import multiprocessing as mp
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle
+    oracle.build()
+    q_all = [s.decode() for _, s in workload.queries]
+    t_all = [s.decode() for _, s in workload.targets]
+    rate = 24e6 * max(1, processes)  # cells/s estimate of the oracle, refined below
+    nq = min(len(q_all), 10)
+    nt = max(1, int(seconds * rate / (sum(map(len, q_all[::max(1, len(q_all) // nq)][:nq])) * 1025)))
+    nt = min(nt, len(t_all))
+    qs = q_all[::max(1, len(q_all) // nq)][:nq]
+    ts = t_all[::max(1, len(t_all) // nt)][:nt]
+    cells = sum(map(len, qs)) * sum(map(len, ts))
+    args = _oracle_args(score, workload.settings)
+    t0 = time.time()
+    if processes <= 1:
+        _oracle_chunk((args, qs, ts))
+    else:
+        chunks = [ts[i::processes] for i in range(processes)]
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(processes) as pool:
+            pool.map(_oracle_chunk, [(args, qs, c) for c in chunks if c])
+    dt = time.time() - t0
+    return {"value": cells / dt / 1e9, "unit": "GCUPS", "cores": processes, "kind": "port",
+            "sample": "%d queries x %d targets (%d cells) of the same workload, full path" % (len(qs), len(ts), cells),
+            "seconds": dt}
+
+
+def _oracle_args(score, settings):
+    gap, ext, affine, ll, mn = score.kernel_constants()
+    return (score.matrix_array(), score.char_offset_code(), float(gap), float(ext), bool(affine), float(ll),
+            float(mn), float(score.highest_score), float(settings.filter_factor), float(settings.minimum_score))
+
+
+def _oracle_chunk(job):
+    args, qs, ts = job
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle
+    m, off, gap, ext, affine, ll, mn, hi, ff, host_min = args
+    p = oracle.OracleParams(m, off, gap, ext, affine, ll, mn)
+    pos = np.array([[np.float32(hi * min(len(q), len(t)) * ff) for q in qs] for t in ts], np.float32)
+    return len(oracle.run(p, qs, ts, pos, host_min)["hits"])
+
+
+def run_reference(args, workload_fn):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return 0
+    w = workload_fn()
+    from pypaswas_b200 import scores
+    score = scores.make_score(w.settings)
+    procs = os.cpu_count() or 1
+    steps = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(w, score, min(args.cpu_seconds, 20.0), processes=procs)
+        if i >= args.warmup:
+            steps.append(r)
+    v = float(np.median([s["value"] for s in steps]))
+    line = {"impl": "reference", "metric": "GCUPS", "value": v, "unit": "GCUPS", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": w.name, "pairs": len(w.queries) * len(w.targets)},
+            "cpu_baseline": {"value": v, "unit": "GCUPS", "cores": procs, "kind": "port",
+                             "sample": steps[0]["sample"]},
+            "e2e": {"value": v, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "CPU restatement of the reference path (oracle/paswas_oracle.c) over all host cores"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    from pypaswas_b200 import workloads
+    if args.impl == "reference":
+        return run_reference(args, workloads.config2)
+    rank, world, local = dist_env()
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    w = workloads.config2()
+    e, score = engine_for(w, local)
+    cells = w.cells
+    affine = score.gap_extension is not None
+    mode = "affine" if affine else "linear"
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > L2 (126 MB)
+
+    for _ in range(args.warmup):
+        e.align()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    times, infos = [], []
+    for _ in range(args.steps):
+        flush.zero_()  # between timed iterations: L2 flushed
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        info = e.align()  # synchronous: returns when the step's device work is done
+        b.record()
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b))
+        infos.append(info.as_dict())
+    clocks = sampler.stop()
+    t_ms = float(sum(times))
+    if world > 1:
+        tt = torch.tensor([t_ms], device="cuda")
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        t_ms = float(tt.item())
+    value = world * cells * args.steps / (t_ms * 1e-3) / 1e9
+    ms_per_step = t_ms / args.steps
+
+    # roofline of the dominant kernel (integer-ALU bound)
+    last = infos[-1]
+    trace_ms = sum(i["trace_kernel_ms"] for i in infos)
+    score_ms = sum(i["score_kernel_ms"] for i in infos)
+    if trace_ms >= score_ms:
+        dom, dom_ms, dom_launch = "direction sweep (sweep_kernel phase 2)", trace_ms, sum(
+            i["trace_launches"] for i in infos)
+        traced_cells = _traced_cells(e, w)
+        ops = traced_cells * OPS_PER_CELL[(mode, "dirs")] * args.steps
+    else:
+        dom, dom_ms, dom_launch = "score sweep (sweep_kernel phase 1)", score_ms, sum(
+            i["score_launches"] for i in infos)
+        ops = cells * OPS_PER_CELL[(mode, "score")] * args.steps
+    peak_ops, _ = e.measure_int_peak()
+    achieved = ops / (dom_ms * 1e-3) / 1e12
+    traffic = load_traffic().get("direction_sweep_bytes_per_launch" if "direction" in dom else
+                                 "score_sweep_bytes_per_launch")
+
+    # end to end through the public driver, host records in, hits out
+    e2e_value, h2d, d2h = _e2e(w, args.steps, local)
+
+    out = {"metric": "GCUPS", "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+           "config": {"workload": w.name + " (400,000 pairs, full path)", "pairs": len(w.queries) * len(w.targets),
+                      "cells_per_step": cells, "traced_pairs": last["traced_pairs"],
+                      "starting_points": last["starting_points"], "hits": last["hits"],
+                      "minimum_score": w.settings.minimum_score, "lower_limit_score": w.settings.lower_limit_score,
+                      "filter_factor": w.settings.filter_factor,
+                      "l2": "flushed between steps (256 MiB write); each step also writes >1e11 B of cell codes",
+                      "parallelism": "replica per GPU" if world > 1 else "single GPU"},
+           "phases_ms": {"score": last["score_ms"], "trace": last["trace_ms"], "walk": last["walk_ms"]},
+           "gpu_launches": int(sum(i["kernel_launches"] for i in infos)),
+           "clocks": clocks,
+           "roofline": {"bound": "int_alu", "kernel": dom, "achieved": achieved,
+                        "peak": peak_ops / 1e12, "unit": "Tops/s", "frac": achieved / (peak_ops / 1e12),
+                        "peak_source": "measured in this run: DPX add-max issue probe (pw_measure_int_peak)",
+                        "ops_per_cell": OPS_PER_CELL[(mode, "dirs" if "direction" in dom else "score")],
+                        "launches": dom_launch, "avg_launch_ms": dom_ms / max(1, dom_launch),
+                        "traffic": traffic,
+                        "hbm_gbs_measured": load_peaks().get("hbm_gbs")},
+           "e2e": {"value": e2e_value, "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(w, score, args.cpu_seconds, processes=1)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    e.close()
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def _traced_cells(engine, w):
+    pm = engine.pair_max()
+    thr = float(np.float32(float(w.settings.minimum_score)))
+    ql = np.array([len(s) for _, s in w.queries], dtype=np.int64)
+    tl = np.array([len(s) for _, s in w.targets], dtype=np.int64)
+    mask = pm >= thr
+    return int((mask * np.outer(ql, tl)).sum())
+
+
+def _e2e(w, steps, device):
+    """Public driver path: Aligner.process on host records -> HitList."""
+    import torch
+    from pypaswas_b200.programs import Aligner
+    from pypaswas_b200.records import SeqRecord
+    queries = [SeqRecord(s, i) for i, s in w.queries]
+    targets = [SeqRecord(s, i) for i, s in w.targets]
+    aligner = Aligner(None, None, w.settings, device=device)
+    aligner.process(queries, targets, None)  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        aligner.process(queries, targets, None)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    sw = aligner.smith_waterman
+    return w.cells * steps / dt / 1e9, int(sw.last_h2d_bytes), int(sw.last_d2h_bytes)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

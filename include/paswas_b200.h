@@ -63,6 +63,9 @@ typedef struct {
     int32_t kernel_launches;
     int32_t truncated;      /* 1 when the starting-point cap cut the walk short */
     double score_ms, trace_ms, walk_ms; /* device time of the three phases */
+    double score_kernel_ms; /* summed duration of the score-sweep launches */
+    double trace_kernel_ms; /* summed duration of the direction-sweep launches */
+    int32_t score_launches, trace_launches;
 } pw_run_info;
 
 /* Creates an engine on CUDA device `device`.
@@ -141,6 +144,12 @@ int pw_get_starting_points(pw_engine* e, void* out36, int64_t max_points, int64_
 
 /* Number of this library's kernels launched by the last pw_align. */
 int pw_last_launch_count(pw_engine* e, int64_t* n);
+
+/* Measurement helper (no counterpart in the reference): runs an issue-rate
+ * probe of the DPX add-max instruction the recurrences use and reports the
+ * device's integer operation rate, counting the add and the max as two
+ * operations.  Used as the roofline denominator by bench.py. */
+int pw_measure_int_peak(pw_engine* e, double* ops_per_second, double* ms);
 
 #ifdef __cplusplus
 }

@@ -167,6 +167,7 @@ class SmithWatermanEmu(SmithWatermanCuda):
         self.device_memory = int(device_memory)
         self.lib = None
         self.raw_batches = []
+        self.batch_offsets = []
         SmithWatermanCuda.__init__(self, logger, score, settings)
 
     def __del__(self):
@@ -250,6 +251,10 @@ class SmithWatermanEmu(SmithWatermanCuda):
                                    _ptr(self.d_global_maxima), _ptr(self.d_global_direction),
                                    _ptr(self.h_global_direction_zero_copy), _ptr(self.d_index_increment),
                                    _ptr(self.h_starting_points_zero_copy), _ptr(self.d_max_possible_score_zero_copy))
+
+    def _print_alignments(self, sequences, targets, start_seq, start_target, hit_list=None):
+        self.batch_offsets.append([int(start_seq), int(start_target)])
+        return SmithWatermanCuda._print_alignments(self, sequences, targets, start_seq, start_target, hit_list)
 
     def _get_number_of_starting_points(self):
         n = int(self.d_index_increment[0])

@@ -29,7 +29,7 @@ PW_FLAG_PLAIN = 2
 EXPORTED_SYMBOLS = (
     "pw_create", "pw_destroy", "pw_last_error", "pw_device_free_memory", "pw_set_scoring",
     "pw_set_queries", "pw_set_targets", "pw_align", "pw_get_pair_max", "pw_get_hits",
-    "pw_get_starting_points", "pw_last_launch_count",
+    "pw_get_starting_points", "pw_last_launch_count", "pw_measure_int_peak",
 )
 
 
@@ -54,7 +54,9 @@ class PwRunInfo(ctypes.Structure):
     _fields_ = [("pairs", ctypes.c_int64), ("cells", ctypes.c_int64), ("traced_pairs", ctypes.c_int64),
                 ("starting_points", ctypes.c_int64), ("hits", ctypes.c_int64), ("string_bytes", ctypes.c_int64),
                 ("kernel_launches", ctypes.c_int32), ("truncated", ctypes.c_int32), ("score_ms", ctypes.c_double),
-                ("trace_ms", ctypes.c_double), ("walk_ms", ctypes.c_double)]
+                ("trace_ms", ctypes.c_double), ("walk_ms", ctypes.c_double),
+                ("score_kernel_ms", ctypes.c_double), ("trace_kernel_ms", ctypes.c_double),
+                ("score_launches", ctypes.c_int32), ("trace_launches", ctypes.c_int32)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -77,6 +79,7 @@ def bind(lib):
         "pw_get_hits": (ctypes.c_int, [P, P, I64, P, I64]),
         "pw_get_starting_points": (ctypes.c_int, [P, P, I64, ctypes.POINTER(I64)]),
         "pw_last_launch_count": (ctypes.c_int, [P, ctypes.POINTER(I64)]),
+        "pw_measure_int_peak": (ctypes.c_int, [P, ctypes.POINTER(D), ctypes.POINTER(D)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -209,6 +212,13 @@ class Engine(object):
                self.lib.pw_get_starting_points(self.handle, _ptr(out), n.value, ctypes.byref(n)),
                "pw_get_starting_points")
         return out
+
+    def measure_int_peak(self):
+        """(integer ops per second, probe duration in ms) of the DPX add-max probe."""
+        r, ms = ctypes.c_double(), ctypes.c_double()
+        _check(self.lib, self.handle, self.lib.pw_measure_int_peak(self.handle, ctypes.byref(r), ctypes.byref(ms)),
+               "pw_measure_int_peak")
+        return r.value, ms.value
 
     def launch_count(self):
         n = ctypes.c_int64()

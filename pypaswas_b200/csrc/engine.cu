@@ -61,6 +61,13 @@ struct HostSeqs {
     bool set = false;
 };
 
+struct Prepared {
+    int alpha = 0;
+    bool int_path = true;
+    std::vector<int32_t> order;  // query indices by length, longest first
+    std::vector<int32_t> qlen, tlen;
+};
+
 struct StartRec {  // one starting point (emission order sortable)
     int32_t query, target, x, y;
     float score;
@@ -87,8 +94,12 @@ struct pw_engine {
     // device buffers
     DevBuf q_codes, q_code_off, q_raw, q_raw_off, q_len, q_key, q_order;
     DevBuf t_codes, t_code_off, t_raw, t_raw_off, t_len, t_key;
-    DevBuf cmat_i8, cmat_f, pair_max, items, counter, bnd_pool;
-    DevBuf codes, metas, cands, cand_base, cand_cap, n_starts, hits, hit_count, ops, allowed;
+    DevBuf cmat_i8, cmat_f, pair_max, items, items_alt, counter, bnd_pool, q_order2;
+    DevBuf codes, metas, cands, cands_alt, cand_base, cand_cap, n_cand, n_starts, start_off, starts, hits,
+        hit_count, ops, allowed;
+    // prepared (device-resident) inputs
+    Prepared pr;
+    int64_t input_gen = 1, prepared_gen = 0;
     // results
     std::vector<float> h_pair_max;
     std::vector<pw_hit> h_hits;
@@ -180,6 +191,7 @@ extern "C" int pw_set_scoring(pw_engine* e, const float* matrix, int dim, int ch
     e->highest = highest;
     e->filter_factor = filter_factor;
     e->scoring_set = true;
+    e->input_gen++;
     return PW_OK;
 }
 
@@ -201,6 +213,7 @@ static int set_seqs(pw_engine* e, HostSeqs& S, const uint8_t* residues, const in
     S.key.assign(id_keys, id_keys + n);
     S.n = n;
     S.set = true;
+    e->input_gen++;
     return PW_OK;
 }
 
@@ -227,8 +240,10 @@ int pick_class(int lt, bool affine) {
     return kS32Multi;
 }
 
+int64_t align_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
+
 template <typename T, int S, bool AFF, bool MULTI, int PH>
-cudaError_t launch_sweep(pw_engine* e, KernelArgs A, int n_items) {
+cudaError_t launch_sweep(pw_engine* e, KernelArgs A, int* counter) {
     auto kern = sweep_kernel<T, S, AFF, MULTI, PH>;
     const int alpha1 = A.P.alpha + 1;
     const int prof_bytes = ((S / 4) * alpha1 * (std::is_integral<T>::value ? 4 : 16) + 15) & ~15;
@@ -241,42 +256,33 @@ cudaError_t launch_sweep(pw_engine* e, KernelArgs A, int n_items) {
     cudaError_t c = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem);
     if (c != cudaSuccess) return c;
     if (per_sm < 1) per_sm = 1;
+    if (per_sm > 16) per_sm = 16;
     int grid = e->sm_count * per_sm;
-    const int need = (n_items + 3) / 4;
+    const int need = (A.n_items + 3) / 4;
     if (grid > need) grid = need;
     if (grid < 1) grid = 1;
-    c = cudaMemsetAsync(A.item_counter, 0, sizeof(int), e->stream);
-    if (c != cudaSuccess) return c;
+    A.item_counter = counter;
     PW_LAUNCH(kern, grid, 128, smem, e->stream, A);
     e->launches++;
     return cudaGetLastError();
 }
 
 template <typename T, int PH>
-cudaError_t launch_class(pw_engine* e, int cls, bool affine, KernelArgs A, int n_items) {
+cudaError_t launch_class(pw_engine* e, int cls, bool affine, const KernelArgs& A, int* counter) {
     if (affine) {
         switch (cls) {
-            case kS16: return launch_sweep<T, 16, true, false, PH>(e, A, n_items);
-            case kS32: return launch_sweep<T, 32, true, false, PH>(e, A, n_items);
-            default: return launch_sweep<T, 32, true, true, PH>(e, A, n_items);
+            case kS16: return launch_sweep<T, 16, true, false, PH>(e, A, counter);
+            case kS32: return launch_sweep<T, 32, true, false, PH>(e, A, counter);
+            default: return launch_sweep<T, 32, true, true, PH>(e, A, counter);
         }
     }
     switch (cls) {
-        case kS16: return launch_sweep<T, 16, false, false, PH>(e, A, n_items);
-        case kS32: return launch_sweep<T, 32, false, false, PH>(e, A, n_items);
-        case kS64: return launch_sweep<T, 64, false, false, PH>(e, A, n_items);
-        default: return launch_sweep<T, 32, false, true, PH>(e, A, n_items);
+        case kS16: return launch_sweep<T, 16, false, false, PH>(e, A, counter);
+        case kS32: return launch_sweep<T, 32, false, false, PH>(e, A, counter);
+        case kS64: return launch_sweep<T, 64, false, false, PH>(e, A, counter);
+        default: return launch_sweep<T, 32, false, true, PH>(e, A, counter);
     }
 }
-
-int64_t align_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
-
-struct Prepared {
-    int alpha = 0;
-    bool int_path = true;
-    std::vector<int32_t> order;  // sorted position -> query
-    int xmax_all4 = 0;
-};
 
 }  // namespace
 
@@ -288,12 +294,25 @@ static cudaError_t upload(pw_engine* e, DevBuf& b, const std::vector<HT>& v) {
     return cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(HT), cudaMemcpyHostToDevice, e->stream);
 }
 
-// Builds device sequence sets, the compact query alphabet and the compact
-// substitution matrix.
-static int prepare(pw_engine* e, Prepared& pr, KernelArgs& A) {
+template <typename HT>
+static cudaError_t download(pw_engine* e, std::vector<HT>& v, const void* src, size_t n) {
+    v.resize(n);
+    if (!n) return cudaSuccess;
+    cudaError_t c = cudaMemcpyAsync(v.data(), src, n * sizeof(HT), cudaMemcpyDeviceToHost, e->stream);
+    if (c != cudaSuccess) return c;
+    return cudaStreamSynchronize(e->stream);
+}
+
+// Builds the device copies of the sequences, the compact query alphabet and the
+// compact substitution matrix.  Cached: nothing is uploaded again while the
+// sequences and the scoring model are unchanged (the target database and the
+// query set stay resident on the device).
+static int prepare(pw_engine* e) {
+    if (e->prepared_gen == e->input_gen) return PW_OK;
     const HostSeqs& Q = e->Q;
     const HostSeqs& T = e->T;
     const int off = e->char_offset, dim = e->dim;
+    Prepared& pr = e->pr;
     // residues must index the matrix (default_main.cu:234 reads matrix[c - offset])
     int map[256];
     for (int i = 0; i < 256; ++i) map[i] = -1;
@@ -322,11 +341,12 @@ static int prepare(pw_engine* e, Prepared& pr, KernelArgs& A) {
             if (std::floor(v) != v || v < -127.0f || v > 127.0f) ints = false;
             maxabs = std::max(maxabs, std::fabs(v));
         }
-    int64_t maxlen = 0;
-    for (int32_t i = 0; i < Q.n; ++i) maxlen = std::max<int64_t>(maxlen, Q.off[i + 1] - Q.off[i]);
-    int64_t maxlt = 0;
-    for (int32_t i = 0; i < T.n; ++i) maxlt = std::max<int64_t>(maxlt, T.off[i + 1] - T.off[i]);
-    if ((double)maxabs * (double)std::min(maxlen, maxlt) + std::fabs(e->gap) + std::fabs(e->ext) >= 16777216.0)
+    pr.qlen.assign(Q.n, 0);
+    pr.tlen.assign(T.n, 0);
+    int64_t maxlq = 0, maxlt = 0;
+    for (int32_t i = 0; i < Q.n; ++i) maxlq = std::max<int64_t>(maxlq, pr.qlen[i] = (int32_t)(Q.off[i + 1] - Q.off[i]));
+    for (int32_t i = 0; i < T.n; ++i) maxlt = std::max<int64_t>(maxlt, pr.tlen[i] = (int32_t)(T.off[i + 1] - T.off[i]));
+    if ((double)maxabs * (double)std::min(maxlq, maxlt) + std::fabs(e->gap) + std::fabs(e->ext) >= 16777216.0)
         ints = false;
     if (std::fabs(e->gap) > 1.0e6f || std::fabs(e->ext) > 1.0e6f) ints = false;
     pr.int_path = ints;
@@ -343,35 +363,31 @@ static int prepare(pw_engine* e, Prepared& pr, KernelArgs& A) {
     // queries: compact codes, each sequence 16-byte aligned and padded to a
     // multiple of 4 with the pad code
     std::vector<int64_t> qco(Q.n + 1, 0);
-    std::vector<int32_t> qlen(Q.n);
     int64_t pos = 0;
     for (int32_t i = 0; i < Q.n; ++i) {
-        qlen[i] = (int32_t)(Q.off[i + 1] - Q.off[i]);
         qco[i] = pos;
-        pos += align_up(std::max<int64_t>(qlen[i], 1), 16);
+        pos += align_up(std::max<int64_t>(pr.qlen[i], 1), 16);
     }
     qco[Q.n] = pos;
     std::vector<uint8_t> qc((size_t)std::max<int64_t>(pos, 16), (uint8_t)pr.alpha);
     for (int32_t i = 0; i < Q.n; ++i)
-        for (int32_t k = 0; k < qlen[i]; ++k) qc[qco[i] + k] = (uint8_t)map[Q.raw[Q.off[i] + k]];
+        for (int32_t k = 0; k < pr.qlen[i]; ++k) qc[qco[i] + k] = (uint8_t)map[Q.raw[Q.off[i] + k]];
     // targets: matrix residue index
     std::vector<int64_t> tco(T.n + 1, 0);
-    std::vector<int32_t> tlen(T.n);
     pos = 0;
     for (int32_t i = 0; i < T.n; ++i) {
-        tlen[i] = (int32_t)(T.off[i + 1] - T.off[i]);
         tco[i] = pos;
-        pos += align_up(std::max<int64_t>(tlen[i], 1), 16);
+        pos += align_up(std::max<int64_t>(pr.tlen[i], 1), 16);
     }
     tco[T.n] = pos;
     std::vector<uint8_t> tc((size_t)std::max<int64_t>(pos, 16), 0);
     for (int32_t i = 0; i < T.n; ++i)
-        for (int32_t k = 0; k < tlen[i]; ++k) tc[tco[i] + k] = (uint8_t)(T.raw[T.off[i] + k] - off);
+        for (int32_t k = 0; k < pr.tlen[i]; ++k) tc[tco[i] + k] = (uint8_t)(T.raw[T.off[i] + k] - off);
 
     pr.order.resize(Q.n);
     std::iota(pr.order.begin(), pr.order.end(), 0);
-    std::stable_sort(pr.order.begin(), pr.order.end(), [&](int a, int b) { return qlen[a] > qlen[b]; });
-    pr.xmax_all4 = Q.n ? (int)align_up(std::max(qlen[pr.order[0]], 1), 4) : 4;
+    std::stable_sort(pr.order.begin(), pr.order.end(),
+                     [&](int a, int b) { return pr.qlen[a] > pr.qlen[b]; });
 
     cudaError_t c;
 #define UP(buf, vec)                                      \
@@ -380,23 +396,31 @@ static int prepare(pw_engine* e, Prepared& pr, KernelArgs& A) {
     UP(e->q_code_off, qco);
     UP(e->q_raw, Q.raw);
     UP(e->q_raw_off, Q.off);
-    UP(e->q_len, qlen);
+    UP(e->q_len, pr.qlen);
     UP(e->q_key, Q.key);
     UP(e->q_order, pr.order);
     UP(e->t_codes, tc);
     UP(e->t_code_off, tco);
     UP(e->t_raw, T.raw);
     UP(e->t_raw_off, T.off);
-    UP(e->t_len, tlen);
+    UP(e->t_len, pr.tlen);
     UP(e->t_key, T.key);
     UP(e->cmat_i8, cm8);
     UP(e->cmat_f, cmf);
 #undef UP
-    if ((c = e->counter.reserve(64)) != cudaSuccess) return cuda_fail(e, c, "alloc counter");
+    if ((c = e->counter.reserve(64 * sizeof(int))) != cudaSuccess) return cuda_fail(e, c, "alloc counter");
+    if ((c = cudaStreamSynchronize(e->stream)) != cudaSuccess) return cuda_fail(e, c, "upload");
+    e->prepared_gen = e->input_gen;
+    return PW_OK;
+}
 
+static KernelArgs base_args(pw_engine* e) {
+    KernelArgs A;
+    memset(&A, 0, sizeof(A));
+    const Prepared& pr = e->pr;
     ScoreParams& P = A.P;
     P.affine = e->affine;
-    P.is_float = ints ? 0 : 1;
+    P.is_float = pr.int_path ? 0 : 1;
     P.gap_i = (int)e->gap;
     P.ext_i = (int)e->ext;
     P.ge_i = (int)e->gap + (int)e->ext;
@@ -409,7 +433,7 @@ static int prepare(pw_engine* e, Prepared& pr, KernelArgs& A) {
     P.highest = e->highest;
     P.filter_factor = e->filter_factor;
     P.alpha = pr.alpha;
-    P.dim = dim;
+    P.dim = e->dim;
     A.q = SeqSet{e->q_codes.as<uint8_t>(), e->q_code_off.as<int64_t>(), e->q_raw.as<uint8_t>(),
                  e->q_raw_off.as<int64_t>(), e->q_len.as<int32_t>(), e->q_key.as<int32_t>()};
     A.t = SeqSet{e->t_codes.as<uint8_t>(), e->t_code_off.as<int64_t>(), e->t_raw.as<uint8_t>(),
@@ -417,67 +441,83 @@ static int prepare(pw_engine* e, Prepared& pr, KernelArgs& A) {
     A.q_order = e->q_order.as<int32_t>();
     A.cmat_i8 = e->cmat_i8.as<int8_t>();
     A.cmat_f = e->cmat_f.as<float>();
-    A.item_counter = e->counter.as<int>();
-    A.nt = T.n;
-    return PW_OK;
+    A.nt = e->T.n;
+    A.pair_max = e->pair_max.as<float>();
+    return A;
 }
 
-// Launches one phase over a list of work items grouped by strip class.
+// Launches a sweep phase over items already sorted by strip class and uploaded
+// as one array; class c covers [cls_begin[c], cls_begin[c + 1]).  Each class
+// gets its own work counter, so there is no host synchronisation in between.
+// Kernel time per launch is accumulated into *kernel_ms after the phase.
 template <int PH>
-static int run_items(pw_engine* e, const Prepared& pr, KernelArgs A, const std::vector<WorkItem> (&by_class)[kNumClasses],
-                     DevBuf& item_buf, int64_t item_base_offset) {
-    (void)item_base_offset;
-    int xmax_multi = 4;
-    for (const WorkItem& w : by_class[kS32Multi]) xmax_multi = std::max(xmax_multi, (int)align_up(w.xmax, 4));
+static int run_phase(pw_engine* e, KernelArgs A, const WorkItem* dev_items, const int (&cls_begin)[kNumClasses + 1],
+                     int xmax_multi4, double* kernel_ms, int* n_launch) {
+    cudaError_t c;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> evs;
+    if (cls_begin[kS32Multi + 1] > cls_begin[kS32Multi]) {
+        // one boundary slot per resident warp (at most 16 blocks of 4 warps per SM)
+        const int64_t slot = (int64_t)xmax_multi4 * kWarp;
+        const int64_t warps = (int64_t)e->sm_count * 16 * 4;
+        const size_t elem = e->pr.int_path ? sizeof(Bnd<int>) : sizeof(Bnd<float>);
+        c = e->bnd_pool.reserve((size_t)(slot * warps) * elem);
+        if (c != cudaSuccess) return cuda_fail(e, c, "alloc boundary pool");
+        A.bnd_pool = e->bnd_pool.p;
+        A.bnd_slot_elems = slot;
+    }
+    if ((c = cudaMemsetAsync(e->counter.p, 0, kNumClasses * sizeof(int), e->stream)) != cudaSuccess)
+        return cuda_fail(e, c, "reset counters");
     for (int cls = 0; cls < kNumClasses; ++cls) {
-        const std::vector<WorkItem>& its = by_class[cls];
-        if (its.empty()) continue;
-        cudaError_t c = upload(e, item_buf, its);
-        if (c != cudaSuccess) return cuda_fail(e, c, "upload items");
-        A.items = item_buf.as<WorkItem>();
-        A.n_items = (int)its.size();
-        if (cls == kS32Multi) {
-            // one boundary slot per resident warp
-            const int64_t slot = (int64_t)xmax_multi * kWarp;
-            const int64_t warps = (int64_t)e->sm_count * 16 * 4;
-            const size_t elem = pr.int_path ? sizeof(Bnd<int>) : sizeof(Bnd<float>);
-            c = e->bnd_pool.reserve((size_t)(slot * warps) * elem);
-            if (c != cudaSuccess) return cuda_fail(e, c, "alloc boundary pool");
-            A.bnd_pool = e->bnd_pool.p;
-            A.bnd_slot_elems = slot;
-        }
-        c = pr.int_path ? launch_class<int, PH>(e, cls, e->affine, A, A.n_items)
-                        : launch_class<float, PH>(e, cls, e->affine, A, A.n_items);
+        const int n = cls_begin[cls + 1] - cls_begin[cls];
+        if (n <= 0) continue;
+        A.items = dev_items + cls_begin[cls];
+        A.n_items = n;
+        cudaEvent_t a, b;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        cudaEventRecord(a, e->stream);
+        c = e->pr.int_path ? launch_class<int, PH>(e, cls, e->affine, A, e->counter.as<int>() + cls)
+                           : launch_class<float, PH>(e, cls, e->affine, A, e->counter.as<int>() + cls);
+        cudaEventRecord(b, e->stream);
+        evs.push_back({a, b});
         if (c != cudaSuccess) return cuda_fail(e, c, "sweep kernel launch");
-        // items buffer is reused by the next class: wait for this launch
-        c = cudaStreamSynchronize(e->stream);
-        if (c != cudaSuccess) return cuda_fail(e, c, "sweep kernel");
+        if (n_launch) ++*n_launch;
+    }
+    if ((c = cudaStreamSynchronize(e->stream)) != cudaSuccess) return cuda_fail(e, c, "sweep kernel");
+    for (auto& ab : evs) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ab.first, ab.second);
+        if (kernel_ms) *kernel_ms += ms;
+        cudaEventDestroy(ab.first);
+        cudaEventDestroy(ab.second);
     }
     return PW_OK;
 }
 
-static void build_items(const std::vector<std::vector<int32_t>>& per_target_sorted_pos, const std::vector<int32_t>& order,
-                        const std::vector<int32_t>& qlen, const std::vector<int32_t>& tlen, bool affine,
-                        std::vector<WorkItem> (&by_class)[kNumClasses], std::vector<int32_t>* pair_query) {
-    for (auto& v : by_class) v.clear();
-    (void)order;
-    for (size_t t = 0; t < per_target_sorted_pos.size(); ++t) {
-        const std::vector<int32_t>& pos = per_target_sorted_pos[t];
-        for (size_t g = 0; g < pos.size(); g += kWarp) {
-            WorkItem w;
-            w.target = (int32_t)t;
-            w.first = (int32_t)g;  // caller rewrites for phase 2
-            w.lanes = (int32_t)std::min<size_t>(kWarp, pos.size() - g);
-            w.xmax = qlen[order[pos[g]]];
-            w.dir_base = 0;
-            w.pair_base = 0;
-            const int cls = pick_class(tlen[t], affine);
-            w.S = class_S(cls);
-            w.index = 0;
-            by_class[cls].push_back(w);
-        }
+// Sorts items by strip class (stable) and returns the class boundaries.
+static void order_by_class(std::vector<WorkItem>& items, std::vector<int>& cls, int (&begin)[kNumClasses + 1]) {
+    std::vector<size_t> idx(items.size());
+    std::iota(idx.begin(), idx.end(), 0);
+    std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return cls[a] < cls[b]; });
+    std::vector<WorkItem> it2(items.size());
+    std::vector<int> c2(items.size());
+    for (size_t k = 0; k < idx.size(); ++k) {
+        it2[k] = items[idx[k]];
+        c2[k] = cls[idx[k]];
     }
-    (void)pair_query;
+    items.swap(it2);
+    cls.swap(c2);
+    for (int c = 0; c <= kNumClasses; ++c) begin[c] = 0;
+    for (int c : cls) begin[c + 1]++;
+    for (int c = 0; c < kNumClasses; ++c) begin[c + 1] += begin[c];
+}
+
+static int emit_key_less(const StartRec& a, const StartRec& b) {
+    auto k = [](const StartRec& r) {
+        return std::make_tuple(-(int64_t)((r.x >> 3) + (r.y >> 3)), -(int64_t)(r.x >> 3), r.target, r.query,
+                               -(int64_t)((r.x & 7) + (r.y & 7)), (int64_t)(r.y & 7));
+    };
+    return k(a) < k(b);
 }
 
 extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_info* info) {
@@ -495,49 +535,81 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     const int nq = e->Q.n, nt = e->T.n;
     e->h_pair_max.assign((size_t)nq * nt, 0.0f);
     inf.pairs = (int64_t)nq * nt;
-    std::vector<int32_t> qlen(nq), tlen(nt);
     int64_t sumq = 0, sumt = 0;
-    for (int i = 0; i < nq; ++i) sumq += (qlen[i] = (int32_t)(e->Q.off[i + 1] - e->Q.off[i]));
-    for (int i = 0; i < nt; ++i) sumt += (tlen[i] = (int32_t)(e->T.off[i + 1] - e->T.off[i]));
+    for (int i = 0; i < nq; ++i) sumq += e->Q.off[i + 1] - e->Q.off[i];
+    for (int i = 0; i < nt; ++i) sumt += e->T.off[i + 1] - e->T.off[i];
     inf.cells = sumq * sumt;
     if (nq == 0 || nt == 0) {
         if (info) *info = inf;
         return PW_OK;
     }
-    KernelArgs A;
-    memset(&A, 0, sizeof(A));
-    Prepared pr;
-    int rc = prepare(e, pr, A);
+    int rc = prepare(e);
     if (rc != PW_OK) return rc;
+    const Prepared& pr = e->pr;
+    const std::vector<int32_t>& qlen = pr.qlen;
+    const std::vector<int32_t>& tlen = pr.tlen;
     cudaError_t c;
     if ((c = e->pair_max.reserve((size_t)nq * nt * sizeof(float))) != cudaSuccess)
         return cuda_fail(e, c, "alloc pair maxima");
-    A.pair_max = e->pair_max.as<float>();
+    KernelArgs A = base_args(e);
+    const bool plain = (flags & PW_FLAG_PLAIN) != 0;
 
     // ---------------------------------------------------------- phase 1
-    std::vector<std::vector<int32_t>> all_pos(nt);
-    for (int t = 0; t < nt; ++t) {
-        all_pos[t].resize(nq);
-        std::iota(all_pos[t].begin(), all_pos[t].end(), 0);
-    }
-    std::vector<WorkItem> by_class[kNumClasses];
-    build_items(all_pos, pr.order, qlen, tlen, e->affine, by_class, nullptr);
-    for (auto& v : by_class)  // largest work first
-        std::stable_sort(v.begin(), v.end(), [&](const WorkItem& a, const WorkItem& b) {
-            return (int64_t)a.xmax * tlen[a.target] > (int64_t)b.xmax * tlen[b.target];
+    // items: one target against 32 consecutive queries of the length order
+    {
+        std::vector<WorkItem> items;
+        std::vector<int> cls;
+        for (int t = 0; t < nt; ++t)
+            for (int g = 0; g < nq; g += (plain ? 1 : kWarp)) {
+                WorkItem w;
+                memset(&w, 0, sizeof(w));
+                w.target = t;
+                w.first = g;
+                w.lanes = plain ? 1 : std::min(kWarp, nq - g);
+                w.xmax = qlen[pr.order[g]];
+                const int k = pick_class(tlen[t], e->affine);
+                w.S = class_S(k);
+                items.push_back(w);
+                cls.push_back(k);
+            }
+        // largest work first inside each class (dynamic scheduling tail)
+        std::vector<size_t> idx(items.size());
+        std::iota(idx.begin(), idx.end(), 0);
+        std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) {
+            return (int64_t)items[a].xmax * tlen[items[a].target] > (int64_t)items[b].xmax * tlen[items[b].target];
         });
-    cudaEventRecord(e->ev[0], e->stream);
-    rc = run_items<1>(e, pr, A, by_class, e->items, 0);
-    if (rc != PW_OK) return rc;
-    cudaEventRecord(e->ev[1], e->stream);
-    c = cudaMemcpyAsync(e->h_pair_max.data(), A.pair_max, (size_t)nq * nt * sizeof(float), cudaMemcpyDeviceToHost,
-                        e->stream);
-    if (c != cudaSuccess) return cuda_fail(e, c, "copy pair maxima");
-    if ((c = cudaStreamSynchronize(e->stream)) != cudaSuccess) return cuda_fail(e, c, "score phase");
-    float ms = 0;
-    cudaEventElapsedTime(&ms, e->ev[0], e->ev[1]);
-    inf.score_ms = ms;
-
+        std::vector<WorkItem> it2;
+        std::vector<int> c2;
+        for (size_t k : idx) {
+            it2.push_back(items[k]);
+            c2.push_back(cls[k]);
+        }
+        int begin[kNumClasses + 1];
+        order_by_class(it2, c2, begin);
+        int xm = 4;
+        for (int k = begin[kS32Multi]; k < begin[kS32Multi + 1]; ++k) xm = std::max(xm, (int)align_up(it2[k].xmax, 4));
+        if ((c = upload(e, e->items, it2)) != cudaSuccess) return cuda_fail(e, c, "upload items");
+        cudaEventRecord(e->ev[0], e->stream);
+        if (plain) {
+            // the unbatched form: one launch per (query, target) pair
+            for (size_t k = 0; k < it2.size(); ++k) {
+                int b1[kNumClasses + 1];
+                for (int q = 0; q <= kNumClasses; ++q) b1[q] = (q > c2[k]) ? 1 : 0;
+                rc = run_phase<1>(e, A, e->items.as<WorkItem>() + k, b1, xm, &inf.score_kernel_ms,
+                                  &inf.score_launches);
+                if (rc != PW_OK) return rc;
+            }
+        } else {
+            rc = run_phase<1>(e, A, e->items.as<WorkItem>(), begin, xm, &inf.score_kernel_ms, &inf.score_launches);
+            if (rc != PW_OK) return rc;
+        }
+        cudaEventRecord(e->ev[1], e->stream);
+        if ((c = download(e, e->h_pair_max, A.pair_max, (size_t)nq * nt)) != cudaSuccess)
+            return cuda_fail(e, c, "copy pair maxima");
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e->ev[0], e->ev[1]);
+        inf.score_ms = ms;
+    }
     if (flags & PW_FLAG_SCORE_ONLY) {
         inf.kernel_launches = (int32_t)e->launches;
         if (info) *info = inf;
@@ -546,183 +618,148 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
 
     // ---------------------------------------------------------- phase 2
     // pairs whose maximum reaches MINIMUM_SCORE (default_main.cu:596), per
-    // target in sorted query order
-    std::vector<std::vector<int32_t>> pass_pos(nt);
-    int64_t n_pass = 0;
-    for (int t = 0; t < nt; ++t)
+    // target in query length order, 32 per work item
+    std::vector<int32_t> p2_order;
+    std::vector<WorkItem> items2;
+    std::vector<int> cls2;
+    std::vector<int64_t> bytes2;
+    for (int t = 0; t < nt; ++t) {
+        std::vector<int32_t> pass;
         for (int sp = 0; sp < nq; ++sp) {
             const int q = pr.order[sp];
-            if (e->h_pair_max[(size_t)q * nt + t] >= e->minimum_score) {
-                pass_pos[t].push_back(sp);
-                ++n_pass;
-            }
+            if (e->h_pair_max[(size_t)q * nt + t] >= e->minimum_score) pass.push_back(q);
         }
-    inf.traced_pairs = n_pass;
-    if (n_pass == 0) {
+        const int per_item = plain ? 1 : kWarp;
+        for (size_t g = 0; g < pass.size(); g += per_item) {
+            WorkItem w;
+            memset(&w, 0, sizeof(w));
+            w.target = t;
+            w.first = (int32_t)p2_order.size();
+            w.lanes = (int32_t)std::min<size_t>(per_item, pass.size() - g);
+            for (int l = 0; l < w.lanes; ++l) p2_order.push_back(pass[g + l]);
+            w.xmax = qlen[p2_order[w.first]];
+            const int k = pick_class(tlen[t], e->affine);
+            w.S = class_S(k);
+            items2.push_back(w);
+            cls2.push_back(k);
+            const int64_t strips = std::max<int64_t>((tlen[t] + w.S - 1) / w.S, 1);
+            bytes2.push_back(strips * w.S * align_up(std::max(w.xmax, 1), 4) * kWarp);
+        }
+    }
+    inf.traced_pairs = (int64_t)p2_order.size();
+    if (p2_order.empty()) {
         inf.kernel_launches = (int32_t)e->launches;
         if (info) *info = inf;
         return PW_OK;
     }
-    // work items over passing pairs; `first` indexes a per-item list of sorted
-    // positions, so phase 2 gets its own query order array
-    std::vector<int32_t> p2_order;
-    std::vector<WorkItem> items2;
-    std::vector<int32_t> items2_cls, items2_S;  // strip class and height per item
-    for (int t = 0; t < nt; ++t) {
-        const std::vector<int32_t>& pos = pass_pos[t];
-        for (size_t g = 0; g < pos.size(); g += kWarp) {
-            WorkItem w;
-            w.target = t;
-            w.first = (int32_t)p2_order.size();
-            w.lanes = (int32_t)std::min<size_t>(kWarp, pos.size() - g);
-            for (int l = 0; l < w.lanes; ++l) p2_order.push_back(pr.order[pos[g + l]]);
-            w.xmax = qlen[p2_order[w.first]];
-            w.dir_base = 0;
-            w.pair_base = 0;
-            const int cls = pick_class(tlen[t], e->affine);
-            w.S = class_S(cls);
-            w.index = 0;
-            items2.push_back(w);
-            items2_cls.push_back(cls);
-            items2_S.push_back(class_S(cls));
-        }
-    }
-    if ((c = upload(e, e->q_order, p2_order)) != cudaSuccess) return cuda_fail(e, c, "upload phase-2 order");
-    A.q_order = e->q_order.as<int32_t>();
+    if ((c = upload(e, e->q_order2, p2_order)) != cudaSuccess) return cuda_fail(e, c, "upload phase-2 order");
+    A.q_order = e->q_order2.as<int32_t>();
 
-    // memory waves: cell codes of one wave must fit the budget
+    // memory waves: the cell codes of one wave must fit the budget
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
-    int64_t budget = (int64_t)(free_b * 0.5);
-    budget = std::min<int64_t>(budget, (int64_t)48 << 30);
-    std::vector<int64_t> item_bytes(items2.size());
-    for (size_t i = 0; i < items2.size(); ++i) {
-        const int S = items2_S[i];
-        const int64_t strips = (tlen[items2[i].target] + S - 1) / S;
-        item_bytes[i] = std::max<int64_t>(strips, 1) * S * align_up(items2[i].xmax, 4) * kWarp;
-    }
+    int64_t budget = std::min<int64_t>((int64_t)(free_b * 0.5) + (int64_t)e->codes.bytes, (int64_t)48 << 30);
     std::vector<std::pair<size_t, size_t>> waves;
     {
         size_t i0 = 0;
         int64_t acc = 0;
         for (size_t i = 0; i < items2.size(); ++i) {
-            if (acc > 0 && acc + item_bytes[i] > budget) {
+            if (acc > 0 && (acc + bytes2[i] > budget || plain)) {
                 waves.push_back({i0, i});
                 i0 = i;
                 acc = 0;
             }
-            acc += item_bytes[i];
+            acc += bytes2[i];
         }
         waves.push_back({i0, items2.size()});
     }
-    if (waves.size() > 1 && start_cap >= 0 && (int64_t)start_cap < n_pass * 1000)
-        ;  // the cap is checked per wave below
 
     double trace_ms = 0, walk_ms = 0;
     int64_t total_starts = 0;
     std::vector<DevHit> all_hits;
     std::vector<char> all_ops;
-    std::vector<int64_t> all_ops_base;
-
     for (size_t wv = 0; wv < waves.size(); ++wv) {
         const size_t i0 = waves[wv].first, i1 = waves[wv].second;
-        std::vector<WorkItem> wave_items(items2.begin() + i0, items2.begin() + i1);
-        int64_t dir_off = 0, pair_off = 0;
-        for (size_t k = 0; k < wave_items.size(); ++k) {
-            wave_items[k].index = (int32_t)k;
-            wave_items[k].dir_base = dir_off;
-            wave_items[k].pair_base = pair_off;
-            dir_off += item_bytes[i0 + k];
-            pair_off += wave_items[k].lanes;
+        std::vector<WorkItem> wi(items2.begin() + i0, items2.begin() + i1);
+        std::vector<int> wc(cls2.begin() + i0, cls2.begin() + i1);
+        int64_t dir_off = 0, n_pairs = 0;
+        for (size_t k = 0; k < wi.size(); ++k) {
+            wi[k].index = (int32_t)k;
+            wi[k].dir_base = dir_off;
+            wi[k].pair_base = n_pairs;
+            dir_off += bytes2[i0 + k];
+            n_pairs += wi[k].lanes;
         }
-        const int64_t n_pairs = pair_off;
+        std::vector<WorkItem> by_index = wi;  // trace kernels index items by wave position
+        int begin[kNumClasses + 1];
+        order_by_class(wi, wc, begin);
+        int xm = 4;
+        for (int k = begin[kS32Multi]; k < begin[kS32Multi + 1]; ++k) xm = std::max(xm, (int)align_up(wi[k].xmax, 4));
         if ((c = e->codes.reserve((size_t)dir_off)) != cudaSuccess) return cuda_fail(e, c, "alloc cell codes");
         if ((c = e->metas.reserve(n_pairs * sizeof(PairMeta))) != cudaSuccess) return cuda_fail(e, c, "alloc metas");
-        std::vector<int32_t> cbase(n_pairs), ccap(n_pairs, kCandCap);
-        for (int64_t p = 0; p < n_pairs; ++p) cbase[p] = (int32_t)(p * kCandCap);
+        if ((c = e->n_cand.reserve(n_pairs * sizeof(int32_t))) != cudaSuccess) return cuda_fail(e, c, "alloc");
+        if ((c = e->n_starts.reserve(n_pairs * sizeof(int32_t))) != cudaSuccess) return cuda_fail(e, c, "alloc");
+        std::vector<int64_t> cbase(n_pairs);
+        std::vector<int32_t> ccap(n_pairs, kCandCap);
+        for (int64_t p = 0; p < n_pairs; ++p) cbase[p] = p * kCandCap;
         int64_t cand_total = n_pairs * kCandCap;
         if ((c = e->cands.reserve(cand_total * sizeof(Cand))) != cudaSuccess) return cuda_fail(e, c, "alloc cands");
         if ((c = upload(e, e->cand_base, cbase)) != cudaSuccess) return cuda_fail(e, c, "upload cand base");
         if ((c = upload(e, e->cand_cap, ccap)) != cudaSuccess) return cuda_fail(e, c, "upload cand cap");
+        if ((c = upload(e, e->items, wi)) != cudaSuccess) return cuda_fail(e, c, "upload items");
         A.codes = e->codes.as<uint8_t>();
         A.metas = e->metas.as<PairMeta>();
         A.cands = e->cands.as<Cand>();
-        A.cand_base = e->cand_base.as<int32_t>();
+        A.cand_base = e->cand_base.as<int64_t>();
         A.cand_cap = e->cand_cap.as<int32_t>();
-
-        // phase 2 by class; the items buffer holds the whole wave, classes are
-        // launched over contiguous sub-ranges
-        std::vector<WorkItem> wave_by_class[kNumClasses];
-        std::vector<int32_t> wave_cls(items2_cls.begin() + i0, items2_cls.begin() + i1);
+        A.n_cand = e->n_cand.as<int32_t>();
         cudaEventRecord(e->ev[0], e->stream);
-        for (int pass = 0; pass < 2; ++pass) {
-            for (auto& v : wave_by_class) v.clear();
-            for (size_t k = 0; k < wave_items.size(); ++k) wave_by_class[wave_cls[k]].push_back(wave_items[k]);
-            rc = run_items<2>(e, pr, A, wave_by_class, e->items, 0);
-            if (rc != PW_OK) return rc;
-            // candidate overflow: give overflowing items exact capacities and
-            // sweep them again (their codes and lists are rewritten)
-            std::vector<PairMeta> metas(n_pairs);
-            c = cudaMemcpy(metas.data(), A.metas, n_pairs * sizeof(PairMeta), cudaMemcpyDeviceToHost);
-            if (c != cudaSuccess) return cuda_fail(e, c, "copy metas");
-            bool overflow = false;
-            for (int64_t p = 0; p < n_pairs; ++p)
-                if (metas[p].n_cand > ccap[p]) overflow = true;
-            if (!overflow) break;
-            if (pass == 1) return fail(e, PW_ERR_KERNEL, "candidate list overflow after resize");
-            std::vector<WorkItem> redo;
-            std::vector<int32_t> redo_cls;
-            int64_t pos = 0;
-            for (int64_t p = 0; p < n_pairs; ++p) {
-                cbase[p] = (int32_t)pos;
-                ccap[p] = std::max<int32_t>(kCandCap, metas[p].n_cand);
-                pos += ccap[p];
+        rc = run_phase<2>(e, A, e->items.as<WorkItem>(), begin, xm, &inf.trace_kernel_ms, &inf.trace_launches);
+        if (rc != PW_OK) return rc;
+        // candidate overflow: pairs with more candidates than their slot get an
+        // exact slot past the regular ones, and their items are swept again
+        std::vector<int32_t> ncand;
+        if ((c = download(e, ncand, A.n_cand, (size_t)n_pairs)) != cudaSuccess) return cuda_fail(e, c, "copy");
+        int64_t extra = 0;
+        std::vector<char> redo_item(wi.size(), 0);
+        for (int64_t p = 0; p < n_pairs; ++p)
+            if (ncand[p] > kCandCap) {
+                cbase[p] = cand_total + extra;
+                ccap[p] = ncand[p];
+                extra += ncand[p];
             }
-            if (pos > INT32_MAX) return fail(e, PW_ERR_CAPACITY, "too many starting-point candidates");
-            for (size_t k = 0; k < wave_items.size(); ++k) {
-                bool ov = false;
-                for (int l = 0; l < wave_items[k].lanes; ++l) {
-                    const int64_t p = wave_items[k].pair_base + l;
-                    if (metas[p].n_cand > kCandCap) ov = true;
-                }
-                if (ov) {
-                    redo.push_back(wave_items[k]);
-                    redo_cls.push_back(wave_cls[k]);
-                }
-            }
-            // keep the non-overflowing lists where they are: copy them over
-            std::vector<Cand> old_c((size_t)n_pairs * kCandCap);
-            c = cudaMemcpy(old_c.data(), A.cands, old_c.size() * sizeof(Cand), cudaMemcpyDeviceToHost);
+        if (extra > 0) {
+            DevBuf& nb = e->cands_alt;
+            if ((c = nb.reserve((cand_total + extra) * sizeof(Cand))) != cudaSuccess)
+                return cuda_fail(e, c, "alloc cands");
+            c = cudaMemcpyAsync(nb.p, e->cands.p, cand_total * sizeof(Cand), cudaMemcpyDeviceToDevice, e->stream);
             if (c != cudaSuccess) return cuda_fail(e, c, "copy cands");
-            std::vector<Cand> new_c((size_t)pos);
-            for (int64_t p = 0; p < n_pairs; ++p)
-                for (int k = 0; k < std::min<int>(metas[p].n_cand, kCandCap); ++k)
-                    new_c[cbase[p] + k] = old_c[(size_t)p * kCandCap + k];
-            if ((c = upload(e, e->cands, new_c)) != cudaSuccess) return cuda_fail(e, c, "upload cands");
+            std::swap(e->cands.p, nb.p);
+            std::swap(e->cands.bytes, nb.bytes);
+            cand_total += extra;
             if ((c = upload(e, e->cand_base, cbase)) != cudaSuccess) return cuda_fail(e, c, "upload cand base");
             if ((c = upload(e, e->cand_cap, ccap)) != cudaSuccess) return cuda_fail(e, c, "upload cand cap");
             A.cands = e->cands.as<Cand>();
-            A.cand_base = e->cand_base.as<int32_t>();
-            A.cand_cap = e->cand_cap.as<int32_t>();
-            wave_items = redo;
-            wave_cls = redo_cls;
-        }
-        cudaEventRecord(e->ev[1], e->stream);
-
-        // collect starting points
-        std::vector<WorkItem> wave_items_all(items2.begin() + i0, items2.begin() + i1);
-        {
-            int64_t d = 0, p = 0;
-            for (size_t k = 0; k < wave_items_all.size(); ++k) {
-                wave_items_all[k].index = (int32_t)k;
-                wave_items_all[k].dir_base = d;
-                wave_items_all[k].pair_base = p;
-                d += item_bytes[i0 + k];
-                p += wave_items_all[k].lanes;
+            std::vector<WorkItem> ri;
+            std::vector<int> rcl;
+            for (size_t k = 0; k < wi.size(); ++k) {
+                bool ov = false;
+                for (int l = 0; l < wi[k].lanes; ++l)
+                    if (ncand[wi[k].pair_base + l] > kCandCap) ov = true;
+                if (ov) {
+                    ri.push_back(wi[k]);
+                    rcl.push_back(wc[k]);
+                }
             }
+            int rb[kNumClasses + 1];
+            order_by_class(ri, rcl, rb);
+            if ((c = upload(e, e->items_alt, ri)) != cudaSuccess) return cuda_fail(e, c, "upload items");
+            rc = run_phase<2>(e, A, e->items_alt.as<WorkItem>(), rb, xm, &inf.trace_kernel_ms, &inf.trace_launches);
+            if (rc != PW_OK) return rc;
         }
-        if ((c = upload(e, e->items, wave_items_all)) != cudaSuccess) return cuda_fail(e, c, "upload items");
-        if ((c = e->n_starts.reserve(n_pairs * sizeof(int32_t))) != cudaSuccess) return cuda_fail(e, c, "alloc");
+
+        // starting points
+        if ((c = upload(e, e->items, by_index)) != cudaSuccess) return cuda_fail(e, c, "upload items");
         TraceArgs TA;
         memset(&TA, 0, sizeof(TA));
         TA.metas = A.metas;
@@ -743,83 +780,72 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
             PW_LAUNCH(collect_kernel<false>, gb, tb, 0, e->stream, TA);
         e->launches++;
         if ((c = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, c, "collect launch");
+        std::vector<int32_t> ns;
+        if ((c = download(e, ns, TA.n_starts, (size_t)n_pairs)) != cudaSuccess) return cuda_fail(e, c, "collect");
         cudaEventRecord(e->ev[2], e->stream);
-
-        // starting points to the host (emission order records, start cap)
-        std::vector<int32_t> ns(n_pairs);
-        std::vector<PairMeta> metas(n_pairs);
-        c = cudaMemcpyAsync(ns.data(), TA.n_starts, n_pairs * sizeof(int32_t), cudaMemcpyDeviceToHost, e->stream);
-        if (c != cudaSuccess) return cuda_fail(e, c, "copy n_starts");
-        c = cudaMemcpyAsync(metas.data(), A.metas, n_pairs * sizeof(PairMeta), cudaMemcpyDeviceToHost, e->stream);
-        if (c != cudaSuccess) return cuda_fail(e, c, "copy metas");
-        const int64_t cand_slots = (int64_t)cbase.back() + ccap.back();
-        std::vector<Cand> hc((size_t)cand_slots);
-        c = cudaMemcpyAsync(hc.data(), A.cands, hc.size() * sizeof(Cand), cudaMemcpyDeviceToHost, e->stream);
-        if (c != cudaSuccess) return cuda_fail(e, c, "copy starts");
-        if ((c = cudaStreamSynchronize(e->stream)) != cudaSuccess) return cuda_fail(e, c, "collect");
-        int64_t wave_starts = 0;
-        for (int64_t p = 0; p < n_pairs; ++p) {
-            wave_starts += ns[p];
-            const PairMeta& pm = metas[p];
+        std::vector<int64_t> soff(n_pairs + 1, 0);
+        for (int64_t p = 0; p < n_pairs; ++p) soff[p + 1] = soff[p] + ns[p];
+        const int64_t wave_starts = soff[n_pairs];
+        if ((c = upload(e, e->start_off, soff)) != cudaSuccess) return cuda_fail(e, c, "upload start offsets");
+        TA.start_off = e->start_off.as<int64_t>();
+        std::vector<StartOut> so;
+        std::vector<PairMeta> metas;
+        if (wave_starts > 0) {
+            if ((c = e->starts.reserve(wave_starts * sizeof(StartOut))) != cudaSuccess) return cuda_fail(e, c, "alloc");
+            PW_LAUNCH(gather_kernel, gb, tb, 0, e->stream, TA, e->starts.as<StartOut>());
+            e->launches++;
+            if ((c = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, c, "gather launch");
+            if ((c = download(e, so, e->starts.p, (size_t)wave_starts)) != cudaSuccess) return cuda_fail(e, c, "copy starts");
+            if ((c = download(e, metas, A.metas, (size_t)n_pairs)) != cudaSuccess) return cuda_fail(e, c, "copy metas");
+        }
+        const size_t first_rec = e->h_starts.size();
+        for (const StartOut& s : so) {
+            const PairMeta& pm = metas[s.pair];
             const int mn = std::min(qlen[pm.query], tlen[pm.target]);
             const float pos = (float)(e->highest * (double)mn * e->filter_factor);
-            for (int k = 0; k < ns[p]; ++k) {
-                const Cand& cc = hc[cbase[p] + k];
-                e->h_starts.push_back(StartRec{pm.query, pm.target, cc.x, cc.y, cc.score_f, pm.max_f, pos});
-            }
+            e->h_starts.push_back(StartRec{pm.query, pm.target, s.x, s.y, s.score, pm.max_f, pos});
         }
         total_starts += wave_starts;
-        const uint8_t* allowed_dev = nullptr;
+        TA.allowed = nullptr;
         if (start_cap >= 0 && total_starts >= start_cap) {
             if (waves.size() > 1)
                 return fail(e, PW_ERR_CAPACITY, "starting-point cap reached with more than one memory wave");
             // walk only the first start_cap starting points in emission order
-            std::vector<int64_t> idx(e->h_starts.size());
+            // (SmithWaterman.py:683-685)
+            std::vector<int64_t> idx(wave_starts);
             std::iota(idx.begin(), idx.end(), 0);
-            std::vector<int64_t> slot_of(e->h_starts.size());
-            {
-                int64_t s = 0;
-                for (int64_t p = 0; p < n_pairs; ++p)
-                    for (int k = 0; k < ns[p]; ++k) slot_of[s++] = cbase[p] + k;
-            }
-            auto key = [&](const StartRec& r) {
-                return std::make_tuple(-(int64_t)((r.x >> 3) + (r.y >> 3)), -(int64_t)(r.x >> 3), r.target, r.query,
-                                       -(int64_t)((r.x & 7) + (r.y & 7)), (int64_t)(r.y & 7));
-            };
-            std::stable_sort(idx.begin(), idx.end(),
-                             [&](int64_t a, int64_t b) { return key(e->h_starts[a]) < key(e->h_starts[b]); });
-            std::vector<uint8_t> allow((size_t)cand_slots, 0);
-            for (int64_t k = 0; k < start_cap && k < (int64_t)idx.size(); ++k) allow[slot_of[idx[k]]] = 1;
+            std::stable_sort(idx.begin(), idx.end(), [&](int64_t a, int64_t b) {
+                return emit_key_less(e->h_starts[first_rec + a], e->h_starts[first_rec + b]);
+            });
+            std::vector<uint8_t> allow((size_t)wave_starts, 0);
+            for (int64_t k = 0; k < start_cap && k < wave_starts; ++k) allow[idx[k]] = 1;
             if ((c = upload(e, e->allowed, allow)) != cudaSuccess) return cuda_fail(e, c, "upload allowed");
-            allowed_dev = e->allowed.as<uint8_t>();
+            TA.allowed = e->allowed.as<uint8_t>();
             inf.truncated = 1;
         }
 
         // walk
-        const int64_t max_hits = std::max<int64_t>(wave_starts, 1);
-        if ((c = e->hits.reserve(max_hits * sizeof(DevHit))) != cudaSuccess) return cuda_fail(e, c, "alloc hits");
-        if ((c = e->hit_count.reserve(16)) != cudaSuccess) return cuda_fail(e, c, "alloc");
-        cudaMemsetAsync(e->hit_count.p, 0, sizeof(int), e->stream);
-        TA.allowed = allowed_dev;
-        TA.hits = e->hits.as<DevHit>();
-        TA.hit_count = e->hit_count.as<int>();
-        TA.max_hits = (int)max_hits;
-        if (e->affine)
-            PW_LAUNCH(walk_kernel<true>, gb, tb, 0, e->stream, TA);
-        else
-            PW_LAUNCH(walk_kernel<false>, gb, tb, 0, e->stream, TA);
-        e->launches++;
-        if ((c = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, c, "walk launch");
         int nh = 0;
-        c = cudaMemcpyAsync(&nh, TA.hit_count, sizeof(int), cudaMemcpyDeviceToHost, e->stream);
-        if ((c = cudaStreamSynchronize(e->stream)) != cudaSuccess) return cuda_fail(e, c, "walk");
-        nh = (int)std::min<int64_t>(nh, max_hits);
-        std::vector<DevHit> hh(nh);
-        if (nh) {
-            c = cudaMemcpy(hh.data(), TA.hits, nh * sizeof(DevHit), cudaMemcpyDeviceToHost);
-            if (c != cudaSuccess) return cuda_fail(e, c, "copy hits");
+        std::vector<DevHit> hh;
+        if (wave_starts > 0) {
+            if ((c = e->hits.reserve(wave_starts * sizeof(DevHit))) != cudaSuccess) return cuda_fail(e, c, "alloc hits");
+            if ((c = e->hit_count.reserve(16)) != cudaSuccess) return cuda_fail(e, c, "alloc");
+            cudaMemsetAsync(e->hit_count.p, 0, sizeof(int), e->stream);
+            TA.hits = e->hits.as<DevHit>();
+            TA.hit_count = e->hit_count.as<int>();
+            TA.max_hits = (int)wave_starts;
+            if (e->affine)
+                PW_LAUNCH(walk_kernel<true>, gb, tb, 0, e->stream, TA);
+            else
+                PW_LAUNCH(walk_kernel<false>, gb, tb, 0, e->stream, TA);
+            e->launches++;
+            if ((c = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, c, "walk launch");
+            std::vector<int> cnt;
+            if ((c = download(e, cnt, TA.hit_count, 1)) != cudaSuccess) return cuda_fail(e, c, "walk");
+            nh = (int)std::min<int64_t>(cnt[0], wave_starts);
+            if ((c = download(e, hh, TA.hits, (size_t)nh)) != cudaSuccess) return cuda_fail(e, c, "copy hits");
         }
-        // column operations
+        // column operations of the kept hits
         int64_t ops_total = 0;
         for (int k = 0; k < nh; ++k) {
             hh[k].ops_offset = ops_total;
@@ -832,21 +858,15 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
             PW_LAUNCH(ops_kernel, (nh + 127) / 128, 128, 0, e->stream, TA, e->hits.as<DevHit>(), nh);
             e->launches++;
             if ((c = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, c, "ops launch");
-            std::vector<char> ops((size_t)ops_total);
-            if (ops_total) {
-                c = cudaMemcpyAsync(ops.data(), TA.ops, ops_total, cudaMemcpyDeviceToHost, e->stream);
-                if (c != cudaSuccess) return cuda_fail(e, c, "copy ops");
-            }
-            cudaEventRecord(e->ev[3], e->stream);
-            if ((c = cudaStreamSynchronize(e->stream)) != cudaSuccess) return cuda_fail(e, c, "ops");
+            std::vector<char> ops;
+            if ((c = download(e, ops, TA.ops, (size_t)ops_total)) != cudaSuccess) return cuda_fail(e, c, "copy ops");
             const int64_t base = (int64_t)all_ops.size();
             for (int k = 0; k < nh; ++k) hh[k].ops_offset += base;
             all_ops.insert(all_ops.end(), ops.begin(), ops.end());
             all_hits.insert(all_hits.end(), hh.begin(), hh.end());
-        } else {
-            cudaEventRecord(e->ev[3], e->stream);
-            cudaStreamSynchronize(e->stream);
         }
+        cudaEventRecord(e->ev[3], e->stream);
+        cudaStreamSynchronize(e->stream);
         float t1 = 0, t2 = 0;
         cudaEventElapsedTime(&t1, e->ev[0], e->ev[2]);
         cudaEventElapsedTime(&t2, e->ev[2], e->ev[3]);
@@ -972,5 +992,25 @@ extern "C" int pw_get_starting_points(pw_engine* e, void* out36, int64_t max_poi
 extern "C" int pw_last_launch_count(pw_engine* e, int64_t* n) {
     if (!e || !n) return PW_ERR_ARG;
     *n = e->launches;
+    return PW_OK;
+}
+
+extern "C" int pw_measure_int_peak(pw_engine* e, double* ops_per_second, double* ms_out) {
+    if (!e || !ops_per_second) return PW_ERR_ARG;
+    cudaSetDevice(e->device);
+    cudaError_t c;
+    if ((c = e->counter.reserve(64 * sizeof(int))) != cudaSuccess) return cuda_fail(e, c, "alloc");
+    const int threads = 256, blocks = e->sm_count * 8, iters = 4096;
+    // warm-up, then the timed launch
+    PW_LAUNCH(int_peak_kernel, blocks, threads, 0, e->stream, 64, 1, e->counter.as<int>());
+    cudaEventRecord(e->ev[0], e->stream);
+    PW_LAUNCH(int_peak_kernel, blocks, threads, 0, e->stream, iters, 3, e->counter.as<int>());
+    cudaEventRecord(e->ev[1], e->stream);
+    if ((c = cudaStreamSynchronize(e->stream)) != cudaSuccess) return cuda_fail(e, c, "int peak probe");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e->ev[0], e->ev[1]);
+    const double instr = (double)blocks * threads * iters * 16.0 * 8.0;
+    *ops_per_second = ms > 0 ? 2.0 * instr / (ms * 1e-3) : 0.0;
+    if (ms_out) *ms_out = ms;
     return PW_OK;
 }

@@ -392,9 +392,9 @@ struct KernelArgs {
     uint8_t* codes;
     PairMeta* metas;
     Cand* cands;
-    const int32_t* cand_base;  // per pair slot: first candidate
+    const int64_t* cand_base;  // per pair slot: first candidate
     const int32_t* cand_cap;   // per pair slot: capacity
-    unsigned long long* launches;  // diagnostic counter (unused on device)
+    int32_t* n_cand;           // per pair slot: candidates found (may exceed the capacity)
 };
 
 template <typename T>
@@ -491,8 +491,10 @@ __global__ void __launch_bounds__(128) sweep_kernel(KernelArgs A) {
         if (active) {
             if (PHASE == 1)
                 A.pair_max[(int64_t)q * A.nt + t] = (float)mx;
-            else
+            else {
                 A.metas[pslot].n_cand = n_cand;
+                A.n_cand[pslot] = n_cand;
+            }
         }
     }
 }
@@ -504,11 +506,12 @@ struct TraceArgs {
     const WorkItem* items;
     uint8_t* codes;
     Cand* cands;
-    const int32_t* cand_base;
+    const int64_t* cand_base;
     int32_t* n_starts;       // per pair: starting points (after collect)
     SeqSet q, t;
     ScoreParams P;
-    const uint8_t* allowed;  // per candidate slot: walk this start (start cap); null = all
+    const uint8_t* allowed;  // per start (packed order, see gather_kernel): walk it; null = all
+    const int64_t* start_off; // per pair: first packed start index
     DevHit* hits;
     int* hit_count;
     int max_hits;
@@ -651,7 +654,7 @@ __global__ void walk_kernel(TraceArgs A) {
     const uint8_t* ts = A.t.raw + A.t.raw_off[pm.target];
     const bool same_id = A.q.key[pm.query] == A.t.key[pm.target];
     for (int k = 0; k < m; ++k) {
-        if (A.allowed && !A.allowed[A.cand_base[p] + k]) continue;
+        if (A.allowed && !A.allowed[A.start_off[p] + k]) continue;
         const Cand st = cl[k];
         int x = st.x, y = st.y;
         int dir = walk_direction<AFFINE>(v, x, y);
@@ -741,6 +744,54 @@ __global__ void ops_kernel(TraceArgs A, const DevHit* hits, int n_hits) {
         }
         o[H.n_cols - 1 - k] = op;
     }
+}
+
+// Packs every pair's ordered starting points into one array (pair slot, cell,
+// score) so that the host reads only what exists.
+struct StartOut {
+    int32_t pair, x, y;
+    float score;
+};
+
+__global__ void gather_kernel(TraceArgs A, StartOut* out) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= A.n_pairs) return;
+    const Cand* cl = A.cands + A.cand_base[p];
+    const int m = A.n_starts[p];
+    const int64_t o = A.start_off[p];
+    for (int k = 0; k < m; ++k) {
+        StartOut s;
+        s.pair = p;
+        s.x = cl[k].x;
+        s.y = cl[k].y;
+        s.score = cl[k].score_f;
+        out[o + k] = s;
+    }
+}
+
+// Integer issue-rate probe for the roofline denominator: independent chains
+// of the DPX add-max used by the recurrences (one __viaddmax_s32 = one add +
+// one max).  Each thread runs 8 independent chains; the result is stored so
+// that nothing is optimised away.
+__global__ void int_peak_kernel(int iters, int seed, int* sink) {
+    int a0 = threadIdx.x + seed, a1 = a0 + 1, a2 = a0 + 2, a3 = a0 + 3, a4 = a0 + 4, a5 = a0 + 5, a6 = a0 + 6,
+        a7 = a0 + 7;
+    const int b = seed & 7, c = -seed;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+            a0 = __viaddmax_s32(a0, b, c);
+            a1 = __viaddmax_s32(a1, b, c);
+            a2 = __viaddmax_s32(a2, b, c);
+            a3 = __viaddmax_s32(a3, b, c);
+            a4 = __viaddmax_s32(a4, b, c);
+            a5 = __viaddmax_s32(a5, b, c);
+            a6 = __viaddmax_s32(a6, b, c);
+            a7 = __viaddmax_s32(a7, b, c);
+        }
+    }
+    const int r = a0 ^ a1 ^ a2 ^ a3 ^ a4 ^ a5 ^ a6 ^ a7;
+    if (r == 0x7fffffff) sink[0] = r;
 }
 
 }  // namespace pw

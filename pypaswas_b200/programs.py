@@ -1,0 +1,52 @@
+"""The aligner and trimmer programs (pyPaSWAS/Core/Programs.py:9-120) on the
+B200 backend.  ``process`` keeps the reference's loop over target blocks and
+merges the per-block HitLists with HitList.extend."""
+import logging
+
+from .hits import HitList
+from .scores import make_score
+from .smith_waterman import SmithWatermanB200
+
+
+class Aligner(object):
+    """Aligns query records against target records (Programs.py:9-86)."""
+
+    def __init__(self, logger, score, settings, device=None):
+        self.logger = logger or logging.getLogger("pypaswas_b200")
+        self.settings = settings
+        self.score = score if score is not None else make_score(settings, self.logger)
+        self.hitlist = HitList(self.logger)
+        self.smith_waterman = SmithWatermanB200(self.logger, self.score, settings, device=device)
+
+    def process(self, records_seqs, targets, pypaswas=None):
+        self.hitlist = HitList(self.logger)
+        target_index = 0
+        all_targets_length = sum(len(s.seq) for s in targets)
+        all_sequences_length = sum(len(s.seq) for s in records_seqs)
+        self.smith_waterman.set_total_work_size(all_targets_length * all_sequences_length)
+        while target_index < len(targets):
+            last = self.smith_waterman.set_targets(targets, target_index, records_seqs=records_seqs,
+                                                   use_all_records_seqs=False)
+            results = self.smith_waterman.align_sequences(records_seqs, targets, target_index)
+            self.hitlist.extend(results)
+            target_index = last
+        return self.hitlist
+
+
+class Trimmer(Aligner):
+    """Same loop; output goes through the trimmedFasta formatter (Programs.py:95-120)."""
+
+    def process(self, records_seqs, targets, pypaswas=None):
+        self.hitlist = HitList(self.logger)
+        target_index = 0
+        max_length = len(targets[0]) if len(targets) > 0 and getattr(self.settings, "recompile", "T") == "F" \
+            else None
+        all_targets_length = sum(len(s.seq) for s in targets)
+        all_sequences_length = sum(len(s.seq) for s in records_seqs)
+        self.smith_waterman.set_total_work_size(all_targets_length * all_sequences_length)
+        while target_index < len(targets):
+            last = self.smith_waterman.set_targets(targets, target_index, max_length, records_seqs)
+            results = self.smith_waterman.align_sequences(records_seqs, targets, target_index)
+            self.hitlist.extend(results)
+            target_index = last
+        return self.hitlist

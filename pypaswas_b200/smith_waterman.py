@@ -1,0 +1,176 @@
+"""SmithWatermanB200: the pyPaSWAS driver interface on the B200 engine.
+
+Public interface of pyPaSWAS/Core/SmithWaterman.py:
+  set_total_work_size(size)                                  (:434-439)
+  set_targets(targets, target_index, max_length=None,
+              records_seqs=None, use_all_records_seqs=True) -> next index  (:370-414)
+  align_sequences(records_seqs, targets, target_index) -> HitList         (:441-560)
+  _filter_hit(hit)                                           (:843-848)
+
+The reference splits the work into memory-sized batches, pads every sequence
+with '\\0' to a multiple of 8 and launches one kernel per block anti-diagonal.
+Here one call hands all queries and the whole target block to the engine,
+which batches internally (length-binned work items, memory waves) and returns
+the hits in the order the reference's walk produces them.  Hit and HitList
+objects are built exactly as SmithWaterman._print_alignments builds them
+(:822-838).
+
+Queries are aligned in full.  (The reference truncates a query that is longer
+than the first query of its batch, SWSeq.extentToFillGPU, which only happens
+when callers pass records that are not sorted by length; its CLI always
+sorts.)
+"""
+import logging
+import math
+import time
+
+import numpy as np
+
+from . import _native
+from .exceptions import InvalidOptionException
+from .hits import Hit, HitList
+
+
+def id_keys(query_ids, target_ids):
+    """Integer keys per record, equal exactly when the ids are equal."""
+    table = {}
+    qk = np.array([table.setdefault(i, len(table)) for i in query_ids], dtype=np.int32)
+    tk = np.array([table.setdefault(i, len(table)) for i in target_ids], dtype=np.int32)
+    return qk, tk
+
+
+def configure_engine(engine, score, settings):
+    """Scoring model and thresholds as the reference's kernels see them."""
+    gap, ext, affine, ll, mn = score.kernel_constants()
+    engine.set_scoring(score.matrix_array(), score.char_offset_code(), gap, ext, affine, ll, mn,
+                       float(settings.minimum_score), float(score.highest_score), float(_filter_factor(settings)))
+
+
+def _filter_factor(settings):
+    ff = getattr(settings, "filter_factor", None)
+    try:
+        return float(ff) if ff else 0.7  # SmithWaterman.py:167,309-315
+    except ValueError:
+        raise InvalidOptionException("Filterfactor should be a float but is {0}".format(ff))
+
+
+class SmithWatermanB200(object):
+    """Drop-in for SmithWatermanCuda: same constructor and driver methods."""
+
+    def __init__(self, logger, score, settings, device=None):
+        self.logger = logger or logging.getLogger("pypaswas_b200")
+        self.score = score
+        self.settings = settings
+        self.device = int(device if device is not None else (getattr(settings, "device_number", 0) or 0))
+        self.filter_factor = _filter_factor(settings)
+        try:
+            self.mem_fill_factor = float(getattr(settings, "maximum_memory_usage", 0.8))
+        except ValueError:
+            raise InvalidOptionException("maximux_memory_usage is not a float")
+        if self.mem_fill_factor > 1.0 or self.mem_fill_factor <= 0.0:
+            raise InvalidOptionException("maximux_memory_usage is not a float between 0.0 and 1.0")
+        self.gap_extension = score.gap_extension is not None
+        self.engine = _native.Engine(self.device)
+        configure_engine(self.engine, score, settings)
+        self.number_of_targets = 0
+        self.number_targets = 0
+        self.total_work_size = 0
+        self.total_processed = 0
+        self.start_time = time.time()
+        self.maximum_number_starting_points = 100  # per pair, SmithWaterman.py:144
+        self.last_info = None
+        self.last_h2d_bytes = 0
+        self.last_d2h_bytes = 0
+
+    def set_total_work_size(self, size):
+        self.total_work_size = size
+        self.total_processed = 0
+        self.start_time = time.time()
+
+    def set_targets(self, targets, target_index, max_length=None, records_seqs=None, use_all_records_seqs=True):
+        """Selects the next block of targets; the engine takes all remaining ones."""
+        self.number_of_targets = len(targets) - target_index
+        self.number_targets = self.number_of_targets
+        self._block = (targets, target_index)
+        return target_index + self.number_of_targets
+
+    def _upload(self, records_seqs, targets, target_index):
+        """Hands the records to the engine (copy_sequences, SmithWatermanCuda.py:176-184);
+        returns the target block and the bytes sent to the device."""
+        block = targets[target_index:target_index + self.number_targets]
+        qkeys, tkeys = id_keys([r.id for r in records_seqs], [r.id for r in block])
+        qs = [str(r.seq).upper().encode("latin-1") for r in records_seqs]
+        ts = [str(r.seq).upper().encode("latin-1") for r in block]
+        self.engine.set_queries(qs, qkeys)
+        self.engine.set_targets(ts, tkeys)
+        h2d = sum(map(len, qs)) + sum(map(len, ts)) + 12 * (len(qs) + len(ts)) + 16
+        return block, h2d
+
+    def align_sequences(self, records_seqs, targets, target_index):
+        """Aligns every record against the current target block; returns a HitList."""
+        hitlist = HitList(self.logger)
+        if self.number_targets <= 0:
+            self.set_targets(targets, target_index)
+        if len(records_seqs) == 0 or self.number_targets == 0:
+            return hitlist
+        t0 = time.time()
+        block, h2d = self._upload(records_seqs, targets, target_index)
+        cap = self.maximum_number_starting_points * len(records_seqs) * len(block)
+        info = self.engine.align(start_cap=cap)
+        self.last_info = info
+        if info.truncated:
+            self.logger.warning("Too many hits returned. Skipping the rest. Please set lower_limit_score "
+                                "higher in config.")
+        hits, strbuf = self.engine.hits()
+        self.last_h2d_bytes = h2d
+        self.last_d2h_bytes = 4 * len(records_seqs) * len(block) + hits.nbytes + len(strbuf)
+        self._build_hits(hits, strbuf, records_seqs, block, hitlist)
+        self._progress(records_seqs, block, t0)
+        return hitlist
+
+    def _build_hits(self, hits, strbuf, sequences, targets, hit_list):
+        """Hit objects in walk order (SmithWaterman._print_alignments :822-838)."""
+        q_col = hits["query"].tolist()
+        t_col = hits["target"].tolist()
+        ss, se = hits["s_start"].tolist(), hits["s_end"].tolist()
+        ts_, te = hits["t_start"].tolist(), hits["t_end"].tolist()
+        sc = hits["score"].tolist()
+        mt, mm = hits["matches"].tolist(), hits["mismatches"].tolist()
+        nc, so = hits["n_cols"].tolist(), hits["str_offset"].tolist()
+        text = strbuf.decode("latin-1")
+        for k in range(len(q_col)):
+            seq_rec, tgt_rec = sequences[q_col[k]], targets[t_col[k]]
+            sp = getattr(seq_rec, "start_position", 0)
+            tp = getattr(tgt_rec, "start_position", 0)
+            if not hasattr(seq_rec, "distance"):
+                seq_rec.distance = 0.0
+            hit = Hit(self.logger, seq_rec, tgt_rec, (ss[k] + sp, se[k] + sp), (ts_[k] + tp, te[k] + tp))
+            n, o = nc[k], so[k]
+            hit.set_sequence_match(text[o:o + n])
+            hit.set_alignment(text[o + n:o + 2 * n])
+            hit.set_target_match(text[o + 2 * n:o + 3 * n])
+            hit.set_scores(sc[k], mt[k], mm[k])
+            if self._filter_hit(hit):
+                hit_list.append(hit)
+
+    def _filter_hit(self, hit):
+        s = self.settings
+        return (hit.relative_score >= float(s.relative_score) and hit.query_identity >= float(s.query_identity)
+                and hit.query_coverage >= float(s.query_coverage) and hit.base_score >= float(s.base_score))
+
+    def _progress(self, sequences, targets, t0):
+        """GCUPS progress line of SmithWaterman.py:544-557."""
+        if self.total_work_size <= 0:
+            return
+        t1 = time.time()
+        processed = sum(len(s.seq) for s in targets) * sum(len(s.seq) for s in sequences)
+        self.total_processed += processed
+        duration = max(t1 - t0, 1e-9)
+        total = max(t1 - self.start_time, 1e-9)
+        progress = self.total_processed / float(self.total_work_size)
+        self.logger.info("Duration: {:5.3f} | Performance: {:5.2f} GCUPS | Avg: {:5.2f} GCUPS | Progress: {:7.3%}"
+                         .format(duration, processed / 1e9 / duration, self.total_processed / 1e9 / total,
+                                 progress))
+
+    def close(self):
+        self.engine.close()

@@ -1,0 +1,89 @@
+"""Host-side semantics that need no GPU: Hit validation and ratios, HitList
+de-duplication, id keys, records and reverse complements."""
+import numpy as np
+import pytest
+
+from pypaswas_b200.exceptions import CudaException, InvalidOptionException
+from pypaswas_b200.hits import Hit, HitList
+from pypaswas_b200.records import SeqRecord, complement_records, sort_records
+from pypaswas_b200.smith_waterman import id_keys
+from pypaswas_b200 import scores, workloads
+
+
+def _hit(s, t, sl, tl, score=10.0, aln="||||"):
+    h = Hit(None, s, t, sl, tl)
+    h.set_alignment(aln)
+    h.set_scores(score, 4, 0)
+    return h
+
+
+def test_hit_location_rules():
+    s, t = SeqRecord("ACGTACGT", "q"), SeqRecord("ACGT", "t")
+    _hit(s, t, (0, 3), (0, 3))
+    for bad in [(3, 3), (4, 3), (0, 8), (-1, 2)]:
+        with pytest.raises(CudaException):
+            Hit(None, s, t, bad, (0, 3))
+    with pytest.raises(CudaException):
+        Hit(None, s, t, (0, 3), (0, 4))
+
+
+def test_hit_ratios():
+    s, t = SeqRecord("ACGTACGT", "q"), SeqRecord("ACGTAC", "t")
+    h = _hit(s, t, (1, 4), (0, 3), score=8.0)
+    assert h.relative_score == 8.0 / 6
+    assert h.query_identity == 4 / 4.0
+    assert h.query_coverage == 4 / 8.0
+    assert h.base_score == 8.0 / 4
+    with pytest.raises(CudaException):
+        h.set_scores(-1.0, 1, 1)
+    with pytest.raises(CudaException):
+        h.set_scores(1.0, 1.5, 1)
+
+
+def test_hitlist_keeps_best_per_start_and_end():
+    s, t = SeqRecord("A" * 20, "q"), SeqRecord("A" * 20, "t")
+    hl = HitList()
+    a = _hit(s, t, (0, 5), (0, 5), 5.0)
+    b = _hit(s, t, (0, 7), (0, 7), 7.0)  # same start, better
+    c = _hit(s, t, (1, 7), (1, 7), 3.0)  # same end as b, worse: rejected
+    d = _hit(s, t, (2, 7), (2, 7), 9.0)  # same end as b, better: replaces b
+    for h in (a, b, c, d):
+        hl.append(h)
+    assert list(hl.real_hits.values()) == [d]
+    assert hl.hits[("q", "t", 0, 0)] is b
+
+
+def test_id_keys_equal_exactly_for_equal_ids():
+    qk, tk = id_keys(["a", "b", "a"], ["b", "c"])
+    assert qk[0] == qk[2] and qk[1] == tk[0] and len({qk[0], qk[1], tk[1]}) == 3
+
+
+def test_records_and_reverse_complement():
+    r = SeqRecord(b"acgtNKM", "x")
+    assert str(r.seq) == "ACGTNKM" and r.original_length == 7
+    rc = complement_records([r])
+    assert [x.id for x in rc] == ["x", "x_RC"] and str(rc[1].seq) == "KMNACGT"
+    assert [len(x) for x in sort_records([SeqRecord("A", "1"), SeqRecord("AAA", "2")])] == [3, 1]
+    assert workloads.reverse_complement(b"ACGTU") == b"AACGT"
+
+
+def test_scores_highest_and_errors():
+    st = workloads.Settings(matrix_name="BLOSUM62")
+    assert scores.make_score(st).highest_score == 4  # max(max(matrix)): the 'A' row
+    assert scores.make_score(workloads.Settings(matrix_name="BLOSUM80")).highest_score == 7
+    with pytest.raises(InvalidOptionException):
+        scores.make_score(workloads.Settings(matrix_name="PAM250"))
+    with pytest.raises(InvalidOptionException):
+        scores.make_score(workloads.Settings(matrix_name="CUSTOM"))
+    b = scores.make_score(workloads.Settings(matrix_name="BASIC", match_score="2", mismatch_score="-1"))
+    m = b.matrix_array()
+    assert m.shape == (255, 255) and m[5, 5] == 2 and m[5, 6] == -1 and b.char_offset_code() == 1
+    ir = scores.make_score(workloads.Settings(matrix_name="IRYS", match_score="3", mismatch_score="-0.5"))
+    assert ir.matrix_array().shape == (62, 62) and ir.matrix_array()[0, 3] == np.float32(-1.5)
+
+
+def test_kernel_constants_follow_compiled_literals():
+    st = workloads.Settings(gap_score="-5", gap_extension="0", lower_limit_score="0.1", minimum_score="15.3")
+    gap, ext, affine, ll, mn = scores.make_score(st).kernel_constants()
+    assert not affine and gap == np.float32(-5.0) and ext == 0
+    assert ll == np.float32(0.1) and mn == np.float32(15.3)
