@@ -56,7 +56,8 @@ typedef struct {
 typedef struct {
     int64_t pairs;          /* query x target pairs aligned */
     int64_t cells;          /* sum of len(q) * len(t) over the pairs */
-    int64_t traced_pairs;   /* pairs whose maximum reached the minimum score */
+    int64_t traced_pairs;   /* pairs swept for starting points (maximum reaches the start threshold) */
+    int64_t minimum_pairs;  /* pairs whose maximum reached MINIMUM_SCORE */
     int64_t starting_points;
     int64_t hits;           /* hits kept by the walk (before the Python filter) */
     int64_t string_bytes;   /* bytes needed for all hit strings (3 * n_cols summed) */

@@ -52,6 +52,7 @@ START_DTYPE = np.dtype([("sequence", "<u4"), ("target", "<u4"), ("block_x", "<u4
 
 class PwRunInfo(ctypes.Structure):
     _fields_ = [("pairs", ctypes.c_int64), ("cells", ctypes.c_int64), ("traced_pairs", ctypes.c_int64),
+                ("minimum_pairs", ctypes.c_int64),
                 ("starting_points", ctypes.c_int64), ("hits", ctypes.c_int64), ("string_bytes", ctypes.c_int64),
                 ("kernel_launches", ctypes.c_int32), ("truncated", ctypes.c_int32), ("score_ms", ctypes.c_double),
                 ("trace_ms", ctypes.c_double), ("walk_ms", ctypes.c_double),

@@ -617,17 +617,29 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     }
 
     // ---------------------------------------------------------- phase 2
-    // pairs whose maximum reaches MINIMUM_SCORE (default_main.cu:596), per
-    // target in query length order, 32 per work item
+    // Pairs that can yield a starting point, per target in query length order,
+    // 32 per work item.  The reference traces every pair whose maximum reaches
+    // MINIMUM_SCORE (default_main.cu:596), but a starting point also needs a
+    // cell with H >= max(LOWER_LIMIT_SCORE * max, maxPossibleScore) (:609) and
+    // no cell exceeds the pair maximum, so a pair whose maximum is below that
+    // threshold has no starting point and contributes nothing: it is skipped.
     std::vector<int32_t> p2_order;
     std::vector<WorkItem> items2;
     std::vector<int> cls2;
     std::vector<int64_t> bytes2;
+    int64_t min_pass = 0;
     for (int t = 0; t < nt; ++t) {
         std::vector<int32_t> pass;
         for (int sp = 0; sp < nq; ++sp) {
             const int q = pr.order[sp];
-            if (e->h_pair_max[(size_t)q * nt + t] >= e->minimum_score) pass.push_back(q);
+            const float mx = e->h_pair_max[(size_t)q * nt + t];
+            if (!(mx >= e->minimum_score)) continue;
+            ++min_pass;
+            const int mn = std::min(qlen[q], tlen[t]);
+            const float pos = (float)(e->highest * (double)mn * e->filter_factor);
+            const volatile float llm = e->lower_limit * mx;  // fp32 product, as the kernel computes it
+            const float thr = std::max((float)llm, pos);
+            if (mx >= thr) pass.push_back(q);
         }
         const int per_item = plain ? 1 : kWarp;
         for (size_t g = 0; g < pass.size(); g += per_item) {
@@ -647,6 +659,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         }
     }
     inf.traced_pairs = (int64_t)p2_order.size();
+    inf.minimum_pairs = min_pass;
     if (p2_order.empty()) {
         inf.kernel_launches = (int32_t)e->launches;
         if (info) *info = inf;
