@@ -152,6 +152,30 @@ int pw_last_launch_count(pw_engine* e, int64_t* n);
  * operations.  Used as the roofline denominator by bench.py. */
 int pw_measure_int_peak(pw_engine* e, double* ops_per_second, double* ms);
 
+/* Pair maxima without any device allocation.  No counterpart in the
+ * reference: it serves callers that cannot call cudaMalloc themselves or have
+ * the library do it -- code running where another component owns all device
+ * memory (a framework's caching allocator, a fixed serving budget), or a
+ * latency-critical path where cudaMalloc's implicit device synchronisation
+ * is not acceptable.
+ *
+ * Same result as pw_align() with PW_FLAG_SCORE_ONLY followed by
+ * pw_get_pair_max(): every query (x axis) against every target (y axis),
+ * pair_max[q * nt + t], host buffers in and out, no engine needed.  Scoring
+ * arguments are those of pw_set_scoring().  All device working memory is one
+ * 64 MiB array inside the library that every GPU loading the library keeps
+ * until the process exits; inputs whose staged size (sequences, work list,
+ * results and the boundary rows of targets longer than one strip) exceeds it
+ * are rejected with PW_ERR_CAPACITY and a message in err.  Calls share that
+ * array: the library serialises them with a host lock, and their GPU work must
+ * not overlap with other users of it.  The first call on a device looks up the
+ * array's device address (make it before any stream capture on that device).
+ * Runs on the legacy default stream and returns when pair_max is filled. */
+int pw_score_max_noalloc(int device, const float* matrix, int dim, int char_offset, float gap, float ext,
+                         int affine, const uint8_t* q_residues, const int64_t* q_offsets, int32_t n_queries,
+                         const uint8_t* t_residues, const int64_t* t_offsets, int32_t n_targets, float* pair_max,
+                         char* err, int32_t err_bytes);
+
 #ifdef __cplusplus
 }
 #endif

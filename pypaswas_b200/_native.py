@@ -29,7 +29,7 @@ PW_FLAG_PLAIN = 2
 EXPORTED_SYMBOLS = (
     "pw_create", "pw_destroy", "pw_last_error", "pw_device_free_memory", "pw_set_scoring",
     "pw_set_queries", "pw_set_targets", "pw_align", "pw_get_pair_max", "pw_get_hits",
-    "pw_get_starting_points", "pw_last_launch_count", "pw_measure_int_peak",
+    "pw_get_starting_points", "pw_last_launch_count", "pw_measure_int_peak", "pw_score_max_noalloc",
 )
 
 
@@ -81,6 +81,8 @@ def bind(lib):
         "pw_get_starting_points": (ctypes.c_int, [P, P, I64, ctypes.POINTER(I64)]),
         "pw_last_launch_count": (ctypes.c_int, [P, ctypes.POINTER(I64)]),
         "pw_measure_int_peak": (ctypes.c_int, [P, ctypes.POINTER(D), ctypes.POINTER(D)]),
+        "pw_score_max_noalloc": (ctypes.c_int, [ctypes.c_int, P, ctypes.c_int, ctypes.c_int, F, F, ctypes.c_int,
+                                                P, P, I32, P, P, I32, P, ctypes.c_char_p, I32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -226,3 +228,25 @@ class Engine(object):
         _check(self.lib, self.handle, self.lib.pw_last_launch_count(self.handle, ctypes.byref(n)),
                "pw_last_launch_count")
         return n.value
+
+
+def score_max_noalloc(device, matrix, char_offset, gap, ext, affine, queries, targets, lib=None):
+    """Pair maxima [n_queries, n_targets] through pw_score_max_noalloc: the
+    library allocates no device memory for this call (see the header)."""
+    lib = lib if lib is not None else load_library()
+    m = np.ascontiguousarray(matrix, dtype=np.float32)
+    qb, qo = pack_sequences(queries)
+    tb, to = pack_sequences(targets)
+    out = np.zeros((len(queries), len(targets)), dtype=np.float32)
+    err = ctypes.create_string_buffer(512)
+    rc = lib.pw_score_max_noalloc(int(device), _ptr(m), int(m.shape[0]), int(char_offset), float(gap), float(ext),
+                                  int(bool(affine)), _ptr(qb), _ptr(qo), len(queries), _ptr(tb), _ptr(to),
+                                  len(targets), _ptr(out), err, len(err))
+    if rc != PW_OK:
+        msg = "pw_score_max_noalloc failed (%d): %s" % (rc, err.value.decode())
+        if rc == PW_ERR_ARG:
+            raise InvalidOptionException(msg)
+        if rc == PW_ERR_DEVICE:
+            raise HardwareException(msg)
+        raise CudaException(msg)
+    return out

@@ -9,7 +9,7 @@ import sys
 PACKAGE_DIR = os.path.dirname(os.path.abspath(__file__))
 REPO_DIR = os.path.dirname(PACKAGE_DIR)
 CSRC = os.path.join(PACKAGE_DIR, "csrc")
-SOURCES = [os.path.join(CSRC, "engine.cu")]
+SOURCES = [os.path.join(CSRC, "engine.cu"), os.path.join(CSRC, "noalloc.cu")]
 DEPENDS = SOURCES + [os.path.join(CSRC, f) for f in ("pw_device.cuh", "pw_kernels.cuh")] + [
     os.path.join(REPO_DIR, "include", "paswas_b200.h")]
 LIBRARY = os.path.join(PACKAGE_DIR, "libpaswas_b200.so")

@@ -718,6 +718,9 @@ __global__ void walk_kernel(TraceArgs A) {
     }
 }
 
+// Translation units that only need the score sweep define PW_SCORE_SWEEP_ONLY
+// so that these non-template kernels are emitted once, by engine.cu.
+#ifndef PW_SCORE_SWEEP_ONLY
 // Column operations of each hit, in alignment order: 'M' both residues,
 // 'I' query residue against a gap, 'D' target residue against a gap.
 __global__ void ops_kernel(TraceArgs A, const DevHit* hits, int n_hits) {
@@ -793,5 +796,7 @@ __global__ void int_peak_kernel(int iters, int seed, int* sink) {
     const int r = a0 ^ a1 ^ a2 ^ a3 ^ a4 ^ a5 ^ a6 ^ a7;
     if (r == 0x7fffffff) sink[0] = r;
 }
+
+#endif  // PW_SCORE_SWEEP_ONLY
 
 }  // namespace pw
