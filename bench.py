@@ -268,7 +268,10 @@ def main():
         dom, dom_ms, dom_launch = "score sweep (sweep_kernel phase 1)", score_ms, sum(
             i["score_launches"] for i in infos)
         ops = cells * OPS_PER_CELL[(mode, "score")] * args.steps
-    peak_ops, _ = e.measure_int_peak()
+    peak32, peak16, _ = e.measure_int_peak()
+    lanes16 = "score" in dom and last.get("overflow_pairs", 0) == 0 and not last.get("int32", False) and \
+        _sixteen_bit(e, w)
+    peak_ops = peak16 if lanes16 else peak32
     achieved = ops / (dom_ms * 1e-3) / 1e12
     traffic = load_traffic().get("direction_sweep_bytes_per_launch" if "direction" in dom else
                                  "score_sweep_bytes_per_launch")
@@ -291,7 +294,8 @@ def main():
            "clocks": clocks,
            "roofline": {"bound": "int_alu", "kernel": dom, "achieved": achieved,
                         "peak": peak_ops / 1e12, "unit": "Tops/s", "frac": achieved / (peak_ops / 1e12),
-                        "peak_source": "measured in this run: DPX add-max issue probe (pw_measure_int_peak)",
+                        "peak_source": "measured in this run: DPX add-max issue probe (pw_measure_int_peak), "
+                                       + ("16x2 form" if lanes16 else "32-bit form"),
                         "ops_per_cell": OPS_PER_CELL[(mode, "dirs" if "direction" in dom else "score")],
                         "launches": dom_launch, "avg_launch_ms": dom_ms / max(1, dom_launch),
                         "traffic": traffic,
@@ -306,6 +310,18 @@ def main():
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
     return 0
+
+
+def _sixteen_bit(engine, w):
+    """The score sweep ran on 16-bit lanes (integer scores; see pw_score16.cuh)."""
+    return engine.last_info is not None and engine.last_info.score_launches > 0 and \
+        engine.last_info.overflow_pairs == 0 and _integer_scores(w)
+
+
+def _integer_scores(w):
+    from pypaswas_b200 import scores
+    m = scores.make_score(w.settings).matrix_array()
+    return bool(np.all(np.floor(m) == m) and np.all(np.abs(m) <= 127))
 
 
 def _traced_cells(engine, w):

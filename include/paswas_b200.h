@@ -34,6 +34,7 @@ extern "C" {
 /* pw_align() flags */
 #define PW_FLAG_SCORE_ONLY 1u /* pair maxima only: no starting points, no walk */
 #define PW_FLAG_PLAIN 2u      /* one pair per kernel launch (the unbatched form) */
+#define PW_FLAG_INT32 4u      /* keep the score sweep on 32-bit lanes (no 16-bit dual-pair sweep) */
 
 typedef struct pw_engine pw_engine;
 
@@ -67,6 +68,8 @@ typedef struct {
     double score_kernel_ms; /* summed duration of the score-sweep launches */
     double trace_kernel_ms; /* summed duration of the direction-sweep launches */
     int32_t score_launches, trace_launches;
+    int32_t orientation;    /* score sweep lanes: 0 = queries, 1 = targets */
+    int64_t overflow_pairs; /* pairs recomputed on 32-bit lanes after reaching the 16-bit limit */
 } pw_run_info;
 
 /* Creates an engine on CUDA device `device`.
@@ -146,11 +149,13 @@ int pw_get_starting_points(pw_engine* e, void* out36, int64_t max_points, int64_
 /* Number of this library's kernels launched by the last pw_align. */
 int pw_last_launch_count(pw_engine* e, int64_t* n);
 
-/* Measurement helper (no counterpart in the reference): runs an issue-rate
- * probe of the DPX add-max instruction the recurrences use and reports the
- * device's integer operation rate, counting the add and the max as two
- * operations.  Used as the roofline denominator by bench.py. */
-int pw_measure_int_peak(pw_engine* e, double* ops_per_second, double* ms);
+/* Measurement helper (no counterpart in the reference): runs issue-rate
+ * probes of the DPX add-max instructions the recurrences use and reports the
+ * device's integer operation rates, counting each add and each max as one
+ * operation: ops32 for __viaddmax_s32 (32-bit lanes), ops16x2 for
+ * __viaddmax_s16x2 (two 16-bit lanes per instruction).  Used as the roofline
+ * denominators by bench.py. */
+int pw_measure_int_peak(pw_engine* e, double* ops32, double* ops16x2, double* ms);
 
 /* Pair maxima without any device allocation.  No counterpart in the
  * reference: it serves callers that cannot call cudaMalloc themselves or have

@@ -24,6 +24,7 @@ PW_ERR_STATE = -6
 
 PW_FLAG_SCORE_ONLY = 1
 PW_FLAG_PLAIN = 2
+PW_FLAG_INT32 = 4
 
 # symbols the header declares, checked by the CPU test-suite
 EXPORTED_SYMBOLS = (
@@ -57,7 +58,8 @@ class PwRunInfo(ctypes.Structure):
                 ("kernel_launches", ctypes.c_int32), ("truncated", ctypes.c_int32), ("score_ms", ctypes.c_double),
                 ("trace_ms", ctypes.c_double), ("walk_ms", ctypes.c_double),
                 ("score_kernel_ms", ctypes.c_double), ("trace_kernel_ms", ctypes.c_double),
-                ("score_launches", ctypes.c_int32), ("trace_launches", ctypes.c_int32)]
+                ("score_launches", ctypes.c_int32), ("trace_launches", ctypes.c_int32),
+                ("orientation", ctypes.c_int32), ("overflow_pairs", ctypes.c_int64)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -80,7 +82,7 @@ def bind(lib):
         "pw_get_hits": (ctypes.c_int, [P, P, I64, P, I64]),
         "pw_get_starting_points": (ctypes.c_int, [P, P, I64, ctypes.POINTER(I64)]),
         "pw_last_launch_count": (ctypes.c_int, [P, ctypes.POINTER(I64)]),
-        "pw_measure_int_peak": (ctypes.c_int, [P, ctypes.POINTER(D), ctypes.POINTER(D)]),
+        "pw_measure_int_peak": (ctypes.c_int, [P, ctypes.POINTER(D), ctypes.POINTER(D), ctypes.POINTER(D)]),
         "pw_score_max_noalloc": (ctypes.c_int, [ctypes.c_int, P, ctypes.c_int, ctypes.c_int, F, F, ctypes.c_int,
                                                 P, P, I32, P, P, I32, P, ctypes.c_char_p, I32]),
     }
@@ -183,9 +185,10 @@ class Engine(object):
                self.lib.pw_set_targets(self.handle, _ptr(buf), _ptr(off), len(seqs), _ptr(keys)), "pw_set_targets")
         self.n_targets = len(seqs)
 
-    def align(self, score_only=False, plain=False, start_cap=-1):
+    def align(self, score_only=False, plain=False, start_cap=-1, int32=False):
         info = PwRunInfo()
-        flags = (PW_FLAG_SCORE_ONLY if score_only else 0) | (PW_FLAG_PLAIN if plain else 0)
+        flags = (PW_FLAG_SCORE_ONLY if score_only else 0) | (PW_FLAG_PLAIN if plain else 0) | \
+            (PW_FLAG_INT32 if int32 else 0)
         rc = self.lib.pw_align(self.handle, flags, int(start_cap), ctypes.byref(info))
         _check(self.lib, self.handle, rc, "pw_align")
         self.last_info = info
@@ -217,11 +220,12 @@ class Engine(object):
         return out
 
     def measure_int_peak(self):
-        """(integer ops per second, probe duration in ms) of the DPX add-max probe."""
-        r, ms = ctypes.c_double(), ctypes.c_double()
-        _check(self.lib, self.handle, self.lib.pw_measure_int_peak(self.handle, ctypes.byref(r), ctypes.byref(ms)),
+        """(ops/s on 32-bit lanes, ops/s on 16x2 lanes, probe ms) of the DPX add-max probes."""
+        r32, r16, ms = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        _check(self.lib, self.handle,
+               self.lib.pw_measure_int_peak(self.handle, ctypes.byref(r32), ctypes.byref(r16), ctypes.byref(ms)),
                "pw_measure_int_peak")
-        return r.value, ms.value
+        return r32.value, r16.value, ms.value
 
     def launch_count(self):
         n = ctypes.c_int64()

@@ -20,6 +20,7 @@
 
 #include "../../include/paswas_b200.h"
 #include "pw_kernels.cuh"
+#include "pw_score16.cuh"
 
 using namespace pw;
 
@@ -62,9 +63,13 @@ struct HostSeqs {
 };
 
 struct Prepared {
-    int alpha = 0;
+    int alpha = 0;               // distinct query residues
+    int alpha_t = 0;             // distinct target residues
     bool int_path = true;
+    bool s16_q = false;          // 16-bit sweep possible with queries on the lanes
+    bool s16_t = false;          // ... with targets on the lanes
     std::vector<int32_t> order;  // query indices by length, longest first
+    std::vector<int32_t> order_t;  // target indices by length, longest first
     std::vector<int32_t> qlen, tlen;
 };
 
@@ -94,6 +99,7 @@ struct pw_engine {
     // device buffers
     DevBuf q_codes, q_code_off, q_raw, q_raw_off, q_len, q_key, q_order;
     DevBuf t_codes, t_code_off, t_raw, t_raw_off, t_len, t_key;
+    DevBuf q_res, t_ccodes, t_order, cmat_t8;  // the other orientation's encodings
     DevBuf cmat_i8, cmat_f, pair_max, items, items_alt, counter, bnd_pool, q_order2;
     DevBuf codes, metas, cands, cands_alt, cand_base, cand_cap, n_cand, n_starts, start_off, starts, hits,
         hit_count, ops, allowed;
@@ -388,6 +394,41 @@ static int prepare(pw_engine* e) {
     std::iota(pr.order.begin(), pr.order.end(), 0);
     std::stable_sort(pr.order.begin(), pr.order.end(),
                      [&](int a, int b) { return pr.qlen[a] > pr.qlen[b]; });
+    pr.order_t.resize(T.n);
+    std::iota(pr.order_t.begin(), pr.order_t.end(), 0);
+    std::stable_sort(pr.order_t.begin(), pr.order_t.end(),
+                     [&](int a, int b) { return pr.tlen[a] > pr.tlen[b]; });
+
+    // the transposed orientation: queries as strips (residue indices), targets
+    // on the lanes (compact target alphabet)
+    int tmap[256];
+    for (int i = 0; i < 256; ++i) tmap[i] = -1;
+    std::vector<int> talpha;
+    for (uint8_t c : T.raw)
+        if (tmap[c] < 0) {
+            tmap[c] = (int)talpha.size();
+            talpha.push_back(c);
+        }
+    pr.alpha_t = (int)talpha.size();
+    std::vector<uint8_t> qres(qc.size(), 0);
+    for (int32_t i = 0; i < Q.n; ++i)
+        for (int32_t k = 0; k < pr.qlen[i]; ++k) qres[qco[i] + k] = (uint8_t)(Q.raw[Q.off[i] + k] - off);
+    std::vector<uint8_t> tcc(tc.size(), (uint8_t)pr.alpha_t);
+    for (int32_t i = 0; i < T.n; ++i)
+        for (int32_t k = 0; k < pr.tlen[i]; ++k) tcc[tco[i] + k] = (uint8_t)tmap[T.raw[T.off[i] + k]];
+    std::vector<int8_t> cmt8((size_t)(pr.alpha_t + 1) * dim, (int8_t)-128);
+    bool t_int8 = pr.alpha_t <= 250;
+    for (int b = 0; b < pr.alpha_t; ++b)
+        for (int j = 0; j < dim; ++j) {
+            const float v = e->matrix[(size_t)j * dim + (talpha[b] - off)];
+            if (std::floor(v) != v || v < -127.0f || v > 127.0f) t_int8 = false;
+            cmt8[(size_t)b * dim + j] = (int8_t)(t_int8 ? v : 0);
+        }
+    // 16-bit halves hold every cell while the maximum stays below 32640; gap
+    // chains must stay well inside the negative half-range
+    const bool gaps16 = std::fabs(e->gap) + std::fabs(e->ext) < 8192.0f;
+    pr.s16_q = ints && gaps16;
+    pr.s16_t = ints && gaps16 && t_int8;
 
     cudaError_t c;
 #define UP(buf, vec)                                      \
@@ -407,6 +448,10 @@ static int prepare(pw_engine* e) {
     UP(e->t_key, T.key);
     UP(e->cmat_i8, cm8);
     UP(e->cmat_f, cmf);
+    UP(e->q_res, qres);
+    UP(e->t_ccodes, tcc);
+    UP(e->t_order, pr.order_t);
+    UP(e->cmat_t8, cmt8);
 #undef UP
     if ((c = e->counter.reserve(64 * sizeof(int))) != cudaSuccess) return cuda_fail(e, c, "alloc counter");
     if ((c = cudaStreamSynchronize(e->stream)) != cudaSuccess) return cuda_fail(e, c, "upload");
@@ -512,6 +557,192 @@ static void order_by_class(std::vector<WorkItem>& items, std::vector<int>& cls, 
     for (int c = 0; c < kNumClasses; ++c) begin[c + 1] += begin[c];
 }
 
+
+// ------------------------------------------------------------ 16-bit phase 1
+template <int S, bool AFF, bool MULTI>
+static cudaError_t launch_s16(pw_engine* e, Score16Args A) {
+    auto kern = score16_kernel<S, AFF, MULTI>;
+    const int prof_bytes = ((S / 4) * A.alpha1 * 4 + 15) & ~15;
+    const int smem = 4 * prof_bytes;
+    if (smem > 48 * 1024) {
+        cudaError_t c = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (c != cudaSuccess) return c;
+    }
+    int per_sm = 0;
+    cudaError_t c = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem);
+    if (c != cudaSuccess) return c;
+    per_sm = std::max(1, std::min(per_sm, 16));
+    int grid = std::min(e->sm_count * per_sm, (A.n_items + 3) / 4);
+    PW_LAUNCH(kern, std::max(grid, 1), 128, smem, e->stream, A);
+    e->launches++;
+    return cudaGetLastError();
+}
+
+static cudaError_t launch_s16_class(pw_engine* e, int cls, bool affine, const Score16Args& A) {
+    if (affine) {
+        if (cls == kS16) return launch_s16<16, true, false>(e, A);
+        if (cls == kS32) return launch_s16<32, true, false>(e, A);
+        return launch_s16<32, true, true>(e, A);
+    }
+    if (cls == kS16) return launch_s16<16, false, false>(e, A);
+    if (cls == kS32) return launch_s16<32, false, false>(e, A);
+    if (cls == kS64) return launch_s16<64, false, false>(e, A);
+    return launch_s16<32, false, true>(e, A);
+}
+
+// Lane-slot cost of an orientation: every work item pays its strip length
+// times its longest lane sequence for all 64 lane slots.
+static double orientation_cost(const std::vector<int32_t>& strip_len, const std::vector<int32_t>& lane_len,
+                               const std::vector<int32_t>& lane_order) {
+    double cost = 0;
+    double lane_groups = 0;
+    for (size_t g = 0; g < lane_order.size(); g += 2 * kWarp) lane_groups += lane_len[lane_order[g]];
+    for (int32_t ls : strip_len) cost += (double)ls * lane_groups * 2 * kWarp;
+    return cost;
+}
+
+// Pair maxima with the 16-bit dual-pair sweep.  Returns the device time of
+// the sweep launches in *kernel_ms.  Pairs whose maximum could overflow
+// 16-bit halves come back as NaN; they are recomputed by the 32-bit sweep.
+static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf) {
+    const Prepared& pr = e->pr;
+    const int nq = e->Q.n, nt = e->T.n;
+    bool trans = false;
+    if (pr.s16_q && pr.s16_t)
+        trans = orientation_cost(pr.qlen, pr.tlen, pr.order_t) < orientation_cost(pr.tlen, pr.qlen, pr.order);
+    else
+        trans = pr.s16_t;
+    inf.orientation = trans ? 1 : 0;
+    const std::vector<int32_t>& strip_len = trans ? pr.qlen : pr.tlen;
+    const std::vector<int32_t>& lane_len = trans ? pr.tlen : pr.qlen;
+    const std::vector<int32_t>& lane_order = trans ? pr.order_t : pr.order;
+    const int n_strip = trans ? nq : nt, n_lane = trans ? nt : nq;
+    std::vector<WorkItem> items;
+    std::vector<int> cls;
+    for (int st = 0; st < n_strip; ++st)
+        for (int g = 0; g < n_lane; g += 2 * kWarp) {
+            WorkItem w;
+            memset(&w, 0, sizeof(w));
+            w.target = st;
+            w.first = g;
+            w.lanes = std::min(2 * kWarp, n_lane - g);
+            w.xmax = lane_len[lane_order[g]];
+            const int k = pick_class(strip_len[st], e->affine);
+            w.S = class_S(k);
+            items.push_back(w);
+            cls.push_back(k);
+        }
+    std::vector<size_t> idx(items.size());
+    std::iota(idx.begin(), idx.end(), 0);
+    std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) {
+        return (int64_t)items[a].xmax * strip_len[items[a].target] > (int64_t)items[b].xmax * strip_len[items[b].target];
+    });
+    std::vector<WorkItem> it2;
+    std::vector<int> c2;
+    for (size_t k : idx) {
+        it2.push_back(items[k]);
+        c2.push_back(cls[k]);
+    }
+    int begin[kNumClasses + 1];
+    order_by_class(it2, c2, begin);
+    cudaError_t c;
+    if ((c = upload(e, e->items, it2)) != cudaSuccess) return cuda_fail(e, c, "upload items");
+    Score16Args S;
+    memset(&S, 0, sizeof(S));
+    S.lane_codes = trans ? e->t_ccodes.as<uint8_t>() : e->q_codes.as<uint8_t>();
+    S.lane_off = trans ? e->t_code_off.as<int64_t>() : e->q_code_off.as<int64_t>();
+    S.lane_len = trans ? e->t_len.as<int32_t>() : e->q_len.as<int32_t>();
+    S.lane_order = trans ? e->t_order.as<int32_t>() : e->q_order.as<int32_t>();
+    S.strip_res = trans ? e->q_res.as<uint8_t>() : e->t_codes.as<uint8_t>();
+    S.strip_off = trans ? e->q_code_off.as<int64_t>() : e->t_code_off.as<int64_t>();
+    S.strip_len = trans ? e->q_len.as<int32_t>() : e->t_len.as<int32_t>();
+    S.cmat = trans ? e->cmat_t8.as<int8_t>() : e->cmat_i8.as<int8_t>();
+    S.alpha1 = (trans ? pr.alpha_t : pr.alpha) + 1;
+    S.dim = e->dim;
+    S.gap = (int)e->gap;
+    S.ext = (int)e->ext;
+    S.ge = S.gap + S.ext;
+    S.pair_max = A32.pair_max;
+    S.stride_strip = trans ? nt : 1;
+    S.stride_lane = trans ? 1 : nt;
+    if (begin[kS32Multi + 1] > begin[kS32Multi]) {
+        int xm = 4;
+        for (int k = begin[kS32Multi]; k < begin[kS32Multi + 1]; ++k) xm = std::max(xm, (int)align_up(it2[k].xmax, 4));
+        const int64_t slot = (int64_t)xm * kWarp;
+        if ((c = e->bnd_pool.reserve((size_t)slot * e->sm_count * 16 * 4 * sizeof(uint4))) != cudaSuccess)
+            return cuda_fail(e, c, "alloc boundary pool");
+        S.bnd_pool = e->bnd_pool.as<uint4>();
+        S.bnd_slot = slot;
+    }
+    if ((c = cudaMemsetAsync(e->counter.p, 0, kNumClasses * sizeof(int), e->stream)) != cudaSuccess)
+        return cuda_fail(e, c, "reset counters");
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, e->stream);
+    for (int k = 0; k < kNumClasses; ++k) {
+        const int n = begin[k + 1] - begin[k];
+        if (n <= 0) continue;
+        S.items = e->items.as<WorkItem>() + begin[k];
+        S.n_items = n;
+        S.counter = e->counter.as<int>() + k;
+        if ((c = launch_s16_class(e, k, e->affine, S)) != cudaSuccess) return cuda_fail(e, c, "score16 launch");
+        inf.score_launches++;
+    }
+    cudaEventRecord(b, e->stream);
+    if ((c = download(e, e->h_pair_max, A32.pair_max, (size_t)nq * nt)) != cudaSuccess)
+        return cuda_fail(e, c, "copy pair maxima");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    inf.score_kernel_ms += ms;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+
+    // pairs that reached the 16-bit limit: the 32-bit sweep, per target
+    std::vector<std::vector<int32_t>> ovf(nt);
+    int64_t n_ovf = 0;
+    for (int sp = 0; sp < nq; ++sp) {
+        const int q = pr.order[sp];
+        for (int t = 0; t < nt; ++t)
+            if (std::isnan(e->h_pair_max[(size_t)q * nt + t])) {
+                ovf[t].push_back(q);
+                ++n_ovf;
+            }
+    }
+    inf.overflow_pairs = n_ovf;
+    if (n_ovf == 0) return PW_OK;
+    std::vector<int32_t> order2;
+    std::vector<WorkItem> its;
+    std::vector<int> cl;
+    for (int t = 0; t < nt; ++t)
+        for (size_t g = 0; g < ovf[t].size(); g += kWarp) {
+            WorkItem w;
+            memset(&w, 0, sizeof(w));
+            w.target = t;
+            w.first = (int32_t)order2.size();
+            w.lanes = (int32_t)std::min<size_t>(kWarp, ovf[t].size() - g);
+            for (int l = 0; l < w.lanes; ++l) order2.push_back(ovf[t][g + l]);
+            w.xmax = pr.qlen[order2[w.first]];
+            const int k = pick_class(pr.tlen[t], e->affine);
+            w.S = class_S(k);
+            its.push_back(w);
+            cl.push_back(k);
+        }
+    int bg[kNumClasses + 1];
+    order_by_class(its, cl, bg);
+    int xm = 4;
+    for (int k = bg[kS32Multi]; k < bg[kS32Multi + 1]; ++k) xm = std::max(xm, (int)align_up(its[k].xmax, 4));
+    if ((c = upload(e, e->q_order2, order2)) != cudaSuccess) return cuda_fail(e, c, "upload order");
+    if ((c = upload(e, e->items, its)) != cudaSuccess) return cuda_fail(e, c, "upload items");
+    KernelArgs A = A32;
+    A.q_order = e->q_order2.as<int32_t>();
+    int rc = run_phase<1>(e, A, e->items.as<WorkItem>(), bg, xm, &inf.score_kernel_ms, &inf.score_launches);
+    if (rc != PW_OK) return rc;
+    if ((c = download(e, e->h_pair_max, A32.pair_max, (size_t)nq * nt)) != cudaSuccess)
+        return cuda_fail(e, c, "copy pair maxima");
+    return PW_OK;
+}
+
 static int emit_key_less(const StartRec& a, const StartRec& b) {
     auto k = [](const StartRec& r) {
         return std::make_tuple(-(int64_t)((r.x >> 3) + (r.y >> 3)), -(int64_t)(r.x >> 3), r.target, r.query,
@@ -555,8 +786,18 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     const bool plain = (flags & PW_FLAG_PLAIN) != 0;
 
     // ---------------------------------------------------------- phase 1
+    const bool use_s16 = !plain && (pr.s16_q || pr.s16_t) && !(flags & PW_FLAG_INT32);
+    if (use_s16) {
+        cudaEventRecord(e->ev[0], e->stream);
+        rc = phase1_s16(e, A, inf);
+        if (rc != PW_OK) return rc;
+        cudaEventRecord(e->ev[1], e->stream);
+        cudaStreamSynchronize(e->stream);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e->ev[0], e->ev[1]);
+        inf.score_ms = ms;
+    } else {
     // items: one target against 32 consecutive queries of the length order
-    {
         std::vector<WorkItem> items;
         std::vector<int> cls;
         for (int t = 0; t < nt; ++t)
@@ -1008,22 +1249,28 @@ extern "C" int pw_last_launch_count(pw_engine* e, int64_t* n) {
     return PW_OK;
 }
 
-extern "C" int pw_measure_int_peak(pw_engine* e, double* ops_per_second, double* ms_out) {
-    if (!e || !ops_per_second) return PW_ERR_ARG;
+extern "C" int pw_measure_int_peak(pw_engine* e, double* ops32, double* ops16x2, double* ms_out) {
+    if (!e || !ops32) return PW_ERR_ARG;
     cudaSetDevice(e->device);
     cudaError_t c;
     if ((c = e->counter.reserve(64 * sizeof(int))) != cudaSuccess) return cuda_fail(e, c, "alloc");
     const int threads = 256, blocks = e->sm_count * 8, iters = 4096;
-    // warm-up, then the timed launch
+    const double instr = (double)blocks * threads * iters * 16.0 * 8.0;
+    float ms = 0, ms16 = 0;
+    // warm-up, then the timed launches
     PW_LAUNCH(int_peak_kernel, blocks, threads, 0, e->stream, 64, 1, e->counter.as<int>());
     cudaEventRecord(e->ev[0], e->stream);
     PW_LAUNCH(int_peak_kernel, blocks, threads, 0, e->stream, iters, 3, e->counter.as<int>());
     cudaEventRecord(e->ev[1], e->stream);
+    PW_LAUNCH(int_peak16_kernel, blocks, threads, 0, e->stream, 64, 1, e->counter.as<int>());
+    cudaEventRecord(e->ev[2], e->stream);
+    PW_LAUNCH(int_peak16_kernel, blocks, threads, 0, e->stream, iters, 3, e->counter.as<int>());
+    cudaEventRecord(e->ev[3], e->stream);
     if ((c = cudaStreamSynchronize(e->stream)) != cudaSuccess) return cuda_fail(e, c, "int peak probe");
-    float ms = 0;
     cudaEventElapsedTime(&ms, e->ev[0], e->ev[1]);
-    const double instr = (double)blocks * threads * iters * 16.0 * 8.0;
-    *ops_per_second = ms > 0 ? 2.0 * instr / (ms * 1e-3) : 0.0;
-    if (ms_out) *ms_out = ms;
+    cudaEventElapsedTime(&ms16, e->ev[2], e->ev[3]);
+    *ops32 = ms > 0 ? 2.0 * instr / (ms * 1e-3) : 0.0;            // add + max
+    if (ops16x2) *ops16x2 = ms16 > 0 ? 4.0 * instr / (ms16 * 1e-3) : 0.0;  // two adds + two maxima
+    if (ms_out) *ms_out = ms + ms16;
     return PW_OK;
 }

@@ -797,6 +797,28 @@ __global__ void int_peak_kernel(int iters, int seed, int* sink) {
     if (r == 0x7fffffff) sink[0] = r;
 }
 
+// Same probe on the 16x2 form (one instruction = two adds and two maxima).
+__global__ void int_peak16_kernel(int iters, int seed, int* sink) {
+    unsigned a0 = threadIdx.x + seed, a1 = a0 + 1, a2 = a0 + 2, a3 = a0 + 3, a4 = a0 + 4, a5 = a0 + 5,
+             a6 = a0 + 6, a7 = a0 + 7;
+    const unsigned b = (unsigned)(seed & 7) * 0x10001u, c = 0xC000C000u;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+            a0 = __viaddmax_s16x2(a0, b, c);
+            a1 = __viaddmax_s16x2(a1, b, c);
+            a2 = __viaddmax_s16x2(a2, b, c);
+            a3 = __viaddmax_s16x2(a3, b, c);
+            a4 = __viaddmax_s16x2(a4, b, c);
+            a5 = __viaddmax_s16x2(a5, b, c);
+            a6 = __viaddmax_s16x2(a6, b, c);
+            a7 = __viaddmax_s16x2(a7, b, c);
+        }
+    }
+    const unsigned r = a0 ^ a1 ^ a2 ^ a3 ^ a4 ^ a5 ^ a6 ^ a7;
+    if (r == 0x7fffffffu) sink[0] = (int)r;
+}
+
 #endif  // PW_SCORE_SWEEP_ONLY
 
 }  // namespace pw

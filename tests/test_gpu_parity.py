@@ -86,3 +86,36 @@ def test_many_pairs_pair_max(engine_lib, oracle_mod):
         pm, hits, _, _ = run_engine(engine_lib, q, t, score, st)
         np.testing.assert_array_equal(pm, o["pair_max"])
         assert hits == o["hits"]
+
+
+def test_sixteen_bit_overflow_is_recomputed(engine_lib, oracle_mod):
+    # match score 120 over 290-400 identical residues: maxima above the 16-bit
+    # limit (32640), so these pairs must come from the 32-bit recompute
+    from pypaswas_b200 import scores
+    rng = np.random.default_rng(12)
+    base = "".join("ACGT"[i] for i in rng.integers(0, 4, 400))
+    q = [base, base[:330] + "A" * 20, "".join("ACGT"[i] for i in rng.integers(0, 4, 90))]
+    t = [base, base[40:]]
+    st = cases.Settings(match_score="120", mismatch_score="-3", minimum_score="50")
+    score = scores.make_score(st)
+    o = _oracle(oracle_mod, q, t, score, st)
+    pm, hits, info, _ = run_engine(engine_lib, q, t, score, st)
+    assert info.overflow_pairs >= 4
+    np.testing.assert_array_equal(pm, o["pair_max"])
+    assert hits == o["hits"]
+
+
+@pytest.mark.parametrize("shape", [(600, 40), (40, 600), (97, 97)])
+def test_lane_orientations_and_32_bit_sweep_agree(engine_lib, oracle_mod, shape):
+    rng = np.random.default_rng(sum(shape))
+    nq, nt = shape
+    q = ["".join(cases.PROTEIN[i] for i in rng.integers(0, 20, int(rng.integers(1, 150)))) for _ in range(nq)]
+    t = ["".join(cases.PROTEIN[i] for i in rng.integers(0, 20, int(rng.integers(1, 150)))) for _ in range(nt)]
+    from pypaswas_b200 import scores
+    for aff in ("0", "-1"):
+        st = cases.Settings(matrix_name="BLOSUM62", gap_score="-11", gap_extension=aff, minimum_score="40")
+        score = scores.make_score(st)
+        pm16 = run_engine(engine_lib, q, t, score, st, score_only=True)[0]
+        pm32 = run_engine(engine_lib, q, t, score, st, score_only=True, int32=True)[0]
+        np.testing.assert_array_equal(pm16, pm32)
+        np.testing.assert_array_equal(pm16, oracle_mod.pair_max(cases.oracle_params(oracle_mod, score), q, t))
