@@ -562,8 +562,7 @@ static void order_by_class(std::vector<WorkItem>& items, std::vector<int>& cls, 
 template <int S, bool AFF, bool MULTI>
 static cudaError_t launch_s16(pw_engine* e, Score16Args A) {
     auto kern = score16_kernel<S, AFF, MULTI>;
-    const int prof_bytes = ((S / 4) * A.alpha1 * 4 + 15) & ~15;
-    const int smem = 4 * prof_bytes;
+    const int smem = 4 * (S / 4) * A.alpha1 * (int)sizeof(uint4);
     if (smem > 48 * 1024) {
         cudaError_t c = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (c != cudaSuccess) return c;
@@ -590,15 +589,16 @@ static cudaError_t launch_s16_class(pw_engine* e, int cls, bool affine, const Sc
     return launch_s16<32, false, true>(e, A);
 }
 
-// Lane-slot cost of an orientation: every work item pays its strip length
-// times its longest lane sequence for all 64 lane slots.
-static double orientation_cost(const std::vector<int32_t>& strip_len, const std::vector<int32_t>& lane_len,
-                               const std::vector<int32_t>& lane_order) {
-    double cost = 0;
+// Cell-slot cost of an orientation: strips are paired in length order (one
+// pair per 16x2 register), lanes grouped 32 at a time in length order; every
+// work item pays its longer strip times its longest lane for all 64 slots.
+static double orientation_cost(const std::vector<int32_t>& strip_len, const std::vector<int32_t>& strip_order,
+                               const std::vector<int32_t>& lane_len, const std::vector<int32_t>& lane_order) {
     double lane_groups = 0;
-    for (size_t g = 0; g < lane_order.size(); g += 2 * kWarp) lane_groups += lane_len[lane_order[g]];
-    for (int32_t ls : strip_len) cost += (double)ls * lane_groups * 2 * kWarp;
-    return cost;
+    for (size_t g = 0; g < lane_order.size(); g += kWarp) lane_groups += lane_len[lane_order[g]];
+    double strips = 0;
+    for (size_t i = 0; i < strip_order.size(); i += 2) strips += strip_len[strip_order[i]];
+    return strips * lane_groups * 2 * kWarp;
 }
 
 // Pair maxima with the 16-bit dual-pair sweep.  Returns the device time of
@@ -609,34 +609,40 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf) {
     const int nq = e->Q.n, nt = e->T.n;
     bool trans = false;
     if (pr.s16_q && pr.s16_t)
-        trans = orientation_cost(pr.qlen, pr.tlen, pr.order_t) < orientation_cost(pr.tlen, pr.qlen, pr.order);
+        trans = orientation_cost(pr.qlen, pr.order, pr.tlen, pr.order_t) <
+                orientation_cost(pr.tlen, pr.order_t, pr.qlen, pr.order);
     else
         trans = pr.s16_t;
     inf.orientation = trans ? 1 : 0;
     const std::vector<int32_t>& strip_len = trans ? pr.qlen : pr.tlen;
+    const std::vector<int32_t>& strip_order = trans ? pr.order : pr.order_t;
     const std::vector<int32_t>& lane_len = trans ? pr.tlen : pr.qlen;
     const std::vector<int32_t>& lane_order = trans ? pr.order_t : pr.order;
     const int n_strip = trans ? nq : nt, n_lane = trans ? nt : nq;
     std::vector<WorkItem> items;
     std::vector<int> cls;
-    for (int st = 0; st < n_strip; ++st)
-        for (int g = 0; g < n_lane; g += 2 * kWarp) {
+    std::vector<int64_t> cost;
+    for (int i = 0; i < n_strip; i += 2) {
+        const int sa = strip_order[i], sb = i + 1 < n_strip ? strip_order[i + 1] : -1;
+        const int ls = std::max(strip_len[sa], sb >= 0 ? strip_len[sb] : 0);
+        for (int g = 0; g < n_lane; g += kWarp) {
             WorkItem w;
             memset(&w, 0, sizeof(w));
-            w.target = st;
+            w.target = sa;
+            w.index = sb;
             w.first = g;
-            w.lanes = std::min(2 * kWarp, n_lane - g);
+            w.lanes = std::min(kWarp, n_lane - g);
             w.xmax = lane_len[lane_order[g]];
-            const int k = pick_class(strip_len[st], e->affine);
+            const int k = pick_class(ls, e->affine);
             w.S = class_S(k);
             items.push_back(w);
             cls.push_back(k);
+            cost.push_back((int64_t)w.xmax * ls);
         }
+    }
     std::vector<size_t> idx(items.size());
     std::iota(idx.begin(), idx.end(), 0);
-    std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) {
-        return (int64_t)items[a].xmax * strip_len[items[a].target] > (int64_t)items[b].xmax * strip_len[items[b].target];
-    });
+    std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return cost[a] > cost[b]; });
     std::vector<WorkItem> it2;
     std::vector<int> c2;
     for (size_t k : idx) {

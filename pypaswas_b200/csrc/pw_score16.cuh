@@ -4,11 +4,13 @@
 // the same DP cell of two different pairs as signed 16-bit halves, and the
 // recurrences run on the DPX 16x2 instructions (__viaddmax_s16x2 and friends),
 // which update two cells per instruction at the rate of one 32-bit update.
-// A warp aligns one "strip" sequence against up to 64 "lane" sequences: lane l
-// carries lane sequences l and l + 32 of its work item (similar lengths, the
-// lane list is sorted by length).  Which input set provides the strips and
-// which the lanes is chosen per run by the host (pair maxima are symmetric in
-// the two sequences, so either orientation gives the same maxima).
+// A warp aligns two "strip" sequences (low and high halves) against up to 32
+// "lane" sequences, one per lane.  Both halves of a lane read the same lane
+// residue, so the strip profile stores ready-made 16x2 score pairs: one
+// 128-bit shared-memory load yields the scores of four strip rows for both
+// strip sequences.  Which input set provides the strips and which the lanes
+// is chosen per run by the host (pair maxima are symmetric in the two
+// sequences, so either orientation gives the same maxima).
 //
 // Overflow: with every score in [-127, 127], no 16-bit operation can exceed
 // 32767 while all cell values stay below kOvf16 (32640 = 32767 - 127).  A pair
@@ -22,37 +24,13 @@ namespace pw {
 constexpr int kOvf16 = 32767 - 127;
 constexpr uint32_t kNeg16x2 = 0xC000C000u;  // -16384 in both halves (boundary of the gap chains)
 
-__device__ __forceinline__ uint32_t prmt_sign(uint32_t a, uint32_t b, uint32_t sel) {
-#ifdef __CUDA_ARCH__
-    uint32_t d;
-    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(sel));
-    return d;
-#else
-    // PTX prmt, default mode: selector nibble n picks byte (n & 7) of {b, a};
-    // with bit 3 set it replicates that byte's sign bit instead.
-    const uint64_t v = ((uint64_t)b << 32) | a;
-    uint32_t r = 0;
-    for (int i = 0; i < 4; ++i) {
-        const uint32_t n = (sel >> (4 * i)) & 0xf;
-        uint32_t byte = (uint32_t)(v >> (8 * (n & 7))) & 0xff;
-        if (n & 8) byte = (byte & 0x80) ? 0xff : 0;
-        r |= byte << (8 * i);
-    }
-    return r;
-#endif
-}
-
-// Scores of strip row k for the two pairs, as signed 16-bit halves: low half
-// from pair A's profile word wa, high half from pair B's word wb.
-__device__ __forceinline__ uint32_t pair_scores(uint32_t wa, uint32_t wb, int k) {
-    const uint32_t sel = (uint32_t)k | ((8u | k) << 4) | ((4u + k) << 8) | ((12u + k) << 12);
-    return prmt_sign(wa, wb, sel);
-}
-
 __device__ __forceinline__ uint32_t pack16(int v) { return ((uint32_t)v & 0xffffu) * 0x00010001u; }
+__device__ __forceinline__ uint32_t pack16x2(int lo, int hi) {
+    return ((uint32_t)lo & 0xffffu) | ((uint32_t)hi << 16);
+}
 
 struct Score16Args {
-    const WorkItem* items;   // target = strip sequence, first/lanes index the lane order
+    const WorkItem* items;   // target = strip A, index = strip B (or -1), first/lanes index the lane order
     int n_items;
     int* counter;
     const uint8_t* lane_codes;   // compact lane-alphabet codes, 16-aligned, pad-coded tail
@@ -71,36 +49,64 @@ struct Score16Args {
     int64_t bnd_slot;            // uint4 elements per warp slot (xmax4 * 32)
 };
 
+// Profile of strip rows [y0, y0 + S): for row group g (4 rows) and lane
+// residue a, one uint4 holds the 16x2 scores of the 4 rows, strip A in the low
+// halves and strip B in the high halves.  Rows past a strip's end get -128.
+// Affine sweeps store score + gap_open in the halves (see sweep16).
+template <int S>
+__device__ __forceinline__ void build_profile16(uint4* prof, const int8_t* cmat, const uint8_t* ra,
+                                                const uint8_t* rb, int y0, int la, int lb, int alpha1, int dim,
+                                                int shift, int lane) {
+    const int n = (S / 4) * alpha1;
+    for (int idx = lane; idx < n; idx += kWarp) {
+        const int g = idx / alpha1, a = idx % alpha1;
+        uint32_t w[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int y = y0 + 4 * g + k;
+            const int sa = y < la ? (int)cmat[a * dim + ra[y]] : -128;
+            const int sb = y < lb ? (int)cmat[a * dim + rb[y]] : -128;
+            w[k] = pack16x2(sa + shift, sb + shift);
+        }
+        prof[idx] = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+}
+
+// One lane, two pairs (strip A / strip B against the lane sequence).
+//   linear: H = max(diag + s, left + gap, up + gap, 0)                 3 DPX / row
+//   affine: carries Mg = M + gap_open (gap_open = gap + ext):
+//     M  = max(Bdiag + s, 0)          Mg = M + ge  (profile holds s + ge,
+//     so Mg = max(Bdiag + (s + ge), ge) in one instruction)
+//     Y  = max(Yup + ext, Mg_up)      strip-axis gap chain
+//     X  = max(Xleft + ext, Mg_left)  sweep-axis gap chain
+//     B  = max(Mg - ge, Y, X)          as max(M, Y, X)                 5 DPX / row
 template <int S, bool AFFINE>
-__device__ __forceinline__ void sweep16(const uint8_t* qa, const uint8_t* qb, int lq4a, int lq4b, uint32_t pad4,
-                                        const uint32_t* prof, int alpha1, int gap, int ext, int ge, bool has_up,
-                                        bool has_down, uint4* bnd, uint32_t& mx) {
-    const int lq4 = lq4a > lq4b ? lq4a : lq4b;
-    const uint32_t g2 = pack16(gap), e2 = pack16(ext), ge2 = pack16(ge);
+__device__ __forceinline__ void sweep16(const uint8_t* qc, int lq4, const uint4* prof, int alpha1, int gap, int ext,
+                                        int ge, bool has_up, bool has_down, uint4* bnd, uint32_t& mx) {
+    const uint32_t g2 = pack16(gap), e2 = pack16(ext), ge2 = pack16(ge), nge2 = pack16(-ge);
     if constexpr (!AFFINE) {
         uint32_t H[S];
 #pragma unroll
         for (int r = 0; r < S; ++r) H[r] = 0;
         uint32_t hb_prev = 0;
         for (int x4 = 0; x4 < lq4; x4 += 4) {
-            const uint32_t cwa = x4 < lq4a ? *(const uint32_t*)(qa + x4) : pad4;
-            const uint32_t cwb = x4 < lq4b ? *(const uint32_t*)(qb + x4) : pad4;
+            const uint32_t cw = *(const uint32_t*)(qc + x4);
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const int x = x4 + j;
-                const int a = (cwa >> (8 * j)) & 0xff, b = (cwb >> (8 * j)) & 0xff;
+                const int a = (cw >> (8 * j)) & 0xff;
                 uint32_t up = has_up ? bnd[(int64_t)x * kWarp].x : 0u;
                 uint32_t diag = hb_prev;
                 hb_prev = up;
 #pragma unroll
                 for (int g = 0; g < S / 4; ++g) {
-                    const uint32_t wa = prof[g * alpha1 + a], wb = prof[g * alpha1 + b];
+                    const uint4 w4 = prof[g * alpha1 + a];
+                    const uint32_t sc[4] = {w4.x, w4.y, w4.z, w4.w};
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
                         const int r = 4 * g + k;
-                        const uint32_t s = pair_scores(wa, wb, k);
                         const uint32_t left = H[r];
-                        uint32_t t = __viaddmax_s16x2(diag, s, kNeg16x2);       // diag + s
+                        uint32_t t = __viaddmax_s16x2(diag, sc[k], kNeg16x2);   // diag + s
                         t = __viaddmax_s16x2(left, g2, t);                      // max(left + gap, .)
                         const uint32_t h = __viaddmax_s16x2_relu(up, g2, t);    // max(up + gap, ., 0)
                         diag = left;
@@ -114,27 +120,24 @@ __device__ __forceinline__ void sweep16(const uint8_t* qa, const uint8_t* qb, in
             }
         }
     } else {
-        // strip-axis gap chain carried down the column (scalar), sweep-axis gap
-        // chain and best score kept per row (arrays); see sweep_score
-        uint32_t Ml[S], Xl[S], Bl[S];
+        uint32_t Mgl[S], Xl[S], Bl[S];
 #pragma unroll
         for (int r = 0; r < S; ++r) {
-            Ml[r] = 0;
+            Mgl[r] = ge2;     // M = 0 left of the matrix
             Xl[r] = kNeg16x2;
             Bl[r] = 0;
         }
         uint32_t bb_prev = 0;
         for (int x4 = 0; x4 < lq4; x4 += 4) {
-            const uint32_t cwa = x4 < lq4a ? *(const uint32_t*)(qa + x4) : pad4;
-            const uint32_t cwb = x4 < lq4b ? *(const uint32_t*)(qb + x4) : pad4;
+            const uint32_t cw = *(const uint32_t*)(qc + x4);
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const int x = x4 + j;
-                const int a = (cwa >> (8 * j)) & 0xff, b = (cwb >> (8 * j)) & 0xff;
-                uint32_t mup = 0, yup = kNeg16x2, bup = 0;
+                const int a = (cw >> (8 * j)) & 0xff;
+                uint32_t mgup = ge2, yup = kNeg16x2, bup = 0;
                 if (has_up) {
                     const uint4 v = bnd[(int64_t)x * kWarp];
-                    mup = v.x;
+                    mgup = v.x;
                     yup = v.y;
                     bup = v.z;
                 }
@@ -142,26 +145,26 @@ __device__ __forceinline__ void sweep16(const uint8_t* qa, const uint8_t* qb, in
                 bb_prev = bup;
 #pragma unroll
                 for (int g = 0; g < S / 4; ++g) {
-                    const uint32_t wa = prof[g * alpha1 + a], wb = prof[g * alpha1 + b];
+                    const uint4 w4 = prof[g * alpha1 + a];
+                    const uint32_t sc[4] = {w4.x, w4.y, w4.z, w4.w};
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
                         const int r = 4 * g + k;
-                        const uint32_t s = pair_scores(wa, wb, k);
-                        const uint32_t m = __viaddmax_s16x2_relu(bdiag, s, kNeg16x2);
-                        const uint32_t y = __viaddmax_s16x2(yup, e2, __viaddmax_s16x2(mup, ge2, kNeg16x2));
-                        const uint32_t xg = __viaddmax_s16x2(Xl[r], e2, __viaddmax_s16x2(Ml[r], ge2, kNeg16x2));
-                        const uint32_t bst = __vimax3_s16x2(m, y, xg);
+                        const uint32_t mg = __viaddmax_s16x2(bdiag, sc[k], ge2);   // M + ge
+                        const uint32_t y = __viaddmax_s16x2(yup, e2, mgup);
+                        const uint32_t xg = __viaddmax_s16x2(Xl[r], e2, Mgl[r]);
+                        const uint32_t bst = __vimax3_s16x2(__viaddmax_s16x2(mg, nge2, kNeg16x2), y, xg);
                         bdiag = Bl[r];
-                        Ml[r] = m;
+                        Mgl[r] = mg;
                         Xl[r] = xg;
                         Bl[r] = bst;
-                        mup = m;
+                        mgup = mg;
                         yup = y;
                     }
                 }
 #pragma unroll
                 for (int r = 0; r < S; r += 2) mx = __vimax3_s16x2(mx, Bl[r], Bl[r + 1]);
-                if (has_down) bnd[(int64_t)x * kWarp] = make_uint4(mup, yup, Bl[S - 1], 0u);
+                if (has_down) bnd[(int64_t)x * kWarp] = make_uint4(mgup, yup, Bl[S - 1], 0u);
             }
         }
     }
@@ -172,46 +175,44 @@ __global__ void __launch_bounds__(128) score16_kernel(Score16Args A) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    const int prof_bytes = ((S / 4) * A.alpha1 * 4 + 15) & ~15;
-    uint32_t* prof = (uint32_t*)(smem + wib * prof_bytes);
+    uint4* prof = (uint4*)smem + wib * ((S / 4) * A.alpha1);
     const int64_t warp_global = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
     uint4* bnd = MULTI ? A.bnd_pool + warp_global * A.bnd_slot + lane : nullptr;
-    const uint32_t pad = (uint32_t)(A.alpha1 - 1);
-    const uint32_t pad4 = pad * 0x01010101u;
+    const int shift = AFFINE ? A.ge : 0;
     for (;;) {
         int it = 0;
         if (lane == 0) it = atomicAdd(A.counter, 1);
         it = __shfl_sync(0xffffffffu, it, 0);
         if (it >= A.n_items) break;
         const WorkItem W = A.items[it];
-        const int st = W.target;
-        const int ls = A.strip_len[st];
-        const bool has_a = lane < W.lanes, has_b = lane + kWarp < W.lanes;
-        const int pa = has_a ? A.lane_order[W.first + lane] : 0;
-        const int pb = has_b ? A.lane_order[W.first + lane + kWarp] : 0;
-        const uint8_t* qa = A.lane_codes + A.lane_off[pa];
-        const uint8_t* qb = A.lane_codes + A.lane_off[pb];
-        const int lq4a = has_a ? (A.lane_len[pa] + 3) & ~3 : 0;
-        const int lq4b = has_b ? (A.lane_len[pb] + 3) & ~3 : 0;
-        const uint8_t* sres = A.strip_res + A.strip_off[st];
+        const int sa = W.target, sb = W.index;
+        const int la = A.strip_len[sa];
+        const int lb = sb >= 0 ? A.strip_len[sb] : 0;
+        const bool active = lane < W.lanes;
+        const int p = active ? A.lane_order[W.first + lane] : 0;
+        const uint8_t* qc = A.lane_codes + A.lane_off[p];
+        const int lq4 = active ? (A.lane_len[p] + 3) & ~3 : 0;
+        const uint8_t* ra = A.strip_res + A.strip_off[sa];
+        const uint8_t* rb = A.strip_res + A.strip_off[sb >= 0 ? sb : sa];
+        const int ls = la > lb ? la : lb;
         const int nstrips = MULTI ? (ls + S - 1) / S : 1;
         uint32_t mx = 0;
         for (int s = 0; s < nstrips; ++s) {
             const int y0 = s * S;
             __syncwarp();
-            build_profile<int, S>(prof, A.cmat, nullptr, sres, y0, ls, A.alpha1, A.dim, lane);
+            build_profile16<S>(prof, A.cmat, ra, rb, y0, la, lb, A.alpha1, A.dim, shift, lane);
             __syncwarp();
-            if (has_a)
-                sweep16<S, AFFINE>(qa, qb, lq4a, lq4b, pad4, prof, A.alpha1, A.gap, A.ext, A.ge, s > 0,
-                                   s + 1 < nstrips, bnd, mx);
+            if (active)
+                sweep16<S, AFFINE>(qc, lq4, prof, A.alpha1, A.gap, A.ext, A.ge, s > 0, s + 1 < nstrips, bnd, mx);
         }
-        const int ma = (int)(int16_t)(mx & 0xffffu), mb = (int)(int16_t)(mx >> 16);
-        if (has_a)
-            A.pair_max[(int64_t)st * A.stride_strip + (int64_t)pa * A.stride_lane] =
+        if (active) {
+            const int ma = (int)(int16_t)(mx & 0xffffu), mb = (int)(int16_t)(mx >> 16);
+            A.pair_max[(int64_t)sa * A.stride_strip + (int64_t)p * A.stride_lane] =
                 ma >= kOvf16 ? __int_as_float(0x7fc00000) : (float)ma;
-        if (has_b)
-            A.pair_max[(int64_t)st * A.stride_strip + (int64_t)pb * A.stride_lane] =
-                mb >= kOvf16 ? __int_as_float(0x7fc00000) : (float)mb;
+            if (sb >= 0)
+                A.pair_max[(int64_t)sb * A.stride_strip + (int64_t)p * A.stride_lane] =
+                    mb >= kOvf16 ? __int_as_float(0x7fc00000) : (float)mb;
+        }
     }
 }
 
