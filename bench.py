@@ -262,15 +262,14 @@ def main():
     if trace_ms >= score_ms:
         dom, dom_ms, dom_launch = "direction sweep (sweep_kernel phase 2)", trace_ms, sum(
             i["trace_launches"] for i in infos)
-        traced_cells = _traced_cells(e, w)
-        ops = traced_cells * OPS_PER_CELL[(mode, "dirs")] * args.steps
+        ops = sum(i["traced_cells"] for i in infos) * OPS_PER_CELL[(mode, "dirs")]
     else:
-        dom, dom_ms, dom_launch = "score sweep (sweep_kernel phase 1)", score_ms, sum(
+        dom, dom_ms, dom_launch = "score sweep (score16_kernel, 16x2 lanes)" if _sixteen_bit(e, w) else \
+            "score sweep (sweep_kernel phase 1)", score_ms, sum(
             i["score_launches"] for i in infos)
         ops = cells * OPS_PER_CELL[(mode, "score")] * args.steps
     peak32, peak16, _ = e.measure_int_peak()
-    lanes16 = "score" in dom and last.get("overflow_pairs", 0) == 0 and not last.get("int32", False) and \
-        _sixteen_bit(e, w)
+    lanes16 = "score" in dom and _sixteen_bit(e, w)
     peak_ops = peak16 if lanes16 else peak32
     achieved = ops / (dom_ms * 1e-3) / 1e12
     traffic = load_traffic().get("direction_sweep_bytes_per_launch" if "direction" in dom else
@@ -285,6 +284,8 @@ def main():
            "config": {"workload": w.name + " (400,000 pairs, full path)", "pairs": len(w.queries) * len(w.targets),
                       "cells_per_step": cells, "traced_pairs": last["traced_pairs"],
                       "starting_points": last["starting_points"], "hits": last["hits"],
+                      "score_lanes": "targets" if last["orientation"] else "queries",
+                      "trace_lanes": "targets" if last["trace_orientation"] else "queries",
                       "minimum_score": w.settings.minimum_score, "lower_limit_score": w.settings.lower_limit_score,
                       "filter_factor": w.settings.filter_factor,
                       "l2": "flushed between steps (256 MiB write); each step also writes >1e11 B of cell codes",
@@ -322,15 +323,6 @@ def _integer_scores(w):
     from pypaswas_b200 import scores
     m = scores.make_score(w.settings).matrix_array()
     return bool(np.all(np.floor(m) == m) and np.all(np.abs(m) <= 127))
-
-
-def _traced_cells(engine, w):
-    pm = engine.pair_max()
-    thr = float(np.float32(float(w.settings.minimum_score)))
-    ql = np.array([len(s) for _, s in w.queries], dtype=np.int64)
-    tl = np.array([len(s) for _, s in w.targets], dtype=np.int64)
-    mask = pm >= thr
-    return int((mask * np.outer(ql, tl)).sum())
 
 
 def _e2e(w, steps, device):

@@ -69,7 +69,9 @@ typedef struct {
     double trace_kernel_ms; /* summed duration of the direction-sweep launches */
     int32_t score_launches, trace_launches;
     int32_t orientation;    /* score sweep lanes: 0 = queries, 1 = targets */
+    int32_t trace_orientation; /* direction sweep lanes: 0 = queries, 1 = targets */
     int64_t overflow_pairs; /* pairs recomputed on 32-bit lanes after reaching the 16-bit limit */
+    int64_t traced_cells;   /* sum of len(q) * len(t) over the traced pairs */
 } pw_run_info;
 
 /* Creates an engine on CUDA device `device`.

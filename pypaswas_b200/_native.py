@@ -59,7 +59,8 @@ class PwRunInfo(ctypes.Structure):
                 ("trace_ms", ctypes.c_double), ("walk_ms", ctypes.c_double),
                 ("score_kernel_ms", ctypes.c_double), ("trace_kernel_ms", ctypes.c_double),
                 ("score_launches", ctypes.c_int32), ("trace_launches", ctypes.c_int32),
-                ("orientation", ctypes.c_int32), ("overflow_pairs", ctypes.c_int64)]
+                ("orientation", ctypes.c_int32), ("trace_orientation", ctypes.c_int32),
+                ("overflow_pairs", ctypes.c_int64), ("traced_cells", ctypes.c_int64)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

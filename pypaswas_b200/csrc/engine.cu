@@ -99,7 +99,7 @@ struct pw_engine {
     // device buffers
     DevBuf q_codes, q_code_off, q_raw, q_raw_off, q_len, q_key, q_order;
     DevBuf t_codes, t_code_off, t_raw, t_raw_off, t_len, t_key;
-    DevBuf q_res, t_ccodes, t_order, cmat_t8;  // the other orientation's encodings
+    DevBuf q_res, t_ccodes, t_order, cmat_t8, cmat_tf;  // the other orientation's encodings
     DevBuf cmat_i8, cmat_f, pair_max, items, items_alt, counter, bnd_pool, q_order2;
     DevBuf codes, metas, cands, cands_alt, cand_base, cand_cap, n_cand, n_starts, start_off, starts, hits,
         hit_count, ops, allowed;
@@ -248,9 +248,9 @@ int pick_class(int lt, bool affine) {
 
 int64_t align_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
 
-template <typename T, int S, bool AFF, bool MULTI, int PH>
+template <typename T, int S, bool AFF, bool MULTI, int PH, bool TR>
 cudaError_t launch_sweep(pw_engine* e, KernelArgs A, int* counter) {
-    auto kern = sweep_kernel<T, S, AFF, MULTI, PH>;
+    auto kern = sweep_kernel<T, S, AFF, MULTI, PH, TR>;
     const int alpha1 = A.P.alpha + 1;
     const int prof_bytes = ((S / 4) * alpha1 * (std::is_integral<T>::value ? 4 : 16) + 15) & ~15;
     const int smem = 4 * prof_bytes;
@@ -273,21 +273,28 @@ cudaError_t launch_sweep(pw_engine* e, KernelArgs A, int* counter) {
     return cudaGetLastError();
 }
 
-template <typename T, int PH>
-cudaError_t launch_class(pw_engine* e, int cls, bool affine, const KernelArgs& A, int* counter) {
+template <typename T, int PH, bool TR>
+cudaError_t launch_class_o(pw_engine* e, int cls, bool affine, const KernelArgs& A, int* counter) {
     if (affine) {
         switch (cls) {
-            case kS16: return launch_sweep<T, 16, true, false, PH>(e, A, counter);
-            case kS32: return launch_sweep<T, 32, true, false, PH>(e, A, counter);
-            default: return launch_sweep<T, 32, true, true, PH>(e, A, counter);
+            case kS16: return launch_sweep<T, 16, true, false, PH, TR>(e, A, counter);
+            case kS32: return launch_sweep<T, 32, true, false, PH, TR>(e, A, counter);
+            default: return launch_sweep<T, 32, true, true, PH, TR>(e, A, counter);
         }
     }
     switch (cls) {
-        case kS16: return launch_sweep<T, 16, false, false, PH>(e, A, counter);
-        case kS32: return launch_sweep<T, 32, false, false, PH>(e, A, counter);
-        case kS64: return launch_sweep<T, 64, false, false, PH>(e, A, counter);
-        default: return launch_sweep<T, 32, false, true, PH>(e, A, counter);
+        case kS16: return launch_sweep<T, 16, false, false, PH, TR>(e, A, counter);
+        case kS32: return launch_sweep<T, 32, false, false, PH, TR>(e, A, counter);
+        case kS64: return launch_sweep<T, 64, false, false, PH, TR>(e, A, counter);
+        default: return launch_sweep<T, 32, false, true, PH, TR>(e, A, counter);
     }
+}
+
+// Phase 1 never needs the transposed form (maxima are orientation-free).
+template <typename T, int PH>
+cudaError_t launch_class(pw_engine* e, int cls, bool affine, const KernelArgs& A, int* counter, bool trans) {
+    if (PH == 2 && trans) return launch_class_o<T, PH, true>(e, cls, affine, A, counter);
+    return launch_class_o<T, PH, false>(e, cls, affine, A, counter);
 }
 
 }  // namespace
@@ -417,12 +424,14 @@ static int prepare(pw_engine* e) {
     for (int32_t i = 0; i < T.n; ++i)
         for (int32_t k = 0; k < pr.tlen[i]; ++k) tcc[tco[i] + k] = (uint8_t)tmap[T.raw[T.off[i] + k]];
     std::vector<int8_t> cmt8((size_t)(pr.alpha_t + 1) * dim, (int8_t)-128);
+    std::vector<float> cmtf((size_t)(pr.alpha_t + 1) * dim, -1.0e30f);
     bool t_int8 = pr.alpha_t <= 250;
     for (int b = 0; b < pr.alpha_t; ++b)
         for (int j = 0; j < dim; ++j) {
             const float v = e->matrix[(size_t)j * dim + (talpha[b] - off)];
             if (std::floor(v) != v || v < -127.0f || v > 127.0f) t_int8 = false;
             cmt8[(size_t)b * dim + j] = (int8_t)(t_int8 ? v : 0);
+            cmtf[(size_t)b * dim + j] = v;
         }
     // 16-bit halves hold every cell while the maximum stays below 32640; gap
     // chains must stay well inside the negative half-range
@@ -452,6 +461,7 @@ static int prepare(pw_engine* e) {
     UP(e->t_ccodes, tcc);
     UP(e->t_order, pr.order_t);
     UP(e->cmat_t8, cmt8);
+    UP(e->cmat_tf, cmtf);
 #undef UP
     if ((c = e->counter.reserve(64 * sizeof(int))) != cudaSuccess) return cuda_fail(e, c, "alloc counter");
     if ((c = cudaStreamSynchronize(e->stream)) != cudaSuccess) return cuda_fail(e, c, "upload");
@@ -487,6 +497,8 @@ static KernelArgs base_args(pw_engine* e) {
     A.cmat_i8 = e->cmat_i8.as<int8_t>();
     A.cmat_f = e->cmat_f.as<float>();
     A.nt = e->T.n;
+    A.pm_lane = e->T.n;
+    A.pm_strip = 1;
     A.pair_max = e->pair_max.as<float>();
     return A;
 }
@@ -497,7 +509,7 @@ static KernelArgs base_args(pw_engine* e) {
 // Kernel time per launch is accumulated into *kernel_ms after the phase.
 template <int PH>
 static int run_phase(pw_engine* e, KernelArgs A, const WorkItem* dev_items, const int (&cls_begin)[kNumClasses + 1],
-                     int xmax_multi4, double* kernel_ms, int* n_launch) {
+                     int xmax_multi4, double* kernel_ms, int* n_launch, bool trans = false) {
     cudaError_t c;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> evs;
     if (cls_begin[kS32Multi + 1] > cls_begin[kS32Multi]) {
@@ -521,8 +533,8 @@ static int run_phase(pw_engine* e, KernelArgs A, const WorkItem* dev_items, cons
         cudaEventCreate(&a);
         cudaEventCreate(&b);
         cudaEventRecord(a, e->stream);
-        c = e->pr.int_path ? launch_class<int, PH>(e, cls, e->affine, A, e->counter.as<int>() + cls)
-                           : launch_class<float, PH>(e, cls, e->affine, A, e->counter.as<int>() + cls);
+        c = e->pr.int_path ? launch_class<int, PH>(e, cls, e->affine, A, e->counter.as<int>() + cls, trans)
+                           : launch_class<float, PH>(e, cls, e->affine, A, e->counter.as<int>() + cls, trans);
         cudaEventRecord(b, e->stream);
         evs.push_back({a, b});
         if (c != cudaSuccess) return cuda_fail(e, c, "sweep kernel launch");
@@ -870,15 +882,12 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     // cell with H >= max(LOWER_LIMIT_SCORE * max, maxPossibleScore) (:609) and
     // no cell exceeds the pair maximum, so a pair whose maximum is below that
     // threshold has no starting point and contributes nothing: it is skipped.
-    std::vector<int32_t> p2_order;
-    std::vector<WorkItem> items2;
-    std::vector<int> cls2;
-    std::vector<int64_t> bytes2;
-    int64_t min_pass = 0;
-    for (int t = 0; t < nt; ++t) {
-        std::vector<int32_t> pass;
-        for (int sp = 0; sp < nq; ++sp) {
-            const int q = pr.order[sp];
+    std::vector<std::vector<int32_t>> pass_t(nt);   // per target: passing queries, length order
+    std::vector<std::vector<int32_t>> pass_q(nq);   // per query: passing targets, length order
+    int64_t min_pass = 0, n_pass = 0;
+    for (int sp = 0; sp < nq; ++sp) {
+        const int q = pr.order[sp];
+        for (int t = 0; t < nt; ++t) {
             const float mx = e->h_pair_max[(size_t)q * nt + t];
             if (!(mx >= e->minimum_score)) continue;
             ++min_pass;
@@ -886,27 +895,59 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
             const float pos = (float)(e->highest * (double)mn * e->filter_factor);
             const volatile float llm = e->lower_limit * mx;  // fp32 product, as the kernel computes it
             const float thr = std::max((float)llm, pos);
-            if (mx >= thr) pass.push_back(q);
+            if (mx >= thr) {
+                pass_t[t].push_back(q);
+                ++n_pass;
+                inf.traced_cells += (int64_t)qlen[q] * tlen[t];
+            }
         }
-        const int per_item = plain ? 1 : kWarp;
+    }
+    // orientation of the direction sweep: lanes over the side where traced
+    // pairs cluster (slot cost = strip length x longest lane x 32 per item)
+    const int per_item = plain ? 1 : kWarp;
+    double cost_t = 0, cost_q = 0;
+    for (int t = 0; t < nt; ++t)
+        for (size_t g = 0; g < pass_t[t].size(); g += per_item) cost_t += (double)tlen[t] * qlen[pass_t[t][g]] * per_item;
+    {
+        std::vector<int32_t> rank_t(nt);
+        for (int k = 0; k < nt; ++k) rank_t[pr.order_t[k]] = k;
+        for (int t = 0; t < nt; ++t)
+            for (int32_t q : pass_t[t]) pass_q[q].push_back(t);
+        for (int q = 0; q < nq; ++q)
+            std::stable_sort(pass_q[q].begin(), pass_q[q].end(), [&](int a, int b) { return rank_t[a] < rank_t[b]; });
+        for (int q = 0; q < nq; ++q)
+            for (size_t g = 0; g < pass_q[q].size(); g += per_item)
+                cost_q += (double)qlen[q] * tlen[pass_q[q][g]] * per_item;
+    }
+    const bool trans2 = cost_q < cost_t;
+    std::vector<int32_t> p2_order;
+    std::vector<WorkItem> items2;
+    std::vector<int> cls2;
+    std::vector<int64_t> bytes2;
+    const int n_strip = trans2 ? nq : nt;
+    for (int st = 0; st < n_strip; ++st) {
+        const std::vector<int32_t>& pass = trans2 ? pass_q[st] : pass_t[st];
+        const int ls = trans2 ? qlen[st] : tlen[st];
         for (size_t g = 0; g < pass.size(); g += per_item) {
             WorkItem w;
             memset(&w, 0, sizeof(w));
-            w.target = t;
+            w.target = st;
             w.first = (int32_t)p2_order.size();
             w.lanes = (int32_t)std::min<size_t>(per_item, pass.size() - g);
             for (int l = 0; l < w.lanes; ++l) p2_order.push_back(pass[g + l]);
-            w.xmax = qlen[p2_order[w.first]];
-            const int k = pick_class(tlen[t], e->affine);
+            w.xmax = trans2 ? tlen[p2_order[w.first]] : qlen[p2_order[w.first]];
+            w.orient = trans2 ? 1 : 0;
+            const int k = pick_class(ls, e->affine);
             w.S = class_S(k);
             items2.push_back(w);
             cls2.push_back(k);
-            const int64_t strips = std::max<int64_t>((tlen[t] + w.S - 1) / w.S, 1);
+            const int64_t strips = std::max<int64_t>((ls + w.S - 1) / w.S, 1);
             bytes2.push_back(strips * w.S * align_up(std::max(w.xmax, 1), 4) * kWarp);
         }
     }
-    inf.traced_pairs = (int64_t)p2_order.size();
+    inf.traced_pairs = n_pass;
     inf.minimum_pairs = min_pass;
+    inf.trace_orientation = trans2 ? 1 : 0;
     if (p2_order.empty()) {
         inf.kernel_launches = (int32_t)e->launches;
         if (info) *info = inf;
@@ -914,6 +955,19 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     }
     if ((c = upload(e, e->q_order2, p2_order)) != cudaSuccess) return cuda_fail(e, c, "upload phase-2 order");
     A.q_order = e->q_order2.as<int32_t>();
+    if (trans2) {
+        // lanes sweep targets (compact target codes), strips are queries
+        A.q = SeqSet{e->t_ccodes.as<uint8_t>(), e->t_code_off.as<int64_t>(), e->t_raw.as<uint8_t>(),
+                     e->t_raw_off.as<int64_t>(), e->t_len.as<int32_t>(), e->t_key.as<int32_t>()};
+        A.t = SeqSet{e->q_res.as<uint8_t>(), e->q_code_off.as<int64_t>(), e->q_raw.as<uint8_t>(),
+                     e->q_raw_off.as<int64_t>(), e->q_len.as<int32_t>(), e->q_key.as<int32_t>()};
+        A.cmat_i8 = e->cmat_t8.as<int8_t>();
+        A.cmat_f = e->cmat_tf.as<float>();
+        A.P.alpha = pr.alpha_t;
+        A.pm_lane = 1;
+        A.pm_strip = nt;
+    }
+    const KernelArgs Aref = base_args(e);  // reference-oriented sets for the trace kernels
 
     // memory waves: the cell codes of one wave must fit the budget
     size_t free_b = 0, total_b = 0;
@@ -974,7 +1028,8 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         A.cand_cap = e->cand_cap.as<int32_t>();
         A.n_cand = e->n_cand.as<int32_t>();
         cudaEventRecord(e->ev[0], e->stream);
-        rc = run_phase<2>(e, A, e->items.as<WorkItem>(), begin, xm, &inf.trace_kernel_ms, &inf.trace_launches);
+        rc = run_phase<2>(e, A, e->items.as<WorkItem>(), begin, xm, &inf.trace_kernel_ms, &inf.trace_launches,
+                          trans2);
         if (rc != PW_OK) return rc;
         // candidate overflow: pairs with more candidates than their slot get an
         // exact slot past the regular ones, and their items are swept again
@@ -1014,7 +1069,8 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
             int rb[kNumClasses + 1];
             order_by_class(ri, rcl, rb);
             if ((c = upload(e, e->items_alt, ri)) != cudaSuccess) return cuda_fail(e, c, "upload items");
-            rc = run_phase<2>(e, A, e->items_alt.as<WorkItem>(), rb, xm, &inf.trace_kernel_ms, &inf.trace_launches);
+            rc = run_phase<2>(e, A, e->items_alt.as<WorkItem>(), rb, xm, &inf.trace_kernel_ms, &inf.trace_launches,
+                              trans2);
             if (rc != PW_OK) return rc;
         }
 
@@ -1029,9 +1085,9 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         TA.cands = A.cands;
         TA.cand_base = A.cand_base;
         TA.n_starts = e->n_starts.as<int32_t>();
-        TA.q = A.q;
-        TA.t = A.t;
-        TA.P = A.P;
+        TA.q = Aref.q;
+        TA.t = Aref.t;
+        TA.P = Aref.P;
         const int tb = 128;
         const int gb = (int)((n_pairs + tb - 1) / tb);
         if (e->affine)

@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(128) noalloc_score_kernel(KernelArgs A) {
             __syncwarp();
             if (active) sweep_score<T, S, AFFINE>(c, prof, alpha1, gap, ext, ge, bnd_slot, mx);
         }
-        if (active) A.pair_max[(int64_t)q * A.nt + t] = (float)mx;
+        if (active) A.pair_max[(int64_t)q * A.pm_lane + (int64_t)t * A.pm_strip] = (float)mx;
     }
 }
 
@@ -351,6 +351,8 @@ extern "C" int pw_score_max_noalloc(int device, const float* matrix, int dim, in
     A.cmat_f = (const float*)(dev_base + o_cmf);
     A.pair_max = (float*)(dev_base + o_pm);
     A.nt = nt;
+    A.pm_lane = nt;
+    A.pm_strip = 1;
     A.bnd_pool = dev_base + o_bnd;
     A.bnd_slot_elems = (int64_t)xmax4 * kWarp;
     for (int cls = 0; cls < 4; ++cls) {

@@ -207,7 +207,11 @@ __device__ __forceinline__ void sweep_score(const LaneCtx& c, const void* prof, 
 //   affine (:467-526): best B = max(M, I, J); source MAIN if B == M, else I if
 //     B == I, else J; NO when B == 0.  Stop flag: MAIN with M(x-1, y-1) == 0
 //     inside the matrix (:724-751).  Candidate: MAIN and M >= threshold (:850).
-template <typename T, int S, bool AFFINE>
+// TRANS: the strip sequence is the query (the reference's x axis) and the
+// lanes sweep targets (its y axis), so the reference's LEFT neighbour is the
+// previous strip row and its UP neighbour the previous column; likewise the
+// affine I matrix (gaps along y) is the per-row chain and J the column chain.
+template <typename T, int S, bool AFFINE, bool TRANS = false>
 __device__ __forceinline__ void sweep_dirs(const LaneCtx& c, const void* prof, int alpha1, T gap, T ext, T ge,
                                            Bnd<T>* bnd, uint8_t* codes, int lane, int xmax4, T thr, Cand* cand,
                                            int cand_cap, int& n_cand) {
@@ -239,7 +243,8 @@ __device__ __forceinline__ void sweep_dirs(const LaneCtx& c, const void* prof, i
                         const T ls = left + gap, us = up + gap, ds = diag + p.s[k];
                         T h = addmax(left, gap, ds);
                         h = relu_addmax(up, gap, h);
-                        uint32_t code = h == ls ? kLeft : (h == us ? kUp : kUL);
+                        uint32_t code = TRANS ? (h == us ? kLeft : (h == ls ? kUp : kUL))
+                                              : (h == ls ? kLeft : (h == us ? kUp : kUL));
                         code = h > T(0) ? code : kNo;
                         const bool ul = code == kUL;
                         const bool yin = (r > 0) || c.has_up;
@@ -252,8 +257,8 @@ __device__ __forceinline__ void sweep_dirs(const LaneCtx& c, const void* prof, i
                                 code |= kCand;
                                 if (n_cand < cand_cap) {
                                     Cand cc;
-                                    cc.x = x;
-                                    cc.y = y;
+                                    cc.x = TRANS ? y : x;
+                                    cc.y = TRANS ? x : y;
                                     cc.score_i = (int32_t)h;
                                     cc.score_f = (float)h;
                                     cand[n_cand] = cc;
@@ -314,7 +319,7 @@ __device__ __forceinline__ void sweep_dirs(const LaneCtx& c, const void* prof, i
                         const T i = addmax(iup, ext, mup + ge);
                         const T jj = addmax(Jl[r], ext, Ml[r] + ge);
                         const T b = max3(m, i, jj);
-                        uint32_t code = b == m ? kUL : (b == i ? kUp : kLeft);
+                        uint32_t code = b == m ? kUL : (b == (TRANS ? jj : i) ? kUp : kLeft);
                         code = b > T(0) ? code : kNo;
                         const bool main_src = code == kUL;
                         const bool yin = (r > 0) || c.has_up;
@@ -327,8 +332,8 @@ __device__ __forceinline__ void sweep_dirs(const LaneCtx& c, const void* prof, i
                                 code |= kCand;
                                 if (n_cand < cand_cap) {
                                     Cand cc;
-                                    cc.x = x;
-                                    cc.y = y;
+                                    cc.x = TRANS ? y : x;
+                                    cc.y = TRANS ? x : y;
                                     cc.score_i = (int32_t)m;
                                     cc.score_f = (float)m;
                                     cand[n_cand] = cc;
@@ -386,6 +391,7 @@ struct KernelArgs {
     ScoreParams P;
     float* pair_max;         // [nq * nt]
     int nt;
+    int64_t pm_lane, pm_strip;  // pair_max index = lane * pm_lane + strip * pm_strip
     void* bnd_pool;
     int64_t bnd_slot_elems;  // elements per warp slot (xmax4 * 32)
     // phase 2
@@ -407,7 +413,7 @@ __device__ __forceinline__ T from_f(float v) {
 
 // Persistent kernel over work items: one warp per item, dynamic scheduling.
 // PHASE 1 writes pair maxima; PHASE 2 writes cell codes and candidates.
-template <typename T, int S, bool AFFINE, bool MULTI, int PHASE>
+template <typename T, int S, bool AFFINE, bool MULTI, int PHASE, bool TRANS = false>
 __global__ void __launch_bounds__(128) sweep_kernel(KernelArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
@@ -446,7 +452,7 @@ __global__ void __launch_bounds__(128) sweep_kernel(KernelArgs A) {
         int cap = 0;
         int64_t pslot = W.pair_base + lane;
         if (PHASE == 2 && active) {
-            const float maxf = A.pair_max[(int64_t)q * A.nt + t];
+            const float maxf = A.pair_max[(int64_t)q * A.pm_lane + (int64_t)t * A.pm_strip];
             const int mn = c.lq < lt ? c.lq : lt;
             // maxPossibleScore, SmithWatermanCuda.py:269-275 (double, stored as fp32)
             const float pos = (float)(A.P.highest * (double)mn * A.P.filter_factor);
@@ -462,8 +468,8 @@ __global__ void __launch_bounds__(128) sweep_kernel(KernelArgs A) {
             cand = A.cands + A.cand_base[pslot];
             cap = A.cand_cap[pslot];
             PairMeta& pm = A.metas[pslot];
-            pm.query = q;
-            pm.target = t;
+            pm.query = TRANS ? t : q;
+            pm.target = TRANS ? q : t;
             pm.item = W.index;
             pm.lane = lane;
             pm.thr_f = thf;
@@ -483,14 +489,14 @@ __global__ void __launch_bounds__(128) sweep_kernel(KernelArgs A) {
                     sweep_score<T, S, AFFINE>(c, prof, alpha1, gap, ext, ge, bnd_slot, mx);
                 } else {
                     uint8_t* codes = A.codes + W.dir_base + (int64_t)s * xmax4 * S * kWarp;
-                    sweep_dirs<T, S, AFFINE>(c, prof, alpha1, gap, ext, ge, bnd_slot, codes, lane, xmax4, thr,
-                                             cand, cap, n_cand);
+                    sweep_dirs<T, S, AFFINE, TRANS>(c, prof, alpha1, gap, ext, ge, bnd_slot, codes, lane, xmax4,
+                                                    thr, cand, cap, n_cand);
                 }
             }
         }
         if (active) {
             if (PHASE == 1)
-                A.pair_max[(int64_t)q * A.nt + t] = (float)mx;
+                A.pair_max[(int64_t)q * A.pm_lane + (int64_t)t * A.pm_strip] = (float)mx;
             else {
                 A.metas[pslot].n_cand = n_cand;
                 A.n_cand[pslot] = n_cand;
@@ -521,8 +527,10 @@ struct TraceArgs {
 struct PairView {
     uint8_t* base;
     int S, lane, xmax4, lq, lt;
+    bool trans;
+    // cell (x, y) in the reference's coordinates (x: query, y: target)
     __device__ __forceinline__ uint8_t& at(int x, int y) const {
-        return base[cell_offset_rt(S, x, y, lane, xmax4)];
+        return base[trans ? cell_offset_rt(S, y, x, lane, xmax4) : cell_offset_rt(S, x, y, lane, xmax4)];
     }
 };
 
@@ -535,6 +543,7 @@ __device__ __forceinline__ PairView pair_view(const TraceArgs& A, const PairMeta
     v.xmax4 = (W.xmax + 3) & ~3;
     v.lq = A.q.len[pm.query];
     v.lt = A.t.len[pm.target];
+    v.trans = W.orient != 0;
     return v;
 }
 
