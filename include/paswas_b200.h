@@ -72,6 +72,8 @@ typedef struct {
     int32_t trace_orientation; /* direction sweep lanes: 0 = queries, 1 = targets */
     int64_t overflow_pairs; /* pairs recomputed on 32-bit lanes after reaching the 16-bit limit */
     int64_t traced_cells;   /* sum of len(q) * len(t) over the traced pairs */
+    int64_t warp_pairs;     /* traced pairs swept one pair per warp (long targets) */
+    int64_t cand_overflow_pairs; /* traced pairs swept twice: more candidates than the first slot held */
 } pw_run_info;
 
 /* Creates an engine on CUDA device `device`.

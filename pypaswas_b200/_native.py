@@ -60,7 +60,8 @@ class PwRunInfo(ctypes.Structure):
                 ("score_kernel_ms", ctypes.c_double), ("trace_kernel_ms", ctypes.c_double),
                 ("score_launches", ctypes.c_int32), ("trace_launches", ctypes.c_int32),
                 ("orientation", ctypes.c_int32), ("trace_orientation", ctypes.c_int32),
-                ("overflow_pairs", ctypes.c_int64), ("traced_cells", ctypes.c_int64)]
+                ("overflow_pairs", ctypes.c_int64), ("traced_cells", ctypes.c_int64),
+                ("warp_pairs", ctypes.c_int64), ("cand_overflow_pairs", ctypes.c_int64)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

@@ -21,6 +21,7 @@
 #include "../../include/paswas_b200.h"
 #include "pw_kernels.cuh"
 #include "pw_score16.cuh"
+#include "pw_trace_warp.cuh"
 
 using namespace pw;
 
@@ -100,7 +101,7 @@ struct pw_engine {
     DevBuf q_codes, q_code_off, q_raw, q_raw_off, q_len, q_key, q_order;
     DevBuf t_codes, t_code_off, t_raw, t_raw_off, t_len, t_key;
     DevBuf q_res, t_ccodes, t_order, cmat_t8, cmat_tf;  // the other orientation's encodings
-    DevBuf cmat_i8, cmat_f, pair_max, items, items_alt, counter, bnd_pool, q_order2;
+    DevBuf cmat_i8, cmat_f, pair_max, items, items_alt, items_warp, counter, bnd_pool, q_order2;
     DevBuf codes, metas, cands, cands_alt, cand_base, cand_cap, n_cand, n_starts, start_off, starts, hits,
         hit_count, ops, allowed;
     // prepared (device-resident) inputs
@@ -761,6 +762,53 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf) {
     return PW_OK;
 }
 
+
+// Direction sweep with one warp per pair (pw_trace_warp.cuh) over n items.
+static int run_warp_phase(pw_engine* e, KernelArgs A, const WorkItem* dev_items, int n, int qmax, double* kernel_ms,
+                          int* n_launch) {
+    if (n <= 0) return PW_OK;
+    const int qmax16 = (int)align_up(std::max(qmax, 1), 16);
+    const int prof_bytes = (int)align_up((int64_t)kWarp * (A.P.alpha + 1) * kWarpRows, 16);
+    const int smem = 4 * (prof_bytes + qmax16);
+    if (smem > 227 * 1024) return fail(e, PW_ERR_CAPACITY, "query too long for the warp direction sweep");
+    auto kern = e->affine ? dir_warp_kernel<true> : dir_warp_kernel<false>;
+    cudaError_t c;
+    if (smem > 48 * 1024 &&
+        (c = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
+        return cuda_fail(e, c, "warp sweep smem");
+    int per_sm = 0;
+    if ((c = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem)) != cudaSuccess)
+        return cuda_fail(e, c, "occupancy");
+    per_sm = std::max(1, std::min(per_sm, 16));
+    const int grid = std::max(1, std::min(e->sm_count * per_sm, (n + 3) / 4));
+    const int64_t slot = align_up(std::max(qmax, 1), 4);
+    if ((c = e->bnd_pool.reserve((size_t)slot * grid * 4 * sizeof(int4))) != cudaSuccess)
+        return cuda_fail(e, c, "alloc boundary pool");
+    A.bnd_pool = e->bnd_pool.p;
+    A.bnd_slot_elems = slot;
+    A.items = dev_items;
+    A.n_items = n;
+    A.item_counter = e->counter.as<int>() + kNumClasses;
+    if ((c = cudaMemsetAsync(A.item_counter, 0, sizeof(int), e->stream)) != cudaSuccess)
+        return cuda_fail(e, c, "reset counter");
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, e->stream);
+    PW_LAUNCH(kern, grid, 128, smem, e->stream, A, qmax16);
+    e->launches++;
+    cudaEventRecord(b, e->stream);
+    if ((c = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, c, "warp sweep launch");
+    if ((c = cudaStreamSynchronize(e->stream)) != cudaSuccess) return cuda_fail(e, c, "warp sweep");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    if (kernel_ms) *kernel_ms += ms;
+    if (n_launch) ++*n_launch;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return PW_OK;
+}
+
 static int emit_key_less(const StartRec& a, const StartRec& b) {
     auto k = [](const StartRec& r) {
         return std::make_tuple(-(int64_t)((r.x >> 3) + (r.y >> 3)), -(int64_t)(r.x >> 3), r.target, r.query,
@@ -902,8 +950,19 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
             }
         }
     }
-    // orientation of the direction sweep: lanes over the side where traced
-    // pairs cluster (slot cost = strip length x longest lane x 32 per item)
+    // Traced pairs with targets longer than one register strip go to the
+    // one-warp-per-pair sweep (pw_trace_warp.cuh); the others are grouped 32 to
+    // a warp, one pair per lane, in the orientation where they cluster
+    // (slot cost = strip length x longest lane x 32 per item).
+    const bool warp_ok = pr.int_path && !plain;
+    std::vector<std::pair<int32_t, int32_t>> warp_pairs;  // (query, target)
+    if (warp_ok) {
+        for (int t = 0; t < nt; ++t) {
+            if (tlen[t] <= 64) continue;
+            for (int32_t q : pass_t[t]) warp_pairs.push_back({q, t});
+            pass_t[t].clear();
+        }
+    }
     const int per_item = plain ? 1 : kWarp;
     double cost_t = 0, cost_q = 0;
     for (int t = 0; t < nt; ++t)
@@ -945,10 +1004,31 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
             bytes2.push_back(strips * w.S * align_up(std::max(w.xmax, 1), 4) * kWarp);
         }
     }
+    // warp items: longest first (dynamic scheduling tail)
+    std::stable_sort(warp_pairs.begin(), warp_pairs.end(), [&](const std::pair<int32_t, int32_t>& a,
+                                                               const std::pair<int32_t, int32_t>& b) {
+        return (int64_t)qlen[a.first] * tlen[a.second] > (int64_t)qlen[b.first] * tlen[b.second];
+    });
+    int qmax_warp = 1;
+    inf.warp_pairs = (int64_t)warp_pairs.size();
+    for (const auto& wp : warp_pairs) {
+        WorkItem w;
+        memset(&w, 0, sizeof(w));
+        w.target = wp.second;
+        w.first = wp.first;
+        w.lanes = 1;
+        w.xmax = qlen[wp.first];
+        w.orient = 2;
+        w.S = kWarpRows;
+        items2.push_back(w);
+        cls2.push_back(kNumClasses);  // marks a warp item
+        bytes2.push_back(align_up(warp_code_bytes(qlen[wp.first], tlen[wp.second]), 16));
+        qmax_warp = std::max(qmax_warp, qlen[wp.first]);
+    }
     inf.traced_pairs = n_pass;
     inf.minimum_pairs = min_pass;
     inf.trace_orientation = trans2 ? 1 : 0;
-    if (p2_order.empty()) {
+    if (items2.empty()) {
         inf.kernel_launches = (int32_t)e->launches;
         if (info) *info = inf;
         return PW_OK;
@@ -1005,6 +1085,21 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
             n_pairs += wi[k].lanes;
         }
         std::vector<WorkItem> by_index = wi;  // trace kernels index items by wave position
+        std::vector<WorkItem> ww;              // one-warp-per-pair items
+        {
+            std::vector<WorkItem> ws;
+            std::vector<int> wsc;
+            for (size_t k = 0; k < wi.size(); ++k) {
+                if (wc[k] == kNumClasses) {
+                    ww.push_back(wi[k]);
+                } else {
+                    ws.push_back(wi[k]);
+                    wsc.push_back(wc[k]);
+                }
+            }
+            wi.swap(ws);
+            wc.swap(wsc);
+        }
         int begin[kNumClasses + 1];
         order_by_class(wi, wc, begin);
         int xm = 4;
@@ -1021,15 +1116,30 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         if ((c = upload(e, e->cand_base, cbase)) != cudaSuccess) return cuda_fail(e, c, "upload cand base");
         if ((c = upload(e, e->cand_cap, ccap)) != cudaSuccess) return cuda_fail(e, c, "upload cand cap");
         if ((c = upload(e, e->items, wi)) != cudaSuccess) return cuda_fail(e, c, "upload items");
+        if (!ww.empty() && (c = upload(e, e->items_warp, ww)) != cudaSuccess) return cuda_fail(e, c, "upload items");
         A.codes = e->codes.as<uint8_t>();
         A.metas = e->metas.as<PairMeta>();
         A.cands = e->cands.as<Cand>();
         A.cand_base = e->cand_base.as<int64_t>();
         A.cand_cap = e->cand_cap.as<int32_t>();
         A.n_cand = e->n_cand.as<int32_t>();
+        KernelArgs Aw = Aref;  // the warp sweep runs in the reference orientation
+        Aw.codes = A.codes;
+        Aw.metas = A.metas;
+        Aw.cands = A.cands;
+        Aw.cand_base = A.cand_base;
+        Aw.cand_cap = A.cand_cap;
+        Aw.n_cand = A.n_cand;
         cudaEventRecord(e->ev[0], e->stream);
-        rc = run_phase<2>(e, A, e->items.as<WorkItem>(), begin, xm, &inf.trace_kernel_ms, &inf.trace_launches,
-                          trans2);
+        if ((c = cudaMemsetAsync(A.n_cand, 0, n_pairs * sizeof(int32_t), e->stream)) != cudaSuccess)
+            return cuda_fail(e, c, "reset candidate counts");
+        if (!wi.empty()) {
+            rc = run_phase<2>(e, A, e->items.as<WorkItem>(), begin, xm, &inf.trace_kernel_ms, &inf.trace_launches,
+                              trans2);
+            if (rc != PW_OK) return rc;
+        }
+        rc = run_warp_phase(e, Aw, e->items_warp.as<WorkItem>(), (int)ww.size(), qmax_warp, &inf.trace_kernel_ms,
+                            &inf.trace_launches);
         if (rc != PW_OK) return rc;
         // candidate overflow: pairs with more candidates than their slot get an
         // exact slot past the regular ones, and their items are swept again
@@ -1039,6 +1149,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         std::vector<char> redo_item(wi.size(), 0);
         for (int64_t p = 0; p < n_pairs; ++p)
             if (ncand[p] > kCandCap) {
+                inf.cand_overflow_pairs++;
                 cbase[p] = cand_total + extra;
                 ccap[p] = ncand[p];
                 extra += ncand[p];
@@ -1055,7 +1166,8 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
             if ((c = upload(e, e->cand_base, cbase)) != cudaSuccess) return cuda_fail(e, c, "upload cand base");
             if ((c = upload(e, e->cand_cap, ccap)) != cudaSuccess) return cuda_fail(e, c, "upload cand cap");
             A.cands = e->cands.as<Cand>();
-            std::vector<WorkItem> ri;
+            Aw.cands = A.cands;
+            std::vector<WorkItem> ri, rw;
             std::vector<int> rcl;
             for (size_t k = 0; k < wi.size(); ++k) {
                 bool ov = false;
@@ -1066,12 +1178,26 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
                     rcl.push_back(wc[k]);
                 }
             }
-            int rb[kNumClasses + 1];
-            order_by_class(ri, rcl, rb);
-            if ((c = upload(e, e->items_alt, ri)) != cudaSuccess) return cuda_fail(e, c, "upload items");
-            rc = run_phase<2>(e, A, e->items_alt.as<WorkItem>(), rb, xm, &inf.trace_kernel_ms, &inf.trace_launches,
-                              trans2);
-            if (rc != PW_OK) return rc;
+            for (const WorkItem& w : ww)
+                if (ncand[w.pair_base] > kCandCap) rw.push_back(w);
+            // the warp sweep counts with atomics from zero; the strip sweep
+            // overwrites its counts, and the other pairs' counts are no longer read
+            if ((c = cudaMemsetAsync(A.n_cand, 0, n_pairs * sizeof(int32_t), e->stream)) != cudaSuccess)
+                return cuda_fail(e, c, "reset candidate counts");
+            if (!ri.empty()) {
+                int rb[kNumClasses + 1];
+                order_by_class(ri, rcl, rb);
+                if ((c = upload(e, e->items_alt, ri)) != cudaSuccess) return cuda_fail(e, c, "upload items");
+                rc = run_phase<2>(e, A, e->items_alt.as<WorkItem>(), rb, xm, &inf.trace_kernel_ms,
+                                  &inf.trace_launches, trans2);
+                if (rc != PW_OK) return rc;
+            }
+            if (!rw.empty()) {
+                if ((c = upload(e, e->items_warp, rw)) != cudaSuccess) return cuda_fail(e, c, "upload items");
+                rc = run_warp_phase(e, Aw, e->items_warp.as<WorkItem>(), (int)rw.size(), qmax_warp,
+                                    &inf.trace_kernel_ms, &inf.trace_launches);
+                if (rc != PW_OK) return rc;
+            }
         }
 
         // starting points

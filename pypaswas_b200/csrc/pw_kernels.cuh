@@ -524,13 +524,22 @@ struct TraceArgs {
     char* ops;
 };
 
+// Offset of cell (x, y) in the layout of the one-warp-per-pair direction sweep
+// (pw_trace_warp.cuh): [band of 256 rows][step][lane][8 rows], step = x + lane.
+__host__ __device__ __forceinline__ int64_t warp_layout_offset(int x, int y, int lq) {
+    const int band = y >> 8, l = (y & 255) >> 3, r = y & 7;
+    const int64_t nsteps = (int64_t)lq + 31;
+    return ((band * nsteps + x + l) * 32 + l) * 8 + r;
+}
+
 struct PairView {
     uint8_t* base;
     int S, lane, xmax4, lq, lt;
-    bool trans;
+    int layout;  // 0: strip sweep, targets as strips; 1: strip sweep, queries as strips; 2: warp sweep
     // cell (x, y) in the reference's coordinates (x: query, y: target)
     __device__ __forceinline__ uint8_t& at(int x, int y) const {
-        return base[trans ? cell_offset_rt(S, y, x, lane, xmax4) : cell_offset_rt(S, x, y, lane, xmax4)];
+        if (layout == 2) return base[warp_layout_offset(x, y, lq)];
+        return base[layout == 1 ? cell_offset_rt(S, y, x, lane, xmax4) : cell_offset_rt(S, x, y, lane, xmax4)];
     }
 };
 
@@ -543,7 +552,7 @@ __device__ __forceinline__ PairView pair_view(const TraceArgs& A, const PairMeta
     v.xmax4 = (W.xmax + 3) & ~3;
     v.lq = A.q.len[pm.query];
     v.lt = A.t.len[pm.target];
-    v.trans = W.orient != 0;
+    v.layout = W.orient;
     return v;
 }
 

@@ -119,3 +119,33 @@ def test_lane_orientations_and_32_bit_sweep_agree(engine_lib, oracle_mod, shape)
         pm32 = run_engine(engine_lib, q, t, score, st, score_only=True, int32=True)[0]
         np.testing.assert_array_equal(pm16, pm32)
         np.testing.assert_array_equal(pm16, oracle_mod.pair_max(cases.oracle_params(oracle_mod, score), q, t))
+
+
+@pytest.mark.parametrize("kind", ["dna", "protein"])
+def test_long_targets_one_warp_per_pair(engine_lib, oracle_mod, kind):
+    # targets longer than 64 are swept one pair per warp in 256-row bands:
+    # lengths around the band edges, planted segments long enough that some
+    # pairs find more candidates than their first slot holds
+    from pypaswas_b200 import scores
+    rng = np.random.default_rng(31 if kind == "dna" else 32)
+    alphabet = cases.DNA if kind == "dna" else cases.PROTEIN
+    draw = lambda n: "".join(alphabet[i] for i in rng.integers(0, len(alphabet), n))
+    targets = [draw(n) for n in (65, 200, 255, 256, 257, 300, 511, 513, 700)]
+    queries = [draw(n) for n in (1, 2, 31, 32, 33, 90)]
+    for _ in range(24):
+        t = targets[int(rng.integers(0, len(targets)))]
+        cut = int(rng.integers(0, len(t) // 2))
+        s = draw(int(rng.integers(0, 60)))
+        p = int(rng.integers(0, len(s) + 1))
+        queries.append(s[:p] + cases.mutate(rng, t[cut:cut + int(rng.integers(20, 400))], alphabet, 0.05, 1) + s[p:])
+    for aff in ("0", "-1"):
+        kw = dict(minimum_score="10", lower_limit_score="0.5", filter_factor="0.1", gap_extension=aff)
+        if kind == "protein":
+            kw.update(matrix_name="BLOSUM62", gap_score="-11")
+        st = cases.Settings(**kw)
+        score = scores.make_score(st)
+        o = _oracle(oracle_mod, queries, targets, score, st)
+        pm, hits, info, _ = run_engine(engine_lib, queries, targets, score, st)
+        assert info.warp_pairs > 0 and info.cand_overflow_pairs > 0
+        np.testing.assert_array_equal(pm, o["pair_max"])
+        assert hits == o["hits"]
