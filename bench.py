@@ -44,7 +44,21 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--targets", type=int, default=0,
+                    help="use only every k-th target so that N targets remain (small cases for ncu captures; "
+                         "the bench line then names the reduced workload)")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (ncu captures)")
     return ap.parse_args()
+
+
+def workload(args):
+    from pypaswas_b200 import workloads
+    w = workloads.config2()
+    if args.targets and args.targets < len(w.targets):
+        step = len(w.targets) // args.targets
+        w = workloads.Workload("%s, sample: every %d-th target (%d targets)" % (w.name, step, args.targets),
+                               w.queries, w.targets[::step][:args.targets], w.settings)
+    return w
 
 
 def dist_env():
@@ -211,7 +225,7 @@ def main():
     args = parse()
     from pypaswas_b200 import workloads
     if args.impl == "reference":
-        return run_reference(args, workloads.config2)
+        return run_reference(args, lambda: workload(args))
     rank, world, local = dist_env()
     import torch
     if world > 1:
@@ -220,7 +234,7 @@ def main():
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     torch.cuda.set_device(local)
-    w = workloads.config2()
+    w = workload(args)
     e, score = engine_for(w, local)
     cells = w.cells
     affine = score.gap_extension is not None
@@ -276,12 +290,13 @@ def main():
                                  "score_sweep_bytes_per_launch")
 
     # end to end through the public driver, host records in, hits out
-    e2e_value, h2d, d2h = _e2e(w, args.steps, local)
+    e2e_value, h2d, d2h = (None, 0, 0) if args.no_e2e else _e2e(w, args.steps, local)
 
     out = {"metric": "GCUPS", "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-           "config": {"workload": w.name + " (400,000 pairs, full path)", "pairs": len(w.queries) * len(w.targets),
+           "config": {"workload": "%s (%d pairs, full path)" % (w.name, len(w.queries) * len(w.targets)),
+                      "pairs": len(w.queries) * len(w.targets),
                       "cells_per_step": cells, "traced_pairs": last["traced_pairs"],
                       "starting_points": last["starting_points"], "hits": last["hits"],
                       "score_lanes": "targets" if last["orientation"] else "queries",

@@ -74,6 +74,9 @@ typedef struct {
     int64_t traced_cells;   /* sum of len(q) * len(t) over the traced pairs */
     int64_t warp_pairs;     /* traced pairs swept one pair per warp (long targets) */
     int64_t cand_overflow_pairs; /* traced pairs swept twice: more candidates than the first slot held */
+    double setup_ms;        /* host wall time between the phases: pruning, work lists, memory waves */
+    double finish_ms;       /* host wall time after the device work: hit order, alignment strings */
+    double total_ms;        /* host wall time of the whole call */
 } pw_run_info;
 
 /* Creates an engine on CUDA device `device`.

@@ -61,7 +61,8 @@ class PwRunInfo(ctypes.Structure):
                 ("score_launches", ctypes.c_int32), ("trace_launches", ctypes.c_int32),
                 ("orientation", ctypes.c_int32), ("trace_orientation", ctypes.c_int32),
                 ("overflow_pairs", ctypes.c_int64), ("traced_cells", ctypes.c_int64),
-                ("warp_pairs", ctypes.c_int64), ("cand_overflow_pairs", ctypes.c_int64)]
+                ("warp_pairs", ctypes.c_int64), ("cand_overflow_pairs", ctypes.c_int64),
+                ("setup_ms", ctypes.c_double), ("finish_ms", ctypes.c_double), ("total_ms", ctypes.c_double)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -817,8 +818,13 @@ static int emit_key_less(const StartRec& a, const StartRec& b) {
     return k(a) < k(b);
 }
 
+static double wall_ms() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
 extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_info* info) {
     if (!e) return PW_ERR_ARG;
+    const double t_call = wall_ms();
     if (!e->scoring_set) return fail(e, PW_ERR_STATE, "pw_set_scoring was not called");
     if (!e->Q.set || !e->T.set) return fail(e, PW_ERR_STATE, "queries and targets must be set");
     if (cudaSetDevice(e->device) != cudaSuccess) return fail(e, PW_ERR_DEVICE, "cudaSetDevice failed");
@@ -924,6 +930,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     }
 
     // ---------------------------------------------------------- phase 2
+    const double t_setup = wall_ms();
     // Pairs that can yield a starting point, per target in query length order,
     // 32 per work item.  The reference traces every pair whose maximum reaches
     // MINIMUM_SCORE (default_main.cu:596), but a starting point also needs a
@@ -957,8 +964,15 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     const bool warp_ok = pr.int_path && !plain;
     std::vector<std::pair<int32_t, int32_t>> warp_pairs;  // (query, target)
     if (warp_ok) {
+        // short targets stay on the strip sweep only when there are enough of
+        // them to give every SM a full warp: a few strip items run one lane per
+        // pair, latency bound, far longer than the same pairs one per warp
+        int64_t n_short = 0;
+        for (int t = 0; t < nt; ++t)
+            if (tlen[t] <= 64) n_short += (int64_t)pass_t[t].size();
+        const bool all_warp = n_short < (int64_t)kWarp * e->sm_count;
         for (int t = 0; t < nt; ++t) {
-            if (tlen[t] <= 64) continue;
+            if (tlen[t] <= 64 && !all_warp) continue;
             for (int32_t q : pass_t[t]) warp_pairs.push_back({q, t});
             pass_t[t].clear();
         }
@@ -1070,6 +1084,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
 
     double trace_ms = 0, walk_ms = 0;
     int64_t total_starts = 0;
+    inf.setup_ms = wall_ms() - t_setup;
     std::vector<DevHit> all_hits;
     std::vector<char> all_ops;
     for (size_t wv = 0; wv < waves.size(); ++wv) {
@@ -1318,6 +1333,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
 
     // hits in the reference's HitList order: ascending score, then the pinned
     // emission order of their starting points (SmithWaterman.py:699)
+    const double t_finish = wall_ms();
     std::vector<int64_t> ord(all_hits.size());
     std::iota(ord.begin(), ord.end(), 0);
     auto hkey = [&](const DevHit& h) {
@@ -1386,6 +1402,8 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     inf.trace_ms = trace_ms;
     inf.walk_ms = walk_ms;
     inf.kernel_launches = (int32_t)e->launches;
+    inf.finish_ms = wall_ms() - t_finish;
+    inf.total_ms = wall_ms() - t_call;
     if (info) *info = inf;
     return PW_OK;
 }

@@ -89,13 +89,20 @@ __device__ __forceinline__ void sweep16(const uint8_t* qc, int lq4, const uint4*
 #pragma unroll
         for (int r = 0; r < S; ++r) H[r] = 0;
         uint32_t hb_prev = 0;
+        // the code word of the next 4 columns and the boundary value of the
+        // next column are loaded one step ahead (their latency hides behind a
+        // column of arithmetic)
+        uint32_t cw_next = lq4 > 0 ? *(const uint32_t*)qc : 0u;
+        uint32_t up_next = has_up && lq4 > 0 ? bnd[0].x : 0u;
         for (int x4 = 0; x4 < lq4; x4 += 4) {
-            const uint32_t cw = *(const uint32_t*)(qc + x4);
+            const uint32_t cw = cw_next;
+            if (x4 + 4 < lq4) cw_next = *(const uint32_t*)(qc + x4 + 4);
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const int x = x4 + j;
                 const int a = (cw >> (8 * j)) & 0xff;
-                uint32_t up = has_up ? bnd[(int64_t)x * kWarp].x : 0u;
+                uint32_t up = up_next;
+                if (has_up && x + 1 < lq4) up_next = bnd[(int64_t)(x + 1) * kWarp].x;
                 uint32_t diag = hb_prev;
                 hb_prev = up;
 #pragma unroll
@@ -128,19 +135,18 @@ __device__ __forceinline__ void sweep16(const uint8_t* qc, int lq4, const uint4*
             Bl[r] = 0;
         }
         uint32_t bb_prev = 0;
+        uint32_t cw_next = lq4 > 0 ? *(const uint32_t*)qc : 0u;
+        uint4 v_next = has_up && lq4 > 0 ? bnd[0] : make_uint4(ge2, kNeg16x2, 0u, 0u);
         for (int x4 = 0; x4 < lq4; x4 += 4) {
-            const uint32_t cw = *(const uint32_t*)(qc + x4);
+            const uint32_t cw = cw_next;
+            if (x4 + 4 < lq4) cw_next = *(const uint32_t*)(qc + x4 + 4);
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const int x = x4 + j;
                 const int a = (cw >> (8 * j)) & 0xff;
-                uint32_t mgup = ge2, yup = kNeg16x2, bup = 0;
-                if (has_up) {
-                    const uint4 v = bnd[(int64_t)x * kWarp];
-                    mgup = v.x;
-                    yup = v.y;
-                    bup = v.z;
-                }
+                const uint4 v = v_next;
+                if (has_up && x + 1 < lq4) v_next = bnd[(int64_t)(x + 1) * kWarp];
+                uint32_t mgup = v.x, yup = v.y, bup = v.z;
                 uint32_t bdiag = bb_prev;
                 bb_prev = bup;
 #pragma unroll

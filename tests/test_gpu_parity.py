@@ -149,3 +149,26 @@ def test_long_targets_one_warp_per_pair(engine_lib, oracle_mod, kind):
         assert info.warp_pairs > 0 and info.cand_overflow_pairs > 0
         np.testing.assert_array_equal(pm, o["pair_max"])
         assert hits == o["hits"]
+
+
+@pytest.mark.parametrize("aff", ["0", "-1"])
+def test_many_short_targets_strip_direction_sweep(engine_lib, oracle_mod, aff):
+    # enough traced pairs with short targets (<= 64) to fill every SM with a
+    # warp: these stay on the per-lane strip sweep
+    from pypaswas_b200 import scores
+    rng = np.random.default_rng(41 if aff == "0" else 42)
+    draw = lambda n: "".join("ACGT"[i] for i in rng.integers(0, 4, n))
+    targets = [draw(int(n)) for n in rng.integers(8, 65, 12)]
+    queries = []
+    for _ in range(640):
+        s = draw(int(rng.integers(10, 150)))
+        t = targets[int(rng.integers(0, len(targets)))]
+        p = int(rng.integers(0, len(s) + 1))
+        queries.append(s[:p] + cases.mutate(rng, t, "ACGT", 0.1, 1) + s[p:])
+    st = cases.Settings(minimum_score="5", lower_limit_score="0.9", filter_factor="0.0", gap_extension=aff)
+    score = scores.make_score(st)
+    o = _oracle(oracle_mod, queries, targets, score, st)
+    pm, hits, info, _ = run_engine(engine_lib, queries, targets, score, st)
+    assert info.traced_pairs >= 148 * 32 and info.warp_pairs == 0
+    np.testing.assert_array_equal(pm, o["pair_max"])
+    assert hits == o["hits"]
