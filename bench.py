@@ -39,7 +39,7 @@ OPS_PER_CELL = {("linear", "score"): 5, ("linear", "dirs"): 8, ("affine", "score
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU baseline sample")
@@ -48,6 +48,7 @@ def parse():
                     help="use only every k-th target so that N targets remain (small cases for ncu captures; "
                          "the bench line then names the reduced workload)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (ncu captures)")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain one-pair-per-launch leg")
     return ap.parse_args()
 
 
@@ -77,6 +78,7 @@ class ClockSampler(object):
         self.gpu = gpu
         self.proc = None
         self.lines = []
+        self.t0 = 0.0
 
     def start(self):
         try:
@@ -90,7 +92,11 @@ class ClockSampler(object):
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
+
+    def mark(self):
+        """Start of the timed region: later samples only."""
+        self.t0 = time.time()
 
     def stop(self):
         if self.proc is None:
@@ -102,7 +108,9 @@ class ClockSampler(object):
             self.proc.kill()
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ts, ln in self.lines:
+            if ts < self.t0:
+                continue
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -248,6 +256,8 @@ def main():
         torch.distributed.barrier()
     sampler = ClockSampler(local)
     sampler.start()
+    time.sleep(0.6)  # nvidia-smi start-up; samples before mark() are dropped
+    sampler.mark()
     times, infos = [], []
     for _ in range(args.steps):
         flush.zero_()  # between timed iterations: L2 flushed
@@ -317,6 +327,8 @@ def main():
                         "traffic": traffic,
                         "hbm_gbs_measured": load_peaks().get("hbm_gbs")},
            "e2e": {"value": e2e_value, "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}}
+    if not args.no_plain:
+        out["plain"] = plain_vs_batched(w, local, value)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(w, score, args.cpu_seconds, processes=1)
     if rank == 0:
@@ -326,6 +338,38 @@ def main():
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
     return 0
+
+
+def plain_vs_batched(w, device, batched_value, n_q=8, n_t=64):
+    """GCUPS of the plain form -- one (query, target) pair per kernel launch,
+    the shape of the reference's per-pair kernel calls -- on an evenly spaced
+    sample of the workload, next to the batched engine on the same sample.
+    Both run the full path (score, starting points, walk)."""
+    import torch
+    from pypaswas_b200 import workloads
+    qs = w.queries[::max(1, len(w.queries) // n_q)][:n_q]
+    ts = w.targets[::max(1, len(w.targets) // n_t)][:n_t]
+    sample = workloads.Workload(w.name + " sample", qs, ts, w.settings)
+    e, _ = engine_for(sample, device)
+    out = {}
+    for label, plain in (("batched", False), ("plain", True)):
+        e.align(plain=plain)  # warm-up
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        info = e.align(plain=plain)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        out[label] = {"value": sample.cells / (ms * 1e-3) / 1e9, "ms": ms, "launches": int(info.kernel_launches),
+                      "hits": int(info.hits)}
+    e.close()
+    return {"value": out["plain"]["value"], "unit": "GCUPS",
+            "sample": "%d queries x %d targets (%d pairs, %d cells), evenly spaced in length order"
+                      % (len(qs), len(ts), len(qs) * len(ts), sample.cells),
+            "launches": out["plain"]["launches"], "batched_same_sample": out["batched"]["value"],
+            "batched_over_plain": batched_value / out["plain"]["value"],
+            "hits_equal": out["plain"]["hits"] == out["batched"]["hits"]}
 
 
 def _sixteen_bit(engine, w):

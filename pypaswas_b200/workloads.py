@@ -146,6 +146,13 @@ C2_SETTINGS = dict(matrix_name="BLOSUM62", gap_score="-11", gap_extension="-1", 
                    query_identity="0", query_coverage="0")
 
 
+C3_SETTINGS = dict(matrix_name="DNA-RNA", match_score="1", mismatch_score="-3", gap_score="-5", gap_extension="0",
+                   any_score="1", minimum_score="100", lower_limit_score="1.0", filter_factor="0.01",
+                   relative_score="0", base_score="0", query_identity="0", query_coverage="0")
+C4_SETTINGS = dict(C1_SETTINGS, program="trimmer", out_format="trimmedFasta", minimum_score="8")
+C5_SETTINGS = dict(C2_SETTINGS)
+
+
 def config1(seed=1):
     q, t = dna_reads_vs_adapters(seed)
     return Workload("C1 DNA reads x adapters (+RC), linear gap", q, t, Settings(**C1_SETTINGS))
@@ -154,3 +161,103 @@ def config1(seed=1):
 def config2(seed=2, **kw):
     q, t = protein_batched(seed, **kw)
     return Workload("C2 protein 200 x 2000, BLOSUM62 affine -11/-1", q, t, Settings(**C2_SETTINGS))
+
+
+def long_dna_pairs(seed=3, n_pairs=64, length=(10000, 50000), shared=(2000, 20000), identity=0.85,
+                   indel_rate=0.02):
+    """Pairs of uniform-ACGT sequences sharing one homologous region: the region
+    is planted in the query as drawn and in the target with (1 - identity)
+    substitutions and the stated indel rate.  Returns (queries, targets, pairs)
+    where target i + n_pairs is the reverse complement of target i and each
+    query i is paired with targets i and i + n_pairs."""
+    rng = np.random.default_rng(seed)
+    queries, fwd = [], []
+    for i in range(n_pairs):
+        lq = int(rng.integers(length[0], length[1] + 1))
+        lt = int(rng.integers(length[0], length[1] + 1))
+        ls = int(rng.integers(shared[0], min(shared[1], lq, lt) + 1))
+        region = _random_seq(rng, ls, DNA)
+        q = _random_seq(rng, lq, DNA)
+        t = _random_seq(rng, lt, DNA)
+        pq = int(rng.integers(0, lq - ls + 1))
+        q = q[:pq] + region + q[pq + ls:]
+        hom = _mutate(rng, region, DNA, 1.0 - identity, indel_rate=indel_rate)
+        pt = int(rng.integers(0, max(1, lt - len(hom)) + 1))
+        t = (t[:pt] + hom + t[pt + len(hom):])[:max(lt, len(hom))]
+        queries.append(("long%d" % i, q))
+        fwd.append(("ref%d" % i, t))
+    targets = fwd + [(tid + "_RC", reverse_complement(s)) for tid, s in fwd]
+    pairs = [(i, i) for i in range(n_pairs)] + [(i, i + n_pairs) for i in range(n_pairs)]
+    return queries, targets, pairs
+
+
+def trimmer_reads(seed=4, n_reads=10_000_000, read_len=150, n_adapters=24, adapter_len=(20, 40), planted=0.40,
+                  frag_len=(8, 40), max_subs=3):
+    """Reads of uniform ACGT; in a fraction of them the 3' end is replaced by a
+    prefix fragment of one adapter (length 8-40, clipped to the adapter) with
+    0-3 substitutions.  Targets: the adapters plus their reverse complements.
+    Vectorised: 10 M reads take a few seconds."""
+    rng = np.random.default_rng(seed)
+    adapters = [_random_seq(rng, int(rng.integers(adapter_len[0], adapter_len[1] + 1)), DNA)
+                for _ in range(n_adapters)]
+    reads = DNA[rng.integers(0, 4, size=(n_reads, read_len), dtype=np.uint8)]
+    carry = np.nonzero(rng.random(n_reads) < planted)[0]
+    which = rng.integers(0, n_adapters, size=len(carry))
+    flen = rng.integers(frag_len[0], frag_len[1] + 1, size=len(carry))
+    nsub = rng.integers(0, max_subs + 1, size=len(carry))
+    amat = np.zeros((n_adapters, adapter_len[1]), dtype=np.uint8)
+    alen = np.array([len(a) for a in adapters])
+    for i, a in enumerate(adapters):
+        amat[i, :len(a)] = np.frombuffer(a, dtype=np.uint8)
+    n = np.minimum(flen, alen[which])
+    for m in np.unique(n):
+        sel = np.nonzero(n == m)[0]
+        reads[carry[sel], read_len - m:] = amat[which[sel], :m]
+    for s in range(1, max_subs + 1):
+        sel = np.nonzero(nsub >= s)[0]
+        pos = read_len - n[sel] + (rng.random(len(sel)) * n[sel]).astype(int)
+        reads[carry[sel], pos] = DNA[rng.integers(0, 4, size=len(sel))]
+    ids = ["read%d" % i for i in range(n_reads)]
+    targets = [("adapter%d" % i, a) for i, a in enumerate(adapters)]
+    targets += [(tid + "_RC", reverse_complement(s)) for tid, s in targets]
+    targets.sort(key=lambda r: len(r[1]), reverse=True)
+    return ids, reads, targets
+
+
+def protein_database(seed=5, n_seqs=100_000, median=300.0, sigma=0.5, clip=(50, 1500)):
+    """Resident database: log-normal lengths, background residue frequencies."""
+    rng = np.random.default_rng(seed)
+    lens = np.clip(np.round(rng.lognormal(np.log(median), sigma, n_seqs)), clip[0], clip[1]).astype(int)
+    flat = AMINO[rng.choice(len(AMINO), size=int(lens.sum()), p=AMINO_FREQ)].tobytes()
+    out, o = [], 0
+    for i, n in enumerate(lens):
+        out.append(("db%d" % i, flat[o:o + int(n)]))
+        o += int(n)
+    return out
+
+
+def query_stream(seed=6, n=1000, median=300.0, sigma=0.5, max_len=5000, min_len=20, rate_hz=100.0,
+                 traceback_fraction=0.30):
+    """Poisson arrivals: (arrival_s, id, sequence, full_traceback) tuples."""
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate_hz, size=n)
+    t = np.cumsum(gaps) - gaps[0]
+    lens = np.clip(np.round(rng.lognormal(np.log(median), sigma, n)), min_len, max_len).astype(int)
+    tb = rng.random(n) < traceback_fraction
+    return [(float(t[i]), "req%d" % i, _random_seq(rng, int(lens[i]), AMINO, AMINO_FREQ), bool(tb[i]))
+            for i in range(n)]
+
+
+def config3(seed=3, **kw):
+    q, t, pairs = long_dna_pairs(seed, **kw)
+    return Workload("C3 long DNA, 64 pairs of 10-50 kb (+RC), linear gap", q, t, Settings(**C3_SETTINGS), pairs)
+
+
+def config4(seed=4, n_reads=10_000_000):
+    """Reads as one contiguous byte block: (ids, reads uint8[n, 150]) plus targets."""
+    ids, reads, targets = trimmer_reads(seed, n_reads=n_reads)
+    w = Workload("C4 trimmer, %d reads of 150 nt x 24 adapters (+RC)" % n_reads, None, targets,
+                 Settings(**C4_SETTINGS))
+    w.read_ids = ids
+    w.reads = reads
+    return w

@@ -79,6 +79,13 @@ def txt_lines(hitlist):
     return [f._format_hit(h) for h in f._get_hits()]
 
 
+def trimmed_lines(hitlist):
+    """Record lines of the trimmedFasta output (Formatters.TrimmerFormatter,
+    Hit.get_trimmed_line), in the formatter's hit order."""
+    f = R.Formatters.TrimmerFormatter(LOG, hitlist, os.devnull)
+    return [h.get_trimmed_line() for h in f._get_hits()]
+
+
 def run_case(name, queries, targets, settings, dna, program="aligner", device_memory=8 << 30):
     q, t = prepare(queries, targets, dna)
     st = R.Settings(**settings)
@@ -95,6 +102,7 @@ def run_case(name, queries, targets, settings, dna, program="aligner", device_me
     out["highest_score"] = float(score.highest_score)
     out["hits"] = [hit_record(h) for h in hl.real_hits.values()]
     out["txt"] = txt_lines(hl)
+    out["trimmed"] = trimmed_lines(hl)
     out["batches"] = []
     for b in sw.raw_batches:
         out["batches"].append({"X": b["X"], "Y": b["Y"], "n_seq": b["n_seq"], "n_tgt": b["n_tgt"],

@@ -1,0 +1,119 @@
+"""The benchmark configurations on the GPU.
+
+Samples of each configuration are checked bit-exact against the oracle (pair
+maxima, every hit, and for the trimmer the trimmedFasta text).  At full size,
+where the oracle would take hours, the checks are properties that need no
+oracle: the 16-bit dual-pair sweep and the 32-bit sweep give the same pair
+maxima, and the batched and plain forms give the same hits."""
+import numpy as np
+import pytest
+
+import cases
+from engine_helpers import run_engine
+from pypaswas_b200 import scores, workloads
+from pypaswas_b200.formatters import TrimmerFormatter
+from pypaswas_b200.hits import Hit, HitList
+from pypaswas_b200.programs import Trimmer
+from pypaswas_b200.records import SeqRecord
+
+pytestmark = pytest.mark.gpu
+
+
+def _spread(items, n):
+    return items[::max(1, len(items) // n)][:n]
+
+
+def _oracle(oracle_mod, q, t, score, st):
+    pos = cases.pos_scores(score, st, q, t)
+    return oracle_mod.run(cases.oracle_params(oracle_mod, score), q, t, pos, float(st.minimum_score))
+
+
+def _bit_exact(engine_lib, oracle_mod, queries, targets, settings):
+    q = [s.decode() for _, s in queries]
+    t = [s.decode() for _, s in targets]
+    score = scores.make_score(settings)
+    o = _oracle(oracle_mod, q, t, score, settings)
+    pm, hits, info, launches = run_engine(engine_lib, q, t, score, settings)
+    assert launches > 0
+    np.testing.assert_array_equal(pm, o["pair_max"])
+    assert hits == o["hits"]
+    return o
+
+
+def test_config1_sample_bit_exact(engine_lib, oracle_mod):
+    w = workloads.config1()
+    o = _bit_exact(engine_lib, oracle_mod, _spread(w.queries, 120), w.targets, w.settings)
+    assert len(o["hits"]) > 10
+
+
+def test_config2_sample_bit_exact(engine_lib, oracle_mod):
+    w = workloads.config2()
+    o = _bit_exact(engine_lib, oracle_mod, _spread(w.queries, 8), _spread(w.targets, 48), w.settings)
+    assert len(o["hits"]) > 0
+
+
+def _c4_sample(n_reads):
+    w = workloads.config4(n_reads=n_reads)
+    reads = [(w.read_ids[i], w.reads[i].tobytes()) for i in range(n_reads)]
+    return w, reads
+
+
+def test_config4_sample_bit_exact_with_trimmed_fasta(engine_lib, oracle_mod):
+    w, reads = _c4_sample(400)
+    o = _bit_exact(engine_lib, oracle_mod, reads, w.targets, w.settings)
+    assert len(o["hits"]) > 50
+    # the trimmer program's output against the oracle's hits put through the
+    # same HitList and formatter
+    qrec = [SeqRecord(s.decode(), i) for i, s in reads]
+    trec = [SeqRecord(s.decode(), i) for i, s in w.targets]
+    prog = Trimmer(None, None, w.settings)
+    try:
+        got = TrimmerFormatter(None, prog.process(qrec, trec, None), None).lines()
+    finally:
+        prog.smith_waterman.close()
+    hl = HitList(None)
+    for h in o["hits"]:
+        hit = Hit(None, qrec[h["query"]], trec[h["target"]], (h["s_start"], h["s_end"]), (h["t_start"], h["t_end"]))
+        hit.set_sequence_match(h["sequence_match"])
+        hit.set_alignment(h["alignment"])
+        hit.set_target_match(h["target_match"])
+        hit.set_scores(h["score"], h["matches"], h["mismatches"])
+        if prog.smith_waterman._filter_hit(hit):
+            hl.append(hit)
+    assert got == TrimmerFormatter(None, hl, None).lines()
+    assert len(got) > 50
+
+
+@pytest.mark.parametrize("config", [1, 2])
+def test_full_size_sixteen_and_thirty_two_bit_sweeps_agree(engine_lib, config):
+    w = workloads.config1() if config == 1 else workloads.config2()
+    score = scores.make_score(w.settings)
+    q = [s.decode() for _, s in w.queries]
+    t = [s.decode() for _, s in w.targets]
+    pm16, _, info16, _ = run_engine(engine_lib, q, t, score, w.settings, score_only=True)
+    pm32, _, info32, _ = run_engine(engine_lib, q, t, score, w.settings, score_only=True, int32=True)
+    assert info16.score_launches > 0 and info32.score_launches > 0
+    np.testing.assert_array_equal(pm16, pm32)
+    assert np.all(pm16 >= 0)
+
+
+def test_config4_one_million_reads_sweeps_agree(engine_lib):
+    w = workloads.config4(n_reads=1_000_000)
+    score = scores.make_score(w.settings)
+    q = [w.reads[i].tobytes().decode() for i in range(len(w.read_ids))]
+    t = [s.decode() for _, s in w.targets]
+    pm16, _, _, _ = run_engine(engine_lib, q, t, score, w.settings, score_only=True)
+    pm32, _, _, _ = run_engine(engine_lib, q, t, score, w.settings, score_only=True, int32=True)
+    np.testing.assert_array_equal(pm16, pm32)
+
+
+def test_plain_and_batched_forms_agree_on_config1_sample(engine_lib):
+    w = workloads.config1()
+    score = scores.make_score(w.settings)
+    q = [s.decode() for _, s in _spread(w.queries, 20)]
+    t = [s.decode() for _, s in w.targets]
+    pm_b, hits_b, info_b, _ = run_engine(engine_lib, q, t, score, w.settings)
+    pm_p, hits_p, info_p, _ = run_engine(engine_lib, q, t, score, w.settings, plain=True)
+    np.testing.assert_array_equal(pm_b, pm_p)
+    assert hits_b == hits_p
+    assert info_p.kernel_launches >= len(q) * len(t)

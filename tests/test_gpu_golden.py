@@ -4,6 +4,7 @@ import pytest
 
 import golden_util as G
 from pypaswas_b200.exceptions import CudaException
+from pypaswas_b200.formatters import DefaultFormatter, TrimmerFormatter
 from pypaswas_b200.programs import Aligner, Trimmer
 from pypaswas_b200.records import SeqRecord
 
@@ -40,5 +41,12 @@ def test_driver_matches_reference(engine_lib, name):
         assert G.hits_by_pair(got) == G.hits_by_pair(ref)
         if len(fx["batches"]) == 1:
             assert got == ref
+        # the program's text output, byte for byte (with several reference
+        # batches, hits of equal ids and score may be listed in another order)
+        txt, trimmed = DefaultFormatter(None, hl, None).lines(), TrimmerFormatter(None, hl, None).lines()
+        if len(fx["batches"]) == 1:
+            assert txt == fx["txt"] and trimmed == fx["trimmed"]
+        else:
+            assert sorted(txt) == sorted(fx["txt"]) and sorted(trimmed) == sorted(fx["trimmed"])
     finally:
         prog.smith_waterman.close()
