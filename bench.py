@@ -49,6 +49,9 @@ def parse():
                          "the bench line then names the reduced workload)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (ncu captures)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain one-pair-per-launch leg")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
+    ap.add_argument("--serve-seconds", type=float, default=10.0, help="length of the serving leg's arrival stream")
+    ap.add_argument("--serve-load", type=float, default=0.7, help="offered load as a fraction of batched peak")
     return ap.parse_args()
 
 
@@ -329,6 +332,8 @@ def main():
            "e2e": {"value": e2e_value, "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}}
     if not args.no_plain:
         out["plain"] = plain_vs_batched(w, local, value)
+    if not args.no_serve and rank == 0:
+        out["serve"] = serve_leg(local, args.serve_seconds, args.serve_load)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(w, score, args.cpu_seconds, processes=1)
     if rank == 0:
@@ -370,6 +375,40 @@ def plain_vs_batched(w, device, batched_value, n_q=8, n_t=64):
             "launches": out["plain"]["launches"], "batched_same_sample": out["batched"]["value"],
             "batched_over_plain": batched_value / out["plain"]["value"],
             "hits_equal": out["plain"]["hits"] == out["batched"]["hits"]}
+
+
+def serve_leg(device, seconds, load, workers=2, max_batch=32):
+    """Serving configuration: a resident database of 100,000 protein sequences
+    (log-normal lengths, median 300, 50-1,500 aa), Poisson arrivals of single
+    queries (log-normal, median 300, max 5,000 aa), 70% top-10 by pair maximum
+    and 30% full affine traceback (BLOSUM62, -11/-1).  First the batched peak:
+    64 requests submitted at once; then an arrival stream at `load` x that
+    peak, reporting p50/p99 latency and the GCUPS served."""
+    from pypaswas_b200 import serving, workloads
+    st = workloads.Settings(**workloads.C5_SETTINGS)
+    db = workloads.protein_database()
+    srv = serving.Server(st, device=device, workers=workers, max_batch=max_batch)
+    try:
+        srv.load_db(db)
+        warm = workloads.query_stream(seed=8, n=16, rate_hz=1e9)
+        serving.run_arrivals(srv, warm)
+        burst = workloads.query_stream(seed=7, n=64, rate_hz=1e9)
+        peak = serving.run_arrivals(srv, burst)
+        probe = workloads.query_stream(seed=9, n=4000, rate_hz=1.0)
+        mean_cells = float(np.mean([len(q[2]) for q in probe])) * srv.db_residues
+        rate = load * peak["gcups"] * 1e9 / mean_cells
+        stream = workloads.query_stream(seed=6, n=max(20, int(rate * seconds)), rate_hz=rate)
+        rep = serving.run_arrivals(srv, stream)
+    finally:
+        srv.close()
+    return {"db": "%d sequences, %d residues, resident" % (len(db), srv.db_residues),
+            "workers": workers, "max_batch": max_batch,
+            "batched_peak_gcups": peak["gcups"], "offered_load": load, "offered_rps": rep["offered_rps"],
+            "gcups": rep["gcups"], "fraction_of_peak": rep["gcups"] / peak["gcups"],
+            "p50_ms": rep["p50_ms"], "p99_ms": rep["p99_ms"], "max_ms": rep["max_ms"],
+            "p99_top_ms": rep["p99_top_ms"], "p99_traceback_ms": rep["p99_traceback_ms"],
+            "requests": rep["requests"], "mean_batch": rep["mean_batch"], "workers_used": rep["workers_used"],
+            "peak_reserved_bytes": rep["peak_reserved_bytes"]}
 
 
 def _sixteen_bit(engine, w):

@@ -30,6 +30,7 @@ extern "C" {
 #define PW_ERR_NOMEM (-4)
 #define PW_ERR_CAPACITY (-5)
 #define PW_ERR_STATE (-6)
+#define PW_ERR_TIMEOUT (-7)
 
 /* pw_align() flags */
 #define PW_FLAG_SCORE_ONLY 1u /* pair maxima only: no starting points, no walk */
@@ -139,6 +140,15 @@ int pw_set_targets(pw_engine* e, const uint8_t* residues, const int64_t* offsets
  * walked, chosen in emission order (SmithWaterman.py:683-685). */
 int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_info* info);
 
+/* Upper bound, in bytes, on the direction-matrix (cell code) memory of one
+ * memory wave of pw_align; 0 restores the automatic choice (half of the free
+ * device memory, at most 48 GiB).  Traced pairs beyond the bound run in
+ * further waves; a single pair larger than the bound runs alone.  Replaces
+ * the batch sizing of SmithWaterman._get_max_number_sequences
+ * (SmithWaterman.py:202-221) with its memory fraction `maximum_memory_usage`
+ * (SmithWaterman.py:420-432). */
+int pw_set_wave_limit(pw_engine* e, int64_t bytes);
+
 /* Pair maxima (the last block of the maxima chain, default_main.cu:591),
  * row-major [n_queries][n_targets]. */
 int pw_get_pair_max(pw_engine* e, float* out, int64_t n);
@@ -163,6 +173,73 @@ int pw_last_launch_count(pw_engine* e, int64_t* n);
  * __viaddmax_s16x2 (two 16-bit lanes per instruction).  Used as the roofline
  * denominators by bench.py. */
 int pw_measure_int_peak(pw_engine* e, double* ops32, double* ops16x2, double* ms);
+
+/* ------------------------------------------------------------------------
+ * Serving loop (no counterpart in the reference, which aligns one batch per
+ * process): continuous batching of single-query requests against a database
+ * kept resident on the device.
+ *
+ * W worker threads each own an engine (one CUDA stream) holding the database.
+ * A worker that becomes free takes the requests waiting at that moment -- up to
+ * max_batch of one mode, oldest first -- and runs them as one pw_align; the
+ * batches of different workers overlap on the device.  Traceback requests are
+ * admitted by direction-matrix memory: each reserves an estimate of its cell
+ * codes (query length x database residues x the traced fraction seen so far,
+ * at least 16 MiB) from `direction_budget` bytes shared by all workers; a
+ * batch starts only when its reservation fits, and the engine's memory waves
+ * (pw_set_wave_limit) keep its cell codes within it.  Every result equals that
+ * of a lone pw_align of the query against the database.
+ * ---------------------------------------------------------------------- */
+#define PW_SERVE_TOP 0        /* pair maxima only; the top_k targets by maximum (ties: lower index) */
+#define PW_SERVE_TRACEBACK 1  /* full path: the walk's hits of the query, in HitList order */
+
+typedef struct pw_server pw_server;
+
+typedef struct {
+    int32_t status;          /* PW_OK or the failure of the request's batch */
+    int32_t mode;
+    int32_t batch_queries;   /* requests in the batch that carried this one */
+    int32_t worker;
+    int64_t cells;           /* len(query) x database residues */
+    int64_t n_hits;          /* top hits (PW_SERVE_TOP) or walk hits (PW_SERVE_TRACEBACK) */
+    int64_t string_bytes;    /* alignment strings of the hits */
+    int64_t reserved_bytes;  /* direction-matrix reservation of the batch */
+    double queue_ms;         /* submit -> batch start */
+    double run_ms;           /* batch start -> result */
+    double latency_ms;       /* submit -> result */
+} pw_request_info;
+
+typedef struct {
+    int64_t submitted, completed, batches, cells, pending;
+    int64_t budget_bytes, reserved_bytes, peak_reserved_bytes;
+    double busy_ms;          /* summed wall time of the workers' batches */
+    double traced_fraction;  /* current estimate used for reservations */
+} pw_server_counters;
+
+/* n_workers 1..16, max_batch 1..4096; direction_budget 0 = 8 GiB. */
+int pw_server_create(int device, int n_workers, int max_batch, int64_t direction_budget, pw_server** out);
+/* Finishes the waiting requests, then stops the workers and frees everything. */
+void pw_server_destroy(pw_server* s);
+const char* pw_server_last_error(pw_server* s);
+/* Same arguments as pw_set_scoring; before pw_server_load_db. */
+int pw_server_set_scoring(pw_server* s, const float* matrix, int dim, int char_offset, float gap, float ext,
+                          int affine, float lower_limit, float minimum_score, double host_minimum, double highest,
+                          double filter_factor);
+/* The resident database (targets); id keys must be >= 0.  Once. */
+int pw_server_load_db(pw_server* s, const uint8_t* residues, const int64_t* offsets, int32_t n,
+                      const int32_t* id_keys);
+/* Queues one query; returns at once with a ticket. */
+int pw_server_submit(pw_server* s, const uint8_t* residues, int64_t length, int32_t mode, int32_t top_k,
+                     int64_t* ticket);
+/* Waits for a request (timeout_ms < 0: no limit; PW_ERR_TIMEOUT when it runs out). */
+int pw_server_wait(pw_server* s, int64_t ticket, int32_t timeout_ms, pw_request_info* info);
+/* Results of a finished request; buffers sized from pw_request_info. */
+int pw_server_top_hits(pw_server* s, int64_t ticket, int32_t* targets, float* scores, int32_t k);
+int pw_server_hits(pw_server* s, int64_t ticket, pw_hit* hits, int64_t max_hits, char* strbuf,
+                   int64_t strbuf_bytes);
+/* Frees a finished request's results. */
+int pw_server_release(pw_server* s, int64_t ticket);
+int pw_server_stats(pw_server* s, pw_server_counters* st);
 
 /* Pair maxima without any device allocation.  No counterpart in the
  * reference: it serves callers that cannot call cudaMalloc themselves or have

@@ -21,6 +21,9 @@ PW_ERR_KERNEL = -3
 PW_ERR_NOMEM = -4
 PW_ERR_CAPACITY = -5
 PW_ERR_STATE = -6
+PW_ERR_TIMEOUT = -7
+PW_SERVE_TOP = 0
+PW_SERVE_TRACEBACK = 1
 
 PW_FLAG_SCORE_ONLY = 1
 PW_FLAG_PLAIN = 2
@@ -31,6 +34,9 @@ EXPORTED_SYMBOLS = (
     "pw_create", "pw_destroy", "pw_last_error", "pw_device_free_memory", "pw_set_scoring",
     "pw_set_queries", "pw_set_targets", "pw_align", "pw_get_pair_max", "pw_get_hits",
     "pw_get_starting_points", "pw_last_launch_count", "pw_measure_int_peak", "pw_score_max_noalloc",
+    "pw_set_wave_limit", "pw_server_create", "pw_server_destroy", "pw_server_last_error", "pw_server_set_scoring",
+    "pw_server_load_db", "pw_server_submit", "pw_server_wait", "pw_server_top_hits", "pw_server_hits",
+    "pw_server_release", "pw_server_stats",
 )
 
 
@@ -68,6 +74,26 @@ class PwRunInfo(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class PwRequestInfo(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int32), ("mode", ctypes.c_int32), ("batch_queries", ctypes.c_int32),
+                ("worker", ctypes.c_int32), ("cells", ctypes.c_int64), ("n_hits", ctypes.c_int64),
+                ("string_bytes", ctypes.c_int64), ("reserved_bytes", ctypes.c_int64), ("queue_ms", ctypes.c_double),
+                ("run_ms", ctypes.c_double), ("latency_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class PwServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("batches", ctypes.c_int64),
+                ("cells", ctypes.c_int64), ("pending", ctypes.c_int64), ("budget_bytes", ctypes.c_int64),
+                ("reserved_bytes", ctypes.c_int64), ("peak_reserved_bytes", ctypes.c_int64),
+                ("busy_ms", ctypes.c_double), ("traced_fraction", ctypes.c_double)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 def bind(lib):
     """Declares the argument and result types of every exported function."""
     P, I32, I64, U32, F, D = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_uint32, ctypes.c_float, \
@@ -88,6 +114,20 @@ def bind(lib):
         "pw_measure_int_peak": (ctypes.c_int, [P, ctypes.POINTER(D), ctypes.POINTER(D), ctypes.POINTER(D)]),
         "pw_score_max_noalloc": (ctypes.c_int, [ctypes.c_int, P, ctypes.c_int, ctypes.c_int, F, F, ctypes.c_int,
                                                 P, P, I32, P, P, I32, P, ctypes.c_char_p, I32]),
+        "pw_set_wave_limit": (ctypes.c_int, [P, I64]),
+        "pw_server_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, I64,
+                                            ctypes.POINTER(ctypes.c_void_p)]),
+        "pw_server_destroy": (None, [P]),
+        "pw_server_last_error": (ctypes.c_char_p, [P]),
+        "pw_server_set_scoring": (ctypes.c_int, [P, P, ctypes.c_int, ctypes.c_int, F, F, ctypes.c_int, F, F, D, D,
+                                                 D]),
+        "pw_server_load_db": (ctypes.c_int, [P, P, P, I32, P]),
+        "pw_server_submit": (ctypes.c_int, [P, P, I64, I32, I32, ctypes.POINTER(I64)]),
+        "pw_server_wait": (ctypes.c_int, [P, I64, I32, ctypes.POINTER(PwRequestInfo)]),
+        "pw_server_top_hits": (ctypes.c_int, [P, I64, P, P, I32]),
+        "pw_server_hits": (ctypes.c_int, [P, I64, P, I64, P, I64]),
+        "pw_server_release": (ctypes.c_int, [P, I64]),
+        "pw_server_stats": (ctypes.c_int, [P, ctypes.POINTER(PwServerStats)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -229,6 +269,9 @@ class Engine(object):
                self.lib.pw_measure_int_peak(self.handle, ctypes.byref(r32), ctypes.byref(r16), ctypes.byref(ms)),
                "pw_measure_int_peak")
         return r32.value, r16.value, ms.value
+
+    def set_wave_limit(self, nbytes):
+        _check(self.lib, self.handle, self.lib.pw_set_wave_limit(self.handle, int(nbytes)), "pw_set_wave_limit")
 
     def launch_count(self):
         n = ctypes.c_int64()

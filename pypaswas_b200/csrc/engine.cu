@@ -73,6 +73,10 @@ struct Prepared {
     std::vector<int32_t> order;  // query indices by length, longest first
     std::vector<int32_t> order_t;  // target indices by length, longest first
     std::vector<int32_t> qlen, tlen;
+    int64_t maxlq = 0, maxlt = 0;
+    float maxabs = 0.0f;         // largest |score| over the query residues' rows
+    bool q_int8 = true;          // query rows: integers in [-127, 127]
+    bool t_int8 = true;          // transposed target rows: the same
 };
 
 struct StartRec {  // one starting point (emission order sortable)
@@ -107,7 +111,9 @@ struct pw_engine {
         hit_count, ops, allowed;
     // prepared (device-resident) inputs
     Prepared pr;
-    int64_t input_gen = 1, prepared_gen = 0;
+    int64_t q_gen = 1, t_gen = 1, s_gen = 1;      // inputs: queries, targets, scoring
+    int64_t prep_q[2] = {0, 0}, prep_t[2] = {0, 0};  // (sequence gen, scoring gen) last prepared
+    int64_t wave_limit = 0;                          // cell-code bytes per memory wave (0: automatic)
     // results
     std::vector<float> h_pair_max;
     std::vector<pw_hit> h_hits;
@@ -199,7 +205,7 @@ extern "C" int pw_set_scoring(pw_engine* e, const float* matrix, int dim, int ch
     e->highest = highest;
     e->filter_factor = filter_factor;
     e->scoring_set = true;
-    e->input_gen++;
+    e->s_gen++;
     return PW_OK;
 }
 
@@ -215,13 +221,20 @@ static int set_seqs(pw_engine* e, HostSeqs& S, const uint8_t* residues, const in
     }
     const int64_t total = n > 0 ? offsets[n] : 0;
     if (total > 0 && !residues) return fail(e, PW_ERR_ARG, "residues missing");
+    // the same set again (a resident database handed in once more): keep the
+    // device copy
+    if (S.set && S.n == n && (int64_t)S.raw.size() == total && S.off.size() == (size_t)(n > 0 ? n + 1 : 1) &&
+        (total == 0 || std::memcmp(S.raw.data(), residues, (size_t)total) == 0) &&
+        (n == 0 || (std::memcmp(S.off.data(), offsets, (size_t)(n + 1) * sizeof(int64_t)) == 0 &&
+                    std::memcmp(S.key.data(), id_keys, (size_t)n * sizeof(int32_t)) == 0)))
+        return PW_OK;
     S.raw.assign(residues, residues + total);
     S.off.assign(offsets, offsets + (n > 0 ? n + 1 : 0));
     if (n == 0) S.off.assign(1, 0);
     S.key.assign(id_keys, id_keys + n);
     S.n = n;
     S.set = true;
-    e->input_gen++;
+    (&S == &e->Q ? e->q_gen : e->t_gen)++;
     return PW_OK;
 }
 
@@ -319,77 +332,25 @@ static cudaError_t download(pw_engine* e, std::vector<HT>& v, const void* src, s
 }
 
 // Builds the device copies of the sequences, the compact query alphabet and the
-// compact substitution matrix.  Cached: nothing is uploaded again while the
-// sequences and the scoring model are unchanged (the target database and the
-// query set stay resident on the device).
-static int prepare(pw_engine* e) {
-    if (e->prepared_gen == e->input_gen) return PW_OK;
-    const HostSeqs& Q = e->Q;
+// compact substitution matrices.  Targets and queries are prepared separately
+// and cached: a target database stays resident on the device while query sets
+// come and go, and nothing is uploaded again while the sequences and the
+// scoring model are unchanged.
+static int prepare_targets(pw_engine* e) {
+    if (e->prep_t[0] == e->t_gen && e->prep_t[1] == e->s_gen) return PW_OK;
     const HostSeqs& T = e->T;
     const int off = e->char_offset, dim = e->dim;
     Prepared& pr = e->pr;
-    // residues must index the matrix (default_main.cu:234 reads matrix[c - offset])
-    int map[256];
-    for (int i = 0; i < 256; ++i) map[i] = -1;
-    std::vector<int> alphabet;
-    for (uint8_t c : Q.raw) {
-        if (map[c] >= 0) continue;
-        if (c == 0 || (int)c < off || (int)c >= off + dim)
-            return fail(e, PW_ERR_ARG, "query residue outside the scoring matrix: code " + std::to_string(c));
-        map[c] = (int)alphabet.size();
-        alphabet.push_back(c);
-    }
     for (uint8_t c : T.raw)
         if (c == 0 || (int)c < off || (int)c >= off + dim)
             return fail(e, PW_ERR_ARG, "target residue outside the scoring matrix: code " + std::to_string(c));
-    if (alphabet.size() > 250) return fail(e, PW_ERR_ARG, "too many distinct query residues");
-    pr.alpha = (int)alphabet.size();
-    const int alpha1 = pr.alpha + 1;
-
-    // integer path: every used score and penalty is an integer, scores fit int8,
-    // and no DP value can reach 2^24 (where fp32 stops being exact)
-    bool ints = std::floor(e->gap) == e->gap && std::floor(e->ext) == e->ext;
-    float maxabs = 0.0f;
-    for (int a = 0; a < pr.alpha; ++a)
-        for (int j = 0; j < dim; ++j) {
-            const float v = e->matrix[(size_t)(alphabet[a] - off) * dim + j];
-            if (std::floor(v) != v || v < -127.0f || v > 127.0f) ints = false;
-            maxabs = std::max(maxabs, std::fabs(v));
-        }
-    pr.qlen.assign(Q.n, 0);
     pr.tlen.assign(T.n, 0);
-    int64_t maxlq = 0, maxlt = 0;
-    for (int32_t i = 0; i < Q.n; ++i) maxlq = std::max<int64_t>(maxlq, pr.qlen[i] = (int32_t)(Q.off[i + 1] - Q.off[i]));
-    for (int32_t i = 0; i < T.n; ++i) maxlt = std::max<int64_t>(maxlt, pr.tlen[i] = (int32_t)(T.off[i + 1] - T.off[i]));
-    if ((double)maxabs * (double)std::min(maxlq, maxlt) + std::fabs(e->gap) + std::fabs(e->ext) >= 16777216.0)
-        ints = false;
-    if (std::fabs(e->gap) > 1.0e6f || std::fabs(e->ext) > 1.0e6f) ints = false;
-    pr.int_path = ints;
-
-    std::vector<int8_t> cm8((size_t)alpha1 * dim, (int8_t)-128);
-    std::vector<float> cmf((size_t)alpha1 * dim, -1.0e30f);
-    for (int a = 0; a < pr.alpha; ++a)
-        for (int j = 0; j < dim; ++j) {
-            const float v = e->matrix[(size_t)(alphabet[a] - off) * dim + j];
-            cmf[(size_t)a * dim + j] = v;
-            cm8[(size_t)a * dim + j] = ints ? (int8_t)v : 0;
-        }
-
-    // queries: compact codes, each sequence 16-byte aligned and padded to a
-    // multiple of 4 with the pad code
-    std::vector<int64_t> qco(Q.n + 1, 0);
-    int64_t pos = 0;
-    for (int32_t i = 0; i < Q.n; ++i) {
-        qco[i] = pos;
-        pos += align_up(std::max<int64_t>(pr.qlen[i], 1), 16);
-    }
-    qco[Q.n] = pos;
-    std::vector<uint8_t> qc((size_t)std::max<int64_t>(pos, 16), (uint8_t)pr.alpha);
-    for (int32_t i = 0; i < Q.n; ++i)
-        for (int32_t k = 0; k < pr.qlen[i]; ++k) qc[qco[i] + k] = (uint8_t)map[Q.raw[Q.off[i] + k]];
-    // targets: matrix residue index
+    pr.maxlt = 0;
+    for (int32_t i = 0; i < T.n; ++i)
+        pr.maxlt = std::max<int64_t>(pr.maxlt, pr.tlen[i] = (int32_t)(T.off[i + 1] - T.off[i]));
+    // targets: matrix residue index, each sequence 16-byte aligned
     std::vector<int64_t> tco(T.n + 1, 0);
-    pos = 0;
+    int64_t pos = 0;
     for (int32_t i = 0; i < T.n; ++i) {
         tco[i] = pos;
         pos += align_up(std::max<int64_t>(pr.tlen[i], 1), 16);
@@ -398,18 +359,12 @@ static int prepare(pw_engine* e) {
     std::vector<uint8_t> tc((size_t)std::max<int64_t>(pos, 16), 0);
     for (int32_t i = 0; i < T.n; ++i)
         for (int32_t k = 0; k < pr.tlen[i]; ++k) tc[tco[i] + k] = (uint8_t)(T.raw[T.off[i] + k] - off);
-
-    pr.order.resize(Q.n);
-    std::iota(pr.order.begin(), pr.order.end(), 0);
-    std::stable_sort(pr.order.begin(), pr.order.end(),
-                     [&](int a, int b) { return pr.qlen[a] > pr.qlen[b]; });
     pr.order_t.resize(T.n);
     std::iota(pr.order_t.begin(), pr.order_t.end(), 0);
     std::stable_sort(pr.order_t.begin(), pr.order_t.end(),
                      [&](int a, int b) { return pr.tlen[a] > pr.tlen[b]; });
-
-    // the transposed orientation: queries as strips (residue indices), targets
-    // on the lanes (compact target alphabet)
+    // the transposed orientation: targets on the lanes in a compact target
+    // alphabet, with the matrix transposed to [target residue][query residue]
     int tmap[256];
     for (int i = 0; i < 256; ++i) tmap[i] = -1;
     std::vector<int> talpha;
@@ -419,9 +374,6 @@ static int prepare(pw_engine* e) {
             talpha.push_back(c);
         }
     pr.alpha_t = (int)talpha.size();
-    std::vector<uint8_t> qres(qc.size(), 0);
-    for (int32_t i = 0; i < Q.n; ++i)
-        for (int32_t k = 0; k < pr.qlen[i]; ++k) qres[qco[i] + k] = (uint8_t)(Q.raw[Q.off[i] + k] - off);
     std::vector<uint8_t> tcc(tc.size(), (uint8_t)pr.alpha_t);
     for (int32_t i = 0; i < T.n; ++i)
         for (int32_t k = 0; k < pr.tlen[i]; ++k) tcc[tco[i] + k] = (uint8_t)tmap[T.raw[T.off[i] + k]];
@@ -435,12 +387,89 @@ static int prepare(pw_engine* e) {
             cmt8[(size_t)b * dim + j] = (int8_t)(t_int8 ? v : 0);
             cmtf[(size_t)b * dim + j] = v;
         }
-    // 16-bit halves hold every cell while the maximum stays below 32640; gap
-    // chains must stay well inside the negative half-range
-    const bool gaps16 = std::fabs(e->gap) + std::fabs(e->ext) < 8192.0f;
-    pr.s16_q = ints && gaps16;
-    pr.s16_t = ints && gaps16 && t_int8;
+    pr.t_int8 = t_int8;
+    cudaError_t c;
+#define UP(buf, vec)                                      \
+    if ((c = upload(e, buf, vec)) != cudaSuccess) return cuda_fail(e, c, "upload " #buf);
+    UP(e->t_codes, tc);
+    UP(e->t_code_off, tco);
+    UP(e->t_raw, T.raw);
+    UP(e->t_raw_off, T.off);
+    UP(e->t_len, pr.tlen);
+    UP(e->t_key, T.key);
+    UP(e->t_ccodes, tcc);
+    UP(e->t_order, pr.order_t);
+    UP(e->cmat_t8, cmt8);
+    UP(e->cmat_tf, cmtf);
+#undef UP
+    if ((c = cudaStreamSynchronize(e->stream)) != cudaSuccess) return cuda_fail(e, c, "upload targets");
+    e->prep_t[0] = e->t_gen;
+    e->prep_t[1] = e->s_gen;
+    return PW_OK;
+}
 
+static int prepare_queries(pw_engine* e) {
+    if (e->prep_q[0] == e->q_gen && e->prep_q[1] == e->s_gen) return PW_OK;
+    const HostSeqs& Q = e->Q;
+    const int off = e->char_offset, dim = e->dim;
+    Prepared& pr = e->pr;
+    // residues must index the matrix (default_main.cu:234 reads matrix[c - offset])
+    int map[256];
+    for (int i = 0; i < 256; ++i) map[i] = -1;
+    std::vector<int> alphabet;
+    for (uint8_t c : Q.raw) {
+        if (map[c] >= 0) continue;
+        if (c == 0 || (int)c < off || (int)c >= off + dim)
+            return fail(e, PW_ERR_ARG, "query residue outside the scoring matrix: code " + std::to_string(c));
+        map[c] = (int)alphabet.size();
+        alphabet.push_back(c);
+    }
+    if (alphabet.size() > 250) return fail(e, PW_ERR_ARG, "too many distinct query residues");
+    pr.alpha = (int)alphabet.size();
+    const int alpha1 = pr.alpha + 1;
+    // scores of the used rows: all integers in the int8 range?
+    bool q_int8 = true;
+    float maxabs = 0.0f;
+    for (int a = 0; a < pr.alpha; ++a)
+        for (int j = 0; j < dim; ++j) {
+            const float v = e->matrix[(size_t)(alphabet[a] - off) * dim + j];
+            if (std::floor(v) != v || v < -127.0f || v > 127.0f) q_int8 = false;
+            maxabs = std::max(maxabs, std::fabs(v));
+        }
+    pr.q_int8 = q_int8;
+    pr.maxabs = maxabs;
+    pr.qlen.assign(Q.n, 0);
+    pr.maxlq = 0;
+    for (int32_t i = 0; i < Q.n; ++i)
+        pr.maxlq = std::max<int64_t>(pr.maxlq, pr.qlen[i] = (int32_t)(Q.off[i + 1] - Q.off[i]));
+    std::vector<int8_t> cm8((size_t)alpha1 * dim, (int8_t)-128);
+    std::vector<float> cmf((size_t)alpha1 * dim, -1.0e30f);
+    for (int a = 0; a < pr.alpha; ++a)
+        for (int j = 0; j < dim; ++j) {
+            const float v = e->matrix[(size_t)(alphabet[a] - off) * dim + j];
+            cmf[(size_t)a * dim + j] = v;
+            cm8[(size_t)a * dim + j] = q_int8 ? (int8_t)v : 0;
+        }
+    // queries: compact codes, each sequence 16-byte aligned and padded to a
+    // multiple of 4 with the pad code
+    std::vector<int64_t> qco(Q.n + 1, 0);
+    int64_t pos = 0;
+    for (int32_t i = 0; i < Q.n; ++i) {
+        qco[i] = pos;
+        pos += align_up(std::max<int64_t>(pr.qlen[i], 1), 16);
+    }
+    qco[Q.n] = pos;
+    std::vector<uint8_t> qc((size_t)std::max<int64_t>(pos, 16), (uint8_t)pr.alpha);
+    for (int32_t i = 0; i < Q.n; ++i)
+        for (int32_t k = 0; k < pr.qlen[i]; ++k) qc[qco[i] + k] = (uint8_t)map[Q.raw[Q.off[i] + k]];
+    pr.order.resize(Q.n);
+    std::iota(pr.order.begin(), pr.order.end(), 0);
+    std::stable_sort(pr.order.begin(), pr.order.end(),
+                     [&](int a, int b) { return pr.qlen[a] > pr.qlen[b]; });
+    // the transposed orientation: queries as strips (matrix residue indices)
+    std::vector<uint8_t> qres(qc.size(), 0);
+    for (int32_t i = 0; i < Q.n; ++i)
+        for (int32_t k = 0; k < pr.qlen[i]; ++k) qres[qco[i] + k] = (uint8_t)(Q.raw[Q.off[i] + k] - off);
     cudaError_t c;
 #define UP(buf, vec)                                      \
     if ((c = upload(e, buf, vec)) != cudaSuccess) return cuda_fail(e, c, "upload " #buf);
@@ -451,23 +480,36 @@ static int prepare(pw_engine* e) {
     UP(e->q_len, pr.qlen);
     UP(e->q_key, Q.key);
     UP(e->q_order, pr.order);
-    UP(e->t_codes, tc);
-    UP(e->t_code_off, tco);
-    UP(e->t_raw, T.raw);
-    UP(e->t_raw_off, T.off);
-    UP(e->t_len, pr.tlen);
-    UP(e->t_key, T.key);
     UP(e->cmat_i8, cm8);
     UP(e->cmat_f, cmf);
     UP(e->q_res, qres);
-    UP(e->t_ccodes, tcc);
-    UP(e->t_order, pr.order_t);
-    UP(e->cmat_t8, cmt8);
-    UP(e->cmat_tf, cmtf);
 #undef UP
+    if ((c = cudaStreamSynchronize(e->stream)) != cudaSuccess) return cuda_fail(e, c, "upload queries");
+    e->prep_q[0] = e->q_gen;
+    e->prep_q[1] = e->s_gen;
+    return PW_OK;
+}
+
+static int prepare(pw_engine* e) {
+    int rc = prepare_targets(e);
+    if (rc != PW_OK) return rc;
+    if ((rc = prepare_queries(e)) != PW_OK) return rc;
+    Prepared& pr = e->pr;
+    // integer path: every used score and penalty is an integer, scores fit int8,
+    // and no DP value can reach 2^24 (where fp32 stops being exact)
+    bool ints = pr.q_int8 && std::floor(e->gap) == e->gap && std::floor(e->ext) == e->ext;
+    if ((double)pr.maxabs * (double)std::min(pr.maxlq, pr.maxlt) + std::fabs(e->gap) + std::fabs(e->ext) >=
+        16777216.0)
+        ints = false;
+    if (std::fabs(e->gap) > 1.0e6f || std::fabs(e->ext) > 1.0e6f) ints = false;
+    pr.int_path = ints;
+    // 16-bit halves hold every cell while the maximum stays below 32640; gap
+    // chains must stay well inside the negative half-range
+    const bool gaps16 = std::fabs(e->gap) + std::fabs(e->ext) < 8192.0f;
+    pr.s16_q = ints && gaps16;
+    pr.s16_t = ints && gaps16 && pr.t_int8;
+    cudaError_t c;
     if ((c = e->counter.reserve(64 * sizeof(int))) != cudaSuccess) return cuda_fail(e, c, "alloc counter");
-    if ((c = cudaStreamSynchronize(e->stream)) != cudaSuccess) return cuda_fail(e, c, "upload");
-    e->prepared_gen = e->input_gen;
     return PW_OK;
 }
 
@@ -1067,6 +1109,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
     int64_t budget = std::min<int64_t>((int64_t)(free_b * 0.5) + (int64_t)e->codes.bytes, (int64_t)48 << 30);
+    if (e->wave_limit > 0) budget = e->wave_limit;
     std::vector<std::pair<size_t, size_t>> waves;
     {
         size_t i0 = 0;
@@ -1405,6 +1448,13 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     inf.finish_ms = wall_ms() - t_finish;
     inf.total_ms = wall_ms() - t_call;
     if (info) *info = inf;
+    return PW_OK;
+}
+
+extern "C" int pw_set_wave_limit(pw_engine* e, int64_t bytes) {
+    if (!e) return PW_ERR_ARG;
+    if (bytes < 0) return fail(e, PW_ERR_ARG, "wave limit must be >= 0");
+    e->wave_limit = bytes;
     return PW_OK;
 }
 

@@ -87,3 +87,11 @@ def test_kernel_constants_follow_compiled_literals():
     gap, ext, affine, ll, mn = scores.make_score(st).kernel_constants()
     assert not affine and gap == np.float32(-5.0) and ext == 0
     assert ll == np.float32(0.1) and mn == np.float32(15.3)
+
+
+def test_serving_percentile_is_nearest_rank():
+    from pypaswas_b200.serving import percentile
+    v = list(range(1, 101))
+    assert percentile(v, 50) == 50 and percentile(v, 99) == 99 and percentile(v, 100) == 100
+    assert percentile([7.0], 99) == 7.0
+    assert percentile([3, 1, 2], 50) == 2
