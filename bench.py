@@ -50,8 +50,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (ncu captures)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain one-pair-per-launch leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
-    ap.add_argument("--serve-seconds", type=float, default=10.0, help="length of the serving leg's arrival stream")
-    ap.add_argument("--serve-load", type=float, default=0.7, help="offered load as a fraction of batched peak")
+    ap.add_argument("--no-chain", action="store_true", help="16-bit sweep without chained strips (comparison)")
+    ap.add_argument("--serve-seconds", type=float, default=6.0, help="length of each arrival stream of the serving leg")
+    ap.add_argument("--serve-loads", default="0.3,0.5,0.7", help="offered loads (fractions of batched peak) swept")
     return ap.parse_args()
 
 
@@ -252,8 +253,9 @@ def main():
     mode = "affine" if affine else "linear"
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > L2 (126 MB)
 
+    chain = not args.no_chain
     for _ in range(args.warmup):
-        e.align()
+        e.align(chain=chain)
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
@@ -268,7 +270,7 @@ def main():
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
         a.record()
-        info = e.align()  # synchronous: returns when the step's device work is done
+        info = e.align(chain=chain)  # synchronous: returns when the step's device work is done
         b.record()
         torch.cuda.synchronize()
         times.append(a.elapsed_time(b))
@@ -318,7 +320,9 @@ def main():
                       "filter_factor": w.settings.filter_factor,
                       "l2": "flushed between steps (256 MiB write); each step also writes >1e11 B of cell codes",
                       "parallelism": "replica per GPU" if world > 1 else "single GPU"},
-           "phases_ms": {"score": last["score_ms"], "trace": last["trace_ms"], "walk": last["walk_ms"]},
+           "phases_ms": {"score": last["score_ms"], "trace": last["trace_ms"], "walk": last["walk_ms"],
+                         "score_kernels": last["score_kernel_ms"], "trace_kernels": last["trace_kernel_ms"],
+                         "host_setup": last["setup_ms"], "host_finish": last["finish_ms"], "call": last["total_ms"]},
            "gpu_launches": int(sum(i["kernel_launches"] for i in infos)),
            "clocks": clocks,
            "roofline": {"bound": "int_alu", "kernel": dom, "achieved": achieved,
@@ -333,7 +337,7 @@ def main():
     if not args.no_plain:
         out["plain"] = plain_vs_batched(w, local, value)
     if not args.no_serve and rank == 0:
-        out["serve"] = serve_leg(local, args.serve_seconds, args.serve_load)
+        out["serve"] = serve_leg(local, args.serve_seconds, [float(x) for x in args.serve_loads.split(",")])
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(w, score, args.cpu_seconds, processes=1)
     if rank == 0:
@@ -377,38 +381,40 @@ def plain_vs_batched(w, device, batched_value, n_q=8, n_t=64):
             "hits_equal": out["plain"]["hits"] == out["batched"]["hits"]}
 
 
-def serve_leg(device, seconds, load, workers=2, max_batch=32):
+def serve_leg(device, seconds, loads, workers=2, max_batch=32):
     """Serving configuration: a resident database of 100,000 protein sequences
     (log-normal lengths, median 300, 50-1,500 aa), Poisson arrivals of single
     queries (log-normal, median 300, max 5,000 aa), 70% top-10 by pair maximum
     and 30% full affine traceback (BLOSUM62, -11/-1).  First the batched peak:
-    64 requests submitted at once; then an arrival stream at `load` x that
-    peak, reporting p50/p99 latency and the GCUPS served."""
+    64 requests submitted at once; then, for each offered load (a fraction of
+    that peak), an arrival stream of `seconds`, reporting p50/p99 latency and
+    the GCUPS served."""
     from pypaswas_b200 import serving, workloads
     st = workloads.Settings(**workloads.C5_SETTINGS)
     db = workloads.protein_database()
     srv = serving.Server(st, device=device, workers=workers, max_batch=max_batch)
+    sweep = []
     try:
         srv.load_db(db)
-        warm = workloads.query_stream(seed=8, n=16, rate_hz=1e9)
-        serving.run_arrivals(srv, warm)
-        burst = workloads.query_stream(seed=7, n=64, rate_hz=1e9)
-        peak = serving.run_arrivals(srv, burst)
+        serving.run_arrivals(srv, workloads.query_stream(seed=8, n=16, rate_hz=1e9))
+        peak = serving.run_arrivals(srv, workloads.query_stream(seed=7, n=64, rate_hz=1e9))
         probe = workloads.query_stream(seed=9, n=4000, rate_hz=1.0)
         mean_cells = float(np.mean([len(q[2]) for q in probe])) * srv.db_residues
-        rate = load * peak["gcups"] * 1e9 / mean_cells
-        stream = workloads.query_stream(seed=6, n=max(20, int(rate * seconds)), rate_hz=rate)
-        rep = serving.run_arrivals(srv, stream)
+        for k, load in enumerate(loads):
+            rate = load * peak["gcups"] * 1e9 / mean_cells
+            stream = workloads.query_stream(seed=60 + k, n=max(20, int(rate * seconds)), rate_hz=rate)
+            rep = serving.run_arrivals(srv, stream)
+            sweep.append({"offered_load": load, "offered_rps": rep["offered_rps"], "gcups": rep["gcups"],
+                          "fraction_of_peak": rep["gcups"] / peak["gcups"], "p50_ms": rep["p50_ms"],
+                          "p99_ms": rep["p99_ms"], "max_ms": rep["max_ms"], "p99_top_ms": rep["p99_top_ms"],
+                          "p99_traceback_ms": rep["p99_traceback_ms"], "requests": rep["requests"],
+                          "mean_batch": rep["mean_batch"], "workers_used": rep["workers_used"],
+                          "peak_reserved_bytes": rep["peak_reserved_bytes"]})
     finally:
         srv.close()
     return {"db": "%d sequences, %d residues, resident" % (len(db), srv.db_residues),
-            "workers": workers, "max_batch": max_batch,
-            "batched_peak_gcups": peak["gcups"], "offered_load": load, "offered_rps": rep["offered_rps"],
-            "gcups": rep["gcups"], "fraction_of_peak": rep["gcups"] / peak["gcups"],
-            "p50_ms": rep["p50_ms"], "p99_ms": rep["p99_ms"], "max_ms": rep["max_ms"],
-            "p99_top_ms": rep["p99_top_ms"], "p99_traceback_ms": rep["p99_traceback_ms"],
-            "requests": rep["requests"], "mean_batch": rep["mean_batch"], "workers_used": rep["workers_used"],
-            "peak_reserved_bytes": rep["peak_reserved_bytes"]}
+            "workers": workers, "max_batch": max_batch, "batched_peak_gcups": peak["gcups"],
+            "seconds_per_rate": seconds, "sweep": sweep}
 
 
 def _sixteen_bit(engine, w):

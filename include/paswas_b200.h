@@ -36,6 +36,7 @@ extern "C" {
 #define PW_FLAG_SCORE_ONLY 1u /* pair maxima only: no starting points, no walk */
 #define PW_FLAG_PLAIN 2u      /* one pair per kernel launch (the unbatched form) */
 #define PW_FLAG_INT32 4u      /* keep the score sweep on 32-bit lanes (no 16-bit dual-pair sweep) */
+#define PW_FLAG_NO_CHAIN 8u   /* 16-bit sweep: run each multi-strip item on one warp (no chained strips) */
 
 typedef struct pw_engine pw_engine;
 
@@ -149,6 +150,16 @@ int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_info* info)
  * (SmithWaterman.py:420-432). */
 int pw_set_wave_limit(pw_engine* e, int64_t bytes);
 
+/* Tuning knobs of the kernels' launch shapes (no counterpart in the
+ * reference, whose shapes are fixed template constants, default_main.cu:7-30).
+ * Values 0 restore the automatic choice.
+ *   PW_TUNE_CHAIN_MIN   16-bit score sweep: multi-strip items whose cost
+ *                       reaches this many thousandths of the mean per-warp
+ *                       load are cut into chained one-strip entries (default
+ *                       500; 1 chains nearly every multi-strip item) */
+#define PW_TUNE_CHAIN_MIN 0
+int pw_set_tuning(pw_engine* e, int key, int64_t value);
+
 /* Pair maxima (the last block of the maxima chain, default_main.cu:591),
  * row-major [n_queries][n_targets]. */
 int pw_get_pair_max(pw_engine* e, float* out, int64_t n);
@@ -207,6 +218,9 @@ typedef struct {
     double queue_ms;         /* submit -> batch start */
     double run_ms;           /* batch start -> result */
     double latency_ms;       /* submit -> result */
+    double batch_score_kernel_ms; /* the batch's pw_run_info: score-sweep kernel time */
+    double batch_setup_ms;   /* ... host planning time */
+    double batch_call_ms;    /* ... whole pw_align call */
 } pw_request_info;
 
 typedef struct {

@@ -28,13 +28,15 @@ PW_SERVE_TRACEBACK = 1
 PW_FLAG_SCORE_ONLY = 1
 PW_FLAG_PLAIN = 2
 PW_FLAG_INT32 = 4
+PW_FLAG_NO_CHAIN = 8
+PW_TUNE_CHAIN_MIN = 0
 
 # symbols the header declares, checked by the CPU test-suite
 EXPORTED_SYMBOLS = (
     "pw_create", "pw_destroy", "pw_last_error", "pw_device_free_memory", "pw_set_scoring",
     "pw_set_queries", "pw_set_targets", "pw_align", "pw_get_pair_max", "pw_get_hits",
     "pw_get_starting_points", "pw_last_launch_count", "pw_measure_int_peak", "pw_score_max_noalloc",
-    "pw_set_wave_limit", "pw_server_create", "pw_server_destroy", "pw_server_last_error", "pw_server_set_scoring",
+    "pw_set_wave_limit", "pw_set_tuning", "pw_server_create", "pw_server_destroy", "pw_server_last_error", "pw_server_set_scoring",
     "pw_server_load_db", "pw_server_submit", "pw_server_wait", "pw_server_top_hits", "pw_server_hits",
     "pw_server_release", "pw_server_stats",
 )
@@ -78,7 +80,9 @@ class PwRequestInfo(ctypes.Structure):
     _fields_ = [("status", ctypes.c_int32), ("mode", ctypes.c_int32), ("batch_queries", ctypes.c_int32),
                 ("worker", ctypes.c_int32), ("cells", ctypes.c_int64), ("n_hits", ctypes.c_int64),
                 ("string_bytes", ctypes.c_int64), ("reserved_bytes", ctypes.c_int64), ("queue_ms", ctypes.c_double),
-                ("run_ms", ctypes.c_double), ("latency_ms", ctypes.c_double)]
+                ("run_ms", ctypes.c_double), ("latency_ms", ctypes.c_double),
+                ("batch_score_kernel_ms", ctypes.c_double), ("batch_setup_ms", ctypes.c_double),
+                ("batch_call_ms", ctypes.c_double)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -115,6 +119,7 @@ def bind(lib):
         "pw_score_max_noalloc": (ctypes.c_int, [ctypes.c_int, P, ctypes.c_int, ctypes.c_int, F, F, ctypes.c_int,
                                                 P, P, I32, P, P, I32, P, ctypes.c_char_p, I32]),
         "pw_set_wave_limit": (ctypes.c_int, [P, I64]),
+        "pw_set_tuning": (ctypes.c_int, [P, ctypes.c_int, I64]),
         "pw_server_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, I64,
                                             ctypes.POINTER(ctypes.c_void_p)]),
         "pw_server_destroy": (None, [P]),
@@ -228,10 +233,10 @@ class Engine(object):
                self.lib.pw_set_targets(self.handle, _ptr(buf), _ptr(off), len(seqs), _ptr(keys)), "pw_set_targets")
         self.n_targets = len(seqs)
 
-    def align(self, score_only=False, plain=False, start_cap=-1, int32=False):
+    def align(self, score_only=False, plain=False, start_cap=-1, int32=False, chain=True):
         info = PwRunInfo()
         flags = (PW_FLAG_SCORE_ONLY if score_only else 0) | (PW_FLAG_PLAIN if plain else 0) | \
-            (PW_FLAG_INT32 if int32 else 0)
+            (PW_FLAG_INT32 if int32 else 0) | (0 if chain else PW_FLAG_NO_CHAIN)
         rc = self.lib.pw_align(self.handle, flags, int(start_cap), ctypes.byref(info))
         _check(self.lib, self.handle, rc, "pw_align")
         self.last_info = info
@@ -269,6 +274,9 @@ class Engine(object):
                self.lib.pw_measure_int_peak(self.handle, ctypes.byref(r32), ctypes.byref(r16), ctypes.byref(ms)),
                "pw_measure_int_peak")
         return r32.value, r16.value, ms.value
+
+    def set_tuning(self, key, value):
+        _check(self.lib, self.handle, self.lib.pw_set_tuning(self.handle, int(key), int(value)), "pw_set_tuning")
 
     def set_wave_limit(self, nbytes):
         _check(self.lib, self.handle, self.lib.pw_set_wave_limit(self.handle, int(nbytes)), "pw_set_wave_limit")

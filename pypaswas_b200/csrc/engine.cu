@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstring>
 #include <numeric>
+#include <queue>
 #include <string>
 #include <vector>
 
@@ -23,12 +24,17 @@
 #include "pw_kernels.cuh"
 #include "pw_score16.cuh"
 #include "pw_trace_warp.cuh"
+#include "pw_plan.h"
 
 using namespace pw;
 
 #ifndef PW_LAUNCH
 #define PW_LAUNCH(kern, grid, block, smem, stream, ...) kern<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__)
 #endif
+
+static double wall_ms() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
 
 namespace {
 
@@ -44,12 +50,29 @@ struct DevBuf {
         p = nullptr;
         bytes = 0;
     }
-    cudaError_t reserve(size_t n) {
+    // Stream-ordered growth (cudaFreeAsync / cudaMallocAsync on the engine's
+    // stream, from the device's memory pool, which keeps freed blocks): unlike
+    // cudaFree, nothing here synchronises the device, so a growing buffer
+    // never stalls other engines (the serving loop's workers).  Grows by half
+    // again (small buffers double) so that slightly larger calls reuse it.
+    cudaError_t reserve(cudaStream_t st, size_t n) {
         if (n <= bytes && p) return cudaSuccess;
-        release();
+        if (p) {
+            cudaError_t e = cudaFreeAsync(p, st);
+            if (e != cudaSuccess) return e;
+            p = nullptr;
+            bytes = 0;
+        }
         size_t want = n ? n : 16;
-        cudaError_t e = cudaMalloc(&p, want);
+        want = want < (1u << 20) ? 2 * want : want + want / 2;
+        cudaError_t e = cudaMallocAsync(&p, want, st);
+        if (e == cudaErrorMemoryAllocation) {  // retry at the exact size
+            cudaGetLastError();
+            want = n ? n : 16;
+            e = cudaMallocAsync(&p, want, st);
+        }
         if (e == cudaSuccess) bytes = want;
+        else p = nullptr;
         return e;
     }
     template <typename T>
@@ -107,6 +130,18 @@ struct pw_engine {
     DevBuf t_codes, t_code_off, t_raw, t_raw_off, t_len, t_key;
     DevBuf q_res, t_ccodes, t_order, cmat_t8, cmat_tf;  // the other orientation's encodings
     DevBuf cmat_i8, cmat_f, pair_max, items, items_alt, items_warp, counter, bnd_pool, q_order2;
+    DevBuf chain_items, chain_info, chain_prog, chain_max, chain_ring_off, chain_ring, chain_abort, p1_items;
+    // plan of the 16-bit score phase (work items, classes, chain queue), kept
+    // on the device and reused while inputs, scoring, flags and tuning stay
+    struct {
+        bool valid = false;
+        int64_t qg = 0, tg = 0, sg = 0, tune = 0;
+        uint32_t flags = 0;
+        bool trans = false, chained = false;
+        int begin[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        int xm_multi = 4;
+        int n_chain_items = 0;
+    } p1;
     DevBuf codes, metas, cands, cands_alt, cand_base, cand_cap, n_cand, n_starts, start_off, starts, hits,
         hit_count, ops, allowed;
     // prepared (device-resident) inputs
@@ -114,6 +149,7 @@ struct pw_engine {
     int64_t q_gen = 1, t_gen = 1, s_gen = 1;      // inputs: queries, targets, scoring
     int64_t prep_q[2] = {0, 0}, prep_t[2] = {0, 0};  // (sequence gen, scoring gen) last prepared
     int64_t wave_limit = 0;                          // cell-code bytes per memory wave (0: automatic)
+    int64_t tune[8] = {0, 0, 0, 0, 0, 0, 0, 0};      // pw_set_tuning values (0: automatic)
     // results
     std::vector<float> h_pair_max;
     std::vector<pw_hit> h_hits;
@@ -157,6 +193,12 @@ extern "C" int pw_create(int device, pw_engine** out) {
         return PW_ERR_DEVICE;
     }
     for (auto& ev : e->ev) cudaEventCreate(&ev);
+    // keep freed blocks in the device's pool for reuse (stream-ordered growth)
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     *out = e;
     return PW_OK;
 }
@@ -316,7 +358,7 @@ cudaError_t launch_class(pw_engine* e, int cls, bool affine, const KernelArgs& A
 
 template <typename HT>
 static cudaError_t upload(pw_engine* e, DevBuf& b, const std::vector<HT>& v) {
-    cudaError_t c = b.reserve(std::max<size_t>(v.size() * sizeof(HT), 16));
+    cudaError_t c = b.reserve(e->stream, std::max<size_t>(v.size() * sizeof(HT), 16));
     if (c != cudaSuccess) return c;
     if (v.empty()) return cudaSuccess;
     return cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(HT), cudaMemcpyHostToDevice, e->stream);
@@ -509,7 +551,7 @@ static int prepare(pw_engine* e) {
     pr.s16_q = ints && gaps16;
     pr.s16_t = ints && gaps16 && pr.t_int8;
     cudaError_t c;
-    if ((c = e->counter.reserve(64 * sizeof(int))) != cudaSuccess) return cuda_fail(e, c, "alloc counter");
+    if ((c = e->counter.reserve(e->stream, 64 * sizeof(int))) != cudaSuccess) return cuda_fail(e, c, "alloc counter");
     return PW_OK;
 }
 
@@ -561,7 +603,7 @@ static int run_phase(pw_engine* e, KernelArgs A, const WorkItem* dev_items, cons
         const int64_t slot = (int64_t)xmax_multi4 * kWarp;
         const int64_t warps = (int64_t)e->sm_count * 16 * 4;
         const size_t elem = e->pr.int_path ? sizeof(Bnd<int>) : sizeof(Bnd<float>);
-        c = e->bnd_pool.reserve((size_t)(slot * warps) * elem);
+        c = e->bnd_pool.reserve(e->stream, (size_t)(slot * warps) * elem);
         if (c != cudaSuccess) return cuda_fail(e, c, "alloc boundary pool");
         A.bnd_pool = e->bnd_pool.p;
         A.bnd_slot_elems = slot;
@@ -645,6 +687,73 @@ static cudaError_t launch_s16_class(pw_engine* e, int cls, bool affine, const Sc
     return launch_s16<32, false, true>(e, A);
 }
 
+// Plans the multi-strip launch.  Items whose sweep cost (columns x strips)
+// reaches `min_permille`/1000 of the mean per-warp load are cut into chains of
+// one-strip entries (score16_chain_kernel); the others stay whole.  The queue
+// order comes from a list-scheduling simulation of `warps` equally fast warps:
+// a free warp takes the next strip of the largest chain whose predecessor is
+// at least kChainLead columns ahead, else the next whole item (longest first),
+// else the strip that becomes ready first.  Every strip is queued after its
+// predecessor, which is what the kernel's waits rely on.
+static int setup_chains(pw_engine* e, const std::vector<WorkItem>& items, int i0, int i1,
+                        const std::vector<int32_t>& strip_len, int warps, int* n_entries) {
+    const int n = i1 - i0;
+    std::vector<int> nstr(n);
+    std::vector<int64_t> xm4(n);
+    for (int k = 0; k < n; ++k) {
+        const WorkItem& W = items[i0 + k];
+        const int ls = std::max(strip_len[W.target], W.index >= 0 ? strip_len[W.index] : 0);
+        nstr[k] = (ls + 31) / 32;
+        xm4[k] = align_up(W.xmax, 4);
+    }
+    const int64_t permille = e->tune[PW_TUNE_CHAIN_MIN] > 0 ? e->tune[PW_TUNE_CHAIN_MIN] : 500;
+    ChainPlan plan;
+    plan_chain_queue(nstr, xm4, warps, permille, kChainLead, plan);
+    std::vector<WorkItem> q(plan.queue.size());
+    std::vector<int4> info(plan.queue.size());
+    for (size_t k = 0; k < plan.queue.size(); ++k) {
+        const PlanEntry& p = plan.queue[k];
+        q[k] = items[i0 + p.item];
+        info[k] = make_int4(p.chain, p.strip, p.pred, 0);
+    }
+    std::vector<int64_t> ring_off(std::max<size_t>(plan.chain_xm4.size(), 1), 0);
+    int64_t ring_elems = 0;
+    for (size_t c = 0; c < plan.chain_xm4.size(); ++c) {
+        ring_off[c] = ring_elems;
+        ring_elems += 2 * plan.chain_xm4[c] * kWarp;
+    }
+    cudaError_t c;
+    if ((c = upload(e, e->chain_items, q)) != cudaSuccess) return cuda_fail(e, c, "upload chain items");
+    if ((c = upload(e, e->chain_info, info)) != cudaSuccess) return cuda_fail(e, c, "upload chain info");
+    if ((c = upload(e, e->chain_ring_off, ring_off)) != cudaSuccess) return cuda_fail(e, c, "upload ring offsets");
+    if ((c = e->chain_prog.reserve(e->stream, q.size() * sizeof(int))) != cudaSuccess) return cuda_fail(e, c, "alloc chain progress");
+    if ((c = e->chain_max.reserve(e->stream, q.size() * kWarp * sizeof(uint32_t))) != cudaSuccess)
+        return cuda_fail(e, c, "alloc chain maxima");
+    if ((c = e->chain_ring.reserve(e->stream, (size_t)std::max<int64_t>(ring_elems, 1) * sizeof(uint4))) != cudaSuccess)
+        return cuda_fail(e, c, "alloc chain ring");
+    if ((c = e->chain_abort.reserve(e->stream, sizeof(int))) != cudaSuccess) return cuda_fail(e, c, "alloc chain status");
+    *n_entries = (int)q.size();
+    return PW_OK;
+}
+
+template <int S, bool AFF>
+static cudaError_t launch_s16_chain(pw_engine* e, Score16Args A) {
+    auto kern = score16_chain_kernel<S, AFF>;
+    const int smem = 4 * (S / 4) * A.alpha1 * (int)sizeof(uint4);
+    if (smem > 48 * 1024) {
+        cudaError_t c = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (c != cudaSuccess) return c;
+    }
+    int per_sm = 0;
+    cudaError_t c = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem);
+    if (c != cudaSuccess) return c;
+    per_sm = std::max(1, std::min(per_sm, 16));
+    const int grid = std::max(1, std::min(e->sm_count * per_sm, (A.n_items + 3) / 4));
+    PW_LAUNCH(kern, grid, 128, smem, e->stream, A);
+    e->launches++;
+    return cudaGetLastError();
+}
+
 // Cell-slot cost of an orientation: strips are paired in length order (one
 // pair per 16x2 register), lanes grouped 32 at a time in length order; every
 // work item pays its longer strip times its longest lane for all 64 slots.
@@ -660,55 +769,93 @@ static double orientation_cost(const std::vector<int32_t>& strip_len, const std:
 // Pair maxima with the 16-bit dual-pair sweep.  Returns the device time of
 // the sweep launches in *kernel_ms.  Pairs whose maximum could overflow
 // 16-bit halves come back as NaN; they are recomputed by the 32-bit sweep.
-static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf) {
+static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uint32_t flags) {
     const Prepared& pr = e->pr;
     const int nq = e->Q.n, nt = e->T.n;
-    bool trans = false;
-    if (pr.s16_q && pr.s16_t)
-        trans = orientation_cost(pr.qlen, pr.order, pr.tlen, pr.order_t) <
-                orientation_cost(pr.tlen, pr.order_t, pr.qlen, pr.order);
-    else
-        trans = pr.s16_t;
-    inf.orientation = trans ? 1 : 0;
-    const std::vector<int32_t>& strip_len = trans ? pr.qlen : pr.tlen;
-    const std::vector<int32_t>& strip_order = trans ? pr.order : pr.order_t;
-    const std::vector<int32_t>& lane_len = trans ? pr.tlen : pr.qlen;
-    const std::vector<int32_t>& lane_order = trans ? pr.order_t : pr.order;
-    const int n_strip = trans ? nq : nt, n_lane = trans ? nt : nq;
-    std::vector<WorkItem> items;
-    std::vector<int> cls;
-    std::vector<int64_t> cost;
-    for (int i = 0; i < n_strip; i += 2) {
-        const int sa = strip_order[i], sb = i + 1 < n_strip ? strip_order[i + 1] : -1;
-        const int ls = std::max(strip_len[sa], sb >= 0 ? strip_len[sb] : 0);
-        for (int g = 0; g < n_lane; g += kWarp) {
-            WorkItem w;
-            memset(&w, 0, sizeof(w));
-            w.target = sa;
-            w.index = sb;
-            w.first = g;
-            w.lanes = std::min(kWarp, n_lane - g);
-            w.xmax = lane_len[lane_order[g]];
-            const int k = pick_class(ls, e->affine);
-            w.S = class_S(k);
-            items.push_back(w);
-            cls.push_back(k);
-            cost.push_back((int64_t)w.xmax * ls);
-        }
-    }
-    std::vector<size_t> idx(items.size());
-    std::iota(idx.begin(), idx.end(), 0);
-    std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return cost[a] > cost[b]; });
-    std::vector<WorkItem> it2;
-    std::vector<int> c2;
-    for (size_t k : idx) {
-        it2.push_back(items[k]);
-        c2.push_back(cls[k]);
-    }
-    int begin[kNumClasses + 1];
-    order_by_class(it2, c2, begin);
+    auto& P1 = e->p1;
+    const uint32_t pflags = flags & PW_FLAG_NO_CHAIN;
+    const bool reuse = P1.valid && P1.qg == e->q_gen && P1.tg == e->t_gen && P1.sg == e->s_gen &&
+                       P1.flags == pflags && P1.tune == e->tune[PW_TUNE_CHAIN_MIN];
     cudaError_t c;
-    if ((c = upload(e, e->items, it2)) != cudaSuccess) return cuda_fail(e, c, "upload items");
+    if (!reuse) {
+        const double t_plan = wall_ms();
+        P1.valid = false;
+        bool trans = false;
+        if (pr.s16_q && pr.s16_t)
+            trans = orientation_cost(pr.qlen, pr.order, pr.tlen, pr.order_t) <
+                    orientation_cost(pr.tlen, pr.order_t, pr.qlen, pr.order);
+        else
+            trans = pr.s16_t;
+        const std::vector<int32_t>& strip_len = trans ? pr.qlen : pr.tlen;
+        const std::vector<int32_t>& strip_order = trans ? pr.order : pr.order_t;
+        const std::vector<int32_t>& lane_len = trans ? pr.tlen : pr.qlen;
+        const std::vector<int32_t>& lane_order = trans ? pr.order_t : pr.order;
+        const int n_strip = trans ? nq : nt, n_lane = trans ? nt : nq;
+        std::vector<WorkItem> items;
+        std::vector<int> cls;
+        std::vector<int64_t> cost;
+        for (int i = 0; i < n_strip; i += 2) {
+            const int sa = strip_order[i], sb = i + 1 < n_strip ? strip_order[i + 1] : -1;
+            const int ls = std::max(strip_len[sa], sb >= 0 ? strip_len[sb] : 0);
+            for (int g = 0; g < n_lane; g += kWarp) {
+                WorkItem w;
+                memset(&w, 0, sizeof(w));
+                w.target = sa;
+                w.index = sb;
+                w.first = g;
+                w.lanes = std::min(kWarp, n_lane - g);
+                w.xmax = lane_len[lane_order[g]];
+                const int k = pick_class(ls, e->affine);
+                w.S = class_S(k);
+                items.push_back(w);
+                cls.push_back(k);
+                cost.push_back((int64_t)w.xmax * ls);
+            }
+        }
+        std::vector<size_t> idx(items.size());
+        std::iota(idx.begin(), idx.end(), 0);
+        std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return cost[a] > cost[b]; });
+        std::vector<WorkItem> it2;
+        std::vector<int> c2;
+        it2.reserve(items.size());
+        c2.reserve(items.size());
+        for (size_t k : idx) {
+            it2.push_back(items[k]);
+            c2.push_back(cls[k]);
+        }
+        int begin[kNumClasses + 1];
+        order_by_class(it2, c2, begin);
+        if ((c = upload(e, e->p1_items, it2)) != cudaSuccess) return cuda_fail(e, c, "upload items");
+        int xm = 4;
+        for (int k = begin[kS32Multi]; k < begin[kS32Multi + 1]; ++k) xm = std::max(xm, (int)align_up(it2[k].xmax, 4));
+        P1.chained = !(flags & PW_FLAG_NO_CHAIN) && begin[kS32Multi + 1] > begin[kS32Multi];
+        P1.n_chain_items = 0;
+        if (P1.chained) {
+            int per_sm = 0;
+            const int smem = 4 * 8 * ((trans ? pr.alpha_t : pr.alpha) + 1) * (int)sizeof(uint4);
+            auto kern = e->affine ? score16_chain_kernel<32, true> : score16_chain_kernel<32, false>;
+            if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            if ((c = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem)) != cudaSuccess)
+                return cuda_fail(e, c, "occupancy");
+            const int rc = setup_chains(e, it2, begin[kS32Multi], begin[kS32Multi + 1], strip_len,
+                                        e->sm_count * std::max(1, std::min(per_sm, 16)) * 4, &P1.n_chain_items);
+            if (rc != PW_OK) return rc;
+        }
+        P1.trans = trans;
+        for (int k = 0; k <= kNumClasses; ++k) P1.begin[k] = begin[k];
+        P1.xm_multi = xm;
+        P1.qg = e->q_gen;
+        P1.tg = e->t_gen;
+        P1.sg = e->s_gen;
+        P1.flags = pflags;
+        P1.tune = e->tune[PW_TUNE_CHAIN_MIN];
+        P1.valid = true;
+        inf.setup_ms += wall_ms() - t_plan;
+    }
+    const bool trans = P1.trans;
+    const bool chained = P1.chained;
+    const int* begin = P1.begin;
+    inf.orientation = trans ? 1 : 0;
     Score16Args S;
     memset(&S, 0, sizeof(S));
     S.lane_codes = trans ? e->t_ccodes.as<uint8_t>() : e->q_codes.as<uint8_t>();
@@ -728,16 +875,27 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf) {
     S.stride_strip = trans ? nt : 1;
     S.stride_lane = trans ? 1 : nt;
     if (begin[kS32Multi + 1] > begin[kS32Multi]) {
-        int xm = 4;
-        for (int k = begin[kS32Multi]; k < begin[kS32Multi + 1]; ++k) xm = std::max(xm, (int)align_up(it2[k].xmax, 4));
-        const int64_t slot = (int64_t)xm * kWarp;
-        if ((c = e->bnd_pool.reserve((size_t)slot * e->sm_count * 16 * 4 * sizeof(uint4))) != cudaSuccess)
+        const int64_t slot = (int64_t)P1.xm_multi * kWarp;
+        if ((c = e->bnd_pool.reserve(e->stream, (size_t)slot * e->sm_count * 16 * 4 * sizeof(uint4))) != cudaSuccess)
             return cuda_fail(e, c, "alloc boundary pool");
         S.bnd_pool = e->bnd_pool.as<uint4>();
         S.bnd_slot = slot;
     }
     if ((c = cudaMemsetAsync(e->counter.p, 0, kNumClasses * sizeof(int), e->stream)) != cudaSuccess)
         return cuda_fail(e, c, "reset counters");
+    if (chained) {
+        S.chain = e->chain_info.as<int4>();
+        S.ring_off = e->chain_ring_off.as<int64_t>();
+        S.ring = e->chain_ring.as<uint4>();
+        S.progress = e->chain_prog.as<int>();
+        S.run_max = e->chain_max.as<uint32_t>();
+        S.pad_code = S.alpha1 - 1;
+        S.abort_flag = e->chain_abort.as<int>();
+        S.n_chain_items = P1.n_chain_items;
+        if ((c = cudaMemsetAsync(e->chain_prog.p, 0, (size_t)P1.n_chain_items * sizeof(int), e->stream)) != cudaSuccess ||
+            (c = cudaMemsetAsync(e->chain_abort.p, 0, sizeof(int), e->stream)) != cudaSuccess)
+            return cuda_fail(e, c, "clear chain state");
+    }
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
@@ -745,7 +903,16 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf) {
     for (int k = 0; k < kNumClasses; ++k) {
         const int n = begin[k + 1] - begin[k];
         if (n <= 0) continue;
-        S.items = e->items.as<WorkItem>() + begin[k];
+        if (k == kS32Multi && chained) {
+            S.items = e->chain_items.as<WorkItem>();
+            S.n_items = S.n_chain_items;
+            S.counter = e->counter.as<int>() + k;
+            c = e->affine ? launch_s16_chain<32, true>(e, S) : launch_s16_chain<32, false>(e, S);
+            if (c != cudaSuccess) return cuda_fail(e, c, "score16 chain launch");
+            inf.score_launches++;
+            continue;
+        }
+        S.items = e->p1_items.as<WorkItem>() + begin[k];
         S.n_items = n;
         S.counter = e->counter.as<int>() + k;
         if ((c = launch_s16_class(e, k, e->affine, S)) != cudaSuccess) return cuda_fail(e, c, "score16 launch");
@@ -759,6 +926,12 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf) {
     inf.score_kernel_ms += ms;
     cudaEventDestroy(a);
     cudaEventDestroy(b);
+    if (chained) {
+        int aborted = 0;
+        if ((c = cudaMemcpy(&aborted, e->chain_abort.p, sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess)
+            return cuda_fail(e, c, "read chain status");
+        if (aborted) return fail(e, PW_ERR_KERNEL, "chained score sweep: a strip waited too long for its predecessor");
+    }
 
     // pairs that reached the 16-bit limit: the 32-bit sweep, per target
     std::vector<std::vector<int32_t>> ovf(nt);
@@ -825,7 +998,7 @@ static int run_warp_phase(pw_engine* e, KernelArgs A, const WorkItem* dev_items,
     per_sm = std::max(1, std::min(per_sm, 16));
     const int grid = std::max(1, std::min(e->sm_count * per_sm, (n + 3) / 4));
     const int64_t slot = align_up(std::max(qmax, 1), 4);
-    if ((c = e->bnd_pool.reserve((size_t)slot * grid * 4 * sizeof(int4))) != cudaSuccess)
+    if ((c = e->bnd_pool.reserve(e->stream, (size_t)slot * grid * 4 * sizeof(int4))) != cudaSuccess)
         return cuda_fail(e, c, "alloc boundary pool");
     A.bnd_pool = e->bnd_pool.p;
     A.bnd_slot_elems = slot;
@@ -860,9 +1033,6 @@ static int emit_key_less(const StartRec& a, const StartRec& b) {
     return k(a) < k(b);
 }
 
-static double wall_ms() {
-    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
-}
 
 extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_info* info) {
     if (!e) return PW_ERR_ARG;
@@ -894,7 +1064,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     const std::vector<int32_t>& qlen = pr.qlen;
     const std::vector<int32_t>& tlen = pr.tlen;
     cudaError_t c;
-    if ((c = e->pair_max.reserve((size_t)nq * nt * sizeof(float))) != cudaSuccess)
+    if ((c = e->pair_max.reserve(e->stream, (size_t)nq * nt * sizeof(float))) != cudaSuccess)
         return cuda_fail(e, c, "alloc pair maxima");
     KernelArgs A = base_args(e);
     const bool plain = (flags & PW_FLAG_PLAIN) != 0;
@@ -903,7 +1073,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     const bool use_s16 = !plain && (pr.s16_q || pr.s16_t) && !(flags & PW_FLAG_INT32);
     if (use_s16) {
         cudaEventRecord(e->ev[0], e->stream);
-        rc = phase1_s16(e, A, inf);
+        rc = phase1_s16(e, A, inf, flags);
         if (rc != PW_OK) return rc;
         cudaEventRecord(e->ev[1], e->stream);
         cudaStreamSynchronize(e->stream);
@@ -967,6 +1137,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     }
     if (flags & PW_FLAG_SCORE_ONLY) {
         inf.kernel_launches = (int32_t)e->launches;
+        inf.total_ms = wall_ms() - t_call;
         if (info) *info = inf;
         return PW_OK;
     }
@@ -1086,6 +1257,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     inf.trace_orientation = trans2 ? 1 : 0;
     if (items2.empty()) {
         inf.kernel_launches = (int32_t)e->launches;
+        inf.total_ms = wall_ms() - t_call;
         if (info) *info = inf;
         return PW_OK;
     }
@@ -1106,10 +1278,12 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     const KernelArgs Aref = base_args(e);  // reference-oriented sets for the trace kernels
 
     // memory waves: the cell codes of one wave must fit the budget
-    size_t free_b = 0, total_b = 0;
-    cudaMemGetInfo(&free_b, &total_b);
-    int64_t budget = std::min<int64_t>((int64_t)(free_b * 0.5) + (int64_t)e->codes.bytes, (int64_t)48 << 30);
-    if (e->wave_limit > 0) budget = e->wave_limit;
+    int64_t budget = e->wave_limit;
+    if (budget <= 0) {
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        budget = std::min<int64_t>((int64_t)(free_b * 0.5) + (int64_t)e->codes.bytes, (int64_t)48 << 30);
+    }
     std::vector<std::pair<size_t, size_t>> waves;
     {
         size_t i0 = 0;
@@ -1127,7 +1301,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
 
     double trace_ms = 0, walk_ms = 0;
     int64_t total_starts = 0;
-    inf.setup_ms = wall_ms() - t_setup;
+    inf.setup_ms += wall_ms() - t_setup;
     std::vector<DevHit> all_hits;
     std::vector<char> all_ops;
     for (size_t wv = 0; wv < waves.size(); ++wv) {
@@ -1162,15 +1336,15 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         order_by_class(wi, wc, begin);
         int xm = 4;
         for (int k = begin[kS32Multi]; k < begin[kS32Multi + 1]; ++k) xm = std::max(xm, (int)align_up(wi[k].xmax, 4));
-        if ((c = e->codes.reserve((size_t)dir_off)) != cudaSuccess) return cuda_fail(e, c, "alloc cell codes");
-        if ((c = e->metas.reserve(n_pairs * sizeof(PairMeta))) != cudaSuccess) return cuda_fail(e, c, "alloc metas");
-        if ((c = e->n_cand.reserve(n_pairs * sizeof(int32_t))) != cudaSuccess) return cuda_fail(e, c, "alloc");
-        if ((c = e->n_starts.reserve(n_pairs * sizeof(int32_t))) != cudaSuccess) return cuda_fail(e, c, "alloc");
+        if ((c = e->codes.reserve(e->stream, (size_t)dir_off)) != cudaSuccess) return cuda_fail(e, c, "alloc cell codes");
+        if ((c = e->metas.reserve(e->stream, n_pairs * sizeof(PairMeta))) != cudaSuccess) return cuda_fail(e, c, "alloc metas");
+        if ((c = e->n_cand.reserve(e->stream, n_pairs * sizeof(int32_t))) != cudaSuccess) return cuda_fail(e, c, "alloc");
+        if ((c = e->n_starts.reserve(e->stream, n_pairs * sizeof(int32_t))) != cudaSuccess) return cuda_fail(e, c, "alloc");
         std::vector<int64_t> cbase(n_pairs);
         std::vector<int32_t> ccap(n_pairs, kCandCap);
         for (int64_t p = 0; p < n_pairs; ++p) cbase[p] = p * kCandCap;
         int64_t cand_total = n_pairs * kCandCap;
-        if ((c = e->cands.reserve(cand_total * sizeof(Cand))) != cudaSuccess) return cuda_fail(e, c, "alloc cands");
+        if ((c = e->cands.reserve(e->stream, cand_total * sizeof(Cand))) != cudaSuccess) return cuda_fail(e, c, "alloc cands");
         if ((c = upload(e, e->cand_base, cbase)) != cudaSuccess) return cuda_fail(e, c, "upload cand base");
         if ((c = upload(e, e->cand_cap, ccap)) != cudaSuccess) return cuda_fail(e, c, "upload cand cap");
         if ((c = upload(e, e->items, wi)) != cudaSuccess) return cuda_fail(e, c, "upload items");
@@ -1214,7 +1388,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
             }
         if (extra > 0) {
             DevBuf& nb = e->cands_alt;
-            if ((c = nb.reserve((cand_total + extra) * sizeof(Cand))) != cudaSuccess)
+            if ((c = nb.reserve(e->stream, (cand_total + extra) * sizeof(Cand))) != cudaSuccess)
                 return cuda_fail(e, c, "alloc cands");
             c = cudaMemcpyAsync(nb.p, e->cands.p, cand_total * sizeof(Cand), cudaMemcpyDeviceToDevice, e->stream);
             if (c != cudaSuccess) return cuda_fail(e, c, "copy cands");
@@ -1291,7 +1465,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         std::vector<StartOut> so;
         std::vector<PairMeta> metas;
         if (wave_starts > 0) {
-            if ((c = e->starts.reserve(wave_starts * sizeof(StartOut))) != cudaSuccess) return cuda_fail(e, c, "alloc");
+            if ((c = e->starts.reserve(e->stream, wave_starts * sizeof(StartOut))) != cudaSuccess) return cuda_fail(e, c, "alloc");
             PW_LAUNCH(gather_kernel, gb, tb, 0, e->stream, TA, e->starts.as<StartOut>());
             e->launches++;
             if ((c = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, c, "gather launch");
@@ -1328,8 +1502,8 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         int nh = 0;
         std::vector<DevHit> hh;
         if (wave_starts > 0) {
-            if ((c = e->hits.reserve(wave_starts * sizeof(DevHit))) != cudaSuccess) return cuda_fail(e, c, "alloc hits");
-            if ((c = e->hit_count.reserve(16)) != cudaSuccess) return cuda_fail(e, c, "alloc");
+            if ((c = e->hits.reserve(e->stream, wave_starts * sizeof(DevHit))) != cudaSuccess) return cuda_fail(e, c, "alloc hits");
+            if ((c = e->hit_count.reserve(e->stream, 16)) != cudaSuccess) return cuda_fail(e, c, "alloc");
             cudaMemsetAsync(e->hit_count.p, 0, sizeof(int), e->stream);
             TA.hits = e->hits.as<DevHit>();
             TA.hit_count = e->hit_count.as<int>();
@@ -1353,7 +1527,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         }
         if (nh) {
             if ((c = upload(e, e->hits, hh)) != cudaSuccess) return cuda_fail(e, c, "upload hits");
-            if ((c = e->ops.reserve(std::max<int64_t>(ops_total, 16))) != cudaSuccess) return cuda_fail(e, c, "alloc ops");
+            if ((c = e->ops.reserve(e->stream, std::max<int64_t>(ops_total, 16))) != cudaSuccess) return cuda_fail(e, c, "alloc ops");
             TA.ops = e->ops.as<char>();
             PW_LAUNCH(ops_kernel, (nh + 127) / 128, 128, 0, e->stream, TA, e->hits.as<DevHit>(), nh);
             e->launches++;
@@ -1451,6 +1625,13 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     return PW_OK;
 }
 
+extern "C" int pw_set_tuning(pw_engine* e, int key, int64_t value) {
+    if (!e) return PW_ERR_ARG;
+    if (key < 0 || key >= 8 || value < 0) return fail(e, PW_ERR_ARG, "unknown tuning key or negative value");
+    e->tune[key] = value;
+    return PW_OK;
+}
+
 extern "C" int pw_set_wave_limit(pw_engine* e, int64_t bytes) {
     if (!e) return PW_ERR_ARG;
     if (bytes < 0) return fail(e, PW_ERR_ARG, "wave limit must be >= 0");
@@ -1509,7 +1690,7 @@ extern "C" int pw_measure_int_peak(pw_engine* e, double* ops32, double* ops16x2,
     if (!e || !ops32) return PW_ERR_ARG;
     cudaSetDevice(e->device);
     cudaError_t c;
-    if ((c = e->counter.reserve(64 * sizeof(int))) != cudaSuccess) return cuda_fail(e, c, "alloc");
+    if ((c = e->counter.reserve(e->stream, 64 * sizeof(int))) != cudaSuccess) return cuda_fail(e, c, "alloc");
     const int threads = 256, blocks = e->sm_count * 8, iters = 4096;
     const double instr = (double)blocks * threads * iters * 16.0 * 8.0;
     float ms = 0, ms16 = 0;

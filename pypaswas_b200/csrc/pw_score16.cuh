@@ -47,6 +47,17 @@ struct Score16Args {
     int64_t stride_strip, stride_lane;  // pair_max[strip * stride_strip + lane * stride_lane]
     uint4* bnd_pool;
     int64_t bnd_slot;            // uint4 elements per warp slot (xmax4 * 32)
+    // multi-strip launch with chains (score16_chain_kernel): per queue entry
+    // (chain, strip, queue index of the chain's previous strip); strip -1 marks
+    // a whole item swept by one warp with its boundary in bnd_pool
+    const int4* chain;
+    const int64_t* ring_off;     // per chain: its two boundary rows (xm4 * 32 uint4 each) in `ring`
+    uint4* ring;
+    int* progress;               // per queue entry: columns whose boundary row is written (kChainDone when finished)
+    uint32_t* run_max;           // per queue entry x 32 lanes: running 16x2 maximum of the chain so far
+    int pad_code;                // lane code of the padding residue
+    int* abort_flag;             // set when a wait runs out of time; every waiting warp then gives up
+    int n_chain_items;           // host-side bookkeeping: entries of the chained launch
 };
 
 // Profile of strip rows [y0, y0 + S): for row group g (4 rows) and lane
@@ -172,6 +183,269 @@ __device__ __forceinline__ void sweep16(const uint8_t* qc, int lq4, const uint4*
                 for (int r = 0; r < S; r += 2) mx = __vimax3_s16x2(mx, Bl[r], Bl[r + 1]);
                 if (has_down) bnd[(int64_t)x * kWarp] = make_uint4(mgup, yup, Bl[S - 1], 0u);
             }
+        }
+    }
+}
+
+// ------------------------------------------------------------ chained strips
+// A multi-strip item (two strip sequences against 32 lane sequences) is cut
+// into one item per 32-row strip.  Strip s of a chain runs on whichever warp
+// takes it, a few columns behind strip s - 1: it reads the boundary row that
+// strip s - 1 writes into the chain's ring slot (two rows, alternating), as
+// far as strip s - 1 has published its progress.  So one long item no longer
+// runs on a single warp from its first row to its last.
+//
+// Ordering: the writer stores its boundary values, every lane fences
+// (fence.acq_rel.gpu), the warp synchronises, and lane 0 publishes the column
+// count with st.release.gpu; readers poll with ld.acquire.gpu and read the
+// ring with ld.global.cg (L2, never a stale L1 line).  A ring row is
+// rewritten by strip s + 2 only after strip s + 1 has published progress past
+// those columns, i.e. after it has read them.
+//
+// Progress: entries are handed out in queue order and a strip waits only for
+// its predecessor, which is queued before it and so was taken by a warp that
+// is running; every wait therefore ends.  Each wait is nevertheless bounded:
+// after kChainWaitNs without progress, or when another warp has given up, the
+// warp sets abort_flag and stops, and the host reports the launch as failed.
+// Only the longest items are chained (the host plans the queue so that a
+// strip is handed out about when its predecessor is kChainLead columns
+// ahead); the others run whole on one warp, as in score16_kernel.
+constexpr int kChainDone = 1 << 30;
+// A strip publishes its progress every kChainPublish columns (one fence per
+// lane each time); its successor starts once kChainLead columns are out and
+// afterwards asks for kChainNeed columns beyond its current block, so that in
+// the steady state it runs a publish period or more behind and its polls
+// find the columns already there.
+constexpr int kChainPublish = 32;
+constexpr int kChainLead = 64;
+constexpr int kChainNeed = 40;
+constexpr unsigned long long kChainWaitNs = 2000000000ull;
+
+__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_gpu(int* p, int v) {
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Warp-uniform wait until *flag >= need.  Returns the smallest value the lanes
+// saw (>= need), or -1 when the wait gave up (abort_flag is then set).
+__device__ __forceinline__ int chain_wait(const int* flag, int need, int* abort_flag) {
+    int v = ld_acquire_gpu(flag);
+    if (__all_sync(0xffffffffu, v >= need)) return __reduce_min_sync(0xffffffffu, v);
+    const unsigned long long t0 = global_ns();
+    unsigned ns = 32;
+    for (;;) {
+        __nanosleep(ns);
+        if (ns < 1024) ns <<= 1;
+        v = ld_acquire_gpu(flag);
+        if (__all_sync(0xffffffffu, v >= need)) return __reduce_min_sync(0xffffffffu, v);
+        const bool give_up = ld_acquire_gpu(abort_flag) != 0 || global_ns() - t0 > kChainWaitNs;
+        if (__any_sync(0xffffffffu, give_up)) {
+            if ((threadIdx.x & 31) == 0) atomicExch(abort_flag, 1);
+            return -1;
+        }
+    }
+}
+
+// Publishes `v` as the item's progress after this warp's boundary stores.
+__device__ __forceinline__ void chain_publish(int* flag, int v) {
+    fence_acq_rel_gpu();
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) st_release_gpu(flag, v);
+}
+
+// sweep16 for one strip of a chain.  The column loop runs to the warp's
+// longest lane (xm4, warp-uniform); a lane past its own sequence sweeps
+// padding-code columns, which cannot raise its maximum.  Returns false when a
+// wait gave up.
+template <int S, bool AFFINE>
+__device__ __forceinline__ bool sweep16_chain(const uint8_t* qc, int lq4, int xm4, uint32_t pad4, const uint4* prof,
+                                              int alpha1, int gap, int ext, int ge, bool has_up, bool has_down,
+                                              const uint4* ring_in, uint4* ring_out, const int* prog_in,
+                                              int* prog_out, int* abort_flag, uint32_t& mx) {
+    const uint32_t g2 = pack16(gap), e2 = pack16(ext), ge2 = pack16(ge), nge2 = pack16(-ge);
+    int avail = 0;  // columns of the predecessor known to be published
+    auto need_cols = [&](int upto) -> bool {  // columns [0, upto) of ring_in readable
+        if (!has_up || avail >= upto) return true;
+        avail = chain_wait(prog_in, upto, abort_flag);
+        return avail >= 0;
+    };
+    auto code_word = [&](int x4) -> uint32_t { return x4 < lq4 ? *(const uint32_t*)(qc + x4) : pad4; };
+    if (!need_cols(min(kChainLead, xm4))) return false;
+    if constexpr (!AFFINE) {
+        uint32_t H[S];
+#pragma unroll
+        for (int r = 0; r < S; ++r) H[r] = 0;
+        uint32_t hb_prev = 0;
+        uint32_t cw_next = xm4 > 0 ? code_word(0) : pad4;
+        uint32_t up_next = has_up && xm4 > 0 ? __ldcg(&ring_in[0]).x : 0u;
+        for (int x4 = 0; x4 < xm4; x4 += 4) {
+            if (!need_cols(min(x4 + kChainNeed, xm4))) return false;
+            const uint32_t cw = cw_next;
+            if (x4 + 4 < xm4) cw_next = code_word(x4 + 4);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int x = x4 + j;
+                const int a = (cw >> (8 * j)) & 0xff;
+                uint32_t up = up_next;
+                if (has_up && x + 1 < xm4) up_next = __ldcg(&ring_in[(int64_t)(x + 1) * kWarp]).x;
+                uint32_t diag = hb_prev;
+                hb_prev = up;
+#pragma unroll
+                for (int g = 0; g < S / 4; ++g) {
+                    const uint4 w4 = prof[g * alpha1 + a];
+                    const uint32_t sc[4] = {w4.x, w4.y, w4.z, w4.w};
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const int r = 4 * g + k;
+                        const uint32_t left = H[r];
+                        uint32_t t = __viaddmax_s16x2(diag, sc[k], kNeg16x2);
+                        t = __viaddmax_s16x2(left, g2, t);
+                        const uint32_t h = __viaddmax_s16x2_relu(up, g2, t);
+                        diag = left;
+                        H[r] = h;
+                        up = h;
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < S; r += 2) mx = __vimax3_s16x2(mx, H[r], H[r + 1]);
+                if (has_down) __stcg(&ring_out[(int64_t)x * kWarp], make_uint4(H[S - 1], 0u, 0u, 0u));
+            }
+            if (has_down && (((x4 + 4) % kChainPublish) == 0 || x4 + 4 >= xm4)) chain_publish(prog_out, x4 + 4);
+        }
+    } else {
+        uint32_t Mgl[S], Xl[S], Bl[S];
+#pragma unroll
+        for (int r = 0; r < S; ++r) {
+            Mgl[r] = ge2;
+            Xl[r] = kNeg16x2;
+            Bl[r] = 0;
+        }
+        uint32_t bb_prev = 0;
+        uint32_t cw_next = xm4 > 0 ? code_word(0) : pad4;
+        uint4 v_next = has_up && xm4 > 0 ? __ldcg(&ring_in[0]) : make_uint4(ge2, kNeg16x2, 0u, 0u);
+        for (int x4 = 0; x4 < xm4; x4 += 4) {
+            if (!need_cols(min(x4 + kChainNeed, xm4))) return false;
+            const uint32_t cw = cw_next;
+            if (x4 + 4 < xm4) cw_next = code_word(x4 + 4);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int x = x4 + j;
+                const int a = (cw >> (8 * j)) & 0xff;
+                const uint4 v = v_next;
+                if (has_up && x + 1 < xm4) v_next = __ldcg(&ring_in[(int64_t)(x + 1) * kWarp]);
+                uint32_t mgup = v.x, yup = v.y, bup = v.z;
+                uint32_t bdiag = bb_prev;
+                bb_prev = bup;
+#pragma unroll
+                for (int g = 0; g < S / 4; ++g) {
+                    const uint4 w4 = prof[g * alpha1 + a];
+                    const uint32_t sc[4] = {w4.x, w4.y, w4.z, w4.w};
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const int r = 4 * g + k;
+                        const uint32_t mg = __viaddmax_s16x2(bdiag, sc[k], ge2);
+                        const uint32_t y = __viaddmax_s16x2(yup, e2, mgup);
+                        const uint32_t xg = __viaddmax_s16x2(Xl[r], e2, Mgl[r]);
+                        const uint32_t bst = __vimax3_s16x2(__viaddmax_s16x2(mg, nge2, kNeg16x2), y, xg);
+                        bdiag = Bl[r];
+                        Mgl[r] = mg;
+                        Xl[r] = xg;
+                        Bl[r] = bst;
+                        mgup = mg;
+                        yup = y;
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < S; r += 2) mx = __vimax3_s16x2(mx, Bl[r], Bl[r + 1]);
+                if (has_down) __stcg(&ring_out[(int64_t)x * kWarp], make_uint4(mgup, yup, Bl[S - 1], 0u));
+            }
+            if (has_down && (((x4 + 4) % kChainPublish) == 0 || x4 + 4 >= xm4)) chain_publish(prog_out, x4 + 4);
+        }
+    }
+    return true;
+}
+
+template <int S, bool AFFINE>
+__global__ void __launch_bounds__(128, 3) score16_chain_kernel(Score16Args A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    uint4* prof = (uint4*)smem + wib * ((S / 4) * A.alpha1);
+    const int shift = AFFINE ? A.ge : 0;
+    const uint32_t pad4 = (uint32_t)A.pad_code * 0x01010101u;
+    const int64_t warp_global = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
+    uint4* bnd = A.bnd_pool + warp_global * A.bnd_slot + lane;
+    for (;;) {
+        int it = 0;
+        if (lane == 0) it = atomicAdd(A.counter, 1);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it >= A.n_items) break;
+        const WorkItem W = A.items[it];
+        const int4 ci = A.chain[it];
+        const int c = ci.x, s = ci.y, pred = ci.z;
+        const int sa = W.target, sb = W.index;
+        const int la = A.strip_len[sa];
+        const int lb = sb >= 0 ? A.strip_len[sb] : 0;
+        const int ls = la > lb ? la : lb;
+        const int nstrips = (ls + S - 1) / S;
+        const bool active = lane < W.lanes;
+        const int p = active ? A.lane_order[W.first + lane] : 0;
+        const uint8_t* qc = A.lane_codes + A.lane_off[p];
+        const int lq4 = active ? (A.lane_len[p] + 3) & ~3 : 0;
+        const uint8_t* ra = A.strip_res + A.strip_off[sa];
+        const uint8_t* rb = A.strip_res + A.strip_off[sb >= 0 ? sb : sa];
+        uint32_t mx = 0;
+        bool finished = true;
+        if (s < 0) {
+            // a whole item on this warp, strip after strip
+            for (int st = 0; st < nstrips; ++st) {
+                __syncwarp();
+                build_profile16<S>(prof, A.cmat, ra, rb, st * S, la, lb, A.alpha1, A.dim, shift, lane);
+                __syncwarp();
+                if (active)
+                    sweep16<S, AFFINE>(qc, lq4, prof, A.alpha1, A.gap, A.ext, A.ge, st > 0, st + 1 < nstrips, bnd, mx);
+            }
+        } else {
+            const int xm4 = (W.xmax + 3) & ~3;
+            const int64_t row = (int64_t)xm4 * kWarp;
+            const uint4* ring_in = A.ring + A.ring_off[c] + ((s + 1) & 1) * row + lane;
+            uint4* ring_out = A.ring + A.ring_off[c] + (s & 1) * row + lane;
+            __syncwarp();
+            build_profile16<S>(prof, A.cmat, ra, rb, s * S, la, lb, A.alpha1, A.dim, shift, lane);
+            __syncwarp();
+            const bool has_down = s + 1 < nstrips;
+            if (!sweep16_chain<S, AFFINE>(qc, lq4, xm4, pad4, prof, A.alpha1, A.gap, A.ext, A.ge, s > 0, has_down,
+                                          ring_in, ring_out, s > 0 ? A.progress + pred : nullptr, A.progress + it,
+                                          A.abort_flag, mx))
+                break;
+            if (s > 0) {
+                // the predecessor's running maximum is final once it has finished
+                if (chain_wait(A.progress + pred, kChainDone, A.abort_flag) < 0) break;
+                mx = __vmaxs2(mx, __ldcg(&A.run_max[(int64_t)pred * kWarp + lane]));
+            }
+            if (has_down) {
+                __stcg(&A.run_max[(int64_t)it * kWarp + lane], mx);
+                chain_publish(A.progress + it, kChainDone);
+                finished = false;
+            }
+        }
+        if (finished && active) {
+            const int ma = (int)(int16_t)(mx & 0xffffu), mb = (int)(int16_t)(mx >> 16);
+            A.pair_max[(int64_t)sa * A.stride_strip + (int64_t)p * A.stride_lane] =
+                ma >= kOvf16 ? __int_as_float(0x7fc00000) : (float)ma;
+            if (sb >= 0)
+                A.pair_max[(int64_t)sb * A.stride_strip + (int64_t)p * A.stride_lane] =
+                    mb >= kOvf16 ? __int_as_float(0x7fc00000) : (float)mb;
         }
     }
 }

@@ -47,6 +47,7 @@ struct Request {
     std::string error;
     int32_t batch_queries = 0, worker = -1;
     int64_t cells = 0, reserved = 0;
+    double score_kernel_ms = 0, setup_ms = 0, call_ms = 0;
     std::vector<int32_t> top_targets;
     std::vector<float> top_scores;
     std::vector<pw_hit> hits;
@@ -165,6 +166,9 @@ void run_batch(pw_server* s, int w, pw_engine* e, std::vector<Request*>& batch, 
         r->worker = w;
         r->cells = (int64_t)r->residues.size() * s->db_residues;
         r->reserved = mode == PW_SERVE_TRACEBACK ? reserve : 0;
+        r->score_kernel_ms = info.score_kernel_ms;
+        r->setup_ms = info.setup_ms;
+        r->call_ms = info.total_ms;
         if (rc != PW_OK) continue;
         if (mode == PW_SERVE_TOP) {
             const float* row = pmax.data() + (size_t)i * s->db_n;
@@ -331,6 +335,23 @@ extern "C" int pw_server_load_db(pw_server* s, const uint8_t* residues, const in
         if (rc == PW_OK) rc = pw_align(w.engine, PW_FLAG_SCORE_ONLY, -1, &info);
         if (rc != PW_OK) return server_fail(s, rc, pw_last_error(w.engine));
     }
+    // warm-up: one full-size batch per worker and mode (database sequences as
+    // queries, so the traceback run walks their self-alignments), so that the
+    // engines' device buffers have grown before the first request arrives
+    {
+        const int m = std::min<int>(s->max_batch, n);
+        std::vector<int64_t> woff(m + 1, 0);
+        for (int i = 0; i < m; ++i) woff[i + 1] = woff[i] + (offsets[i + 1] - offsets[i]);
+        std::vector<int32_t> wkey(m, -1);
+        for (Worker& w : s->workers) {
+            int rc = pw_set_queries(w.engine, residues, woff.data(), m, wkey.data());
+            pw_run_info info;
+            if (rc == PW_OK) rc = pw_align(w.engine, PW_FLAG_SCORE_ONLY, -1, &info);
+            if (rc == PW_OK) rc = pw_set_wave_limit(w.engine, std::min<int64_t>(s->budget, (int64_t)1 << 30));
+            if (rc == PW_OK) rc = pw_align(w.engine, 0u, -1, &info);
+            if (rc != PW_OK) return server_fail(s, rc, pw_last_error(w.engine));
+        }
+    }
     {
         std::lock_guard<std::mutex> g(s->mu);
         s->db_n = n;
@@ -399,6 +420,9 @@ extern "C" int pw_server_wait(pw_server* s, int64_t ticket, int32_t timeout_ms, 
         info->queue_ms = r->t_admit - r->t_submit;
         info->run_ms = r->t_done - r->t_admit;
         info->latency_ms = r->t_done - r->t_submit;
+        info->batch_score_kernel_ms = r->score_kernel_ms;
+        info->batch_setup_ms = r->setup_ms;
+        info->batch_call_ms = r->call_ms;
     }
     if (r->status != PW_OK) s->err = r->error;
     return r->status;

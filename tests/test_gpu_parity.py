@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 import cases
-from engine_helpers import run_engine
+from engine_helpers import configure, run_engine
 
 pytestmark = pytest.mark.gpu
 
@@ -172,3 +172,38 @@ def test_many_short_targets_strip_direction_sweep(engine_lib, oracle_mod, aff):
     assert info.traced_pairs >= 148 * 32 and info.warp_pairs == 0
     np.testing.assert_array_equal(pm, o["pair_max"])
     assert hits == o["hits"]
+
+
+@pytest.mark.parametrize("kind", ["dna", "protein", "protein_linear"])
+@pytest.mark.parametrize("chain_min", [0, 1])
+def test_chained_strips_match_one_warp_items_and_oracle(engine_lib, oracle_mod, kind, chain_min):
+    """Multi-strip items cut into chained strips (the default share, and with
+    chain_min 1 nearly every multi-strip item) give the same pair maxima as
+    the one-warp items and the oracle, in both lane orientations."""
+    from pypaswas_b200 import _native, scores
+    rng = np.random.default_rng({"dna": 5, "protein": 6, "protein_linear": 7}[kind] * 10 + chain_min)
+    alphabet = cases.DNA if kind == "dna" else cases.PROTEIN
+    for nq, nt in ((14, 40), (40, 14)):
+        q = ["".join(alphabet[i] for i in rng.integers(0, len(alphabet), int(n)))
+             for n in rng.integers(33, 300, nq)]
+        t = ["".join(alphabet[i] for i in rng.integers(0, len(alphabet), int(n)))
+             for n in rng.integers(20, 260, nt)]
+        q[0] = t[0][10:120] + q[0]  # a shared segment
+        st = cases.Settings(gap_extension="-1" if kind in ("dna", "protein") else "0", minimum_score="5",
+                            **({} if kind == "dna" else dict(matrix_name="BLOSUM62", gap_score="-11")))
+        score = scores.make_score(st)
+        ref = oracle_mod.pair_max(cases.oracle_params(oracle_mod, score), q, t)
+        e = _native.Engine(0, lib=engine_lib)
+        try:
+            configure(e, score, st)
+            e.set_queries([s.encode() for s in q], np.arange(nq))
+            e.set_targets([s.encode() for s in t], np.arange(nt) + nq)
+            e.set_tuning(_native.PW_TUNE_CHAIN_MIN, chain_min)
+            e.align(score_only=True)
+            chained = e.pair_max()
+            e.align(score_only=True, chain=False)
+            single = e.pair_max()
+        finally:
+            e.close()
+        np.testing.assert_array_equal(chained, ref)
+        np.testing.assert_array_equal(single, ref)
