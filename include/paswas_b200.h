@@ -141,6 +141,17 @@ int pw_set_targets(pw_engine* e, const uint8_t* residues, const int64_t* offsets
  * walked, chosen in emission order (SmithWaterman.py:683-685). */
 int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_info* info);
 
+/* Restricts pw_align to explicit (query, target) pairs instead of every query
+ * against every target; n = 0 restores all-vs-all.  Indices refer to the
+ * lists of pw_set_queries / pw_set_targets (checked by pw_align).  The
+ * reference always aligns all-vs-all (SmithWaterman.align_sequences,
+ * SmithWaterman.py:441-560); a caller who runs it once per pair, one query
+ * and one target file each, gets exactly the hits of these pairs.  With
+ * integer scores every listed pair is swept one warp per 256-row band, the
+ * bands of a pair chained across warps (long pairs use the whole GPU).
+ * pw_get_pair_max then holds -1 for the pairs that are not listed. */
+int pw_set_pairs(pw_engine* e, const int32_t* query_idx, const int32_t* target_idx, int64_t n);
+
 /* Upper bound, in bytes, on the direction-matrix (cell code) memory of one
  * memory wave of pw_align; 0 restores the automatic choice (half of the free
  * device memory, at most 48 GiB).  Traced pairs beyond the bound run in

@@ -36,7 +36,7 @@ EXPORTED_SYMBOLS = (
     "pw_create", "pw_destroy", "pw_last_error", "pw_device_free_memory", "pw_set_scoring",
     "pw_set_queries", "pw_set_targets", "pw_align", "pw_get_pair_max", "pw_get_hits",
     "pw_get_starting_points", "pw_last_launch_count", "pw_measure_int_peak", "pw_score_max_noalloc",
-    "pw_set_wave_limit", "pw_set_tuning", "pw_server_create", "pw_server_destroy", "pw_server_last_error", "pw_server_set_scoring",
+    "pw_set_wave_limit", "pw_set_tuning", "pw_set_pairs", "pw_server_create", "pw_server_destroy", "pw_server_last_error", "pw_server_set_scoring",
     "pw_server_load_db", "pw_server_submit", "pw_server_wait", "pw_server_top_hits", "pw_server_hits",
     "pw_server_release", "pw_server_stats",
 )
@@ -120,6 +120,7 @@ def bind(lib):
                                                 P, P, I32, P, P, I32, P, ctypes.c_char_p, I32]),
         "pw_set_wave_limit": (ctypes.c_int, [P, I64]),
         "pw_set_tuning": (ctypes.c_int, [P, ctypes.c_int, I64]),
+        "pw_set_pairs": (ctypes.c_int, [P, P, P, I64]),
         "pw_server_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, I64,
                                             ctypes.POINTER(ctypes.c_void_p)]),
         "pw_server_destroy": (None, [P]),
@@ -274,6 +275,15 @@ class Engine(object):
                self.lib.pw_measure_int_peak(self.handle, ctypes.byref(r32), ctypes.byref(r16), ctypes.byref(ms)),
                "pw_measure_int_peak")
         return r32.value, r16.value, ms.value
+
+    def set_pairs(self, query_idx, target_idx):
+        """Explicit (query, target) pairs for the next align() calls; empty lists restore all-vs-all."""
+        qi = np.ascontiguousarray(query_idx, dtype=np.int32)
+        ti = np.ascontiguousarray(target_idx, dtype=np.int32)
+        if qi.shape != ti.shape:
+            raise InvalidOptionException("query and target index lists differ in length")
+        self._pairs = (qi, ti)
+        _check(self.lib, self.handle, self.lib.pw_set_pairs(self.handle, _ptr(qi), _ptr(ti), len(qi)), "pw_set_pairs")
 
     def set_tuning(self, key, value):
         _check(self.lib, self.handle, self.lib.pw_set_tuning(self.handle, int(key), int(value)), "pw_set_tuning")

@@ -23,7 +23,7 @@
 #include "../../include/paswas_b200.h"
 #include "pw_kernels.cuh"
 #include "pw_score16.cuh"
-#include "pw_trace_warp.cuh"
+#include "pw_band.cuh"
 #include "pw_plan.h"
 
 using namespace pw;
@@ -129,7 +129,8 @@ struct pw_engine {
     DevBuf q_codes, q_code_off, q_raw, q_raw_off, q_len, q_key, q_order;
     DevBuf t_codes, t_code_off, t_raw, t_raw_off, t_len, t_key;
     DevBuf q_res, t_ccodes, t_order, cmat_t8, cmat_tf;  // the other orientation's encodings
-    DevBuf cmat_i8, cmat_f, pair_max, items, items_alt, items_warp, counter, bnd_pool, q_order2;
+    DevBuf cmat_i8, cmat_f, pair_max, items, items_alt, counter, bnd_pool, q_order2;
+    DevBuf band_pairs, band_entries, band_prog, band_max, band_ring, band_out;  // band sweep (pw_band.cuh)
     DevBuf chain_items, chain_info, chain_prog, chain_max, chain_ring_off, chain_ring, chain_abort, p1_items;
     // plan of the 16-bit score phase (work items, classes, chain queue), kept
     // on the device and reused while inputs, scoring, flags and tuning stay
@@ -149,6 +150,7 @@ struct pw_engine {
     int64_t q_gen = 1, t_gen = 1, s_gen = 1;      // inputs: queries, targets, scoring
     int64_t prep_q[2] = {0, 0}, prep_t[2] = {0, 0};  // (sequence gen, scoring gen) last prepared
     int64_t wave_limit = 0;                          // cell-code bytes per memory wave (0: automatic)
+    std::vector<int32_t> pair_q, pair_t;             // pw_set_pairs: explicit (query, target) pairs
     int64_t tune[8] = {0, 0, 0, 0, 0, 0, 0, 0};      // pw_set_tuning values (0: automatic)
     // results
     std::vector<float> h_pair_max;
@@ -979,50 +981,116 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uin
 }
 
 
-// Direction sweep with one warp per pair (pw_trace_warp.cuh) over n items.
-static int run_warp_phase(pw_engine* e, KernelArgs A, const WorkItem* dev_items, int n, int qmax, double* kernel_ms,
+// Launches band_kernel over `pairs` (one warp per band, the bands of a pair
+// chained across warps, pw_band.cuh).  DIRS: the direction sweep of traced
+// pairs; otherwise pair maxima into band_max (indexed by BandPair.slot).
+template <bool DIRS>
+static int run_band_phase(pw_engine* e, KernelArgs A, std::vector<BandPair>& pairs, double* kernel_ms,
                           int* n_launch) {
-    if (n <= 0) return PW_OK;
-    const int qmax16 = (int)align_up(std::max(qmax, 1), 16);
+    if (pairs.empty()) return PW_OK;
     const int prof_bytes = (int)align_up((int64_t)kWarp * (A.P.alpha + 1) * kWarpRows, 16);
-    const int smem = 4 * (prof_bytes + qmax16);
-    if (smem > 227 * 1024) return fail(e, PW_ERR_CAPACITY, "query too long for the warp direction sweep");
-    auto kern = e->affine ? dir_warp_kernel<true> : dir_warp_kernel<false>;
+    const int smem = 4 * prof_bytes;
+    auto kern = e->affine ? band_kernel<true, DIRS> : band_kernel<false, DIRS>;
     cudaError_t c;
     if (smem > 48 * 1024 &&
         (c = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
-        return cuda_fail(e, c, "warp sweep smem");
+        return cuda_fail(e, c, "band sweep smem");
     int per_sm = 0;
     if ((c = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem)) != cudaSuccess)
         return cuda_fail(e, c, "occupancy");
     per_sm = std::max(1, std::min(per_sm, 16));
-    const int grid = std::max(1, std::min(e->sm_count * per_sm, (n + 3) / 4));
-    const int64_t slot = align_up(std::max(qmax, 1), 4);
-    if ((c = e->bnd_pool.reserve(e->stream, (size_t)slot * grid * 4 * sizeof(int4))) != cudaSuccess)
-        return cuda_fail(e, c, "alloc boundary pool");
-    A.bnd_pool = e->bnd_pool.p;
-    A.bnd_slot_elems = slot;
-    A.items = dev_items;
-    A.n_items = n;
-    A.item_counter = e->counter.as<int>() + kNumClasses;
-    if ((c = cudaMemsetAsync(A.item_counter, 0, sizeof(int), e->stream)) != cudaSuccess)
-        return cuda_fail(e, c, "reset counter");
+    const int warps = e->sm_count * per_sm * 4;
+    // queue: the bands of each pair form a chain (pw_plan.h), longest pairs first
+    std::vector<int> order(pairs.size());
+    std::iota(order.begin(), order.end(), 0);
+    std::vector<int64_t> steps(pairs.size());
+    for (size_t k = 0; k < pairs.size(); ++k) {
+        pairs[k].nbands = std::max(1, pairs[k].nbands);
+        steps[k] = (int64_t)e->pr.qlen[pairs[k].q] + kWarp - 1;
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        return steps[x] * pairs[x].nbands > steps[y] * pairs[y].nbands;
+    });
+    std::vector<BandPair> sorted(pairs.size());
+    std::vector<int> nstr(pairs.size());
+    std::vector<int64_t> xm(pairs.size());
+    int64_t ring_elems = 0;
+    for (size_t k = 0; k < order.size(); ++k) {
+        sorted[k] = pairs[order[k]];
+        nstr[k] = sorted[k].nbands;
+        xm[k] = steps[order[k]];
+        sorted[k].ring_off = ring_elems;
+        if (sorted[k].nbands > 1) ring_elems += 2 * (int64_t)e->pr.qlen[sorted[k].q];
+    }
+    ChainPlan plan;
+    plan_chain_queue(nstr, xm, warps, 1, kBandLead, plan);
+    std::vector<int4> entries(plan.queue.size());
+    for (size_t k = 0; k < plan.queue.size(); ++k) {
+        const PlanEntry& p = plan.queue[k];
+        entries[k] = make_int4(p.item, p.chain >= 0 ? p.strip : 0, p.pred, 0);
+    }
+    const size_t n = entries.size();
+    if ((c = upload(e, e->band_pairs, sorted)) != cudaSuccess) return cuda_fail(e, c, "upload band pairs");
+    if ((c = upload(e, e->band_entries, entries)) != cudaSuccess) return cuda_fail(e, c, "upload band queue");
+    if ((c = e->band_prog.reserve(e->stream, n * sizeof(int))) != cudaSuccess ||
+        (c = e->band_max.reserve(e->stream, n * sizeof(int))) != cudaSuccess ||
+        (c = e->band_ring.reserve(e->stream, (size_t)std::max<int64_t>(ring_elems, 1) * sizeof(int4))) != cudaSuccess ||
+        (c = e->chain_abort.reserve(e->stream, sizeof(int))) != cudaSuccess)
+        return cuda_fail(e, c, "alloc band state");
+    if ((c = cudaMemsetAsync(e->band_prog.p, 0, n * sizeof(int), e->stream)) != cudaSuccess ||
+        (c = cudaMemsetAsync(e->chain_abort.p, 0, sizeof(int), e->stream)) != cudaSuccess ||
+        (c = cudaMemsetAsync(e->counter.as<int>() + kNumClasses, 0, sizeof(int), e->stream)) != cudaSuccess)
+        return cuda_fail(e, c, "reset band state");
+    BandArgs B;
+    memset(&B, 0, sizeof(B));
+    B.entries = e->band_entries.as<int4>();
+    B.pairs = e->band_pairs.as<BandPair>();
+    B.n_entries = (int)n;
+    B.counter = e->counter.as<int>() + kNumClasses;
+    B.ring = e->band_ring.as<int4>();
+    B.progress = e->band_prog.as<int>();
+    B.run_max = e->band_max.as<int>();
+    B.abort_flag = e->chain_abort.as<int>();
+    B.max_out = e->band_out.as<float>();
+    const int grid = std::max(1, std::min(e->sm_count * per_sm, (int)((n + 3) / 4)));
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
     cudaEventRecord(a, e->stream);
-    PW_LAUNCH(kern, grid, 128, smem, e->stream, A, qmax16);
+    PW_LAUNCH(kern, grid, 128, smem, e->stream, A, B);
     e->launches++;
     cudaEventRecord(b, e->stream);
-    if ((c = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, c, "warp sweep launch");
-    if ((c = cudaStreamSynchronize(e->stream)) != cudaSuccess) return cuda_fail(e, c, "warp sweep");
+    if ((c = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, c, "band sweep launch");
+    int aborted = 0;
+    if ((c = cudaMemcpyAsync(&aborted, e->chain_abort.p, sizeof(int), cudaMemcpyDeviceToHost, e->stream)) != cudaSuccess ||
+        (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
+        return cuda_fail(e, c, "band sweep");
     float ms = 0;
     cudaEventElapsedTime(&ms, a, b);
     if (kernel_ms) *kernel_ms += ms;
     if (n_launch) ++*n_launch;
     cudaEventDestroy(a);
     cudaEventDestroy(b);
+    if (aborted) return fail(e, PW_ERR_KERNEL, "band sweep: a band waited too long for the band above");
     return PW_OK;
+}
+
+// The phase-2 warp items as band pairs.
+static std::vector<BandPair> band_pairs_of(pw_engine* e, const std::vector<WorkItem>& items) {
+    std::vector<BandPair> v(items.size());
+    for (size_t k = 0; k < items.size(); ++k) {
+        const WorkItem& W = items[k];
+        BandPair& p = v[k];
+        memset(&p, 0, sizeof(p));
+        p.q = W.first;
+        p.t = W.target;
+        const int lt = e->pr.tlen[W.target];
+        p.nbands = lt > 0 ? (lt + kBandRows - 1) / kBandRows : 1;
+        p.meta_item = W.index;
+        p.dir_base = W.dir_base;
+        p.slot = W.pair_base;
+    }
+    return v;
 }
 
 static int emit_key_less(const StartRec& a, const StartRec& b) {
@@ -1054,6 +1122,17 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     for (int i = 0; i < nq; ++i) sumq += e->Q.off[i + 1] - e->Q.off[i];
     for (int i = 0; i < nt; ++i) sumt += e->T.off[i + 1] - e->T.off[i];
     inf.cells = sumq * sumt;
+    const bool pair_mode = !e->pair_q.empty();
+    if (pair_mode) {
+        inf.pairs = (int64_t)e->pair_q.size();
+        inf.cells = 0;
+        for (size_t k = 0; k < e->pair_q.size(); ++k) {
+            if (e->pair_q[k] < 0 || e->pair_q[k] >= nq || e->pair_t[k] < 0 || e->pair_t[k] >= nt)
+                return fail(e, PW_ERR_ARG, "pair list index outside the query or target list");
+            inf.cells += (e->Q.off[e->pair_q[k] + 1] - e->Q.off[e->pair_q[k]]) *
+                         (e->T.off[e->pair_t[k] + 1] - e->T.off[e->pair_t[k]]);
+        }
+    }
     if (nq == 0 || nt == 0) {
         if (info) *info = inf;
         return PW_OK;
@@ -1070,8 +1149,33 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     const bool plain = (flags & PW_FLAG_PLAIN) != 0;
 
     // ---------------------------------------------------------- phase 1
-    const bool use_s16 = !plain && (pr.s16_q || pr.s16_t) && !(flags & PW_FLAG_INT32);
-    if (use_s16) {
+    const bool band1 = pair_mode && pr.int_path;
+    const bool use_s16 = !band1 && !plain && (pr.s16_q || pr.s16_t) && !(flags & PW_FLAG_INT32);
+    if (band1) {
+        // explicit pairs: one warp per 256-row band, bands chained (pw_band.cuh)
+        const size_t np = e->pair_q.size();
+        std::vector<BandPair> bp(np);
+        for (size_t k = 0; k < np; ++k) {
+            memset(&bp[k], 0, sizeof(BandPair));
+            bp[k].q = e->pair_q[k];
+            bp[k].t = e->pair_t[k];
+            const int lt = tlen[bp[k].t];
+            bp[k].nbands = lt > 0 ? (lt + kBandRows - 1) / kBandRows : 1;
+            bp[k].slot = (int64_t)k;
+        }
+        if ((c = e->band_out.reserve(e->stream, np * sizeof(float))) != cudaSuccess)
+            return cuda_fail(e, c, "alloc band maxima");
+        cudaEventRecord(e->ev[0], e->stream);
+        rc = run_band_phase<false>(e, A, bp, &inf.score_kernel_ms, &inf.score_launches);
+        if (rc != PW_OK) return rc;
+        cudaEventRecord(e->ev[1], e->stream);
+        std::vector<float> bm;
+        if ((c = download(e, bm, e->band_out.p, np)) != cudaSuccess) return cuda_fail(e, c, "copy pair maxima");
+        for (size_t k = 0; k < np; ++k) e->h_pair_max[(size_t)e->pair_q[k] * nt + e->pair_t[k]] = bm[k];
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e->ev[0], e->ev[1]);
+        inf.score_ms = ms;
+    } else if (use_s16) {
         cudaEventRecord(e->ev[0], e->stream);
         rc = phase1_s16(e, A, inf, flags);
         if (rc != PW_OK) return rc;
@@ -1135,6 +1239,17 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         cudaEventElapsedTime(&ms, e->ev[0], e->ev[1]);
         inf.score_ms = ms;
     }
+    if (pair_mode) {
+        // pairs outside the list get -1: below MINIMUM_SCORE, never traced
+        std::vector<uint8_t> listed((size_t)nq * nt, 0);
+        for (size_t k = 0; k < e->pair_q.size(); ++k) listed[(size_t)e->pair_q[k] * nt + e->pair_t[k]] = 1;
+        for (size_t k = 0; k < listed.size(); ++k)
+            if (!listed[k]) e->h_pair_max[k] = -1.0f;
+        if ((c = cudaMemcpyAsync(A.pair_max, e->h_pair_max.data(), e->h_pair_max.size() * sizeof(float),
+                                 cudaMemcpyHostToDevice, e->stream)) != cudaSuccess ||
+            (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
+            return cuda_fail(e, c, "upload pair maxima");
+    }
     if (flags & PW_FLAG_SCORE_ONLY) {
         inf.kernel_launches = (int32_t)e->launches;
         inf.total_ms = wall_ms() - t_call;
@@ -1171,7 +1286,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         }
     }
     // Traced pairs with targets longer than one register strip go to the
-    // one-warp-per-pair sweep (pw_trace_warp.cuh); the others are grouped 32 to
+    // one-warp-per-pair sweep (pw_band.cuh); the others are grouped 32 to
     // a warp, one pair per lane, in the orientation where they cluster
     // (slot cost = strip length x longest lane x 32 per item).
     const bool warp_ok = pr.int_path && !plain;
@@ -1348,7 +1463,6 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         if ((c = upload(e, e->cand_base, cbase)) != cudaSuccess) return cuda_fail(e, c, "upload cand base");
         if ((c = upload(e, e->cand_cap, ccap)) != cudaSuccess) return cuda_fail(e, c, "upload cand cap");
         if ((c = upload(e, e->items, wi)) != cudaSuccess) return cuda_fail(e, c, "upload items");
-        if (!ww.empty() && (c = upload(e, e->items_warp, ww)) != cudaSuccess) return cuda_fail(e, c, "upload items");
         A.codes = e->codes.as<uint8_t>();
         A.metas = e->metas.as<PairMeta>();
         A.cands = e->cands.as<Cand>();
@@ -1370,9 +1484,11 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
                               trans2);
             if (rc != PW_OK) return rc;
         }
-        rc = run_warp_phase(e, Aw, e->items_warp.as<WorkItem>(), (int)ww.size(), qmax_warp, &inf.trace_kernel_ms,
-                            &inf.trace_launches);
-        if (rc != PW_OK) return rc;
+        {
+            std::vector<BandPair> bp = band_pairs_of(e, ww);
+            rc = run_band_phase<true>(e, Aw, bp, &inf.trace_kernel_ms, &inf.trace_launches);
+            if (rc != PW_OK) return rc;
+        }
         // candidate overflow: pairs with more candidates than their slot get an
         // exact slot past the regular ones, and their items are swept again
         std::vector<int32_t> ncand;
@@ -1425,9 +1541,8 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
                 if (rc != PW_OK) return rc;
             }
             if (!rw.empty()) {
-                if ((c = upload(e, e->items_warp, rw)) != cudaSuccess) return cuda_fail(e, c, "upload items");
-                rc = run_warp_phase(e, Aw, e->items_warp.as<WorkItem>(), (int)rw.size(), qmax_warp,
-                                    &inf.trace_kernel_ms, &inf.trace_launches);
+                std::vector<BandPair> bp = band_pairs_of(e, rw);
+                rc = run_band_phase<true>(e, Aw, bp, &inf.trace_kernel_ms, &inf.trace_launches);
                 if (rc != PW_OK) return rc;
             }
         }
@@ -1622,6 +1737,14 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     inf.finish_ms = wall_ms() - t_finish;
     inf.total_ms = wall_ms() - t_call;
     if (info) *info = inf;
+    return PW_OK;
+}
+
+extern "C" int pw_set_pairs(pw_engine* e, const int32_t* query_idx, const int32_t* target_idx, int64_t n) {
+    if (!e) return PW_ERR_ARG;
+    if (n < 0 || (n > 0 && (!query_idx || !target_idx))) return fail(e, PW_ERR_ARG, "bad pair list");
+    e->pair_q.assign(query_idx, query_idx + n);
+    e->pair_t.assign(target_idx, target_idx + n);
     return PW_OK;
 }
 

@@ -1,0 +1,324 @@
+// pw_band.cuh -- one pair per warp, its 256-row bands chained across warps.
+//
+// The 32 lanes of a warp share one (query, target) pair: lane l owns target
+// rows [y0 + 8l, y0 + 8l + 8) of a 256-row band and the warp walks the query
+// columns as a skewed wavefront (lane l works on column s - l at step s).  The
+// values lane l needs from the row above its slice -- computed one step
+// earlier by lane l - 1 -- arrive through __shfl_up_sync; lane 0 reads them
+// from the boundary row that the band above stored (lane 31's bottom row).
+//
+// Each band is a queue entry of its own, so the bands of one long pair run on
+// different warps at the same time, each a publish period or more behind the
+// band above: the band's lane 31 stores its bottom row into the pair's ring
+// (two rows, alternating by band parity) and publishes every 32 steps how many
+// columns are stored (st.release.gpu, by the storing thread itself); the band
+// below polls that count (ld.acquire.gpu, bounded wait) and reads the ring
+// with ld.global.cg.  A ring row is rewritten by band b + 2 only after band
+// b + 1 has published progress past those columns, which it does only after
+// its lane 0 has read them.  The queue is planned like the chained strips
+// (pw_plan.h): every band after the band above it.
+//
+// DIRS = false: pair maxima only (the score sweep of long pairs).
+// DIRS = true: the direction sweep of traced pairs: per cell the code byte of
+// the reference's classification (direction, stop flag, candidate flag) and
+// the pair's candidate list, exactly as the strip sweep computes them; cell
+// codes are stored [band][step][lane][8 rows] (warp_layout_offset).
+#pragma once
+#include "pw_kernels.cuh"
+#include "pw_score16.cuh"
+
+namespace pw {
+
+constexpr int kWarpRows = 8;                   // rows per lane
+constexpr int kBandRows = kWarpRows * kWarp;   // 256 rows per band
+constexpr int kBandLead = 128;                 // planning lead between bands (steps)
+
+static_assert(kBandRows == 256 && kWarpRows == 8, "warp_layout_offset (pw_kernels.cuh) assumes 8 x 32 rows");
+
+__host__ __device__ __forceinline__ int64_t warp_code_bytes(int lq, int lt) {
+    const int64_t bands = lt > 0 ? (lt + kBandRows - 1) / kBandRows : 1;
+    return bands * ((int64_t)lq + kWarp - 1) * kWarp * kWarpRows;
+}
+
+struct BandPair {
+    int32_t q, t;        // query / target index (reference orientation)
+    int32_t nbands;
+    int32_t meta_item;   // DIRS: value for PairMeta.item (the pair's work item in the wave)
+    int64_t ring_off;    // int4 offset of the pair's two boundary rows (2 x lq)
+    int64_t dir_base;    // DIRS: byte offset of the pair's cell codes
+    int64_t slot;        // DIRS: pair slot (metas, candidates); score sweep: pair_max index
+};
+
+struct BandArgs {
+    const int4* entries;  // per queue entry: (pair, band, queue index of the band above, 0)
+    const BandPair* pairs;
+    int n_entries;
+    int* counter;
+    int4* ring;
+    int* progress;        // per entry: columns of the bottom row stored (kChainDone when finished)
+    int* run_max;         // per entry: running maximum of the pair's bands so far
+    int* abort_flag;
+    float* max_out;       // score sweep: pair maxima, indexed by BandPair.slot
+};
+
+template <bool AFFINE, bool DIRS>
+__global__ void __launch_bounds__(128) band_kernel(KernelArgs A, BandArgs B) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int alpha1 = A.P.alpha + 1;
+    const int prof_bytes = ((kWarp * alpha1 * kWarpRows) + 15) & ~15;
+    uint2* prof = (uint2*)(smem + wib * prof_bytes);  // [lane][alpha1] -> 8 int8 scores of that lane's rows
+    const int gap = A.P.gap_i, ext = A.P.ext_i, ge = A.P.ge_i;
+    const int neg = kNeg;
+
+    for (;;) {
+        int it = 0;
+        if (lane == 0) it = atomicAdd(B.counter, 1);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it >= B.n_entries) break;
+        const int4 en = B.entries[it];
+        const BandPair BP = B.pairs[en.x];
+        const int band = en.y, pred = en.z;
+        const int q = BP.q, t = BP.t;
+        const int lq = A.q.len[q], lt = A.t.len[t];
+        const int nbands = BP.nbands;
+        int thr = 0;
+        Cand* cand = nullptr;
+        int cap = 0;
+        int* ncand = nullptr;
+        uint8_t* codes = nullptr;
+        if constexpr (DIRS) {
+            // threshold of the pair (default_main.cu:609, SmithWatermanCuda.py:269-275)
+            const float maxf = A.pair_max[(int64_t)q * A.pm_lane + (int64_t)t * A.pm_strip];
+            const int mn = lq < lt ? lq : lt;
+            const float pos = (float)(A.P.highest * (double)mn * A.P.filter_factor);
+            const float thf = fmaxf(__fmul_rn(A.P.lower_limit, maxf), pos);
+            thr = (int)fminf(fmaxf(ceilf(thf), -1.0e9f), 1.0e9f);
+            if (band == 0 && lane == 0) {
+                PairMeta& pm = A.metas[BP.slot];
+                pm.query = q;
+                pm.target = t;
+                pm.item = BP.meta_item;
+                pm.lane = 0;
+                pm.thr_f = thf;
+                pm.thr_i = thr;
+                pm.max_f = maxf;
+            }
+            cand = A.cands + A.cand_base[BP.slot];
+            cap = A.cand_cap[BP.slot];
+            ncand = A.n_cand + BP.slot;
+            codes = A.codes + BP.dir_base;
+        }
+        const uint8_t* qg = A.q.codes + A.q.code_off[q];
+        const uint8_t* tres = A.t.codes + A.t.code_off[t];
+        const int64_t nsteps = (int64_t)lq + kWarp - 1;
+        const int yb = band * kBandRows;
+        __syncwarp();
+        for (int idx = lane; idx < kWarp * alpha1; idx += kWarp) {
+            const int ll = idx / alpha1, a = idx % alpha1;
+            uint32_t w0 = 0, w1 = 0;
+#pragma unroll
+            for (int r = 0; r < kWarpRows; ++r) {
+                const int y = yb + ll * kWarpRows + r;
+                const int8_t sc = y < lt ? A.cmat_i8[a * A.P.dim + tres[y]] : (int8_t)-128;
+                if (r < 4)
+                    w0 |= (uint32_t)(uint8_t)sc << (8 * r);
+                else
+                    w1 |= (uint32_t)(uint8_t)sc << (8 * (r - 4));
+            }
+            prof[idx] = make_uint2(w0, w1);
+        }
+        __syncwarp();
+        const bool has_up = band > 0;
+        const bool store_bnd = band + 1 < nbands;
+        const int4* ring_in = B.ring + BP.ring_off + (int64_t)((band + 1) & 1) * lq;
+        int4* ring_out = B.ring + BP.ring_off + (int64_t)(band & 1) * lq;
+        const int* prog_in = B.progress + pred;
+        int* prog_out = B.progress + it;
+        const int ymine = yb + lane * kWarpRows;
+        int Hl[kWarpRows], Ml[kWarpRows], Jl[kWarpRows], Bl[kWarpRows];
+#pragma unroll
+        for (int r = 0; r < kWarpRows; ++r) {
+            Hl[r] = 0;
+            Ml[r] = 0;
+            Jl[r] = neg;
+            Bl[r] = 0;
+        }
+        int up_h = 0, up_m = 0, up_i = neg, up_b = 0;
+        int dg_h = 0, dg_m = 0, dg_b = 0;
+        int bt_h = 0, bt_m = 0, bt_i = neg, bt_b = 0;
+        int mx = 0;
+        int avail = 0;
+        bool ok = true;
+        for (int64_t s = 0; s < nsteps; ++s) {
+            if (has_up && (s & 31) == 0) {
+                const int need = (int)(s + 32 < (int64_t)lq ? s + 32 : (int64_t)lq);
+                if (avail < need) {
+                    avail = chain_wait(prog_in, need, B.abort_flag);
+                    if (avail < 0) {
+                        ok = false;
+                        break;
+                    }
+                }
+            }
+            const int x = (int)s - lane;
+            const bool active = x >= 0 && x < lq;
+            int rh = 0, rm = 0, ri = neg, rb = 0;
+            if constexpr (AFFINE) {
+                rm = __shfl_up_sync(0xffffffffu, bt_m, 1);
+                ri = __shfl_up_sync(0xffffffffu, bt_i, 1);
+                rb = __shfl_up_sync(0xffffffffu, bt_b, 1);
+            } else {
+                rh = __shfl_up_sync(0xffffffffu, bt_h, 1);
+            }
+            if (lane == 0) {
+                if (has_up && active) {
+                    const int4 v = __ldcg(&ring_in[x]);
+                    rh = v.x;
+                    rm = v.x;
+                    ri = v.y;
+                    rb = v.z;
+                } else {
+                    rh = 0;
+                    rm = 0;
+                    ri = neg;
+                    rb = 0;
+                }
+            }
+            dg_h = x == 0 ? 0 : up_h;
+            dg_m = x == 0 ? 0 : up_m;
+            dg_b = x == 0 ? 0 : up_b;
+            up_h = rh;
+            up_m = rm;
+            up_i = ri;
+            up_b = rb;
+            if (active) {
+                const int a = __ldg(qg + x);
+                const uint2 pw = prof[lane * alpha1 + a];
+                const bool xin = x > 0;
+                uint32_t w0 = 0, w1 = 0;
+                if constexpr (!AFFINE) {
+                    int up = up_h, diag = dg_h;
+#pragma unroll
+                    for (int r = 0; r < kWarpRows; ++r) {
+                        const int sc = (int)(int8_t)(uint8_t)((r < 4 ? pw.x : pw.y) >> (8 * (r & 3)));
+                        const int left = Hl[r];
+                        int h = addmax(left, gap, diag + sc);
+                        h = addmax_relu(up, gap, h);
+                        if constexpr (DIRS) {
+                            const int ls = left + gap, us = up + gap;
+                            uint32_t code = h == ls ? kLeft : (h == us ? kUp : kUL);
+                            code = h > 0 ? code : kNo;
+                            const int y = ymine + r;
+                            const bool ul = code == kUL;
+                            const bool stop = ul && xin && y > 0 && diag == 0;
+                            code |= stop ? kStopFlag : 0u;
+                            if (ul && h >= thr && y < lt) {
+                                code |= kCand;
+                                const int k = atomicAdd(ncand, 1);
+                                if (k < cap) {
+                                    Cand cc;
+                                    cc.x = x;
+                                    cc.y = y;
+                                    cc.score_i = h;
+                                    cc.score_f = (float)h;
+                                    cand[k] = cc;
+                                }
+                            }
+                            if (r < 4)
+                                w0 |= code << (8 * r);
+                            else
+                                w1 |= code << (8 * (r - 4));
+                        } else {
+                            mx = max(mx, h);
+                        }
+                        diag = left;
+                        Hl[r] = h;
+                        up = h;
+                    }
+                    bt_h = up;
+                } else {
+                    int mup = up_m, iup = up_i, bdiag = dg_b, mdiag = dg_m;
+#pragma unroll
+                    for (int r = 0; r < kWarpRows; ++r) {
+                        const int sc = (int)(int8_t)(uint8_t)((r < 4 ? pw.x : pw.y) >> (8 * (r & 3)));
+                        const int m = addmax_relu(bdiag, sc, neg);
+                        const int i = addmax(iup, ext, mup + ge);
+                        const int jj = addmax(Jl[r], ext, Ml[r] + ge);
+                        const int b = max3(m, i, jj);
+                        if constexpr (DIRS) {
+                            uint32_t code = b == m ? kUL : (b == i ? kUp : kLeft);
+                            code = b > 0 ? code : kNo;
+                            const int y = ymine + r;
+                            const bool main_src = code == kUL;
+                            const bool stop = main_src && xin && y > 0 && mdiag == 0;
+                            code |= stop ? kStopFlag : 0u;
+                            if (main_src && m >= thr && y < lt) {
+                                code |= kCand;
+                                const int k = atomicAdd(ncand, 1);
+                                if (k < cap) {
+                                    Cand cc;
+                                    cc.x = x;
+                                    cc.y = y;
+                                    cc.score_i = m;
+                                    cc.score_f = (float)m;
+                                    cand[k] = cc;
+                                }
+                            }
+                            if (r < 4)
+                                w0 |= code << (8 * r);
+                            else
+                                w1 |= code << (8 * (r - 4));
+                        } else {
+                            mx = max(mx, b);
+                        }
+                        bdiag = Bl[r];
+                        mdiag = Ml[r];
+                        Ml[r] = m;
+                        Jl[r] = jj;
+                        Bl[r] = b;
+                        mup = m;
+                        iup = i;
+                    }
+                    bt_m = mup;
+                    bt_i = iup;
+                    bt_b = Bl[kWarpRows - 1];
+                }
+                if constexpr (DIRS)
+                    *(uint2*)(codes + ((band * nsteps + s) * kWarp + lane) * kWarpRows) = make_uint2(w0, w1);
+                if (lane == kWarp - 1 && store_bnd) __stcg(&ring_out[x], make_int4(AFFINE ? bt_m : bt_h, bt_i, bt_b, 0));
+            } else {
+                // not started (x < 0): hand the left-boundary values down
+                bt_h = 0;
+                bt_m = 0;
+                bt_i = neg;
+                bt_b = 0;
+            }
+            // lane 31 stored columns 0 .. s - 31 of the bottom row
+            if (store_bnd && lane == kWarp - 1 && ((s + 1) & 31) == 0 && s >= kWarp - 1)
+                st_release_gpu(prog_out, (int)(s - (kWarp - 2)));
+        }
+        if (!ok) break;
+        if (store_bnd && lane == kWarp - 1) st_release_gpu(prog_out, lq);
+        // pair maximum (score sweep) / candidate count (direction sweep)
+        if constexpr (!DIRS) mx = __reduce_max_sync(0xffffffffu, mx);
+        if (has_up) {
+            // the band above has finished: its running maximum and its candidates are final
+            if (chain_wait(prog_in, kChainDone, B.abort_flag) < 0) break;
+            if constexpr (!DIRS) mx = max(mx, __ldcg(&B.run_max[pred]));
+        }
+        if (store_bnd) {
+            if constexpr (!DIRS)
+                if (lane == 0) __stcg(&B.run_max[it], mx);
+            chain_publish(prog_out, kChainDone);
+        } else if (lane == 0) {
+            if constexpr (DIRS)
+                A.metas[BP.slot].n_cand = atomicAdd(ncand, 0);
+            else
+                B.max_out[BP.slot] = (float)mx;
+        }
+    }
+}
+
+}  // namespace pw

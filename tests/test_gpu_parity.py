@@ -207,3 +207,63 @@ def test_chained_strips_match_one_warp_items_and_oracle(engine_lib, oracle_mod, 
             e.close()
         np.testing.assert_array_equal(chained, ref)
         np.testing.assert_array_equal(single, ref)
+
+
+def _oracle_pairs(oracle_mod, queries, targets, pairs, score, st):
+    """Oracle hits and maxima of explicit pairs, one pair at a time."""
+    p = cases.oracle_params(oracle_mod, score)
+    hits, maxima = {}, {}
+    for qi, ti in pairs:
+        q, t = queries[qi], targets[ti]
+        pos = cases.pos_scores(score, st, [q], [t])
+        o = oracle_mod.run(p, [q], [t], pos, float(st.minimum_score))
+        maxima[(qi, ti)] = float(o["pair_max"][0, 0])
+        hits[(qi, ti)] = [dict(h, query=qi, target=ti) for h in o["hits"]]
+    return hits, maxima
+
+
+@pytest.mark.parametrize("affine", ["0", "-1"])
+def test_pair_list_long_pairs_bands_chained(engine_lib, oracle_mod, affine):
+    """Explicit pairs, long ones swept band by band on different warps (score
+    and direction sweeps), against the oracle pair by pair."""
+    from pypaswas_b200 import _native, scores
+    rng = np.random.default_rng(42 if affine == "0" else 43)
+
+    def rs(n):
+        return "".join("ACGT"[i] for i in rng.integers(0, 4, n))
+    queries, targets = [], []
+    for lq, lt in ((2600, 2200), (700, 1900), (1800, 300), (40, 1200), (900, 900), (257, 513)):
+        shared = rs(min(lq, lt) // 2)
+        mut = "".join(c if rng.random() > 0.12 else "ACGT"[int(rng.integers(0, 4))] for c in shared)
+        a = int(rng.integers(0, lq - len(shared) + 1))
+        b = int(rng.integers(0, lt - len(shared) + 1))
+        q = rs(lq)
+        t = rs(lt)
+        queries.append(q[:a] + shared + q[a + len(shared):])
+        targets.append(t[:b] + mut + t[b + len(mut):])
+    pairs = [(k, k) for k in range(len(queries))] + [(0, 1), (3, 0)]
+    st = cases.Settings(gap_extension=affine, minimum_score="20", lower_limit_score="0.9", filter_factor="0.02")
+    score = scores.make_score(st)
+    ref_hits, ref_max = _oracle_pairs(oracle_mod, queries, targets, pairs, score, st)
+    e = _native.Engine(0, lib=engine_lib)
+    try:
+        configure(e, score, st)
+        e.set_queries([s.encode() for s in queries], np.arange(len(queries)))
+        e.set_targets([s.encode() for s in targets], np.arange(len(targets)) + len(queries))
+        e.set_pairs([p[0] for p in pairs], [p[1] for p in pairs])
+        info = e.align()
+        pm = e.pair_max()
+        from engine_helpers import decode_hits
+        got = decode_hits(*e.hits())
+    finally:
+        e.close()
+    assert info.pairs == len(pairs)
+    for (qi, ti), m in ref_max.items():
+        assert pm[qi, ti] == m
+    listed = set(pairs)
+    assert all(pm[i, j] == -1.0 for i in range(len(queries)) for j in range(len(targets)) if (i, j) not in listed)
+    by_pair = {}
+    for h in got:
+        by_pair.setdefault((h["query"], h["target"]), []).append(h)
+    assert {k: v for k, v in by_pair.items()} == {k: v for k, v in ref_hits.items() if v}
+    assert sum(len(v) for v in ref_hits.values()) >= 4
