@@ -42,6 +42,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", type=int, choices=[1, 2, 3], default=2,
+                    help="workload: 1 DNA reads x adapters, 2 protein batched (the metric's configuration), "
+                         "3 long DNA pairs")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--targets", type=int, default=0,
@@ -58,6 +61,10 @@ def parse():
 
 def workload(args):
     from pypaswas_b200 import workloads
+    if args.config == 1:
+        return workloads.config1()
+    if args.config == 3:
+        return workloads.config3()
     w = workloads.config2()
     if args.targets and args.targets < len(w.targets):
         step = len(w.targets) // args.targets
@@ -156,38 +163,52 @@ def engine_for(workload, device):
     qk, tk = id_keys([i for i, _ in workload.queries], [i for i, _ in workload.targets])
     e.set_queries([s for _, s in workload.queries], qk)
     e.set_targets([s for _, s in workload.targets], tk)
+    if workload.pairs is not None:
+        e.set_pairs([p[0] for p in workload.pairs], [p[1] for p in workload.pairs])
     return e, score
 
 
 def cpu_baseline(workload, score, seconds, processes=1):
     """The oracle (CPU restatement of the reference path) on a bounded sample of
-    the workload: queries x targets taken evenly from the length-sorted lists,
-    grown until the estimated run time reaches `seconds`."""
+    the workload: queries x targets taken evenly from the length-sorted lists
+    (or, with explicit pairs, the first pairs), grown until the estimated run
+    time reaches `seconds`."""
     import multiprocessing as mp
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle
     oracle.build()
     q_all = [s.decode() for _, s in workload.queries]
     t_all = [s.decode() for _, s in workload.targets]
-    rate = 24e6 * max(1, processes)  # cells/s estimate of the oracle, refined below
-    nq = min(len(q_all), 10)
-    nt = max(1, int(seconds * rate / (sum(map(len, q_all[::max(1, len(q_all) // nq)][:nq])) * 1025)))
-    nt = min(nt, len(t_all))
-    qs = q_all[::max(1, len(q_all) // nq)][:nq]
-    ts = t_all[::max(1, len(t_all) // nt)][:nt]
-    cells = sum(map(len, qs)) * sum(map(len, ts))
+    rate = 24e6 * max(1, processes)  # cells/s estimate of the oracle
     args = _oracle_args(score, workload.settings)
+    if workload.pairs is not None:
+        jobs, cells = [], 0
+        for qi, ti in workload.pairs:
+            if cells and cells + len(q_all[qi]) * len(t_all[ti]) > seconds * rate:
+                break
+            jobs.append((args, [q_all[qi]], [t_all[ti]]))
+            cells += len(q_all[qi]) * len(t_all[ti])
+        sample = "the first %d explicit pairs (%d cells) of the same workload, full path" % (len(jobs), cells)
+    else:
+        nq = min(len(q_all), 10)
+        nt = max(1, int(seconds * rate / (sum(map(len, q_all[::max(1, len(q_all) // nq)][:nq])) * 1025)))
+        nt = min(nt, len(t_all))
+        qs = q_all[::max(1, len(q_all) // nq)][:nq]
+        ts = t_all[::max(1, len(t_all) // nt)][:nt]
+        cells = sum(map(len, qs)) * sum(map(len, ts))
+        jobs = [(args, qs, ts[i::processes]) for i in range(max(1, processes))]
+        jobs = [j for j in jobs if j[2]]
+        sample = "%d queries x %d targets (%d cells) of the same workload, full path" % (len(qs), len(ts), cells)
     t0 = time.time()
     if processes <= 1:
-        _oracle_chunk((args, qs, ts))
+        for j in jobs:
+            _oracle_chunk(j)
     else:
-        chunks = [ts[i::processes] for i in range(processes)]
         ctx = mp.get_context("spawn")
         with ctx.Pool(processes) as pool:
-            pool.map(_oracle_chunk, [(args, qs, c) for c in chunks if c])
+            pool.map(_oracle_chunk, jobs)
     dt = time.time() - t0
-    return {"value": cells / dt / 1e9, "unit": "GCUPS", "cores": processes, "kind": "port",
-            "sample": "%d queries x %d targets (%d cells) of the same workload, full path" % (len(qs), len(ts), cells),
+    return {"value": cells / dt / 1e9, "unit": "GCUPS", "cores": processes, "kind": "port", "sample": sample,
             "seconds": dt}
 
 
@@ -282,6 +303,7 @@ def main():
         torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
         t_ms = float(tt.item())
     value = world * cells * args.steps / (t_ms * 1e-3) / 1e9
+    n_pairs = len(w.pairs) if w.pairs is not None else len(w.queries) * len(w.targets)
     ms_per_step = t_ms / args.steps
 
     # roofline of the dominant kernel (integer-ALU bound)
@@ -293,8 +315,9 @@ def main():
             i["trace_launches"] for i in infos)
         ops = sum(i["traced_cells"] for i in infos) * OPS_PER_CELL[(mode, "dirs")]
     else:
-        dom, dom_ms, dom_launch = "score sweep (score16_kernel, 16x2 lanes)" if _sixteen_bit(e, w) else \
-            "score sweep (sweep_kernel phase 1)", score_ms, sum(
+        dom, dom_ms, dom_launch = "score sweep (score16_chain_kernel, 16x2 lanes)" if _sixteen_bit(e, w) else \
+            ("score sweep (band_kernel, bands chained across warps)" if e.last_info.score_path == 2 else
+             "score sweep (sweep_kernel phase 1)"), score_ms, sum(
             i["score_launches"] for i in infos)
         ops = cells * OPS_PER_CELL[(mode, "score")] * args.steps
     peak32, peak16, _ = e.measure_int_peak()
@@ -310,8 +333,8 @@ def main():
     out = {"metric": "GCUPS", "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-           "config": {"workload": "%s (%d pairs, full path)" % (w.name, len(w.queries) * len(w.targets)),
-                      "pairs": len(w.queries) * len(w.targets),
+           "config": {"workload": "%s (%d pairs, full path)" % (w.name, n_pairs),
+                      "pairs": n_pairs,
                       "cells_per_step": cells, "traced_pairs": last["traced_pairs"],
                       "starting_points": last["starting_points"], "hits": last["hits"],
                       "score_lanes": "targets" if last["orientation"] else "queries",
@@ -334,9 +357,9 @@ def main():
                         "traffic": traffic,
                         "hbm_gbs_measured": load_peaks().get("hbm_gbs")},
            "e2e": {"value": e2e_value, "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}}
-    if not args.no_plain:
+    if not args.no_plain and w.pairs is None:
         out["plain"] = plain_vs_batched(w, local, value)
-    if not args.no_serve and rank == 0:
+    if not args.no_serve and rank == 0 and args.config == 2:
         out["serve"] = serve_leg(local, args.serve_seconds, [float(x) for x in args.serve_loads.split(",")])
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(w, score, args.cpu_seconds, processes=1)
@@ -420,7 +443,7 @@ def serve_leg(device, seconds, loads, workers=2, max_batch=32):
 def _sixteen_bit(engine, w):
     """The score sweep ran on 16-bit lanes (integer scores; see pw_score16.cuh)."""
     return engine.last_info is not None and engine.last_info.score_launches > 0 and \
-        engine.last_info.overflow_pairs == 0 and _integer_scores(w)
+        engine.last_info.score_path == 0 and engine.last_info.overflow_pairs == 0 and _integer_scores(w)
 
 
 def _integer_scores(w):
@@ -430,22 +453,36 @@ def _integer_scores(w):
 
 
 def _e2e(w, steps, device):
-    """Public driver path: Aligner.process on host records -> HitList."""
+    """Public driver path: Aligner.process on host records -> HitList.  With
+    explicit pairs (long DNA), one process() call per query against its
+    targets, as the reference would be run once per pair."""
     import torch
     from pypaswas_b200.programs import Aligner
     from pypaswas_b200.records import SeqRecord
     queries = [SeqRecord(s, i) for i, s in w.queries]
     targets = [SeqRecord(s, i) for i, s in w.targets]
+    if w.pairs is None:
+        calls = [(queries, targets)]
+    else:
+        per_q = {}
+        for qi, ti in w.pairs:
+            per_q.setdefault(qi, []).append(targets[ti])
+        calls = [([queries[qi]], ts) for qi, ts in sorted(per_q.items())]
     aligner = Aligner(None, None, w.settings, device=device)
-    aligner.process(queries, targets, None)  # warm-up
+    for qs, ts in calls[:2]:
+        aligner.process(qs, ts, None)  # warm-up
     torch.cuda.synchronize()
+    h2d = d2h = 0
     t0 = time.perf_counter()
     for _ in range(steps):
-        aligner.process(queries, targets, None)
+        h2d = d2h = 0
+        for qs, ts in calls:
+            aligner.process(qs, ts, None)
+            h2d += int(aligner.smith_waterman.last_h2d_bytes)
+            d2h += int(aligner.smith_waterman.last_d2h_bytes)
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
-    sw = aligner.smith_waterman
-    return w.cells * steps / dt / 1e9, int(sw.last_h2d_bytes), int(sw.last_d2h_bytes)
+    return w.cells * steps / dt / 1e9, h2d, d2h
 
 
 if __name__ == "__main__":

@@ -79,6 +79,9 @@ typedef struct {
     double setup_ms;        /* host wall time between the phases: pruning, work lists, memory waves */
     double finish_ms;       /* host wall time after the device work: hit order, alignment strings */
     double total_ms;        /* host wall time of the whole call */
+    int32_t score_path;     /* score sweep used: 0 16-bit strips, 1 32-bit / fp32 strips, 2 bands (pw_set_pairs
+                               or few long sequences) */
+    int32_t reserved_;
 } pw_run_info;
 
 /* Creates an engine on CUDA device `device`.

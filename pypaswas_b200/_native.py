@@ -70,7 +70,8 @@ class PwRunInfo(ctypes.Structure):
                 ("orientation", ctypes.c_int32), ("trace_orientation", ctypes.c_int32),
                 ("overflow_pairs", ctypes.c_int64), ("traced_cells", ctypes.c_int64),
                 ("warp_pairs", ctypes.c_int64), ("cand_overflow_pairs", ctypes.c_int64),
-                ("setup_ms", ctypes.c_double), ("finish_ms", ctypes.c_double), ("total_ms", ctypes.c_double)]
+                ("setup_ms", ctypes.c_double), ("finish_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
+                ("score_path", ctypes.c_int32), ("reserved_", ctypes.c_int32)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

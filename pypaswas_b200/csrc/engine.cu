@@ -1122,7 +1122,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     for (int i = 0; i < nq; ++i) sumq += e->Q.off[i + 1] - e->Q.off[i];
     for (int i = 0; i < nt; ++i) sumt += e->T.off[i + 1] - e->T.off[i];
     inf.cells = sumq * sumt;
-    const bool pair_mode = !e->pair_q.empty();
+    bool pair_mode = !e->pair_q.empty();
     if (pair_mode) {
         inf.pairs = (int64_t)e->pair_q.size();
         inf.cells = 0;
@@ -1149,16 +1149,31 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     const bool plain = (flags & PW_FLAG_PLAIN) != 0;
 
     // ---------------------------------------------------------- phase 1
-    const bool band1 = pair_mode && pr.int_path;
+    // All-vs-all calls too small for the inter-sequence sweeps to give every
+    // SM a warp (a few long sequences, e.g. one query against one target and
+    // its reverse complement) are swept band by band like explicit pairs.
+    std::vector<int32_t> auto_q, auto_t;
+    if (!pair_mode && pr.int_path && !plain && !(flags & PW_FLAG_INT32) &&
+        (int64_t)((nq + 1) / 2) * ((nt + kWarp - 1) / kWarp) < e->sm_count &&
+        (int64_t)((nt + 1) / 2) * ((nq + kWarp - 1) / kWarp) < e->sm_count && inf.cells >= (int64_t)1 << 24) {
+        for (int q = 0; q < nq; ++q)
+            for (int t = 0; t < nt; ++t) {
+                auto_q.push_back(q);
+                auto_t.push_back(t);
+            }
+    }
+    const std::vector<int32_t>& list_q = pair_mode ? e->pair_q : auto_q;
+    const std::vector<int32_t>& list_t = pair_mode ? e->pair_t : auto_t;
+    const bool band1 = !list_q.empty() && pr.int_path;
     const bool use_s16 = !band1 && !plain && (pr.s16_q || pr.s16_t) && !(flags & PW_FLAG_INT32);
     if (band1) {
         // explicit pairs: one warp per 256-row band, bands chained (pw_band.cuh)
-        const size_t np = e->pair_q.size();
+        const size_t np = list_q.size();
         std::vector<BandPair> bp(np);
         for (size_t k = 0; k < np; ++k) {
             memset(&bp[k], 0, sizeof(BandPair));
-            bp[k].q = e->pair_q[k];
-            bp[k].t = e->pair_t[k];
+            bp[k].q = list_q[k];
+            bp[k].t = list_t[k];
             const int lt = tlen[bp[k].t];
             bp[k].nbands = lt > 0 ? (lt + kBandRows - 1) / kBandRows : 1;
             bp[k].slot = (int64_t)k;
@@ -1171,10 +1186,11 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         cudaEventRecord(e->ev[1], e->stream);
         std::vector<float> bm;
         if ((c = download(e, bm, e->band_out.p, np)) != cudaSuccess) return cuda_fail(e, c, "copy pair maxima");
-        for (size_t k = 0; k < np; ++k) e->h_pair_max[(size_t)e->pair_q[k] * nt + e->pair_t[k]] = bm[k];
+        for (size_t k = 0; k < np; ++k) e->h_pair_max[(size_t)list_q[k] * nt + list_t[k]] = bm[k];
         float ms = 0;
         cudaEventElapsedTime(&ms, e->ev[0], e->ev[1]);
         inf.score_ms = ms;
+        inf.score_path = 2;
     } else if (use_s16) {
         cudaEventRecord(e->ev[0], e->stream);
         rc = phase1_s16(e, A, inf, flags);
@@ -1185,6 +1201,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         cudaEventElapsedTime(&ms, e->ev[0], e->ev[1]);
         inf.score_ms = ms;
     } else {
+        inf.score_path = 1;
     // items: one target against 32 consecutive queries of the length order
         std::vector<WorkItem> items;
         std::vector<int> cls;
@@ -1238,6 +1255,13 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         float ms = 0;
         cudaEventElapsedTime(&ms, e->ev[0], e->ev[1]);
         inf.score_ms = ms;
+    }
+    if (band1 && !pair_mode) {
+        // the band sweep wrote host maxima only: the trace kernels read them on the device
+        if ((c = cudaMemcpyAsync(A.pair_max, e->h_pair_max.data(), e->h_pair_max.size() * sizeof(float),
+                                 cudaMemcpyHostToDevice, e->stream)) != cudaSuccess ||
+            (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
+            return cuda_fail(e, c, "upload pair maxima");
     }
     if (pair_mode) {
         // pairs outside the list get -1: below MINIMUM_SCORE, never traced

@@ -117,3 +117,54 @@ def test_plain_and_batched_forms_agree_on_config1_sample(engine_lib):
     np.testing.assert_array_equal(pm_b, pm_p)
     assert hits_b == hits_p
     assert info_p.kernel_launches >= len(q) * len(t)
+
+
+def test_config3_sample_pairs_bit_exact_and_driver_agrees(engine_lib, oracle_mod):
+    """Long DNA pairs (scaled down) with their reverse-complement targets:
+    explicit pairs through the engine against the oracle pair by pair, and
+    the driver run once per query (as the reference is run per pair) giving
+    the same hits."""
+    from engine_helpers import configure, decode_hits
+    from pypaswas_b200 import _native
+    from pypaswas_b200.programs import Aligner
+    w = workloads.config3(n_pairs=3, length=(2500, 4000), shared=(800, 2000))
+    score = scores.make_score(w.settings)
+    q = [s.decode() for _, s in w.queries]
+    t = [s.decode() for _, s in w.targets]
+    ref = {}
+    p = cases.oracle_params(oracle_mod, score)
+    for qi, ti in w.pairs:
+        o = oracle_mod.run(p, [q[qi]], [t[ti]], cases.pos_scores(score, w.settings, [q[qi]], [t[ti]]),
+                           float(w.settings.minimum_score))
+        ref[(qi, ti)] = [dict(h, query=qi, target=ti) for h in o["hits"]]
+    e = _native.Engine(0, lib=engine_lib)
+    try:
+        configure(e, score, w.settings)
+        e.set_queries([s.encode() for s in q], np.arange(len(q)))
+        e.set_targets([s.encode() for s in t], np.arange(len(t)) + len(q))
+        e.set_pairs([a for a, _ in w.pairs], [b for _, b in w.pairs])
+        info = e.align()
+        got = decode_hits(*e.hits())
+    finally:
+        e.close()
+    assert info.score_path == 2
+    by_pair = {}
+    for h in got:
+        by_pair.setdefault((h["query"], h["target"]), []).append(h)
+    assert by_pair == {k: v for k, v in ref.items() if v}
+    assert all(ref[(i, i)] for i in range(3))  # every planted pair is found
+    # the driver, once per query against its forward and reverse-complement target
+    qrec = [SeqRecord(s, i) for i, s in zip([i for i, _ in w.queries], q)]
+    trec = [SeqRecord(s, i) for i, s in zip([i for i, _ in w.targets], t)]
+    for qi in range(3):
+        prog = Aligner(None, None, w.settings)
+        try:
+            hl = prog.process([qrec[qi]], [trec[qi], trec[qi + 3]], None)
+        finally:
+            prog.smith_waterman.close()
+        assert prog.smith_waterman.last_info.score_path == 2
+        got_d = sorted((h.target_info.id, h.seq_location, h.target_location, h.score, h.sequence_match)
+                       for h in hl.real_hits.values())
+        want = sorted((trec[r["target"]].id, (r["s_start"], r["s_end"]), (r["t_start"], r["t_end"]), r["score"],
+                       r["sequence_match"]) for r in ref[(qi, qi)] + ref[(qi, qi + 3)])
+        assert got_d == want
