@@ -228,6 +228,17 @@ class Engine(object):
                self.lib.pw_set_queries(self.handle, _ptr(buf), _ptr(off), len(seqs), _ptr(keys)), "pw_set_queries")
         self.n_queries = len(seqs)
 
+    def set_queries_packed(self, residues, offsets, id_keys):
+        """Queries as one concatenated uint8 array plus int64 offsets (n + 1):
+        no per-sequence Python objects (millions of reads)."""
+        buf = np.ascontiguousarray(residues, dtype=np.uint8).reshape(-1)
+        off = np.ascontiguousarray(offsets, dtype=np.int64)
+        keys = np.ascontiguousarray(id_keys, dtype=np.int32)
+        n = len(off) - 1
+        _check(self.lib, self.handle, self.lib.pw_set_queries(self.handle, _ptr(buf), _ptr(off), n, _ptr(keys)),
+               "pw_set_queries")
+        self.n_queries = n
+
     def set_targets(self, seqs, id_keys):
         buf, off = pack_sequences(seqs)
         keys = np.ascontiguousarray(id_keys, dtype=np.int32)

@@ -18,6 +18,8 @@
 #include <numeric>
 #include <queue>
 #include <string>
+#include <mutex>
+#include <thread>
 #include <vector>
 
 #include "../../include/paswas_b200.h"
@@ -35,6 +37,66 @@ using namespace pw;
 static double wall_ms() {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
+
+// Runs f(begin, end) over [0, n) split into contiguous ranges, one host
+// thread each (ranges in order: range k covers [n * k / T, n * (k + 1) / T)).
+template <typename F>
+static void parallel_for(int64_t n, F&& f, int64_t min_chunk = 1 << 15) {
+    const int64_t hw = std::max<int64_t>(1, (int64_t)std::thread::hardware_concurrency());
+    const int T = (int)std::min<int64_t>(std::min<int64_t>(hw, 32), std::max<int64_t>(1, n / min_chunk));
+    if (T <= 1) {
+        f((int64_t)0, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    th.reserve(T);
+    for (int k = 0; k < T; ++k) th.emplace_back([&, k] { f(n * k / T, n * (k + 1) / T); });
+    for (auto& t : th) t.join();
+}
+
+// Host array in page-locked memory when the driver grants it (faster device
+// copies of large results such as the pair maxima), else in ordinary memory.
+template <typename T>
+struct HostBuf {
+    T* p = nullptr;
+    size_t n = 0, cap = 0;
+    bool pinned = false;
+    HostBuf() = default;
+    HostBuf(const HostBuf&) = delete;
+    HostBuf& operator=(const HostBuf&) = delete;
+    ~HostBuf() { release(); }
+    void release() {
+        if (p) {
+            if (pinned)
+                cudaFreeHost(p);
+            else
+                free(p);
+        }
+        p = nullptr;
+        n = cap = 0;
+    }
+    bool resize(size_t m) {  // contents are not kept
+        if (m > cap) {
+            release();
+            const size_t want = std::max<size_t>(m, 1);
+            pinned = cudaMallocHost((void**)&p, want * sizeof(T)) == cudaSuccess;
+            if (!pinned) {
+                cudaGetLastError();
+                p = (T*)malloc(want * sizeof(T));
+                if (!p) return false;
+            }
+            cap = want;
+        }
+        n = m;
+        return true;
+    }
+    void fill(T v) { std::fill(p, p + n, v); }
+    size_t size() const { return n; }
+    T* data() { return p; }
+    const T* data() const { return p; }
+    T& operator[](size_t i) { return p[i]; }
+    const T& operator[](size_t i) const { return p[i]; }
+};
 
 namespace {
 
@@ -153,7 +215,7 @@ struct pw_engine {
     std::vector<int32_t> pair_q, pair_t;             // pw_set_pairs: explicit (query, target) pairs
     int64_t tune[8] = {0, 0, 0, 0, 0, 0, 0, 0};      // pw_set_tuning values (0: automatic)
     // results
-    std::vector<float> h_pair_max;
+    HostBuf<float> h_pair_max;
     std::vector<pw_hit> h_hits;
     std::vector<char> h_strings;
     std::vector<StartRec> h_starts;
@@ -364,6 +426,14 @@ static cudaError_t upload(pw_engine* e, DevBuf& b, const std::vector<HT>& v) {
     if (c != cudaSuccess) return c;
     if (v.empty()) return cudaSuccess;
     return cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(HT), cudaMemcpyHostToDevice, e->stream);
+}
+
+static cudaError_t download(pw_engine* e, HostBuf<float>& v, const void* src, size_t n) {
+    if (!v.resize(n)) return cudaErrorMemoryAllocation;
+    if (!n) return cudaSuccess;
+    cudaError_t c = cudaMemcpyAsync(v.data(), src, n * sizeof(float), cudaMemcpyDeviceToHost, e->stream);
+    if (c != cudaSuccess) return c;
+    return cudaStreamSynchronize(e->stream);
 }
 
 template <typename HT>
@@ -883,8 +953,9 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uin
         S.bnd_pool = e->bnd_pool.as<uint4>();
         S.bnd_slot = slot;
     }
-    if ((c = cudaMemsetAsync(e->counter.p, 0, kNumClasses * sizeof(int), e->stream)) != cudaSuccess)
+    if ((c = cudaMemsetAsync(e->counter.p, 0, 16 * sizeof(int), e->stream)) != cudaSuccess)
         return cuda_fail(e, c, "reset counters");
+    S.ovf_count = e->counter.as<int>() + 8;
     if (chained) {
         S.chain = e->chain_info.as<int4>();
         S.ring_off = e->chain_ring_off.as<int64_t>();
@@ -928,17 +999,19 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uin
     inf.score_kernel_ms += ms;
     cudaEventDestroy(a);
     cudaEventDestroy(b);
-    if (chained) {
-        int aborted = 0;
-        if ((c = cudaMemcpy(&aborted, e->chain_abort.p, sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess)
-            return cuda_fail(e, c, "read chain status");
-        if (aborted) return fail(e, PW_ERR_KERNEL, "chained score sweep: a strip waited too long for its predecessor");
-    }
+    int status[2] = {0, 0};  // overflow count, chain abort flag
+    if ((c = cudaMemcpyAsync(&status[0], S.ovf_count, sizeof(int), cudaMemcpyDeviceToHost, e->stream)) != cudaSuccess ||
+        (chained &&
+         (c = cudaMemcpyAsync(&status[1], e->chain_abort.p, sizeof(int), cudaMemcpyDeviceToHost, e->stream)) !=
+             cudaSuccess) ||
+        (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
+        return cuda_fail(e, c, "read score status");
+    if (status[1]) return fail(e, PW_ERR_KERNEL, "chained score sweep: a strip waited too long for its predecessor");
 
     // pairs that reached the 16-bit limit: the 32-bit sweep, per target
     std::vector<std::vector<int32_t>> ovf(nt);
     int64_t n_ovf = 0;
-    for (int sp = 0; sp < nq; ++sp) {
+    for (int sp = 0; sp < nq && status[0] > 0; ++sp) {
         const int q = pr.order[sp];
         for (int t = 0; t < nt; ++t)
             if (std::isnan(e->h_pair_max[(size_t)q * nt + t])) {
@@ -1116,7 +1189,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     pw_run_info inf;
     memset(&inf, 0, sizeof(inf));
     const int nq = e->Q.n, nt = e->T.n;
-    e->h_pair_max.assign((size_t)nq * nt, 0.0f);
+    if (!e->h_pair_max.resize((size_t)nq * nt)) return fail(e, PW_ERR_NOMEM, "host pair maxima");
     inf.pairs = (int64_t)nq * nt;
     int64_t sumq = 0, sumt = 0;
     for (int i = 0; i < nq; ++i) sumq += e->Q.off[i + 1] - e->Q.off[i];
@@ -1186,6 +1259,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         cudaEventRecord(e->ev[1], e->stream);
         std::vector<float> bm;
         if ((c = download(e, bm, e->band_out.p, np)) != cudaSuccess) return cuda_fail(e, c, "copy pair maxima");
+        e->h_pair_max.fill(-1.0f);
         for (size_t k = 0; k < np; ++k) e->h_pair_max[(size_t)list_q[k] * nt + list_t[k]] = bm[k];
         float ms = 0;
         cudaEventElapsedTime(&ms, e->ev[0], e->ev[1]);
@@ -1290,24 +1364,37 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     // no cell exceeds the pair maximum, so a pair whose maximum is below that
     // threshold has no starting point and contributes nothing: it is skipped.
     std::vector<std::vector<int32_t>> pass_t(nt);   // per target: passing queries, length order
-    std::vector<std::vector<int32_t>> pass_q(nq);   // per query: passing targets, length order
+    std::vector<std::vector<int32_t>> pass_q;       // per query: passing targets, length order (when needed)
     int64_t min_pass = 0, n_pass = 0;
-    for (int sp = 0; sp < nq; ++sp) {
-        const int q = pr.order[sp];
-        for (int t = 0; t < nt; ++t) {
-            const float mx = e->h_pair_max[(size_t)q * nt + t];
-            if (!(mx >= e->minimum_score)) continue;
-            ++min_pass;
-            const int mn = std::min(qlen[q], tlen[t]);
-            const float pos = (float)(e->highest * (double)mn * e->filter_factor);
-            const volatile float llm = e->lower_limit * mx;  // fp32 product, as the kernel computes it
-            const float thr = std::max((float)llm, pos);
-            if (mx >= thr) {
-                pass_t[t].push_back(q);
-                ++n_pass;
-                inf.traced_cells += (int64_t)qlen[q] * tlen[t];
+    {
+        std::mutex mu;
+        // one target column per task, all queries in length order (so each
+        // list comes out in that order); host threads split the targets
+        parallel_for(nt, [&](int64_t t0, int64_t t1) {
+            int64_t mp = 0, np_ = 0, tc = 0;
+            for (int64_t t = t0; t < t1; ++t) {
+                std::vector<int32_t>& lst = pass_t[t];
+                for (int sp = 0; sp < nq; ++sp) {
+                    const int q = pr.order[sp];
+                    const float mx = e->h_pair_max[(size_t)q * nt + t];
+                    if (!(mx >= e->minimum_score)) continue;
+                    ++mp;
+                    const int mn = std::min(qlen[q], tlen[t]);
+                    const float pos = (float)(e->highest * (double)mn * e->filter_factor);
+                    const volatile float llm = e->lower_limit * mx;  // fp32 product, as the kernel computes it
+                    const float thr = std::max((float)llm, pos);
+                    if (mx >= thr) {
+                        lst.push_back(q);
+                        ++np_;
+                        tc += (int64_t)qlen[q] * tlen[t];
+                    }
+                }
             }
-        }
+            std::lock_guard<std::mutex> g(mu);
+            min_pass += mp;
+            n_pass += np_;
+            inf.traced_cells += tc;
+        }, std::max<int64_t>(1, ((int64_t)1 << 20) / std::max(nq, 1)));
     }
     // Traced pairs with targets longer than one register strip go to the
     // one-warp-per-pair sweep (pw_band.cuh); the others are grouped 32 to
@@ -1333,18 +1420,34 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     double cost_t = 0, cost_q = 0;
     for (int t = 0; t < nt; ++t)
         for (size_t g = 0; g < pass_t[t].size(); g += per_item) cost_t += (double)tlen[t] * qlen[pass_t[t][g]] * per_item;
+    // the transposed orientation (queries as strips) can only win if even a
+    // lower bound of its slot cost -- every query's groups paying the
+    // shortest target -- is below the cost of the direct one
+    bool trans2 = false;
     {
-        std::vector<int32_t> rank_t(nt);
-        for (int k = 0; k < nt; ++k) rank_t[pr.order_t[k]] = k;
+        std::vector<int32_t> kq(nq, 0);
         for (int t = 0; t < nt; ++t)
-            for (int32_t q : pass_t[t]) pass_q[q].push_back(t);
+            for (int32_t q : pass_t[t]) ++kq[q];
+        int tmin = INT32_MAX;
+        for (int t = 0; t < nt; ++t) tmin = std::min(tmin, std::max(tlen[t], 1));
+        double lb_q = 0;
         for (int q = 0; q < nq; ++q)
-            std::stable_sort(pass_q[q].begin(), pass_q[q].end(), [&](int a, int b) { return rank_t[a] < rank_t[b]; });
-        for (int q = 0; q < nq; ++q)
-            for (size_t g = 0; g < pass_q[q].size(); g += per_item)
-                cost_q += (double)qlen[q] * tlen[pass_q[q][g]] * per_item;
+            if (kq[q]) lb_q += (double)((kq[q] + per_item - 1) / per_item) * per_item * qlen[q] * tmin;
+        if (lb_q < cost_t) {
+            pass_q.resize(nq);
+            std::vector<int32_t> rank_t(nt);
+            for (int k = 0; k < nt; ++k) rank_t[pr.order_t[k]] = k;
+            for (int t = 0; t < nt; ++t)
+                for (int32_t q : pass_t[t]) pass_q[q].push_back(t);
+            for (int q = 0; q < nq; ++q)
+                std::stable_sort(pass_q[q].begin(), pass_q[q].end(),
+                                 [&](int a, int b) { return rank_t[a] < rank_t[b]; });
+            for (int q = 0; q < nq; ++q)
+                for (size_t g = 0; g < pass_q[q].size(); g += per_item)
+                    cost_q += (double)qlen[q] * tlen[pass_q[q][g]] * per_item;
+            trans2 = cost_q < cost_t;
+        }
     }
-    const bool trans2 = cost_q < cost_t;
     std::vector<int32_t> p2_order;
     std::vector<WorkItem> items2;
     std::vector<int> cls2;
@@ -1690,68 +1793,119 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     // hits in the reference's HitList order: ascending score, then the pinned
     // emission order of their starting points (SmithWaterman.py:699)
     const double t_finish = wall_ms();
-    std::vector<int64_t> ord(all_hits.size());
-    std::iota(ord.begin(), ord.end(), 0);
-    auto hkey = [&](const DevHit& h) {
-        return std::make_tuple(h.score, -(int64_t)((h.end_x >> 3) + (h.end_y >> 3)), -(int64_t)(h.end_x >> 3),
-                               h.target, h.query, -(int64_t)((h.end_x & 7) + (h.end_y & 7)), (int64_t)(h.end_y & 7));
+    struct HKey {
+        uint64_t a, b, c;
+        int64_t idx;
+        bool operator<(const HKey& o) const {
+            return a != o.a ? a < o.a : (b != o.b ? b < o.b : (c != o.c ? c < o.c : idx < o.idx));
+        }
     };
-    std::stable_sort(ord.begin(), ord.end(),
-                     [&](int64_t a, int64_t b) { return hkey(all_hits[a]) < hkey(all_hits[b]); });
-    int64_t str_bytes = 0;
-    e->h_hits.resize(all_hits.size());
-    for (size_t k = 0; k < ord.size(); ++k) {
-        const DevHit& d = all_hits[ord[k]];
-        pw_hit& h = e->h_hits[k];
-        h.query = d.query;
-        h.target = d.target;
-        h.s_start = d.s_start;
-        h.s_end = d.s_end;
-        h.t_start = d.t_start;
-        h.t_end = d.t_end;
-        h.score = d.score;
-        h.matches = d.matches;
-        h.mismatches = d.mismatches;
-        h.n_cols = d.n_cols;
-        h.str_offset = str_bytes;
-        str_bytes += 3 * (int64_t)d.n_cols;
-    }
-    // alignment strings from the column operations
-    e->h_strings.resize((size_t)str_bytes);
-    for (size_t k = 0; k < ord.size(); ++k) {
-        const DevHit& d = all_hits[ord[k]];
-        const pw_hit& h = e->h_hits[k];
-        char* sq = e->h_strings.data() + h.str_offset;
-        char* al = sq + h.n_cols;
-        char* tg = al + h.n_cols;
-        const uint8_t* qs = e->Q.raw.data() + e->Q.off[d.query];
-        const uint8_t* ts = e->T.raw.data() + e->T.off[d.target];
-        int x = d.s_start, y = d.t_start;
-        const char* ops = all_ops.data() + d.ops_offset;
-        for (int i = 0; i < d.n_cols; ++i) {
-            const char op = ops[i];
-            if (op == 'M') {
-                const uint8_t a = ts[y], b = qs[x];
-                const bool la = (a >= 'A' && a <= 'Z') || (a >= 'a' && a <= 'z');
-                const bool eq = la ? ((a | 0x20) == (b | 0x20)) : a == b;
-                sq[i] = (char)b;
-                tg[i] = (char)a;
-                al[i] = eq ? '|' : '.';
-                ++x;
-                ++y;
-            } else if (op == 'I') {
-                sq[i] = (char)qs[x];
-                tg[i] = '-';
-                al[i] = ' ';
-                ++x;
-            } else {
-                sq[i] = '-';
-                tg[i] = (char)ts[y];
-                al[i] = ' ';
-                ++y;
+    const int64_t nhits = (int64_t)all_hits.size();
+    std::vector<HKey> keys((size_t)nhits);
+    // (score ascending; block anti-diagonal, block x descending; target, query
+    // ascending; cell anti-diagonal descending; row ascending) packed into
+    // three words; scores are >= 0, so their fp32 bits order like the values
+    parallel_for(nhits, [&](int64_t k0, int64_t k1) {
+        for (int64_t k = k0; k < k1; ++k) {
+            const DevHit& h = all_hits[k];
+            uint32_t sb;
+            std::memcpy(&sb, &h.score, 4);
+            const uint32_t diag = (uint32_t)((h.end_x >> 3) + (h.end_y >> 3));
+            const uint32_t small = (uint32_t)((h.end_x & 7) + (h.end_y & 7));
+            keys[k] = HKey{((uint64_t)sb << 32) | (0xFFFFFFFFu - diag),
+                           ((uint64_t)(0xFFFFFFFFu - (uint32_t)(h.end_x >> 3)) << 32) | (uint32_t)h.target,
+                           ((uint64_t)(uint32_t)h.query << 32) | ((uint64_t)(0xFFu - small) << 8) | (uint32_t)(h.end_y & 7),
+                           k};
+        }
+    });
+    {
+        // sort runs in parallel, then merge them pairwise
+        const int64_t hw = std::max<int64_t>(1, (int64_t)std::thread::hardware_concurrency());
+        int runs = (int)std::min<int64_t>(std::min<int64_t>(hw, 32), std::max<int64_t>(1, nhits / (1 << 16)));
+        std::vector<int64_t> bnd(runs + 1);
+        for (int r = 0; r <= runs; ++r) bnd[r] = nhits * r / runs;
+        {
+            std::vector<std::thread> th;
+            for (int r = 0; r < runs; ++r)
+                th.emplace_back([&, r] { std::sort(keys.begin() + bnd[r], keys.begin() + bnd[r + 1]); });
+            for (auto& t : th) t.join();
+        }
+        std::vector<HKey> tmp(runs > 1 ? keys.size() : 0);
+        while (runs > 1) {
+            std::vector<int64_t> nb;
+            std::vector<std::thread> th;
+            for (int r = 0; r < runs; r += 2) {
+                nb.push_back(bnd[r]);
+                if (r + 1 < runs)
+                    th.emplace_back([&, r] {
+                        std::merge(keys.begin() + bnd[r], keys.begin() + bnd[r + 1], keys.begin() + bnd[r + 1],
+                                   keys.begin() + bnd[r + 2], tmp.begin() + bnd[r]);
+                    });
+                else
+                    th.emplace_back([&, r] {
+                        std::copy(keys.begin() + bnd[r], keys.begin() + bnd[r + 1], tmp.begin() + bnd[r]);
+                    });
             }
+            for (auto& t : th) t.join();
+            nb.push_back(nhits);
+            keys.swap(tmp);
+            bnd.swap(nb);
+            runs = (int)bnd.size() - 1;
         }
     }
+    std::vector<int64_t> soff2((size_t)nhits + 1, 0);
+    for (int64_t k = 0; k < nhits; ++k) soff2[k + 1] = soff2[k] + 3 * (int64_t)all_hits[keys[k].idx].n_cols;
+    const int64_t str_bytes = soff2[nhits];
+    e->h_hits.resize((size_t)nhits);
+    e->h_strings.resize((size_t)str_bytes);
+    // hits and their alignment strings (from the column operations), in order
+    parallel_for(nhits, [&](int64_t k0, int64_t k1) {
+        for (int64_t k = k0; k < k1; ++k) {
+            const DevHit& d = all_hits[keys[k].idx];
+            pw_hit& h = e->h_hits[k];
+            h.query = d.query;
+            h.target = d.target;
+            h.s_start = d.s_start;
+            h.s_end = d.s_end;
+            h.t_start = d.t_start;
+            h.t_end = d.t_end;
+            h.score = d.score;
+            h.matches = d.matches;
+            h.mismatches = d.mismatches;
+            h.n_cols = d.n_cols;
+            h.str_offset = soff2[k];
+            char* sq = e->h_strings.data() + h.str_offset;
+            char* al = sq + h.n_cols;
+            char* tg = al + h.n_cols;
+            const uint8_t* qs = e->Q.raw.data() + e->Q.off[d.query];
+            const uint8_t* ts = e->T.raw.data() + e->T.off[d.target];
+            int x = d.s_start, y = d.t_start;
+            const char* ops = all_ops.data() + d.ops_offset;
+            for (int i = 0; i < d.n_cols; ++i) {
+                const char op = ops[i];
+                if (op == 'M') {
+                    const uint8_t ca = ts[y], cb = qs[x];
+                    const bool la = (ca >= 'A' && ca <= 'Z') || (ca >= 'a' && ca <= 'z');
+                    const bool eq = la ? ((ca | 0x20) == (cb | 0x20)) : ca == cb;
+                    sq[i] = (char)cb;
+                    tg[i] = (char)ca;
+                    al[i] = eq ? '|' : '.';
+                    ++x;
+                    ++y;
+                } else if (op == 'I') {
+                    sq[i] = (char)qs[x];
+                    tg[i] = '-';
+                    al[i] = ' ';
+                    ++x;
+                } else {
+                    sq[i] = '-';
+                    tg[i] = (char)ts[y];
+                    al[i] = ' ';
+                    ++y;
+                }
+            }
+        }
+    }, 1 << 12);
     inf.starting_points = total_starts;
     inf.hits = (int64_t)e->h_hits.size();
     inf.string_bytes = str_bytes;

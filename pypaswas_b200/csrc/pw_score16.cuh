@@ -58,6 +58,7 @@ struct Score16Args {
     int pad_code;                // lane code of the padding residue
     int* abort_flag;             // set when a wait runs out of time; every waiting warp then gives up
     int n_chain_items;           // host-side bookkeeping: entries of the chained launch
+    int* ovf_count;              // pairs reported as NaN (16-bit limit reached)
 };
 
 // Profile of strip rows [y0, y0 + S): for row group g (4 rows) and lane
@@ -446,6 +447,7 @@ __global__ void __launch_bounds__(128, 3) score16_chain_kernel(Score16Args A) {
             if (sb >= 0)
                 A.pair_max[(int64_t)sb * A.stride_strip + (int64_t)p * A.stride_lane] =
                     mb >= kOvf16 ? __int_as_float(0x7fc00000) : (float)mb;
+            if (ma >= kOvf16 || (sb >= 0 && mb >= kOvf16)) atomicAdd(A.ovf_count, 1);
         }
     }
 }
@@ -492,6 +494,7 @@ __global__ void __launch_bounds__(128) score16_kernel(Score16Args A) {
             if (sb >= 0)
                 A.pair_max[(int64_t)sb * A.stride_strip + (int64_t)p * A.stride_lane] =
                     mb >= kOvf16 ? __int_as_float(0x7fc00000) : (float)mb;
+            if (ma >= kOvf16 || (sb >= 0 && mb >= kOvf16)) atomicAdd(A.ovf_count, 1);
         }
     }
 }
