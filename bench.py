@@ -33,6 +33,10 @@ import numpy as np  # noqa: E402
 
 # algorithmic operations per cell (add and max counted separately) of the
 # recurrences: linear/affine, score only / with direction classification
+# the trimmer workload's end-to-end leg builds Python Hit objects: it runs on
+# the first reads only (the bench line names the sample)
+E2E_READS = 200_000
+
 OPS_PER_CELL = {("linear", "score"): 5, ("linear", "dirs"): 8, ("affine", "score"): 10, ("affine", "dirs"): 14}
 
 
@@ -42,9 +46,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", type=int, choices=[1, 2, 3], default=2,
+    ap.add_argument("--config", type=int, choices=[1, 2, 3, 4], default=2,
                     help="workload: 1 DNA reads x adapters, 2 protein batched (the metric's configuration), "
-                         "3 long DNA pairs")
+                         "3 long DNA pairs, 4 trimmer reads x adapters")
+    ap.add_argument("--reads", type=int, default=10_000_000, help="config 4: number of reads")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--targets", type=int, default=0,
@@ -65,6 +70,8 @@ def workload(args):
         return workloads.config1()
     if args.config == 3:
         return workloads.config3()
+    if args.config == 4:
+        return workloads.config4(n_reads=args.reads)
     w = workloads.config2()
     if args.targets and args.targets < len(w.targets):
         step = len(w.targets) // args.targets
@@ -160,9 +167,14 @@ def engine_for(workload, device):
     score = scores.make_score(workload.settings)
     e = _native.Engine(device)
     configure_engine(e, score, workload.settings)
-    qk, tk = id_keys([i for i, _ in workload.queries], [i for i, _ in workload.targets])
-    e.set_queries([s for _, s in workload.queries], qk)
-    e.set_targets([s for _, s in workload.targets], tk)
+    if workload.queries is None:  # packed reads (trimmer workload): read ids never equal target ids
+        n, L = workload.reads.shape
+        e.set_queries_packed(workload.reads, np.arange(n + 1, dtype=np.int64) * L, np.arange(n, dtype=np.int32))
+        e.set_targets([s for _, s in workload.targets], np.arange(len(workload.targets), dtype=np.int32) + n)
+    else:
+        qk, tk = id_keys([i for i, _ in workload.queries], [i for i, _ in workload.targets])
+        e.set_queries([s for _, s in workload.queries], qk)
+        e.set_targets([s for _, s in workload.targets], tk)
     if workload.pairs is not None:
         e.set_pairs([p[0] for p in workload.pairs], [p[1] for p in workload.pairs])
     return e, score
@@ -171,33 +183,50 @@ def engine_for(workload, device):
 def cpu_baseline(workload, score, seconds, processes=1):
     """The oracle (CPU restatement of the reference path) on a bounded sample of
     the workload: queries x targets taken evenly from the length-sorted lists
-    (or, with explicit pairs, the first pairs), grown until the estimated run
-    time reaches `seconds`."""
+    (or, with explicit pairs, the first pairs).  The sample is sized for about
+    `seconds` of work: a first run at an estimated rate calibrates a second,
+    larger one if the first was much shorter."""
+    rate = 24e6 * max(1, processes)  # cells/s first estimate of the oracle
+    r = None
+    for _ in range(3):
+        r = _cpu_sample(workload, score, seconds * rate, processes)
+        if r["seconds"] >= 0.4 * seconds or r["full"]:
+            break
+        rate = r["cells"] / max(r["seconds"], 1e-3)
+    return {k: v for k, v in r.items() if k not in ("cells", "full")}
+
+
+def _cpu_sample(workload, score, budget_cells, processes):
     import multiprocessing as mp
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle
     oracle.build()
     q_all = [s.decode() for _, s in workload.queries]
     t_all = [s.decode() for _, s in workload.targets]
-    rate = 24e6 * max(1, processes)  # cells/s estimate of the oracle
     args = _oracle_args(score, workload.settings)
     if workload.pairs is not None:
         jobs, cells = [], 0
         for qi, ti in workload.pairs:
-            if cells and cells + len(q_all[qi]) * len(t_all[ti]) > seconds * rate:
+            if cells and cells + len(q_all[qi]) * len(t_all[ti]) > budget_cells:
                 break
             jobs.append((args, [q_all[qi]], [t_all[ti]]))
             cells += len(q_all[qi]) * len(t_all[ti])
+        full = len(jobs) == len(workload.pairs)
         sample = "the first %d explicit pairs (%d cells) of the same workload, full path" % (len(jobs), cells)
     else:
+        # targets first (up to all of them) against 10 queries, then more queries
         nq = min(len(q_all), 10)
-        nt = max(1, int(seconds * rate / (sum(map(len, q_all[::max(1, len(q_all) // nq)][:nq])) * 1025)))
-        nt = min(nt, len(t_all))
-        qs = q_all[::max(1, len(q_all) // nq)][:nq]
+        q10 = sum(map(len, q_all[::max(1, len(q_all) // nq)][:nq]))
+        t_avg = sum(map(len, t_all)) / max(1, len(t_all))
+        nt = min(len(t_all), max(1, int(budget_cells / (q10 * t_avg))))
         ts = t_all[::max(1, len(t_all) // nt)][:nt]
+        q_avg = sum(map(len, q_all)) / max(1, len(q_all))
+        nq = min(len(q_all), max(nq, int(budget_cells / (q_avg * sum(map(len, ts))))))
+        qs = q_all[::max(1, len(q_all) // nq)][:nq]
         cells = sum(map(len, qs)) * sum(map(len, ts))
         jobs = [(args, qs, ts[i::processes]) for i in range(max(1, processes))]
         jobs = [j for j in jobs if j[2]]
+        full = len(qs) == len(q_all) and len(ts) == len(t_all)
         sample = "%d queries x %d targets (%d cells) of the same workload, full path" % (len(qs), len(ts), cells)
     t0 = time.time()
     if processes <= 1:
@@ -209,7 +238,7 @@ def cpu_baseline(workload, score, seconds, processes=1):
             pool.map(_oracle_chunk, jobs)
     dt = time.time() - t0
     return {"value": cells / dt / 1e9, "unit": "GCUPS", "cores": processes, "kind": "port", "sample": sample,
-            "seconds": dt}
+            "seconds": dt, "cells": cells, "full": full}
 
 
 def _oracle_args(score, settings):
@@ -238,14 +267,16 @@ def run_reference(args, workload_fn):
     procs = os.cpu_count() or 1
     steps = []
     for i in range(args.warmup + args.steps):
-        r = cpu_baseline(w, score, min(args.cpu_seconds, 20.0), processes=procs)
+        r = cpu_baseline(w if w.queries is not None else w.head(200000), score, min(args.cpu_seconds, 20.0),
+                         processes=procs)
         if i >= args.warmup:
             steps.append(r)
     v = float(np.median([s["value"] for s in steps]))
     line = {"impl": "reference", "metric": "GCUPS", "value": v, "unit": "GCUPS", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": w.name, "pairs": len(w.queries) * len(w.targets)},
+            "config": {"workload": w.name,
+                       "pairs": len(w.pairs) if w.pairs is not None else w.n_queries * len(w.targets)},
             "cpu_baseline": {"value": v, "unit": "GCUPS", "cores": procs, "kind": "port",
                              "sample": steps[0]["sample"]},
             "e2e": {"value": v, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -303,7 +334,7 @@ def main():
         torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
         t_ms = float(tt.item())
     value = world * cells * args.steps / (t_ms * 1e-3) / 1e9
-    n_pairs = len(w.pairs) if w.pairs is not None else len(w.queries) * len(w.targets)
+    n_pairs = len(w.pairs) if w.pairs is not None else w.n_queries * len(w.targets)
     ms_per_step = t_ms / args.steps
 
     # roofline of the dominant kernel (integer-ALU bound)
@@ -328,7 +359,8 @@ def main():
                                  "score_sweep_bytes_per_launch")
 
     # end to end through the public driver, host records in, hits out
-    e2e_value, h2d, d2h = (None, 0, 0) if args.no_e2e else _e2e(w, args.steps, local)
+    e2e_w = w if w.queries is not None else w.head(E2E_READS)
+    e2e_value, h2d, d2h = (None, 0, 0) if args.no_e2e else _e2e(e2e_w, args.steps, local)
 
     out = {"metric": "GCUPS", "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
@@ -356,13 +388,15 @@ def main():
                         "launches": dom_launch, "avg_launch_ms": dom_ms / max(1, dom_launch),
                         "traffic": traffic,
                         "hbm_gbs_measured": load_peaks().get("hbm_gbs")},
-           "e2e": {"value": e2e_value, "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}}
+           "e2e": {"value": e2e_value, "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                   "workload": e2e_w.name}}
     if not args.no_plain and w.pairs is None:
-        out["plain"] = plain_vs_batched(w, local, value)
+        out["plain"] = plain_vs_batched(w if w.queries is not None else w.head(64), local, value)
     if not args.no_serve and rank == 0 and args.config == 2:
         out["serve"] = serve_leg(local, args.serve_seconds, [float(x) for x in args.serve_loads.split(",")])
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(w, score, args.cpu_seconds, processes=1)
+        out["cpu_baseline"] = cpu_baseline(w if w.queries is not None else w.head(20000), score, args.cpu_seconds,
+                                           processes=1)
     if rank == 0:
         print(json.dumps(out), flush=True)
     e.close()
@@ -457,8 +491,10 @@ def _e2e(w, steps, device):
     explicit pairs (long DNA), one process() call per query against its
     targets, as the reference would be run once per pair."""
     import torch
-    from pypaswas_b200.programs import Aligner
+    from pypaswas_b200.formatters import TrimmerFormatter
+    from pypaswas_b200.programs import Aligner, Trimmer
     from pypaswas_b200.records import SeqRecord
+    trimmer = getattr(w.settings, "program", "aligner") == "trimmer"
     queries = [SeqRecord(s, i) for i, s in w.queries]
     targets = [SeqRecord(s, i) for i, s in w.targets]
     if w.pairs is None:
@@ -468,7 +504,7 @@ def _e2e(w, steps, device):
         for qi, ti in w.pairs:
             per_q.setdefault(qi, []).append(targets[ti])
         calls = [([queries[qi]], ts) for qi, ts in sorted(per_q.items())]
-    aligner = Aligner(None, None, w.settings, device=device)
+    aligner = (Trimmer if trimmer else Aligner)(None, None, w.settings, device=device)
     for qs, ts in calls[:2]:
         aligner.process(qs, ts, None)  # warm-up
     torch.cuda.synchronize()
@@ -477,7 +513,9 @@ def _e2e(w, steps, device):
     for _ in range(steps):
         h2d = d2h = 0
         for qs, ts in calls:
-            aligner.process(qs, ts, None)
+            hl = aligner.process(qs, ts, None)
+            if trimmer:
+                TrimmerFormatter(None, hl, None).lines()  # the program's trimmedFasta records
             h2d += int(aligner.smith_waterman.last_h2d_bytes)
             d2h += int(aligner.smith_waterman.last_d2h_bytes)
     torch.cuda.synchronize()

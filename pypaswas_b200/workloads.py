@@ -55,7 +55,21 @@ class Workload(object):
         self.pairs = pairs
 
     @property
+    def n_queries(self):
+        return len(self.queries) if self.queries is not None else int(self.reads.shape[0])
+
+    def head(self, n_queries):
+        """The same workload on its first n queries (all targets; explicit
+        pairs kept where both ends remain)."""
+        qs = self.queries[:n_queries] if self.queries is not None else [
+            (self.read_ids[i], self.reads[i].tobytes()) for i in range(min(n_queries, len(self.read_ids)))]
+        pairs = None if self.pairs is None else [(q, t) for q, t in self.pairs if q < n_queries]
+        return Workload("%s, first %d queries" % (self.name, len(qs)), qs, self.targets, self.settings, pairs)
+
+    @property
     def cells(self):
+        if self.queries is None:  # packed reads
+            return int(self.reads.shape[0]) * int(self.reads.shape[1]) * sum(len(s) for _, s in self.targets)
         if self.pairs is not None:
             return sum(len(self.queries[q][1]) * len(self.targets[t][1]) for q, t in self.pairs)
         return sum(len(s) for _, s in self.queries) * sum(len(s) for _, s in self.targets)
