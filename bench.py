@@ -329,6 +329,7 @@ def main():
         infos.append(info.as_dict())
     clocks = sampler.stop()
     t_ms = float(sum(times))
+    step_stats = {"min": float(min(times)), "median": float(np.median(times)), "max": float(max(times))}
     if world > 1:
         tt = torch.tensor([t_ms], device="cuda")
         torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
@@ -363,7 +364,8 @@ def main():
     e2e_value, h2d, d2h = (None, 0, 0) if args.no_e2e else _e2e(e2e_w, args.steps, local)
 
     out = {"metric": "GCUPS", "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+           "warmup": args.warmup, "ms_per_step": ms_per_step, "step_ms": step_stats,
+           "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "int32", "data": "synthetic",
            "config": {"workload": "%s (%d pairs, full path)" % (w.name, n_pairs),
                       "pairs": n_pairs,
