@@ -172,6 +172,11 @@ int pw_set_wave_limit(pw_engine* e, int64_t bytes);
  *                       load are cut into chained one-strip entries (default
  *                       500; 1 chains nearly every multi-strip item) */
 #define PW_TUNE_CHAIN_MIN 0
+/*   PW_TUNE_GRID_SHARE  thousandths of the GPU's resident-block capacity this
+ *                       engine's persistent kernels may occupy (default all);
+ *                       several engines (the serving loop's workers) can then
+ *                       keep kernels resident side by side */
+#define PW_TUNE_GRID_SHARE 1
 int pw_set_tuning(pw_engine* e, int key, int64_t value);
 
 /* Pair maxima (the last block of the maxima chain, default_main.cu:591),
@@ -265,6 +270,8 @@ int pw_server_wait(pw_server* s, int64_t ticket, int32_t timeout_ms, pw_request_
 int pw_server_top_hits(pw_server* s, int64_t ticket, int32_t* targets, float* scores, int32_t k);
 int pw_server_hits(pw_server* s, int64_t ticket, pw_hit* hits, int64_t max_hits, char* strbuf,
                    int64_t strbuf_bytes);
+/* pw_set_tuning on every worker engine. */
+int pw_server_tune(pw_server* s, int key, int64_t value);
 /* Frees a finished request's results. */
 int pw_server_release(pw_server* s, int64_t ticket);
 int pw_server_stats(pw_server* s, pw_server_counters* st);

@@ -30,6 +30,7 @@ PW_FLAG_PLAIN = 2
 PW_FLAG_INT32 = 4
 PW_FLAG_NO_CHAIN = 8
 PW_TUNE_CHAIN_MIN = 0
+PW_TUNE_GRID_SHARE = 1
 
 # symbols the header declares, checked by the CPU test-suite
 EXPORTED_SYMBOLS = (
@@ -38,7 +39,7 @@ EXPORTED_SYMBOLS = (
     "pw_get_starting_points", "pw_last_launch_count", "pw_measure_int_peak", "pw_score_max_noalloc",
     "pw_set_wave_limit", "pw_set_tuning", "pw_set_pairs", "pw_server_create", "pw_server_destroy", "pw_server_last_error", "pw_server_set_scoring",
     "pw_server_load_db", "pw_server_submit", "pw_server_wait", "pw_server_top_hits", "pw_server_hits",
-    "pw_server_release", "pw_server_stats",
+    "pw_server_release", "pw_server_stats", "pw_server_tune",
 )
 
 
@@ -135,6 +136,7 @@ def bind(lib):
         "pw_server_hits": (ctypes.c_int, [P, I64, P, I64, P, I64]),
         "pw_server_release": (ctypes.c_int, [P, I64]),
         "pw_server_stats": (ctypes.c_int, [P, ctypes.POINTER(PwServerStats)]),
+        "pw_server_tune": (ctypes.c_int, [P, ctypes.c_int, I64]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -198,7 +198,7 @@ struct pw_engine {
     // on the device and reused while inputs, scoring, flags and tuning stay
     struct {
         bool valid = false;
-        int64_t qg = 0, tg = 0, sg = 0, tune = 0;
+        int64_t qg = 0, tg = 0, sg = 0, tune = 0, share = 0;
         uint32_t flags = 0;
         bool trans = false, chained = false;
         int begin[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -221,6 +221,16 @@ struct pw_engine {
     std::vector<StartRec> h_starts;
     int64_t launches = 0;
 };
+
+// Resident-block budget of this engine's persistent kernels: all SMs' worth,
+// or the share set with PW_TUNE_GRID_SHARE (thousandths), so that the kernels
+// of several engines (the serving loop's workers) can be resident together.
+static int grid_cap(const pw_engine* e, int per_sm) {
+    const int64_t share = e->tune[PW_TUNE_GRID_SHARE];
+    const int64_t full = (int64_t)e->sm_count * std::max(1, per_sm);
+    if (share <= 0 || share >= 1000) return (int)full;
+    return (int)std::max<int64_t>(1, full * share / 1000);
+}
 
 static int fail(pw_engine* e, int code, const std::string& msg) {
     if (e) e->err = msg;
@@ -384,7 +394,7 @@ cudaError_t launch_sweep(pw_engine* e, KernelArgs A, int* counter) {
     if (c != cudaSuccess) return c;
     if (per_sm < 1) per_sm = 1;
     if (per_sm > 16) per_sm = 16;
-    int grid = e->sm_count * per_sm;
+    int grid = grid_cap(e, per_sm);
     const int need = (A.n_items + 3) / 4;
     if (grid > need) grid = need;
     if (grid < 1) grid = 1;
@@ -741,7 +751,7 @@ static cudaError_t launch_s16(pw_engine* e, Score16Args A) {
     cudaError_t c = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem);
     if (c != cudaSuccess) return c;
     per_sm = std::max(1, std::min(per_sm, 16));
-    int grid = std::min(e->sm_count * per_sm, (A.n_items + 3) / 4);
+    int grid = std::min(grid_cap(e, per_sm), (A.n_items + 3) / 4);
     PW_LAUNCH(kern, std::max(grid, 1), 128, smem, e->stream, A);
     e->launches++;
     return cudaGetLastError();
@@ -820,7 +830,7 @@ static cudaError_t launch_s16_chain(pw_engine* e, Score16Args A) {
     cudaError_t c = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem);
     if (c != cudaSuccess) return c;
     per_sm = std::max(1, std::min(per_sm, 16));
-    const int grid = std::max(1, std::min(e->sm_count * per_sm, (A.n_items + 3) / 4));
+    const int grid = std::max(1, std::min(grid_cap(e, per_sm), (A.n_items + 3) / 4));
     PW_LAUNCH(kern, grid, 128, smem, e->stream, A);
     e->launches++;
     return cudaGetLastError();
@@ -847,7 +857,8 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uin
     auto& P1 = e->p1;
     const uint32_t pflags = flags & PW_FLAG_NO_CHAIN;
     const bool reuse = P1.valid && P1.qg == e->q_gen && P1.tg == e->t_gen && P1.sg == e->s_gen &&
-                       P1.flags == pflags && P1.tune == e->tune[PW_TUNE_CHAIN_MIN];
+                       P1.flags == pflags && P1.tune == e->tune[PW_TUNE_CHAIN_MIN] &&
+                       P1.share == e->tune[PW_TUNE_GRID_SHARE];
     cudaError_t c;
     if (!reuse) {
         const double t_plan = wall_ms();
@@ -910,7 +921,7 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uin
             if ((c = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem)) != cudaSuccess)
                 return cuda_fail(e, c, "occupancy");
             const int rc = setup_chains(e, it2, begin[kS32Multi], begin[kS32Multi + 1], strip_len,
-                                        e->sm_count * std::max(1, std::min(per_sm, 16)) * 4, &P1.n_chain_items);
+                                        grid_cap(e, std::max(1, std::min(per_sm, 16))) * 4, &P1.n_chain_items);
             if (rc != PW_OK) return rc;
         }
         P1.trans = trans;
@@ -921,6 +932,7 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uin
         P1.sg = e->s_gen;
         P1.flags = pflags;
         P1.tune = e->tune[PW_TUNE_CHAIN_MIN];
+        P1.share = e->tune[PW_TUNE_GRID_SHARE];
         P1.valid = true;
         inf.setup_ms += wall_ms() - t_plan;
     }
@@ -1072,7 +1084,7 @@ static int run_band_phase(pw_engine* e, KernelArgs A, std::vector<BandPair>& pai
     if ((c = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem)) != cudaSuccess)
         return cuda_fail(e, c, "occupancy");
     per_sm = std::max(1, std::min(per_sm, 16));
-    const int warps = e->sm_count * per_sm * 4;
+    const int warps = grid_cap(e, per_sm) * 4;
     // queue: the bands of each pair form a chain (pw_plan.h), longest pairs first
     std::vector<int> order(pairs.size());
     std::iota(order.begin(), order.end(), 0);
@@ -1125,7 +1137,7 @@ static int run_band_phase(pw_engine* e, KernelArgs A, std::vector<BandPair>& pai
     B.run_max = e->band_max.as<int>();
     B.abort_flag = e->chain_abort.as<int>();
     B.max_out = e->band_out.as<float>();
-    const int grid = std::max(1, std::min(e->sm_count * per_sm, (int)((n + 3) / 4)));
+    const int grid = std::max(1, std::min(grid_cap(e, per_sm), (int)((n + 3) / 4)));
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);

@@ -310,6 +310,15 @@ extern "C" int pw_server_set_scoring(pw_server* s, const float* matrix, int dim,
     return PW_OK;
 }
 
+extern "C" int pw_server_tune(pw_server* s, int key, int64_t value) {
+    if (!s) return PW_ERR_ARG;
+    for (Worker& w : s->workers) {
+        const int rc = pw_set_tuning(w.engine, key, value);
+        if (rc != PW_OK) return server_fail(s, rc, pw_last_error(w.engine));
+    }
+    return PW_OK;
+}
+
 extern "C" int pw_server_load_db(pw_server* s, const uint8_t* residues, const int64_t* offsets, int32_t n,
                                  const int32_t* id_keys) {
     if (!s) return PW_ERR_ARG;

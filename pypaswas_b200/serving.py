@@ -108,6 +108,10 @@ class Server(object):
             self._check(self.lib.pw_server_release(self.handle, int(ticket)), "pw_server_release")
         return out
 
+    def tune(self, key, value):
+        """pw_set_tuning on every worker engine (e.g. _native.PW_TUNE_GRID_SHARE)."""
+        self._check(self.lib.pw_server_tune(self.handle, int(key), int(value)), "pw_server_tune")
+
     def stats(self):
         st = _native.PwServerStats()
         self._check(self.lib.pw_server_stats(self.handle, ctypes.byref(st)), "pw_server_stats")
