@@ -306,15 +306,14 @@ def main():
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > L2 (126 MB)
 
     chain = not args.no_chain
+    sampler = ClockSampler(local)
+    sampler.start()  # started before the warm-up: nvidia-smi is up when timing begins
     for _ in range(args.warmup):
         e.align(chain=chain)
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
-    sampler = ClockSampler(local)
-    sampler.start()
-    time.sleep(0.6)  # nvidia-smi start-up; samples before mark() are dropped
-    sampler.mark()
+    sampler.mark()  # samples before this point are dropped
     times, infos = [], []
     for _ in range(args.steps):
         flush.zero_()  # between timed iterations: L2 flushed

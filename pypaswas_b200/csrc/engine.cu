@@ -1727,6 +1727,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
             if ((c = download(e, metas, A.metas, (size_t)n_pairs)) != cudaSuccess) return cuda_fail(e, c, "copy metas");
         }
         const size_t first_rec = e->h_starts.size();
+        e->h_starts.reserve(first_rec + so.size());
         for (const StartOut& s : so) {
             const PairMeta& pm = metas[s.pair];
             const int mn = std::min(qlen[pm.query], tlen[pm.target]);
@@ -1752,15 +1753,17 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
             inf.truncated = 1;
         }
 
-        // walk
+        // walk; each kept hit reserves its column operations (ops offsets)
         int nh = 0;
         std::vector<DevHit> hh;
+        std::vector<char> ops;
         if (wave_starts > 0) {
             if ((c = e->hits.reserve(e->stream, wave_starts * sizeof(DevHit))) != cudaSuccess) return cuda_fail(e, c, "alloc hits");
             if ((c = e->hit_count.reserve(e->stream, 16)) != cudaSuccess) return cuda_fail(e, c, "alloc");
-            cudaMemsetAsync(e->hit_count.p, 0, sizeof(int), e->stream);
+            cudaMemsetAsync(e->hit_count.p, 0, 16, e->stream);
             TA.hits = e->hits.as<DevHit>();
             TA.hit_count = e->hit_count.as<int>();
+            TA.ops_total = (unsigned long long*)(e->hit_count.as<char>() + 8);
             TA.max_hits = (int)wave_starts;
             if (e->affine)
                 PW_LAUNCH(walk_kernel<true>, gb, tb, 0, e->stream, TA);
@@ -1768,30 +1771,32 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
                 PW_LAUNCH(walk_kernel<false>, gb, tb, 0, e->stream, TA);
             e->launches++;
             if ((c = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, c, "walk launch");
-            std::vector<int> cnt;
-            if ((c = download(e, cnt, TA.hit_count, 1)) != cudaSuccess) return cuda_fail(e, c, "walk");
-            nh = (int)std::min<int64_t>(cnt[0], wave_starts);
-            if ((c = download(e, hh, TA.hits, (size_t)nh)) != cudaSuccess) return cuda_fail(e, c, "copy hits");
-        }
-        // column operations of the kept hits
-        int64_t ops_total = 0;
-        for (int k = 0; k < nh; ++k) {
-            hh[k].ops_offset = ops_total;
-            ops_total += hh[k].n_cols;
+            std::vector<int64_t> cnt;
+            if ((c = download(e, cnt, TA.hit_count, 2)) != cudaSuccess) return cuda_fail(e, c, "walk");
+            nh = (int)std::min<int64_t>((int32_t)(cnt[0] & 0xffffffff), wave_starts);
+            const int64_t ops_total = cnt[1];
+            if (nh) {
+                // column operations of the kept hits, then hits and operations to the host
+                if ((c = e->ops.reserve(e->stream, std::max<int64_t>(ops_total, 16))) != cudaSuccess)
+                    return cuda_fail(e, c, "alloc ops");
+                TA.ops = e->ops.as<char>();
+                PW_LAUNCH(ops_kernel, (nh + 127) / 128, 128, 0, e->stream, TA, e->hits.as<DevHit>(), nh);
+                e->launches++;
+                if ((c = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, c, "ops launch");
+                if ((c = download(e, hh, TA.hits, (size_t)nh)) != cudaSuccess) return cuda_fail(e, c, "copy hits");
+                if ((c = download(e, ops, TA.ops, (size_t)ops_total)) != cudaSuccess) return cuda_fail(e, c, "copy ops");
+            }
         }
         if (nh) {
-            if ((c = upload(e, e->hits, hh)) != cudaSuccess) return cuda_fail(e, c, "upload hits");
-            if ((c = e->ops.reserve(e->stream, std::max<int64_t>(ops_total, 16))) != cudaSuccess) return cuda_fail(e, c, "alloc ops");
-            TA.ops = e->ops.as<char>();
-            PW_LAUNCH(ops_kernel, (nh + 127) / 128, 128, 0, e->stream, TA, e->hits.as<DevHit>(), nh);
-            e->launches++;
-            if ((c = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, c, "ops launch");
-            std::vector<char> ops;
-            if ((c = download(e, ops, TA.ops, (size_t)ops_total)) != cudaSuccess) return cuda_fail(e, c, "copy ops");
             const int64_t base = (int64_t)all_ops.size();
-            for (int k = 0; k < nh; ++k) hh[k].ops_offset += base;
-            all_ops.insert(all_ops.end(), ops.begin(), ops.end());
-            all_hits.insert(all_hits.end(), hh.begin(), hh.end());
+            if (all_hits.empty()) {
+                all_hits.swap(hh);
+                all_ops.swap(ops);
+            } else {
+                for (DevHit& h : hh) h.ops_offset += base;
+                all_ops.insert(all_ops.end(), ops.begin(), ops.end());
+                all_hits.insert(all_hits.end(), hh.begin(), hh.end());
+            }
         }
         cudaEventRecord(e->ev[3], e->stream);
         cudaStreamSynchronize(e->stream);

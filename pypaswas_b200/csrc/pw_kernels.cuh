@@ -522,6 +522,7 @@ struct TraceArgs {
     int* hit_count;
     int max_hits;
     char* ops;
+    unsigned long long* ops_total;  // column operations reserved so far (walk_kernel assigns ops offsets)
 };
 
 // Offset of cell (x, y) in the layout of the one-warp-per-pair direction sweep
@@ -729,7 +730,7 @@ __global__ void walk_kernel(TraceArgs A) {
                 o.n_cols = ncols;
                 o.end_x = st.x;
                 o.end_y = st.y;
-                o.ops_offset = -1;
+                o.ops_offset = (int64_t)atomicAdd(A.ops_total, (unsigned long long)ncols);
                 A.hits[h] = o;
             }
         }

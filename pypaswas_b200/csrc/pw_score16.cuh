@@ -149,6 +149,7 @@ __device__ __forceinline__ void sweep16(const uint8_t* qc, int lq4, const uint4*
         uint32_t bb_prev = 0;
         uint32_t cw_next = lq4 > 0 ? *(const uint32_t*)qc : 0u;
         uint4 v_next = has_up && lq4 > 0 ? bnd[0] : make_uint4(ge2, kNeg16x2, 0u, 0u);
+        uint4 v_next2 = has_up && lq4 > 1 ? bnd[kWarp] : make_uint4(ge2, kNeg16x2, 0u, 0u);
         for (int x4 = 0; x4 < lq4; x4 += 4) {
             const uint32_t cw = cw_next;
             if (x4 + 4 < lq4) cw_next = *(const uint32_t*)(qc + x4 + 4);
@@ -157,7 +158,8 @@ __device__ __forceinline__ void sweep16(const uint8_t* qc, int lq4, const uint4*
                 const int x = x4 + j;
                 const int a = (cw >> (8 * j)) & 0xff;
                 const uint4 v = v_next;
-                if (has_up && x + 1 < lq4) v_next = bnd[(int64_t)(x + 1) * kWarp];
+                v_next = v_next2;
+                if (has_up && x + 2 < lq4) v_next2 = bnd[(int64_t)(x + 2) * kWarp];
                 uint32_t mgup = v.x, yup = v.y, bup = v.z;
                 uint32_t bdiag = bb_prev;
                 bb_prev = bup;
@@ -334,6 +336,7 @@ __device__ __forceinline__ bool sweep16_chain(const uint8_t* qc, int lq4, int xm
         uint32_t bb_prev = 0;
         uint32_t cw_next = xm4 > 0 ? code_word(0) : pad4;
         uint4 v_next = has_up && xm4 > 0 ? __ldcg(&ring_in[0]) : make_uint4(ge2, kNeg16x2, 0u, 0u);
+        uint4 v_next2 = has_up && xm4 > 1 ? __ldcg(&ring_in[kWarp]) : make_uint4(ge2, kNeg16x2, 0u, 0u);
         for (int x4 = 0; x4 < xm4; x4 += 4) {
             if (!need_cols(min(x4 + kChainNeed, xm4))) return false;
             const uint32_t cw = cw_next;
@@ -343,7 +346,8 @@ __device__ __forceinline__ bool sweep16_chain(const uint8_t* qc, int lq4, int xm
                 const int x = x4 + j;
                 const int a = (cw >> (8 * j)) & 0xff;
                 const uint4 v = v_next;
-                if (has_up && x + 1 < xm4) v_next = __ldcg(&ring_in[(int64_t)(x + 1) * kWarp]);
+                v_next = v_next2;
+                if (has_up && x + 2 < xm4) v_next2 = __ldcg(&ring_in[(int64_t)(x + 2) * kWarp]);
                 uint32_t mgup = v.x, yup = v.y, bup = v.z;
                 uint32_t bdiag = bb_prev;
                 bb_prev = bup;
