@@ -1107,12 +1107,29 @@ static int run_band_phase(pw_engine* e, KernelArgs A, std::vector<BandPair>& pai
         sorted[k].ring_off = ring_elems;
         if (sorted[k].nbands > 1) ring_elems += 2 * (int64_t)e->pr.qlen[sorted[k].q];
     }
-    ChainPlan plan;
-    plan_chain_queue(nstr, xm, warps, 1, kBandLead, plan);
-    std::vector<int4> entries(plan.queue.size());
-    for (size_t k = 0; k < plan.queue.size(); ++k) {
-        const PlanEntry& p = plan.queue[k];
-        entries[k] = make_int4(p.item, p.chain >= 0 ? p.strip : 0, p.pred, 0);
+    std::vector<int4> entries;
+    if ((int64_t)sorted.size() * 2 >= warps) {
+        // many pairs: band-major order (every band 0, then every band 1, ...,
+        // longest pairs first within a band); a band's predecessor was handed
+        // out at least a whole band generation earlier, so nobody waits long
+        int maxb = 0;
+        for (const BandPair& bp : sorted) maxb = std::max(maxb, bp.nbands);
+        std::vector<int32_t> last(sorted.size(), -1);
+        for (int b = 0; b < maxb; ++b)
+            for (size_t k = 0; k < sorted.size(); ++k)
+                if (b < sorted[k].nbands) {
+                    entries.push_back(make_int4((int)k, b, last[k], 0));
+                    last[k] = (int32_t)entries.size() - 1;
+                }
+    } else {
+        // few (long) pairs: a list-scheduling plan pipelines each pair's bands
+        ChainPlan plan;
+        plan_chain_queue(nstr, xm, warps, 1, kBandLead, plan);
+        entries.resize(plan.queue.size());
+        for (size_t k = 0; k < plan.queue.size(); ++k) {
+            const PlanEntry& p = plan.queue[k];
+            entries[k] = make_int4(p.item, p.chain >= 0 ? p.strip : 0, p.pred, 0);
+        }
     }
     const size_t n = entries.size();
     if ((c = upload(e, e->band_pairs, sorted)) != cudaSuccess) return cuda_fail(e, c, "upload band pairs");

@@ -15,8 +15,9 @@
 // below polls that count (ld.acquire.gpu, bounded wait) and reads the ring
 // with ld.global.cg.  A ring row is rewritten by band b + 2 only after band
 // b + 1 has published progress past those columns, which it does only after
-// its lane 0 has read them.  The queue is planned like the chained strips
-// (pw_plan.h): every band after the band above it.
+// its lane 0 has read them.  In the queue every band comes after the band
+// above it: band-major when there are many pairs, otherwise planned like the
+// chained strips (pw_plan.h) so that the bands of a few long pairs pipeline.
 //
 // DIRS = false: pair maxima only (the score sweep of long pairs).
 // DIRS = true: the direction sweep of traced pairs: per cell the code byte of
