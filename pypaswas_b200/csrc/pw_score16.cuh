@@ -139,11 +139,13 @@ __device__ __forceinline__ void sweep16(const uint8_t* qc, int lq4, const uint4*
             }
         }
     } else {
-        uint32_t Mgl[S], Xl[S], Bl[S];
+        // Zl[r] = max(X + ext, M + gap_open) of the previous column: exactly
+        // this column's X (the sweep-axis gap chain), one row array instead of
+        // two (X and M + gap_open); M = 0 and X = -inf left of the matrix
+        uint32_t Zl[S], Bl[S];
 #pragma unroll
         for (int r = 0; r < S; ++r) {
-            Mgl[r] = ge2;     // M = 0 left of the matrix
-            Xl[r] = kNeg16x2;
+            Zl[r] = ge2;
             Bl[r] = 0;
         }
         uint32_t bb_prev = 0;
@@ -172,11 +174,10 @@ __device__ __forceinline__ void sweep16(const uint8_t* qc, int lq4, const uint4*
                         const int r = 4 * g + k;
                         const uint32_t mg = __viaddmax_s16x2(bdiag, sc[k], ge2);   // M + ge
                         const uint32_t y = __viaddmax_s16x2(yup, e2, mgup);
-                        const uint32_t xg = __viaddmax_s16x2(Xl[r], e2, Mgl[r]);
+                        const uint32_t xg = Zl[r];
                         const uint32_t bst = __vimax3_s16x2(__viaddmax_s16x2(mg, nge2, kNeg16x2), y, xg);
+                        Zl[r] = __viaddmax_s16x2(xg, e2, mg);
                         bdiag = Bl[r];
-                        Mgl[r] = mg;
-                        Xl[r] = xg;
                         Bl[r] = bst;
                         mgup = mg;
                         yup = y;
@@ -326,11 +327,10 @@ __device__ __forceinline__ bool sweep16_chain(const uint8_t* qc, int lq4, int xm
             if (has_down && (((x4 + 4) % kChainPublish) == 0 || x4 + 4 >= xm4)) chain_publish(prog_out, x4 + 4);
         }
     } else {
-        uint32_t Mgl[S], Xl[S], Bl[S];
+        uint32_t Zl[S], Bl[S];  // as in sweep16
 #pragma unroll
         for (int r = 0; r < S; ++r) {
-            Mgl[r] = ge2;
-            Xl[r] = kNeg16x2;
+            Zl[r] = ge2;
             Bl[r] = 0;
         }
         uint32_t bb_prev = 0;
@@ -360,11 +360,10 @@ __device__ __forceinline__ bool sweep16_chain(const uint8_t* qc, int lq4, int xm
                         const int r = 4 * g + k;
                         const uint32_t mg = __viaddmax_s16x2(bdiag, sc[k], ge2);
                         const uint32_t y = __viaddmax_s16x2(yup, e2, mgup);
-                        const uint32_t xg = __viaddmax_s16x2(Xl[r], e2, Mgl[r]);
+                        const uint32_t xg = Zl[r];
                         const uint32_t bst = __vimax3_s16x2(__viaddmax_s16x2(mg, nge2, kNeg16x2), y, xg);
+                        Zl[r] = __viaddmax_s16x2(xg, e2, mg);
                         bdiag = Bl[r];
-                        Mgl[r] = mg;
-                        Xl[r] = xg;
                         Bl[r] = bst;
                         mgup = mg;
                         yup = y;
