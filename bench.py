@@ -80,6 +80,24 @@ def workload(args):
     return w
 
 
+def reduce_max(x):
+    """Max of a float over the ranks of the default process group (identity
+    without one): the job's time is its slowest rank's."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_gcups(cells_per_rank, steps, seconds, world):
+    """Weak scaling: every rank aligns its own replica; GCUPS of the whole job."""
+    return world * cells_per_rank * steps / seconds / 1e9
+
+
 def dist_env():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), \
         int(os.environ.get("LOCAL_RANK", "0"))
@@ -327,13 +345,9 @@ def main():
         times.append(a.elapsed_time(b))
         infos.append(info.as_dict())
     clocks = sampler.stop()
-    t_ms = float(sum(times))
+    t_ms = reduce_max(float(sum(times)))
     step_stats = {"min": float(min(times)), "median": float(np.median(times)), "max": float(max(times))}
-    if world > 1:
-        tt = torch.tensor([t_ms], device="cuda")
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        t_ms = float(tt.item())
-    value = world * cells * args.steps / (t_ms * 1e-3) / 1e9
+    value = whole_job_gcups(cells, args.steps, t_ms * 1e-3, world)
     n_pairs = len(w.pairs) if w.pairs is not None else w.n_queries * len(w.targets)
     ms_per_step = t_ms / args.steps
 
@@ -360,7 +374,13 @@ def main():
 
     # end to end through the public driver, host records in, hits out
     e2e_w = w if w.queries is not None else w.head(E2E_READS)
-    e2e_value, h2d, d2h = (None, 0, 0) if args.no_e2e else _e2e(e2e_w, args.steps, local)
+    e2e_value, h2d, d2h = None, 0, 0
+    if not args.no_e2e:
+        if world > 1:
+            torch.distributed.barrier()
+        dt, h2d, d2h = _e2e(e2e_w, args.steps, local)
+        dt = reduce_max(dt)  # whole job: every rank's replica, the slowest rank's time
+        e2e_value = whole_job_gcups(e2e_w.cells, args.steps, dt, world)
 
     out = {"metric": "GCUPS", "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms_per_step, "step_ms": step_stats,
@@ -521,7 +541,7 @@ def _e2e(w, steps, device):
             d2h += int(aligner.smith_waterman.last_d2h_bytes)
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
-    return w.cells * steps / dt / 1e9, h2d, d2h
+    return dt, h2d, d2h
 
 
 if __name__ == "__main__":
