@@ -120,19 +120,22 @@ class HitList(object):
         keys = hit.keys()
         if keys is None:
             return
-        better_start = keys[0] in self.hits and self.hits[keys[0]].score < hit.score
-        better_end = keys[1] in self.hits and self.hits[keys[1]].score < hit.score
-        new = keys[0] not in self.hits and keys[1] not in self.hits
+        hits = self.hits
+        k0, k1 = keys[0], keys[1]
+        old0, old1 = hits.get(k0), hits.get(k1)
+        better_start = old0 is not None and old0.score < hit.score
+        better_end = old1 is not None and old1.score < hit.score
+        new = old0 is None and old1 is None
         if better_start or better_end or new:
-            if better_end and self.hits[keys[1]].keys()[2] in self.real_hits:
+            if better_end and old1.keys()[2] in self.real_hits:
                 # same end location: drop the previous hit's start entry
-                del self.real_hits[self.hits[keys[1]].keys()[2]]
-            self.hits[keys[0]] = hit
-            self.hits[keys[1]] = hit
+                del self.real_hits[old1.keys()[2]]
+            hits[k0] = hit
+            hits[k1] = hit
             self.real_hits[keys[2]] = hit
             if self.logger is not None:
-                self.logger.info("Added hit (query ID: {}, target ID: {}) to hitlist".format(
-                    hit.get_seq_id(), hit.get_target_id()))
+                self.logger.info("Added hit (query ID: %s, target ID: %s) to hitlist", hit.get_seq_id(),
+                                 hit.get_target_id())
         elif self.logger is not None:
-            self.logger.debug("Rejected hit (query ID: {}, target ID: {}) from addition to hitlist".format(
-                hit.get_seq_id(), hit.get_target_id()))
+            self.logger.debug("Rejected hit (query ID: %s, target ID: %s) from addition to hitlist",
+                              hit.get_seq_id(), hit.get_target_id())

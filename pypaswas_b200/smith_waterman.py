@@ -129,22 +129,70 @@ class SmithWatermanB200(object):
         return hitlist
 
     def _build_hits(self, hits, strbuf, sequences, targets, hit_list):
-        """Hit objects in walk order (SmithWaterman._print_alignments :822-838)."""
-        q_col = hits["query"].tolist()
-        t_col = hits["target"].tolist()
-        ss, se = hits["s_start"].tolist(), hits["s_end"].tolist()
-        ts_, te = hits["t_start"].tolist(), hits["t_end"].tolist()
+        """Hit objects in walk order (SmithWaterman._print_alignments :822-838).
+
+        Locations, ratios and the filter are evaluated for all hits at once
+        (float64, the same IEEE operations as the reference's Python floats);
+        when every location is valid the Hit objects are filled directly,
+        otherwise each Hit is built through its validating constructor, which
+        raises at the first invalid one like the reference."""
+        n_hits = len(hits)
+        if n_hits == 0:
+            return
+        q_col, t_col = hits["query"].astype(np.int64), hits["target"].astype(np.int64)
+        sp = np.array([getattr(r, "start_position", 0) for r in sequences], dtype=np.int64)
+        tp = np.array([getattr(r, "start_position", 0) for r in targets], dtype=np.int64)
+        qlen = np.array([r.original_length for r in sequences], dtype=np.int64)
+        tlen = np.array([r.original_length for r in targets], dtype=np.int64)
+        s0 = hits["s_start"].astype(np.int64) + sp[q_col]
+        s1 = hits["s_end"].astype(np.int64) + sp[q_col]
+        t0 = hits["t_start"].astype(np.int64) + tp[t_col]
+        t1 = hits["t_end"].astype(np.int64) + tp[t_col]
+        ql, tl = qlen[q_col], tlen[t_col]
+        valid = ((0 <= s0) & (s0 < s1) & (s1 < ql) & (0 <= t0) & (t0 < t1) & (t1 < tl)).all()
+        text = strbuf.decode("latin-1")
+        if not valid:
+            self._build_hits_checked(hits, text, sequences, targets, hit_list, s0, s1, t0, t1)
+            return
+        score = hits["score"].astype(np.float64)
+        mt, mm = hits["matches"].astype(np.int64), hits["mismatches"].astype(np.int64)
+        nc, so = hits["n_cols"].tolist(), hits["str_offset"].tolist()
+        span = (s1 - s0 + 1).astype(np.float64)
+        rel = score / np.minimum(ql, tl).astype(np.float64)
+        ident = mt.astype(np.float64) / span
+        cov = span / ql.astype(np.float64)
+        base = score / hits["n_cols"].astype(np.float64)
+        thr = self._filter_thresholds()
+        keep = np.nonzero((rel >= thr[0]) & (ident >= thr[1]) & (cov >= thr[2]) & (base >= thr[3]))[0].tolist()
+        for qi in set(q_col[keep].tolist()):
+            if not hasattr(sequences[qi], "distance"):
+                sequences[qi].distance = 0.0
+        cols = [c.tolist() for c in (q_col, t_col, s0, s1, t0, t1, score, mt, mm, rel, ident, cov, base)]
+        qc_, tc_, s0_, s1_, t0_, t1_, sc_, mt_, mm_, rel_, id_, cov_, base_ = cols
+        logger = self.logger
+        new = Hit.__new__
+        for k in keep:
+            n, o = nc[k], so[k]
+            h = new(Hit)
+            h.__dict__.update(
+                logger=logger, sequence_info=sequences[qc_[k]], target_info=targets[tc_[k]],
+                seq_location=(s0_[k], s1_[k]), target_location=(t0_[k], t1_[k]),
+                sequence_match=text[o:o + n], alignment=text[o + n:o + 2 * n], target_match=text[o + 2 * n:o + 3 * n],
+                score=sc_[k], matches=mt_[k], mismatches=mm_[k], query_identity=id_[k], query_coverage=cov_[k],
+                relative_score=rel_[k], base_score=base_[k], distance=None, rc=False)
+            hit_list.append(h)
+
+    def _build_hits_checked(self, hits, text, sequences, targets, hit_list, s0, s1, t0, t1):
+        q_col, t_col = hits["query"].tolist(), hits["target"].tolist()
+        s0, s1, t0, t1 = s0.tolist(), s1.tolist(), t0.tolist(), t1.tolist()
         sc = hits["score"].tolist()
         mt, mm = hits["matches"].tolist(), hits["mismatches"].tolist()
         nc, so = hits["n_cols"].tolist(), hits["str_offset"].tolist()
-        text = strbuf.decode("latin-1")
         for k in range(len(q_col)):
             seq_rec, tgt_rec = sequences[q_col[k]], targets[t_col[k]]
-            sp = getattr(seq_rec, "start_position", 0)
-            tp = getattr(tgt_rec, "start_position", 0)
             if not hasattr(seq_rec, "distance"):
                 seq_rec.distance = 0.0
-            hit = Hit(self.logger, seq_rec, tgt_rec, (ss[k] + sp, se[k] + sp), (ts_[k] + tp, te[k] + tp))
+            hit = Hit(self.logger, seq_rec, tgt_rec, (s0[k], s1[k]), (t0[k], t1[k]))
             n, o = nc[k], so[k]
             hit.set_sequence_match(text[o:o + n])
             hit.set_alignment(text[o + n:o + 2 * n])
@@ -153,10 +201,15 @@ class SmithWatermanB200(object):
             if self._filter_hit(hit):
                 hit_list.append(hit)
 
-    def _filter_hit(self, hit):
+    def _filter_thresholds(self):
         s = self.settings
-        return (hit.relative_score >= float(s.relative_score) and hit.query_identity >= float(s.query_identity)
-                and hit.query_coverage >= float(s.query_coverage) and hit.base_score >= float(s.base_score))
+        return (float(s.relative_score), float(s.query_identity), float(s.query_coverage), float(s.base_score))
+
+    def _filter_hit(self, hit):
+        """SmithWaterman._filter_hit (SmithWaterman.py:843-848)."""
+        thr = self._filter_thresholds()
+        return (hit.relative_score >= thr[0] and hit.query_identity >= thr[1] and hit.query_coverage >= thr[2]
+                and hit.base_score >= thr[3])
 
     def _progress(self, sequences, targets, t0):
         """GCUPS progress line of SmithWaterman.py:544-557."""
