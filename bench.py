@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain one-pair-per-launch leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
     ap.add_argument("--no-chain", action="store_true", help="16-bit sweep without chained strips (comparison)")
+    ap.add_argument("--tune", action="append", default=[], metavar="KEY=VALUE",
+                    help="engine tuning knob (chain_min, grid_share), e.g. --tune chain_min=250; "
+                         "without chain_min the autotuner picks it during the warm-up")
     ap.add_argument("--serve-seconds", type=float, default=6.0, help="length of each arrival stream of the serving leg")
     ap.add_argument("--serve-loads", default="0.3,0.5,0.7", help="offered loads (fractions of batched peak) swept")
     return ap.parse_args()
@@ -324,6 +327,16 @@ def main():
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > L2 (126 MB)
 
     chain = not args.no_chain
+    from pypaswas_b200 import _native
+    knobs = {"chain_min": _native.PW_TUNE_CHAIN_MIN, "grid_share": _native.PW_TUNE_GRID_SHARE}
+    tuning = {}
+    for kv in args.tune:
+        key, val = kv.split("=")
+        e.set_tuning(knobs[key], int(val))
+        tuning[key] = int(val)
+    if "chain_min" not in tuning and chain and w.pairs is None:
+        from pypaswas_b200.autotune import autotune
+        tuning["autotune"] = autotune(e)  # untimed: score sweeps on this workload
     sampler = ClockSampler(local)
     sampler.start()  # started before the warm-up: nvidia-smi is up when timing begins
     for _ in range(args.warmup):
@@ -395,7 +408,8 @@ def main():
                       "minimum_score": w.settings.minimum_score, "lower_limit_score": w.settings.lower_limit_score,
                       "filter_factor": w.settings.filter_factor,
                       "l2": "flushed between steps (256 MiB write); each step also writes >1e11 B of cell codes",
-                      "parallelism": "replica per GPU" if world > 1 else "single GPU"},
+                      "parallelism": "replica per GPU" if world > 1 else "single GPU",
+                      "tuning": tuning},
            "phases_ms": {"score": last["score_ms"], "trace": last["trace_ms"], "walk": last["walk_ms"],
                          "score_kernels": last["score_kernel_ms"], "trace_kernels": last["trace_kernel_ms"],
                          "host_setup": last["setup_ms"], "host_finish": last["finish_ms"], "call": last["total_ms"]},

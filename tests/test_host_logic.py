@@ -95,3 +95,32 @@ def test_serving_percentile_is_nearest_rank():
     assert percentile(v, 50) == 50 and percentile(v, 99) == 99 and percentile(v, 100) == 100
     assert percentile([7.0], 99) == 7.0
     assert percentile([3, 1, 2], 50) == 2
+
+
+def test_autotune_keeps_the_fastest_candidate():
+    from pypaswas_b200 import _native
+    from pypaswas_b200.autotune import autotune
+
+    class Info(object):
+        def __init__(self, ms):
+            self.score_kernel_ms = ms
+
+    class FakeEngine(object):
+        """Score-sweep time as a function of the chaining threshold."""
+        cost = {250: 9.0, 500: 7.5, 1000: 8.0, 2000: 7.5}
+
+        def __init__(self):
+            self.tune = {}
+
+        def set_tuning(self, key, value):
+            self.tune[key] = value
+
+        def align(self, score_only=False):
+            assert score_only
+            return Info(self.cost[self.tune[_native.PW_TUNE_CHAIN_MIN]])
+
+    e = FakeEngine()
+    r = autotune(e)
+    assert r["chain_min"] == 500  # ties go to the smaller value
+    assert e.tune[_native.PW_TUNE_CHAIN_MIN] == 500
+    assert r["score_kernel_ms"] == FakeEngine.cost
