@@ -177,6 +177,10 @@ int pw_set_wave_limit(pw_engine* e, int64_t bytes);
  *                       several engines (the serving loop's workers) can then
  *                       keep kernels resident side by side */
 #define PW_TUNE_GRID_SHARE 1
+/*   PW_TUNE_SEGMENT     chained 16-bit score sweep: queue entries per launch
+ *                       (default all in one); shorter launches let other
+ *                       engines' kernels in between (the serving loop) */
+#define PW_TUNE_SEGMENT 2
 int pw_set_tuning(pw_engine* e, int key, int64_t value);
 
 /* Pair maxima (the last block of the maxima chain, default_main.cu:591),

@@ -31,6 +31,7 @@ PW_FLAG_INT32 = 4
 PW_FLAG_NO_CHAIN = 8
 PW_TUNE_CHAIN_MIN = 0
 PW_TUNE_GRID_SHARE = 1
+PW_TUNE_SEGMENT = 2
 
 # symbols the header declares, checked by the CPU test-suite
 EXPORTED_SYMBOLS = (

@@ -830,7 +830,7 @@ static cudaError_t launch_s16_chain(pw_engine* e, Score16Args A) {
     cudaError_t c = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem);
     if (c != cudaSuccess) return c;
     per_sm = std::max(1, std::min(per_sm, 16));
-    const int grid = std::max(1, std::min(grid_cap(e, per_sm), (A.n_items + 3) / 4));
+    const int grid = std::max(1, std::min(grid_cap(e, per_sm), (A.n_items - A.item_base + 3) / 4));
     PW_LAUNCH(kern, grid, 128, smem, e->stream, A);
     e->launches++;
     return cudaGetLastError();
@@ -989,12 +989,22 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uin
         const int n = begin[k + 1] - begin[k];
         if (n <= 0) continue;
         if (k == kS32Multi && chained) {
+            // the queue in consecutive segments, one launch each (PW_TUNE_SEGMENT):
+            // every strip's predecessor is in the same or an earlier segment
             S.items = e->chain_items.as<WorkItem>();
-            S.n_items = S.n_chain_items;
             S.counter = e->counter.as<int>() + k;
-            c = e->affine ? launch_s16_chain<32, true>(e, S) : launch_s16_chain<32, false>(e, S);
-            if (c != cudaSuccess) return cuda_fail(e, c, "score16 chain launch");
-            inf.score_launches++;
+            const int total = S.n_chain_items;
+            const int seg = e->tune[PW_TUNE_SEGMENT] > 0 ? (int)std::min<int64_t>(e->tune[PW_TUNE_SEGMENT], total)
+                                                          : total;
+            for (int base = 0; base < total; base += std::max(seg, 1)) {
+                S.item_base = base;
+                S.n_items = std::min(total, base + std::max(seg, 1));
+                if (base > 0 && (c = cudaMemsetAsync(S.counter, 0, sizeof(int), e->stream)) != cudaSuccess)
+                    return cuda_fail(e, c, "reset counter");
+                c = e->affine ? launch_s16_chain<32, true>(e, S) : launch_s16_chain<32, false>(e, S);
+                if (c != cudaSuccess) return cuda_fail(e, c, "score16 chain launch");
+                inf.score_launches++;
+            }
             continue;
         }
         S.items = e->p1_items.as<WorkItem>() + begin[k];

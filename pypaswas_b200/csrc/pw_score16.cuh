@@ -58,6 +58,7 @@ struct Score16Args {
     int pad_code;                // lane code of the padding residue
     int* abort_flag;             // set when a wait runs out of time; every waiting warp then gives up
     int n_chain_items;           // host-side bookkeeping: entries of the chained launch
+    int item_base;               // chained launch: first queue entry of this launch (entries [item_base, n_items))
     int* ovf_count;              // pairs reported as NaN (16-bit limit reached)
 };
 
@@ -391,7 +392,7 @@ __global__ void __launch_bounds__(128, 3) score16_chain_kernel(Score16Args A) {
     uint4* bnd = A.bnd_pool + warp_global * A.bnd_slot + lane;
     for (;;) {
         int it = 0;
-        if (lane == 0) it = atomicAdd(A.counter, 1);
+        if (lane == 0) it = A.item_base + atomicAdd(A.counter, 1);
         it = __shfl_sync(0xffffffffu, it, 0);
         if (it >= A.n_items) break;
         const WorkItem W = A.items[it];

@@ -175,11 +175,12 @@ def test_many_short_targets_strip_direction_sweep(engine_lib, oracle_mod, aff):
 
 
 @pytest.mark.parametrize("kind", ["dna", "protein", "protein_linear"])
-@pytest.mark.parametrize("chain_min", [0, 1])
-def test_chained_strips_match_one_warp_items_and_oracle(engine_lib, oracle_mod, kind, chain_min):
+@pytest.mark.parametrize("chain_min,segment", [(0, 0), (1, 0), (1, 37)])
+def test_chained_strips_match_one_warp_items_and_oracle(engine_lib, oracle_mod, kind, chain_min, segment):
     """Multi-strip items cut into chained strips (the default share, and with
-    chain_min 1 nearly every multi-strip item) give the same pair maxima as
-    the one-warp items and the oracle, in both lane orientations."""
+    chain_min 1 nearly every multi-strip item; segment 37 splits the queue
+    into launches of 37 entries, so chains cross launches) give the same pair
+    maxima as the one-warp items and the oracle, in both lane orientations."""
     from pypaswas_b200 import _native, scores
     rng = np.random.default_rng({"dna": 5, "protein": 6, "protein_linear": 7}[kind] * 10 + chain_min)
     alphabet = cases.DNA if kind == "dna" else cases.PROTEIN
@@ -199,6 +200,7 @@ def test_chained_strips_match_one_warp_items_and_oracle(engine_lib, oracle_mod, 
             e.set_queries([s.encode() for s in q], np.arange(nq))
             e.set_targets([s.encode() for s in t], np.arange(nt) + nq)
             e.set_tuning(_native.PW_TUNE_CHAIN_MIN, chain_min)
+            e.set_tuning(_native.PW_TUNE_SEGMENT, segment)
             e.align(score_only=True)
             chained = e.pair_max()
             e.align(score_only=True, chain=False)
