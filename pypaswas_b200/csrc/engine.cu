@@ -9,6 +9,7 @@
 //                 column operations of each kept hit
 // The host only builds work lists, sizes memory waves and formats results.
 #include <cuda_runtime.h>
+#include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 #include <chrono>
@@ -164,11 +165,6 @@ struct Prepared {
     bool t_int8 = true;          // transposed target rows: the same
 };
 
-struct StartRec {  // one starting point (emission order sortable)
-    int32_t query, target, x, y;
-    float score;
-    float max_score, pos_score;
-};
 
 }  // namespace
 
@@ -193,6 +189,7 @@ struct pw_engine {
     DevBuf q_res, t_ccodes, t_order, cmat_t8, cmat_tf;  // the other orientation's encodings
     DevBuf cmat_i8, cmat_f, pair_max, items, items_alt, counter, bnd_pool, q_order2;
     DevBuf band_pairs, band_entries, band_prog, band_max, band_ring, band_out;  // band sweep (pw_band.cuh)
+    DevBuf scan_tmp;  // CUB scan scratch
     DevBuf chain_items, chain_info, chain_prog, chain_max, chain_ring_off, chain_ring, chain_abort, p1_items;
     // plan of the 16-bit score phase (work items, classes, chain queue), kept
     // on the device and reused while inputs, scoring, flags and tuning stay
@@ -1735,31 +1732,41 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
             PW_LAUNCH(collect_kernel<false>, gb, tb, 0, e->stream, TA);
         e->launches++;
         if ((c = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, c, "collect launch");
-        std::vector<int32_t> ns;
-        if ((c = download(e, ns, TA.n_starts, (size_t)n_pairs)) != cudaSuccess) return cuda_fail(e, c, "collect");
+        // packed start offsets: exclusive scan of the per-pair counts on the device
+        {
+            size_t tmp = 0;
+            cub::DeviceScan::ExclusiveScan(nullptr, tmp, TA.n_starts, (int64_t*)nullptr, cub::Sum(), (int64_t)0,
+                                           (int)n_pairs, e->stream);
+            if ((c = e->start_off.reserve(e->stream, (size_t)(n_pairs + 1) * sizeof(int64_t))) != cudaSuccess ||
+                (c = e->scan_tmp.reserve(e->stream, std::max<size_t>(tmp, 16))) != cudaSuccess)
+                return cuda_fail(e, c, "alloc start offsets");
+            tmp = e->scan_tmp.bytes;
+            if ((c = cub::DeviceScan::ExclusiveScan(e->scan_tmp.p, tmp, TA.n_starts, e->start_off.as<int64_t>(),
+                                                    cub::Sum(), (int64_t)0, (int)n_pairs, e->stream)) != cudaSuccess)
+                return cuda_fail(e, c, "scan start counts");
+        }
         cudaEventRecord(e->ev[2], e->stream);
-        std::vector<int64_t> soff(n_pairs + 1, 0);
-        for (int64_t p = 0; p < n_pairs; ++p) soff[p + 1] = soff[p] + ns[p];
-        const int64_t wave_starts = soff[n_pairs];
-        if ((c = upload(e, e->start_off, soff)) != cudaSuccess) return cuda_fail(e, c, "upload start offsets");
+        int64_t last_off = 0;
+        int32_t last_n = 0;
+        if ((c = cudaMemcpyAsync(&last_off, e->start_off.as<int64_t>() + n_pairs - 1, sizeof(int64_t),
+                                 cudaMemcpyDeviceToHost, e->stream)) != cudaSuccess ||
+            (c = cudaMemcpyAsync(&last_n, TA.n_starts + n_pairs - 1, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                 e->stream)) != cudaSuccess ||
+            (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
+            return cuda_fail(e, c, "collect");
+        const int64_t wave_starts = last_off + last_n;
         TA.start_off = e->start_off.as<int64_t>();
-        std::vector<StartOut> so;
-        std::vector<PairMeta> metas;
+        const size_t first_rec = e->h_starts.size();
         if (wave_starts > 0) {
-            if ((c = e->starts.reserve(e->stream, wave_starts * sizeof(StartOut))) != cudaSuccess) return cuda_fail(e, c, "alloc");
-            PW_LAUNCH(gather_kernel, gb, tb, 0, e->stream, TA, e->starts.as<StartOut>());
+            if ((c = e->starts.reserve(e->stream, wave_starts * sizeof(StartRec))) != cudaSuccess) return cuda_fail(e, c, "alloc");
+            PW_LAUNCH(gather_kernel, gb, tb, 0, e->stream, TA, e->starts.as<StartRec>());
             e->launches++;
             if ((c = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, c, "gather launch");
-            if ((c = download(e, so, e->starts.p, (size_t)wave_starts)) != cudaSuccess) return cuda_fail(e, c, "copy starts");
-            if ((c = download(e, metas, A.metas, (size_t)n_pairs)) != cudaSuccess) return cuda_fail(e, c, "copy metas");
-        }
-        const size_t first_rec = e->h_starts.size();
-        e->h_starts.reserve(first_rec + so.size());
-        for (const StartOut& s : so) {
-            const PairMeta& pm = metas[s.pair];
-            const int mn = std::min(qlen[pm.query], tlen[pm.target]);
-            const float pos = (float)(e->highest * (double)mn * e->filter_factor);
-            e->h_starts.push_back(StartRec{pm.query, pm.target, s.x, s.y, s.score, pm.max_f, pos});
+            e->h_starts.resize(first_rec + (size_t)wave_starts);
+            if ((c = cudaMemcpyAsync(e->h_starts.data() + first_rec, e->starts.p, wave_starts * sizeof(StartRec),
+                                     cudaMemcpyDeviceToHost, e->stream)) != cudaSuccess ||
+                (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
+                return cuda_fail(e, c, "copy starts");
         }
         total_starts += wave_starts;
         TA.allowed = nullptr;

@@ -525,8 +525,8 @@ struct TraceArgs {
     unsigned long long* ops_total;  // column operations reserved so far (walk_kernel assigns ops offsets)
 };
 
-// Offset of cell (x, y) in the layout of the one-warp-per-pair direction sweep
-// (pw_trace_warp.cuh): [band of 256 rows][step][lane][8 rows], step = x + lane.
+// Offset of cell (x, y) in the layout of the band direction sweep
+// (pw_band.cuh): [band of 256 rows][step][lane][8 rows], step = x + lane.
 __host__ __device__ __forceinline__ int64_t warp_layout_offset(int x, int y, int lq) {
     const int band = y >> 8, l = (y & 255) >> 3, r = y & 7;
     const int64_t nsteps = (int64_t)lq + 31;
@@ -770,23 +770,36 @@ __global__ void ops_kernel(TraceArgs A, const DevHit* hits, int n_hits) {
 
 // Packs every pair's ordered starting points into one array (pair slot, cell,
 // score) so that the host reads only what exists.
-struct StartOut {
-    int32_t pair, x, y;
+// One starting point as the host orders and reports it (StartingPoint of
+// default_main.cu:66-76 with the pair resolved to query / target indices).
+struct StartRec {
+    int32_t query, target, x, y;
     float score;
+    float max_score, pos_score;
 };
 
-__global__ void gather_kernel(TraceArgs A, StartOut* out) {
+// Starting points of every pair, packed by start_off (an exclusive scan of
+// n_starts), with the pair's maximum and maxPossibleScore
+// (fp32(highest * min(len_q, len_t) * filter_factor) in double,
+// SmithWatermanCuda.py:269-275).
+__global__ void gather_kernel(TraceArgs A, StartRec* out) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= A.n_pairs) return;
     const Cand* cl = A.cands + A.cand_base[p];
     const int m = A.n_starts[p];
     const int64_t o = A.start_off[p];
+    const PairMeta pm = A.metas[p];
+    const int lq = A.q.len[pm.query], lt = A.t.len[pm.target];
+    const float pos = (float)(A.P.highest * (double)(lq < lt ? lq : lt) * A.P.filter_factor);
     for (int k = 0; k < m; ++k) {
-        StartOut s;
-        s.pair = p;
+        StartRec s;
+        s.query = pm.query;
+        s.target = pm.target;
         s.x = cl[k].x;
         s.y = cl[k].y;
         s.score = cl[k].score_f;
+        s.max_score = pm.max_f;
+        s.pos_score = pos;
         out[o + k] = s;
     }
 }
