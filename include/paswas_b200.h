@@ -81,7 +81,8 @@ typedef struct {
     double total_ms;        /* host wall time of the whole call */
     int32_t score_path;     /* score sweep used: 0 16-bit strips, 1 32-bit / fp32 strips, 2 bands (pw_set_pairs
                                or few long sequences) */
-    int32_t reserved_;
+    int32_t dual_lanes;     /* 16-bit score sweep in the dual-lane form: each strip against two lane
+                               sequences per lane (1) instead of two strips against one (0) */
 } pw_run_info;
 
 /* Creates an engine on CUDA device `device`.
@@ -181,6 +182,12 @@ int pw_set_wave_limit(pw_engine* e, int64_t bytes);
  *                       (default all in one); shorter launches let other
  *                       engines' kernels in between (the serving loop) */
 #define PW_TUNE_SEGMENT 2
+/*   PW_TUNE_DUAL        16-bit score sweep form: 1 always dual lanes (one strip
+ *                       against two lane sequences per lane), 2 never (two
+ *                       strips against one lane sequence), 0 the cheaper of the
+ *                       two by the cell-slot cost model (dual lanes win when
+ *                       few sequences sit on the strip side, e.g. one query) */
+#define PW_TUNE_DUAL 3
 int pw_set_tuning(pw_engine* e, int key, int64_t value);
 
 /* Pair maxima (the last block of the maxima chain, default_main.cu:591),

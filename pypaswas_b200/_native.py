@@ -32,6 +32,7 @@ PW_FLAG_NO_CHAIN = 8
 PW_TUNE_CHAIN_MIN = 0
 PW_TUNE_GRID_SHARE = 1
 PW_TUNE_SEGMENT = 2
+PW_TUNE_DUAL = 3
 
 # symbols the header declares, checked by the CPU test-suite
 EXPORTED_SYMBOLS = (
@@ -73,7 +74,7 @@ class PwRunInfo(ctypes.Structure):
                 ("overflow_pairs", ctypes.c_int64), ("traced_cells", ctypes.c_int64),
                 ("warp_pairs", ctypes.c_int64), ("cand_overflow_pairs", ctypes.c_int64),
                 ("setup_ms", ctypes.c_double), ("finish_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
-                ("score_path", ctypes.c_int32), ("reserved_", ctypes.c_int32)]
+                ("score_path", ctypes.c_int32), ("dual_lanes", ctypes.c_int32)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

@@ -195,9 +195,9 @@ struct pw_engine {
     // on the device and reused while inputs, scoring, flags and tuning stay
     struct {
         bool valid = false;
-        int64_t qg = 0, tg = 0, sg = 0, tune = 0, share = 0;
+        int64_t qg = 0, tg = 0, sg = 0, tune = 0, share = 0, dual_mode = 0;
         uint32_t flags = 0;
-        bool trans = false, chained = false;
+        bool trans = false, chained = false, dual = false;
         int begin[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         int xm_multi = 4;
         int n_chain_items = 0;
@@ -736,10 +736,10 @@ static void order_by_class(std::vector<WorkItem>& items, std::vector<int>& cls, 
 
 
 // ------------------------------------------------------------ 16-bit phase 1
-template <int S, bool AFF, bool MULTI>
+template <int S, bool AFF, bool MULTI, bool DL>
 static cudaError_t launch_s16(pw_engine* e, Score16Args A) {
-    auto kern = score16_kernel<S, AFF, MULTI>;
-    const int smem = 4 * (S / 4) * A.alpha1 * (int)sizeof(uint4);
+    auto kern = score16_kernel<S, AFF, MULTI, DL>;
+    const int smem = 4 * (S / 4) * A.alpha1 * prof_entry_bytes<DL>();
     if (smem > 48 * 1024) {
         cudaError_t c = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (c != cudaSuccess) return c;
@@ -754,16 +754,17 @@ static cudaError_t launch_s16(pw_engine* e, Score16Args A) {
     return cudaGetLastError();
 }
 
+template <bool DL>
 static cudaError_t launch_s16_class(pw_engine* e, int cls, bool affine, const Score16Args& A) {
     if (affine) {
-        if (cls == kS16) return launch_s16<16, true, false>(e, A);
-        if (cls == kS32) return launch_s16<32, true, false>(e, A);
-        return launch_s16<32, true, true>(e, A);
+        if (cls == kS16) return launch_s16<16, true, false, DL>(e, A);
+        if (cls == kS32) return launch_s16<32, true, false, DL>(e, A);
+        return launch_s16<32, true, true, DL>(e, A);
     }
-    if (cls == kS16) return launch_s16<16, false, false>(e, A);
-    if (cls == kS32) return launch_s16<32, false, false>(e, A);
-    if (cls == kS64) return launch_s16<64, false, false>(e, A);
-    return launch_s16<32, false, true>(e, A);
+    if (cls == kS16) return launch_s16<16, false, false, DL>(e, A);
+    if (cls == kS32) return launch_s16<32, false, false, DL>(e, A);
+    if (cls == kS64) return launch_s16<64, false, false, DL>(e, A);
+    return launch_s16<32, false, true, DL>(e, A);
 }
 
 // Plans the multi-strip launch.  Items whose sweep cost (columns x strips)
@@ -815,10 +816,10 @@ static int setup_chains(pw_engine* e, const std::vector<WorkItem>& items, int i0
     return PW_OK;
 }
 
-template <int S, bool AFF>
+template <int S, bool AFF, bool DL>
 static cudaError_t launch_s16_chain(pw_engine* e, Score16Args A) {
-    auto kern = score16_chain_kernel<S, AFF>;
-    const int smem = 4 * (S / 4) * A.alpha1 * (int)sizeof(uint4);
+    auto kern = score16_chain_kernel<S, AFF, DL>;
+    const int smem = 4 * (S / 4) * A.alpha1 * prof_entry_bytes<DL>();
     if (smem > 48 * 1024) {
         cudaError_t c = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (c != cudaSuccess) return c;
@@ -845,6 +846,22 @@ static double orientation_cost(const std::vector<int32_t>& strip_len, const std:
     return strips * lane_groups * 2 * kWarp;
 }
 
+// Cell-slot cost of the dual-lane form: every strip alone, against lane
+// groups taken 64 at a time (two 32-lane groups in the low and high halves).
+static double dual_cost(const std::vector<int32_t>& strip_len, const std::vector<int32_t>& lane_len,
+                        const std::vector<int32_t>& lane_order) {
+    double lane_pairs = 0;
+    for (size_t g = 0; g < lane_order.size(); g += 2 * kWarp) lane_pairs += lane_len[lane_order[g]];
+    double strips = 0;
+    for (int32_t l : strip_len) strips += l;
+    return strips * lane_pairs * 2 * kWarp;
+}
+
+// Relative cost of a dual-lane cell slot: its profile fetch interleaves two
+// residues' words (two 64-bit shared loads and four byte permutes per four
+// rows instead of one 128-bit load).
+constexpr double kDualSlotCost = 1.15;
+
 // Pair maxima with the 16-bit dual-pair sweep.  Returns the device time of
 // the sweep launches in *kernel_ms.  Pairs whose maximum could overflow
 // 16-bit halves come back as NaN; they are recomputed by the 32-bit sweep.
@@ -855,17 +872,35 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uin
     const uint32_t pflags = flags & PW_FLAG_NO_CHAIN;
     const bool reuse = P1.valid && P1.qg == e->q_gen && P1.tg == e->t_gen && P1.sg == e->s_gen &&
                        P1.flags == pflags && P1.tune == e->tune[PW_TUNE_CHAIN_MIN] &&
-                       P1.share == e->tune[PW_TUNE_GRID_SHARE];
+                       P1.share == e->tune[PW_TUNE_GRID_SHARE] && P1.dual_mode == e->tune[PW_TUNE_DUAL];
     cudaError_t c;
     if (!reuse) {
         const double t_plan = wall_ms();
         P1.valid = false;
-        bool trans = false;
-        if (pr.s16_q && pr.s16_t)
-            trans = orientation_cost(pr.qlen, pr.order, pr.tlen, pr.order_t) <
-                    orientation_cost(pr.tlen, pr.order_t, pr.qlen, pr.order);
-        else
-            trans = pr.s16_t;
+        // four forms: targets or queries as strips, strip pairs or dual lanes
+        // (PW_TUNE_DUAL: 1 always dual lanes, 2 never, else the cheaper form)
+        bool trans = false, dual = false;
+        {
+            const int64_t dm = e->tune[PW_TUNE_DUAL];
+            double best = -1;
+            for (int o = 0; o < 2; ++o) {
+                if (o == 1 ? !pr.s16_t : !pr.s16_q) continue;
+                const bool tr = o == 1;
+                const auto& sl = tr ? pr.qlen : pr.tlen;
+                const auto& so = tr ? pr.order : pr.order_t;
+                const auto& ll = tr ? pr.tlen : pr.qlen;
+                const auto& lo = tr ? pr.order_t : pr.order;
+                for (int d = 0; d < 2; ++d) {
+                    if ((d == 1 && dm == 2) || (d == 0 && dm == 1)) continue;
+                    const double cst = d ? dual_cost(sl, ll, lo) * kDualSlotCost : orientation_cost(sl, so, ll, lo);
+                    if (best < 0 || cst < best) {
+                        best = cst;
+                        trans = tr;
+                        dual = d == 1;
+                    }
+                }
+            }
+        }
         const std::vector<int32_t>& strip_len = trans ? pr.qlen : pr.tlen;
         const std::vector<int32_t>& strip_order = trans ? pr.order : pr.order_t;
         const std::vector<int32_t>& lane_len = trans ? pr.tlen : pr.qlen;
@@ -874,16 +909,18 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uin
         std::vector<WorkItem> items;
         std::vector<int> cls;
         std::vector<int64_t> cost;
-        for (int i = 0; i < n_strip; i += 2) {
-            const int sa = strip_order[i], sb = i + 1 < n_strip ? strip_order[i + 1] : -1;
+        const int strip_step = dual ? 1 : 2, lane_step = dual ? 2 * kWarp : kWarp;
+        for (int i = 0; i < n_strip; i += strip_step) {
+            const int sa = strip_order[i], sb = !dual && i + 1 < n_strip ? strip_order[i + 1] : -1;
             const int ls = std::max(strip_len[sa], sb >= 0 ? strip_len[sb] : 0);
-            for (int g = 0; g < n_lane; g += kWarp) {
+            for (int g = 0; g < n_lane; g += lane_step) {
                 WorkItem w;
                 memset(&w, 0, sizeof(w));
                 w.target = sa;
                 w.index = sb;
                 w.first = g;
                 w.lanes = std::min(kWarp, n_lane - g);
+                w.lanes_hi = dual ? std::max(0, std::min(kWarp, n_lane - g - kWarp)) : 0;
                 w.xmax = lane_len[lane_order[g]];
                 const int k = pick_class(ls, e->affine);
                 w.S = class_S(k);
@@ -912,8 +949,9 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uin
         P1.n_chain_items = 0;
         if (P1.chained) {
             int per_sm = 0;
-            const int smem = 4 * 8 * ((trans ? pr.alpha_t : pr.alpha) + 1) * (int)sizeof(uint4);
-            auto kern = e->affine ? score16_chain_kernel<32, true> : score16_chain_kernel<32, false>;
+            const int smem = 4 * 8 * ((trans ? pr.alpha_t : pr.alpha) + 1) * (dual ? 8 : 16);
+            auto kern = e->affine ? (dual ? score16_chain_kernel<32, true, true> : score16_chain_kernel<32, true, false>)
+                                  : (dual ? score16_chain_kernel<32, false, true> : score16_chain_kernel<32, false, false>);
             if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
             if ((c = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem)) != cudaSuccess)
                 return cuda_fail(e, c, "occupancy");
@@ -922,6 +960,8 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uin
             if (rc != PW_OK) return rc;
         }
         P1.trans = trans;
+        P1.dual = dual;
+        P1.dual_mode = e->tune[PW_TUNE_DUAL];
         for (int k = 0; k <= kNumClasses; ++k) P1.begin[k] = begin[k];
         P1.xm_multi = xm;
         P1.qg = e->q_gen;
@@ -935,8 +975,10 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uin
     }
     const bool trans = P1.trans;
     const bool chained = P1.chained;
+    const bool dual = P1.dual;
     const int* begin = P1.begin;
     inf.orientation = trans ? 1 : 0;
+    inf.dual_lanes = dual ? 1 : 0;
     Score16Args S;
     memset(&S, 0, sizeof(S));
     S.lane_codes = trans ? e->t_ccodes.as<uint8_t>() : e->q_codes.as<uint8_t>();
@@ -955,6 +997,7 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uin
     S.pair_max = A32.pair_max;
     S.stride_strip = trans ? nt : 1;
     S.stride_lane = trans ? 1 : nt;
+    S.pad_code = S.alpha1 - 1;
     if (begin[kS32Multi + 1] > begin[kS32Multi]) {
         const int64_t slot = (int64_t)P1.xm_multi * kWarp;
         if ((c = e->bnd_pool.reserve(e->stream, (size_t)slot * e->sm_count * 16 * 4 * sizeof(uint4))) != cudaSuccess)
@@ -971,7 +1014,6 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uin
         S.ring = e->chain_ring.as<uint4>();
         S.progress = e->chain_prog.as<int>();
         S.run_max = e->chain_max.as<uint32_t>();
-        S.pad_code = S.alpha1 - 1;
         S.abort_flag = e->chain_abort.as<int>();
         S.n_chain_items = P1.n_chain_items;
         if ((c = cudaMemsetAsync(e->chain_prog.p, 0, (size_t)P1.n_chain_items * sizeof(int), e->stream)) != cudaSuccess ||
@@ -998,7 +1040,8 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uin
                 S.n_items = std::min(total, base + std::max(seg, 1));
                 if (base > 0 && (c = cudaMemsetAsync(S.counter, 0, sizeof(int), e->stream)) != cudaSuccess)
                     return cuda_fail(e, c, "reset counter");
-                c = e->affine ? launch_s16_chain<32, true>(e, S) : launch_s16_chain<32, false>(e, S);
+                c = e->affine ? (dual ? launch_s16_chain<32, true, true>(e, S) : launch_s16_chain<32, true, false>(e, S))
+                              : (dual ? launch_s16_chain<32, false, true>(e, S) : launch_s16_chain<32, false, false>(e, S));
                 if (c != cudaSuccess) return cuda_fail(e, c, "score16 chain launch");
                 inf.score_launches++;
             }
@@ -1007,7 +1050,8 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uin
         S.items = e->p1_items.as<WorkItem>() + begin[k];
         S.n_items = n;
         S.counter = e->counter.as<int>() + k;
-        if ((c = launch_s16_class(e, k, e->affine, S)) != cudaSuccess) return cuda_fail(e, c, "score16 launch");
+        c = dual ? launch_s16_class<true>(e, k, e->affine, S) : launch_s16_class<false>(e, k, e->affine, S);
+        if (c != cudaSuccess) return cuda_fail(e, c, "score16 launch");
         inf.score_launches++;
     }
     cudaEventRecord(b, e->stream);

@@ -58,7 +58,7 @@ struct WorkItem {
     int32_t index;         // position of the item in its wave (phase 2); 16-bit sweep: second strip
     int32_t S;             // strip height of the item's sweep
     int32_t orient;        // 0: targets are the strips, queries the lanes; 1: the reverse
-    int32_t pad_;
+    int32_t lanes_hi;      // 16-bit dual-lane sweep: lanes of the second group (sorted positions first + 32 ...)
     int64_t dir_base;      // byte offset of the group's cell codes (phase 2)
     int64_t pair_base;     // index of lane 0's per-pair slot (phase 2)
 };

@@ -85,6 +85,57 @@ __device__ __forceinline__ void build_profile16(uint4* prof, const int8_t* cmat,
     }
 }
 
+// Dual-lane form: one strip sequence against two lane sequences per lane (the
+// lanes' own group in the low halves, the next 32-lane group in the high
+// halves).  The halves then read different lane residues, so the profile
+// holds plain 16-bit scores, [row group][lane residue] -> 4 rows in a uint2,
+// and the sweep interleaves the two residues' words with byte permutes.
+template <int S>
+__device__ __forceinline__ void build_profile16_dual(uint2* prof, const int8_t* cmat, const uint8_t* ra, int y0,
+                                                     int la, int alpha1, int dim, int shift, int lane) {
+    const int n = (S / 4) * alpha1;
+    for (int idx = lane; idx < n; idx += kWarp) {
+        const int g = idx / alpha1, a = idx % alpha1;
+        int v[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int y = y0 + 4 * g + k;
+            v[k] = (y < la ? (int)cmat[a * dim + ra[y]] : -128) + shift;
+        }
+        prof[idx] = make_uint2(pack16x2(v[0], v[1]), pack16x2(v[2], v[3]));
+    }
+}
+
+// The 16x2 scores of rows 4g .. 4g + 3: profile entries `ia` (low halves) and
+// `ib` (high halves; the dual-lane form only).
+template <bool DL>
+__device__ __forceinline__ void fetch16(const void* prof, int ia, int ib, uint32_t (&sc)[4]) {
+    if constexpr (!DL) {
+        const uint4 w = ((const uint4*)prof)[ia];
+        sc[0] = w.x;
+        sc[1] = w.y;
+        sc[2] = w.z;
+        sc[3] = w.w;
+    } else {
+        const uint2 lo = ((const uint2*)prof)[ia], hi = ((const uint2*)prof)[ib];
+        sc[0] = __byte_perm(lo.x, hi.x, 0x5410);
+        sc[1] = __byte_perm(lo.x, hi.x, 0x7632);
+        sc[2] = __byte_perm(lo.y, hi.y, 0x5410);
+        sc[3] = __byte_perm(lo.y, hi.y, 0x7632);
+    }
+}
+
+template <bool DL>
+__host__ __device__ constexpr int prof_entry_bytes() { return DL ? (int)sizeof(uint2) : (int)sizeof(uint4); }
+
+// This warp's profile in shared memory (typed offsets keep the address a
+// 32-bit shared-window computation).
+template <int S, bool DL>
+__device__ __forceinline__ void* warp_profile(unsigned char* smem, int wib, int alpha1) {
+    if constexpr (DL) return (uint2*)smem + wib * ((S / 4) * alpha1);
+    else return (uint4*)smem + wib * ((S / 4) * alpha1);
+}
+
 // One lane, two pairs (strip A / strip B against the lane sequence).
 //   linear: H = max(diag + s, left + gap, up + gap, 0)                 3 DPX / row
 //   affine: carries Mg = M + gap_open (gap_open = gap + ext):
@@ -93,10 +144,21 @@ __device__ __forceinline__ void build_profile16(uint4* prof, const int8_t* cmat,
 //     Y  = max(Yup + ext, Mg_up)      strip-axis gap chain
 //     X  = max(Xleft + ext, Mg_left)  sweep-axis gap chain
 //     B  = max(Mg - ge, Y, X)          as max(M, Y, X)                 5 DPX / row
-template <int S, bool AFFINE>
-__device__ __forceinline__ void sweep16(const uint8_t* qc, int lq4, const uint4* prof, int alpha1, int gap, int ext,
-                                        int ge, bool has_up, bool has_down, uint4* bnd, uint32_t& mx) {
+//
+// Dual-lane form (DL): the high halves sweep a second lane sequence (qc2,
+// lq42) against the same strip; the column loop runs to the longer of the two
+// and a sequence past its end reads padding codes (pad4), which cannot raise
+// its maximum.
+template <int S, bool AFFINE, bool DL>
+__device__ __forceinline__ void sweep16(const uint8_t* qc, int lq4, const uint8_t* qc2, int lq42, uint32_t pad4,
+                                        const void* prof, int alpha1, int gap, int ext, int ge, bool has_up,
+                                        bool has_down, uint4* bnd, uint32_t& mx) {
     const uint32_t g2 = pack16(gap), e2 = pack16(ext), ge2 = pack16(ge), nge2 = pack16(-ge);
+    auto word = [&](const uint8_t* q, int lim, int x4) -> uint32_t {
+        return !DL || x4 < lim ? *(const uint32_t*)(q + x4) : pad4;
+    };
+    const int lqa = lq4;  // the low halves' own columns
+    if constexpr (DL) lq4 = lq4 > lq42 ? lq4 : lq42;
     if constexpr (!AFFINE) {
         uint32_t H[S];
 #pragma unroll
@@ -105,23 +167,28 @@ __device__ __forceinline__ void sweep16(const uint8_t* qc, int lq4, const uint4*
         // the code word of the next 4 columns and the boundary value of the
         // next column are loaded one step ahead (their latency hides behind a
         // column of arithmetic)
-        uint32_t cw_next = lq4 > 0 ? *(const uint32_t*)qc : 0u;
+        uint32_t cw_next = lq4 > 0 ? word(qc, lqa, 0) : 0u;
+        uint32_t cw2_next = DL && lq4 > 0 ? word(qc2, lq42, 0) : 0u;
         uint32_t up_next = has_up && lq4 > 0 ? bnd[0].x : 0u;
         for (int x4 = 0; x4 < lq4; x4 += 4) {
-            const uint32_t cw = cw_next;
-            if (x4 + 4 < lq4) cw_next = *(const uint32_t*)(qc + x4 + 4);
+            const uint32_t cw = cw_next, cw2 = cw2_next;
+            if (x4 + 4 < lq4) {
+                cw_next = word(qc, lqa, x4 + 4);
+                if constexpr (DL) cw2_next = word(qc2, lq42, x4 + 4);
+            }
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const int x = x4 + j;
                 const int a = (cw >> (8 * j)) & 0xff;
+                const int a2 = DL ? (cw2 >> (8 * j)) & 0xff : 0;
                 uint32_t up = up_next;
                 if (has_up && x + 1 < lq4) up_next = bnd[(int64_t)(x + 1) * kWarp].x;
                 uint32_t diag = hb_prev;
                 hb_prev = up;
 #pragma unroll
                 for (int g = 0; g < S / 4; ++g) {
-                    const uint4 w4 = prof[g * alpha1 + a];
-                    const uint32_t sc[4] = {w4.x, w4.y, w4.z, w4.w};
+                    uint32_t sc[4];
+                    fetch16<DL>(prof, g * alpha1 + a, g * alpha1 + a2, sc);
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
                         const int r = 4 * g + k;
@@ -150,16 +217,21 @@ __device__ __forceinline__ void sweep16(const uint8_t* qc, int lq4, const uint4*
             Bl[r] = 0;
         }
         uint32_t bb_prev = 0;
-        uint32_t cw_next = lq4 > 0 ? *(const uint32_t*)qc : 0u;
+        uint32_t cw_next = lq4 > 0 ? word(qc, lqa, 0) : 0u;
+        uint32_t cw2_next = DL && lq4 > 0 ? word(qc2, lq42, 0) : 0u;
         uint4 v_next = has_up && lq4 > 0 ? bnd[0] : make_uint4(ge2, kNeg16x2, 0u, 0u);
         uint4 v_next2 = has_up && lq4 > 1 ? bnd[kWarp] : make_uint4(ge2, kNeg16x2, 0u, 0u);
         for (int x4 = 0; x4 < lq4; x4 += 4) {
-            const uint32_t cw = cw_next;
-            if (x4 + 4 < lq4) cw_next = *(const uint32_t*)(qc + x4 + 4);
+            const uint32_t cw = cw_next, cw2 = cw2_next;
+            if (x4 + 4 < lq4) {
+                cw_next = word(qc, lqa, x4 + 4);
+                if constexpr (DL) cw2_next = word(qc2, lq42, x4 + 4);
+            }
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const int x = x4 + j;
                 const int a = (cw >> (8 * j)) & 0xff;
+                const int a2 = DL ? (cw2 >> (8 * j)) & 0xff : 0;
                 const uint4 v = v_next;
                 v_next = v_next2;
                 if (has_up && x + 2 < lq4) v_next2 = bnd[(int64_t)(x + 2) * kWarp];
@@ -168,8 +240,8 @@ __device__ __forceinline__ void sweep16(const uint8_t* qc, int lq4, const uint4*
                 bb_prev = bup;
 #pragma unroll
                 for (int g = 0; g < S / 4; ++g) {
-                    const uint4 w4 = prof[g * alpha1 + a];
-                    const uint32_t sc[4] = {w4.x, w4.y, w4.z, w4.w};
+                    uint32_t sc[4];
+                    fetch16<DL>(prof, g * alpha1 + a, g * alpha1 + a2, sc);
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
                         const int r = 4 * g + k;
@@ -272,11 +344,11 @@ __device__ __forceinline__ void chain_publish(int* flag, int v) {
 // longest lane (xm4, warp-uniform); a lane past its own sequence sweeps
 // padding-code columns, which cannot raise its maximum.  Returns false when a
 // wait gave up.
-template <int S, bool AFFINE>
-__device__ __forceinline__ bool sweep16_chain(const uint8_t* qc, int lq4, int xm4, uint32_t pad4, const uint4* prof,
-                                              int alpha1, int gap, int ext, int ge, bool has_up, bool has_down,
-                                              const uint4* ring_in, uint4* ring_out, const int* prog_in,
-                                              int* prog_out, int* abort_flag, uint32_t& mx) {
+template <int S, bool AFFINE, bool DL>
+__device__ __forceinline__ bool sweep16_chain(const uint8_t* qc, int lq4, const uint8_t* qc2, int lq42, int xm4,
+                                              uint32_t pad4, const void* prof, int alpha1, int gap, int ext, int ge,
+                                              bool has_up, bool has_down, const uint4* ring_in, uint4* ring_out,
+                                              const int* prog_in, int* prog_out, int* abort_flag, uint32_t& mx) {
     const uint32_t g2 = pack16(gap), e2 = pack16(ext), ge2 = pack16(ge), nge2 = pack16(-ge);
     int avail = 0;  // columns of the predecessor known to be published
     auto need_cols = [&](int upto) -> bool {  // columns [0, upto) of ring_in readable
@@ -285,6 +357,7 @@ __device__ __forceinline__ bool sweep16_chain(const uint8_t* qc, int lq4, int xm
         return avail >= 0;
     };
     auto code_word = [&](int x4) -> uint32_t { return x4 < lq4 ? *(const uint32_t*)(qc + x4) : pad4; };
+    auto code_word2 = [&](int x4) -> uint32_t { return DL && x4 < lq42 ? *(const uint32_t*)(qc2 + x4) : pad4; };
     if (!need_cols(min(kChainLead, xm4))) return false;
     if constexpr (!AFFINE) {
         uint32_t H[S];
@@ -292,23 +365,28 @@ __device__ __forceinline__ bool sweep16_chain(const uint8_t* qc, int lq4, int xm
         for (int r = 0; r < S; ++r) H[r] = 0;
         uint32_t hb_prev = 0;
         uint32_t cw_next = xm4 > 0 ? code_word(0) : pad4;
+        uint32_t cw2_next = DL && xm4 > 0 ? code_word2(0) : pad4;
         uint32_t up_next = has_up && xm4 > 0 ? __ldcg(&ring_in[0]).x : 0u;
         for (int x4 = 0; x4 < xm4; x4 += 4) {
             if (!need_cols(min(x4 + kChainNeed, xm4))) return false;
-            const uint32_t cw = cw_next;
-            if (x4 + 4 < xm4) cw_next = code_word(x4 + 4);
+            const uint32_t cw = cw_next, cw2 = cw2_next;
+            if (x4 + 4 < xm4) {
+                cw_next = code_word(x4 + 4);
+                if constexpr (DL) cw2_next = code_word2(x4 + 4);
+            }
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const int x = x4 + j;
                 const int a = (cw >> (8 * j)) & 0xff;
+                const int a2 = DL ? (cw2 >> (8 * j)) & 0xff : 0;
                 uint32_t up = up_next;
                 if (has_up && x + 1 < xm4) up_next = __ldcg(&ring_in[(int64_t)(x + 1) * kWarp]).x;
                 uint32_t diag = hb_prev;
                 hb_prev = up;
 #pragma unroll
                 for (int g = 0; g < S / 4; ++g) {
-                    const uint4 w4 = prof[g * alpha1 + a];
-                    const uint32_t sc[4] = {w4.x, w4.y, w4.z, w4.w};
+                    uint32_t sc[4];
+                    fetch16<DL>(prof, g * alpha1 + a, g * alpha1 + a2, sc);
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
                         const int r = 4 * g + k;
@@ -336,16 +414,21 @@ __device__ __forceinline__ bool sweep16_chain(const uint8_t* qc, int lq4, int xm
         }
         uint32_t bb_prev = 0;
         uint32_t cw_next = xm4 > 0 ? code_word(0) : pad4;
+        uint32_t cw2_next = DL && xm4 > 0 ? code_word2(0) : pad4;
         uint4 v_next = has_up && xm4 > 0 ? __ldcg(&ring_in[0]) : make_uint4(ge2, kNeg16x2, 0u, 0u);
         uint4 v_next2 = has_up && xm4 > 1 ? __ldcg(&ring_in[kWarp]) : make_uint4(ge2, kNeg16x2, 0u, 0u);
         for (int x4 = 0; x4 < xm4; x4 += 4) {
             if (!need_cols(min(x4 + kChainNeed, xm4))) return false;
-            const uint32_t cw = cw_next;
-            if (x4 + 4 < xm4) cw_next = code_word(x4 + 4);
+            const uint32_t cw = cw_next, cw2 = cw2_next;
+            if (x4 + 4 < xm4) {
+                cw_next = code_word(x4 + 4);
+                if constexpr (DL) cw2_next = code_word2(x4 + 4);
+            }
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const int x = x4 + j;
                 const int a = (cw >> (8 * j)) & 0xff;
+                const int a2 = DL ? (cw2 >> (8 * j)) & 0xff : 0;
                 const uint4 v = v_next;
                 v_next = v_next2;
                 if (has_up && x + 2 < xm4) v_next2 = __ldcg(&ring_in[(int64_t)(x + 2) * kWarp]);
@@ -354,8 +437,8 @@ __device__ __forceinline__ bool sweep16_chain(const uint8_t* qc, int lq4, int xm
                 bb_prev = bup;
 #pragma unroll
                 for (int g = 0; g < S / 4; ++g) {
-                    const uint4 w4 = prof[g * alpha1 + a];
-                    const uint32_t sc[4] = {w4.x, w4.y, w4.z, w4.w};
+                    uint32_t sc[4];
+                    fetch16<DL>(prof, g * alpha1 + a, g * alpha1 + a2, sc);
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
                         const int r = 4 * g + k;
@@ -380,12 +463,63 @@ __device__ __forceinline__ bool sweep16_chain(const uint8_t* qc, int lq4, int xm
     return true;
 }
 
-template <int S, bool AFFINE>
+// One item's lanes.  Strip-pair form: strip A (W.target) in the low halves,
+// strip B (W.index, or none) in the high halves, one lane sequence per lane.
+// Dual-lane form (DL): strip W.target in both halves, the lane sequences of
+// sorted positions W.first + lane (low) and W.first + 32 + lane (high, the
+// first W.lanes_hi lanes).
+struct Lanes16 {
+    bool active;        // the low half's lane sequence exists
+    int p, p2;          // lane sequences of the low / high halves
+    const uint8_t* qc;  // their codes
+    const uint8_t* qc2;
+    int lq4, lq42;      // their lengths rounded up to 4 (0: padding only)
+};
+
+template <bool DL>
+__device__ __forceinline__ Lanes16 item_lanes(const Score16Args& A, const WorkItem& W, int lane) {
+    Lanes16 L;
+    L.active = lane < W.lanes;
+    L.p = L.active ? A.lane_order[W.first + lane] : 0;
+    L.qc = A.lane_codes + A.lane_off[L.p];
+    L.lq4 = L.active ? (A.lane_len[L.p] + 3) & ~3 : 0;
+    const bool hi = DL && lane < W.lanes_hi;
+    L.p2 = hi ? A.lane_order[W.first + kWarp + lane] : -1;
+    L.qc2 = hi ? A.lane_codes + A.lane_off[L.p2] : L.qc;
+    L.lq42 = hi ? (A.lane_len[L.p2] + 3) & ~3 : 0;
+    return L;
+}
+
+// Writes a lane's two pair maxima (NaN where the 16-bit limit was reached).
+template <bool DL>
+__device__ __forceinline__ void store_max16(const Score16Args& A, const WorkItem& W, const Lanes16& L, uint32_t mx) {
+    const int sa = W.target;
+    const int s_hi = DL ? (L.p2 >= 0 ? sa : -1) : W.index;
+    const int p_hi = DL ? L.p2 : L.p;
+    const int ma = (int)(int16_t)(mx & 0xffffu), mb = (int)(int16_t)(mx >> 16);
+    A.pair_max[(int64_t)sa * A.stride_strip + (int64_t)L.p * A.stride_lane] =
+        ma >= kOvf16 ? __int_as_float(0x7fc00000) : (float)ma;
+    if (s_hi >= 0)
+        A.pair_max[(int64_t)s_hi * A.stride_strip + (int64_t)p_hi * A.stride_lane] =
+            mb >= kOvf16 ? __int_as_float(0x7fc00000) : (float)mb;
+    if (ma >= kOvf16 || (s_hi >= 0 && mb >= kOvf16)) atomicAdd(A.ovf_count, 1);
+}
+
+template <int S, bool DL>
+__device__ __forceinline__ void build_item_profile(void* prof, const Score16Args& A, const uint8_t* ra,
+                                                   const uint8_t* rb, int y0, int la, int lb, int shift, int lane) {
+    if constexpr (DL)
+        build_profile16_dual<S>((uint2*)prof, A.cmat, ra, y0, la, A.alpha1, A.dim, shift, lane);
+    else
+        build_profile16<S>((uint4*)prof, A.cmat, ra, rb, y0, la, lb, A.alpha1, A.dim, shift, lane);
+}
+
+template <int S, bool AFFINE, bool DL>
 __global__ void __launch_bounds__(128, 3) score16_chain_kernel(Score16Args A) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    uint4* prof = (uint4*)smem + wib * ((S / 4) * A.alpha1);
+    void* prof = warp_profile<S, DL>(smem, wib, A.alpha1);
     const int shift = AFFINE ? A.ge : 0;
     const uint32_t pad4 = (uint32_t)A.pad_code * 0x01010101u;
     const int64_t warp_global = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
@@ -398,15 +532,12 @@ __global__ void __launch_bounds__(128, 3) score16_chain_kernel(Score16Args A) {
         const WorkItem W = A.items[it];
         const int4 ci = A.chain[it];
         const int c = ci.x, s = ci.y, pred = ci.z;
-        const int sa = W.target, sb = W.index;
+        const int sa = W.target, sb = DL ? -1 : W.index;
         const int la = A.strip_len[sa];
         const int lb = sb >= 0 ? A.strip_len[sb] : 0;
         const int ls = la > lb ? la : lb;
         const int nstrips = (ls + S - 1) / S;
-        const bool active = lane < W.lanes;
-        const int p = active ? A.lane_order[W.first + lane] : 0;
-        const uint8_t* qc = A.lane_codes + A.lane_off[p];
-        const int lq4 = active ? (A.lane_len[p] + 3) & ~3 : 0;
+        const Lanes16 L = item_lanes<DL>(A, W, lane);
         const uint8_t* ra = A.strip_res + A.strip_off[sa];
         const uint8_t* rb = A.strip_res + A.strip_off[sb >= 0 ? sb : sa];
         uint32_t mx = 0;
@@ -415,10 +546,11 @@ __global__ void __launch_bounds__(128, 3) score16_chain_kernel(Score16Args A) {
             // a whole item on this warp, strip after strip
             for (int st = 0; st < nstrips; ++st) {
                 __syncwarp();
-                build_profile16<S>(prof, A.cmat, ra, rb, st * S, la, lb, A.alpha1, A.dim, shift, lane);
+                build_item_profile<S, DL>(prof, A, ra, rb, st * S, la, lb, shift, lane);
                 __syncwarp();
-                if (active)
-                    sweep16<S, AFFINE>(qc, lq4, prof, A.alpha1, A.gap, A.ext, A.ge, st > 0, st + 1 < nstrips, bnd, mx);
+                if (L.active)
+                    sweep16<S, AFFINE, DL>(L.qc, L.lq4, L.qc2, L.lq42, pad4, prof, A.alpha1, A.gap, A.ext, A.ge,
+                                           st > 0, st + 1 < nstrips, bnd, mx);
             }
         } else {
             const int xm4 = (W.xmax + 3) & ~3;
@@ -426,12 +558,12 @@ __global__ void __launch_bounds__(128, 3) score16_chain_kernel(Score16Args A) {
             const uint4* ring_in = A.ring + A.ring_off[c] + ((s + 1) & 1) * row + lane;
             uint4* ring_out = A.ring + A.ring_off[c] + (s & 1) * row + lane;
             __syncwarp();
-            build_profile16<S>(prof, A.cmat, ra, rb, s * S, la, lb, A.alpha1, A.dim, shift, lane);
+            build_item_profile<S, DL>(prof, A, ra, rb, s * S, la, lb, shift, lane);
             __syncwarp();
             const bool has_down = s + 1 < nstrips;
-            if (!sweep16_chain<S, AFFINE>(qc, lq4, xm4, pad4, prof, A.alpha1, A.gap, A.ext, A.ge, s > 0, has_down,
-                                          ring_in, ring_out, s > 0 ? A.progress + pred : nullptr, A.progress + it,
-                                          A.abort_flag, mx))
+            if (!sweep16_chain<S, AFFINE, DL>(L.qc, L.lq4, L.qc2, L.lq42, xm4, pad4, prof, A.alpha1, A.gap, A.ext,
+                                              A.ge, s > 0, has_down, ring_in, ring_out,
+                                              s > 0 ? A.progress + pred : nullptr, A.progress + it, A.abort_flag, mx))
                 break;
             if (s > 0) {
                 // the predecessor's running maximum is final once it has finished
@@ -444,40 +576,30 @@ __global__ void __launch_bounds__(128, 3) score16_chain_kernel(Score16Args A) {
                 finished = false;
             }
         }
-        if (finished && active) {
-            const int ma = (int)(int16_t)(mx & 0xffffu), mb = (int)(int16_t)(mx >> 16);
-            A.pair_max[(int64_t)sa * A.stride_strip + (int64_t)p * A.stride_lane] =
-                ma >= kOvf16 ? __int_as_float(0x7fc00000) : (float)ma;
-            if (sb >= 0)
-                A.pair_max[(int64_t)sb * A.stride_strip + (int64_t)p * A.stride_lane] =
-                    mb >= kOvf16 ? __int_as_float(0x7fc00000) : (float)mb;
-            if (ma >= kOvf16 || (sb >= 0 && mb >= kOvf16)) atomicAdd(A.ovf_count, 1);
-        }
+        if (finished && L.active) store_max16<DL>(A, W, L, mx);
     }
 }
 
-template <int S, bool AFFINE, bool MULTI>
+template <int S, bool AFFINE, bool MULTI, bool DL>
 __global__ void __launch_bounds__(128) score16_kernel(Score16Args A) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    uint4* prof = (uint4*)smem + wib * ((S / 4) * A.alpha1);
+    void* prof = warp_profile<S, DL>(smem, wib, A.alpha1);
     const int64_t warp_global = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
     uint4* bnd = MULTI ? A.bnd_pool + warp_global * A.bnd_slot + lane : nullptr;
     const int shift = AFFINE ? A.ge : 0;
+    const uint32_t pad4 = (uint32_t)A.pad_code * 0x01010101u;
     for (;;) {
         int it = 0;
         if (lane == 0) it = atomicAdd(A.counter, 1);
         it = __shfl_sync(0xffffffffu, it, 0);
         if (it >= A.n_items) break;
         const WorkItem W = A.items[it];
-        const int sa = W.target, sb = W.index;
+        const int sa = W.target, sb = DL ? -1 : W.index;
         const int la = A.strip_len[sa];
         const int lb = sb >= 0 ? A.strip_len[sb] : 0;
-        const bool active = lane < W.lanes;
-        const int p = active ? A.lane_order[W.first + lane] : 0;
-        const uint8_t* qc = A.lane_codes + A.lane_off[p];
-        const int lq4 = active ? (A.lane_len[p] + 3) & ~3 : 0;
+        const Lanes16 L = item_lanes<DL>(A, W, lane);
         const uint8_t* ra = A.strip_res + A.strip_off[sa];
         const uint8_t* rb = A.strip_res + A.strip_off[sb >= 0 ? sb : sa];
         const int ls = la > lb ? la : lb;
@@ -486,20 +608,13 @@ __global__ void __launch_bounds__(128) score16_kernel(Score16Args A) {
         for (int s = 0; s < nstrips; ++s) {
             const int y0 = s * S;
             __syncwarp();
-            build_profile16<S>(prof, A.cmat, ra, rb, y0, la, lb, A.alpha1, A.dim, shift, lane);
+            build_item_profile<S, DL>(prof, A, ra, rb, y0, la, lb, shift, lane);
             __syncwarp();
-            if (active)
-                sweep16<S, AFFINE>(qc, lq4, prof, A.alpha1, A.gap, A.ext, A.ge, s > 0, s + 1 < nstrips, bnd, mx);
+            if (L.active)
+                sweep16<S, AFFINE, DL>(L.qc, L.lq4, L.qc2, L.lq42, pad4, prof, A.alpha1, A.gap, A.ext, A.ge, s > 0,
+                                       s + 1 < nstrips, bnd, mx);
         }
-        if (active) {
-            const int ma = (int)(int16_t)(mx & 0xffffu), mb = (int)(int16_t)(mx >> 16);
-            A.pair_max[(int64_t)sa * A.stride_strip + (int64_t)p * A.stride_lane] =
-                ma >= kOvf16 ? __int_as_float(0x7fc00000) : (float)ma;
-            if (sb >= 0)
-                A.pair_max[(int64_t)sb * A.stride_strip + (int64_t)p * A.stride_lane] =
-                    mb >= kOvf16 ? __int_as_float(0x7fc00000) : (float)mb;
-            if (ma >= kOvf16 || (sb >= 0 && mb >= kOvf16)) atomicAdd(A.ovf_count, 1);
-        }
+        if (L.active) store_max16<DL>(A, W, L, mx);
     }
 }
 

@@ -10,13 +10,15 @@ def configure(engine, score, settings):
                        float(settings.minimum_score), float(score.highest_score), float(settings.filter_factor))
 
 
-def run_engine(lib, queries, targets, score, settings, q_keys=None, t_keys=None, **align_kw):
+def run_engine(lib, queries, targets, score, settings, q_keys=None, t_keys=None, tuning=None, **align_kw):
     e = _native.Engine(0, lib=lib)
     try:
         configure(e, score, settings)
         e.set_queries([q.encode() for q in queries], np.arange(len(queries)) if q_keys is None else q_keys)
         e.set_targets([t.encode() for t in targets],
                       np.arange(len(targets)) + len(queries) if t_keys is None else t_keys)
+        for key, value in (tuning or {}).items():
+            e.set_tuning(key, value)
         info = e.align(**align_kw)
         pm = e.pair_max()
         hits = decode_hits(*e.hits()) if not align_kw.get("score_only") else []

@@ -211,6 +211,37 @@ def test_chained_strips_match_one_warp_items_and_oracle(engine_lib, oracle_mod, 
         np.testing.assert_array_equal(single, ref)
 
 
+@pytest.mark.parametrize("kind", ["dna", "protein", "protein_linear"])
+@pytest.mark.parametrize("shape", [(1, 150), (3, 97), (14, 40), (40, 14)])
+@pytest.mark.parametrize("chain_min", [0, 1])
+def test_dual_lane_sweep_matches_oracle(engine_lib, oracle_mod, kind, shape, chain_min):
+    """The dual-lane form of the 16-bit sweep (one strip against two lane
+    sequences per lane; forced on with PW_TUNE_DUAL 1) gives the oracle's pair
+    maxima and hits: single-strip and multi-strip lengths, lane groups cut
+    short (97 and 150 lanes leave the second group partly empty), chained and
+    one-warp items.  The automatic choice picks it for a single query."""
+    from pypaswas_b200 import _native, scores
+    rng = np.random.default_rng({"dna": 8, "protein": 9, "protein_linear": 10}[kind] * 100 + sum(shape) + chain_min)
+    alphabet = cases.DNA if kind == "dna" else cases.PROTEIN
+    nq, nt = shape
+    q = ["".join(alphabet[i] for i in rng.integers(0, len(alphabet), int(n))) for n in rng.integers(5, 300, nq)]
+    t = ["".join(alphabet[i] for i in rng.integers(0, len(alphabet), int(n))) for n in rng.integers(5, 260, nt)]
+    q[0] = t[0][:100] + q[0]  # a shared segment
+    st = cases.Settings(gap_extension="-1" if kind in ("dna", "protein") else "0", minimum_score="20",
+                        **({} if kind == "dna" else dict(matrix_name="BLOSUM62", gap_score="-11")))
+    score = scores.make_score(st)
+    o = _oracle(oracle_mod, q, t, score, st)
+    tuning = {_native.PW_TUNE_DUAL: 1, _native.PW_TUNE_CHAIN_MIN: chain_min}
+    pm, hits, info, _ = run_engine(engine_lib, q, t, score, st, tuning=tuning)
+    assert info.dual_lanes == 1 and info.score_path == 0
+    np.testing.assert_array_equal(pm, o["pair_max"])
+    assert hits == o["hits"]
+    if nq == 1 and chain_min == 0:
+        pm_auto, _, info_auto, _ = run_engine(engine_lib, q, t, score, st, score_only=True)
+        assert info_auto.dual_lanes == 1
+        np.testing.assert_array_equal(pm_auto, o["pair_max"])
+
+
 def _oracle_pairs(oracle_mod, queries, targets, pairs, score, st):
     """Oracle hits and maxima of explicit pairs, one pair at a time."""
     p = cases.oracle_params(oracle_mod, score)
