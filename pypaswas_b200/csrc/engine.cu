@@ -10,6 +10,8 @@
 // The host only builds work lists, sizes memory waves and formats results.
 #include <cuda_runtime.h>
 #include <cub/device/device_scan.cuh>
+#include <cub/device/device_select.cuh>
+#include <thrust/iterator/counting_iterator.h>
 
 #include <algorithm>
 #include <chrono>
@@ -189,7 +191,9 @@ struct pw_engine {
     DevBuf q_res, t_ccodes, t_order, cmat_t8, cmat_tf;  // the other orientation's encodings
     DevBuf cmat_i8, cmat_f, pair_max, items, items_alt, counter, bnd_pool, q_order2;
     DevBuf band_pairs, band_entries, band_prog, band_max, band_ring, band_out;  // band sweep (pw_band.cuh)
-    DevBuf scan_tmp;  // CUB scan scratch
+    DevBuf scan_tmp;  // CUB scan / select scratch
+    DevBuf prune_flags, prune_cnt, prune_sel;  // phase-2 pruning on the device
+    HostBuf<int64_t> h_sel;
     DevBuf chain_items, chain_info, chain_prog, chain_max, chain_ring_off, chain_ring, chain_abort, p1_items;
     // plan of the 16-bit score phase (work items, classes, chain queue), kept
     // on the device and reused while inputs, scoring, flags and tuning stay
@@ -1447,34 +1451,64 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     std::vector<std::vector<int32_t>> pass_q;       // per query: passing targets, length order (when needed)
     int64_t min_pass = 0, n_pass = 0;
     {
-        std::mutex mu;
-        // one target column per task, all queries in length order (so each
-        // list comes out in that order); host threads split the targets
-        parallel_for(nt, [&](int64_t t0, int64_t t1) {
-            int64_t mp = 0, np_ = 0, tc = 0;
-            for (int64_t t = t0; t < t1; ++t) {
-                std::vector<int32_t>& lst = pass_t[t];
-                for (int sp = 0; sp < nq; ++sp) {
-                    const int q = pr.order[sp];
-                    const float mx = e->h_pair_max[(size_t)q * nt + t];
-                    if (!(mx >= e->minimum_score)) continue;
-                    ++mp;
-                    const int mn = std::min(qlen[q], tlen[t]);
-                    const float pos = (float)(e->highest * (double)mn * e->filter_factor);
-                    const volatile float llm = e->lower_limit * mx;  // fp32 product, as the kernel computes it
-                    const float thr = std::max((float)llm, pos);
-                    if (mx >= thr) {
+        // the test runs on the device over the resident maxima (prune_kernel);
+        // the passing pairs come back as a target-major list of pair indices
+        const int64_t npairs = (int64_t)nq * nt;
+        unsigned long long cnt[2] = {0, 0};
+        if ((c = e->prune_flags.reserve(e->stream, (size_t)std::max<int64_t>(npairs, 16))) != cudaSuccess ||
+            (c = e->prune_cnt.reserve(e->stream, 4 * sizeof(unsigned long long))) != cudaSuccess ||
+            (c = cudaMemsetAsync(e->prune_cnt.p, 0, 4 * sizeof(unsigned long long), e->stream)) != cudaSuccess)
+            return cuda_fail(e, c, "alloc pruning flags");
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((npairs + 255) / 256, (int64_t)e->sm_count * 16));
+        PW_LAUNCH(prune_kernel, grid, 256, 0, e->stream, (const float*)A.pair_max, e->q_order.as<int32_t>(),
+                  e->q_len.as<int32_t>(), e->t_len.as<int32_t>(), nq, nt, e->minimum_score, e->highest,
+                  e->filter_factor, e->lower_limit, e->prune_flags.as<uint8_t>(),
+                  e->prune_cnt.as<unsigned long long>());
+        e->launches++;
+        if ((c = cudaGetLastError()) != cudaSuccess ||
+            (c = cudaMemcpyAsync(cnt, e->prune_cnt.p, sizeof(cnt), cudaMemcpyDeviceToHost, e->stream)) != cudaSuccess ||
+            (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
+            return cuda_fail(e, c, "prune pairs");
+        min_pass = (int64_t)cnt[0];
+        n_pass = (int64_t)cnt[1];
+        if (n_pass > 0) {
+            int64_t* d_count = e->prune_cnt.as<int64_t>() + 2;
+            thrust::counting_iterator<int64_t> ids(0);
+            size_t tmp_bytes = 0;
+            if ((c = cub::DeviceSelect::Flagged(nullptr, tmp_bytes, ids, e->prune_flags.as<uint8_t>(), (int64_t*)nullptr,
+                                                d_count, npairs, e->stream)) != cudaSuccess ||
+                (c = e->scan_tmp.reserve(e->stream, std::max<size_t>(tmp_bytes, 16))) != cudaSuccess ||
+                (c = e->prune_sel.reserve(e->stream, (size_t)n_pass * sizeof(int64_t))) != cudaSuccess ||
+                (c = cub::DeviceSelect::Flagged(e->scan_tmp.p, tmp_bytes, ids, e->prune_flags.as<uint8_t>(),
+                                                e->prune_sel.as<int64_t>(), d_count, npairs, e->stream)) != cudaSuccess)
+                return cuda_fail(e, c, "select passing pairs");
+            e->launches++;
+            if (!e->h_sel.resize((size_t)n_pass)) return fail(e, PW_ERR_NOMEM, "host memory for the passing pairs");
+            if ((c = cudaMemcpyAsync(e->h_sel.data(), e->prune_sel.p, (size_t)n_pass * sizeof(int64_t),
+                                     cudaMemcpyDeviceToHost, e->stream)) != cudaSuccess ||
+                (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
+                return cuda_fail(e, c, "copy passing pairs");
+            const int64_t* sel = e->h_sel.data();
+            std::mutex mu;
+            parallel_for(nt, [&](int64_t t0, int64_t t1) {
+                int64_t lo = std::lower_bound(sel, sel + n_pass, t0 * (int64_t)nq) - sel, tc = 0;
+                for (int64_t t = t0; t < t1; ++t) {
+                    const int64_t end = (t + 1) * (int64_t)nq;
+                    int64_t hi = lo;
+                    while (hi < n_pass && sel[hi] < end) ++hi;
+                    std::vector<int32_t>& lst = pass_t[t];
+                    lst.reserve((size_t)(hi - lo));
+                    for (int64_t j = lo; j < hi; ++j) {
+                        const int q = pr.order[(size_t)(sel[j] - t * (int64_t)nq)];
                         lst.push_back(q);
-                        ++np_;
                         tc += (int64_t)qlen[q] * tlen[t];
                     }
+                    lo = hi;
                 }
-            }
-            std::lock_guard<std::mutex> g(mu);
-            min_pass += mp;
-            n_pass += np_;
-            inf.traced_cells += tc;
-        }, std::max<int64_t>(1, ((int64_t)1 << 20) / std::max(nq, 1)));
+                std::lock_guard<std::mutex> g(mu);
+                inf.traced_cells += tc;
+            }, std::max<int64_t>(1, std::min<int64_t>(nt, ((int64_t)1 << 16) * nt / std::max<int64_t>(n_pass, 1))));
+        }
     }
     // Traced pairs with targets longer than one register strip go to the
     // one-warp-per-pair sweep (pw_band.cuh); the others are grouped 32 to

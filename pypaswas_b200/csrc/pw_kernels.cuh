@@ -851,6 +851,51 @@ __global__ void int_peak16_kernel(int iters, int seed, int* sink) {
     if (r == 0x7fffffffu) sink[0] = (int)r;
 }
 
+// Pruning of the traced pairs on the device (the host then reads only the
+// pairs that pass).  Pair k = t * nq + sp (target-major, sp the query's sorted
+// position) passes when its maximum reaches MINIMUM_SCORE and
+// max(LOWER_LIMIT_SCORE * max, maxPossibleScore) -- the starting-point
+// threshold of default_main.cu:596,609, maxPossibleScore =
+// highest * min(len) * filter_factor in double precision, stored as fp32 as
+// the reference's host does (SmithWatermanCuda._set_max_possible_score,
+// SmithWatermanCuda.py:268-274) -- so that no pair without a starting point
+// is swept.  flags[k] = pass; counts[0] += pairs
+// reaching MINIMUM_SCORE, counts[1] += passing pairs.
+__global__ void prune_kernel(const float* pair_max, const int32_t* q_order, const int32_t* q_len,
+                             const int32_t* t_len, int nq, int nt, float minimum, double highest,
+                             double filter_factor, float lower_limit, uint8_t* flags,
+                             unsigned long long* counts) {
+    const int64_t n = (int64_t)nq * nt;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    unsigned long long n_min = 0, n_pass = 0;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
+        const int64_t k = base + threadIdx.x;
+        bool m = false, pass = false;
+        if (k < n) {
+            const int t = (int)(k / nq), sp = (int)(k - (int64_t)t * nq);
+            const int q = q_order[sp];
+            const float mx = pair_max[(int64_t)q * nt + t];
+            m = mx >= minimum;
+            if (m) {
+                const int mn = min(q_len[q], t_len[t]);
+                const float pos = (float)(highest * (double)mn * filter_factor);
+                const float llm = __fmul_rn(lower_limit, mx);
+                pass = mx >= fmaxf(llm, pos);
+            }
+            flags[k] = pass ? 1 : 0;
+        }
+        const unsigned bm = __ballot_sync(0xffffffffu, m), bp = __ballot_sync(0xffffffffu, pass);
+        if ((threadIdx.x & 31) == 0) {
+            n_min += __popc(bm);
+            n_pass += __popc(bp);
+        }
+    }
+    if ((threadIdx.x & 31) == 0 && (n_min | n_pass)) {
+        atomicAdd(&counts[0], n_min);
+        atomicAdd(&counts[1], n_pass);
+    }
+}
+
 #endif  // PW_SCORE_SWEEP_ONLY
 
 }  // namespace pw
