@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 #include <cub/device/device_scan.cuh>
 #include <cub/device/device_select.cuh>
+#include <cub/device/device_radix_sort.cuh>
 #include <thrust/iterator/counting_iterator.h>
 
 #include <algorithm>
@@ -30,6 +31,7 @@
 #include "pw_score16.cuh"
 #include "pw_band.cuh"
 #include "pw_plan.h"
+#include "pw_finish.cuh"
 
 using namespace pw;
 
@@ -93,6 +95,29 @@ struct HostBuf {
         n = m;
         return true;
     }
+    bool resize_keep(size_t m) {  // contents [0, min(n, m)) are kept; capacity grows by half
+        if (m > cap) {
+            const size_t want = std::max<size_t>(m, cap + cap / 2);
+            T* q = nullptr;
+            bool pin = cudaMallocHost((void**)&q, want * sizeof(T)) == cudaSuccess;
+            if (!pin) {
+                cudaGetLastError();
+                q = (T*)malloc(want * sizeof(T));
+                if (!q) return false;
+            }
+            if (n) std::memcpy(q, p, n * sizeof(T));
+            const size_t keep = n;
+            release();
+            p = q;
+            pinned = pin;
+            cap = want;
+            n = keep;
+        }
+        n = m;
+        return true;
+    }
+    void clear() { n = 0; }
+    bool empty() const { return n == 0; }
     void fill(T v) { std::fill(p, p + n, v); }
     size_t size() const { return n; }
     T* data() { return p; }
@@ -139,6 +164,25 @@ struct DevBuf {
         if (e == cudaSuccess) bytes = want;
         else p = nullptr;
         return e;
+    }
+    // Growth that keeps the first `used` bytes (stream-ordered copy into the
+    // new block), for buffers appended to across memory waves.
+    cudaError_t grow_keep(cudaStream_t st, size_t used, size_t n) {
+        if (n <= bytes && p) return cudaSuccess;
+        size_t want = std::max<size_t>(n, bytes + bytes / 2);
+        void* q = nullptr;
+        cudaError_t e = cudaMallocAsync(&q, want, st);
+        if (e == cudaErrorMemoryAllocation) {
+            cudaGetLastError();
+            want = n;
+            e = cudaMallocAsync(&q, want, st);
+        }
+        if (e != cudaSuccess) return e;
+        if (p && used && (e = cudaMemcpyAsync(q, p, used, cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return e;
+        if (p && (e = cudaFreeAsync(p, st)) != cudaSuccess) return e;
+        p = q;
+        bytes = want;
+        return cudaSuccess;
     }
     template <typename T>
     T* as() const { return (T*)p; }
@@ -193,6 +237,8 @@ struct pw_engine {
     DevBuf band_pairs, band_entries, band_prog, band_max, band_ring, band_out;  // band sweep (pw_band.cuh)
     DevBuf scan_tmp;  // CUB scan / select scratch
     DevBuf prune_flags, prune_cnt, prune_sel;  // phase-2 pruning on the device
+    // hits and column operations of all memory waves, then their order and strings
+    DevBuf acc_hits, acc_ops, fk_a, fk_b, fk_c, fk_t, fk_g, fi_a, fi_b, f_len, f_soff, f_out, f_str;
     HostBuf<int64_t> h_sel;
     DevBuf chain_items, chain_info, chain_prog, chain_max, chain_ring_off, chain_ring, chain_abort, p1_items;
     // plan of the 16-bit score phase (work items, classes, chain queue), kept
@@ -217,9 +263,9 @@ struct pw_engine {
     int64_t tune[8] = {0, 0, 0, 0, 0, 0, 0, 0};      // pw_set_tuning values (0: automatic)
     // results
     HostBuf<float> h_pair_max;
-    std::vector<pw_hit> h_hits;
-    std::vector<char> h_strings;
-    std::vector<StartRec> h_starts;
+    HostBuf<pw_hit> h_hits;
+    HostBuf<char> h_strings;
+    HostBuf<StartRec> h_starts;
     int64_t launches = 0;
 };
 
@@ -1121,6 +1167,84 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uin
 }
 
 
+// Orders the n accumulated hits (acc_hits / acc_ops) as the reference's
+// HitList and spells their strings on the device; the records land in
+// h_hits / h_strings.
+static cudaError_t finish_hits(pw_engine* e, int64_t n, int64_t* str_bytes) {
+    *str_bytes = 0;
+    e->h_hits.clear();
+    e->h_strings.clear();
+    if (n <= 0) return cudaSuccess;
+    if (n > (int64_t)INT32_MAX) return cudaErrorInvalidValue;
+    cudaError_t c;
+    const size_t k8 = (size_t)n * sizeof(uint64_t), k4 = (size_t)n * sizeof(int32_t);
+    if ((c = e->fk_a.reserve(e->stream, k8)) != cudaSuccess || (c = e->fk_b.reserve(e->stream, k8)) != cudaSuccess ||
+        (c = e->fk_c.reserve(e->stream, k8)) != cudaSuccess || (c = e->fk_t.reserve(e->stream, k8)) != cudaSuccess ||
+        (c = e->fk_g.reserve(e->stream, k8)) != cudaSuccess || (c = e->fi_a.reserve(e->stream, k4)) != cudaSuccess ||
+        (c = e->fi_b.reserve(e->stream, k4)) != cudaSuccess || (c = e->f_len.reserve(e->stream, k8)) != cudaSuccess ||
+        (c = e->f_soff.reserve(e->stream, k8)) != cudaSuccess)
+        return c;
+    const DevHit* h = e->acc_hits.as<DevHit>();
+    uint64_t *ka = e->fk_a.as<uint64_t>(), *kb = e->fk_b.as<uint64_t>(), *kc = e->fk_c.as<uint64_t>();
+    uint64_t *kt = e->fk_t.as<uint64_t>(), *kg = e->fk_g.as<uint64_t>();
+    int32_t *ia = e->fi_a.as<int32_t>(), *ib = e->fi_b.as<int32_t>();
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)e->sm_count * 16));
+    PW_LAUNCH(hit_key_kernel, grid, 256, 0, e->stream, h, n, ka, kb, kc, ia);
+    size_t tmp = 0;
+    if ((c = cub::DeviceRadixSort::SortPairs(nullptr, tmp, kc, kt, ia, ib, (int)n, 0, 64, e->stream)) != cudaSuccess ||
+        (c = e->scan_tmp.reserve(e->stream, std::max<size_t>(tmp, 16))) != cudaSuccess)
+        return c;
+    tmp = e->scan_tmp.bytes;
+    // three stable passes, least significant word first
+    if ((c = cub::DeviceRadixSort::SortPairs(e->scan_tmp.p, tmp, kc, kt, ia, ib, (int)n, 0, 64, e->stream)) !=
+        cudaSuccess)
+        return c;
+    PW_LAUNCH(gather_key_kernel, grid, 256, 0, e->stream, kb, ib, n, kg);
+    tmp = e->scan_tmp.bytes;
+    if ((c = cub::DeviceRadixSort::SortPairs(e->scan_tmp.p, tmp, kg, kt, ib, ia, (int)n, 0, 64, e->stream)) !=
+        cudaSuccess)
+        return c;
+    PW_LAUNCH(gather_key_kernel, grid, 256, 0, e->stream, ka, ia, n, kg);
+    tmp = e->scan_tmp.bytes;
+    if ((c = cub::DeviceRadixSort::SortPairs(e->scan_tmp.p, tmp, kg, kt, ia, ib, (int)n, 0, 64, e->stream)) !=
+        cudaSuccess)
+        return c;
+    // string offsets in the final order
+    int64_t *len = e->f_len.as<int64_t>(), *soff = e->f_soff.as<int64_t>();
+    PW_LAUNCH(hit_len_kernel, grid, 256, 0, e->stream, h, ib, n, len);
+    size_t stmp = 0;
+    if ((c = cub::DeviceScan::ExclusiveSum(nullptr, stmp, len, soff, (int64_t)n, e->stream)) != cudaSuccess) return c;
+    if (stmp > e->scan_tmp.bytes && (c = e->scan_tmp.reserve(e->stream, stmp)) != cudaSuccess) return c;
+    stmp = e->scan_tmp.bytes;
+    if ((c = cub::DeviceScan::ExclusiveSum(e->scan_tmp.p, stmp, len, soff, (int64_t)n, e->stream)) != cudaSuccess)
+        return c;
+    int64_t tail[2] = {0, 0};
+    if ((c = cudaMemcpyAsync(&tail[0], soff + n - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, e->stream)) !=
+            cudaSuccess ||
+        (c = cudaMemcpyAsync(&tail[1], len + n - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, e->stream)) !=
+            cudaSuccess ||
+        (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
+        return c;
+    const int64_t total = tail[0] + tail[1];
+    if ((c = e->f_out.reserve(e->stream, (size_t)n * sizeof(pw_hit))) != cudaSuccess ||
+        (c = e->f_str.reserve(e->stream, (size_t)std::max<int64_t>(total, 16))) != cudaSuccess)
+        return c;
+    PW_LAUNCH(hit_out_kernel, grid, 256, 0, e->stream, h, ib, soff, n, e->acc_ops.as<char>(), e->q_raw.as<uint8_t>(),
+              e->q_raw_off.as<int64_t>(), e->t_raw.as<uint8_t>(), e->t_raw_off.as<int64_t>(), e->f_out.as<pw_hit>(),
+              e->f_str.as<char>());
+    e->launches += 9;
+    if ((c = cudaGetLastError()) != cudaSuccess) return c;
+    if (!e->h_hits.resize((size_t)n) || !e->h_strings.resize((size_t)total)) return cudaErrorMemoryAllocation;
+    if ((c = cudaMemcpyAsync(e->h_hits.data(), e->f_out.p, (size_t)n * sizeof(pw_hit), cudaMemcpyDeviceToHost,
+                             e->stream)) != cudaSuccess ||
+        (total > 0 && (c = cudaMemcpyAsync(e->h_strings.data(), e->f_str.p, (size_t)total, cudaMemcpyDeviceToHost,
+                                           e->stream)) != cudaSuccess) ||
+        (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
+        return c;
+    *str_bytes = total;
+    return cudaSuccess;
+}
+
 // Launches band_kernel over `pairs` (one warp per band, the bands of a pair
 // chained across warps, pw_band.cuh).  DIRS: the direction sweep of traced
 // pairs; otherwise pair maxima into band_max (indexed by BandPair.slot).
@@ -1657,9 +1781,8 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
 
     double trace_ms = 0, walk_ms = 0;
     int64_t total_starts = 0;
+    int64_t acc_n = 0, acc_ops = 0;  // hits and operation bytes accumulated over the waves
     inf.setup_ms += wall_ms() - t_setup;
-    std::vector<DevHit> all_hits;
-    std::vector<char> all_ops;
     for (size_t wv = 0; wv < waves.size(); ++wv) {
         const size_t i0 = waves[wv].first, i1 = waves[wv].second;
         std::vector<WorkItem> wi(items2.begin() + i0, items2.begin() + i1);
@@ -1840,7 +1963,8 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
             PW_LAUNCH(gather_kernel, gb, tb, 0, e->stream, TA, e->starts.as<StartRec>());
             e->launches++;
             if ((c = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, c, "gather launch");
-            e->h_starts.resize(first_rec + (size_t)wave_starts);
+            if (!e->h_starts.resize_keep(first_rec + (size_t)wave_starts))
+                return fail(e, PW_ERR_NOMEM, "host memory for the starting points");
             if ((c = cudaMemcpyAsync(e->h_starts.data() + first_rec, e->starts.p, wave_starts * sizeof(StartRec),
                                      cudaMemcpyDeviceToHost, e->stream)) != cudaSuccess ||
                 (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
@@ -1865,15 +1989,19 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
             inf.truncated = 1;
         }
 
-        // walk; each kept hit reserves its column operations (ops offsets)
-        int nh = 0;
-        std::vector<DevHit> hh;
-        std::vector<char> ops;
+        // walk; the hits go straight into the accumulated hit array, and each
+        // reserves its column operations at an absolute offset of the
+        // accumulated operations (ops_total starts at the bytes used so far)
         if (wave_starts > 0) {
-            if ((c = e->hits.reserve(e->stream, wave_starts * sizeof(DevHit))) != cudaSuccess) return cuda_fail(e, c, "alloc hits");
+            if ((c = e->acc_hits.grow_keep(e->stream, (size_t)acc_n * sizeof(DevHit),
+                                           (size_t)(acc_n + wave_starts) * sizeof(DevHit))) != cudaSuccess)
+                return cuda_fail(e, c, "alloc hits");
             if ((c = e->hit_count.reserve(e->stream, 16)) != cudaSuccess) return cuda_fail(e, c, "alloc");
-            cudaMemsetAsync(e->hit_count.p, 0, 16, e->stream);
-            TA.hits = e->hits.as<DevHit>();
+            const unsigned long long init[2] = {0ull, (unsigned long long)acc_ops};
+            if ((c = cudaMemcpyAsync(e->hit_count.p, init, sizeof(init), cudaMemcpyHostToDevice, e->stream)) !=
+                cudaSuccess)
+                return cuda_fail(e, c, "reset hit count");
+            TA.hits = e->acc_hits.as<DevHit>() + acc_n;
             TA.hit_count = e->hit_count.as<int>();
             TA.ops_total = (unsigned long long*)(e->hit_count.as<char>() + 8);
             TA.max_hits = (int)wave_starts;
@@ -1885,29 +2013,19 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
             if ((c = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, c, "walk launch");
             std::vector<int64_t> cnt;
             if ((c = download(e, cnt, TA.hit_count, 2)) != cudaSuccess) return cuda_fail(e, c, "walk");
-            nh = (int)std::min<int64_t>((int32_t)(cnt[0] & 0xffffffff), wave_starts);
-            const int64_t ops_total = cnt[1];
+            const int nh = (int)std::min<int64_t>((int32_t)(cnt[0] & 0xffffffff), wave_starts);
+            const int64_t ops_end = cnt[1];
             if (nh) {
-                // column operations of the kept hits, then hits and operations to the host
-                if ((c = e->ops.reserve(e->stream, std::max<int64_t>(ops_total, 16))) != cudaSuccess)
+                // column operations of the kept hits
+                if ((c = e->acc_ops.grow_keep(e->stream, (size_t)acc_ops, (size_t)std::max<int64_t>(ops_end, 16))) !=
+                    cudaSuccess)
                     return cuda_fail(e, c, "alloc ops");
-                TA.ops = e->ops.as<char>();
-                PW_LAUNCH(ops_kernel, (nh + 127) / 128, 128, 0, e->stream, TA, e->hits.as<DevHit>(), nh);
+                TA.ops = e->acc_ops.as<char>();
+                PW_LAUNCH(ops_kernel, (nh + 127) / 128, 128, 0, e->stream, TA, TA.hits, nh);
                 e->launches++;
                 if ((c = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, c, "ops launch");
-                if ((c = download(e, hh, TA.hits, (size_t)nh)) != cudaSuccess) return cuda_fail(e, c, "copy hits");
-                if ((c = download(e, ops, TA.ops, (size_t)ops_total)) != cudaSuccess) return cuda_fail(e, c, "copy ops");
-            }
-        }
-        if (nh) {
-            const int64_t base = (int64_t)all_ops.size();
-            if (all_hits.empty()) {
-                all_hits.swap(hh);
-                all_ops.swap(ops);
-            } else {
-                for (DevHit& h : hh) h.ops_offset += base;
-                all_ops.insert(all_ops.end(), ops.begin(), ops.end());
-                all_hits.insert(all_hits.end(), hh.begin(), hh.end());
+                acc_n += nh;
+                acc_ops = ops_end;
             }
         }
         cudaEventRecord(e->ev[3], e->stream);
@@ -1919,122 +2037,11 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         walk_ms += t2;
     }
 
-    // hits in the reference's HitList order: ascending score, then the pinned
-    // emission order of their starting points (SmithWaterman.py:699)
+    // hits in the reference's HitList order and their strings, on the device
+    // (pw_finish.cuh), then both to the host
     const double t_finish = wall_ms();
-    struct HKey {
-        uint64_t a, b, c;
-        int64_t idx;
-        bool operator<(const HKey& o) const {
-            return a != o.a ? a < o.a : (b != o.b ? b < o.b : (c != o.c ? c < o.c : idx < o.idx));
-        }
-    };
-    const int64_t nhits = (int64_t)all_hits.size();
-    std::vector<HKey> keys((size_t)nhits);
-    // (score ascending; block anti-diagonal, block x descending; target, query
-    // ascending; cell anti-diagonal descending; row ascending) packed into
-    // three words; scores are >= 0, so their fp32 bits order like the values
-    parallel_for(nhits, [&](int64_t k0, int64_t k1) {
-        for (int64_t k = k0; k < k1; ++k) {
-            const DevHit& h = all_hits[k];
-            uint32_t sb;
-            std::memcpy(&sb, &h.score, 4);
-            const uint32_t diag = (uint32_t)((h.end_x >> 3) + (h.end_y >> 3));
-            const uint32_t small = (uint32_t)((h.end_x & 7) + (h.end_y & 7));
-            keys[k] = HKey{((uint64_t)sb << 32) | (0xFFFFFFFFu - diag),
-                           ((uint64_t)(0xFFFFFFFFu - (uint32_t)(h.end_x >> 3)) << 32) | (uint32_t)h.target,
-                           ((uint64_t)(uint32_t)h.query << 32) | ((uint64_t)(0xFFu - small) << 8) | (uint32_t)(h.end_y & 7),
-                           k};
-        }
-    });
-    {
-        // sort runs in parallel, then merge them pairwise
-        const int64_t hw = std::max<int64_t>(1, (int64_t)std::thread::hardware_concurrency());
-        int runs = (int)std::min<int64_t>(std::min<int64_t>(hw, 32), std::max<int64_t>(1, nhits / (1 << 16)));
-        std::vector<int64_t> bnd(runs + 1);
-        for (int r = 0; r <= runs; ++r) bnd[r] = nhits * r / runs;
-        {
-            std::vector<std::thread> th;
-            for (int r = 0; r < runs; ++r)
-                th.emplace_back([&, r] { std::sort(keys.begin() + bnd[r], keys.begin() + bnd[r + 1]); });
-            for (auto& t : th) t.join();
-        }
-        std::vector<HKey> tmp(runs > 1 ? keys.size() : 0);
-        while (runs > 1) {
-            std::vector<int64_t> nb;
-            std::vector<std::thread> th;
-            for (int r = 0; r < runs; r += 2) {
-                nb.push_back(bnd[r]);
-                if (r + 1 < runs)
-                    th.emplace_back([&, r] {
-                        std::merge(keys.begin() + bnd[r], keys.begin() + bnd[r + 1], keys.begin() + bnd[r + 1],
-                                   keys.begin() + bnd[r + 2], tmp.begin() + bnd[r]);
-                    });
-                else
-                    th.emplace_back([&, r] {
-                        std::copy(keys.begin() + bnd[r], keys.begin() + bnd[r + 1], tmp.begin() + bnd[r]);
-                    });
-            }
-            for (auto& t : th) t.join();
-            nb.push_back(nhits);
-            keys.swap(tmp);
-            bnd.swap(nb);
-            runs = (int)bnd.size() - 1;
-        }
-    }
-    std::vector<int64_t> soff2((size_t)nhits + 1, 0);
-    for (int64_t k = 0; k < nhits; ++k) soff2[k + 1] = soff2[k] + 3 * (int64_t)all_hits[keys[k].idx].n_cols;
-    const int64_t str_bytes = soff2[nhits];
-    e->h_hits.resize((size_t)nhits);
-    e->h_strings.resize((size_t)str_bytes);
-    // hits and their alignment strings (from the column operations), in order
-    parallel_for(nhits, [&](int64_t k0, int64_t k1) {
-        for (int64_t k = k0; k < k1; ++k) {
-            const DevHit& d = all_hits[keys[k].idx];
-            pw_hit& h = e->h_hits[k];
-            h.query = d.query;
-            h.target = d.target;
-            h.s_start = d.s_start;
-            h.s_end = d.s_end;
-            h.t_start = d.t_start;
-            h.t_end = d.t_end;
-            h.score = d.score;
-            h.matches = d.matches;
-            h.mismatches = d.mismatches;
-            h.n_cols = d.n_cols;
-            h.str_offset = soff2[k];
-            char* sq = e->h_strings.data() + h.str_offset;
-            char* al = sq + h.n_cols;
-            char* tg = al + h.n_cols;
-            const uint8_t* qs = e->Q.raw.data() + e->Q.off[d.query];
-            const uint8_t* ts = e->T.raw.data() + e->T.off[d.target];
-            int x = d.s_start, y = d.t_start;
-            const char* ops = all_ops.data() + d.ops_offset;
-            for (int i = 0; i < d.n_cols; ++i) {
-                const char op = ops[i];
-                if (op == 'M') {
-                    const uint8_t ca = ts[y], cb = qs[x];
-                    const bool la = (ca >= 'A' && ca <= 'Z') || (ca >= 'a' && ca <= 'z');
-                    const bool eq = la ? ((ca | 0x20) == (cb | 0x20)) : ca == cb;
-                    sq[i] = (char)cb;
-                    tg[i] = (char)ca;
-                    al[i] = eq ? '|' : '.';
-                    ++x;
-                    ++y;
-                } else if (op == 'I') {
-                    sq[i] = (char)qs[x];
-                    tg[i] = '-';
-                    al[i] = ' ';
-                    ++x;
-                } else {
-                    sq[i] = '-';
-                    tg[i] = (char)ts[y];
-                    al[i] = ' ';
-                    ++y;
-                }
-            }
-        }
-    }, 1 << 12);
+    int64_t str_bytes = 0;
+    if ((c = finish_hits(e, acc_n, &str_bytes)) != cudaSuccess) return cuda_fail(e, c, "order hits");
     inf.starting_points = total_starts;
     inf.hits = (int64_t)e->h_hits.size();
     inf.string_bytes = str_bytes;
@@ -2089,7 +2096,7 @@ extern "C" int pw_get_starting_points(pw_engine* e, void* out36, int64_t max_poi
     if (!e) return PW_ERR_ARG;
     // emission order: block anti-diagonal descending, block x descending,
     // target, query, cell anti-diagonal descending, thread y ascending
-    std::vector<StartRec> s = e->h_starts;
+    std::vector<StartRec> s(e->h_starts.data(), e->h_starts.data() + e->h_starts.size());
     std::stable_sort(s.begin(), s.end(), [](const StartRec& a, const StartRec& b) {
         auto k = [](const StartRec& r) {
             return std::make_tuple(-(int64_t)((r.x >> 3) + (r.y >> 3)), -(int64_t)(r.x >> 3), r.target, r.query,

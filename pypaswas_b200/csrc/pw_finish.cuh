@@ -1,0 +1,103 @@
+// pw_finish.cuh -- hit order and alignment strings on the device.
+//
+// The walk leaves its hits (DevHit) and their column operations ('M', 'I',
+// 'D' per alignment column) in device memory, appended across memory waves.
+// These kernels put the hits in the order the reference's HitList has them
+// and spell out the three alignment strings of every hit, so that the host
+// receives the final records in two copies.
+//
+// Order (SmithWaterman._print_alignments appends in the pinned emission
+// order of the starting points and HitList sorts by score,
+// SmithWaterman.py:699): score ascending; then block anti-diagonal
+// descending, block x descending, target, query, cell anti-diagonal
+// descending, row ascending; then walk order.  The key is packed into three
+// 64-bit words (scores are >= 0, so their fp32 bits order like the values)
+// and sorted by three stable radix passes, least significant word first,
+// starting from the walk order, which gives the last tie-break.
+#pragma once
+#include "../../include/paswas_b200.h"
+#include "pw_device.cuh"
+
+namespace pw {
+
+__global__ void hit_key_kernel(const DevHit* h, int64_t n, uint64_t* ka, uint64_t* kb, uint64_t* kc, int32_t* idx) {
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const DevHit d = h[k];
+        const uint32_t sb = __float_as_uint(d.score);
+        const uint32_t diag = (uint32_t)((d.end_x >> 3) + (d.end_y >> 3));
+        const uint32_t small = (uint32_t)((d.end_x & 7) + (d.end_y & 7));
+        ka[k] = ((uint64_t)sb << 32) | (0xFFFFFFFFu - diag);
+        kb[k] = ((uint64_t)(0xFFFFFFFFu - (uint32_t)(d.end_x >> 3)) << 32) | (uint32_t)d.target;
+        kc[k] = ((uint64_t)(uint32_t)d.query << 32) | ((uint64_t)(0xFFu - small) << 8) | (uint32_t)(d.end_y & 7);
+        idx[k] = (int32_t)k;
+    }
+}
+
+__global__ void gather_key_kernel(const uint64_t* src, const int32_t* idx, int64_t n, uint64_t* dst) {
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+        dst[k] = src[idx[k]];
+}
+
+// String bytes of the hit at each sorted position (three strings of n_cols).
+__global__ void hit_len_kernel(const DevHit* h, const int32_t* idx, int64_t n, int64_t* len) {
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+        len[k] = 3 * (int64_t)h[idx[k]].n_cols;
+}
+
+// The hit records in order and their strings: sequence_match (query residue
+// or '-'), alignment ('|' for equal residues -- letters compared without
+// case -- '.' for a mismatch, ' ' in a gap) and target_match, one column per
+// operation, as SmithWaterman._print_alignments spells them
+// (SmithWaterman.py:765-815).
+__global__ void hit_out_kernel(const DevHit* h, const int32_t* idx, const int64_t* soff, int64_t n, const char* ops,
+                               const uint8_t* q_raw, const int64_t* q_off, const uint8_t* t_raw,
+                               const int64_t* t_off, pw_hit* out, char* str) {
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const DevHit d = h[idx[k]];
+        pw_hit o;
+        o.query = d.query;
+        o.target = d.target;
+        o.s_start = d.s_start;
+        o.s_end = d.s_end;
+        o.t_start = d.t_start;
+        o.t_end = d.t_end;
+        o.score = d.score;
+        o.matches = d.matches;
+        o.mismatches = d.mismatches;
+        o.n_cols = d.n_cols;
+        o.str_offset = soff[k];
+        out[k] = o;
+        char* sq = str + o.str_offset;
+        char* al = sq + d.n_cols;
+        char* tg = al + d.n_cols;
+        const uint8_t* qs = q_raw + q_off[d.query];
+        const uint8_t* ts = t_raw + t_off[d.target];
+        const char* op = ops + d.ops_offset;
+        int x = d.s_start, y = d.t_start;
+        for (int i = 0; i < d.n_cols; ++i) {
+            const char c = op[i];
+            if (c == 'M') {
+                const uint8_t ca = ts[y], cb = qs[x];
+                const bool la = (ca >= 'A' && ca <= 'Z') || (ca >= 'a' && ca <= 'z');
+                const bool eq = la ? ((ca | 0x20) == (cb | 0x20)) : ca == cb;
+                sq[i] = (char)cb;
+                tg[i] = (char)ca;
+                al[i] = eq ? '|' : '.';
+                ++x;
+                ++y;
+            } else if (c == 'I') {
+                sq[i] = (char)qs[x];
+                tg[i] = '-';
+                al[i] = ' ';
+                ++x;
+            } else {
+                sq[i] = '-';
+                tg[i] = (char)ts[y];
+                al[i] = ' ';
+                ++y;
+            }
+        }
+    }
+}
+
+}  // namespace pw
