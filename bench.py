@@ -359,7 +359,11 @@ def main():
         infos.append(info.as_dict())
     clocks = sampler.stop()
     t_ms = reduce_max(float(sum(times)))
-    step_stats = {"min": float(min(times)), "median": float(np.median(times)), "max": float(max(times))}
+    step_stats = {"min": float(min(times)), "median": float(np.median(times)), "max": float(max(times)),
+                  "all": [round(float(t), 3) for t in times],
+                  "call_ms": [round(float(i["total_ms"]), 3) for i in infos],
+                  "phase_ms": {k: [round(float(i[k]), 2) for i in infos] for k in
+                               ("score_ms", "trace_ms", "walk_ms", "setup_ms", "finish_ms")}}
     value = whole_job_gcups(cells, args.steps, t_ms * 1e-3, world)
     n_pairs = len(w.pairs) if w.pairs is not None else w.n_queries * len(w.targets)
     ms_per_step = t_ms / args.steps

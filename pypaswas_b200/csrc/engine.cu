@@ -45,6 +45,20 @@ static double wall_ms() {
 
 // Runs f(begin, end) over [0, n) split into contiguous ranges, one host
 // thread each (ranges in order: range k covers [n * k / T, n * (k + 1) / T)).
+// Host-phase timing on stderr when the environment sets PW_HOST_TRACE
+// (diagnostics of the host orchestration between kernels; off by default).
+struct HostTrace {
+    bool on;
+    double t;
+    HostTrace() : on(std::getenv("PW_HOST_TRACE") != nullptr), t(wall_ms()) {}
+    void mark(const char* what) {
+        if (!on) return;
+        const double n = wall_ms();
+        std::fprintf(stderr, "[pw host] %-34s %10.3f ms\n", what, n - t);
+        t = n;
+    }
+};
+
 template <typename F>
 static void parallel_for(int64_t n, F&& f, int64_t min_chunk = 1 << 15) {
     const int64_t hw = std::max<int64_t>(1, (int64_t)std::thread::hardware_concurrency());
@@ -236,10 +250,11 @@ struct pw_engine {
     DevBuf cmat_i8, cmat_f, pair_max, items, items_alt, counter, bnd_pool, q_order2;
     DevBuf band_pairs, band_entries, band_prog, band_max, band_ring, band_out;  // band sweep (pw_band.cuh)
     DevBuf scan_tmp;  // CUB scan / select scratch
-    DevBuf prune_flags, prune_cnt, prune_sel;  // phase-2 pruning on the device
+    DevBuf prune_flags, prune_cnt, prune_sel, t_skip, q_count;  // phase-2 pruning on the device
     // hits and column operations of all memory waves, then their order and strings
     DevBuf acc_hits, acc_ops, fk_a, fk_b, fk_c, fk_t, fk_g, fi_a, fi_b, f_len, f_soff, f_out, f_str;
     HostBuf<int64_t> h_sel;
+    HostBuf<int32_t> h_ptq, h_p2order;  // phase-2 pair lists (kept across calls: no page faults, no zero fill)
     DevBuf chain_items, chain_info, chain_prog, chain_max, chain_ring_off, chain_ring, chain_abort, p1_items;
     // plan of the 16-bit score phase (work items, classes, chain queue), kept
     // on the device and reused while inputs, scoring, flags and tuning stay
@@ -413,13 +428,16 @@ extern "C" int pw_set_targets(pw_engine* e, const uint8_t* residues, const int64
 
 namespace {
 
-enum SClass { kS16 = 0, kS32 = 1, kS64 = 2, kS32Multi = 3, kNumClasses = 4 };
+// Strip classes: one-strip sweeps of 16, 32, 48 (linear) and 64 (linear)
+// rows, and multi-strip items of 32-row strips.
+enum SClass { kS16 = 0, kS32 = 1, kS64 = 2, kS32Multi = 3, kS48 = 4, kNumClasses = 5 };
 
-int class_S(int c) { return c == kS16 ? 16 : (c == kS64 ? 64 : 32); }
+int class_S(int c) { return c == kS16 ? 16 : (c == kS64 ? 64 : (c == kS48 ? 48 : 32)); }
 
 int pick_class(int lt, bool affine) {
     if (lt <= 16) return kS16;
     if (lt <= 32) return kS32;
+    if (!affine && lt <= 48) return kS48;
     if (!affine && lt <= 64) return kS64;
     return kS32Multi;
 }
@@ -463,6 +481,7 @@ cudaError_t launch_class_o(pw_engine* e, int cls, bool affine, const KernelArgs&
     switch (cls) {
         case kS16: return launch_sweep<T, 16, false, false, PH, TR>(e, A, counter);
         case kS32: return launch_sweep<T, 32, false, false, PH, TR>(e, A, counter);
+        case kS48: return launch_sweep<T, 48, false, false, PH, TR>(e, A, counter);
         case kS64: return launch_sweep<T, 64, false, false, PH, TR>(e, A, counter);
         default: return launch_sweep<T, 32, false, true, PH, TR>(e, A, counter);
     }
@@ -476,6 +495,14 @@ cudaError_t launch_class(pw_engine* e, int cls, bool affine, const KernelArgs& A
 }
 
 }  // namespace
+
+template <typename HT>
+static cudaError_t upload(pw_engine* e, DevBuf& b, const HostBuf<HT>& v) {
+    cudaError_t c = b.reserve(e->stream, std::max<size_t>(v.size() * sizeof(HT), 16));
+    if (c != cudaSuccess) return c;
+    if (v.empty()) return cudaSuccess;
+    return cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(HT), cudaMemcpyHostToDevice, e->stream);
+}
 
 template <typename HT>
 static cudaError_t upload(pw_engine* e, DevBuf& b, const std::vector<HT>& v) {
@@ -813,6 +840,7 @@ static cudaError_t launch_s16_class(pw_engine* e, int cls, bool affine, const Sc
     }
     if (cls == kS16) return launch_s16<16, false, false, DL>(e, A);
     if (cls == kS32) return launch_s16<32, false, false, DL>(e, A);
+    if (cls == kS48) return launch_s16<48, false, false, DL>(e, A);
     if (cls == kS64) return launch_s16<64, false, false, DL>(e, A);
     return launch_s16<32, false, true, DL>(e, A);
 }
@@ -1565,14 +1593,17 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
 
     // ---------------------------------------------------------- phase 2
     const double t_setup = wall_ms();
+    HostTrace ht;
     // Pairs that can yield a starting point, per target in query length order,
     // 32 per work item.  The reference traces every pair whose maximum reaches
     // MINIMUM_SCORE (default_main.cu:596), but a starting point also needs a
     // cell with H >= max(LOWER_LIMIT_SCORE * max, maxPossibleScore) (:609) and
     // no cell exceeds the pair maximum, so a pair whose maximum is below that
     // threshold has no starting point and contributes nothing: it is skipped.
-    std::vector<std::vector<int32_t>> pass_t(nt);   // per target: passing queries, length order
-    std::vector<std::vector<int32_t>> pass_q;       // per query: passing targets, length order (when needed)
+    // passing pairs per target, query length order: pt_q[pt_off[t] .. pt_off[t + 1])
+    std::vector<int64_t> pt_off((size_t)nt + 1, 0);
+    HostBuf<int32_t>& pt_q = e->h_ptq;
+    pt_q.clear();
     int64_t min_pass = 0, n_pass = 0;
     {
         // the test runs on the device over the resident maxima (prune_kernel);
@@ -1595,6 +1626,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
             return cuda_fail(e, c, "prune pairs");
         min_pass = (int64_t)cnt[0];
         n_pass = (int64_t)cnt[1];
+        ht.mark("prune kernel + counts");
         if (n_pass > 0) {
             int64_t* d_count = e->prune_cnt.as<int64_t>() + 2;
             thrust::counting_iterator<int64_t> ids(0);
@@ -1613,70 +1645,86 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
                 (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
                 return cuda_fail(e, c, "copy passing pairs");
             const int64_t* sel = e->h_sel.data();
+            for (int t = 0; t <= nt; ++t) pt_off[t] = std::lower_bound(sel, sel + n_pass, (int64_t)t * nq) - sel;
+            if (!pt_q.resize((size_t)n_pass)) return fail(e, PW_ERR_NOMEM, "host memory for the passing pairs");
             std::mutex mu;
-            parallel_for(nt, [&](int64_t t0, int64_t t1) {
-                int64_t lo = std::lower_bound(sel, sel + n_pass, t0 * (int64_t)nq) - sel, tc = 0;
-                for (int64_t t = t0; t < t1; ++t) {
-                    const int64_t end = (t + 1) * (int64_t)nq;
-                    int64_t hi = lo;
-                    while (hi < n_pass && sel[hi] < end) ++hi;
-                    std::vector<int32_t>& lst = pass_t[t];
-                    lst.reserve((size_t)(hi - lo));
-                    for (int64_t j = lo; j < hi; ++j) {
-                        const int q = pr.order[(size_t)(sel[j] - t * (int64_t)nq)];
-                        lst.push_back(q);
-                        tc += (int64_t)qlen[q] * tlen[t];
-                    }
-                    lo = hi;
+            parallel_for(n_pass, [&](int64_t j0, int64_t j1) {
+                int64_t tc = 0;
+                for (int64_t j = j0; j < j1; ++j) {
+                    const int t = (int)(sel[j] / nq);
+                    const int q = pr.order[(size_t)(sel[j] - (int64_t)t * nq)];
+                    pt_q[j] = q;
+                    tc += (int64_t)qlen[q] * tlen[t];
                 }
                 std::lock_guard<std::mutex> g(mu);
                 inf.traced_cells += tc;
-            }, std::max<int64_t>(1, std::min<int64_t>(nt, ((int64_t)1 << 16) * nt / std::max<int64_t>(n_pass, 1))));
+            }, (int64_t)1 << 16);
         }
+        ht.mark("passing pairs to per-target lists");
     }
+    auto span_n = [&](int t) -> int64_t { return pt_off[t + 1] - pt_off[t]; };
     // Traced pairs with targets longer than one register strip go to the
     // one-warp-per-pair sweep (pw_band.cuh); the others are grouped 32 to
     // a warp, one pair per lane, in the orientation where they cluster
     // (slot cost = strip length x longest lane x 32 per item).
     const bool warp_ok = pr.int_path && !plain;
     std::vector<std::pair<int32_t, int32_t>> warp_pairs;  // (query, target)
+    std::vector<char> t_warp((size_t)nt, 0);              // targets whose pairs went to the warp sweep
     if (warp_ok) {
         // short targets stay on the strip sweep only when there are enough of
         // them to give every SM a full warp: a few strip items run one lane per
         // pair, latency bound, far longer than the same pairs one per warp
         int64_t n_short = 0;
         for (int t = 0; t < nt; ++t)
-            if (tlen[t] <= 64) n_short += (int64_t)pass_t[t].size();
+            if (tlen[t] <= 64) n_short += span_n(t);
         const bool all_warp = n_short < (int64_t)kWarp * e->sm_count;
         for (int t = 0; t < nt; ++t) {
             if (tlen[t] <= 64 && !all_warp) continue;
-            for (int32_t q : pass_t[t]) warp_pairs.push_back({q, t});
-            pass_t[t].clear();
+            for (int64_t j = pt_off[t]; j < pt_off[t + 1]; ++j) warp_pairs.push_back({pt_q[j], t});
+            t_warp[t] = 1;
         }
     }
+    auto live_n = [&](int t) -> int64_t { return t_warp[t] ? 0 : span_n(t); };
+    ht.mark("warp-sweep routing");
     const int per_item = plain ? 1 : kWarp;
     double cost_t = 0, cost_q = 0;
     for (int t = 0; t < nt; ++t)
-        for (size_t g = 0; g < pass_t[t].size(); g += per_item) cost_t += (double)tlen[t] * qlen[pass_t[t][g]] * per_item;
+        for (int64_t g = 0; g < live_n(t); g += per_item) cost_t += (double)tlen[t] * qlen[pt_q[pt_off[t] + g]] * per_item;
     // the transposed orientation (queries as strips) can only win if even a
     // lower bound of its slot cost -- every query's groups paying the
-    // shortest target -- is below the cost of the direct one
+    // shortest target -- is below the cost of the direct one; the per-query
+    // group counts of that bound are summed on the device
     bool trans2 = false;
-    {
-        std::vector<int32_t> kq(nq, 0);
-        for (int t = 0; t < nt; ++t)
-            for (int32_t q : pass_t[t]) ++kq[q];
+    std::vector<std::vector<int32_t>> pass_q;  // per query: passing targets, length order (when needed)
+    if (n_pass > 0 && cost_t > 0) {
         int tmin = INT32_MAX;
         for (int t = 0; t < nt; ++t) tmin = std::min(tmin, std::max(tlen[t], 1));
-        double lb_q = 0;
-        for (int q = 0; q < nq; ++q)
-            if (kq[q]) lb_q += (double)((kq[q] + per_item - 1) / per_item) * per_item * qlen[q] * tmin;
+        std::vector<uint8_t> skip(t_warp.begin(), t_warp.end());
+        unsigned long long lb_units = 0;  // sum over queries of ceil(k / per_item) * per_item * len
+        if ((c = upload(e, e->t_skip, skip)) != cudaSuccess ||
+            (c = e->q_count.reserve(e->stream, (size_t)nq * sizeof(int32_t))) != cudaSuccess ||
+            (c = cudaMemsetAsync(e->q_count.p, 0, (size_t)nq * sizeof(int32_t), e->stream)) != cudaSuccess ||
+            (c = cudaMemsetAsync(e->prune_cnt.p, 0, sizeof(unsigned long long), e->stream)) != cudaSuccess)
+            return cuda_fail(e, c, "query counts");
+        const int g1 = (int)std::max<int64_t>(1, std::min<int64_t>((n_pass + 255) / 256, (int64_t)e->sm_count * 16));
+        PW_LAUNCH(query_count_kernel, g1, 256, 0, e->stream, (const int64_t*)e->prune_sel.as<int64_t>(), n_pass, nq,
+                  e->q_order.as<int32_t>(), e->t_skip.as<uint8_t>(), e->q_count.as<int32_t>());
+        const int g2 = (int)std::max<int64_t>(1, std::min<int64_t>((nq + 255) / 256, (int64_t)e->sm_count * 16));
+        PW_LAUNCH(group_bound_kernel, g2, 256, 0, e->stream, (const int32_t*)e->q_count.as<int32_t>(), nq,
+                  e->q_len.as<int32_t>(), per_item, e->prune_cnt.as<unsigned long long>());
+        e->launches += 2;
+        if ((c = cudaGetLastError()) != cudaSuccess ||
+            (c = cudaMemcpyAsync(&lb_units, e->prune_cnt.p, sizeof(lb_units), cudaMemcpyDeviceToHost, e->stream)) !=
+                cudaSuccess ||
+            (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
+            return cuda_fail(e, c, "query counts");
+        const double lb_q = (double)lb_units * tmin;
         if (lb_q < cost_t) {
             pass_q.resize(nq);
             std::vector<int32_t> rank_t(nt);
             for (int k = 0; k < nt; ++k) rank_t[pr.order_t[k]] = k;
             for (int t = 0; t < nt; ++t)
-                for (int32_t q : pass_t[t]) pass_q[q].push_back(t);
+                for (int64_t j = pt_off[t]; j < pt_off[t] + live_n(t); ++j) pass_q[pt_q[j]].push_back(t);
             for (int q = 0; q < nq; ++q)
                 std::stable_sort(pass_q[q].begin(), pass_q[q].end(),
                                  [&](int a, int b) { return rank_t[a] < rank_t[b]; });
@@ -1686,31 +1734,45 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
             trans2 = cost_q < cost_t;
         }
     }
-    std::vector<int32_t> p2_order;
-    std::vector<WorkItem> items2;
-    std::vector<int> cls2;
-    std::vector<int64_t> bytes2;
+    ht.mark("phase-2 orientation");
     const int n_strip = trans2 ? nq : nt;
+    // per strip: its pairs and items at offsets from prefix sums, filled by host threads
+    std::vector<int64_t> s_pairs((size_t)n_strip + 1, 0), s_items((size_t)n_strip + 1, 0);
     for (int st = 0; st < n_strip; ++st) {
-        const std::vector<int32_t>& pass = trans2 ? pass_q[st] : pass_t[st];
-        const int ls = trans2 ? qlen[st] : tlen[st];
-        for (size_t g = 0; g < pass.size(); g += per_item) {
-            WorkItem w;
-            memset(&w, 0, sizeof(w));
-            w.target = st;
-            w.first = (int32_t)p2_order.size();
-            w.lanes = (int32_t)std::min<size_t>(per_item, pass.size() - g);
-            for (int l = 0; l < w.lanes; ++l) p2_order.push_back(pass[g + l]);
-            w.xmax = trans2 ? tlen[p2_order[w.first]] : qlen[p2_order[w.first]];
-            w.orient = trans2 ? 1 : 0;
-            const int k = pick_class(ls, e->affine);
-            w.S = class_S(k);
-            items2.push_back(w);
-            cls2.push_back(k);
-            const int64_t strips = std::max<int64_t>((ls + w.S - 1) / w.S, 1);
-            bytes2.push_back(strips * w.S * align_up(std::max(w.xmax, 1), 4) * kWarp);
-        }
+        const int64_t np_ = trans2 ? (int64_t)pass_q[st].size() : live_n(st);
+        s_pairs[st + 1] = s_pairs[st] + np_;
+        s_items[st + 1] = s_items[st] + (np_ + per_item - 1) / per_item;
     }
+    HostBuf<int32_t>& p2_order = e->h_p2order;
+    if (!p2_order.resize((size_t)s_pairs[n_strip])) return fail(e, PW_ERR_NOMEM, "host memory for the phase-2 order");
+    std::vector<WorkItem> items2((size_t)s_items[n_strip]);
+    std::vector<int> cls2((size_t)s_items[n_strip]);
+    std::vector<int64_t> bytes2((size_t)s_items[n_strip]);
+    parallel_for(n_strip, [&](int64_t s0, int64_t s1) {
+        for (int64_t st = s0; st < s1; ++st) {
+            const int32_t* pass = trans2 ? pass_q[st].data() : pt_q.data() + pt_off[st];
+            const int64_t np_ = s_pairs[st + 1] - s_pairs[st];
+            const int ls = trans2 ? qlen[st] : tlen[st];
+            const int k = pick_class(ls, e->affine);
+            const int S = class_S(k);
+            const int64_t strips = std::max<int64_t>((ls + S - 1) / S, 1);
+            int64_t it = s_items[st];
+            for (int64_t g = 0; g < np_; g += per_item, ++it) {
+                WorkItem w;
+                memset(&w, 0, sizeof(w));
+                w.target = (int32_t)st;
+                w.first = (int32_t)(s_pairs[st] + g);
+                w.lanes = (int32_t)std::min<int64_t>(per_item, np_ - g);
+                std::memcpy(p2_order.data() + w.first, pass + g, (size_t)w.lanes * sizeof(int32_t));
+                w.xmax = trans2 ? tlen[pass[g]] : qlen[pass[g]];
+                w.orient = trans2 ? 1 : 0;
+                w.S = S;
+                items2[it] = w;
+                cls2[it] = k;
+                bytes2[it] = strips * S * align_up(std::max(w.xmax, 1), 4) * kWarp;
+            }
+        }
+    }, std::max<int64_t>(1, (int64_t)n_strip * ((int64_t)1 << 15) / std::max<int64_t>(s_pairs[n_strip], 1)));
     // warp items: longest first (dynamic scheduling tail)
     std::stable_sort(warp_pairs.begin(), warp_pairs.end(), [&](const std::pair<int32_t, int32_t>& a,
                                                                const std::pair<int32_t, int32_t>& b) {
@@ -1732,6 +1794,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         bytes2.push_back(align_up(warp_code_bytes(qlen[wp.first], tlen[wp.second]), 16));
         qmax_warp = std::max(qmax_warp, qlen[wp.first]);
     }
+    ht.mark("phase-2 work items");
     inf.traced_pairs = n_pass;
     inf.minimum_pairs = min_pass;
     inf.trace_orientation = trans2 ? 1 : 0;
@@ -1819,14 +1882,18 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         if ((c = e->metas.reserve(e->stream, n_pairs * sizeof(PairMeta))) != cudaSuccess) return cuda_fail(e, c, "alloc metas");
         if ((c = e->n_cand.reserve(e->stream, n_pairs * sizeof(int32_t))) != cudaSuccess) return cuda_fail(e, c, "alloc");
         if ((c = e->n_starts.reserve(e->stream, n_pairs * sizeof(int32_t))) != cudaSuccess) return cuda_fail(e, c, "alloc");
-        std::vector<int64_t> cbase(n_pairs);
-        std::vector<int32_t> ccap(n_pairs, kCandCap);
-        for (int64_t p = 0; p < n_pairs; ++p) cbase[p] = p * kCandCap;
+        // every pair starts with a slot of kCandCap candidates (filled on the device)
         int64_t cand_total = n_pairs * kCandCap;
         if ((c = e->cands.reserve(e->stream, cand_total * sizeof(Cand))) != cudaSuccess) return cuda_fail(e, c, "alloc cands");
-        if ((c = upload(e, e->cand_base, cbase)) != cudaSuccess) return cuda_fail(e, c, "upload cand base");
-        if ((c = upload(e, e->cand_cap, ccap)) != cudaSuccess) return cuda_fail(e, c, "upload cand cap");
+        if ((c = e->cand_base.reserve(e->stream, (size_t)std::max<int64_t>(n_pairs, 2) * sizeof(int64_t))) != cudaSuccess ||
+            (c = e->cand_cap.reserve(e->stream, (size_t)std::max<int64_t>(n_pairs, 4) * sizeof(int32_t))) != cudaSuccess)
+            return cuda_fail(e, c, "alloc candidate slots");
+        const int gslot = (int)std::max<int64_t>(1, std::min<int64_t>((n_pairs + 255) / 256, (int64_t)e->sm_count * 16));
+        PW_LAUNCH(cand_slot_kernel, gslot, 256, 0, e->stream, e->cand_base.as<int64_t>(), e->cand_cap.as<int32_t>(),
+                  n_pairs, kCandCap);
+        e->launches++;
         if ((c = upload(e, e->items, wi)) != cudaSuccess) return cuda_fail(e, c, "upload items");
+        ht.mark("wave buffers");
         A.codes = e->codes.as<uint8_t>();
         A.metas = e->metas.as<PairMeta>();
         A.cands = e->cands.as<Cand>();
@@ -1855,17 +1922,37 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         }
         // candidate overflow: pairs with more candidates than their slot get an
         // exact slot past the regular ones, and their items are swept again
+        // (counted on the device; the host reads the per-pair counts only then)
+        unsigned long long n_over = 0;
+        if ((c = e->prune_cnt.reserve(e->stream, 4 * sizeof(unsigned long long))) != cudaSuccess ||
+            (c = cudaMemsetAsync(e->prune_cnt.p, 0, sizeof(unsigned long long), e->stream)) != cudaSuccess)
+            return cuda_fail(e, c, "candidate overflow count");
+        PW_LAUNCH(cand_overflow_kernel, gslot, 256, 0, e->stream, (const int32_t*)A.n_cand, n_pairs, kCandCap,
+                  e->prune_cnt.as<unsigned long long>());
+        e->launches++;
+        if ((c = cudaMemcpyAsync(&n_over, e->prune_cnt.p, sizeof(n_over), cudaMemcpyDeviceToHost, e->stream)) !=
+                cudaSuccess ||
+            (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
+            return cuda_fail(e, c, "candidate overflow count");
+        ht.mark("direction sweep");
         std::vector<int32_t> ncand;
-        if ((c = download(e, ncand, A.n_cand, (size_t)n_pairs)) != cudaSuccess) return cuda_fail(e, c, "copy");
+        std::vector<int64_t> cbase;
+        std::vector<int32_t> ccap;
         int64_t extra = 0;
-        std::vector<char> redo_item(wi.size(), 0);
-        for (int64_t p = 0; p < n_pairs; ++p)
-            if (ncand[p] > kCandCap) {
-                inf.cand_overflow_pairs++;
-                cbase[p] = cand_total + extra;
-                ccap[p] = ncand[p];
-                extra += ncand[p];
+        if (n_over > 0) {
+            if ((c = download(e, ncand, A.n_cand, (size_t)n_pairs)) != cudaSuccess) return cuda_fail(e, c, "copy");
+            cbase.resize(n_pairs);
+            ccap.assign(n_pairs, kCandCap);
+            for (int64_t p = 0; p < n_pairs; ++p) {
+                cbase[p] = p * kCandCap;
+                if (ncand[p] > kCandCap) {
+                    inf.cand_overflow_pairs++;
+                    cbase[p] = cand_total + extra;
+                    ccap[p] = ncand[p];
+                    extra += ncand[p];
+                }
             }
+        }
         if (extra > 0) {
             DevBuf& nb = e->cands_alt;
             if ((c = nb.reserve(e->stream, (cand_total + extra) * sizeof(Cand))) != cudaSuccess)
@@ -1913,6 +2000,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
 
         // starting points
         if ((c = upload(e, e->items, by_index)) != cudaSuccess) return cuda_fail(e, c, "upload items");
+        ht.mark("candidate overflow");
         TraceArgs TA;
         memset(&TA, 0, sizeof(TA));
         TA.metas = A.metas;
@@ -1971,6 +2059,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
                 return cuda_fail(e, c, "copy starts");
         }
         total_starts += wave_starts;
+        ht.mark("starting points");
         TA.allowed = nullptr;
         if (start_cap >= 0 && total_starts >= start_cap) {
             if (waves.size() > 1)
@@ -2030,6 +2119,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         }
         cudaEventRecord(e->ev[3], e->stream);
         cudaStreamSynchronize(e->stream);
+        ht.mark("walk");
         float t1 = 0, t2 = 0;
         cudaEventElapsedTime(&t1, e->ev[0], e->ev[2]);
         cudaEventElapsedTime(&t2, e->ev[2], e->ev[3]);
@@ -2042,6 +2132,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     const double t_finish = wall_ms();
     int64_t str_bytes = 0;
     if ((c = finish_hits(e, acc_n, &str_bytes)) != cudaSuccess) return cuda_fail(e, c, "order hits");
+    ht.mark("hit order + strings");
     inf.starting_points = total_starts;
     inf.hits = (int64_t)e->h_hits.size();
     inf.string_bytes = str_bytes;

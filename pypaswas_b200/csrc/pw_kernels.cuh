@@ -851,6 +851,44 @@ __global__ void int_peak16_kernel(int iters, int seed, int* sink) {
     if (r == 0x7fffffffu) sink[0] = (int)r;
 }
 
+// Passing pairs per query (target-major pair indices k = t * nq + sp from the
+// pruning selection; pairs of targets marked in skip are left out).
+__global__ void query_count_kernel(const int64_t* sel, int64_t n, int nq, const int32_t* q_order,
+                                   const uint8_t* skip, int32_t* count) {
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = sel[j];
+        const int t = (int)(k / nq);
+        if (!skip[t]) atomicAdd(&count[q_order[k - (int64_t)t * nq]], 1);
+    }
+}
+
+// Sum over queries of ceil(count / per_item) * per_item * len: the lane slots
+// of the transposed orientation's groups, in units of one shortest target.
+__global__ void group_bound_kernel(const int32_t* count, int nq, const int32_t* q_len, int per_item,
+                                   unsigned long long* sum) {
+    unsigned long long acc = 0;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x)
+        if (count[q] > 0)
+            acc += (unsigned long long)((count[q] + per_item - 1) / per_item) * per_item * (unsigned long long)q_len[q];
+    if (acc) atomicAdd(sum, acc);
+}
+
+// Candidate slots of a wave's pairs: pair p owns [p * cap, (p + 1) * cap).
+__global__ void cand_slot_kernel(int64_t* cand_base, int32_t* cand_cap, int64_t n_pairs, int cap) {
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n_pairs; p += (int64_t)gridDim.x * blockDim.x) {
+        cand_base[p] = p * cap;
+        cand_cap[p] = cap;
+    }
+}
+
+// Pairs whose candidate count exceeds their slot (*count += such pairs).
+__global__ void cand_overflow_kernel(const int32_t* n_cand, int64_t n_pairs, int cap, unsigned long long* count) {
+    unsigned long long k = 0;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n_pairs; p += (int64_t)gridDim.x * blockDim.x)
+        k += n_cand[p] > cap ? 1 : 0;
+    if (k) atomicAdd(count, k);
+}
+
 // Pruning of the traced pairs on the device (the host then reads only the
 // pairs that pass).  Pair k = t * nq + sp (target-major, sp the query's sorted
 // position) passes when its maximum reaches MINIMUM_SCORE and
