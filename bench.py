@@ -328,7 +328,8 @@ def main():
 
     chain = not args.no_chain
     from pypaswas_b200 import _native
-    knobs = {"chain_min": _native.PW_TUNE_CHAIN_MIN, "grid_share": _native.PW_TUNE_GRID_SHARE}
+    knobs = {"chain_min": _native.PW_TUNE_CHAIN_MIN, "grid_share": _native.PW_TUNE_GRID_SHARE,
+             "segment": _native.PW_TUNE_SEGMENT, "dual": _native.PW_TUNE_DUAL, "cand_slot": _native.PW_TUNE_CAND_SLOT}
     tuning = {}
     for kv in args.tune:
         key, val = kv.split("=")
@@ -373,7 +374,10 @@ def main():
     trace_ms = sum(i["trace_kernel_ms"] for i in infos)
     score_ms = sum(i["score_kernel_ms"] for i in infos)
     if trace_ms >= score_ms:
-        dom, dom_ms, dom_launch = "direction sweep (sweep_kernel phase 2)", trace_ms, sum(
+        wp, tp = last["warp_pairs"], last["traced_pairs"]
+        which = "band_kernel, one pair per warp" if wp >= tp else (
+            "sweep_kernel phase 2" if wp == 0 else "sweep_kernel phase 2 + band_kernel")
+        dom, dom_ms, dom_launch = "direction sweep (%s)" % which, trace_ms, sum(
             i["trace_launches"] for i in infos)
         ops = sum(i["traced_cells"] for i in infos) * OPS_PER_CELL[(mode, "dirs")]
     else:
@@ -406,6 +410,7 @@ def main():
            "config": {"workload": "%s (%d pairs, full path)" % (w.name, n_pairs),
                       "pairs": n_pairs,
                       "cells_per_step": cells, "traced_pairs": last["traced_pairs"],
+                      "cand_overflow_pairs": last["cand_overflow_pairs"],
                       "starting_points": last["starting_points"], "hits": last["hits"],
                       "score_lanes": "targets" if last["orientation"] else "queries",
                       "trace_lanes": "targets" if last["trace_orientation"] else "queries",

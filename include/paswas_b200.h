@@ -188,6 +188,10 @@ int pw_set_wave_limit(pw_engine* e, int64_t bytes);
  *                       two by the cell-slot cost model (dual lanes win when
  *                       few sequences sit on the strip side, e.g. one query) */
 #define PW_TUNE_DUAL 3
+/*   PW_TUNE_CAND_SLOT   starting-point candidates held per traced pair before
+ *                       its sweep is repeated with an exact slot (default
+ *                       64); a small value exercises the repeat path */
+#define PW_TUNE_CAND_SLOT 4
 int pw_set_tuning(pw_engine* e, int key, int64_t value);
 
 /* Pair maxima (the last block of the maxima chain, default_main.cu:591),

@@ -33,6 +33,7 @@ PW_TUNE_CHAIN_MIN = 0
 PW_TUNE_GRID_SHARE = 1
 PW_TUNE_SEGMENT = 2
 PW_TUNE_DUAL = 3
+PW_TUNE_CAND_SLOT = 4
 
 # symbols the header declares, checked by the CPU test-suite
 EXPORTED_SYMBOLS = (

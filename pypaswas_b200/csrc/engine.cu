@@ -1050,6 +1050,9 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uin
         P1.share = e->tune[PW_TUNE_GRID_SHARE];
         P1.valid = true;
         inf.setup_ms += wall_ms() - t_plan;
+        HostTrace ht;
+        ht.t = t_plan;
+        ht.mark("phase-1 plan (rebuilt)");
     }
     const bool trans = P1.trans;
     const bool chained = P1.chained;
@@ -1882,16 +1885,20 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         if ((c = e->metas.reserve(e->stream, n_pairs * sizeof(PairMeta))) != cudaSuccess) return cuda_fail(e, c, "alloc metas");
         if ((c = e->n_cand.reserve(e->stream, n_pairs * sizeof(int32_t))) != cudaSuccess) return cuda_fail(e, c, "alloc");
         if ((c = e->n_starts.reserve(e->stream, n_pairs * sizeof(int32_t))) != cudaSuccess) return cuda_fail(e, c, "alloc");
-        // every pair starts with a slot of kCandCap candidates (filled on the device)
-        int64_t cand_total = n_pairs * kCandCap;
-        if ((c = e->cands.reserve(e->stream, cand_total * sizeof(Cand))) != cudaSuccess) return cuda_fail(e, c, "alloc cands");
+        // every pair starts with a slot of kCandCap candidates, filled on the
+        // device (PW_TUNE_CAND_SLOT: another capacity); pairs that outgrow it
+        // are swept again with an exact slot
+        const int64_t slot_tune = e->tune[PW_TUNE_CAND_SLOT];
+        const int cap0 = slot_tune > 0 ? (int)std::min<int64_t>(slot_tune, (int64_t)1 << 20) : kCandCap;
+        int64_t cand_total = n_pairs * cap0;
         if ((c = e->cand_base.reserve(e->stream, (size_t)std::max<int64_t>(n_pairs, 2) * sizeof(int64_t))) != cudaSuccess ||
             (c = e->cand_cap.reserve(e->stream, (size_t)std::max<int64_t>(n_pairs, 4) * sizeof(int32_t))) != cudaSuccess)
             return cuda_fail(e, c, "alloc candidate slots");
         const int gslot = (int)std::max<int64_t>(1, std::min<int64_t>((n_pairs + 255) / 256, (int64_t)e->sm_count * 16));
         PW_LAUNCH(cand_slot_kernel, gslot, 256, 0, e->stream, e->cand_base.as<int64_t>(), e->cand_cap.as<int32_t>(),
-                  n_pairs, kCandCap);
+                  n_pairs, cap0);
         e->launches++;
+        if ((c = e->cands.reserve(e->stream, cand_total * sizeof(Cand))) != cudaSuccess) return cuda_fail(e, c, "alloc cands");
         if ((c = upload(e, e->items, wi)) != cudaSuccess) return cuda_fail(e, c, "upload items");
         ht.mark("wave buffers");
         A.codes = e->codes.as<uint8_t>();
@@ -1927,8 +1934,8 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         if ((c = e->prune_cnt.reserve(e->stream, 4 * sizeof(unsigned long long))) != cudaSuccess ||
             (c = cudaMemsetAsync(e->prune_cnt.p, 0, sizeof(unsigned long long), e->stream)) != cudaSuccess)
             return cuda_fail(e, c, "candidate overflow count");
-        PW_LAUNCH(cand_overflow_kernel, gslot, 256, 0, e->stream, (const int32_t*)A.n_cand, n_pairs, kCandCap,
-                  e->prune_cnt.as<unsigned long long>());
+        PW_LAUNCH(cand_overflow_kernel, gslot, 256, 0, e->stream, (const int32_t*)A.n_cand, (const int32_t*)A.cand_cap,
+                  n_pairs, e->prune_cnt.as<unsigned long long>());
         e->launches++;
         if ((c = cudaMemcpyAsync(&n_over, e->prune_cnt.p, sizeof(n_over), cudaMemcpyDeviceToHost, e->stream)) !=
                 cudaSuccess ||
@@ -1938,14 +1945,17 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         std::vector<int32_t> ncand;
         std::vector<int64_t> cbase;
         std::vector<int32_t> ccap;
+        std::vector<char> over;  // pairs that outgrew their slot
         int64_t extra = 0;
         if (n_over > 0) {
-            if ((c = download(e, ncand, A.n_cand, (size_t)n_pairs)) != cudaSuccess) return cuda_fail(e, c, "copy");
-            cbase.resize(n_pairs);
-            ccap.assign(n_pairs, kCandCap);
+            over.assign((size_t)n_pairs, 0);
+            if ((c = download(e, ncand, A.n_cand, (size_t)n_pairs)) != cudaSuccess ||
+                (c = download(e, cbase, A.cand_base, (size_t)n_pairs)) != cudaSuccess ||
+                (c = download(e, ccap, A.cand_cap, (size_t)n_pairs)) != cudaSuccess)
+                return cuda_fail(e, c, "copy");
             for (int64_t p = 0; p < n_pairs; ++p) {
-                cbase[p] = p * kCandCap;
-                if (ncand[p] > kCandCap) {
+                if (ncand[p] > ccap[p]) {
+                    over[p] = 1;
                     inf.cand_overflow_pairs++;
                     cbase[p] = cand_total + extra;
                     ccap[p] = ncand[p];
@@ -1971,14 +1981,14 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
             for (size_t k = 0; k < wi.size(); ++k) {
                 bool ov = false;
                 for (int l = 0; l < wi[k].lanes; ++l)
-                    if (ncand[wi[k].pair_base + l] > kCandCap) ov = true;
+                    if (over[wi[k].pair_base + l]) ov = true;
                 if (ov) {
                     ri.push_back(wi[k]);
                     rcl.push_back(wc[k]);
                 }
             }
             for (const WorkItem& w : ww)
-                if (ncand[w.pair_base] > kCandCap) rw.push_back(w);
+                if (over[w.pair_base]) rw.push_back(w);
             // the warp sweep counts with atomics from zero; the strip sweep
             // overwrites its counts, and the other pairs' counts are no longer read
             if ((c = cudaMemsetAsync(A.n_cand, 0, n_pairs * sizeof(int32_t), e->stream)) != cudaSuccess)

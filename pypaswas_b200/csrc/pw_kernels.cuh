@@ -882,10 +882,11 @@ __global__ void cand_slot_kernel(int64_t* cand_base, int32_t* cand_cap, int64_t 
 }
 
 // Pairs whose candidate count exceeds their slot (*count += such pairs).
-__global__ void cand_overflow_kernel(const int32_t* n_cand, int64_t n_pairs, int cap, unsigned long long* count) {
+__global__ void cand_overflow_kernel(const int32_t* n_cand, const int32_t* cand_cap, int64_t n_pairs,
+                                     unsigned long long* count) {
     unsigned long long k = 0;
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n_pairs; p += (int64_t)gridDim.x * blockDim.x)
-        k += n_cand[p] > cap ? 1 : 0;
+        k += n_cand[p] > cand_cap[p] ? 1 : 0;
     if (k) atomicAdd(count, k);
 }
 

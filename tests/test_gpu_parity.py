@@ -126,7 +126,7 @@ def test_long_targets_one_warp_per_pair(engine_lib, oracle_mod, kind):
     # targets longer than 64 are swept one pair per warp in 256-row bands:
     # lengths around the band edges, planted segments long enough that some
     # pairs find more candidates than their first slot holds
-    from pypaswas_b200 import scores
+    from pypaswas_b200 import _native, scores
     rng = np.random.default_rng(31 if kind == "dna" else 32)
     alphabet = cases.DNA if kind == "dna" else cases.PROTEIN
     draw = lambda n: "".join(alphabet[i] for i in rng.integers(0, len(alphabet), n))
@@ -146,6 +146,12 @@ def test_long_targets_one_warp_per_pair(engine_lib, oracle_mod, kind):
         score = scores.make_score(st)
         o = _oracle(oracle_mod, queries, targets, score, st)
         pm, hits, info, _ = run_engine(engine_lib, queries, targets, score, st)
+        assert info.warp_pairs > 0
+        np.testing.assert_array_equal(pm, o["pair_max"])
+        assert hits == o["hits"]
+        # slots of 4 candidates: pairs outgrow them and are swept again
+        pm, hits, info, _ = run_engine(engine_lib, queries, targets, score, st,
+                                       tuning={_native.PW_TUNE_CAND_SLOT: 4})
         assert info.warp_pairs > 0 and info.cand_overflow_pairs > 0
         np.testing.assert_array_equal(pm, o["pair_max"])
         assert hits == o["hits"]
@@ -170,6 +176,12 @@ def test_many_short_targets_strip_direction_sweep(engine_lib, oracle_mod, aff):
     o = _oracle(oracle_mod, queries, targets, score, st)
     pm, hits, info, _ = run_engine(engine_lib, queries, targets, score, st)
     assert info.traced_pairs >= 148 * 32 and info.warp_pairs == 0
+    np.testing.assert_array_equal(pm, o["pair_max"])
+    assert hits == o["hits"]
+    # slots of 2 candidates: the strip items of pairs that outgrow them are swept again
+    from pypaswas_b200 import _native
+    pm, hits, info, _ = run_engine(engine_lib, queries, targets, score, st, tuning={_native.PW_TUNE_CAND_SLOT: 2})
+    assert info.cand_overflow_pairs > 0
     np.testing.assert_array_equal(pm, o["pair_max"])
     assert hits == o["hits"]
 
