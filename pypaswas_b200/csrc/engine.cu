@@ -429,10 +429,21 @@ extern "C" int pw_set_targets(pw_engine* e, const uint8_t* residues, const int64
 namespace {
 
 // Strip classes: one-strip sweeps of 16, 32, 48 (linear) and 64 (linear)
-// rows, and multi-strip items of 32-row strips.
-enum SClass { kS16 = 0, kS32 = 1, kS64 = 2, kS32Multi = 3, kS48 = 4, kNumClasses = 5 };
+// rows, and multi-strip items of 32-row strips; the 16-bit score sweep also
+// has one-strip classes of 24 and 40 (linear) rows (its strips need a
+// multiple of 4 rows, the cell-code layout of the other sweeps 16).
+enum SClass { kS16 = 0, kS32 = 1, kS64 = 2, kS32Multi = 3, kS48 = 4, kS24 = 5, kS40 = 6, kNumClasses = 7 };
 
-int class_S(int c) { return c == kS16 ? 16 : (c == kS64 ? 64 : (c == kS48 ? 48 : 32)); }
+int class_S(int c) {
+    switch (c) {
+        case kS16: return 16;
+        case kS24: return 24;
+        case kS40: return 40;
+        case kS48: return 48;
+        case kS64: return 64;
+        default: return 32;
+    }
+}
 
 int pick_class(int lt, bool affine) {
     if (lt <= 16) return kS16;
@@ -440,6 +451,13 @@ int pick_class(int lt, bool affine) {
     if (!affine && lt <= 48) return kS48;
     if (!affine && lt <= 64) return kS64;
     return kS32Multi;
+}
+
+// The 16-bit score sweep's class of a strip pair whose longer strip has lt rows.
+int pick_class16(int lt, bool affine) {
+    if (lt > 16 && lt <= 24) return kS24;
+    if (!affine && lt > 32 && lt <= 40) return kS40;
+    return pick_class(lt, affine);
 }
 
 int64_t align_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
@@ -835,11 +853,14 @@ template <bool DL>
 static cudaError_t launch_s16_class(pw_engine* e, int cls, bool affine, const Score16Args& A) {
     if (affine) {
         if (cls == kS16) return launch_s16<16, true, false, DL>(e, A);
+        if (cls == kS24) return launch_s16<24, true, false, DL>(e, A);
         if (cls == kS32) return launch_s16<32, true, false, DL>(e, A);
         return launch_s16<32, true, true, DL>(e, A);
     }
     if (cls == kS16) return launch_s16<16, false, false, DL>(e, A);
+    if (cls == kS24) return launch_s16<24, false, false, DL>(e, A);
     if (cls == kS32) return launch_s16<32, false, false, DL>(e, A);
+    if (cls == kS40) return launch_s16<40, false, false, DL>(e, A);
     if (cls == kS48) return launch_s16<48, false, false, DL>(e, A);
     if (cls == kS64) return launch_s16<64, false, false, DL>(e, A);
     return launch_s16<32, false, true, DL>(e, A);
@@ -1000,7 +1021,7 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uin
                 w.lanes = std::min(kWarp, n_lane - g);
                 w.lanes_hi = dual ? std::max(0, std::min(kWarp, n_lane - g - kWarp)) : 0;
                 w.xmax = lane_len[lane_order[g]];
-                const int k = pick_class(ls, e->affine);
+                const int k = pick_class16(ls, e->affine);
                 w.S = class_S(k);
                 items.push_back(w);
                 cls.push_back(k);
