@@ -157,8 +157,9 @@ int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_info* info)
 int pw_set_pairs(pw_engine* e, const int32_t* query_idx, const int32_t* target_idx, int64_t n);
 
 /* Upper bound, in bytes, on the direction-matrix (cell code) memory of one
- * memory wave of pw_align; 0 restores the automatic choice (half of the free
- * device memory, at most 48 GiB).  Traced pairs beyond the bound run in
+ * memory wave of pw_align; 0 restores the automatic choice (55% of the free
+ * device memory with the candidate slots counted, at most 100 GiB).  Traced
+ * pairs beyond the bound run in
  * further waves; a single pair larger than the bound runs alone.  Replaces
  * the batch sizing of SmithWaterman._get_max_number_sequences
  * (SmithWaterman.py:202-221) with its memory fraction `maximum_memory_usage`

@@ -1844,24 +1844,31 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     }
     const KernelArgs Aref = base_args(e);  // reference-oriented sets for the trace kernels
 
-    // memory waves: the cell codes of one wave must fit the budget
+    // memory waves: the cell codes of one wave must fit the budget (set by
+    // pw_set_wave_limit); the automatic budget, 55% of the free memory plus
+    // the buffers kept from the previous call, also counts each pair's
+    // candidate slot and bookkeeping
     int64_t budget = e->wave_limit;
-    if (budget <= 0) {
+    const bool auto_budget = budget <= 0;
+    if (auto_budget) {
         size_t free_b = 0, total_b = 0;
         cudaMemGetInfo(&free_b, &total_b);
-        budget = std::min<int64_t>((int64_t)(free_b * 0.5) + (int64_t)e->codes.bytes, (int64_t)48 << 30);
+        const int64_t kept = (int64_t)(e->codes.bytes + e->cands.bytes + e->metas.bytes);
+        budget = std::min<int64_t>((int64_t)(free_b * 0.55) + kept, (int64_t)100 << 30);
     }
+    const int64_t pair_bytes = auto_budget ? (int64_t)(kCandCap * sizeof(Cand) + sizeof(PairMeta)) + 64 : 0;
     std::vector<std::pair<size_t, size_t>> waves;
     {
         size_t i0 = 0;
         int64_t acc = 0;
         for (size_t i = 0; i < items2.size(); ++i) {
-            if (acc > 0 && (acc + bytes2[i] > budget || plain)) {
+            const int64_t b = bytes2[i] + items2[i].lanes * pair_bytes;
+            if (acc > 0 && (acc + b > budget || plain)) {
                 waves.push_back({i0, i});
                 i0 = i;
                 acc = 0;
             }
-            acc += bytes2[i];
+            acc += b;
         }
         waves.push_back({i0, items2.size()});
     }

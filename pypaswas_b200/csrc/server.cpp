@@ -157,6 +157,29 @@ void run_batch(pw_server* s, int w, pw_engine* e, std::vector<Request*>& batch, 
         rc = pw_get_hits(e, hits.data(), info.hits, strings.data(), info.string_bytes);
     }
     const std::string msg = rc == PW_OK ? std::string() : std::string(pw_last_error(e));
+    // top hits of the score-only requests: one host thread per request
+    if (rc == PW_OK && mode == PW_SERVE_TOP) {
+        auto top = [&](int i) {
+            Request* r = batch[i];
+            const float* row = pmax.data() + (size_t)i * s->db_n;
+            std::vector<int32_t> idx(s->db_n);
+            for (int32_t t = 0; t < s->db_n; ++t) idx[t] = t;
+            const int k = std::min<int>(r->top_k, s->db_n);
+            auto better = [&](int32_t a, int32_t b) { return row[a] > row[b] || (row[a] == row[b] && a < b); };
+            std::partial_sort(idx.begin(), idx.begin() + k, idx.end(), better);
+            r->top_targets.assign(idx.begin(), idx.begin() + k);
+            r->top_scores.resize(k);
+            for (int j = 0; j < k; ++j) r->top_scores[j] = row[idx[j]];
+        };
+        if (n == 1) {
+            top(0);
+        } else {
+            std::vector<std::thread> th;
+            th.reserve(n);
+            for (int i = 0; i < n; ++i) th.emplace_back(top, i);
+            for (auto& t : th) t.join();
+        }
+    }
     // per-request results
     for (int i = 0; i < n; ++i) {
         Request* r = batch[i];
@@ -171,15 +194,7 @@ void run_batch(pw_server* s, int w, pw_engine* e, std::vector<Request*>& batch, 
         r->call_ms = info.total_ms;
         if (rc != PW_OK) continue;
         if (mode == PW_SERVE_TOP) {
-            const float* row = pmax.data() + (size_t)i * s->db_n;
-            std::vector<int32_t> idx(s->db_n);
-            for (int32_t t = 0; t < s->db_n; ++t) idx[t] = t;
-            const int k = std::min<int>(r->top_k, s->db_n);
-            auto better = [&](int32_t a, int32_t b) { return row[a] > row[b] || (row[a] == row[b] && a < b); };
-            std::partial_sort(idx.begin(), idx.begin() + k, idx.end(), better);
-            r->top_targets.assign(idx.begin(), idx.begin() + k);
-            r->top_scores.resize(k);
-            for (int j = 0; j < k; ++j) r->top_scores[j] = row[idx[j]];
+            // filled above
         } else {
             for (const pw_hit& h : hits) {
                 if (h.query != i) continue;
