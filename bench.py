@@ -63,7 +63,7 @@ def parse():
                     help="engine tuning knob (chain_min, grid_share), e.g. --tune chain_min=250; "
                          "without chain_min the autotuner picks it during the warm-up")
     ap.add_argument("--serve-seconds", type=float, default=6.0, help="length of each arrival stream of the serving leg")
-    ap.add_argument("--serve-loads", default="0.3,0.5,0.7", help="offered loads (fractions of batched peak) swept")
+    ap.add_argument("--serve-loads", default="0.3,0.5,0.6,0.7", help="offered loads (fractions of batched peak) swept")
     return ap.parse_args()
 
 

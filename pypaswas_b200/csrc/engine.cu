@@ -255,6 +255,8 @@ struct pw_engine {
     DevBuf acc_hits, acc_ops, fk_a, fk_b, fk_c, fk_t, fk_g, fi_a, fi_b, f_len, f_soff, f_out, f_str;
     HostBuf<int64_t> h_sel;
     HostBuf<int32_t> h_ptq, h_p2order;  // phase-2 pair lists (kept across calls: no page faults, no zero fill)
+    int64_t free_mem = 0;    // free device memory plus this engine's kept wave buffers, as last queried
+    double free_mem_t = -1;  // wall_ms() of that query
     DevBuf chain_items, chain_info, chain_prog, chain_max, chain_ring_off, chain_ring, chain_abort, p1_items;
     // plan of the 16-bit score phase (work items, classes, chain queue), kept
     // on the device and reused while inputs, scoring, flags and tuning stay
@@ -1851,10 +1853,19 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     int64_t budget = e->wave_limit;
     const bool auto_budget = budget <= 0;
     if (auto_budget) {
-        size_t free_b = 0, total_b = 0;
-        cudaMemGetInfo(&free_b, &total_b);
+        // the free-memory query goes to the driver, which tools polling the
+        // GPU (nvidia-smi) can hold for tens of milliseconds: it is refreshed
+        // at most once a second
+        const double now = wall_ms();
+        if (e->free_mem_t < 0 || now - e->free_mem_t > 1000.0) {
+            size_t free_b = 0, total_b = 0;
+            cudaMemGetInfo(&free_b, &total_b);
+            e->free_mem = (int64_t)free_b + (int64_t)(e->codes.bytes + e->cands.bytes + e->metas.bytes);
+            e->free_mem_t = now;
+        }
         const int64_t kept = (int64_t)(e->codes.bytes + e->cands.bytes + e->metas.bytes);
-        budget = std::min<int64_t>((int64_t)(free_b * 0.55) + kept, (int64_t)100 << 30);
+        budget = std::min<int64_t>((int64_t)(std::max<int64_t>(e->free_mem - kept, 0) * 0.55) + kept,
+                                   (int64_t)100 << 30);
     }
     const int64_t pair_bytes = auto_budget ? (int64_t)(kCandCap * sizeof(Cand) + sizeof(PairMeta)) + 64 : 0;
     std::vector<std::pair<size_t, size_t>> waves;
