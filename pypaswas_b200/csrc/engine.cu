@@ -1286,7 +1286,13 @@ static cudaError_t finish_hits(pw_engine* e, int64_t n, int64_t* str_bytes) {
     PW_LAUNCH(hit_out_kernel, grid, 256, 0, e->stream, h, ib, soff, n, e->acc_ops.as<char>(), e->q_raw.as<uint8_t>(),
               e->q_raw_off.as<int64_t>(), e->t_raw.as<uint8_t>(), e->t_raw_off.as<int64_t>(), e->f_out.as<pw_hit>(),
               e->f_str.as<char>());
-    e->launches += 9;
+    {
+        const int wgrid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 127) / 128, (int64_t)e->sm_count * 16));
+        PW_LAUNCH(hit_strings_warp_kernel, wgrid, 128, 0, e->stream, h, ib, soff, n, e->acc_ops.as<char>(),
+                  e->q_raw.as<uint8_t>(), e->q_raw_off.as<int64_t>(), e->t_raw.as<uint8_t>(),
+                  e->t_raw_off.as<int64_t>(), e->f_str.as<char>());
+    }
+    e->launches += 10;
     if ((c = cudaGetLastError()) != cudaSuccess) return c;
     if (!e->h_hits.resize((size_t)n) || !e->h_strings.resize((size_t)total)) return cudaErrorMemoryAllocation;
     if ((c = cudaMemcpyAsync(e->h_hits.data(), e->f_out.p, (size_t)n * sizeof(pw_hit), cudaMemcpyDeviceToHost,

@@ -49,6 +49,10 @@ __global__ void hit_len_kernel(const DevHit* h, const int32_t* idx, int64_t n, i
 // case -- '.' for a mismatch, ' ' in a gap) and target_match, one column per
 // operation, as SmithWaterman._print_alignments spells them
 // (SmithWaterman.py:765-815).
+// Hits longer than kWarpStringCols columns get only their record here; a
+// warp spells their strings (hit_strings_warp_kernel).
+constexpr int kWarpStringCols = 512;
+
 __global__ void hit_out_kernel(const DevHit* h, const int32_t* idx, const int64_t* soff, int64_t n, const char* ops,
                                const uint8_t* q_raw, const int64_t* q_off, const uint8_t* t_raw,
                                const int64_t* t_off, pw_hit* out, char* str) {
@@ -67,6 +71,7 @@ __global__ void hit_out_kernel(const DevHit* h, const int32_t* idx, const int64_
         o.n_cols = d.n_cols;
         o.str_offset = soff[k];
         out[k] = o;
+        if (d.n_cols > kWarpStringCols) continue;
         char* sq = str + o.str_offset;
         char* al = sq + d.n_cols;
         char* tg = al + d.n_cols;
@@ -95,6 +100,68 @@ __global__ void hit_out_kernel(const DevHit* h, const int32_t* idx, const int64_
                 tg[i] = (char)ts[y];
                 al[i] = ' ';
                 ++y;
+            }
+        }
+    }
+}
+
+// The strings of the long hits, one warp per hit and 32 columns per step:
+// the query / target position of every column is the starting position plus
+// an exclusive warp scan of the columns that consume a query residue ('M',
+// 'I') or a target residue ('M', 'D'); the characters are those of
+// hit_out_kernel.
+__global__ void hit_strings_warp_kernel(const DevHit* h, const int32_t* idx, const int64_t* soff, int64_t n,
+                                        const char* ops, const uint8_t* q_raw, const int64_t* q_off,
+                                        const uint8_t* t_raw, const int64_t* t_off, char* str) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t k = warp; k < n; k += warps) {
+        {
+            const DevHit d = h[idx[k]];
+            if (d.n_cols <= kWarpStringCols) continue;
+            char* sq = str + soff[k];
+            char* al = sq + d.n_cols;
+            char* tg = al + d.n_cols;
+            const uint8_t* qs = q_raw + q_off[d.query];
+            const uint8_t* ts = t_raw + t_off[d.target];
+            const char* op = ops + d.ops_offset;
+            int x = d.s_start, y = d.t_start;
+            for (int c0 = 0; c0 < d.n_cols; c0 += 32) {
+                const int i = c0 + lane;
+                const bool act = i < d.n_cols;
+                const char c = act ? op[i] : 'M';
+                const int dx = act && c != 'D' ? 1 : 0, dy = act && c != 'I' ? 1 : 0;
+                int sx = dx, sy = dy;
+#pragma unroll
+                for (int off = 1; off < 32; off <<= 1) {
+                    const int tx = __shfl_up_sync(0xffffffffu, sx, off), ty = __shfl_up_sync(0xffffffffu, sy, off);
+                    if (lane >= off) {
+                        sx += tx;
+                        sy += ty;
+                    }
+                }
+                if (act) {
+                    const int px = x + sx - dx, py = y + sy - dy;
+                    if (c == 'M') {
+                        const uint8_t ca = ts[py], cb = qs[px];
+                        const bool la = (ca >= 'A' && ca <= 'Z') || (ca >= 'a' && ca <= 'z');
+                        const bool eq = la ? ((ca | 0x20) == (cb | 0x20)) : ca == cb;
+                        sq[i] = (char)cb;
+                        tg[i] = (char)ca;
+                        al[i] = eq ? '|' : '.';
+                    } else if (c == 'I') {
+                        sq[i] = (char)qs[px];
+                        tg[i] = '-';
+                        al[i] = ' ';
+                    } else {
+                        sq[i] = '-';
+                        tg[i] = (char)ts[py];
+                        al[i] = ' ';
+                    }
+                }
+                x += __shfl_sync(0xffffffffu, sx, 31);
+                y += __shfl_sync(0xffffffffu, sy, 31);
             }
         }
     }
