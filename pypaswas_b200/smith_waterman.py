@@ -171,16 +171,57 @@ class SmithWatermanB200(object):
         qc_, tc_, s0_, s1_, t0_, t1_, sc_, mt_, mm_, rel_, id_, cov_, base_ = cols
         logger = self.logger
         new = Hit.__new__
+        if type(hit_list) is not HitList:
+            for k in keep:
+                n, o = nc[k], so[k]
+                h = new(Hit)
+                h.__dict__ = dict(
+                    logger=logger, sequence_info=sequences[qc_[k]], target_info=targets[tc_[k]],
+                    seq_location=(s0_[k], s1_[k]), target_location=(t0_[k], t1_[k]),
+                    sequence_match=text[o:o + n], alignment=text[o + n:o + 2 * n],
+                    target_match=text[o + 2 * n:o + 3 * n], score=sc_[k], matches=mt_[k], mismatches=mm_[k],
+                    query_identity=id_[k], query_coverage=cov_[k], relative_score=rel_[k], base_score=base_[k],
+                    distance=None, rc=False)
+                hit_list.append(h)
+            return
+        # HitList.append inlined (same keys, same replacement rule, same log
+        # records): the ids come from the record lists, the keys from the arrays
+        hits_d, real = hit_list.hits, hit_list.real_hits
+        hl_log = hit_list.logger
+        enabled = getattr(hl_log, "isEnabledFor", lambda level: True)
+        log_info = hl_log is not None and enabled(logging.INFO)
+        log_debug = hl_log is not None and enabled(logging.DEBUG)
+        qid = [r.id for r in sequences]
+        tid = [r.id for r in targets]
         for k in keep:
             n, o = nc[k], so[k]
+            qi, ti = qc_[k], tc_[k]
+            sid, gid = qid[qi], tid[ti]
+            sc = sc_[k]
             h = new(Hit)
-            h.__dict__.update(
-                logger=logger, sequence_info=sequences[qc_[k]], target_info=targets[tc_[k]],
-                seq_location=(s0_[k], s1_[k]), target_location=(t0_[k], t1_[k]),
-                sequence_match=text[o:o + n], alignment=text[o + n:o + 2 * n], target_match=text[o + 2 * n:o + 3 * n],
-                score=sc_[k], matches=mt_[k], mismatches=mm_[k], query_identity=id_[k], query_coverage=cov_[k],
-                relative_score=rel_[k], base_score=base_[k], distance=None, rc=False)
-            hit_list.append(h)
+            h.__dict__ = {
+                "logger": logger, "sequence_info": sequences[qi], "target_info": targets[ti],
+                "seq_location": (s0_[k], s1_[k]), "target_location": (t0_[k], t1_[k]),
+                "sequence_match": text[o:o + n], "alignment": text[o + n:o + 2 * n],
+                "target_match": text[o + 2 * n:o + 3 * n], "score": sc, "matches": mt_[k], "mismatches": mm_[k],
+                "query_identity": id_[k], "query_coverage": cov_[k], "relative_score": rel_[k],
+                "base_score": base_[k], "distance": None, "rc": False}
+            k0 = (sid, gid, s0_[k], t0_[k])
+            k1 = (sid, gid, s1_[k], t1_[k])
+            old0, old1 = hits_d.get(k0), hits_d.get(k1)
+            better_end = old1 is not None and old1.score < sc
+            if (old0 is None and old1 is None) or better_end or (old0 is not None and old0.score < sc):
+                if better_end:
+                    ok = old1.keys()[2]
+                    if ok in real:
+                        del real[ok]
+                hits_d[k0] = h
+                hits_d[k1] = h
+                real[k0] = h
+                if log_info:
+                    hl_log.info("Added hit (query ID: %s, target ID: %s) to hitlist", sid, gid)
+            elif log_debug:
+                hl_log.debug("Rejected hit (query ID: %s, target ID: %s) from addition to hitlist", sid, gid)
 
     def _build_hits_checked(self, hits, text, sequences, targets, hit_list, s0, s1, t0, t1):
         q_col, t_col = hits["query"].tolist(), hits["target"].tolist()

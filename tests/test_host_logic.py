@@ -124,3 +124,66 @@ def test_autotune_keeps_the_fastest_candidate():
     assert r["chain_min"] == 500  # ties go to the smaller value
     assert e.tune[_native.PW_TUNE_CHAIN_MIN] == 500
     assert r["score_kernel_ms"] == FakeEngine.cost
+
+
+def test_fast_hit_building_matches_hitlist_append_and_checked_path():
+    """SmithWaterman hit building: the vectorised path with HitList.append
+    inlined gives the same HitList (keys, replacement rule, Hit fields) as
+    appending through HitList.append, and as the validating constructor path."""
+    import logging
+    import numpy as np
+    from pypaswas_b200 import _native
+    from pypaswas_b200.hits import HitList
+    from pypaswas_b200.records import SeqRecord
+    from pypaswas_b200.smith_waterman import SmithWatermanB200
+    import cases
+
+    class PlainList(HitList):  # a subclass takes the generic append path
+        pass
+
+    rng = np.random.default_rng(7)
+    seqs = [SeqRecord("".join("ACGT"[i] for i in rng.integers(0, 4, 60)), "q%d" % i) for i in range(5)]
+    tgts = [SeqRecord("".join("ACGT"[i] for i in rng.integers(0, 4, 50)), "t%d" % i) for i in range(4)]
+    rows = []
+    for _ in range(300):
+        q, t = int(rng.integers(0, 5)), int(rng.integers(0, 4))
+        s0, t0 = int(rng.integers(0, 20)), int(rng.integers(0, 20))
+        n = int(rng.integers(2, 25))
+        s1, t1 = min(s0 + n, 59), min(t0 + n, 49)
+        rows.append((q, t, s0, s1, t0, t1, float(rng.integers(5, 40)), n))
+    rows += rows[:40]  # repeated keys: equal scores are rejected, higher ones replace
+    hits = np.zeros(len(rows), dtype=_native.HIT_DTYPE)
+    text, off = [], 0
+    for k, (q, t, s0, s1, t0, t1, sc, n) in enumerate(rows):
+        hits[k] = 0
+        for name, v in (("query", q), ("target", t), ("s_start", s0), ("s_end", s1), ("t_start", t0),
+                        ("t_end", t1), ("score", sc), ("matches", n // 2), ("mismatches", n - n // 2),
+                        ("n_cols", n), ("str_offset", off)):
+            hits[k][name] = v
+        text.append("A" * n + "|" * n + "C" * n)
+        off += 3 * n
+    strbuf = "".join(text).encode("latin-1")
+    st = cases.Settings(relative_score="0.1", query_identity="0.2", query_coverage="0", base_score="0")
+    sw = SmithWatermanB200.__new__(SmithWatermanB200)
+    sw.logger = logging.getLogger("test")
+    sw.settings = st
+
+    def run(hl):
+        sw._build_hits(hits, strbuf, seqs, tgts, hl)
+        return hl
+
+    def view(hl):
+        out = {}
+        for name in ("hits", "real_hits"):
+            d = getattr(hl, name)
+            out[name] = {k: tuple(sorted((a, v) for a, v in h.__dict__.items() if a != "logger")) for k, h in d.items()}
+        return out
+
+    fast, generic = run(HitList(sw.logger)), run(PlainList(sw.logger))
+    assert len(fast.hits) > 50
+    assert view(fast) == view(generic)
+    checked = HitList(sw.logger)
+    s0 = hits["s_start"].astype(np.int64)
+    sw._build_hits_checked(hits, strbuf.decode("latin-1"), seqs, tgts, checked, s0, hits["s_end"].astype(np.int64),
+                           hits["t_start"].astype(np.int64), hits["t_end"].astype(np.int64))
+    assert view(fast) == view(checked)
