@@ -287,9 +287,10 @@ def run_reference(args, workload_fn):
     score = scores.make_score(w.settings)
     procs = os.cpu_count() or 1
     steps = []
+    # each step a bounded sample: the whole run stays near two minutes
+    per_step = max(1.0, min(args.cpu_seconds, 20.0, 120.0 / max(1, args.warmup + args.steps)))
     for i in range(args.warmup + args.steps):
-        r = cpu_baseline(w if w.queries is not None else w.head(200000), score, min(args.cpu_seconds, 20.0),
-                         processes=procs)
+        r = cpu_baseline(w if w.queries is not None else w.head(200000), score, per_step, processes=procs)
         if i >= args.warmup:
             steps.append(r)
     v = float(np.median([s["value"] for s in steps]))
