@@ -684,8 +684,24 @@ __global__ void walk_kernel(TraceArgs A) {
         }
         if ((double)st.score_f < A.P.host_minimum) show = false;  // :758-759
         int s_start = x + 1, t_start = y + 1, ncols = 0, mt = 0, mm = 0;
+        // Affine stop rule: whether a candidate lies on the cell's diagonal
+        // run of MAIN cells (run_has_candidate).  Along a diagonal stretch of
+        // the walk it follows from the cell the walk came from (-1: unknown,
+        // after a gap move), so the run is scanned only when that is unknown.
+        int run_next = -1;
         while (show && x >= 0 && y >= 0 && dir != kStopDir && dir != 32) {  // :761
-            dir = walk_direction<AFFINE>(v, x, y);
+            const uint8_t cd = v.at(x, y);
+            const int d = cd & 3;
+            int run_here = (cd & kCand) ? 1 : (d != kUL ? 0 : run_next);
+            if (cd & kVisited) {
+                dir = kInAlignment;
+            } else if (d == kUL && (cd & kStopFlag)) {
+                if (AFFINE && run_here < 0) run_here = run_has_candidate(v, x + 1, y + 1) ? 1 : 0;
+                dir = (!AFFINE || run_here) ? kStopDir : kUL;
+            } else {
+                dir = d;
+            }
+            run_next = dir == kUL ? run_here : -1;
             v.at(x, y) |= kVisited;
             if (dir == kInAlignment) {
                 show = false;
