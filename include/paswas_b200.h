@@ -64,7 +64,7 @@ typedef struct {
     int64_t starting_points;
     int64_t hits;           /* hits kept by the walk (before the Python filter) */
     int64_t string_bytes;   /* bytes needed for all hit strings (3 * n_cols summed) */
-    int32_t kernel_launches;
+    int32_t kernel_launches; /* launches of this library's kernels (library sorts and scans not counted) */
     int32_t truncated;      /* 1 when the starting-point cap cut the walk short */
     double score_ms, trace_ms, walk_ms; /* device time of the three phases */
     double score_kernel_ms; /* summed duration of the score-sweep launches */

@@ -1292,7 +1292,7 @@ static cudaError_t finish_hits(pw_engine* e, int64_t n, int64_t* str_bytes) {
                   e->q_raw.as<uint8_t>(), e->q_raw_off.as<int64_t>(), e->t_raw.as<uint8_t>(),
                   e->t_raw_off.as<int64_t>(), e->f_str.as<char>());
     }
-    e->launches += 10;
+    e->launches += 6;  // this library's kernels (the CUB sorts and scan are not counted)
     if ((c = cudaGetLastError()) != cudaSuccess) return c;
     if (!e->h_hits.resize((size_t)n) || !e->h_strings.resize((size_t)total)) return cudaErrorMemoryAllocation;
     if ((c = cudaMemcpyAsync(e->h_hits.data(), e->f_out.p, (size_t)n * sizeof(pw_hit), cudaMemcpyDeviceToHost,
@@ -1670,7 +1670,6 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
                 (c = cub::DeviceSelect::Flagged(e->scan_tmp.p, tmp_bytes, ids, e->prune_flags.as<uint8_t>(),
                                                 e->prune_sel.as<int64_t>(), d_count, npairs, e->stream)) != cudaSuccess)
                 return cuda_fail(e, c, "select passing pairs");
-            e->launches++;
             if (!e->h_sel.resize((size_t)n_pass)) return fail(e, PW_ERR_NOMEM, "host memory for the passing pairs");
             if ((c = cudaMemcpyAsync(e->h_sel.data(), e->prune_sel.p, (size_t)n_pass * sizeof(int64_t),
                                      cudaMemcpyDeviceToHost, e->stream)) != cudaSuccess ||
