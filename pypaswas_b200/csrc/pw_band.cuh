@@ -138,6 +138,8 @@ __global__ void __launch_bounds__(128) band_kernel(KernelArgs A, BandArgs B) {
         const int* prog_in = B.progress + pred;
         int* prog_out = B.progress + it;
         const int ymine = yb + lane * kWarpRows;
+        const bool ypos = ymine > 0;       // this lane's first row is not row 0
+        const int rows_left = lt - ymine;  // rows r < rows_left of this lane lie inside the target
         int Hl[kWarpRows], Ml[kWarpRows], Jl[kWarpRows], Bl[kWarpRows];
 #pragma unroll
         for (int r = 0; r < kWarpRows; ++r) {
@@ -211,11 +213,12 @@ __global__ void __launch_bounds__(128) band_kernel(KernelArgs A, BandArgs B) {
                             const int ls = left + gap, us = up + gap;
                             uint32_t code = h == ls ? kLeft : (h == us ? kUp : kUL);
                             code = h > 0 ? code : kNo;
-                            const int y = ymine + r;
                             const bool ul = code == kUL;
-                            const bool stop = ul && xin && y > 0 && diag == 0;
+                            // y = ymine + r > 0 unless r == 0 and the lane's first row is row 0
+                            const bool stop = ul && xin && (r > 0 || ypos) && diag == 0;
                             code |= stop ? kStopFlag : 0u;
-                            if (ul && h >= thr && y < lt) {
+                            if (ul && h >= thr && r < rows_left) {
+                                const int y = ymine + r;
                                 code |= kCand;
                                 const int k = atomicAdd(ncand, 1);
                                 if (k < cap) {
@@ -251,11 +254,11 @@ __global__ void __launch_bounds__(128) band_kernel(KernelArgs A, BandArgs B) {
                         if constexpr (DIRS) {
                             uint32_t code = b == m ? kUL : (b == i ? kUp : kLeft);
                             code = b > 0 ? code : kNo;
-                            const int y = ymine + r;
                             const bool main_src = code == kUL;
-                            const bool stop = main_src && xin && y > 0 && mdiag == 0;
+                            const bool stop = main_src && xin && (r > 0 || ypos) && mdiag == 0;
                             code |= stop ? kStopFlag : 0u;
-                            if (main_src && m >= thr && y < lt) {
+                            if (main_src && m >= thr && r < rows_left) {
+                                const int y = ymine + r;
                                 code |= kCand;
                                 const int k = atomicAdd(ncand, 1);
                                 if (k < cap) {
