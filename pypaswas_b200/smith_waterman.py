@@ -163,52 +163,50 @@ class SmithWatermanB200(object):
         cov = span / ql.astype(np.float64)
         base = score / hits["n_cols"].astype(np.float64)
         thr = self._filter_thresholds()
-        keep = np.nonzero((rel >= thr[0]) & (ident >= thr[1]) & (cov >= thr[2]) & (base >= thr[3]))[0].tolist()
-        for qi in set(q_col[keep].tolist()):
+        kidx = np.nonzero((rel >= thr[0]) & (ident >= thr[1]) & (cov >= thr[2]) & (base >= thr[3]))[0]
+        for qi in set(q_col[kidx].tolist()):
             if not hasattr(sequences[qi], "distance"):
                 sequences[qi].distance = 0.0
-        cols = [c.tolist() for c in (q_col, t_col, s0, s1, t0, t1, score, mt, mm, rel, ident, cov, base)]
-        qc_, tc_, s0_, s1_, t0_, t1_, sc_, mt_, mm_, rel_, id_, cov_, base_ = cols
+        # the kept hits' columns, one list each, walked together
+        cols = [c[kidx].tolist() for c in (q_col, t_col, s0, s1, t0, t1, score, mt, mm, rel, ident, cov, base,
+                                            hits["n_cols"], hits["str_offset"])]
         logger = self.logger
         new = Hit.__new__
         if type(hit_list) is not HitList:
-            for k in keep:
-                n, o = nc[k], so[k]
+            for qi, ti, a0, a1, b0, b1, sc, m1, m2, rl, idn, cv, bs, n, o in zip(*cols):
                 h = new(Hit)
                 h.__dict__ = dict(
-                    logger=logger, sequence_info=sequences[qc_[k]], target_info=targets[tc_[k]],
-                    seq_location=(s0_[k], s1_[k]), target_location=(t0_[k], t1_[k]),
+                    logger=logger, sequence_info=sequences[qi], target_info=targets[ti],
+                    seq_location=(a0, a1), target_location=(b0, b1),
                     sequence_match=text[o:o + n], alignment=text[o + n:o + 2 * n],
-                    target_match=text[o + 2 * n:o + 3 * n], score=sc_[k], matches=mt_[k], mismatches=mm_[k],
-                    query_identity=id_[k], query_coverage=cov_[k], relative_score=rel_[k], base_score=base_[k],
+                    target_match=text[o + 2 * n:o + 3 * n], score=sc, matches=m1, mismatches=m2,
+                    query_identity=idn, query_coverage=cv, relative_score=rl, base_score=bs,
                     distance=None, rc=False)
                 hit_list.append(h)
             return
         # HitList.append inlined (same keys, same replacement rule, same log
         # records): the ids come from the record lists, the keys from the arrays
         hits_d, real = hit_list.hits, hit_list.real_hits
+        get = hits_d.get
         hl_log = hit_list.logger
         enabled = getattr(hl_log, "isEnabledFor", lambda level: True)
         log_info = hl_log is not None and enabled(logging.INFO)
         log_debug = hl_log is not None and enabled(logging.DEBUG)
         qid = [r.id for r in sequences]
         tid = [r.id for r in targets]
-        for k in keep:
-            n, o = nc[k], so[k]
-            qi, ti = qc_[k], tc_[k]
+        for qi, ti, a0, a1, b0, b1, sc, m1, m2, rl, idn, cv, bs, n, o in zip(*cols):
             sid, gid = qid[qi], tid[ti]
-            sc = sc_[k]
             h = new(Hit)
             h.__dict__ = {
                 "logger": logger, "sequence_info": sequences[qi], "target_info": targets[ti],
-                "seq_location": (s0_[k], s1_[k]), "target_location": (t0_[k], t1_[k]),
+                "seq_location": (a0, a1), "target_location": (b0, b1),
                 "sequence_match": text[o:o + n], "alignment": text[o + n:o + 2 * n],
-                "target_match": text[o + 2 * n:o + 3 * n], "score": sc, "matches": mt_[k], "mismatches": mm_[k],
-                "query_identity": id_[k], "query_coverage": cov_[k], "relative_score": rel_[k],
-                "base_score": base_[k], "distance": None, "rc": False}
-            k0 = (sid, gid, s0_[k], t0_[k])
-            k1 = (sid, gid, s1_[k], t1_[k])
-            old0, old1 = hits_d.get(k0), hits_d.get(k1)
+                "target_match": text[o + 2 * n:o + 3 * n], "score": sc, "matches": m1, "mismatches": m2,
+                "query_identity": idn, "query_coverage": cv, "relative_score": rl,
+                "base_score": bs, "distance": None, "rc": False}
+            k0 = (sid, gid, a0, b0)
+            k1 = (sid, gid, a1, b1)
+            old0, old1 = get(k0), get(k1)
             better_end = old1 is not None and old1.score < sc
             if (old0 is None and old1 is None) or better_end or (old0 is not None and old0.score < sc):
                 if better_end:
