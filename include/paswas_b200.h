@@ -316,6 +316,29 @@ int pw_score_max_noalloc(int device, const float* matrix, int dim, int char_offs
                          const uint8_t* t_residues, const int64_t* t_offsets, int32_t n_targets, float* pair_max,
                          char* err, int32_t err_bytes);
 
+/* ---------------------------------------------------------------------------
+ * trimmedFasta output without Python Hit objects (host only, no device).
+ * Replaces, for the trimmer's output, the chain Hit construction
+ * (SmithWaterman._print_alignments, SmithWaterman.py:822-838) -> _filter_hit
+ * (:843-848) -> HitList.append (HitList.py:28-52) -> TrimmerFormatter
+ * (Formatters.py:110-150, Hit.get_trimmed_line, Hit.py:274-286), byte for
+ * byte.  `hits` are pw_get_hits records in walk order.  Per query q (index of
+ * the hits' `query`): q_rank[q] the rank of its id in Python's string order
+ * (equal ids, equal ranks), its original length and start position, its id
+ * bytes q_id[q_id_off[q] .. q_id_off[q + 1]) and its sequence as given
+ * q_seq[q_seq_off[q] ..) (ASCII).  Per target: the same, t_id with the "_RC"
+ * suffix already removed as the formatter removes it.  thresholds: relative
+ * score, query identity, query coverage, base score.  With out == NULL the
+ * call only stores the byte count in *out_len; otherwise it writes the
+ * records (each ">target query\n trimmed query \n") and fails with
+ * PW_ERR_CAPACITY when out_cap is too small.  An invalid hit location returns
+ * PW_ERR_ARG (the reference raises there). */
+int pw_trimmed_fasta(const pw_hit* hits, int64_t n_hits, const int32_t* q_rank, const int64_t* q_orig_len,
+                     const int64_t* q_start_pos, const char* q_id, const int64_t* q_id_off, const char* q_seq,
+                     const int64_t* q_seq_off, const int32_t* t_rank, const int64_t* t_orig_len,
+                     const int64_t* t_start_pos, const char* t_id, const int64_t* t_id_off, const double* thresholds,
+                     char* out, int64_t out_cap, int64_t* out_len);
+
 #ifdef __cplusplus
 }
 #endif

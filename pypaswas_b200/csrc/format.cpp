@@ -1,0 +1,214 @@
+// format.cpp -- trimmedFasta output of a hit set without Python Hit objects.
+//
+// The trimmer's output path of the reference builds a Hit per walk result
+// (SmithWaterman._print_alignments, SmithWaterman.py:822-838), filters it
+// (_filter_hit, :843-848), de-duplicates it in a HitList (HitList.append,
+// HitList.py:28-52) and prints HitList.real_hits sorted by (query id, target
+// id, score) as trimmedFasta records (Formatters.py:110-150,
+// Hit.get_trimmed_line, Hit.py:274-286).  pw_trimmed_fasta does the same on
+// the engine's hit records and writes the same bytes.  Ids are ranked by the
+// caller (Python's string order), so ordering and de-duplication compare
+// integers; the target ids arrive with the "_RC" suffix already stripped.
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "../../include/paswas_b200.h"
+
+namespace {
+
+struct Key {
+    int32_t q, t;
+    int64_t a, b;
+    bool operator==(const Key& o) const { return q == o.q && t == o.t && a == o.a && b == o.b; }
+};
+
+// splitmix64 finaliser over the four fields
+inline uint64_t mix64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+struct KeyHash {
+    size_t operator()(const Key& k) const {
+        const uint64_t ids = ((uint64_t)(uint32_t)k.q << 32) | (uint32_t)k.t;
+        return (size_t)mix64(mix64(ids) ^ (uint64_t)k.a ^ ((uint64_t)k.b << 29) ^ ((uint64_t)k.b >> 35));
+    }
+};
+
+// Open-addressing table Key -> int64 (linear probing, tombstones on erase).
+struct FlatMap {
+    std::vector<Key> keys;
+    std::vector<int64_t> vals;
+    std::vector<uint8_t> state;  // 0 empty, 1 used, 2 erased
+    size_t mask = 0;
+    explicit FlatMap(size_t n) {
+        size_t cap = 16;
+        while (cap < 2 * n + 16) cap <<= 1;
+        keys.resize(cap);
+        vals.resize(cap);
+        state.assign(cap, 0);
+        mask = cap - 1;
+    }
+    int64_t* find(const Key& k) {
+        for (size_t i = KeyHash()(k) & mask;; i = (i + 1) & mask) {
+            if (state[i] == 0) return nullptr;
+            if (state[i] == 1 && keys[i] == k) return &vals[i];
+        }
+    }
+    void put(const Key& k, int64_t v) {
+        size_t slot = SIZE_MAX;
+        for (size_t i = KeyHash()(k) & mask;; i = (i + 1) & mask) {
+            if (state[i] == 0) {
+                if (slot == SIZE_MAX) slot = i;
+                break;
+            }
+            if (state[i] == 2) {
+                if (slot == SIZE_MAX) slot = i;
+            } else if (keys[i] == k) {
+                vals[i] = v;
+                return;
+            }
+        }
+        keys[slot] = k;
+        vals[slot] = v;
+        state[slot] = 1;
+    }
+    void erase(const Key& k) {
+        for (size_t i = KeyHash()(k) & mask;; i = (i + 1) & mask) {
+            if (state[i] == 0) return;
+            if (state[i] == 1 && keys[i] == k) {
+                state[i] = 2;
+                return;
+            }
+        }
+    }
+};
+
+struct Rec {
+    int32_t q, t;     // query / target list indices
+    int32_t qr, tr;   // id ranks
+    int64_t s0, t0;   // start of the hit (query, target), start positions added
+    int64_t t1;       // end on the target
+    double score;
+};
+
+}  // namespace
+
+extern "C" int pw_trimmed_fasta(const pw_hit* hits, int64_t n_hits, const int32_t* q_rank, const int64_t* q_orig_len,
+                                const int64_t* q_start_pos, const char* q_id, const int64_t* q_id_off,
+                                const char* q_seq, const int64_t* q_seq_off, const int32_t* t_rank,
+                                const int64_t* t_orig_len, const int64_t* t_start_pos, const char* t_id,
+                                const int64_t* t_id_off, const double* thresholds, char* out, int64_t out_cap,
+                                int64_t* out_len) {
+    if (n_hits < 0 || (n_hits > 0 && (!hits || !q_rank || !q_orig_len || !q_start_pos || !q_id || !q_id_off ||
+                                      !q_seq || !q_seq_off || !t_rank || !t_orig_len || !t_start_pos || !t_id ||
+                                      !t_id_off)) ||
+        !thresholds || !out_len)
+        return PW_ERR_ARG;
+    // locations, as the Hit constructor checks them (Hit.py:16-60): any
+    // invalid one fails the whole call, as the reference's exception does
+    std::vector<Rec> rec((size_t)n_hits);
+    for (int64_t i = 0; i < n_hits; ++i) {
+        const pw_hit& h = hits[i];
+        const int q = h.query, t = h.target;
+        const int64_t s0 = h.s_start + q_start_pos[q], s1 = h.s_end + q_start_pos[q];
+        const int64_t t0 = h.t_start + t_start_pos[t], t1 = h.t_end + t_start_pos[t];
+        if (!(0 <= s0 && s0 < s1 && s1 < q_orig_len[q] && 0 <= t0 && t0 < t1 && t1 < t_orig_len[t]))
+            return PW_ERR_ARG;
+        rec[i] = Rec{q, t, q_rank[q], t_rank[t], s0, t0, t1, (double)h.score};
+    }
+    // filter (SmithWaterman._filter_hit) and HitList.append, in walk order;
+    // `real` keeps Python's dict order: a new key goes last, a replaced one
+    // keeps its place, a deleted one is gone
+    FlatMap best((size_t)n_hits * 2);   // key -> hit
+    FlatMap real_pos((size_t)n_hits);   // start key -> slot of `real`
+    std::vector<int64_t> real;          // slot -> hit (-1: deleted)
+    real.reserve((size_t)n_hits);
+    for (int64_t i = 0; i < n_hits; ++i) {
+        const pw_hit& h = hits[i];
+        const Rec& r = rec[i];
+        const int64_t s1 = h.s_end + q_start_pos[r.q];
+        const double span = (double)(s1 - r.s0 + 1);
+        const double rel = r.score / (double)std::min(q_orig_len[r.q], t_orig_len[r.t]);
+        const double ident = (double)h.matches / span;
+        const double cov = span / (double)q_orig_len[r.q];
+        const double base = r.score / (double)h.n_cols;
+        if (!(rel >= thresholds[0] && ident >= thresholds[1] && cov >= thresholds[2] && base >= thresholds[3]))
+            continue;
+        const Key k0{r.qr, r.tr, r.s0, r.t0}, k1{r.qr, r.tr, s1, r.t1};
+        const int64_t* f0 = best.find(k0);
+        const int64_t* f1 = best.find(k1);
+        const bool better_end = f1 && rec[*f1].score < r.score;
+        if ((!f0 && !f1) || better_end || (f0 && rec[*f0].score < r.score)) {
+            if (better_end) {
+                const Rec& o = rec[*f1];
+                const Key ok{o.qr, o.tr, o.s0, o.t0};
+                if (int64_t* slot = real_pos.find(ok)) {
+                    real[*slot] = -1;
+                    real_pos.erase(ok);
+                }
+            }
+            best.put(k0, i);
+            best.put(k1, i);
+            if (int64_t* slot = real_pos.find(k0)) {
+                real[*slot] = i;
+            } else {
+                real_pos.put(k0, (int64_t)real.size());
+                real.push_back(i);
+            }
+        }
+    }
+    // sorted by (query id, target id, score), stable (Formatters.py:34-37)
+    struct SortKey {
+        int32_t qr, tr;
+        double score;
+        int64_t hit;
+    };
+    std::vector<SortKey> sk;
+    sk.reserve(real.size());
+    for (int64_t i : real)
+        if (i >= 0) sk.push_back(SortKey{rec[i].qr, rec[i].tr, rec[i].score, i});
+    std::stable_sort(sk.begin(), sk.end(), [](const SortKey& x, const SortKey& y) {
+        if (x.qr != y.qr) return x.qr < y.qr;
+        if (x.tr != y.tr) return x.tr < y.tr;
+        return x.score < y.score;
+    });
+    std::vector<int64_t> order(sk.size());
+    for (size_t k = 0; k < sk.size(); ++k) order[k] = sk[k].hit;
+    // ">" target id " " query id "\n" query[:t0] query[t1 + 1:] "\n": the
+    // query cut by the hit's TARGET coordinates, as Hit.get_trimmed_line does
+    int64_t need = 0;
+    for (int64_t i : order) {
+        const Rec& r = rec[i];
+        const int64_t L = q_seq_off[r.q + 1] - q_seq_off[r.q];
+        const int64_t a = std::min(r.t0, L), b = std::min(r.t1 + 1, L);
+        need += 1 + (t_id_off[r.t + 1] - t_id_off[r.t]) + 1 + (q_id_off[r.q + 1] - q_id_off[r.q]) + 1 + a + (L - b) + 1;
+    }
+    *out_len = need;
+    if (!out) return PW_OK;
+    if (out_cap < need) return PW_ERR_CAPACITY;
+    char* p = out;
+    auto put = [&](const char* s, int64_t n) {
+        if (n > 0) std::memcpy(p, s, (size_t)n);
+        p += n;
+    };
+    for (int64_t i : order) {
+        const Rec& r = rec[i];
+        const char* seq = q_seq + q_seq_off[r.q];
+        const int64_t L = q_seq_off[r.q + 1] - q_seq_off[r.q];
+        const int64_t a = std::min(r.t0, L), b = std::min(r.t1 + 1, L);
+        *p++ = '>';
+        put(t_id + t_id_off[r.t], t_id_off[r.t + 1] - t_id_off[r.t]);
+        *p++ = ' ';
+        put(q_id + q_id_off[r.q], q_id_off[r.q + 1] - q_id_off[r.q]);
+        *p++ = '\n';
+        put(seq, a);
+        put(seq + b, L - b);
+        *p++ = '\n';
+    }
+    return PW_OK;
+}

@@ -45,6 +45,60 @@ def trimmed_record(hit):
     return "".join((">", _strip_rc(hit.get_target_id()), " ", hit.sequence_info.id, "\n", seq[:t0], seq[t1 + 1:]))
 
 
+def trimmed_fasta(hits, sequences, targets, settings, lib=None):
+    """The trimmedFasta text of engine hit records (pw_get_hits order) -- the
+    bytes TrimmerFormatter(...).print_results writes for the HitList that the
+    driver builds from the same records, built in native code without Hit
+    objects (pw_trimmed_fasta).  `sequences` / `targets` are the records the
+    engine aligned (query / target indices of the hits); sequences must be
+    ASCII, as DNA, RNA and protein alphabets are."""
+    import ctypes
+    import numpy as np
+    from . import _native
+    from .exceptions import InvalidOptionException
+    lib = lib if lib is not None else _native.load_library()
+    hits = np.ascontiguousarray(hits, dtype=_native.HIT_DTYPE)
+
+    def ranks(ids):
+        order = {v: k for k, v in enumerate(sorted(set(ids)))}
+        return np.array([order[v] for v in ids], dtype=np.int32)
+
+    def blob(items):
+        data = [x.encode("utf-8") for x in items]
+        off = np.zeros(len(data) + 1, dtype=np.int64)
+        np.cumsum([len(x) for x in data], out=off[1:])
+        return np.frombuffer(b"".join(data) or b"\0", dtype=np.uint8), off
+
+    qids, tids = [r.id for r in sequences], [r.id for r in targets]
+    qseqs = [str(r.seq) for r in sequences]
+    if not all(q.isascii() for q in qseqs):
+        raise InvalidOptionException("trimmed_fasta needs ASCII sequences")
+    q_rank, t_rank = ranks(qids), ranks(tids)
+    q_len = np.array([r.original_length for r in sequences], dtype=np.int64)
+    t_len = np.array([r.original_length for r in targets], dtype=np.int64)
+    q_sp = np.array([getattr(r, "start_position", 0) for r in sequences], dtype=np.int64)
+    t_sp = np.array([getattr(r, "start_position", 0) for r in targets], dtype=np.int64)
+    q_id, q_id_off = blob([str(i) for i in qids])
+    t_id, t_id_off = blob([_strip_rc(str(i)) for i in tids])
+    q_seq, q_seq_off = blob(qseqs)
+    thr = np.array([float(settings.relative_score), float(settings.query_identity),
+                    float(settings.query_coverage), float(settings.base_score)], dtype=np.float64)
+    arrays = (q_rank, q_len, q_sp, q_id, q_id_off, q_seq, q_seq_off, t_rank, t_len, t_sp, t_id, t_id_off, thr)
+    ptrs = [a.ctypes.data_as(ctypes.c_void_p) for a in arrays]
+    n = ctypes.c_int64()
+    hp = hits.ctypes.data_as(ctypes.c_void_p) if len(hits) else None
+    rc = lib.pw_trimmed_fasta(hp, len(hits), *ptrs, None, 0, ctypes.byref(n))
+    if rc == _native.PW_ERR_ARG:
+        raise CudaException("Invalid hit location in the engine's records")
+    if rc != _native.PW_OK:
+        raise CudaException("pw_trimmed_fasta failed (%d)" % rc)
+    out = np.empty(max(n.value, 1), dtype=np.uint8)
+    rc = lib.pw_trimmed_fasta(hp, len(hits), *ptrs, out.ctypes.data_as(ctypes.c_void_p), n.value, ctypes.byref(n))
+    if rc != _native.PW_OK:
+        raise CudaException("pw_trimmed_fasta failed (%d)" % rc)
+    return out[:n.value].tobytes().decode("utf-8")
+
+
 class DefaultFormatter(object):
     """TXT output (Formatters.py:3-47)."""
 

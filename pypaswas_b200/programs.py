@@ -50,3 +50,21 @@ class Trimmer(Aligner):
             self.hitlist.extend(results)
             target_index = last
         return self.hitlist
+
+    def trimmed_fasta(self, records_seqs, targets):
+        """The trimmedFasta output of process() + TrimmerFormatter, byte for
+        byte, with the HitList and the records built in native code
+        (formatters.trimmed_fasta).  The engine takes every target in one
+        block, so the per-block HitList merge does not arise."""
+        from .formatters import trimmed_fasta
+        all_targets_length = sum(len(s.seq) for s in targets)
+        all_sequences_length = sum(len(s.seq) for s in records_seqs)
+        self.smith_waterman.set_total_work_size(all_targets_length * all_sequences_length)
+        if len(targets) == 0:
+            return ""
+        max_length = len(targets[0]) if getattr(self.settings, "recompile", "T") == "F" else None
+        last = self.smith_waterman.set_targets(targets, 0, max_length, records_seqs)
+        if last != len(targets):
+            raise AssertionError("the engine takes every target in one block")
+        hits, block = self.smith_waterman.align_records(records_seqs, targets, 0)
+        return trimmed_fasta(hits, records_seqs, block, self.settings)

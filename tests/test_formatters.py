@@ -48,3 +48,73 @@ def test_trimmed_record_cuts_target_span_from_query():
     hl = HitList(None)
     hl.real_hits[0] = h
     assert TrimmerFormatter(None, hl, None).lines() == [">adapter3 read7\nAAACGGGG"]
+
+
+def _synthetic_trimmer_hits(seed, n=400):
+    import numpy as np
+    from pypaswas_b200 import _native
+    from pypaswas_b200.records import SeqRecord
+    rng = np.random.default_rng(seed)
+    seqs = [SeqRecord("".join("acgtACGT"[i] for i in rng.integers(0, 8, int(rng.integers(40, 90)))),
+                      "read%d" % (i % 7)) for i in range(12)]  # repeated ids
+    seqs[3].id = "réad-ü"  # non-ASCII id
+    for r in seqs[:4]:
+        r.start_position = 5
+    tgts = [SeqRecord("".join("ACGT"[i] for i in rng.integers(0, 4, int(rng.integers(20, 45)))),
+                      "adapter%d%s" % (i // 2, "_RC" if i % 2 else "")) for i in range(6)]
+    rows = []
+    for _ in range(n):
+        q, t = int(rng.integers(0, len(seqs))), int(rng.integers(0, len(tgts)))
+        lq, lt = len(seqs[q].seq), len(tgts[t].seq)
+        s0 = int(rng.integers(0, lq - 17))  # room for the start position of 5
+        t0 = int(rng.integers(0, lt - 12))
+        k = int(rng.integers(2, 10))
+        rows.append((q, t, s0, s0 + k, t0, t0 + k, float(rng.integers(3, 12)), k))
+    rows += rows[: n // 5]
+    rows += [(q, t, s0, s1, t0, t1, sc + 1.0, k) for (q, t, s0, s1, t0, t1, sc, k) in rows[: n // 10]]
+    hits = np.zeros(len(rows), dtype=_native.HIT_DTYPE)
+    text, off = [], 0
+    for i, (q, t, s0, s1, t0, t1, sc, k) in enumerate(rows):
+        for name, v in (("query", q), ("target", t), ("s_start", s0), ("s_end", s1), ("t_start", t0),
+                        ("t_end", t1), ("score", sc), ("matches", k // 2), ("mismatches", k - k // 2),
+                        ("n_cols", k), ("str_offset", off)):
+            hits[i][name] = v
+        text.append("A" * k + "|" * k + "C" * k)
+        off += 3 * k
+    return hits, "".join(text).encode("latin-1"), seqs, tgts
+
+
+def test_native_trimmed_fasta_matches_hitlist_and_formatter():
+    """formatters.trimmed_fasta (pw_trimmed_fasta) writes exactly the bytes of
+    the driver's HitList (filter, de-duplication, dict order) printed by
+    TrimmerFormatter: repeated ids, _RC targets, start positions, a non-ASCII
+    id, trimming coordinates past the query's end."""
+    import logging
+    import cases
+    from pypaswas_b200.formatters import TrimmerFormatter, trimmed_fasta
+    from pypaswas_b200.hits import HitList
+    from pypaswas_b200.smith_waterman import SmithWatermanB200
+    for seed, thr in ((1, ("0", "0", "0", "0")), (2, ("0.1", "0.3", "0.05", "0.5"))):
+        hits, strbuf, seqs, tgts = _synthetic_trimmer_hits(seed)
+        st = cases.Settings(relative_score=thr[0], query_identity=thr[1], query_coverage=thr[2],
+                            base_score=thr[3])
+        sw = SmithWatermanB200.__new__(SmithWatermanB200)
+        sw.logger = logging.getLogger("test")
+        sw.settings = st
+        hl = HitList(sw.logger)
+        sw._build_hits(hits, strbuf, seqs, tgts, hl)
+        expect = "".join(line + "\n" for line in TrimmerFormatter(None, hl, None).lines())
+        assert len(hl.real_hits) > 20
+        assert trimmed_fasta(hits, seqs, tgts, st) == expect
+
+
+def test_native_trimmed_fasta_rejects_an_invalid_location():
+    import pytest
+    import cases
+    from pypaswas_b200.exceptions import CudaException
+    from pypaswas_b200.formatters import trimmed_fasta
+    hits, strbuf, seqs, tgts = _synthetic_trimmer_hits(3, n=20)
+    hits[5]["s_end"] = hits[5]["s_start"]  # a one-column hit: start == end
+    st = cases.Settings(relative_score="0", query_identity="0", query_coverage="0", base_score="0")
+    with pytest.raises(CudaException):
+        trimmed_fasta(hits, seqs, tgts, st)
