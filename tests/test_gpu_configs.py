@@ -82,6 +82,13 @@ def test_config4_sample_bit_exact_with_trimmed_fasta(engine_lib, oracle_mod):
             hl.append(hit)
     assert got == TrimmerFormatter(None, hl, None).lines()
     assert len(got) > 50
+    # the native output path (engine records -> trimmedFasta bytes, no Hit objects)
+    prog2 = Trimmer(None, None, w.settings)
+    try:
+        text = prog2.trimmed_fasta(qrec, trec)
+    finally:
+        prog2.smith_waterman.close()
+    assert text == "".join(line + "\n" for line in got)
 
 
 @pytest.mark.parametrize("config", [1, 2])
