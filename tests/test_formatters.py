@@ -84,7 +84,7 @@ def _synthetic_trimmer_hits(seed, n=400):
     return hits, "".join(text).encode("latin-1"), seqs, tgts
 
 
-def test_native_trimmed_fasta_matches_hitlist_and_formatter():
+def test_native_trimmed_fasta_matches_hitlist_and_formatter(engine_lib):
     """formatters.trimmed_fasta (pw_trimmed_fasta) writes exactly the bytes of
     the driver's HitList (filter, de-duplication, dict order) printed by
     TrimmerFormatter: repeated ids, _RC targets, start positions, a non-ASCII
@@ -105,10 +105,10 @@ def test_native_trimmed_fasta_matches_hitlist_and_formatter():
         sw._build_hits(hits, strbuf, seqs, tgts, hl)
         expect = "".join(line + "\n" for line in TrimmerFormatter(None, hl, None).lines())
         assert len(hl.real_hits) > 20
-        assert trimmed_fasta(hits, seqs, tgts, st) == expect
+        assert trimmed_fasta(hits, seqs, tgts, st, lib=engine_lib) == expect
 
 
-def test_native_trimmed_fasta_rejects_an_invalid_location():
+def test_native_trimmed_fasta_rejects_an_invalid_location(engine_lib):
     import pytest
     import cases
     from pypaswas_b200.exceptions import CudaException
@@ -117,4 +117,4 @@ def test_native_trimmed_fasta_rejects_an_invalid_location():
     hits[5]["s_end"] = hits[5]["s_start"]  # a one-column hit: start == end
     st = cases.Settings(relative_score="0", query_identity="0", query_coverage="0", base_score="0")
     with pytest.raises(CudaException):
-        trimmed_fasta(hits, seqs, tgts, st)
+        trimmed_fasta(hits, seqs, tgts, st, lib=engine_lib)
