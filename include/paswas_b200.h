@@ -339,6 +339,17 @@ int pw_trimmed_fasta(const pw_hit* hits, int64_t n_hits, const int32_t* q_rank, 
                      const int64_t* t_start_pos, const char* t_id, const int64_t* t_id_off, const double* thresholds,
                      char* out, int64_t out_cap, int64_t* out_len);
 
+/* TXT output (DefaultFormatter, Formatters.py:3-47) of the same HitList, byte
+ * for byte, Python's float repr included: per record the summary line and the
+ * three alignment strings, each line ending in a newline.  Arguments as
+ * pw_trimmed_fasta's, plus strbuf / strbuf_bytes (the pw_get_hits strings)
+ * and without the query sequences; t_id holds the target ids as they are. */
+int pw_txt_records(const pw_hit* hits, int64_t n_hits, const char* strbuf, int64_t strbuf_bytes,
+                   const int32_t* q_rank, const int64_t* q_orig_len, const int64_t* q_start_pos, const char* q_id,
+                   const int64_t* q_id_off, const int32_t* t_rank, const int64_t* t_orig_len,
+                   const int64_t* t_start_pos, const char* t_id, const int64_t* t_id_off, const double* thresholds,
+                   char* out, int64_t out_cap, int64_t* out_len);
+
 #ifdef __cplusplus
 }
 #endif

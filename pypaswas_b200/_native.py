@@ -42,7 +42,7 @@ EXPORTED_SYMBOLS = (
     "pw_get_starting_points", "pw_last_launch_count", "pw_measure_int_peak", "pw_score_max_noalloc",
     "pw_set_wave_limit", "pw_set_tuning", "pw_set_pairs", "pw_server_create", "pw_server_destroy", "pw_server_last_error", "pw_server_set_scoring",
     "pw_server_load_db", "pw_server_submit", "pw_server_wait", "pw_server_top_hits", "pw_server_hits",
-    "pw_server_release", "pw_server_stats", "pw_server_tune", "pw_trimmed_fasta",
+    "pw_server_release", "pw_server_stats", "pw_server_tune", "pw_trimmed_fasta", "pw_txt_records",
 )
 
 
@@ -142,6 +142,8 @@ def bind(lib):
         "pw_server_tune": (ctypes.c_int, [P, ctypes.c_int, I64]),
         "pw_trimmed_fasta": (ctypes.c_int, [P, I64, P, P, P, P, P, P, P, P, P, P, P, P, P, P, I64,
                                             ctypes.POINTER(I64)]),
+        "pw_txt_records": (ctypes.c_int, [P, I64, P, I64, P, P, P, P, P, P, P, P, P, P, P, P, I64,
+                                          ctypes.POINTER(I64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -10,8 +10,12 @@
 // caller (Python's string order), so ordering and de-duplication compare
 // integers; the target ids arrive with the "_RC" suffix already stripped.
 #include <algorithm>
+#include <charconv>
+#include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "../../include/paswas_b200.h"
@@ -98,20 +102,18 @@ struct Rec {
 
 }  // namespace
 
-extern "C" int pw_trimmed_fasta(const pw_hit* hits, int64_t n_hits, const int32_t* q_rank, const int64_t* q_orig_len,
-                                const int64_t* q_start_pos, const char* q_id, const int64_t* q_id_off,
-                                const char* q_seq, const int64_t* q_seq_off, const int32_t* t_rank,
-                                const int64_t* t_orig_len, const int64_t* t_start_pos, const char* t_id,
-                                const int64_t* t_id_off, const double* thresholds, char* out, int64_t out_cap,
-                                int64_t* out_len) {
-    if (n_hits < 0 || (n_hits > 0 && (!hits || !q_rank || !q_orig_len || !q_start_pos || !q_id || !q_id_off ||
-                                      !q_seq || !q_seq_off || !t_rank || !t_orig_len || !t_start_pos || !t_id ||
-                                      !t_id_off)) ||
-        !thresholds || !out_len)
-        return PW_ERR_ARG;
-    // locations, as the Hit constructor checks them (Hit.py:16-60): any
-    // invalid one fails the whole call, as the reference's exception does
-    std::vector<Rec> rec((size_t)n_hits);
+// The driver's HitList for these records: locations checked as the Hit
+// constructor checks them (Hit.py:16-60; any invalid one fails the call, as
+// the reference's exception does), the filter (SmithWaterman._filter_hit),
+// HitList.append in walk order, then HitList.real_hits sorted by (query id,
+// target id, score), stable (Formatters.py:34-37).  `real` keeps Python's
+// dict order: a new key goes last, a replaced one keeps its place, a deleted
+// one is gone.
+static int ordered_real_hits(const pw_hit* hits, int64_t n_hits, const int32_t* q_rank, const int64_t* q_orig_len,
+                             const int64_t* q_start_pos, const int32_t* t_rank, const int64_t* t_orig_len,
+                             const int64_t* t_start_pos, const double* thresholds, std::vector<Rec>& rec,
+                             std::vector<int64_t>& order) {
+    rec.resize((size_t)n_hits);
     for (int64_t i = 0; i < n_hits; ++i) {
         const pw_hit& h = hits[i];
         const int q = h.query, t = h.target;
@@ -121,9 +123,6 @@ extern "C" int pw_trimmed_fasta(const pw_hit* hits, int64_t n_hits, const int32_
             return PW_ERR_ARG;
         rec[i] = Rec{q, t, q_rank[q], t_rank[t], s0, t0, t1, (double)h.score};
     }
-    // filter (SmithWaterman._filter_hit) and HitList.append, in walk order;
-    // `real` keeps Python's dict order: a new key goes last, a replaced one
-    // keeps its place, a deleted one is gone
     FlatMap best((size_t)n_hits * 2);   // key -> hit
     FlatMap real_pos((size_t)n_hits);   // start key -> slot of `real`
     std::vector<int64_t> real;          // slot -> hit (-1: deleted)
@@ -162,7 +161,6 @@ extern "C" int pw_trimmed_fasta(const pw_hit* hits, int64_t n_hits, const int32_
             }
         }
     }
-    // sorted by (query id, target id, score), stable (Formatters.py:34-37)
     struct SortKey {
         int32_t qr, tr;
         double score;
@@ -177,8 +175,27 @@ extern "C" int pw_trimmed_fasta(const pw_hit* hits, int64_t n_hits, const int32_
         if (x.tr != y.tr) return x.tr < y.tr;
         return x.score < y.score;
     });
-    std::vector<int64_t> order(sk.size());
+    order.resize(sk.size());
     for (size_t k = 0; k < sk.size(); ++k) order[k] = sk[k].hit;
+    return PW_OK;
+}
+
+extern "C" int pw_trimmed_fasta(const pw_hit* hits, int64_t n_hits, const int32_t* q_rank, const int64_t* q_orig_len,
+                                const int64_t* q_start_pos, const char* q_id, const int64_t* q_id_off,
+                                const char* q_seq, const int64_t* q_seq_off, const int32_t* t_rank,
+                                const int64_t* t_orig_len, const int64_t* t_start_pos, const char* t_id,
+                                const int64_t* t_id_off, const double* thresholds, char* out, int64_t out_cap,
+                                int64_t* out_len) {
+    if (n_hits < 0 || (n_hits > 0 && (!hits || !q_rank || !q_orig_len || !q_start_pos || !q_id || !q_id_off ||
+                                      !q_seq || !q_seq_off || !t_rank || !t_orig_len || !t_start_pos || !t_id ||
+                                      !t_id_off)) ||
+        !thresholds || !out_len)
+        return PW_ERR_ARG;
+    std::vector<Rec> rec;
+    std::vector<int64_t> order;
+    const int rc = ordered_real_hits(hits, n_hits, q_rank, q_orig_len, q_start_pos, t_rank, t_orig_len, t_start_pos,
+                                     thresholds, rec, order);
+    if (rc != PW_OK) return rc;
     // ">" target id " " query id "\n" query[:t0] query[t1 + 1:] "\n": the
     // query cut by the hit's TARGET coordinates, as Hit.get_trimmed_line does
     int64_t need = 0;
@@ -210,5 +227,130 @@ extern "C" int pw_trimmed_fasta(const pw_hit* hits, int64_t n_hits, const int32_
         put(seq + b, L - b);
         *p++ = '\n';
     }
+    return PW_OK;
+}
+
+// Python's repr of a float (str(float) in Python 3): the shortest digits that
+// round-trip (std::to_chars), laid out as Python's float_repr does --
+// exponent form when the decimal point falls before the 4th leading zero or
+// after the 16th digit, else fixed form, with ".0" after an integer value.
+static void put_pyfloat(std::string& o, double v) {
+    if (std::isnan(v)) {
+        o += "nan";
+        return;
+    }
+    if (std::isinf(v)) {
+        o += v < 0 ? "-inf" : "inf";
+        return;
+    }
+    char buf[64];
+    const auto r = std::to_chars(buf, buf + sizeof(buf) - 1, v, std::chars_format::scientific);
+    *r.ptr = '\0';  // the exponent is read up to here
+    const char* p = buf;
+    if (*p == '-') {
+        o += '-';
+        ++p;
+    }
+    std::string digits(1, *p++);
+    if (*p == '.') {
+        ++p;
+        while (*p != 'e') digits += *p++;
+    }
+    const int decpt = std::atoi(p + 1) + 1;  // value = 0.digits x 10^decpt
+    const int n = (int)digits.size();
+    if (decpt <= -4 || decpt > 16) {
+        o += digits[0];
+        if (n > 1) {
+            o += '.';
+            o.append(digits, 1, std::string::npos);
+        }
+        int e = decpt - 1;
+        o += e < 0 ? "e-" : "e+";
+        e = e < 0 ? -e : e;
+        if (e < 10) o += '0';
+        o += std::to_string(e);
+    } else if (decpt <= 0) {
+        o += "0.";
+        o.append((size_t)(-decpt), '0');
+        o += digits;
+    } else if (decpt >= n) {
+        o += digits;
+        o.append((size_t)(decpt - n), '0');
+        o += ".0";
+    } else {
+        o.append(digits, 0, (size_t)decpt);
+        o += '.';
+        o.append(digits, (size_t)decpt, std::string::npos);
+    }
+}
+
+// TXT records (DefaultFormatter, Formatters.py:19-31) of the same HitList:
+// "query, target, s_start, s_end, t_start, t_end, score, matches, mismatches,
+// gaps, columns, score/columns, query length, target length, score/query
+// length, score/target length, distance" and the three alignment strings,
+// each record followed by a newline.  Only the record bytes differ from
+// pw_trimmed_fasta's arguments: strbuf holds the hits' strings (pw_get_hits)
+// and t_id the target ids as they are.
+extern "C" int pw_txt_records(const pw_hit* hits, int64_t n_hits, const char* strbuf, int64_t strbuf_bytes,
+                              const int32_t* q_rank, const int64_t* q_orig_len, const int64_t* q_start_pos,
+                              const char* q_id, const int64_t* q_id_off, const int32_t* t_rank,
+                              const int64_t* t_orig_len, const int64_t* t_start_pos, const char* t_id,
+                              const int64_t* t_id_off, const double* thresholds, char* out, int64_t out_cap,
+                              int64_t* out_len) {
+    if (n_hits < 0 || (n_hits > 0 && (!hits || !strbuf || !q_rank || !q_orig_len || !q_start_pos || !q_id ||
+                                      !q_id_off || !t_rank || !t_orig_len || !t_start_pos || !t_id || !t_id_off)) ||
+        !thresholds || !out_len)
+        return PW_ERR_ARG;
+    for (int64_t i = 0; i < n_hits; ++i)
+        if (hits[i].n_cols < 0 || hits[i].str_offset < 0 || hits[i].str_offset + 3 * (int64_t)hits[i].n_cols > strbuf_bytes)
+            return PW_ERR_ARG;
+    std::vector<Rec> rec;
+    std::vector<int64_t> order;
+    const int rc = ordered_real_hits(hits, n_hits, q_rank, q_orig_len, q_start_pos, t_rank, t_orig_len, t_start_pos,
+                                     thresholds, rec, order);
+    if (rc != PW_OK) return rc;
+    std::string o;
+    for (int64_t i : order) {
+        const pw_hit& h = hits[i];
+        const Rec& r = rec[i];
+        const int64_t n = h.n_cols;
+        const int64_t s1 = h.s_end + q_start_pos[r.q];
+        const int64_t ql = q_orig_len[r.q], tl = t_orig_len[r.t];
+        o.append(q_id + q_id_off[r.q], (size_t)(q_id_off[r.q + 1] - q_id_off[r.q]));
+        o += ", ";
+        o.append(t_id + t_id_off[r.t], (size_t)(t_id_off[r.t + 1] - t_id_off[r.t]));
+        for (int64_t v : {r.s0, s1, r.t0, r.t1}) {
+            o += ", ";
+            o += std::to_string(v);
+        }
+        o += ", ";
+        put_pyfloat(o, r.score);
+        for (int64_t v : {(int64_t)h.matches, (int64_t)h.mismatches, n - h.matches - h.mismatches, n}) {
+            o += ", ";
+            o += std::to_string(v);
+        }
+        o += ", ";
+        put_pyfloat(o, r.score / (double)n);
+        o += ", ";
+        o += std::to_string(ql);
+        o += ", ";
+        o += std::to_string(tl);
+        o += ", ";
+        put_pyfloat(o, r.score / (double)ql);
+        o += ", ";
+        put_pyfloat(o, r.score / (double)tl);
+        o += ", None\n";
+        const char* sb = strbuf + h.str_offset;
+        o.append(sb, (size_t)n);
+        o += '\n';
+        o.append(sb + n, (size_t)n);
+        o += '\n';
+        o.append(sb + 2 * n, (size_t)n);
+        o += '\n';
+    }
+    *out_len = (int64_t)o.size();
+    if (!out) return PW_OK;
+    if (out_cap < (int64_t)o.size()) return PW_ERR_CAPACITY;
+    if (!o.empty()) std::memcpy(out, o.data(), o.size());
     return PW_OK;
 }

@@ -45,6 +45,67 @@ def trimmed_record(hit):
     return "".join((">", _strip_rc(hit.get_target_id()), " ", hit.sequence_info.id, "\n", seq[:t0], seq[t1 + 1:]))
 
 
+def _record_arrays(sequences, targets, settings, strip_target_rc):
+    """Per-record inputs of the native formatters: id ranks in Python's
+    order, lengths, start positions, id bytes, thresholds."""
+    import numpy as np
+
+    def ranks(ids):
+        order = {v: k for k, v in enumerate(sorted(set(ids)))}
+        return np.array([order[v] for v in ids], dtype=np.int32)
+
+    def blob(items):
+        data = [x.encode("utf-8") for x in items]
+        off = np.zeros(len(data) + 1, dtype=np.int64)
+        np.cumsum([len(x) for x in data], out=off[1:])
+        return np.frombuffer(b"".join(data) or b"\0", dtype=np.uint8), off
+
+    qids, tids = [r.id for r in sequences], [r.id for r in targets]
+    q = (ranks(qids), np.array([r.original_length for r in sequences], dtype=np.int64),
+         np.array([getattr(r, "start_position", 0) for r in sequences], dtype=np.int64)) + \
+        blob([str(i) for i in qids])
+    t = (ranks(tids), np.array([r.original_length for r in targets], dtype=np.int64),
+         np.array([getattr(r, "start_position", 0) for r in targets], dtype=np.int64)) + \
+        blob([_strip_rc(str(i)) if strip_target_rc else str(i) for i in tids])
+    thr = np.array([float(settings.relative_score), float(settings.query_identity),
+                    float(settings.query_coverage), float(settings.base_score)], dtype=np.float64)
+    return q, t, thr, blob
+
+
+def _call_twice(fn, head, tail):
+    """Size query, then the write, of a native formatter; returns the text."""
+    import ctypes
+    import numpy as np
+    from . import _native
+    n = ctypes.c_int64()
+    rc = fn(*head, *tail, None, 0, ctypes.byref(n))
+    if rc == _native.PW_ERR_ARG:
+        raise CudaException("Invalid hit location in the engine's records")
+    if rc != _native.PW_OK:
+        raise CudaException("native formatter failed (%d)" % rc)
+    out = np.empty(max(n.value, 1), dtype=np.uint8)
+    rc = fn(*head, *tail, out.ctypes.data_as(ctypes.c_void_p), n.value, ctypes.byref(n))
+    if rc != _native.PW_OK:
+        raise CudaException("native formatter failed (%d)" % rc)
+    return out[:n.value].tobytes().decode("utf-8")
+
+
+def txt_records(hits, strbuf, sequences, targets, settings, lib=None):
+    """The TXT text (DefaultFormatter.print_results) of engine hit records and
+    their strings (Engine.hits()), built in native code (pw_txt_records)."""
+    import ctypes
+    import numpy as np
+    from . import _native
+    lib = lib if lib is not None else _native.load_library()
+    hits = np.ascontiguousarray(hits, dtype=_native.HIT_DTYPE)
+    q, t, thr, _ = _record_arrays(sequences, targets, settings, False)
+    sb = np.frombuffer(bytes(strbuf) or b"\0", dtype=np.uint8)
+    vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    head = (vp(hits) if len(hits) else None, len(hits), vp(sb), len(strbuf))
+    tail = tuple(vp(a) for a in q) + tuple(vp(a) for a in t) + (vp(thr),)
+    return _call_twice(lib.pw_txt_records, head, tail)
+
+
 def trimmed_fasta(hits, sequences, targets, settings, lib=None):
     """The trimmedFasta text of engine hit records (pw_get_hits order) -- the
     bytes TrimmerFormatter(...).print_results writes for the HitList that the

@@ -8,6 +8,18 @@ from .scores import make_score
 from .smith_waterman import SmithWatermanB200
 
 
+def _one_block(program, records_seqs, targets, max_length=None):
+    """The driver's single target block (the engine takes every target):
+    the engine's hit records, their strings and the block."""
+    all_targets_length = sum(len(s.seq) for s in targets)
+    all_sequences_length = sum(len(s.seq) for s in records_seqs)
+    program.smith_waterman.set_total_work_size(all_targets_length * all_sequences_length)
+    last = program.smith_waterman.set_targets(targets, 0, max_length, records_seqs)
+    if last != len(targets):
+        raise AssertionError("the engine takes every target in one block")
+    return program.smith_waterman.align_records(records_seqs, targets, 0)
+
+
 class Aligner(object):
     """Aligns query records against target records (Programs.py:9-86)."""
 
@@ -31,6 +43,16 @@ class Aligner(object):
             self.hitlist.extend(results)
             target_index = last
         return self.hitlist
+
+    def txt(self, records_seqs, targets):
+        """The TXT output of process() + DefaultFormatter, byte for byte, with
+        the HitList and the records built in native code
+        (formatters.txt_records)."""
+        from .formatters import txt_records
+        if len(targets) == 0:
+            return ""
+        hits, strbuf, block = _one_block(self, records_seqs, targets)
+        return txt_records(hits, strbuf, records_seqs, block, self.settings)
 
 
 class Trimmer(Aligner):
@@ -57,14 +79,8 @@ class Trimmer(Aligner):
         (formatters.trimmed_fasta).  The engine takes every target in one
         block, so the per-block HitList merge does not arise."""
         from .formatters import trimmed_fasta
-        all_targets_length = sum(len(s.seq) for s in targets)
-        all_sequences_length = sum(len(s.seq) for s in records_seqs)
-        self.smith_waterman.set_total_work_size(all_targets_length * all_sequences_length)
         if len(targets) == 0:
             return ""
         max_length = len(targets[0]) if getattr(self.settings, "recompile", "T") == "F" else None
-        last = self.smith_waterman.set_targets(targets, 0, max_length, records_seqs)
-        if last != len(targets):
-            raise AssertionError("the engine takes every target in one block")
-        hits, block = self.smith_waterman.align_records(records_seqs, targets, 0)
+        hits, _, block = _one_block(self, records_seqs, targets, max_length)
         return trimmed_fasta(hits, records_seqs, block, self.settings)

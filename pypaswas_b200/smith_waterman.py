@@ -130,11 +130,12 @@ class SmithWatermanB200(object):
 
     def align_records(self, records_seqs, targets, target_index):
         """align_sequences without the Python Hit objects: the engine's hit
-        records of the current target block (walk order) and the block."""
+        records of the current target block (walk order), their alignment
+        strings and the block."""
         if self.number_targets <= 0:
             self.set_targets(targets, target_index)
         if len(records_seqs) == 0 or self.number_targets == 0:
-            return np.zeros(0, dtype=_native.HIT_DTYPE), []
+            return np.zeros(0, dtype=_native.HIT_DTYPE), b"", []
         t0 = time.time()
         block, h2d = self._upload(records_seqs, targets, target_index)
         info = self.engine.align(start_cap=self.maximum_number_starting_points * len(records_seqs) * len(block))
@@ -146,7 +147,7 @@ class SmithWatermanB200(object):
         self.last_h2d_bytes = h2d
         self.last_d2h_bytes = 4 * len(records_seqs) * len(block) + hits.nbytes + len(strbuf)
         self._progress(records_seqs, block, t0)
-        return hits, block
+        return hits, strbuf, block
 
     def _build_hits(self, hits, strbuf, sequences, targets, hit_list):
         """Hit objects in walk order (SmithWaterman._print_alignments :822-838).

@@ -118,3 +118,54 @@ def test_native_trimmed_fasta_rejects_an_invalid_location(engine_lib):
     st = cases.Settings(relative_score="0", query_identity="0", query_coverage="0", base_score="0")
     with pytest.raises(CudaException):
         trimmed_fasta(hits, seqs, tgts, st, lib=engine_lib)
+
+
+def test_native_txt_records_match_default_formatter(engine_lib):
+    """formatters.txt_records (pw_txt_records) writes exactly what
+    DefaultFormatter.print_results writes for the driver's HitList, Python's
+    float repr of the ratios included (fractional scores, long and short
+    ratios, an exponent-form value)."""
+    import logging
+    import cases
+    from pypaswas_b200.formatters import DefaultFormatter, txt_records
+    from pypaswas_b200.hits import HitList
+    from pypaswas_b200.smith_waterman import SmithWatermanB200
+    for seed in (4, 5):
+        hits, strbuf, seqs, tgts = _synthetic_trimmer_hits(seed)
+        hits["score"] = hits["score"] + (seed - 4) * 0.25  # fractional fp32 scores
+        hits["score"][0] = 1e-5  # a ratio printed in exponent form
+        st = cases.Settings(relative_score="0", query_identity="0", query_coverage="0", base_score="0")
+        sw = SmithWatermanB200.__new__(SmithWatermanB200)
+        sw.logger = logging.getLogger("test")
+        sw.settings = st
+        hl = HitList(sw.logger)
+        sw._build_hits(hits, strbuf, seqs, tgts, hl)
+        expect = "".join(line + "\n" for line in DefaultFormatter(None, hl, None).lines())
+        assert len(hl.real_hits) > 20
+        assert txt_records(hits, strbuf, seqs, tgts, st, lib=engine_lib) == expect
+
+
+def test_native_txt_float_repr_over_many_magnitudes(engine_lib):
+    """The scores and ratios of the TXT records printed natively equal
+    Python's repr across fp32 magnitudes from 1e-38 to 1e38 (the exponent
+    and fixed forms, the boundaries at 1e-4 and 1e16)."""
+    import logging
+    import numpy as np
+    import cases
+    from pypaswas_b200.formatters import DefaultFormatter, txt_records
+    from pypaswas_b200.hits import HitList
+    from pypaswas_b200.smith_waterman import SmithWatermanB200
+    hits, strbuf, seqs, tgts = _synthetic_trimmer_hits(6, n=300)
+    rng = np.random.default_rng(6)
+    special = [0.0, 1e-4, 9.999e-5, 1e-5, 1e15, 1e16, 1e17, 0.1, 0.5, 1.0, 2.0 ** 24, 3.4e38, 1.2e-38, 123456.78]
+    vals = np.concatenate([special, 10.0 ** rng.uniform(-38, 38, len(hits) - len(special))]).astype(np.float32)
+    hits["score"] = vals[: len(hits)]
+    st = cases.Settings(relative_score="0", query_identity="0", query_coverage="0", base_score="0")
+    sw = SmithWatermanB200.__new__(SmithWatermanB200)
+    sw.logger = logging.getLogger("test")
+    sw.settings = st
+    hl = HitList(sw.logger)
+    sw._build_hits(hits, strbuf, seqs, tgts, hl)
+    expect = "".join(line + "\n" for line in DefaultFormatter(None, hl, None).lines())
+    assert len(hl.real_hits) > 100
+    assert txt_records(hits, strbuf, seqs, tgts, st, lib=engine_lib) == expect

@@ -11,9 +11,9 @@ import pytest
 import cases
 from engine_helpers import run_engine
 from pypaswas_b200 import scores, workloads
-from pypaswas_b200.formatters import TrimmerFormatter
+from pypaswas_b200.formatters import DefaultFormatter, TrimmerFormatter
 from pypaswas_b200.hits import Hit, HitList
-from pypaswas_b200.programs import Trimmer
+from pypaswas_b200.programs import Aligner, Trimmer
 from pypaswas_b200.records import SeqRecord
 
 pytestmark = pytest.mark.gpu
@@ -44,6 +44,22 @@ def test_config1_sample_bit_exact(engine_lib, oracle_mod):
     w = workloads.config1()
     o = _bit_exact(engine_lib, oracle_mod, _spread(w.queries, 120), w.targets, w.settings)
     assert len(o["hits"]) > 10
+
+
+def test_config1_aligner_native_txt_matches_the_formatter(engine_lib):
+    """Aligner.txt (engine records -> TXT bytes natively) equals
+    DefaultFormatter over Aligner.process's HitList."""
+    w = workloads.config1()
+    qrec = [SeqRecord(s.decode(), i) for i, s in _spread(w.queries, 120)]
+    trec = [SeqRecord(s.decode(), i) for i, s in w.targets]
+    prog = Aligner(None, None, w.settings)
+    try:
+        want = "".join(line + "\n" for line in DefaultFormatter(None, prog.process(qrec, trec, None), None).lines())
+        got = prog.txt(qrec, trec)
+    finally:
+        prog.smith_waterman.close()
+    assert len(want) > 1000
+    assert got == want
 
 
 def test_config2_sample_bit_exact(engine_lib, oracle_mod):
