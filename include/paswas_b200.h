@@ -322,8 +322,8 @@ int pw_score_max_noalloc(int device, const float* matrix, int dim, int char_offs
  * (SmithWaterman._print_alignments, SmithWaterman.py:822-838) -> _filter_hit
  * (:843-848) -> HitList.append (HitList.py:28-52) -> TrimmerFormatter
  * (Formatters.py:110-150, Hit.get_trimmed_line, Hit.py:274-286), byte for
- * byte.  `hits` are pw_get_hits records in walk order.  Per query q (index of
- * the hits' `query`): q_rank[q] the rank of its id in Python's string order
+ * byte.  `hits` are pw_get_hits records in walk order, their query / target
+ * indices below n_queries / n_targets.  Per query q: q_rank[q] the rank of its id in Python's string order
  * (equal ids, equal ranks), its original length and start position, its id
  * bytes q_id[q_id_off[q] .. q_id_off[q + 1]) and its sequence as given
  * q_seq[q_seq_off[q] ..) (ASCII).  Per target: the same, t_id with the "_RC"
@@ -333,7 +333,8 @@ int pw_score_max_noalloc(int device, const float* matrix, int dim, int char_offs
  * records (each ">target query\n trimmed query \n") and fails with
  * PW_ERR_CAPACITY when out_cap is too small.  An invalid hit location returns
  * PW_ERR_ARG (the reference raises there). */
-int pw_trimmed_fasta(const pw_hit* hits, int64_t n_hits, const int32_t* q_rank, const int64_t* q_orig_len,
+int pw_trimmed_fasta(const pw_hit* hits, int64_t n_hits, int32_t n_queries, int32_t n_targets,
+                     const int32_t* q_rank, const int64_t* q_orig_len,
                      const int64_t* q_start_pos, const char* q_id, const int64_t* q_id_off, const char* q_seq,
                      const int64_t* q_seq_off, const int32_t* t_rank, const int64_t* t_orig_len,
                      const int64_t* t_start_pos, const char* t_id, const int64_t* t_id_off, const double* thresholds,
@@ -344,7 +345,8 @@ int pw_trimmed_fasta(const pw_hit* hits, int64_t n_hits, const int32_t* q_rank, 
  * three alignment strings, each line ending in a newline.  Arguments as
  * pw_trimmed_fasta's, plus strbuf / strbuf_bytes (the pw_get_hits strings)
  * and without the query sequences; t_id holds the target ids as they are. */
-int pw_txt_records(const pw_hit* hits, int64_t n_hits, const char* strbuf, int64_t strbuf_bytes,
+int pw_txt_records(const pw_hit* hits, int64_t n_hits, int32_t n_queries, int32_t n_targets,
+                   const char* strbuf, int64_t strbuf_bytes,
                    const int32_t* q_rank, const int64_t* q_orig_len, const int64_t* q_start_pos, const char* q_id,
                    const int64_t* q_id_off, const int32_t* t_rank, const int64_t* t_orig_len,
                    const int64_t* t_start_pos, const char* t_id, const int64_t* t_id_off, const double* thresholds,

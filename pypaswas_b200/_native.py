@@ -140,9 +140,9 @@ def bind(lib):
         "pw_server_release": (ctypes.c_int, [P, I64]),
         "pw_server_stats": (ctypes.c_int, [P, ctypes.POINTER(PwServerStats)]),
         "pw_server_tune": (ctypes.c_int, [P, ctypes.c_int, I64]),
-        "pw_trimmed_fasta": (ctypes.c_int, [P, I64, P, P, P, P, P, P, P, P, P, P, P, P, P, P, I64,
+        "pw_trimmed_fasta": (ctypes.c_int, [P, I64, I32, I32, P, P, P, P, P, P, P, P, P, P, P, P, P, P, I64,
                                             ctypes.POINTER(I64)]),
-        "pw_txt_records": (ctypes.c_int, [P, I64, P, I64, P, P, P, P, P, P, P, P, P, P, P, P, I64,
+        "pw_txt_records": (ctypes.c_int, [P, I64, I32, I32, P, I64, P, P, P, P, P, P, P, P, P, P, P, P, I64,
                                           ctypes.POINTER(I64)]),
     }
     for name, (res, args) in sig.items():

@@ -109,14 +109,15 @@ struct Rec {
 // target id, score), stable (Formatters.py:34-37).  `real` keeps Python's
 // dict order: a new key goes last, a replaced one keeps its place, a deleted
 // one is gone.
-static int ordered_real_hits(const pw_hit* hits, int64_t n_hits, const int32_t* q_rank, const int64_t* q_orig_len,
-                             const int64_t* q_start_pos, const int32_t* t_rank, const int64_t* t_orig_len,
-                             const int64_t* t_start_pos, const double* thresholds, std::vector<Rec>& rec,
-                             std::vector<int64_t>& order) {
+static int ordered_real_hits(const pw_hit* hits, int64_t n_hits, int32_t n_queries, int32_t n_targets,
+                             const int32_t* q_rank, const int64_t* q_orig_len, const int64_t* q_start_pos,
+                             const int32_t* t_rank, const int64_t* t_orig_len, const int64_t* t_start_pos,
+                             const double* thresholds, std::vector<Rec>& rec, std::vector<int64_t>& order) {
     rec.resize((size_t)n_hits);
     for (int64_t i = 0; i < n_hits; ++i) {
         const pw_hit& h = hits[i];
         const int q = h.query, t = h.target;
+        if (q < 0 || q >= n_queries || t < 0 || t >= n_targets) return PW_ERR_ARG;
         const int64_t s0 = h.s_start + q_start_pos[q], s1 = h.s_end + q_start_pos[q];
         const int64_t t0 = h.t_start + t_start_pos[t], t1 = h.t_end + t_start_pos[t];
         if (!(0 <= s0 && s0 < s1 && s1 < q_orig_len[q] && 0 <= t0 && t0 < t1 && t1 < t_orig_len[t]))
@@ -180,7 +181,8 @@ static int ordered_real_hits(const pw_hit* hits, int64_t n_hits, const int32_t* 
     return PW_OK;
 }
 
-extern "C" int pw_trimmed_fasta(const pw_hit* hits, int64_t n_hits, const int32_t* q_rank, const int64_t* q_orig_len,
+extern "C" int pw_trimmed_fasta(const pw_hit* hits, int64_t n_hits, int32_t n_queries, int32_t n_targets,
+                                const int32_t* q_rank, const int64_t* q_orig_len,
                                 const int64_t* q_start_pos, const char* q_id, const int64_t* q_id_off,
                                 const char* q_seq, const int64_t* q_seq_off, const int32_t* t_rank,
                                 const int64_t* t_orig_len, const int64_t* t_start_pos, const char* t_id,
@@ -193,8 +195,8 @@ extern "C" int pw_trimmed_fasta(const pw_hit* hits, int64_t n_hits, const int32_
         return PW_ERR_ARG;
     std::vector<Rec> rec;
     std::vector<int64_t> order;
-    const int rc = ordered_real_hits(hits, n_hits, q_rank, q_orig_len, q_start_pos, t_rank, t_orig_len, t_start_pos,
-                                     thresholds, rec, order);
+    const int rc = ordered_real_hits(hits, n_hits, n_queries, n_targets, q_rank, q_orig_len, q_start_pos, t_rank,
+                                     t_orig_len, t_start_pos, thresholds, rec, order);
     if (rc != PW_OK) return rc;
     // ">" target id " " query id "\n" query[:t0] query[t1 + 1:] "\n": the
     // query cut by the hit's TARGET coordinates, as Hit.get_trimmed_line does
@@ -291,8 +293,8 @@ static void put_pyfloat(std::string& o, double v) {
 // each record followed by a newline.  Only the record bytes differ from
 // pw_trimmed_fasta's arguments: strbuf holds the hits' strings (pw_get_hits)
 // and t_id the target ids as they are.
-extern "C" int pw_txt_records(const pw_hit* hits, int64_t n_hits, const char* strbuf, int64_t strbuf_bytes,
-                              const int32_t* q_rank, const int64_t* q_orig_len, const int64_t* q_start_pos,
+extern "C" int pw_txt_records(const pw_hit* hits, int64_t n_hits, int32_t n_queries, int32_t n_targets,
+                              const char* strbuf, int64_t strbuf_bytes, const int32_t* q_rank, const int64_t* q_orig_len, const int64_t* q_start_pos,
                               const char* q_id, const int64_t* q_id_off, const int32_t* t_rank,
                               const int64_t* t_orig_len, const int64_t* t_start_pos, const char* t_id,
                               const int64_t* t_id_off, const double* thresholds, char* out, int64_t out_cap,
@@ -306,8 +308,8 @@ extern "C" int pw_txt_records(const pw_hit* hits, int64_t n_hits, const char* st
             return PW_ERR_ARG;
     std::vector<Rec> rec;
     std::vector<int64_t> order;
-    const int rc = ordered_real_hits(hits, n_hits, q_rank, q_orig_len, q_start_pos, t_rank, t_orig_len, t_start_pos,
-                                     thresholds, rec, order);
+    const int rc = ordered_real_hits(hits, n_hits, n_queries, n_targets, q_rank, q_orig_len, q_start_pos, t_rank,
+                                     t_orig_len, t_start_pos, thresholds, rec, order);
     if (rc != PW_OK) return rc;
     std::string o;
     for (int64_t i : order) {

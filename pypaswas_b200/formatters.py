@@ -101,7 +101,7 @@ def txt_records(hits, strbuf, sequences, targets, settings, lib=None):
     q, t, thr, _ = _record_arrays(sequences, targets, settings, False)
     sb = np.frombuffer(bytes(strbuf) or b"\0", dtype=np.uint8)
     vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)
-    head = (vp(hits) if len(hits) else None, len(hits), vp(sb), len(strbuf))
+    head = (vp(hits) if len(hits) else None, len(hits), len(sequences), len(targets), vp(sb), len(strbuf))
     tail = tuple(vp(a) for a in q) + tuple(vp(a) for a in t) + (vp(thr),)
     return _call_twice(lib.pw_txt_records, head, tail)
 
@@ -148,13 +148,14 @@ def trimmed_fasta(hits, sequences, targets, settings, lib=None):
     ptrs = [a.ctypes.data_as(ctypes.c_void_p) for a in arrays]
     n = ctypes.c_int64()
     hp = hits.ctypes.data_as(ctypes.c_void_p) if len(hits) else None
-    rc = lib.pw_trimmed_fasta(hp, len(hits), *ptrs, None, 0, ctypes.byref(n))
+    rc = lib.pw_trimmed_fasta(hp, len(hits), len(sequences), len(targets), *ptrs, None, 0, ctypes.byref(n))
     if rc == _native.PW_ERR_ARG:
         raise CudaException("Invalid hit location in the engine's records")
     if rc != _native.PW_OK:
         raise CudaException("pw_trimmed_fasta failed (%d)" % rc)
     out = np.empty(max(n.value, 1), dtype=np.uint8)
-    rc = lib.pw_trimmed_fasta(hp, len(hits), *ptrs, out.ctypes.data_as(ctypes.c_void_p), n.value, ctypes.byref(n))
+    rc = lib.pw_trimmed_fasta(hp, len(hits), len(sequences), len(targets), *ptrs,
+                              out.ctypes.data_as(ctypes.c_void_p), n.value, ctypes.byref(n))
     if rc != _native.PW_OK:
         raise CudaException("pw_trimmed_fasta failed (%d)" % rc)
     return out[:n.value].tobytes().decode("utf-8")

@@ -118,6 +118,10 @@ def test_native_trimmed_fasta_rejects_an_invalid_location(engine_lib):
     st = cases.Settings(relative_score="0", query_identity="0", query_coverage="0", base_score="0")
     with pytest.raises(CudaException):
         trimmed_fasta(hits, seqs, tgts, st, lib=engine_lib)
+    hits, strbuf, seqs, tgts = _synthetic_trimmer_hits(3, n=20)
+    hits[2]["query"] = len(seqs)  # no such query record
+    with pytest.raises(CudaException):
+        trimmed_fasta(hits, seqs, tgts, st, lib=engine_lib)
 
 
 def test_native_txt_records_match_default_formatter(engine_lib):
