@@ -51,14 +51,29 @@ def _record_arrays(sequences, targets, settings, strip_target_rc):
     import numpy as np
 
     def ranks(ids):
+        # Python's order of the ids: numpy's sort agrees with it for all-str
+        # ids (code points; no NUL, which fixed-width strings would drop) and
+        # for all-int ids; anything else takes sorted()
+        if ids and ((all(type(v) is str for v in ids) and "\0" not in "".join(ids)) or
+                    all(type(v) is int for v in ids)):
+            arr = np.array(ids)
+            if arr.dtype.kind in "Ui" and arr.ndim == 1:
+                return np.unique(arr, return_inverse=True)[1].astype(np.int32).reshape(-1)
         order = {v: k for k, v in enumerate(sorted(set(ids)))}
         return np.array([order[v] for v in ids], dtype=np.int32)
 
     def blob(items):
-        data = [x.encode("utf-8") for x in items]
-        off = np.zeros(len(data) + 1, dtype=np.int64)
-        np.cumsum([len(x) for x in data], out=off[1:])
-        return np.frombuffer(b"".join(data) or b"\0", dtype=np.uint8), off
+        text = "".join(items)
+        if text.isascii():
+            data = text.encode("ascii")
+            lens = np.fromiter(map(len, items), dtype=np.int64, count=len(items))
+        else:
+            enc = [x.encode("utf-8") for x in items]
+            data = b"".join(enc)
+            lens = np.fromiter(map(len, enc), dtype=np.int64, count=len(enc))
+        off = np.zeros(len(items) + 1, dtype=np.int64)
+        np.cumsum(lens, out=off[1:])
+        return np.frombuffer(data or b"\0", dtype=np.uint8), off
 
     qids, tids = [r.id for r in sequences], [r.id for r in targets]
     q = (ranks(qids), np.array([r.original_length for r in sequences], dtype=np.int64),
@@ -72,19 +87,20 @@ def _record_arrays(sequences, targets, settings, strip_target_rc):
     return q, t, thr, blob
 
 
-def _call_twice(fn, head, tail):
-    """Size query, then the write, of a native formatter; returns the text."""
+def _call_twice(fn, head, tail, estimate):
+    """A native formatter into a buffer of `estimate` bytes, once more with
+    the exact size when the estimate was short; returns the text."""
     import ctypes
     import numpy as np
     from . import _native
     n = ctypes.c_int64()
-    rc = fn(*head, *tail, None, 0, ctypes.byref(n))
+    out = np.empty(max(int(estimate), 1), dtype=np.uint8)
+    rc = fn(*head, *tail, out.ctypes.data_as(ctypes.c_void_p), len(out), ctypes.byref(n))
+    if rc == _native.PW_ERR_CAPACITY:
+        out = np.empty(max(n.value, 1), dtype=np.uint8)
+        rc = fn(*head, *tail, out.ctypes.data_as(ctypes.c_void_p), len(out), ctypes.byref(n))
     if rc == _native.PW_ERR_ARG:
         raise CudaException("Invalid hit location in the engine's records")
-    if rc != _native.PW_OK:
-        raise CudaException("native formatter failed (%d)" % rc)
-    out = np.empty(max(n.value, 1), dtype=np.uint8)
-    rc = fn(*head, *tail, out.ctypes.data_as(ctypes.c_void_p), n.value, ctypes.byref(n))
     if rc != _native.PW_OK:
         raise CudaException("native formatter failed (%d)" % rc)
     return out[:n.value].tobytes().decode("utf-8")
@@ -103,7 +119,9 @@ def txt_records(hits, strbuf, sequences, targets, settings, lib=None):
     vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)
     head = (vp(hits) if len(hits) else None, len(hits), len(sequences), len(targets), vp(sb), len(strbuf))
     tail = tuple(vp(a) for a in q) + tuple(vp(a) for a in t) + (vp(thr),)
-    return _call_twice(lib.pw_txt_records, head, tail)
+    longest = lambda blob_off: int(np.diff(blob_off).max()) if len(blob_off) > 1 else 0
+    per = longest(q[4]) + longest(t[4]) + 3 * (int(hits["n_cols"].max()) if len(hits) else 0) + 220
+    return _call_twice(lib.pw_txt_records, head, tail, len(hits) * per)
 
 
 def trimmed_fasta(hits, sequences, targets, settings, lib=None):
@@ -119,46 +137,17 @@ def trimmed_fasta(hits, sequences, targets, settings, lib=None):
     from .exceptions import InvalidOptionException
     lib = lib if lib is not None else _native.load_library()
     hits = np.ascontiguousarray(hits, dtype=_native.HIT_DTYPE)
-
-    def ranks(ids):
-        order = {v: k for k, v in enumerate(sorted(set(ids)))}
-        return np.array([order[v] for v in ids], dtype=np.int32)
-
-    def blob(items):
-        data = [x.encode("utf-8") for x in items]
-        off = np.zeros(len(data) + 1, dtype=np.int64)
-        np.cumsum([len(x) for x in data], out=off[1:])
-        return np.frombuffer(b"".join(data) or b"\0", dtype=np.uint8), off
-
-    qids, tids = [r.id for r in sequences], [r.id for r in targets]
     qseqs = [str(r.seq) for r in sequences]
-    if not all(q.isascii() for q in qseqs):
+    if not "".join(qseqs).isascii():
         raise InvalidOptionException("trimmed_fasta needs ASCII sequences")
-    q_rank, t_rank = ranks(qids), ranks(tids)
-    q_len = np.array([r.original_length for r in sequences], dtype=np.int64)
-    t_len = np.array([r.original_length for r in targets], dtype=np.int64)
-    q_sp = np.array([getattr(r, "start_position", 0) for r in sequences], dtype=np.int64)
-    t_sp = np.array([getattr(r, "start_position", 0) for r in targets], dtype=np.int64)
-    q_id, q_id_off = blob([str(i) for i in qids])
-    t_id, t_id_off = blob([_strip_rc(str(i)) for i in tids])
+    q, t, thr, blob = _record_arrays(sequences, targets, settings, True)
     q_seq, q_seq_off = blob(qseqs)
-    thr = np.array([float(settings.relative_score), float(settings.query_identity),
-                    float(settings.query_coverage), float(settings.base_score)], dtype=np.float64)
-    arrays = (q_rank, q_len, q_sp, q_id, q_id_off, q_seq, q_seq_off, t_rank, t_len, t_sp, t_id, t_id_off, thr)
-    ptrs = [a.ctypes.data_as(ctypes.c_void_p) for a in arrays]
-    n = ctypes.c_int64()
-    hp = hits.ctypes.data_as(ctypes.c_void_p) if len(hits) else None
-    rc = lib.pw_trimmed_fasta(hp, len(hits), len(sequences), len(targets), *ptrs, None, 0, ctypes.byref(n))
-    if rc == _native.PW_ERR_ARG:
-        raise CudaException("Invalid hit location in the engine's records")
-    if rc != _native.PW_OK:
-        raise CudaException("pw_trimmed_fasta failed (%d)" % rc)
-    out = np.empty(max(n.value, 1), dtype=np.uint8)
-    rc = lib.pw_trimmed_fasta(hp, len(hits), len(sequences), len(targets), *ptrs,
-                              out.ctypes.data_as(ctypes.c_void_p), n.value, ctypes.byref(n))
-    if rc != _native.PW_OK:
-        raise CudaException("pw_trimmed_fasta failed (%d)" % rc)
-    return out[:n.value].tobytes().decode("utf-8")
+    vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    head = (vp(hits) if len(hits) else None, len(hits), len(sequences), len(targets))
+    tail = tuple(vp(a) for a in q) + (vp(q_seq), vp(q_seq_off)) + tuple(vp(a) for a in t) + (vp(thr),)
+    longest = lambda blob_off: int(np.diff(blob_off).max()) if len(blob_off) > 1 else 0
+    per = longest(q[4]) + longest(t[4]) + longest(q_seq_off) + 4
+    return _call_twice(lib.pw_trimmed_fasta, head, tail, len(hits) * per)
 
 
 class DefaultFormatter(object):

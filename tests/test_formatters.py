@@ -173,3 +173,16 @@ def test_native_txt_float_repr_over_many_magnitudes(engine_lib):
     expect = "".join(line + "\n" for line in DefaultFormatter(None, hl, None).lines())
     assert len(hl.real_hits) > 100
     assert txt_records(hits, strbuf, seqs, tgts, st, lib=engine_lib) == expect
+
+
+def test_native_formatter_retries_with_the_exact_size(engine_lib, monkeypatch):
+    """A short output estimate costs a second call, not a wrong result."""
+    import cases
+    from pypaswas_b200 import formatters
+    hits, strbuf, seqs, tgts = _synthetic_trimmer_hits(8, n=50)
+    st = cases.Settings(relative_score="0", query_identity="0", query_coverage="0", base_score="0")
+    full = formatters.trimmed_fasta(hits, seqs, tgts, st, lib=engine_lib)
+    real = formatters._call_twice
+    monkeypatch.setattr(formatters, "_call_twice", lambda fn, head, tail, estimate: real(fn, head, tail, 1))
+    assert formatters.trimmed_fasta(hits, seqs, tgts, st, lib=engine_lib) == full
+    assert formatters.txt_records(hits, strbuf, seqs, tgts, st, lib=engine_lib)
