@@ -370,7 +370,7 @@ def main():
     n_pairs = len(w.pairs) if w.pairs is not None else w.n_queries * len(w.targets)
     ms_per_step = t_ms / args.steps
 
-    # roofline of the dominant kernel (integer-ALU bound)
+    # roofline of the dominant kernel (integer-ALU bound: DPX add-max issue rate)
     last = infos[-1]
     trace_ms = sum(i["trace_kernel_ms"] for i in infos)
     score_ms = sum(i["score_kernel_ms"] for i in infos)
