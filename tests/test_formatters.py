@@ -186,3 +186,19 @@ def test_native_formatter_retries_with_the_exact_size(engine_lib, monkeypatch):
     monkeypatch.setattr(formatters, "_call_twice", lambda fn, head, tail, estimate: real(fn, head, tail, 1))
     assert formatters.trimmed_fasta(hits, seqs, tgts, st, lib=engine_lib) == full
     assert formatters.txt_records(hits, strbuf, seqs, tgts, st, lib=engine_lib)
+
+
+def test_native_formatter_id_ranks_follow_python_order():
+    """The id ranks given to the native formatters order ids as Python's
+    sorted() does: mixed case, digits, non-ASCII, prefixes, whitespace, and
+    integer ids."""
+    import cases
+    from pypaswas_b200.formatters import _record_arrays
+    from pypaswas_b200.records import SeqRecord
+    st = cases.Settings(relative_score="0", query_identity="0", query_coverage="0", base_score="0")
+    for ids in (["b", "B", "a10", "a9", "a", "ä", "Z", "a", "é", "ab", "a b", "a\t"],
+                ["r%d" % i for i in (10, 2, 33, 2, 1)], [5, 3, 10, 3, -1]):
+        recs = [SeqRecord("ACGT", i) for i in ids]
+        q, _, _, _ = _record_arrays(recs, recs, st, False)
+        order = {v: k for k, v in enumerate(sorted(set(ids)))}
+        assert q[0].tolist() == [order[v] for v in ids]
