@@ -310,7 +310,8 @@ int pw_server_stats(pw_server* s, pw_server_counters* st);
  * array: the library serialises them with a host lock, and their GPU work must
  * not overlap with other users of it.  The first call on a device looks up the
  * array's device address (make it before any stream capture on that device).
- * Runs on the legacy default stream and returns when pair_max is filled. */
+ * Runs on the legacy default stream and returns when pair_max is filled; the
+ * calling thread's current device is the same on return as on entry. */
 int pw_score_max_noalloc(int device, const float* matrix, int dim, int char_offset, float gap, float ext,
                          int affine, const uint8_t* q_residues, const int64_t* q_offsets, int32_t n_queries,
                          const uint8_t* t_residues, const int64_t* t_offsets, int32_t n_targets, float* pair_max,

@@ -69,6 +69,24 @@ int S_of(int cls) { return cls == 0 ? 16 : (cls == 2 ? 64 : 32); }
 
 size_t align_to(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
+// Makes `device` current for the lifetime of the guard and gives the caller
+// back the device that was current before, on every return path.
+struct DeviceGuard {
+    int previous = -1;
+    bool switched = false;
+    cudaError_t enter(int device) {
+        cudaError_t c = cudaGetDevice(&previous);
+        if (c != cudaSuccess) return c;
+        if (previous == device) return cudaSuccess;
+        c = cudaSetDevice(device);
+        switched = c == cudaSuccess;
+        return c;
+    }
+    ~DeviceGuard() {
+        if (switched) cudaSetDevice(previous);
+    }
+};
+
 // Score-sweep variant: the same per-lane sweep as sweep_kernel's first phase
 // (sweep_score / build_profile), with the work counter and boundary rows in
 // the caller-free scratch array.
@@ -168,7 +186,8 @@ extern "C" int pw_score_max_noalloc(int device, const float* matrix, int dim, in
         return report(err, err_bytes, PW_ERR_ARG, "bad sequence or output arguments");
     if (nq == 0 || nt == 0) return PW_OK;
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (cudaSetDevice(device) != cudaSuccess)
+    DeviceGuard guard;  // the caller's current device is restored on return
+    if (guard.enter(device) != cudaSuccess)
         return report(err, err_bytes, PW_ERR_DEVICE, "cudaSetDevice(%d) failed", device);
     if (!g_scratch_addr[device]) {
         void* p = nullptr;

@@ -1,12 +1,15 @@
 """Output formatters of the aligner and trimmer programs
-(pyPaSWAS/Core/Formatters.py:3-150).
+(pyPaSWAS/Core/Formatters.py:3-186).
 
-Both formatters visit HitList.real_hits sorted by (query id, target id, score)
+Every formatter visits HitList.real_hits sorted by (query id, target id, score)
 (Formatters.py:34-37; a stable sort, so equal keys keep HitList order) and
 produce the reference's text byte for byte:
 
 * DefaultFormatter ("TXT"): one comma-separated summary line per hit followed by
   the three alignment strings (Formatters.py:19-31).
+* SamFormatter ("SAM"): header lines, then Hit.get_sam_line per hit
+  (Formatters.py:51-106, Hit.py:222-272,338-406).
+* FastaFormatter ("FASTA"): the whole query per hit (Formatters.py:152-186).
 * TrimmerFormatter ("trimmedFasta"): one FASTA record per hit, the query with
   the span [target_start, target_end] cut out (Hit.get_trimmed_line,
   pyPaSWAS/Core/Hit.py:274-286, which slices the query by the hit's TARGET
@@ -87,6 +90,26 @@ def _record_arrays(sequences, targets, settings, strip_target_rc):
     return q, t, thr, blob
 
 
+# first output buffer at most this large; a longer text takes the exact-size retry
+_ESTIMATE_CAP = 256 << 20
+
+
+def _per_hit_estimate(hits, q_id_off, t_id_off, body):
+    """Bytes of the records of `hits` if none were filtered out: each hit's
+    own query and target id lengths plus `body` (per hit, or a scalar), capped
+    at _ESTIMATE_CAP."""
+    import numpy as np
+    if len(hits) == 0:
+        return 1
+    q_ids, t_ids = np.diff(q_id_off), np.diff(t_id_off)
+    # indices outside the record lists are rejected by the native call; clip them here
+    qi = np.clip(hits["query"].astype(np.int64), 0, max(len(q_ids) - 1, 0))
+    ti = np.clip(hits["target"].astype(np.int64), 0, max(len(t_ids) - 1, 0))
+    total = int((np.sum(q_ids[qi]) if len(q_ids) else 0) + (np.sum(t_ids[ti]) if len(t_ids) else 0)
+                + np.sum(body))
+    return min(total, _ESTIMATE_CAP)
+
+
 def _call_twice(fn, head, tail, estimate):
     """A native formatter into a buffer of `estimate` bytes, once more with
     the exact size when the estimate was short; returns the text."""
@@ -119,9 +142,9 @@ def txt_records(hits, strbuf, sequences, targets, settings, lib=None):
     vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)
     head = (vp(hits) if len(hits) else None, len(hits), len(sequences), len(targets), vp(sb), len(strbuf))
     tail = tuple(vp(a) for a in q) + tuple(vp(a) for a in t) + (vp(thr),)
-    longest = lambda blob_off: int(np.diff(blob_off).max()) if len(blob_off) > 1 else 0
-    per = longest(q[4]) + longest(t[4]) + 3 * (int(hits["n_cols"].max()) if len(hits) else 0) + 220
-    return _call_twice(lib.pw_txt_records, head, tail, len(hits) * per)
+    # each hit's own record: its two ids, three strings of n_cols and the numbers
+    est = _per_hit_estimate(hits, q[4], t[4], 3 * hits["n_cols"].astype(np.int64) + 220)
+    return _call_twice(lib.pw_txt_records, head, tail, est)
 
 
 def trimmed_fasta(hits, sequences, targets, settings, lib=None):
@@ -145,9 +168,11 @@ def trimmed_fasta(hits, sequences, targets, settings, lib=None):
     vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)
     head = (vp(hits) if len(hits) else None, len(hits), len(sequences), len(targets))
     tail = tuple(vp(a) for a in q) + (vp(q_seq), vp(q_seq_off)) + tuple(vp(a) for a in t) + (vp(thr),)
-    longest = lambda blob_off: int(np.diff(blob_off).max()) if len(blob_off) > 1 else 0
-    per = longest(q[4]) + longest(t[4]) + longest(q_seq_off) + 4
-    return _call_twice(lib.pw_trimmed_fasta, head, tail, len(hits) * per)
+    # each hit's own record: its two ids and its query's residues
+    q_len = np.diff(q_seq_off)
+    qi = np.clip(hits["query"].astype(np.int64), 0, max(len(q_len) - 1, 0))
+    est = _per_hit_estimate(hits, q[4], t[4], q_len[qi] + 4 if len(hits) and len(q_len) else 0)
+    return _call_twice(lib.pw_trimmed_fasta, head, tail, est)
 
 
 class DefaultFormatter(object):
@@ -173,3 +198,53 @@ class TrimmerFormatter(DefaultFormatter):
     """trimmedFasta output (Formatters.py:110-150)."""
 
     record = staticmethod(trimmed_record)
+
+
+def sam_header_and_records(hits):
+    """The @SQ lines (one per target id without its RC suffix, first seen
+    first) and the alignment lines of `hits` in the given order
+    (SamFormatter._format_hit, Formatters.py:67-83).  Hit.get_sam_line
+    reverses an RC hit's alignment strings in place, as the reference does."""
+    sq = {}
+    records = []
+    for h in hits:
+        tid = h.get_target_id()
+        if tid not in sq:
+            sq[tid[:-3] if tid[-2:] == "RC" else tid] = h.get_sam_sq()
+        records.append(h.get_sam_line())
+    return list(sq.values()), records
+
+
+class SamFormatter(DefaultFormatter):
+    """SAM output (Formatters.py:51-106): the @HD line, one @SQ line per
+    target, the @PG line, then one alignment line per hit in the formatter's
+    order (query id, target id, score)."""
+
+    HD = "@HD\tVN:1.4\tSO:unknown"
+    PG = "@PG\tID:0\tPN:paswas\tVN:3.0"
+
+    def lines(self):
+        sq, records = sam_header_and_records(ordered_hits(self.hitlist))
+        return [self.HD] + sq + [self.PG] + records
+
+
+class FastaFormatter(DefaultFormatter):
+    """FASTA output (Formatters.py:152-186, class FASTA): the whole query of
+    every hit, in the formatter's order."""
+
+    @staticmethod
+    def record(hit):
+        return hit.get_full_fasta()
+
+
+FORMATTERS = {"TXT": DefaultFormatter, "SAM": SamFormatter, "TRIMMEDFASTA": TrimmerFormatter,
+              "FASTA": FastaFormatter}
+
+
+def formatter_for(out_format):
+    """Formatter class of an --outputformat value (pypaswasall.py:58-72,150-164)."""
+    from .exceptions import InvalidOptionException
+    key = str(out_format).upper()
+    if key not in FORMATTERS:
+        raise InvalidOptionException("Invalid output format {0}.".format(out_format))
+    return FORMATTERS[key]

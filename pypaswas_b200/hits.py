@@ -4,8 +4,26 @@
 A Hit validates its locations exactly like the reference (start < end, both
 inside the sequence), so a one-column alignment raises CudaException as it does
 there.  HitList keeps the reference's de-duplication by start/end keys.
+
+The output-side methods (get_sam_line, get_sam_sq, get_trimmed_line,
+get_fasta, get_full_fasta, _check_rc) restate Hit.py:159-406 so the
+reference's own formatters (Formatters.py) print these hits unchanged.
 """
 from .exceptions import CudaException
+
+
+def _strip_rc(identifier):
+    """An id without its reverse-complement suffix: ids ending in "RC" lose
+    their last three characters (the "_RC" that Readers.complement_records
+    appends), as every output method of Hit.py does."""
+    return identifier[:-3] if identifier[-2:] == "RC" else identifier
+
+
+def _reverse_complement(seq):
+    """IUPAC reverse complement of a residue string (case kept), the
+    complement the reverse-complement targets are built with."""
+    from .workloads import reverse_complement
+    return reverse_complement(str(seq).encode("latin-1")).decode("latin-1")
 
 
 class Hit(object):
@@ -90,6 +108,121 @@ class Hit(object):
 
     def get_target_id(self):
         return self.target_info.id
+
+    def _check_rc(self):
+        """True when both ids carry the reverse-complement suffix (Hit.py:159-164)."""
+        return self.get_seq_id()[-2:] == "RC" and self.get_target_id()[-2:] == "RC"
+
+    def get_euclidian_distance(self):
+        """The target record's distance, 0.0 when unset (Hit.py:174-179)."""
+        d = getattr(self.target_info, "distance", None)
+        return 0.0 if d is None else d
+
+    def _require_strings(self):
+        if len(self.sequence_match) == 0 or len(self.target_match) == 0 or len(self.alignment) == 0:
+            raise CudaException("sequence_match, target_match and alignment should be set and have lengths > 0.")
+
+    # ---------------------------------------------------------------- SAM
+    def get_sam_line(self):
+        """One SAM alignment line (Hit.py:222-272): QNAME and RNAME without the
+        RC suffix, FLAG 16 on an RC id, POS 1-based on the target, MAPQ 255,
+        the extended CIGAR, SEQ the query (reverse-complemented on RC), then
+        the AS/RS/BS/QC/QI fields.  On an RC hit the alignment and query match
+        strings are reversed in place, as the reference does, before the CIGAR
+        is read from them."""
+        query_id, target_id = self.get_seq_id(), self.get_target_id()
+        self.rc = query_id[-2:] == "RC" or target_id[-2:] == "RC"
+        pos = self.target_location[0] + 1
+        sam_seq = str(self.sequence_info.seq)
+        if self.rc:
+            self.alignment = self.alignment[::-1]
+            self.sequence_match = self.sequence_match[::-1]
+            sam_seq = _reverse_complement(sam_seq)
+            pos = self.target_info.original_length - self.target_location[1]
+        self._require_strings()
+        fields = (_strip_rc(query_id), self._get_sam_flag(), _strip_rc(target_id), str(pos), Hit._get_sam_mapq(),
+                  self._get_sam_cigar(), "*", "0", "0", sam_seq, "*", self._get_sam_alignment_score(),
+                  self._get_sam_relative_score(), self._get_sam_relative_base_score(),
+                  self._get_sam_query_coverage(), self._get_sam_query_identity())
+        return "\t".join(fields)
+
+    def get_sam_sq(self):
+        """The @SQ header line of the hit's target (Hit.py:298-304)."""
+        return "\t".join(("@SQ", "SN:{0}".format(_strip_rc(self.get_target_id())),
+                          "LN:{0}".format(self.target_info.original_length)))
+
+    def _get_sam_alignment_score(self):
+        return "AS:i:" + str(int(self.score))
+
+    def _get_sam_flag(self):
+        rc = self.get_seq_id()[-2:] == "RC" or self.get_target_id()[-2:] == "RC"
+        return "16" if rc else "0"
+
+    @staticmethod
+    def _get_sam_mapq():
+        return "255"
+
+    def _get_sam_cigar(self):
+        """Extended CIGAR (Hit.py:338-372): soft clips for the query outside
+        the alignment (mirrored on RC hits), then one run per maximal stretch
+        of equal alignment characters, named by the last column of the run."""
+        parts = []
+        if self.rc:
+            parts.append(str(len(self.sequence_info.seq) - self.seq_location[1] - 1) + "S")
+        elif self.seq_location[0] > 0:
+            parts.append(str(self.seq_location[0]) + "S")
+        aln = self.alignment
+        run_start = 0
+        for i in range(1, len(aln)):
+            if aln[i] != aln[run_start]:
+                parts.append(str(i - run_start) + self._get_cigar_char(i - 1))
+                run_start = i
+        parts.append(str(len(aln) - run_start) + self._get_cigar_char(len(aln) - 1))
+        tail = self.seq_location[0] if self.rc else self.sequence_info.original_length - self.seq_location[1] - 1
+        if tail > 0:
+            parts.append(str(tail) + "S")
+        return "".join(parts)
+
+    def _get_sam_relative_score(self):
+        return "RS:f:" + str(self.relative_score)
+
+    def _get_sam_query_coverage(self):
+        return "QC:f:" + str(self.query_coverage)
+
+    def _get_sam_query_identity(self):
+        return "QI:f:" + str(self.query_identity)
+
+    def _get_sam_relative_base_score(self):
+        return "BS:f:" + str(self.base_score)
+
+    def _get_cigar_char(self, position):
+        """'=' for a match column, 'X' for a mismatch, 'D' for a gap in the
+        query, 'I' for a gap in the target (Hit.py:392-406)."""
+        c = self.alignment[position]
+        if c == "|":
+            return "="
+        if c == ".":
+            return "X"
+        return "D" if self.sequence_match[position] == "-" else "I"
+
+    # ------------------------------------------------------------- FASTA
+    def get_trimmed_line(self):
+        """trimmedFasta record (Hit.py:274-286): the query with the span
+        [target_start, target_end] cut out -- the reference slices the QUERY
+        by the TARGET coordinates, and that is kept."""
+        self._require_strings()
+        seq = self.sequence_info.seq
+        t0, t1 = self.target_location
+        return "".join((">", _strip_rc(self.get_target_id()), " ", self.sequence_info.id, "\n",
+                        str(seq[:t0] + seq[t1 + 1:])))
+
+    def get_fasta(self):
+        """Same record as get_trimmed_line (Hit.py:289-301)."""
+        return self.get_trimmed_line()
+
+    def get_full_fasta(self):
+        """The whole query as a FASTA record (Hit.py:303-305)."""
+        return ">{}\n{}".format(self.get_seq_id(), str(self.sequence_info.seq))
 
     def keys(self):
         """De-duplication keys: start and end positions per id pair (Hit.py:151-158)."""

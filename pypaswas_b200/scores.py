@@ -119,26 +119,60 @@ class Score(object):
 
     # ------------------------------------------------------------ engine view
     def matrix_array(self):
-        """float32 [dim, dim] matrix; string entries are parsed like the C
-        compiler parses the reference's generated source."""
-        return np.array([[float(v) for v in row] for row in self.matrix], dtype=np.float32)
+        return matrix_array(self)
 
     def char_offset_code(self):
-        return ord(self.char_offset)
-
-    @staticmethod
-    def _compiled_float(value):
-        """A Python float formatted with str() and read back as a C float
-        literal, which is how the reference bakes constants into its kernels
-        (PaSWAS.py:64-72)."""
-        return np.float32(float(str(value)))
+        return char_offset_code(self)
 
     def kernel_constants(self):
-        """(gap, ext, affine, lower_limit, minimum_score) as the kernel sees them."""
-        gap = self._compiled_float(self.gap_score if self.gap_score is not None else 0.0)
-        ext = self._compiled_float(self.gap_extension if self.gap_extension is not None else 0.0)
-        return (gap, ext, self.gap_extension is not None, self._compiled_float(self.lower_limit_score),
-                self._compiled_float(self.minimum_score))
+        return kernel_constants(self)
+
+
+# ---------------------------------------------------------------------------
+# The engine's view of a scoring model, read from the public attributes that
+# every Score of the reference has (Scores.py:9-98): matrix, dimensions,
+# char_offset, gap_score, gap_extension, lower_limit_score, minimum_score and
+# highest_score.  They accept this module's Score classes and the reference's
+# own pyPaSWAS.Core.Scores objects alike, so the driver can be handed either.
+
+def _compiled_float(value):
+    """A Python value formatted with str() and read back as a C float literal,
+    which is how the reference bakes constants into its kernels
+    (PaSWAS.py:64-72 substitutes str(value) into default_score.cu)."""
+    return np.float32(float(str(value)))
+
+
+def matrix_array(score):
+    """float32 [dim, dim] substitution matrix, rows and columns 0..dim-1 as
+    Score.__str__ emits them (Scores.py:87-98).  The generated source holds
+    each entry as a double literal in a float array, so the value is the
+    decimal read as a double and rounded to float -- what float() followed by
+    the float32 conversion does, for numbers and for the IRYS model's string
+    entries alike."""
+    dim = int(score.dimensions)
+    m = score.matrix
+    return np.array([[float(v) for v in row[:dim]] for row in m[:dim]], dtype=np.float32)
+
+
+def char_offset_code(score):
+    """Residue code of matrix row 0 (``CHAR_OFFSET``, default_variable.cu)."""
+    return ord(score.char_offset)
+
+
+def kernel_constants(score):
+    """(gap, ext, affine, lower_limit, minimum_score) as the kernel sees them:
+    an unset gap extension selects the linear kernel and compiles as 0.0
+    (PaSWAS.py:58-61, SmithWaterman.py:149)."""
+    gap = _compiled_float(score.gap_score if score.gap_score is not None else 0.0)
+    ext = _compiled_float(score.gap_extension if score.gap_extension is not None else 0.0)
+    return (gap, ext, score.gap_extension is not None, _compiled_float(score.lower_limit_score),
+            _compiled_float(score.minimum_score))
+
+
+def highest_score(score):
+    """``highest_score`` as a float (the per-pair bound of
+    SmithWatermanCuda._set_max_possible_score multiplies it as a float)."""
+    return float(score.highest_score)
 
 
 class BasicScore(Score):

@@ -26,7 +26,7 @@ import time
 
 import numpy as np
 
-from . import _native
+from . import _native, scores
 from .exceptions import InvalidOptionException
 from .hits import Hit, HitList
 
@@ -40,10 +40,13 @@ def id_keys(query_ids, target_ids):
 
 
 def configure_engine(engine, score, settings):
-    """Scoring model and thresholds as the reference's kernels see them."""
-    gap, ext, affine, ll, mn = score.kernel_constants()
-    engine.set_scoring(score.matrix_array(), score.char_offset_code(), gap, ext, affine, ll, mn,
-                       float(settings.minimum_score), float(score.highest_score), float(_filter_factor(settings)))
+    """Scoring model and thresholds as the reference's kernels see them.
+    `score` is any scoring model with the reference Score's public attributes:
+    one of pypaswas_b200.scores, or the reference's own pyPaSWAS.Core.Scores
+    object that pypaswasall.py:126-144 builds."""
+    gap, ext, affine, ll, mn = scores.kernel_constants(score)
+    engine.set_scoring(scores.matrix_array(score), scores.char_offset_code(score), gap, ext, affine, ll, mn,
+                       float(settings.minimum_score), scores.highest_score(score), float(_filter_factor(settings)))
 
 
 def _filter_factor(settings):

@@ -15,7 +15,8 @@ oracle/ref/ref_driver.py for the stand-ins it needs (Bio.Seq, pycuda, NumPy 2).
 A fixture records the inputs exactly as the program received them (after the
 CLI's reverse-complement and length sort), the settings, the scoring matrix and
 highest_score the reference built, and its results: the HitList in insertion
-order, the TXT formatter line of every hit, and the raw device results of each
+order, the TXT formatter line of every hit, the trimmedFasta lines, the whole
+FASTA and SAM files the reference's formatters write, and the raw device results of each
 batch (pair maxima, starting points in emission order).  The test-suite uses
 them to pin the oracle and the engine; nothing at test time reads the
 reference tree.
@@ -86,6 +87,16 @@ def trimmed_lines(hitlist):
     return [h.get_trimmed_line() for h in f._get_hits()]
 
 
+def formatter_text(cls, hitlist):
+    """The whole file a reference formatter's print_results writes."""
+    import tempfile
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "out")
+        cls(LOG, hitlist, path).print_results()
+        with open(path) as f:
+            return f.read()
+
+
 def run_case(name, queries, targets, settings, dna, program="aligner", device_memory=8 << 30):
     q, t = prepare(queries, targets, dna)
     st = R.Settings(**settings)
@@ -103,6 +114,9 @@ def run_case(name, queries, targets, settings, dna, program="aligner", device_me
     out["hits"] = [hit_record(h) for h in hl.real_hits.values()]
     out["txt"] = txt_lines(hl)
     out["trimmed"] = trimmed_lines(hl)
+    out["fasta_text"] = formatter_text(R.Formatters.FASTA, hl)
+    # last: get_sam_line reverses the alignment strings of RC hits in place
+    out["sam_text"] = formatter_text(R.Formatters.SamFormatter, hl)
     out["batches"] = []
     for b in sw.raw_batches:
         out["batches"].append({"X": b["X"], "Y": b["Y"], "n_seq": b["n_seq"], "n_tgt": b["n_tgt"],

@@ -68,6 +68,23 @@ def test_no_alloc_matches_regular_entry_point_twice(engine_lib):
     np.testing.assert_array_equal(_no_alloc_pair_max(engine_lib, q1, t1, s1), want1)
 
 
+def test_no_alloc_call_takes_no_device_memory(engine_lib):
+    # the property the entry point exists for: after a first call (which loads
+    # the library's kernels and its fixed array), further calls leave the
+    # device's free memory exactly where it was
+    import torch
+    q, t, s, _ = _workload(303, "dna", 70, 30, (5, 160), (1, 200))
+    first = _no_alloc_pair_max(engine_lib, q, t, s)
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info(0)[0]
+    again = [_no_alloc_pair_max(engine_lib, q, t, s) for _ in range(3)]
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info(0)[0] == free_before
+    for a in again:
+        np.testing.assert_array_equal(a, first)
+    assert torch.cuda.current_device() == 0
+
+
 def test_no_alloc_rejects_inputs_beyond_its_limit(engine_lib):
     # 4096 x 4096 pair maxima alone need 64 MiB of results: over the limit
     q = ["ACGT"] * 4096
