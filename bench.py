@@ -1,22 +1,39 @@
 #!/usr/bin/env python
 """GCUPS of the Smith-Waterman hot path on B200.
 
-Workload (the configuration the metric is quoted on): protein, affine gap,
-batched uneven lengths -- 200 queries (log-normal, median 350 aa, 100-1000)
-against 2,000 targets (50-2,000 aa), BLOSUM62, gap open -11 / extension -1,
-10% of pairs sharing a planted 150-aa domain at 40% identity: 400,000 pairs,
-all-vs-all, full path (score sweep, starting points, traceback walk, hits).
-Synthetic, seeded (pypaswas_b200.workloads.config2).
+Headline workload (the configuration the metric is quoted on): protein, affine
+gap, batched uneven lengths -- 200 queries (log-normal, median 350 aa,
+100-1000) against 2,000 targets (50-2,000 aa), BLOSUM62, gap open -11 /
+extension -1, 10% of pairs sharing a planted 150-aa domain at 40% identity:
+400,000 pairs, all-vs-all, full path (score sweep, starting points, traceback
+walk, hits).  Synthetic, seeded (pypaswas_b200.workloads.config2).
 
-One "step" = one pw_align over all 400,000 pairs with the sequences resident
-in HBM.  `e2e` repeats the step through the public driver
-(SmithWatermanB200.align_sequences) from host sequence records, host<->device
-copies and Hit construction included.
+The same JSON line carries one record per further configuration under
+"configs": DNA reads x adapters (C1), long DNA pairs (C3) and the trimmer's
+10 M reads (C4), each with the same legs.
+
+Legs of every configuration:
+  value     one step = one pw_align over the whole workload, sequences
+            resident in HBM, the score sweep's work list rebuilt every step
+            (PW_FLAG_REPLAN); CUDA events around each step, L2 flushed between
+            steps
+  e2e       the same metric through the public driver API with host records:
+            Aligner.process -> HitList (Trimmer.trimmed_fasta -> text for the
+            trimmer), inputs alternating between two seeded sets of the same
+            shape so that every step copies and prepares its inputs anew; the
+            bytes are the engine's own count of its host<->device copies
+  plain     the unbatched form (one pair per launch) against the batched
+            engine on the same sample
+  parity    the engine against the oracle on the CPU baseline's sample
+  roofline  the dominant kernel's algorithmic ops per second against the DPX
+            issue peak measured in the same run
+  cpu_baseline  the oracle on one host core over a bounded sample
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Under torchrun (N > 1) every rank aligns its own replica of the workload
-(pairs are independent; no collective on the data path): weak scaling.
+Under torchrun (N > 1) every rank aligns its own replica of the headline
+workload (pairs are independent; no collective on the data path): weak
+scaling; the further configurations and the serving leg run at N = 1 only.
 """
 import argparse
 import json
@@ -33,11 +50,10 @@ import numpy as np  # noqa: E402
 
 # algorithmic operations per cell (add and max counted separately) of the
 # recurrences: linear/affine, score only / with direction classification
-# the trimmer workload's end-to-end leg builds Python Hit objects: it runs on
-# the first reads only (the bench line names the sample)
-E2E_READS = 200_000
-
 OPS_PER_CELL = {("linear", "score"): 5, ("linear", "dirs"): 8, ("affine", "score"): 10, ("affine", "dirs"): 14}
+# the trimmer workload's end-to-end leg aligns this many reads per step
+E2E_READS = 200_000
+NAMES = {1: "C1", 2: "C2", 3: "C3", 4: "C4"}
 
 
 def parse():
@@ -47,35 +63,42 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", type=int, choices=[1, 2, 3, 4], default=2,
-                    help="workload: 1 DNA reads x adapters, 2 protein batched (the metric's configuration), "
-                         "3 long DNA pairs, 4 trimmer reads x adapters")
+                    help="headline workload: 1 DNA reads x adapters, 2 protein batched (the metric's "
+                         "configuration), 3 long DNA pairs, 4 trimmer reads x adapters")
+    ap.add_argument("--also", default="auto",
+                    help="further configurations in the same line, e.g. 1,3,4; 'auto' = the other three when the "
+                         "headline is config 2, 'none' = headline only")
     ap.add_argument("--reads", type=int, default=10_000_000, help="config 4: number of reads")
-    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU baseline sample")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="length of the headline's CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--targets", type=int, default=0,
-                    help="use only every k-th target so that N targets remain (small cases for ncu captures; "
-                         "the bench line then names the reduced workload)")
+                    help="config 2: use only every k-th target so that N targets remain (small cases for ncu "
+                         "captures; the bench line then names the reduced workload)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (ncu captures)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain one-pair-per-launch leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
     ap.add_argument("--no-chain", action="store_true", help="16-bit sweep without chained strips (comparison)")
+    ap.add_argument("--plan-cached", action="store_true",
+                    help="keep the score sweep's work list between steps (inputs unchanged)")
     ap.add_argument("--tune", action="append", default=[], metavar="KEY=VALUE",
-                    help="engine tuning knob (chain_min, grid_share), e.g. --tune chain_min=250; "
-                         "without chain_min the autotuner picks it during the warm-up")
+                    help="engine tuning knob (chain_min, grid_share, segment, dual, cand_slot), e.g. "
+                         "--tune chain_min=250; without chain_min the autotuner picks it during the warm-up")
     ap.add_argument("--serve-seconds", type=float, default=6.0, help="length of each arrival stream of the serving leg")
     ap.add_argument("--serve-loads", default="0.3,0.5,0.6,0.7", help="offered loads (fractions of batched peak) swept")
     return ap.parse_args()
 
 
-def workload(args):
+def workload(cfg, args, seed=None):
+    """The configuration's workload; `seed` draws another set of the same shape."""
     from pypaswas_b200 import workloads
-    if args.config == 1:
-        return workloads.config1()
-    if args.config == 3:
-        return workloads.config3()
-    if args.config == 4:
-        return workloads.config4(n_reads=args.reads)
-    w = workloads.config2()
+    kw = {} if seed is None else {"seed": seed}
+    if cfg == 1:
+        return workloads.config1(**kw)
+    if cfg == 3:
+        return workloads.config3(**kw)
+    if cfg == 4:
+        return workloads.config4(n_reads=args.reads, **kw)
+    w = workloads.config2(**kw)
     if args.targets and args.targets < len(w.targets):
         step = len(w.targets) // args.targets
         w = workloads.Workload("%s, sample: every %d-th target (%d targets)" % (w.name, step, args.targets),
@@ -118,6 +141,7 @@ class ClockSampler(object):
         self.proc = None
         self.lines = []
         self.t0 = 0.0
+        self.t1 = None
 
     def start(self):
         try:
@@ -136,19 +160,17 @@ class ClockSampler(object):
     def mark(self):
         """Start of the timed region: later samples only."""
         self.t0 = time.time()
+        self.t1 = None
 
-    def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
+    def mark_end(self):
+        """End of the timed region: samples after it are not counted."""
+        self.t1 = time.time()
+
+    def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ts, ln in self.lines:
-            if ts < self.t0:
+        for ts, ln in list(self.lines):
+            if ts < self.t0 or (self.t1 is not None and ts > self.t1):
                 continue
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
@@ -161,8 +183,18 @@ class ClockSampler(object):
             for name, val in zip(names, parts[5:9]):
                 if val.lower() == "active":
                     reasons.add(name)
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
                 "samples": len(sm)}
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
 
 
 def load_peaks():
@@ -174,7 +206,7 @@ def load_peaks():
 
 
 def load_traffic():
-    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+    """DRAM bytes per launch of dominant kernels from the committed ncu summaries."""
     try:
         with open(os.path.join(REPO, "profiles", "traffic.json")) as f:
             return json.load(f)
@@ -182,86 +214,204 @@ def load_traffic():
         return {}
 
 
-def engine_for(workload, device):
+def engine_for(w, device):
     from pypaswas_b200 import _native, scores
     from pypaswas_b200.smith_waterman import configure_engine, id_keys
-    score = scores.make_score(workload.settings)
+    score = scores.make_score(w.settings)
     e = _native.Engine(device)
-    configure_engine(e, score, workload.settings)
-    if workload.queries is None:  # packed reads (trimmer workload): read ids never equal target ids
-        n, L = workload.reads.shape
-        e.set_queries_packed(workload.reads, np.arange(n + 1, dtype=np.int64) * L, np.arange(n, dtype=np.int32))
-        e.set_targets([s for _, s in workload.targets], np.arange(len(workload.targets), dtype=np.int32) + n)
+    configure_engine(e, score, w.settings)
+    if w.queries is None:  # packed reads (trimmer workload): read ids never equal target ids
+        n, L = w.reads.shape
+        e.set_queries_packed(w.reads, np.arange(n + 1, dtype=np.int64) * L, np.arange(n, dtype=np.int32))
+        e.set_targets([s for _, s in w.targets], np.arange(len(w.targets), dtype=np.int32) + n)
     else:
-        qk, tk = id_keys([i for i, _ in workload.queries], [i for i, _ in workload.targets])
-        e.set_queries([s for _, s in workload.queries], qk)
-        e.set_targets([s for _, s in workload.targets], tk)
-    if workload.pairs is not None:
-        e.set_pairs([p[0] for p in workload.pairs], [p[1] for p in workload.pairs])
+        qk, tk = id_keys([i for i, _ in w.queries], [i for i, _ in w.targets])
+        e.set_queries([s for _, s in w.queries], qk)
+        e.set_targets([s for _, s in w.targets], tk)
+    if w.pairs is not None:
+        e.set_pairs([p[0] for p in w.pairs], [p[1] for p in w.pairs])
     return e, score
 
 
-def cpu_baseline(workload, score, seconds, processes=1):
-    """The oracle (CPU restatement of the reference path) on a bounded sample of
-    the workload: queries x targets taken evenly from the length-sorted lists
-    (or, with explicit pairs, the first pairs).  The sample is sized for about
-    `seconds` of work: a first run at an estimated rate calibrates a second,
-    larger one if the first was much shorter."""
-    rate = 24e6 * max(1, processes)  # cells/s first estimate of the oracle
-    r = None
-    for _ in range(3):
-        r = _cpu_sample(workload, score, seconds * rate, processes)
-        if r["seconds"] >= 0.4 * seconds or r["full"]:
-            break
-        rate = r["cells"] / max(r["seconds"], 1e-3)
-    return {k: v for k, v in r.items() if k not in ("cells", "full")}
+def _mode(score):
+    return "affine" if score.gap_extension is not None else "linear"
 
 
-def _cpu_sample(workload, score, budget_cells, processes):
-    import multiprocessing as mp
-    sys.path.insert(0, os.path.join(REPO, "oracle"))
-    import oracle
-    oracle.build()
-    q_all = [s.decode() for _, s in workload.queries]
-    t_all = [s.decode() for _, s in workload.targets]
-    args = _oracle_args(score, workload.settings)
-    if workload.pairs is not None:
-        jobs, cells = [], 0
-        for qi, ti in workload.pairs:
-            if cells and cells + len(q_all[qi]) * len(t_all[ti]) > budget_cells:
-                break
-            jobs.append((args, [q_all[qi]], [t_all[ti]]))
-            cells += len(q_all[qi]) * len(t_all[ti])
-        full = len(jobs) == len(workload.pairs)
-        sample = "the first %d explicit pairs (%d cells) of the same workload, full path" % (len(jobs), cells)
+# ------------------------------------------------------------------ device step
+def device_steps(e, steps, warmup, replan, chain, flush, sampler=None, world=1):
+    """`steps` timed pw_align calls after `warmup` untimed ones: CUDA events
+    around each call (which returns when its device work is done), L2 flushed
+    before each.  Returns (per-step ms, per-step run infos)."""
+    import torch
+    for _ in range(warmup):
+        e.align(chain=chain, replan=replan)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    if sampler is not None:
+        sampler.mark()
+    times, infos = [], []
+    for _ in range(steps):
+        flush.zero_()  # between timed iterations: L2 flushed
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        info = e.align(chain=chain, replan=replan)
+        b.record()
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b))
+        infos.append(info.as_dict())
+    if sampler is not None:
+        sampler.mark_end()
+    return times, infos
+
+
+def roofline(e, w, score, infos, steps):
+    """The dominant kernel (score or direction sweep) against the DPX issue
+    peak measured now: algorithmic ops / its summed launch time."""
+    mode = _mode(score)
+    last = infos[-1]
+    trace_ms = sum(i["trace_kernel_ms"] for i in infos)
+    score_ms = sum(i["score_kernel_ms"] for i in infos)
+    sixteen = last["score_path"] == 0 and last["overflow_pairs"] == 0 and last["score_launches"] > 0
+    if trace_ms >= score_ms:
+        wp, tp = last["warp_pairs"], last["traced_pairs"]
+        which = "band_kernel, one pair per warp" if wp >= tp else (
+            "sweep_kernel phase 2" if wp == 0 else "sweep_kernel phase 2 + band_kernel")
+        dom, dom_ms, launches = "direction sweep (%s)" % which, trace_ms, sum(i["trace_launches"] for i in infos)
+        ops = sum(i["traced_cells"] for i in infos) * OPS_PER_CELL[(mode, "dirs")]
+        per_cell = OPS_PER_CELL[(mode, "dirs")]
+        lanes16 = False
     else:
-        # targets first (up to all of them) against 10 queries, then more queries
-        nq = min(len(q_all), 10)
-        q10 = sum(map(len, q_all[::max(1, len(q_all) // nq)][:nq]))
-        t_avg = sum(map(len, t_all)) / max(1, len(t_all))
-        nt = min(len(t_all), max(1, int(budget_cells / (q10 * t_avg))))
-        ts = t_all[::max(1, len(t_all) // nt)][:nt]
-        q_avg = sum(map(len, q_all)) / max(1, len(q_all))
-        nq = min(len(q_all), max(nq, int(budget_cells / (q_avg * sum(map(len, ts))))))
-        qs = q_all[::max(1, len(q_all) // nq)][:nq]
-        cells = sum(map(len, qs)) * sum(map(len, ts))
-        jobs = [(args, qs, ts[i::processes]) for i in range(max(1, processes))]
-        jobs = [j for j in jobs if j[2]]
-        full = len(qs) == len(q_all) and len(ts) == len(t_all)
-        sample = "%d queries x %d targets (%d cells) of the same workload, full path" % (len(qs), len(ts), cells)
-    t0 = time.time()
-    if processes <= 1:
-        for j in jobs:
-            _oracle_chunk(j)
+        dom = {0: "score sweep (score16_chain_kernel / score16_kernel, 16x2 lanes)",
+               1: "score sweep (sweep_kernel phase 1, 32-bit lanes)",
+               2: "score sweep (band_kernel, bands chained across warps)"}.get(last["score_path"], "score sweep")
+        dom_ms, launches = score_ms, sum(i["score_launches"] for i in infos)
+        ops = w.cells * OPS_PER_CELL[(mode, "score")] * steps
+        per_cell = OPS_PER_CELL[(mode, "score")]
+        lanes16 = sixteen
+    peak32, peak16, _ = e.measure_int_peak()
+    peak = peak16 if lanes16 else peak32
+    achieved = ops / (dom_ms * 1e-3) / 1e12
+    return {"bound": "int_alu", "kernel": dom, "achieved": achieved, "peak": peak / 1e12, "unit": "Tops/s",
+            "frac": achieved / (peak / 1e12),
+            "peak_source": "measured in this run: DPX add-max issue probe (pw_measure_int_peak), "
+                           + ("16x2 form" if lanes16 else "32-bit form"),
+            "ops_per_cell": per_cell, "launches": launches, "avg_launch_ms": dom_ms / max(1, launches)}
+
+
+# ------------------------------------------------------------------ end to end
+def _records(w):
+    from pypaswas_b200.records import SeqRecord
+    if w.queries is None:
+        qs = [SeqRecord(w.reads[i].tobytes(), w.read_ids[i]) for i in range(len(w.read_ids))]
     else:
-        ctx = mp.get_context("spawn")
-        with ctx.Pool(processes) as pool:
-            pool.map(_oracle_chunk, jobs)
-    dt = time.time() - t0
-    return {"value": cells / dt / 1e9, "unit": "GCUPS", "cores": processes, "kind": "port", "sample": sample,
-            "seconds": dt, "cells": cells, "full": full}
+        qs = [SeqRecord(s, i) for i, s in w.queries]
+    return qs, [SeqRecord(s, i) for i, s in w.targets]
 
 
+def _e2e_calls(w):
+    """(queries, targets) per public-API call: one call for all-vs-all; with
+    explicit pairs one call per query against its targets, as the reference
+    is run once per pair file."""
+    qs, ts = _records(w)
+    if w.pairs is None:
+        return [(qs, ts)]
+    per_q = {}
+    for qi, ti in w.pairs:
+        per_q.setdefault(qi, []).append(ts[ti])
+    return [([qs[qi]], t) for qi, t in sorted(per_q.items())]
+
+
+def e2e_leg(ws, steps, device, trimmer):
+    """The public driver API with host records; step k runs input set
+    ws[k % len(ws)] (two sets: every step's inputs are new to the engine).
+    Returns (GCUPS, seconds, h2d bytes per step, d2h bytes per step, reuse bits seen)."""
+    import torch
+    from pypaswas_b200.programs import Aligner, Trimmer
+    sets = [(_e2e_calls(w), w.cells) for w in ws]
+    prog = (Trimmer if trimmer else Aligner)(None, None, ws[0].settings, device=device)
+    sw = prog.smith_waterman
+
+    def step(calls):
+        h2d = d2h = 0
+        reuse = 0
+        for qs, ts in calls:
+            if trimmer:
+                prog.trimmed_fasta(qs, ts)  # the program's output text, natively (Trimmer.trimmed_fasta)
+            else:
+                prog.process(qs, ts, None)  # HitList of Hit objects
+            h2d += sw.last_h2d_bytes
+            d2h += sw.last_d2h_bytes
+            reuse |= int(sw.last_info.reuse)
+        return h2d, d2h, reuse
+
+    try:
+        for k in range(2):
+            step(sets[k % len(sets)][0])  # warm-up
+        torch.cuda.synchronize()
+        h2d = d2h = reuse = 0
+        cells = 0
+        t0 = time.perf_counter()
+        for k in range(steps):
+            calls, c = sets[k % len(sets)]
+            a, b, r = step(calls)
+            h2d += a
+            d2h += b
+            reuse |= r
+            cells += c
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+    finally:
+        sw.close()
+    return cells, dt, h2d // steps, d2h // steps, reuse
+
+
+# ------------------------------------------------------------------ plain form
+def plain_leg(w, device, n_q, n_t):
+    """GCUPS of the plain form -- one (query, target) pair per launch, the
+    shape of the reference's per-pair kernel calls -- against the batched
+    engine on the same sample; both the full path (score, starting points,
+    walk).  Explicit pairs: the first n_q queries' pairs."""
+    import torch
+    from pypaswas_b200 import workloads
+    if w.pairs is not None:
+        sample = w.head(n_q)
+        desc = "%d explicit pairs (%d cells)" % (len(sample.pairs), sample.cells)
+    else:
+        qs = w.queries[::max(1, len(w.queries) // n_q)][:n_q]
+        ts = w.targets[::max(1, len(w.targets) // n_t)][:n_t]
+        sample = workloads.Workload(w.name + " sample", qs, ts, w.settings)
+        desc = "%d queries x %d targets (%d pairs, %d cells), evenly spaced in length order" % (
+            len(qs), len(ts), len(qs) * len(ts), sample.cells)
+    e, _ = engine_for(sample, device)
+    out = {}
+    try:
+        for label, plain in (("batched", False), ("plain", True)):
+            e.align(plain=plain)  # warm-up
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            info = e.align(plain=plain)
+            b.record()
+            torch.cuda.synchronize()
+            ms = a.elapsed_time(b)
+            pm = e.pair_max()
+            hits, sb = e.hits()
+            out[label] = {"value": sample.cells / (ms * 1e-3) / 1e9, "ms": ms, "launches": int(info.kernel_launches),
+                          "hits": hits, "sb": sb, "pm": pm, "score_path": int(info.score_path)}
+    finally:
+        e.close()
+    p, bt = out["plain"], out["batched"]
+    return {"value": p["value"], "unit": "GCUPS", "sample": desc, "launches": p["launches"],
+            "score_path": p["score_path"], "batched_same_sample": bt["value"],
+            "batched_over_plain": bt["value"] / p["value"],
+            "hits_equal": bool(np.array_equal(p["hits"], bt["hits"]) and p["sb"] == bt["sb"]),
+            "pair_max_equal": bool(np.array_equal(p["pm"], bt["pm"]))}
+
+
+# ------------------------------------------------------------------ CPU oracle
 def _oracle_args(score, settings):
     gap, ext, affine, ll, mn = score.kernel_constants()
     return (score.matrix_array(), score.char_offset_code(), float(gap), float(ext), bool(affine), float(ll),
@@ -269,220 +419,131 @@ def _oracle_args(score, settings):
 
 
 def _oracle_chunk(job):
+    """The oracle's full path on queries x targets: (pair maxima, hits)."""
     args, qs, ts = job
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle
     m, off, gap, ext, affine, ll, mn, hi, ff, host_min = args
     p = oracle.OracleParams(m, off, gap, ext, affine, ll, mn)
     pos = np.array([[np.float32(hi * min(len(q), len(t)) * ff) for q in qs] for t in ts], np.float32)
-    return len(oracle.run(p, qs, ts, pos, host_min)["hits"])
+    o = oracle.run(p, qs, ts, pos, host_min)
+    return o["pair_max"], o["hits"]
 
 
-def run_reference(args, workload_fn):
-    rank, world, local = dist_env()
-    if rank != 0:
-        return 0
-    w = workload_fn()
+def cpu_sample_spec(w, budget_cells):
+    """A bounded sample of the workload: explicit pairs, smallest first, or
+    queries x targets taken evenly from the length-sorted lists.  Returns
+    (jobs as [(query strings, target strings)], index map, cells, full, text)."""
+    q_all = [s.decode() for _, s in w.queries] if w.queries is not None else None
+    t_all = [s.decode() for _, s in w.targets]
+    if w.pairs is not None:
+        order = sorted(w.pairs, key=lambda p: len(q_all[p[0]]) * len(t_all[p[1]]))
+        jobs, idx, cells = [], [], 0
+        for qi, ti in order:
+            c = len(q_all[qi]) * len(t_all[ti])
+            if cells and cells + c > budget_cells:
+                break
+            jobs.append(([q_all[qi]], [t_all[ti]]))
+            idx.append(([qi], [ti]))
+            cells += c
+        return jobs, idx, cells, len(jobs) == len(w.pairs), \
+            "the %d smallest explicit pairs (%d cells) of the same workload, full path" % (len(jobs), cells)
+    if q_all is None:  # packed reads: the first reads only
+        n = min(int(w.reads.shape[0]), 20000)
+        q_all = [w.reads[i].tobytes().decode() for i in range(n)]
+    nq = min(len(q_all), 10)
+    q_step = max(1, len(q_all) // nq)
+    q10 = sum(map(len, q_all[::q_step][:nq]))
+    t_avg = sum(map(len, t_all)) / max(1, len(t_all))
+    nt = min(len(t_all), max(1, int(budget_cells / (q10 * t_avg))))
+    ti = list(range(0, len(t_all), max(1, len(t_all) // nt)))[:nt]
+    q_avg = sum(map(len, q_all)) / max(1, len(q_all))
+    nq = min(len(q_all), max(nq, int(budget_cells / (q_avg * sum(len(t_all[i]) for i in ti)))))
+    qi = list(range(0, len(q_all), max(1, len(q_all) // nq)))[:nq]
+    qs, ts = [q_all[i] for i in qi], [t_all[i] for i in ti]
+    cells = sum(map(len, qs)) * sum(map(len, ts))
+    full = len(qs) == (w.n_queries if w.queries is not None else -1) and len(ts) == len(t_all)
+    return [(qs, ts)], [(qi, ti)], cells, full, \
+        "%d queries x %d targets (%d cells) of the same workload, full path" % (len(qs), len(ts), cells)
+
+
+def cpu_baseline(w, score, seconds, processes=1):
+    """The oracle (CPU restatement of the reference path) on a bounded sample
+    sized for about `seconds`: a first run at an estimated rate calibrates a
+    second, larger one if the first was much shorter.  Returns (baseline
+    record, sample jobs, index map, oracle results per job)."""
+    import multiprocessing as mp
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle
+    oracle.build()
+    args = _oracle_args(score, w.settings)
+    rate = 24e6 * max(1, processes)  # cells/s first estimate of the oracle
+    for _ in range(3):
+        jobs, idx, cells, full, text = cpu_sample_spec(w, seconds * rate)
+        work = []
+        for qs, ts in jobs:  # split each job's targets over the processes
+            for k in range(max(1, processes)):
+                if ts[k::processes]:
+                    work.append((args, qs, ts[k::processes]))
+        t0 = time.time()
+        if processes <= 1:
+            res = [_oracle_chunk(j) for j in work]
+        else:
+            with mp.get_context("spawn").Pool(processes) as pool:
+                res = pool.map(_oracle_chunk, work)
+        dt = time.time() - t0
+        if dt >= 0.4 * seconds or full:
+            break
+        rate = cells / max(dt, 1e-3)
+    rec = {"value": cells / dt / 1e9, "unit": "GCUPS", "cores": processes, "kind": "port", "sample": text,
+           "seconds": dt}
+    return rec, jobs, idx, (res if processes <= 1 else None)
+
+
+def engine_hits(qs, ts, score, settings, device):
+    """The engine on query x target strings, ids all distinct (the oracle's
+    default keys): (pair maxima [nq, nt], hits as the oracle reports them)."""
+    from pypaswas_b200 import _native
+    from pypaswas_b200.smith_waterman import configure_engine
+    e = _native.Engine(device)
+    try:
+        configure_engine(e, score, settings)
+        e.set_queries([q.encode() for q in qs], np.arange(len(qs), dtype=np.int32))
+        e.set_targets([t.encode() for t in ts], np.arange(len(ts), dtype=np.int32) + len(qs))
+        e.align()
+        pm = e.pair_max()
+        hits, sb = e.hits()
+    finally:
+        e.close()
+    out = []
+    for h in hits:
+        n, o = int(h["n_cols"]), int(h["str_offset"])
+        out.append({"query": int(h["query"]), "target": int(h["target"]), "s_start": int(h["s_start"]),
+                    "s_end": int(h["s_end"]), "t_start": int(h["t_start"]), "t_end": int(h["t_end"]),
+                    "score": float(h["score"]), "matches": int(h["matches"]), "mismatches": int(h["mismatches"]),
+                    "sequence_match": sb[o:o + n].decode("latin-1"), "alignment": sb[o + n:o + 2 * n].decode("latin-1"),
+                    "target_match": sb[o + 2 * n:o + 3 * n].decode("latin-1")})
+    return pm, out
+
+
+def parity_leg(w, jobs, idx, oracle_res, device):
+    """The engine on the CPU baseline's sample against the oracle's results
+    for it: pair maxima and every hit (coordinates, score, counts, strings)."""
     from pypaswas_b200 import scores
     score = scores.make_score(w.settings)
-    procs = os.cpu_count() or 1
-    steps = []
-    # each step a bounded sample: the whole run stays near two minutes
-    per_step = max(1.0, min(args.cpu_seconds, 20.0, 120.0 / max(1, args.warmup + args.steps)))
-    for i in range(args.warmup + args.steps):
-        r = cpu_baseline(w if w.queries is not None else w.head(200000), score, per_step, processes=procs)
-        if i >= args.warmup:
-            steps.append(r)
-    v = float(np.median([s["value"] for s in steps]))
-    line = {"impl": "reference", "metric": "GCUPS", "value": v, "unit": "GCUPS", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": w.name,
-                       "pairs": len(w.pairs) if w.pairs is not None else w.n_queries * len(w.targets)},
-            "cpu_baseline": {"value": v, "unit": "GCUPS", "cores": procs, "kind": "port",
-                             "sample": steps[0]["sample"]},
-            "e2e": {"value": v, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "note": "CPU restatement of the reference path (oracle/paswas_oracle.c) over all host cores"}
-    print(json.dumps(line), flush=True)
-    return 0
+    pairs = hits_n = 0
+    pm_eq = hits_eq = True
+    for (qs, ts), (qi, ti), (o_pm, o_hits) in zip(jobs, idx, oracle_res):
+        pm, hits = engine_hits(qs, ts, score, w.settings, device)
+        pairs += len(qs) * len(ts)
+        hits_n += len(o_hits)
+        pm_eq = pm_eq and bool(np.array_equal(pm, o_pm))
+        hits_eq = hits_eq and hits == o_hits
+    return {"sample": "the CPU baseline's sample", "pairs": pairs, "oracle_hits": hits_n,
+            "pair_max_equal": pm_eq, "hits_equal": hits_eq}
 
 
-def main():
-    args = parse()
-    from pypaswas_b200 import workloads
-    if args.impl == "reference":
-        return run_reference(args, lambda: workload(args))
-    rank, world, local = dist_env()
-    import torch
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
-    torch.cuda.set_device(local)
-    w = workload(args)
-    e, score = engine_for(w, local)
-    cells = w.cells
-    affine = score.gap_extension is not None
-    mode = "affine" if affine else "linear"
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > L2 (126 MB)
-
-    chain = not args.no_chain
-    from pypaswas_b200 import _native
-    knobs = {"chain_min": _native.PW_TUNE_CHAIN_MIN, "grid_share": _native.PW_TUNE_GRID_SHARE,
-             "segment": _native.PW_TUNE_SEGMENT, "dual": _native.PW_TUNE_DUAL, "cand_slot": _native.PW_TUNE_CAND_SLOT}
-    tuning = {}
-    for kv in args.tune:
-        key, val = kv.split("=")
-        e.set_tuning(knobs[key], int(val))
-        tuning[key] = int(val)
-    if "chain_min" not in tuning and chain and w.pairs is None:
-        from pypaswas_b200.autotune import autotune
-        tuning["autotune"] = autotune(e)  # untimed: score sweeps on this workload
-    sampler = ClockSampler(local)
-    sampler.start()  # started before the warm-up: nvidia-smi is up when timing begins
-    for _ in range(args.warmup):
-        e.align(chain=chain)
-    torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
-    sampler.mark()  # samples before this point are dropped
-    times, infos = [], []
-    for _ in range(args.steps):
-        flush.zero_()  # between timed iterations: L2 flushed
-        torch.cuda.synchronize()
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        a.record()
-        info = e.align(chain=chain)  # synchronous: returns when the step's device work is done
-        b.record()
-        torch.cuda.synchronize()
-        times.append(a.elapsed_time(b))
-        infos.append(info.as_dict())
-    clocks = sampler.stop()
-    t_ms = reduce_max(float(sum(times)))
-    step_stats = {"min": float(min(times)), "median": float(np.median(times)), "max": float(max(times)),
-                  "all": [round(float(t), 3) for t in times],
-                  "call_ms": [round(float(i["total_ms"]), 3) for i in infos],
-                  "phase_ms": {k: [round(float(i[k]), 2) for i in infos] for k in
-                               ("score_ms", "trace_ms", "walk_ms", "setup_ms", "finish_ms")}}
-    value = whole_job_gcups(cells, args.steps, t_ms * 1e-3, world)
-    n_pairs = len(w.pairs) if w.pairs is not None else w.n_queries * len(w.targets)
-    ms_per_step = t_ms / args.steps
-
-    # roofline of the dominant kernel (integer-ALU bound: DPX add-max issue rate)
-    last = infos[-1]
-    trace_ms = sum(i["trace_kernel_ms"] for i in infos)
-    score_ms = sum(i["score_kernel_ms"] for i in infos)
-    if trace_ms >= score_ms:
-        wp, tp = last["warp_pairs"], last["traced_pairs"]
-        which = "band_kernel, one pair per warp" if wp >= tp else (
-            "sweep_kernel phase 2" if wp == 0 else "sweep_kernel phase 2 + band_kernel")
-        dom, dom_ms, dom_launch = "direction sweep (%s)" % which, trace_ms, sum(
-            i["trace_launches"] for i in infos)
-        ops = sum(i["traced_cells"] for i in infos) * OPS_PER_CELL[(mode, "dirs")]
-    else:
-        dom, dom_ms, dom_launch = "score sweep (score16_chain_kernel, 16x2 lanes)" if _sixteen_bit(e, w) else \
-            ("score sweep (band_kernel, bands chained across warps)" if e.last_info.score_path == 2 else
-             "score sweep (sweep_kernel phase 1)"), score_ms, sum(
-            i["score_launches"] for i in infos)
-        ops = cells * OPS_PER_CELL[(mode, "score")] * args.steps
-    peak32, peak16, _ = e.measure_int_peak()
-    lanes16 = "score" in dom and _sixteen_bit(e, w)
-    peak_ops = peak16 if lanes16 else peak32
-    achieved = ops / (dom_ms * 1e-3) / 1e12
-    traffic = load_traffic().get("direction_sweep_bytes_per_launch" if "direction" in dom else
-                                 "score_sweep_bytes_per_launch")
-
-    # end to end through the public driver, host records in, hits out
-    e2e_w = w if w.queries is not None else w.head(E2E_READS)
-    e2e_value, h2d, d2h = None, 0, 0
-    if not args.no_e2e:
-        if world > 1:
-            torch.distributed.barrier()
-        dt, h2d, d2h = _e2e(e2e_w, args.steps, local)
-        dt = reduce_max(dt)  # whole job: every rank's replica, the slowest rank's time
-        e2e_value = whole_job_gcups(e2e_w.cells, args.steps, dt, world)
-
-    out = {"metric": "GCUPS", "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": ms_per_step, "step_ms": step_stats,
-           "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-           "config": {"workload": "%s (%d pairs, full path)" % (w.name, n_pairs),
-                      "pairs": n_pairs,
-                      "cells_per_step": cells, "traced_pairs": last["traced_pairs"],
-                      "cand_overflow_pairs": last["cand_overflow_pairs"],
-                      "starting_points": last["starting_points"], "hits": last["hits"],
-                      "score_lanes": "targets" if last["orientation"] else "queries",
-                      "trace_lanes": "targets" if last["trace_orientation"] else "queries",
-                      "minimum_score": w.settings.minimum_score, "lower_limit_score": w.settings.lower_limit_score,
-                      "filter_factor": w.settings.filter_factor,
-                      "l2": "flushed between steps (256 MiB write); each step also writes >1e11 B of cell codes",
-                      "parallelism": "replica per GPU" if world > 1 else "single GPU",
-                      "tuning": tuning},
-           "phases_ms": {"score": last["score_ms"], "trace": last["trace_ms"], "walk": last["walk_ms"],
-                         "score_kernels": last["score_kernel_ms"], "trace_kernels": last["trace_kernel_ms"],
-                         "host_setup": last["setup_ms"], "host_finish": last["finish_ms"], "call": last["total_ms"]},
-           "gpu_launches": int(sum(i["kernel_launches"] for i in infos)),
-           "clocks": clocks,
-           "roofline": {"bound": "int_alu", "kernel": dom, "achieved": achieved,
-                        "peak": peak_ops / 1e12, "unit": "Tops/s", "frac": achieved / (peak_ops / 1e12),
-                        "peak_source": "measured in this run: DPX add-max issue probe (pw_measure_int_peak), "
-                                       + ("16x2 form" if lanes16 else "32-bit form"),
-                        "ops_per_cell": OPS_PER_CELL[(mode, "dirs" if "direction" in dom else "score")],
-                        "launches": dom_launch, "avg_launch_ms": dom_ms / max(1, dom_launch),
-                        "traffic": traffic,
-                        "hbm_gbs_measured": load_peaks().get("hbm_gbs")},
-           "e2e": {"value": e2e_value, "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                   "workload": e2e_w.name}}
-    if not args.no_plain and w.pairs is None:
-        out["plain"] = plain_vs_batched(w if w.queries is not None else w.head(64), local, value)
-    if not args.no_serve and rank == 0 and args.config == 2:
-        out["serve"] = serve_leg(local, args.serve_seconds, [float(x) for x in args.serve_loads.split(",")])
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(w if w.queries is not None else w.head(20000), score, args.cpu_seconds,
-                                           processes=1)
-    if rank == 0:
-        print(json.dumps(out), flush=True)
-    e.close()
-    if world > 1:
-        torch.distributed.barrier()
-        torch.distributed.destroy_process_group()
-    return 0
-
-
-def plain_vs_batched(w, device, batched_value, n_q=8, n_t=64):
-    """GCUPS of the plain form -- one (query, target) pair per kernel launch,
-    the shape of the reference's per-pair kernel calls -- on an evenly spaced
-    sample of the workload, next to the batched engine on the same sample.
-    Both run the full path (score, starting points, walk)."""
-    import torch
-    from pypaswas_b200 import workloads
-    qs = w.queries[::max(1, len(w.queries) // n_q)][:n_q]
-    ts = w.targets[::max(1, len(w.targets) // n_t)][:n_t]
-    sample = workloads.Workload(w.name + " sample", qs, ts, w.settings)
-    e, _ = engine_for(sample, device)
-    out = {}
-    for label, plain in (("batched", False), ("plain", True)):
-        e.align(plain=plain)  # warm-up
-        torch.cuda.synchronize()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record()
-        info = e.align(plain=plain)
-        b.record()
-        torch.cuda.synchronize()
-        ms = a.elapsed_time(b)
-        out[label] = {"value": sample.cells / (ms * 1e-3) / 1e9, "ms": ms, "launches": int(info.kernel_launches),
-                      "hits": int(info.hits)}
-    e.close()
-    return {"value": out["plain"]["value"], "unit": "GCUPS",
-            "sample": "%d queries x %d targets (%d pairs, %d cells), evenly spaced in length order"
-                      % (len(qs), len(ts), len(qs) * len(ts), sample.cells),
-            "launches": out["plain"]["launches"], "batched_same_sample": out["batched"]["value"],
-            "batched_over_plain": batched_value / out["plain"]["value"],
-            "hits_equal": out["plain"]["hits"] == out["batched"]["hits"]}
-
-
+# ------------------------------------------------------------------ serving
 def serve_leg(device, seconds, loads, workers=2, max_batch=32):
     """Serving configuration: a resident database of 100,000 protein sequences
     (log-normal lengths, median 300, 50-1,500 aa), Poisson arrivals of single
@@ -519,53 +580,167 @@ def serve_leg(device, seconds, loads, workers=2, max_batch=32):
             "seconds_per_rate": seconds, "sweep": sweep}
 
 
-def _sixteen_bit(engine, w):
-    """The score sweep ran on 16-bit lanes (integer scores; see pw_score16.cuh)."""
-    return engine.last_info is not None and engine.last_info.score_launches > 0 and \
-        engine.last_info.score_path == 0 and engine.last_info.overflow_pairs == 0 and _integer_scores(w)
+# ------------------------------------------------------------------ one config
+def run_config(cfg, args, device, world, flush, sampler, headline):
+    """Every leg of one configuration; returns its record."""
+    from pypaswas_b200 import _native
+    w = workload(cfg, args)
+    e, score = engine_for(w, device)
+    chain = not args.no_chain
+    knobs = {"chain_min": _native.PW_TUNE_CHAIN_MIN, "grid_share": _native.PW_TUNE_GRID_SHARE,
+             "segment": _native.PW_TUNE_SEGMENT, "dual": _native.PW_TUNE_DUAL, "cand_slot": _native.PW_TUNE_CAND_SLOT}
+    tuning = {}
+    for kv in args.tune:
+        key, val = kv.split("=")
+        e.set_tuning(knobs[key], int(val))
+        tuning[key] = int(val)
+    if "chain_min" not in tuning and chain and w.pairs is None:
+        from pypaswas_b200.autotune import autotune
+        tuning["autotune"] = autotune(e)  # untimed: score sweeps on this workload
+    replan = not args.plan_cached
+    times, infos = device_steps(e, args.steps, args.warmup, replan, chain, flush, sampler if headline else None,
+                                world)
+    t_ms = reduce_max(float(sum(times))) if headline else float(sum(times))
+    value = whole_job_gcups(w.cells, args.steps, t_ms * 1e-3, world if headline else 1)
+    last = infos[-1]
+    n_pairs = len(w.pairs) if w.pairs is not None else w.n_queries * len(w.targets)
+    rec = {"metric": "GCUPS", "value": value, "unit": "GCUPS", "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": t_ms / args.steps,
+           "step_ms": {"min": float(min(times)), "median": float(np.median(times)), "max": float(max(times)),
+                       "all": [round(float(t), 3) for t in times]},
+           "dtype": "int32", "data": "synthetic",
+           "config": {"workload": "%s (%d pairs, full path)" % (w.name, n_pairs), "pairs": n_pairs,
+                      "cells_per_step": w.cells, "traced_pairs": last["traced_pairs"],
+                      "cand_overflow_pairs": last["cand_overflow_pairs"],
+                      "starting_points": last["starting_points"], "hits": last["hits"],
+                      "memory_waves": last["waves"],
+                      "score_lanes": "targets" if last["orientation"] else "queries",
+                      "trace_lanes": "targets" if last["trace_orientation"] else "queries",
+                      "minimum_score": w.settings.minimum_score,
+                      "lower_limit_score": w.settings.lower_limit_score,
+                      "filter_factor": w.settings.filter_factor,
+                      "l2": "flushed between steps (256 MiB write)",
+                      "step": "sequences resident in HBM; the score sweep's work list "
+                              + ("kept from the previous step" if not replan else "rebuilt every step")
+                              + " (reuse bits seen: %d)" % int(np.bitwise_or.reduce([i["reuse"] for i in infos])),
+                      "tuning": tuning},
+           "phases_ms": {k: [round(float(i[k]), 2) for i in infos] for k in
+                         ("score_ms", "trace_ms", "walk_ms", "setup_ms", "finish_ms", "total_ms")},
+           "gpu_launches": int(sum(i["kernel_launches"] for i in infos))}
+    rec["roofline"] = roofline(e, w, score, infos, args.steps)
+    traffic = load_traffic().get("%s_%s" % (NAMES[cfg], "direction" if "direction" in rec["roofline"]["kernel"]
+                                             else "score"))
+    rec["roofline"]["traffic"] = traffic
+    rec["roofline"]["hbm_gbs_measured"] = load_peaks().get("hbm_gbs")
+    e.close()
+    # end to end through the public API, fresh inputs every step
+    if not args.no_e2e:
+        if cfg == 4:
+            ws = [workload(4, argparse.Namespace(**dict(vars(args), reads=E2E_READS)), seed=s) for s in (4, 14)]
+        else:
+            ws = [w, workload(cfg, args, seed={1: 11, 2: 12, 3: 13}[cfg])]
+        if world > 1 and headline:
+            import torch
+            torch.distributed.barrier()
+        steps_e2e = args.steps if headline else max(3, min(args.steps, 5))
+        cells, dt, h2d, d2h, reuse = e2e_leg(ws, steps_e2e, device, trimmer=cfg == 4)
+        if headline:
+            dt = reduce_max(dt)
+        rec["e2e"] = {"value": whole_job_gcups(cells / steps_e2e, steps_e2e, dt, world if headline else 1),
+                      "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                      "steps": steps_e2e, "ms_per_step": dt * 1e3 / steps_e2e,
+                      "api": "Trimmer.trimmed_fasta (records -> trimmedFasta text)" if cfg == 4 else
+                             ("Aligner.process per query (records -> HitList)" if w.pairs is not None else
+                              "Aligner.process (records -> HitList)"),
+                      "inputs": "two seeded input sets of the same shape, alternating: every step copies and "
+                                "prepares its inputs and rebuilds its plan (reuse bits seen: %d)" % reuse,
+                      "workload": ws[0].name}
+    return w, score, rec
 
 
-def _integer_scores(w):
-    from pypaswas_b200 import scores
-    m = scores.make_score(w.settings).matrix_array()
-    return bool(np.all(np.floor(m) == m) and np.all(np.abs(m) <= 127))
-
-
-def _e2e(w, steps, device):
-    """Public driver path: Aligner.process on host records -> HitList.  With
-    explicit pairs (long DNA), one process() call per query against its
-    targets, as the reference would be run once per pair."""
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    rank, world, local = dist_env()
     import torch
-    from pypaswas_b200.formatters import TrimmerFormatter
-    from pypaswas_b200.programs import Aligner, Trimmer
-    from pypaswas_b200.records import SeqRecord
-    trimmer = getattr(w.settings, "program", "aligner") == "trimmer"
-    queries = [SeqRecord(s, i) for i, s in w.queries]
-    targets = [SeqRecord(s, i) for i, s in w.targets]
-    if w.pairs is None:
-        calls = [(queries, targets)]
-    else:
-        per_q = {}
-        for qi, ti in w.pairs:
-            per_q.setdefault(qi, []).append(targets[ti])
-        calls = [([queries[qi]], ts) for qi, ts in sorted(per_q.items())]
-    aligner = (Trimmer if trimmer else Aligner)(None, None, w.settings, device=device)
-    for qs, ts in calls[:2]:
-        aligner.process(qs, ts, None)  # warm-up
-    torch.cuda.synchronize()
-    h2d = d2h = 0
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        h2d = d2h = 0
-        for qs, ts in calls:
-            hl = aligner.process(qs, ts, None)
-            if trimmer:
-                TrimmerFormatter(None, hl, None).lines()  # the program's trimmedFasta records
-            h2d += int(aligner.smith_waterman.last_h2d_bytes)
-            d2h += int(aligner.smith_waterman.last_d2h_bytes)
-    torch.cuda.synchronize()
-    dt = time.perf_counter() - t0
-    return dt, h2d, d2h
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > L2 (126 MB)
+    sampler = ClockSampler(local)
+    sampler.start()  # started before the warm-up: nvidia-smi is up when timing begins
+    try:
+        w, score, out = run_config(args.config, args, local, world, flush, sampler, headline=True)
+        out.update({"n_gpus": world, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                    "clocks": sampler.summary()})
+        out["config"]["parallelism"] = "replica per GPU" if world > 1 else "single GPU"
+        n_plain = {1: (8, 100), 2: (8, 64), 3: (4, 0), 4: (64, 48)}
+        if not args.no_plain:
+            out["plain"] = plain_leg(w if w.queries is not None else w.head(64), local, *n_plain[args.config])
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            rec, jobs, idx, res = cpu_baseline(w, score, args.cpu_seconds, processes=1)
+            out["cpu_baseline"] = rec
+            out["parity"] = parity_leg(w, jobs, idx, res, local)
+        also = ([c for c in (1, 3, 4) if args.config == 2] if args.also == "auto" else
+                [] if args.also == "none" else [int(c) for c in args.also.split(",") if c.strip()])
+        if world == 1 and also:
+            out["configs"] = {}
+            for c in also:
+                wc, sc, rec = run_config(c, args, local, 1, flush, sampler, headline=False)
+                if not args.no_plain:
+                    rec["plain"] = plain_leg(wc if wc.queries is not None else wc.head(64), local, *n_plain[c])
+                if not args.no_cpu_baseline:
+                    b, jobs, idx, res = cpu_baseline(wc, sc, max(5.0, args.cpu_seconds / 2), processes=1)
+                    rec["cpu_baseline"] = b
+                    rec["parity"] = parity_leg(wc, jobs, idx, res, local)
+                out["configs"][NAMES[c]] = rec
+                del wc
+        if not args.no_serve and rank == 0 and world == 1 and args.config == 2:
+            out["serve"] = serve_leg(local, args.serve_seconds, [float(x) for x in args.serve_loads.split(",")])
+    finally:
+        sampler.stop()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+# ------------------------------------------------------------------ reference arm
+def run_reference(args):
+    """The reference path's CPU implementation (the oracle port) over all host
+    cores, each step a bounded sample of the headline workload."""
+    rank, world, local = dist_env()
+    if rank != 0:
+        return 0
+    w = workload(args.config, args)
+    from pypaswas_b200 import scores
+    score = scores.make_score(w.settings)
+    procs = os.cpu_count() or 1
+    steps = []
+    # each step a bounded sample: the whole run stays near two minutes
+    per_step = max(1.0, min(args.cpu_seconds, 20.0, 120.0 / max(1, args.warmup + args.steps)))
+    for i in range(args.warmup + args.steps):
+        rec = cpu_baseline(w, score, per_step, processes=procs)[0]
+        if i >= args.warmup:
+            steps.append(rec)
+    v = float(np.median([s["value"] for s in steps]))
+    line = {"impl": "reference", "metric": "GCUPS", "value": v, "unit": "GCUPS", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": w.name,
+                       "pairs": len(w.pairs) if w.pairs is not None else w.n_queries * len(w.targets)},
+            "cpu_baseline": {"value": v, "unit": "GCUPS", "cores": procs, "kind": "port",
+                             "sample": steps[0]["sample"]},
+            "e2e": {"value": v, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "CPU restatement of the reference path (oracle/paswas_oracle.c) over all host cores"}
+    print(json.dumps(line), flush=True)
+    return 0
 
 
 if __name__ == "__main__":

@@ -34,9 +34,13 @@ extern "C" {
 
 /* pw_align() flags */
 #define PW_FLAG_SCORE_ONLY 1u /* pair maxima only: no starting points, no walk */
-#define PW_FLAG_PLAIN 2u      /* one pair per kernel launch (the unbatched form) */
+#define PW_FLAG_PLAIN 2u      /* the unbatched form: one (query, target) pair per launch, as the reference
+                                 launches one pair's kernels at a time; with integer scores each pair runs
+                                 on the single-pair wavefront kernel (a warp per 256-row band), with fp32
+                                 scores on one lane of the inter-sequence sweep */
 #define PW_FLAG_INT32 4u      /* keep the score sweep on 32-bit lanes (no 16-bit dual-pair sweep) */
 #define PW_FLAG_NO_CHAIN 8u   /* 16-bit sweep: run each multi-strip item on one warp (no chained strips) */
+#define PW_FLAG_REPLAN 16u    /* rebuild the score sweep's work list even when inputs are unchanged */
 
 typedef struct pw_engine pw_engine;
 
@@ -80,10 +84,21 @@ typedef struct {
     double finish_ms;       /* host wall time after the device work: hit order, alignment strings */
     double total_ms;        /* host wall time of the whole call */
     int32_t score_path;     /* score sweep used: 0 16-bit strips, 1 32-bit / fp32 strips, 2 bands (pw_set_pairs
-                               or few long sequences) */
+                               or few long sequences), 3 bands one pair per launch (PW_FLAG_PLAIN) */
     int32_t dual_lanes;     /* 16-bit score sweep in the dual-lane form: each strip against two lane
                                sequences per lane (1) instead of two strips against one (0) */
+    int32_t waves;          /* memory waves of the direction sweep (0 when no pair was traced) */
+    int32_t reuse;          /* work this call skipped because its inputs were unchanged since the last
+                               call: PW_REUSE_QUERIES / PW_REUSE_TARGETS (the device copy and encodings of
+                               that sequence set were kept), PW_REUSE_PLAN (the score sweep's work list
+                               was kept) */
+    int64_t h2d_bytes;      /* bytes this call copied host -> device (sequences, encodings, work lists) */
+    int64_t d2h_bytes;      /* bytes this call copied device -> host (maxima, pair lists, starts, hits) */
 } pw_run_info;
+
+#define PW_REUSE_QUERIES 1
+#define PW_REUSE_TARGETS 2
+#define PW_REUSE_PLAN 4
 
 /* Creates an engine on CUDA device `device`.
  * Replaces SmithWatermanCuda._initialize_device (SmithWatermanCuda.py:46-62). */
@@ -166,7 +181,7 @@ int pw_set_pairs(pw_engine* e, const int32_t* query_idx, const int32_t* target_i
  * (SmithWaterman.py:420-432). */
 int pw_set_wave_limit(pw_engine* e, int64_t bytes);
 
-/* Tuning knobs of the kernels' launch shapes (no counterpart in the
+/* Tuning knobs of the kernels' launch shapes and waits (no counterpart in the
  * reference, whose shapes are fixed template constants, default_main.cu:7-30).
  * Values 0 restore the automatic choice.
  *   PW_TUNE_CHAIN_MIN   16-bit score sweep: multi-strip items whose cost
@@ -193,6 +208,16 @@ int pw_set_wave_limit(pw_engine* e, int64_t bytes);
  *                       its sweep is repeated with an exact slot (default
  *                       64); a small value exercises the repeat path */
 #define PW_TUNE_CAND_SLOT 4
+/*   PW_TUNE_WAIT_NS     longest wait, in nanoseconds, of a chained strip or
+ *                       band for its predecessor's progress before the launch
+ *                       gives up and pw_align fails with PW_ERR_KERNEL
+ *                       (default 2,000,000,000) */
+#define PW_TUNE_WAIT_NS 5
+/*   PW_TUNE_STALL_TEST  1: the next chained launch makes one queue entry wait
+ *                       on a progress flag that nothing sets, so that its wait
+ *                       runs out (PW_TUNE_WAIT_NS) and pw_align reports the
+ *                       failure; a test of the bounded waits.  0: off */
+#define PW_TUNE_STALL_TEST 6
 int pw_set_tuning(pw_engine* e, int key, int64_t value);
 
 /* Pair maxima (the last block of the maxima chain, default_main.cu:591),
@@ -352,6 +377,39 @@ int pw_txt_records(const pw_hit* hits, int64_t n_hits, int32_t n_queries, int32_
                    const int64_t* q_id_off, const int32_t* t_rank, const int64_t* t_orig_len,
                    const int64_t* t_start_pos, const char* t_id, const int64_t* t_id_off, const double* thresholds,
                    char* out, int64_t out_cap, int64_t* out_len);
+
+/* ---------------------------------------------------------------------------
+ * Sequence records read natively (host only, no device).  Replaces the
+ * reference's record preparation for the engine: BioPythonReader.read_records
+ * (pyPaSWAS/Core/Readers.py:90-118; Biopython's FASTA / FASTQ parsing, the
+ * islice(start, end) of the file's records, the limit_length filter that keeps
+ * 0 < len <= limit_length when limit_length > 0, SWSeqRecord's upper-casing,
+ * SWSeqRecord.py:16), the target transforms complement_records,
+ * complement_records_only and reverse_records (Readers.py:68-86, ids + "_RC")
+ * and sort_records (Readers.py:30-34: stable, longest first), as
+ * Pypaswas._get_query_sequences / _get_target_sequences chain them
+ * (pypaswasall.py:98-124).  The records come out packed: residues with
+ * offsets (n + 1) and ids with offsets (n + 1), in the final order. */
+#define PW_FORMAT_FASTA 0
+#define PW_FORMAT_FASTQ 1
+#define PW_RECORDS_AS_READ 0        /* queries, and targets of non-DNA scores */
+#define PW_RECORDS_APPEND_RC 1      /* complement_records: + reverse complements */
+#define PW_RECORDS_RC_ONLY 2        /* complement_records_only: the reverse complements alone */
+#define PW_RECORDS_APPEND_REVERSED 3 /* reverse_records: + reversed copies */
+typedef struct pw_records pw_records;
+/* Parses `bytes` of FASTA / FASTQ text; end < 0 reads to the last record.
+ * Malformed FASTQ fails with PW_ERR_ARG and a message in err. */
+int pw_records_parse(const char* data, int64_t bytes, int format, int64_t start, int64_t end, int64_t limit_length,
+                     int transform, int sort_desc, pw_records** out, char* err, int32_t err_bytes);
+/* The same on a file (BioPythonReader's path argument). */
+int pw_records_read(const char* path, int format, int64_t start, int64_t end, int64_t limit_length, int transform,
+                    int sort_desc, pw_records** out, char* err, int32_t err_bytes);
+/* Record count, residue bytes, id bytes and the records the length limit removed. */
+int pw_records_sizes(const pw_records* r, int64_t* n_records, int64_t* residue_bytes, int64_t* id_bytes,
+                     int64_t* dropped);
+/* Copies the packed records into caller buffers sized from pw_records_sizes. */
+int pw_records_copy(const pw_records* r, uint8_t* residues, int64_t* offsets, char* ids, int64_t* id_offsets);
+void pw_records_free(pw_records* r);
 
 #ifdef __cplusplus
 }

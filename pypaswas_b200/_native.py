@@ -29,11 +29,23 @@ PW_FLAG_SCORE_ONLY = 1
 PW_FLAG_PLAIN = 2
 PW_FLAG_INT32 = 4
 PW_FLAG_NO_CHAIN = 8
+PW_FLAG_REPLAN = 16
 PW_TUNE_CHAIN_MIN = 0
 PW_TUNE_GRID_SHARE = 1
 PW_TUNE_SEGMENT = 2
 PW_TUNE_DUAL = 3
 PW_TUNE_CAND_SLOT = 4
+PW_TUNE_WAIT_NS = 5
+PW_TUNE_STALL_TEST = 6
+PW_FORMAT_FASTA = 0
+PW_FORMAT_FASTQ = 1
+PW_RECORDS_AS_READ = 0
+PW_RECORDS_APPEND_RC = 1
+PW_RECORDS_RC_ONLY = 2
+PW_RECORDS_APPEND_REVERSED = 3
+PW_REUSE_QUERIES = 1
+PW_REUSE_TARGETS = 2
+PW_REUSE_PLAN = 4
 
 # symbols the header declares, checked by the CPU test-suite
 EXPORTED_SYMBOLS = (
@@ -43,6 +55,7 @@ EXPORTED_SYMBOLS = (
     "pw_set_wave_limit", "pw_set_tuning", "pw_set_pairs", "pw_server_create", "pw_server_destroy", "pw_server_last_error", "pw_server_set_scoring",
     "pw_server_load_db", "pw_server_submit", "pw_server_wait", "pw_server_top_hits", "pw_server_hits",
     "pw_server_release", "pw_server_stats", "pw_server_tune", "pw_trimmed_fasta", "pw_txt_records",
+    "pw_records_parse", "pw_records_read", "pw_records_sizes", "pw_records_copy", "pw_records_free",
 )
 
 
@@ -75,7 +88,9 @@ class PwRunInfo(ctypes.Structure):
                 ("overflow_pairs", ctypes.c_int64), ("traced_cells", ctypes.c_int64),
                 ("warp_pairs", ctypes.c_int64), ("cand_overflow_pairs", ctypes.c_int64),
                 ("setup_ms", ctypes.c_double), ("finish_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
-                ("score_path", ctypes.c_int32), ("dual_lanes", ctypes.c_int32)]
+                ("score_path", ctypes.c_int32), ("dual_lanes", ctypes.c_int32),
+                ("waves", ctypes.c_int32), ("reuse", ctypes.c_int32),
+                ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -144,6 +159,14 @@ def bind(lib):
                                             ctypes.POINTER(I64)]),
         "pw_txt_records": (ctypes.c_int, [P, I64, I32, I32, P, I64, P, P, P, P, P, P, P, P, P, P, P, P, I64,
                                           ctypes.POINTER(I64)]),
+        "pw_records_parse": (ctypes.c_int, [P, I64, ctypes.c_int, I64, I64, I64, ctypes.c_int, ctypes.c_int,
+                                            ctypes.POINTER(ctypes.c_void_p), ctypes.c_char_p, I32]),
+        "pw_records_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, I64, I64, I64, ctypes.c_int,
+                                           ctypes.c_int, ctypes.POINTER(ctypes.c_void_p), ctypes.c_char_p, I32]),
+        "pw_records_sizes": (ctypes.c_int, [P, ctypes.POINTER(I64), ctypes.POINTER(I64), ctypes.POINTER(I64),
+                                            ctypes.POINTER(I64)]),
+        "pw_records_copy": (ctypes.c_int, [P, P, P, P, P]),
+        "pw_records_free": (None, [P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -248,6 +271,16 @@ class Engine(object):
                "pw_set_queries")
         self.n_queries = n
 
+    def set_targets_packed(self, residues, offsets, id_keys):
+        """Targets as one concatenated uint8 array plus int64 offsets (n + 1)."""
+        buf = np.ascontiguousarray(residues, dtype=np.uint8).reshape(-1)
+        off = np.ascontiguousarray(offsets, dtype=np.int64)
+        keys = np.ascontiguousarray(id_keys, dtype=np.int32)
+        n = len(off) - 1
+        _check(self.lib, self.handle, self.lib.pw_set_targets(self.handle, _ptr(buf), _ptr(off), n, _ptr(keys)),
+               "pw_set_targets")
+        self.n_targets = n
+
     def set_targets(self, seqs, id_keys):
         buf, off = pack_sequences(seqs)
         keys = np.ascontiguousarray(id_keys, dtype=np.int32)
@@ -255,10 +288,10 @@ class Engine(object):
                self.lib.pw_set_targets(self.handle, _ptr(buf), _ptr(off), len(seqs), _ptr(keys)), "pw_set_targets")
         self.n_targets = len(seqs)
 
-    def align(self, score_only=False, plain=False, start_cap=-1, int32=False, chain=True):
+    def align(self, score_only=False, plain=False, start_cap=-1, int32=False, chain=True, replan=False):
         info = PwRunInfo()
         flags = (PW_FLAG_SCORE_ONLY if score_only else 0) | (PW_FLAG_PLAIN if plain else 0) | \
-            (PW_FLAG_INT32 if int32 else 0) | (0 if chain else PW_FLAG_NO_CHAIN)
+            (PW_FLAG_INT32 if int32 else 0) | (0 if chain else PW_FLAG_NO_CHAIN) | (PW_FLAG_REPLAN if replan else 0)
         rc = self.lib.pw_align(self.handle, flags, int(start_cap), ctypes.byref(info))
         _check(self.lib, self.handle, rc, "pw_align")
         self.last_info = info

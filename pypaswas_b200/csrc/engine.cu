@@ -284,6 +284,10 @@ struct pw_engine {
     HostBuf<char> h_strings;
     HostBuf<StartRec> h_starts;
     int64_t launches = 0;
+    int64_t h2d = 0, d2h = 0;  // bytes copied by the current pw_align
+    int32_t reuse = 0;         // PW_REUSE_* bits of the current pw_align
+    std::vector<int4> h_chain_info;  // the chained queue's (chain, strip, pred) entries, host copy
+    DevBuf stall_buf;          // PW_TUNE_STALL_TEST: the queue with one entry re-pointed at a silent flag
 };
 
 // Resident-block budget of this engine's persistent kernels: all SMs' worth,
@@ -296,6 +300,12 @@ static int grid_cap(const pw_engine* e, int per_sm) {
     return (int)std::max<int64_t>(1, full * share / 1000);
 }
 
+// Bound of one chain or band wait (PW_TUNE_WAIT_NS, else kChainWaitNs).
+static unsigned long long wait_limit(const pw_engine* e) {
+    const int64_t v = e->tune[PW_TUNE_WAIT_NS];
+    return v > 0 ? (unsigned long long)v : kChainWaitNs;
+}
+
 static int fail(pw_engine* e, int code, const std::string& msg) {
     if (e) e->err = msg;
     return code;
@@ -305,6 +315,17 @@ static int cuda_fail(pw_engine* e, cudaError_t c, const char* what) {
     std::string m = std::string(what) + ": " + cudaGetErrorString(c);
     int code = (c == cudaErrorMemoryAllocation) ? PW_ERR_NOMEM : PW_ERR_KERNEL;
     return fail(e, code, m);
+}
+
+// Host <-> device copies on the engine's stream, counted for pw_run_info.
+static cudaError_t copy_h2d(pw_engine* e, void* dst, const void* src, size_t n) {
+    e->h2d += (int64_t)n;
+    return cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, e->stream);
+}
+
+static cudaError_t copy_d2h(pw_engine* e, void* dst, const void* src, size_t n) {
+    e->d2h += (int64_t)n;
+    return cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, e->stream);
 }
 
 #define PW_CUDA(call, what)                                   \
@@ -521,7 +542,7 @@ static cudaError_t upload(pw_engine* e, DevBuf& b, const HostBuf<HT>& v) {
     cudaError_t c = b.reserve(e->stream, std::max<size_t>(v.size() * sizeof(HT), 16));
     if (c != cudaSuccess) return c;
     if (v.empty()) return cudaSuccess;
-    return cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(HT), cudaMemcpyHostToDevice, e->stream);
+    return copy_h2d(e, b.p, v.data(), v.size() * sizeof(HT));
 }
 
 template <typename HT>
@@ -529,13 +550,13 @@ static cudaError_t upload(pw_engine* e, DevBuf& b, const std::vector<HT>& v) {
     cudaError_t c = b.reserve(e->stream, std::max<size_t>(v.size() * sizeof(HT), 16));
     if (c != cudaSuccess) return c;
     if (v.empty()) return cudaSuccess;
-    return cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(HT), cudaMemcpyHostToDevice, e->stream);
+    return copy_h2d(e, b.p, v.data(), v.size() * sizeof(HT));
 }
 
 static cudaError_t download(pw_engine* e, HostBuf<float>& v, const void* src, size_t n) {
     if (!v.resize(n)) return cudaErrorMemoryAllocation;
     if (!n) return cudaSuccess;
-    cudaError_t c = cudaMemcpyAsync(v.data(), src, n * sizeof(float), cudaMemcpyDeviceToHost, e->stream);
+    cudaError_t c = copy_d2h(e, v.data(), src, n * sizeof(float));
     if (c != cudaSuccess) return c;
     return cudaStreamSynchronize(e->stream);
 }
@@ -544,7 +565,7 @@ template <typename HT>
 static cudaError_t download(pw_engine* e, std::vector<HT>& v, const void* src, size_t n) {
     v.resize(n);
     if (!n) return cudaSuccess;
-    cudaError_t c = cudaMemcpyAsync(v.data(), src, n * sizeof(HT), cudaMemcpyDeviceToHost, e->stream);
+    cudaError_t c = copy_d2h(e, v.data(), src, n * sizeof(HT));
     if (c != cudaSuccess) return c;
     return cudaStreamSynchronize(e->stream);
 }
@@ -555,7 +576,10 @@ static cudaError_t download(pw_engine* e, std::vector<HT>& v, const void* src, s
 // come and go, and nothing is uploaded again while the sequences and the
 // scoring model are unchanged.
 static int prepare_targets(pw_engine* e) {
-    if (e->prep_t[0] == e->t_gen && e->prep_t[1] == e->s_gen) return PW_OK;
+    if (e->prep_t[0] == e->t_gen && e->prep_t[1] == e->s_gen) {
+        e->reuse |= PW_REUSE_TARGETS;
+        return PW_OK;
+    }
     const HostSeqs& T = e->T;
     const int off = e->char_offset, dim = e->dim;
     Prepared& pr = e->pr;
@@ -627,7 +651,10 @@ static int prepare_targets(pw_engine* e) {
 }
 
 static int prepare_queries(pw_engine* e) {
-    if (e->prep_q[0] == e->q_gen && e->prep_q[1] == e->s_gen) return PW_OK;
+    if (e->prep_q[0] == e->q_gen && e->prep_q[1] == e->s_gen) {
+        e->reuse |= PW_REUSE_QUERIES;
+        return PW_OK;
+    }
     const HostSeqs& Q = e->Q;
     const int off = e->char_offset, dim = e->dim;
     Prepared& pr = e->pr;
@@ -906,8 +933,11 @@ static int setup_chains(pw_engine* e, const std::vector<WorkItem>& items, int i0
     cudaError_t c;
     if ((c = upload(e, e->chain_items, q)) != cudaSuccess) return cuda_fail(e, c, "upload chain items");
     if ((c = upload(e, e->chain_info, info)) != cudaSuccess) return cuda_fail(e, c, "upload chain info");
+    e->h_chain_info = info;
     if ((c = upload(e, e->chain_ring_off, ring_off)) != cudaSuccess) return cuda_fail(e, c, "upload ring offsets");
-    if ((c = e->chain_prog.reserve(e->stream, q.size() * sizeof(int))) != cudaSuccess) return cuda_fail(e, c, "alloc chain progress");
+    // one progress flag per entry, plus one that no entry ever sets (PW_TUNE_STALL_TEST)
+    if ((c = e->chain_prog.reserve(e->stream, (q.size() + 1) * sizeof(int))) != cudaSuccess)
+        return cuda_fail(e, c, "alloc chain progress");
     if ((c = e->chain_max.reserve(e->stream, q.size() * kWarp * sizeof(uint32_t))) != cudaSuccess)
         return cuda_fail(e, c, "alloc chain maxima");
     if ((c = e->chain_ring.reserve(e->stream, (size_t)std::max<int64_t>(ring_elems, 1) * sizeof(uint4))) != cudaSuccess)
@@ -971,10 +1001,12 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uin
     const int nq = e->Q.n, nt = e->T.n;
     auto& P1 = e->p1;
     const uint32_t pflags = flags & PW_FLAG_NO_CHAIN;
-    const bool reuse = P1.valid && P1.qg == e->q_gen && P1.tg == e->t_gen && P1.sg == e->s_gen &&
+    const bool reuse = !(flags & PW_FLAG_REPLAN) && P1.valid && P1.qg == e->q_gen && P1.tg == e->t_gen &&
+                       P1.sg == e->s_gen &&
                        P1.flags == pflags && P1.tune == e->tune[PW_TUNE_CHAIN_MIN] &&
                        P1.share == e->tune[PW_TUNE_GRID_SHARE] && P1.dual_mode == e->tune[PW_TUNE_DUAL];
     cudaError_t c;
+    if (reuse) e->reuse |= PW_REUSE_PLAN;
     if (!reuse) {
         const double t_plan = wall_ms();
         P1.valid = false;
@@ -1102,6 +1134,7 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uin
     S.stride_strip = trans ? nt : 1;
     S.stride_lane = trans ? 1 : nt;
     S.pad_code = S.alpha1 - 1;
+    S.wait_ns = wait_limit(e);
     if (begin[kS32Multi + 1] > begin[kS32Multi]) {
         const int64_t slot = (int64_t)P1.xm_multi * kWarp;
         if ((c = e->bnd_pool.reserve(e->stream, (size_t)slot * e->sm_count * 16 * 4 * sizeof(uint4))) != cudaSuccess)
@@ -1120,7 +1153,20 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uin
         S.run_max = e->chain_max.as<uint32_t>();
         S.abort_flag = e->chain_abort.as<int>();
         S.n_chain_items = P1.n_chain_items;
-        if ((c = cudaMemsetAsync(e->chain_prog.p, 0, (size_t)P1.n_chain_items * sizeof(int), e->stream)) != cudaSuccess ||
+        if (e->tune[PW_TUNE_STALL_TEST]) {
+            // one entry with a predecessor waits on the spare flag instead
+            e->tune[PW_TUNE_STALL_TEST] = 0;
+            std::vector<int4> info = e->h_chain_info;
+            for (int4& v : info)
+                if (v.y > 0) {
+                    v.z = P1.n_chain_items;
+                    break;
+                }
+            if ((c = upload(e, e->stall_buf, info)) != cudaSuccess) return cuda_fail(e, c, "upload stalled queue");
+            S.chain = e->stall_buf.as<int4>();
+        }
+        if ((c = cudaMemsetAsync(e->chain_prog.p, 0, (size_t)(P1.n_chain_items + 1) * sizeof(int), e->stream)) !=
+                cudaSuccess ||
             (c = cudaMemsetAsync(e->chain_abort.p, 0, sizeof(int), e->stream)) != cudaSuccess)
             return cuda_fail(e, c, "clear chain state");
     }
@@ -1167,9 +1213,9 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uin
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     int status[2] = {0, 0};  // overflow count, chain abort flag
-    if ((c = cudaMemcpyAsync(&status[0], S.ovf_count, sizeof(int), cudaMemcpyDeviceToHost, e->stream)) != cudaSuccess ||
+    if ((c = copy_d2h(e, &status[0], S.ovf_count, sizeof(int))) != cudaSuccess ||
         (chained &&
-         (c = cudaMemcpyAsync(&status[1], e->chain_abort.p, sizeof(int), cudaMemcpyDeviceToHost, e->stream)) !=
+         (c = copy_d2h(e, &status[1], e->chain_abort.p, sizeof(int))) !=
              cudaSuccess) ||
         (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
         return cuda_fail(e, c, "read score status");
@@ -1273,9 +1319,9 @@ static cudaError_t finish_hits(pw_engine* e, int64_t n, int64_t* str_bytes) {
     if ((c = cub::DeviceScan::ExclusiveSum(e->scan_tmp.p, stmp, len, soff, (int64_t)n, e->stream)) != cudaSuccess)
         return c;
     int64_t tail[2] = {0, 0};
-    if ((c = cudaMemcpyAsync(&tail[0], soff + n - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, e->stream)) !=
+    if ((c = copy_d2h(e, &tail[0], soff + n - 1, sizeof(int64_t))) !=
             cudaSuccess ||
-        (c = cudaMemcpyAsync(&tail[1], len + n - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, e->stream)) !=
+        (c = copy_d2h(e, &tail[1], len + n - 1, sizeof(int64_t))) !=
             cudaSuccess ||
         (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
         return c;
@@ -1295,10 +1341,8 @@ static cudaError_t finish_hits(pw_engine* e, int64_t n, int64_t* str_bytes) {
     e->launches += 6;  // this library's kernels (the CUB sorts and scan are not counted)
     if ((c = cudaGetLastError()) != cudaSuccess) return c;
     if (!e->h_hits.resize((size_t)n) || !e->h_strings.resize((size_t)total)) return cudaErrorMemoryAllocation;
-    if ((c = cudaMemcpyAsync(e->h_hits.data(), e->f_out.p, (size_t)n * sizeof(pw_hit), cudaMemcpyDeviceToHost,
-                             e->stream)) != cudaSuccess ||
-        (total > 0 && (c = cudaMemcpyAsync(e->h_strings.data(), e->f_str.p, (size_t)total, cudaMemcpyDeviceToHost,
-                                           e->stream)) != cudaSuccess) ||
+    if ((c = copy_d2h(e, e->h_hits.data(), e->f_out.p, (size_t)n * sizeof(pw_hit))) != cudaSuccess ||
+        (total > 0 && (c = copy_d2h(e, e->h_strings.data(), e->f_str.p, (size_t)total)) != cudaSuccess) ||
         (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
         return c;
     *str_bytes = total;
@@ -1373,12 +1417,21 @@ static int run_band_phase(pw_engine* e, KernelArgs A, std::vector<BandPair>& pai
     const size_t n = entries.size();
     if ((c = upload(e, e->band_pairs, sorted)) != cudaSuccess) return cuda_fail(e, c, "upload band pairs");
     if ((c = upload(e, e->band_entries, entries)) != cudaSuccess) return cuda_fail(e, c, "upload band queue");
-    if ((c = e->band_prog.reserve(e->stream, n * sizeof(int))) != cudaSuccess ||
+    if (e->tune[PW_TUNE_STALL_TEST]) {
+        // one band below another waits on the spare flag (index n) instead
+        for (int4& v : entries)
+            if (v.y > 0) {
+                e->tune[PW_TUNE_STALL_TEST] = 0;
+                v.z = (int)n;
+                break;
+            }
+    }
+    if ((c = e->band_prog.reserve(e->stream, (n + 1) * sizeof(int))) != cudaSuccess ||
         (c = e->band_max.reserve(e->stream, n * sizeof(int))) != cudaSuccess ||
         (c = e->band_ring.reserve(e->stream, (size_t)std::max<int64_t>(ring_elems, 1) * sizeof(int4))) != cudaSuccess ||
         (c = e->chain_abort.reserve(e->stream, sizeof(int))) != cudaSuccess)
         return cuda_fail(e, c, "alloc band state");
-    if ((c = cudaMemsetAsync(e->band_prog.p, 0, n * sizeof(int), e->stream)) != cudaSuccess ||
+    if ((c = cudaMemsetAsync(e->band_prog.p, 0, (n + 1) * sizeof(int), e->stream)) != cudaSuccess ||
         (c = cudaMemsetAsync(e->chain_abort.p, 0, sizeof(int), e->stream)) != cudaSuccess ||
         (c = cudaMemsetAsync(e->counter.as<int>() + kNumClasses, 0, sizeof(int), e->stream)) != cudaSuccess)
         return cuda_fail(e, c, "reset band state");
@@ -1393,6 +1446,7 @@ static int run_band_phase(pw_engine* e, KernelArgs A, std::vector<BandPair>& pai
     B.run_max = e->band_max.as<int>();
     B.abort_flag = e->chain_abort.as<int>();
     B.max_out = e->band_out.as<float>();
+    B.wait_ns = wait_limit(e);
     const int grid = std::max(1, std::min(grid_cap(e, per_sm), (int)((n + 3) / 4)));
     cudaEvent_t a, b;
     cudaEventCreate(&a);
@@ -1403,7 +1457,7 @@ static int run_band_phase(pw_engine* e, KernelArgs A, std::vector<BandPair>& pai
     cudaEventRecord(b, e->stream);
     if ((c = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, c, "band sweep launch");
     int aborted = 0;
-    if ((c = cudaMemcpyAsync(&aborted, e->chain_abort.p, sizeof(int), cudaMemcpyDeviceToHost, e->stream)) != cudaSuccess ||
+    if ((c = copy_d2h(e, &aborted, e->chain_abort.p, sizeof(int))) != cudaSuccess ||
         (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
         return cuda_fail(e, c, "band sweep");
     float ms = 0;
@@ -1454,6 +1508,8 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     e->h_strings.clear();
     e->h_starts.clear();
     e->launches = 0;
+    e->h2d = e->d2h = 0;
+    e->reuse = 0;
     pw_run_info inf;
     memset(&inf, 0, sizeof(inf));
     const int nq = e->Q.n, nt = e->T.n;
@@ -1475,6 +1531,9 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         }
     }
     if (nq == 0 || nt == 0) {
+        inf.h2d_bytes = e->h2d;
+        inf.d2h_bytes = e->d2h;
+        inf.reuse = e->reuse;
         if (info) *info = inf;
         return PW_OK;
     }
@@ -1505,7 +1564,8 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     }
     const std::vector<int32_t>& list_q = pair_mode ? e->pair_q : auto_q;
     const std::vector<int32_t>& list_t = pair_mode ? e->pair_t : auto_t;
-    const bool band1 = !list_q.empty() && pr.int_path;
+    const bool band1 = !list_q.empty() && pr.int_path && !plain;
+    const bool plain_band = plain && pr.int_path;
     const bool use_s16 = !band1 && !plain && (pr.s16_q || pr.s16_t) && !(flags & PW_FLAG_INT32);
     if (band1) {
         // explicit pairs: one warp per 256-row band, bands chained (pw_band.cuh)
@@ -1533,6 +1593,38 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         cudaEventElapsedTime(&ms, e->ev[0], e->ev[1]);
         inf.score_ms = ms;
         inf.score_path = 2;
+    } else if (plain_band) {
+        // the unbatched form: one launch per (query, target) pair, as the
+        // reference launches one pair's kernels at a time, each pair on the
+        // single-pair wavefront kernel (a warp per 256-row band, the bands of
+        // a long pair chained across warps)
+        inf.score_path = 3;
+        if ((c = e->band_out.reserve(e->stream, sizeof(float))) != cudaSuccess)
+            return cuda_fail(e, c, "alloc band maxima");
+        e->h_pair_max.fill(-1.0f);
+        cudaEventRecord(e->ev[0], e->stream);
+        const size_t np = pair_mode ? e->pair_q.size() : (size_t)nq * nt;
+        for (size_t k = 0; k < np; ++k) {
+            const int q = pair_mode ? e->pair_q[k] : (int)(k / nt);
+            const int t = pair_mode ? e->pair_t[k] : (int)(k % nt);
+            std::vector<BandPair> bp(1);
+            memset(&bp[0], 0, sizeof(BandPair));
+            bp[0].q = q;
+            bp[0].t = t;
+            bp[0].nbands = tlen[t] > 0 ? (tlen[t] + kBandRows - 1) / kBandRows : 1;
+            rc = run_band_phase<false>(e, A, bp, &inf.score_kernel_ms, &inf.score_launches);
+            if (rc != PW_OK) return rc;
+            float m = 0.0f;
+            if ((c = copy_d2h(e, &m, e->band_out.p, sizeof(float))) != cudaSuccess ||
+                (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
+                return cuda_fail(e, c, "copy pair maximum");
+            e->h_pair_max[(size_t)q * nt + t] = m;
+        }
+        cudaEventRecord(e->ev[1], e->stream);
+        cudaStreamSynchronize(e->stream);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e->ev[0], e->ev[1]);
+        inf.score_ms = ms;
     } else if (use_s16) {
         cudaEventRecord(e->ev[0], e->stream);
         rc = phase1_s16(e, A, inf, flags);
@@ -1598,10 +1690,9 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         cudaEventElapsedTime(&ms, e->ev[0], e->ev[1]);
         inf.score_ms = ms;
     }
-    if (band1 && !pair_mode) {
+    if ((band1 || plain_band) && !pair_mode) {
         // the band sweep wrote host maxima only: the trace kernels read them on the device
-        if ((c = cudaMemcpyAsync(A.pair_max, e->h_pair_max.data(), e->h_pair_max.size() * sizeof(float),
-                                 cudaMemcpyHostToDevice, e->stream)) != cudaSuccess ||
+        if ((c = copy_h2d(e, A.pair_max, e->h_pair_max.data(), e->h_pair_max.size() * sizeof(float))) != cudaSuccess ||
             (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
             return cuda_fail(e, c, "upload pair maxima");
     }
@@ -1611,14 +1702,16 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         for (size_t k = 0; k < e->pair_q.size(); ++k) listed[(size_t)e->pair_q[k] * nt + e->pair_t[k]] = 1;
         for (size_t k = 0; k < listed.size(); ++k)
             if (!listed[k]) e->h_pair_max[k] = -1.0f;
-        if ((c = cudaMemcpyAsync(A.pair_max, e->h_pair_max.data(), e->h_pair_max.size() * sizeof(float),
-                                 cudaMemcpyHostToDevice, e->stream)) != cudaSuccess ||
+        if ((c = copy_h2d(e, A.pair_max, e->h_pair_max.data(), e->h_pair_max.size() * sizeof(float))) != cudaSuccess ||
             (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
             return cuda_fail(e, c, "upload pair maxima");
     }
     if (flags & PW_FLAG_SCORE_ONLY) {
         inf.kernel_launches = (int32_t)e->launches;
         inf.total_ms = wall_ms() - t_call;
+        inf.h2d_bytes = e->h2d;
+        inf.d2h_bytes = e->d2h;
+        inf.reuse = e->reuse;
         if (info) *info = inf;
         return PW_OK;
     }
@@ -1653,7 +1746,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
                   e->prune_cnt.as<unsigned long long>());
         e->launches++;
         if ((c = cudaGetLastError()) != cudaSuccess ||
-            (c = cudaMemcpyAsync(cnt, e->prune_cnt.p, sizeof(cnt), cudaMemcpyDeviceToHost, e->stream)) != cudaSuccess ||
+            (c = copy_d2h(e, cnt, e->prune_cnt.p, sizeof(cnt))) != cudaSuccess ||
             (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
             return cuda_fail(e, c, "prune pairs");
         min_pass = (int64_t)cnt[0];
@@ -1671,8 +1764,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
                                                 e->prune_sel.as<int64_t>(), d_count, npairs, e->stream)) != cudaSuccess)
                 return cuda_fail(e, c, "select passing pairs");
             if (!e->h_sel.resize((size_t)n_pass)) return fail(e, PW_ERR_NOMEM, "host memory for the passing pairs");
-            if ((c = cudaMemcpyAsync(e->h_sel.data(), e->prune_sel.p, (size_t)n_pass * sizeof(int64_t),
-                                     cudaMemcpyDeviceToHost, e->stream)) != cudaSuccess ||
+            if ((c = copy_d2h(e, e->h_sel.data(), e->prune_sel.p, (size_t)n_pass * sizeof(int64_t))) != cudaSuccess ||
                 (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
                 return cuda_fail(e, c, "copy passing pairs");
             const int64_t* sel = e->h_sel.data();
@@ -1698,7 +1790,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     // one-warp-per-pair sweep (pw_band.cuh); the others are grouped 32 to
     // a warp, one pair per lane, in the orientation where they cluster
     // (slot cost = strip length x longest lane x 32 per item).
-    const bool warp_ok = pr.int_path && !plain;
+    const bool warp_ok = pr.int_path;
     std::vector<std::pair<int32_t, int32_t>> warp_pairs;  // (query, target)
     std::vector<char> t_warp((size_t)nt, 0);              // targets whose pairs went to the warp sweep
     if (warp_ok) {
@@ -1708,7 +1800,8 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         int64_t n_short = 0;
         for (int t = 0; t < nt; ++t)
             if (tlen[t] <= 64) n_short += span_n(t);
-        const bool all_warp = n_short < (int64_t)kWarp * e->sm_count;
+        // (the unbatched form sweeps every traced pair alone on a warp)
+        const bool all_warp = plain || n_short < (int64_t)kWarp * e->sm_count;
         for (int t = 0; t < nt; ++t) {
             if (tlen[t] <= 64 && !all_warp) continue;
             for (int64_t j = pt_off[t]; j < pt_off[t + 1]; ++j) warp_pairs.push_back({pt_q[j], t});
@@ -1745,7 +1838,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
                   e->q_len.as<int32_t>(), per_item, e->prune_cnt.as<unsigned long long>());
         e->launches += 2;
         if ((c = cudaGetLastError()) != cudaSuccess ||
-            (c = cudaMemcpyAsync(&lb_units, e->prune_cnt.p, sizeof(lb_units), cudaMemcpyDeviceToHost, e->stream)) !=
+            (c = copy_d2h(e, &lb_units, e->prune_cnt.p, sizeof(lb_units))) !=
                 cudaSuccess ||
             (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
             return cuda_fail(e, c, "query counts");
@@ -1832,6 +1925,9 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     if (items2.empty()) {
         inf.kernel_launches = (int32_t)e->launches;
         inf.total_ms = wall_ms() - t_call;
+        inf.h2d_bytes = e->h2d;
+        inf.d2h_bytes = e->d2h;
+        inf.reuse = e->reuse;
         if (info) *info = inf;
         return PW_OK;
     }
@@ -1888,6 +1984,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         }
         waves.push_back({i0, items2.size()});
     }
+    inf.waves = (int32_t)waves.size();
 
     double trace_ms = 0, walk_ms = 0;
     int64_t total_starts = 0;
@@ -1981,7 +2078,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         PW_LAUNCH(cand_overflow_kernel, gslot, 256, 0, e->stream, (const int32_t*)A.n_cand, (const int32_t*)A.cand_cap,
                   n_pairs, e->prune_cnt.as<unsigned long long>());
         e->launches++;
-        if ((c = cudaMemcpyAsync(&n_over, e->prune_cnt.p, sizeof(n_over), cudaMemcpyDeviceToHost, e->stream)) !=
+        if ((c = copy_d2h(e, &n_over, e->prune_cnt.p, sizeof(n_over))) !=
                 cudaSuccess ||
             (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
             return cuda_fail(e, c, "candidate overflow count");
@@ -2091,10 +2188,8 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         cudaEventRecord(e->ev[2], e->stream);
         int64_t last_off = 0;
         int32_t last_n = 0;
-        if ((c = cudaMemcpyAsync(&last_off, e->start_off.as<int64_t>() + n_pairs - 1, sizeof(int64_t),
-                                 cudaMemcpyDeviceToHost, e->stream)) != cudaSuccess ||
-            (c = cudaMemcpyAsync(&last_n, TA.n_starts + n_pairs - 1, sizeof(int32_t), cudaMemcpyDeviceToHost,
-                                 e->stream)) != cudaSuccess ||
+        if ((c = copy_d2h(e, &last_off, e->start_off.as<int64_t>() + n_pairs - 1, sizeof(int64_t))) != cudaSuccess ||
+            (c = copy_d2h(e, &last_n, TA.n_starts + n_pairs - 1, sizeof(int32_t))) != cudaSuccess ||
             (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
             return cuda_fail(e, c, "collect");
         const int64_t wave_starts = last_off + last_n;
@@ -2107,8 +2202,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
             if ((c = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, c, "gather launch");
             if (!e->h_starts.resize_keep(first_rec + (size_t)wave_starts))
                 return fail(e, PW_ERR_NOMEM, "host memory for the starting points");
-            if ((c = cudaMemcpyAsync(e->h_starts.data() + first_rec, e->starts.p, wave_starts * sizeof(StartRec),
-                                     cudaMemcpyDeviceToHost, e->stream)) != cudaSuccess ||
+            if ((c = copy_d2h(e, e->h_starts.data() + first_rec, e->starts.p, wave_starts * sizeof(StartRec))) != cudaSuccess ||
                 (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
                 return cuda_fail(e, c, "copy starts");
         }
@@ -2141,7 +2235,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
                 return cuda_fail(e, c, "alloc hits");
             if ((c = e->hit_count.reserve(e->stream, 16)) != cudaSuccess) return cuda_fail(e, c, "alloc");
             const unsigned long long init[2] = {0ull, (unsigned long long)acc_ops};
-            if ((c = cudaMemcpyAsync(e->hit_count.p, init, sizeof(init), cudaMemcpyHostToDevice, e->stream)) !=
+            if ((c = copy_h2d(e, e->hit_count.p, init, sizeof(init))) !=
                 cudaSuccess)
                 return cuda_fail(e, c, "reset hit count");
             TA.hits = e->acc_hits.as<DevHit>() + acc_n;
@@ -2195,6 +2289,9 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     inf.kernel_launches = (int32_t)e->launches;
     inf.finish_ms = wall_ms() - t_finish;
     inf.total_ms = wall_ms() - t_call;
+    inf.h2d_bytes = e->h2d;
+    inf.d2h_bytes = e->d2h;
+    inf.reuse = e->reuse;
     if (info) *info = inf;
     return PW_OK;
 }

@@ -60,6 +60,7 @@ struct BandArgs {
     int* run_max;         // per entry: running maximum of the pair's bands so far
     int* abort_flag;
     float* max_out;       // score sweep: pair maxima, indexed by BandPair.slot
+    unsigned long long wait_ns;  // bound of one wait for the band above
 };
 
 template <bool AFFINE, bool DIRS>
@@ -158,7 +159,7 @@ __global__ void __launch_bounds__(128) band_kernel(KernelArgs A, BandArgs B) {
             if (has_up && (s & 31) == 0) {
                 const int need = (int)(s + 32 < (int64_t)lq ? s + 32 : (int64_t)lq);
                 if (avail < need) {
-                    avail = chain_wait(prog_in, need, B.abort_flag);
+                    avail = chain_wait(prog_in, need, B.abort_flag, B.wait_ns);
                     if (avail < 0) {
                         ok = false;
                         break;
@@ -309,7 +310,7 @@ __global__ void __launch_bounds__(128) band_kernel(KernelArgs A, BandArgs B) {
         if constexpr (!DIRS) mx = __reduce_max_sync(0xffffffffu, mx);
         if (has_up) {
             // the band above has finished: its running maximum and its candidates are final
-            if (chain_wait(prog_in, kChainDone, B.abort_flag) < 0) break;
+            if (chain_wait(prog_in, kChainDone, B.abort_flag, B.wait_ns) < 0) break;
             if constexpr (!DIRS) mx = max(mx, __ldcg(&B.run_max[pred]));
         }
         if (store_bnd) {

@@ -60,6 +60,7 @@ struct Score16Args {
     int n_chain_items;           // host-side bookkeeping: entries of the chained launch
     int item_base;               // chained launch: first queue entry of this launch (entries [item_base, n_items))
     int* ovf_count;              // pairs reported as NaN (16-bit limit reached)
+    unsigned long long wait_ns;  // bound of one chain wait
 };
 
 // Profile of strip rows [y0, y0 + S): for row group g (4 rows) and lane
@@ -282,7 +283,8 @@ __device__ __forceinline__ void sweep16(const uint8_t* qc, int lq4, const uint8_
 // Progress: entries are handed out in queue order and a strip waits only for
 // its predecessor, which is queued before it and so was taken by a warp that
 // is running; every wait therefore ends.  Each wait is nevertheless bounded:
-// after kChainWaitNs without progress, or when another warp has given up, the
+// after the launch's wait limit (kChainWaitNs unless the host sets another)
+// without progress, or when another warp has given up, the
 // warp sets abort_flag and stops, and the host reports the launch as failed.
 // Only the longest items are chained (the host plans the queue so that a
 // strip is handed out about when its predecessor is kChainLead columns
@@ -296,6 +298,7 @@ constexpr int kChainDone = 1 << 30;
 constexpr int kChainPublish = 32;
 constexpr int kChainLead = 64;
 constexpr int kChainNeed = 40;
+// Default bound of one wait (PW_TUNE_WAIT_NS overrides it per launch).
 constexpr unsigned long long kChainWaitNs = 2000000000ull;
 
 __device__ __forceinline__ int ld_acquire_gpu(const int* p) {
@@ -314,8 +317,9 @@ __device__ __forceinline__ unsigned long long global_ns() {
 }
 
 // Warp-uniform wait until *flag >= need.  Returns the smallest value the lanes
-// saw (>= need), or -1 when the wait gave up (abort_flag is then set).
-__device__ __forceinline__ int chain_wait(const int* flag, int need, int* abort_flag) {
+// saw (>= need), or -1 when the wait gave up after limit_ns without success or
+// because another warp had given up (abort_flag is then set).
+__device__ __forceinline__ int chain_wait(const int* flag, int need, int* abort_flag, unsigned long long limit_ns) {
     int v = ld_acquire_gpu(flag);
     if (__all_sync(0xffffffffu, v >= need)) return __reduce_min_sync(0xffffffffu, v);
     const unsigned long long t0 = global_ns();
@@ -325,7 +329,7 @@ __device__ __forceinline__ int chain_wait(const int* flag, int need, int* abort_
         if (ns < 1024) ns <<= 1;
         v = ld_acquire_gpu(flag);
         if (__all_sync(0xffffffffu, v >= need)) return __reduce_min_sync(0xffffffffu, v);
-        const bool give_up = ld_acquire_gpu(abort_flag) != 0 || global_ns() - t0 > kChainWaitNs;
+        const bool give_up = ld_acquire_gpu(abort_flag) != 0 || global_ns() - t0 > limit_ns;
         if (__any_sync(0xffffffffu, give_up)) {
             if ((threadIdx.x & 31) == 0) atomicExch(abort_flag, 1);
             return -1;
@@ -348,12 +352,13 @@ template <int S, bool AFFINE, bool DL>
 __device__ __forceinline__ bool sweep16_chain(const uint8_t* qc, int lq4, const uint8_t* qc2, int lq42, int xm4,
                                               uint32_t pad4, const void* prof, int alpha1, int gap, int ext, int ge,
                                               bool has_up, bool has_down, const uint4* ring_in, uint4* ring_out,
-                                              const int* prog_in, int* prog_out, int* abort_flag, uint32_t& mx) {
+                                              const int* prog_in, int* prog_out, int* abort_flag,
+                                              unsigned long long wait_ns, uint32_t& mx) {
     const uint32_t g2 = pack16(gap), e2 = pack16(ext), ge2 = pack16(ge), nge2 = pack16(-ge);
     int avail = 0;  // columns of the predecessor known to be published
     auto need_cols = [&](int upto) -> bool {  // columns [0, upto) of ring_in readable
         if (!has_up || avail >= upto) return true;
-        avail = chain_wait(prog_in, upto, abort_flag);
+        avail = chain_wait(prog_in, upto, abort_flag, wait_ns);
         return avail >= 0;
     };
     auto code_word = [&](int x4) -> uint32_t { return x4 < lq4 ? *(const uint32_t*)(qc + x4) : pad4; };
@@ -563,11 +568,12 @@ __global__ void __launch_bounds__(128, 3) score16_chain_kernel(Score16Args A) {
             const bool has_down = s + 1 < nstrips;
             if (!sweep16_chain<S, AFFINE, DL>(L.qc, L.lq4, L.qc2, L.lq42, xm4, pad4, prof, A.alpha1, A.gap, A.ext,
                                               A.ge, s > 0, has_down, ring_in, ring_out,
-                                              s > 0 ? A.progress + pred : nullptr, A.progress + it, A.abort_flag, mx))
+                                              s > 0 ? A.progress + pred : nullptr, A.progress + it, A.abort_flag,
+                                              A.wait_ns, mx))
                 break;
             if (s > 0) {
                 // the predecessor's running maximum is final once it has finished
-                if (chain_wait(A.progress + pred, kChainDone, A.abort_flag) < 0) break;
+                if (chain_wait(A.progress + pred, kChainDone, A.abort_flag, A.wait_ns) < 0) break;
                 mx = __vmaxs2(mx, __ldcg(&A.run_max[(int64_t)pred * kWarp + lane]));
             }
             if (has_down) {

@@ -57,6 +57,40 @@ def _filter_factor(settings):
         raise InvalidOptionException("Filterfactor should be a float but is {0}".format(ff))
 
 
+def _packed(records):
+    """(residues uint8, offsets int64) of the records' upper-cased sequences."""
+    seqs = [str(r.seq) for r in records]
+    lens = np.fromiter(map(len, seqs), dtype=np.int64, count=len(seqs))
+    off = np.zeros(len(seqs) + 1, dtype=np.int64)
+    np.cumsum(lens, out=off[1:])
+    text = "".join(seqs).upper()
+    if len(text) != off[-1]:  # a character whose upper case is longer: per record
+        text = "".join(s.upper() for s in seqs)
+        lens = np.fromiter((len(s.upper()) for s in seqs), dtype=np.int64, count=len(seqs))
+        np.cumsum(lens, out=off[1:])
+    data = text.encode("latin-1")
+    return np.frombuffer(data, dtype=np.uint8) if data else np.zeros(0, np.uint8), off
+
+
+def _hitbuild():
+    """The native Hit builder (pypaswas_b200/_hitbuild*.so, csrc/hitbuild.c)."""
+    try:
+        from . import _hitbuild as mod
+    except ImportError as exc:
+        raise ImportError("pypaswas_b200._hitbuild is not built: run python -m pypaswas_b200.build") from exc
+    return mod
+
+
+def _logs_hits(hit_list):
+    """HitList.append logs every added (INFO) and rejected (DEBUG) hit; the
+    native builder is used only when neither record would be emitted."""
+    lg = hit_list.logger
+    if lg is None:
+        return False
+    enabled = getattr(lg, "isEnabledFor", None)
+    return enabled is None or enabled(logging.INFO) or enabled(logging.DEBUG)
+
+
 class SmithWatermanB200(object):
     """Drop-in for SmithWatermanCuda: same constructor and driver methods."""
 
@@ -98,16 +132,15 @@ class SmithWatermanB200(object):
         return target_index + self.number_of_targets
 
     def _upload(self, records_seqs, targets, target_index):
-        """Hands the records to the engine (copy_sequences, SmithWatermanCuda.py:176-184);
-        returns the target block and the bytes sent to the device."""
+        """Hands the records to the engine (copy_sequences, SmithWatermanCuda.py:176-184):
+        upper-cased residues of each list concatenated, with offsets and id
+        keys.  The device copy happens in the engine's next pw_align.
+        Returns the target block."""
         block = targets[target_index:target_index + self.number_targets]
         qkeys, tkeys = id_keys([r.id for r in records_seqs], [r.id for r in block])
-        qs = [str(r.seq).upper().encode("latin-1") for r in records_seqs]
-        ts = [str(r.seq).upper().encode("latin-1") for r in block]
-        self.engine.set_queries(qs, qkeys)
-        self.engine.set_targets(ts, tkeys)
-        h2d = sum(map(len, qs)) + sum(map(len, ts)) + 12 * (len(qs) + len(ts)) + 16
-        return block, h2d
+        self.engine.set_queries_packed(*_packed(records_seqs), qkeys)
+        self.engine.set_targets_packed(*_packed(block), tkeys)
+        return block
 
     def align_sequences(self, records_seqs, targets, target_index):
         """Aligns every record against the current target block; returns a HitList."""
@@ -117,7 +150,7 @@ class SmithWatermanB200(object):
         if len(records_seqs) == 0 or self.number_targets == 0:
             return hitlist
         t0 = time.time()
-        block, h2d = self._upload(records_seqs, targets, target_index)
+        block = self._upload(records_seqs, targets, target_index)
         cap = self.maximum_number_starting_points * len(records_seqs) * len(block)
         info = self.engine.align(start_cap=cap)
         self.last_info = info
@@ -125,8 +158,8 @@ class SmithWatermanB200(object):
             self.logger.warning("Too many hits returned. Skipping the rest. Please set lower_limit_score "
                                 "higher in config.")
         hits, strbuf = self.engine.hits()
-        self.last_h2d_bytes = h2d
-        self.last_d2h_bytes = 4 * len(records_seqs) * len(block) + hits.nbytes + len(strbuf)
+        self.last_h2d_bytes = int(info.h2d_bytes)  # counted by the engine, copy by copy
+        self.last_d2h_bytes = int(info.d2h_bytes)
         self._build_hits(hits, strbuf, records_seqs, block, hitlist)
         self._progress(records_seqs, block, t0)
         return hitlist
@@ -140,15 +173,15 @@ class SmithWatermanB200(object):
         if len(records_seqs) == 0 or self.number_targets == 0:
             return np.zeros(0, dtype=_native.HIT_DTYPE), b"", []
         t0 = time.time()
-        block, h2d = self._upload(records_seqs, targets, target_index)
+        block = self._upload(records_seqs, targets, target_index)
         info = self.engine.align(start_cap=self.maximum_number_starting_points * len(records_seqs) * len(block))
         self.last_info = info
         if info.truncated:
             self.logger.warning("Too many hits returned. Skipping the rest. Please set lower_limit_score "
                                 "higher in config.")
         hits, strbuf = self.engine.hits()
-        self.last_h2d_bytes = h2d
-        self.last_d2h_bytes = 4 * len(records_seqs) * len(block) + hits.nbytes + len(strbuf)
+        self.last_h2d_bytes = int(info.h2d_bytes)  # counted by the engine, copy by copy
+        self.last_d2h_bytes = int(info.d2h_bytes)
         self._progress(records_seqs, block, t0)
         return hits, strbuf, block
 
@@ -163,11 +196,25 @@ class SmithWatermanB200(object):
         n_hits = len(hits)
         if n_hits == 0:
             return
-        q_col, t_col = hits["query"].astype(np.int64), hits["target"].astype(np.int64)
         sp = np.array([getattr(r, "start_position", 0) for r in sequences], dtype=np.int64)
         tp = np.array([getattr(r, "start_position", 0) for r in targets], dtype=np.int64)
         qlen = np.array([r.original_length for r in sequences], dtype=np.int64)
         tlen = np.array([r.original_length for r in targets], dtype=np.int64)
+        if type(hit_list) is HitList and not _logs_hits(hit_list):
+            # the same objects, built in native code (csrc/hitbuild.c); None
+            # means an invalid location, reported below by the checked path
+            kept = _hitbuild().build(np.ascontiguousarray(hits, dtype=_native.HIT_DTYPE), bytes(strbuf),
+                                     list(sequences), list(targets), [r.id for r in sequences],
+                                     [r.id for r in targets], qlen, tlen, sp, tp, self._filter_thresholds(), Hit,
+                                     self.logger, hit_list.hits, hit_list.real_hits)
+            if kept is not None:
+                return
+        self._build_hits_python(hits, strbuf, sequences, targets, hit_list, sp, tp, qlen, tlen)
+
+    def _build_hits_python(self, hits, strbuf, sequences, targets, hit_list, sp, tp, qlen, tlen):
+        """_build_hits in the interpreter: HitLists of other classes, loggers
+        that record every append, and inputs with an invalid location."""
+        q_col, t_col = hits["query"].astype(np.int64), hits["target"].astype(np.int64)
         s0 = hits["s_start"].astype(np.int64) + sp[q_col]
         s1 = hits["s_end"].astype(np.int64) + sp[q_col]
         t0 = hits["t_start"].astype(np.int64) + tp[t_col]

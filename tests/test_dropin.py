@@ -169,3 +169,55 @@ def test_formatter_for_names_every_output_format():
     assert formatter_for("trimmedFasta") is TrimmerFormatter and formatter_for("FASTA") is FastaFormatter
     with pytest.raises(InvalidOptionException):
         formatter_for("graphml")
+
+
+def _hit_state(hl):
+    def rec(h):
+        d = dict(vars(h))
+        d["sequence_info"] = id(d["sequence_info"])
+        d["target_info"] = id(d["target_info"])
+        return tuple(sorted(d.items(), key=lambda kv: kv[0]))
+    return ([(k, rec(h)) for k, h in hl.hits.items()], [(k, rec(h)) for k, h in hl.real_hits.items()])
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_native_hit_builder_equals_the_interpreter_path(seed):
+    """csrc/hitbuild.c builds the same Hit objects and HitList dicts (keys,
+    order, replacement rule, filter) as the Python loop, on records whose
+    start and end keys collide with different scores."""
+    rng = np.random.default_rng(seed)
+    queries = [SeqRecord("ACGT" * int(rng.integers(20, 40)), "q%d" % (i % 5)) for i in range(9)]
+    targets = [SeqRecord("TTGCA" * int(rng.integers(10, 30)), "t%d" % (i % 4)) for i in range(7)]
+    queries[2].start_position = 3
+    n = 600
+    hits = np.zeros(n, dtype=_native.HIT_DTYPE)
+    text = []
+    off = 0
+    for k in range(n):
+        q, t = int(rng.integers(0, 9)), int(rng.integers(0, 7))
+        lq = len(queries[q].seq) - queries[q].start_position
+        lt = len(targets[t].seq)
+        s0 = int(rng.integers(0, 4))
+        t0 = int(rng.integers(0, 4))
+        ncol = int(rng.integers(2, 12))
+        s1 = min(s0 + ncol - 1 + int(rng.integers(0, 2)), lq - 1)
+        t1 = min(t0 + ncol - 1, lt - 1)
+        hits[k] = (q, t, s0, s1, t0, t1, float(rng.integers(1, 30)), int(rng.integers(0, ncol)),
+                   int(rng.integers(0, 3)), ncol, off)
+        for _ in range(3):
+            text.append("".join("ACGT|. -"[i] for i in rng.integers(0, 8, ncol)))
+        off += 3 * ncol
+    strbuf = "".join(text).encode("latin-1")
+    st = G.FixtureSettings(G.load("dna_linear_0"))
+    st.relative_score, st.query_identity = "0.1", "0.2"  # the filter drops some
+    sw = SmithWatermanB200.__new__(SmithWatermanB200)
+    sw.logger, sw.settings = None, st
+    native, python = HitList(None), HitList(None)
+    sw._build_hits(hits, strbuf, queries, targets, native)
+    sp = np.array([r.start_position for r in queries], np.int64)
+    tp = np.zeros(len(targets), np.int64)
+    ql = np.array([r.original_length for r in queries], np.int64)
+    tl = np.array([r.original_length for r in targets], np.int64)
+    sw._build_hits_python(hits, strbuf, queries, targets, python, sp, tp, ql, tl)
+    assert 0 < len(native.real_hits) < n
+    assert _hit_state(native) == _hit_state(python)
