@@ -18,8 +18,9 @@ Legs of every configuration:
             (PW_FLAG_REPLAN); CUDA events around each step, L2 flushed between
             steps
   e2e       the same metric through the public driver API with host records:
-            Aligner.process -> HitList (Trimmer.trimmed_fasta -> text for the
-            trimmer), inputs alternating between two seeded sets of the same
+            Aligner.process -> HitList (for the trimmer: FASTA text -> native
+            reader -> Trimmer.trimmed_fasta -> text), inputs alternating between
+            two seeded sets of the same
             shape so that every step copies and prepares its inputs anew; the
             bytes are the engine's own count of its host<->device copies
   plain     the unbatched form (one pair per launch) against the batched
@@ -52,7 +53,7 @@ import numpy as np  # noqa: E402
 # recurrences: linear/affine, score only / with direction classification
 OPS_PER_CELL = {("linear", "score"): 5, ("linear", "dirs"): 8, ("affine", "score"): 10, ("affine", "dirs"): 14}
 # the trimmer workload's end-to-end leg aligns this many reads per step
-E2E_READS = 200_000
+E2E_READS = 2_000_000
 NAMES = {1: "C1", 2: "C2", 3: "C3", 4: "C4"}
 
 
@@ -324,24 +325,45 @@ def _e2e_calls(w):
     return [([qs[qi]], t) for qi, t in sorted(per_q.items())]
 
 
+def _fasta_bytes(w):
+    """The trimmer workload as the two FASTA files a user hands the program:
+    (reads, adapters) as bytes."""
+    n = w.reads.shape[0]
+    lines = []
+    for i in range(n):
+        lines.append(b">" + str(w.read_ids[i]).encode())
+        lines.append(w.reads[i].tobytes())
+    reads = b"\n".join(lines) + b"\n"
+    adapters = b"".join(b">%s\n%s\n" % (i.encode(), s) for i, s in w.targets if not i.endswith("_RC"))
+    return reads, adapters
+
+
 def e2e_leg(ws, steps, device, trimmer):
-    """The public driver API with host records; step k runs input set
+    """The public driver API with host inputs; step k runs input set
     ws[k % len(ws)] (two sets: every step's inputs are new to the engine).
-    Returns (GCUPS, seconds, h2d bytes per step, d2h bytes per step, reuse bits seen)."""
+    Aligner: records -> Aligner.process -> HitList.  Trimmer: FASTA text ->
+    native reader (reads sorted, adapters with their reverse complements)
+    -> Trimmer.trimmed_fasta -> trimmedFasta text.
+    Returns (cells, seconds, h2d bytes per step, d2h bytes per step, reuse bits seen)."""
     import torch
+    from pypaswas_b200 import readers, scores
     from pypaswas_b200.programs import Aligner, Trimmer
-    sets = [(_e2e_calls(w), w.cells) for w in ws]
-    prog = (Trimmer if trimmer else Aligner)(None, None, ws[0].settings, device=device)
+    st = ws[0].settings
+    sets = [(_fasta_bytes(w) if trimmer else _e2e_calls(w), w.cells) for w in ws]
+    prog = (Trimmer if trimmer else Aligner)(None, None, st, device=device)
     sw = prog.smith_waterman
+    score = scores.make_score(st)
 
     def step(calls):
         h2d = d2h = 0
         reuse = 0
+        if trimmer:
+            q = readers.read_query_records(st, calls[0])
+            t = readers.read_target_records(st, score, calls[1])
+            prog.trimmed_fasta(q, t)  # the program's output text, natively
+            return sw.last_h2d_bytes, sw.last_d2h_bytes, int(sw.last_info.reuse)
         for qs, ts in calls:
-            if trimmer:
-                prog.trimmed_fasta(qs, ts)  # the program's output text, natively (Trimmer.trimmed_fasta)
-            else:
-                prog.process(qs, ts, None)  # HitList of Hit objects
+            prog.process(qs, ts, None)  # HitList of Hit objects
             h2d += sw.last_h2d_bytes
             d2h += sw.last_d2h_bytes
             reuse |= int(sw.last_info.reuse)
@@ -649,7 +671,8 @@ def run_config(cfg, args, device, world, flush, sampler, headline):
         rec["e2e"] = {"value": whole_job_gcups(cells / steps_e2e, steps_e2e, dt, world if headline else 1),
                       "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                       "steps": steps_e2e, "ms_per_step": dt * 1e3 / steps_e2e,
-                      "api": "Trimmer.trimmed_fasta (records -> trimmedFasta text)" if cfg == 4 else
+                      "api": "FASTA text -> readers (native) -> Trimmer.trimmed_fasta -> trimmedFasta text"
+                             if cfg == 4 else
                              ("Aligner.process per query (records -> HitList)" if w.pairs is not None else
                               "Aligner.process (records -> HitList)"),
                       "inputs": "two seeded input sets of the same shape, alternating: every step copies and "

@@ -397,7 +397,8 @@ int pw_txt_records(const pw_hit* hits, int64_t n_hits, int32_t n_queries, int32_
 #define PW_RECORDS_RC_ONLY 2        /* complement_records_only: the reverse complements alone */
 #define PW_RECORDS_APPEND_REVERSED 3 /* reverse_records: + reversed copies */
 typedef struct pw_records pw_records;
-/* Parses `bytes` of FASTA / FASTQ text; end < 0 reads to the last record.
+/* Parses `bytes` of FASTA / FASTQ text; end < 0 reads to the last record, an
+ * end before start selects no record (as islice does).
  * Malformed FASTQ fails with PW_ERR_ARG and a message in err. */
 int pw_records_parse(const char* data, int64_t bytes, int format, int64_t start, int64_t end, int64_t limit_length,
                      int transform, int sort_desc, pw_records** out, char* err, int32_t err_bytes);

@@ -88,12 +88,17 @@ void first_word(const char* b, const char* e, int64_t& wb, int64_t& wl, const ch
 
 // appends a sequence line: spaces and carriage returns removed
 inline void append_seq(std::vector<uint8_t>& seq, const char* b, const char* e) {
-    for (const char* c = b; c < e; ++c)
-        if (*c != ' ' && *c != '\r') seq.push_back((uint8_t)*c);
+    while (b < e) {
+        const char* c = b;
+        while (c < e && *c != ' ' && *c != '\r') ++c;
+        seq.insert(seq.end(), (const uint8_t*)b, (const uint8_t*)c);  // the run up to the next removed byte
+        b = c < e ? c + 1 : e;
+    }
 }
 
 int parse_fasta(const char* data, int64_t n, std::vector<Rec>& recs, std::vector<uint8_t>& seq) {
     Lines L{data, data + n};
+    seq.reserve((size_t)n);
     const char *b, *e;
     bool in_rec = false;
     while (L.next(b, e)) {
@@ -164,17 +169,19 @@ int parse_fastq(const char* data, int64_t n, std::vector<Rec>& recs, std::vector
 }
 
 // IUPAC complement (case kept), the table the reverse-complement targets use
-uint8_t complement(uint8_t c) {
-    static uint8_t table[256];
-    static bool init = false;
-    if (!init) {
-        for (int i = 0; i < 256; ++i) table[i] = (uint8_t)i;
+struct ComplementTable {
+    uint8_t t[256];
+    ComplementTable() {
+        for (int i = 0; i < 256; ++i) t[i] = (uint8_t)i;
         const char* from = "ACGTUNKMRYSWBDHVacgtunkmryswbdhv";
         const char* to = "TGCAANMKYRSWVHDBtgcaanmkyrswvhdb";
-        for (int i = 0; from[i]; ++i) table[(uint8_t)from[i]] = (uint8_t)to[i];
-        init = true;
+        for (int i = 0; from[i]; ++i) t[(uint8_t)from[i]] = (uint8_t)to[i];
     }
-    return table[c];
+};
+
+uint8_t complement(uint8_t c) {
+    static const ComplementTable table;  // initialised once, thread-safe
+    return table.t[c];
 }
 
 int build(const char* data, int64_t n, int format, int64_t start, int64_t end, int64_t limit_length,
@@ -182,8 +189,8 @@ int build(const char* data, int64_t n, int format, int64_t start, int64_t end, i
     if (!out) return report(err, err_bytes, PW_ERR_ARG, "no output handle");
     *out = nullptr;
     if (n < 0 || (n > 0 && !data)) return report(err, err_bytes, PW_ERR_ARG, "bad input buffer");
-    if (start < 0 || (end >= 0 && end < start))
-        return report(err, err_bytes, PW_ERR_ARG, "bad record range [%lld, %lld)", (long long)start, (long long)end);
+    // islice(records, start, end): an end before the start selects nothing
+    if (start < 0) return report(err, err_bytes, PW_ERR_ARG, "bad record range start %lld", (long long)start);
     if (transform < PW_RECORDS_AS_READ || transform > PW_RECORDS_APPEND_REVERSED)
         return report(err, err_bytes, PW_ERR_ARG, "unknown record transform %d", transform);
     std::vector<Rec> recs;
@@ -198,7 +205,7 @@ int build(const char* data, int64_t n, int format, int64_t start, int64_t end, i
     if (rc != PW_OK) return rc;
     // islice(records, start, end)
     const int64_t total = (int64_t)recs.size();
-    const int64_t r0 = std::min(start, total), r1 = end < 0 ? total : std::min(end, total);
+    const int64_t r0 = std::min(start, total), r1 = end < 0 ? total : std::max(r0, std::min(end, total));
     pw_records* R = new pw_records();
     std::vector<int64_t> keep;
     keep.reserve((size_t)(r1 - r0));
@@ -249,11 +256,14 @@ int build(const char* data, int64_t n, int format, int64_t start, int64_t end, i
         R->off[j] = p;
         const uint8_t* s = seq.data() + r.seq_begin;
         uint8_t* d = R->res.data() + p;
-        for (int64_t k = 0; k < r.seq_len; ++k) {
-            // SWSeqRecord upper-cases; the complement of an upper-case residue is upper case
-            const uint8_t c = kind[i] == 0 ? s[k] : s[r.seq_len - 1 - k];
-            const uint8_t v = kind[i] == 1 ? complement(c) : c;
-            d[k] = (v >= 'a' && v <= 'z') ? (uint8_t)(v - 32) : v;
+        // SWSeqRecord upper-cases; the complement of an upper-case residue is upper case
+        auto upper = [](uint8_t v) { return (v >= 'a' && v <= 'z') ? (uint8_t)(v - 32) : v; };
+        if (kind[i] == 0) {
+            for (int64_t k = 0; k < r.seq_len; ++k) d[k] = upper(s[k]);
+        } else if (kind[i] == 1) {
+            for (int64_t k = 0; k < r.seq_len; ++k) d[k] = upper(complement(s[r.seq_len - 1 - k]));
+        } else {
+            for (int64_t k = 0; k < r.seq_len; ++k) d[k] = upper(s[r.seq_len - 1 - k]);
         }
         p += r.seq_len;
         R->id_off[j] = q;

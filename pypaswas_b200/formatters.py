@@ -48,6 +48,12 @@ def trimmed_record(hit):
     return "".join((">", _strip_rc(hit.get_target_id()), " ", hit.sequence_info.id, "\n", seq[:t0], seq[t1 + 1:]))
 
 
+def _is_packed(records):
+    """Records given as one packed set (residues, offsets, ids; see
+    pypaswas_b200.readers.RecordSet) instead of a list of record objects."""
+    return hasattr(records, "id_blob") and hasattr(records, "residues")
+
+
 def _record_arrays(sequences, targets, settings, strip_target_rc):
     """Per-record inputs of the native formatters: id ranks in Python's
     order, lengths, start positions, id bytes, thresholds."""
@@ -78,13 +84,18 @@ def _record_arrays(sequences, targets, settings, strip_target_rc):
         np.cumsum(lens, out=off[1:])
         return np.frombuffer(data or b"\0", dtype=np.uint8), off
 
-    qids, tids = [r.id for r in sequences], [r.id for r in targets]
-    q = (ranks(qids), np.array([r.original_length for r in sequences], dtype=np.int64),
-         np.array([getattr(r, "start_position", 0) for r in sequences], dtype=np.int64)) + \
-        blob([str(i) for i in qids])
-    t = (ranks(tids), np.array([r.original_length for r in targets], dtype=np.int64),
-         np.array([getattr(r, "start_position", 0) for r in targets], dtype=np.int64)) + \
-        blob([_strip_rc(str(i)) if strip_target_rc else str(i) for i in tids])
+    def arrays(records, strip_rc):
+        if _is_packed(records):  # packed records (pypaswas_b200.readers): no per-record objects
+            ids = records.ids
+            b = blob([_strip_rc(i) for i in ids]) if strip_rc else (records.id_blob, records.id_offsets)
+            return (ranks(ids), records.lengths.astype(np.int64), np.zeros(len(ids), dtype=np.int64)) + tuple(b)
+        ids = [r.id for r in records]
+        return (ranks(ids), np.array([r.original_length for r in records], dtype=np.int64),
+                np.array([getattr(r, "start_position", 0) for r in records], dtype=np.int64)) + \
+            blob([_strip_rc(str(i)) if strip_rc else str(i) for i in ids])
+
+    q = arrays(sequences, False)
+    t = arrays(targets, strip_target_rc)
     thr = np.array([float(settings.relative_score), float(settings.query_identity),
                     float(settings.query_coverage), float(settings.base_score)], dtype=np.float64)
     return q, t, thr, blob
@@ -160,11 +171,16 @@ def trimmed_fasta(hits, sequences, targets, settings, lib=None):
     from .exceptions import InvalidOptionException
     lib = lib if lib is not None else _native.load_library()
     hits = np.ascontiguousarray(hits, dtype=_native.HIT_DTYPE)
-    qseqs = [str(r.seq) for r in sequences]
-    if not "".join(qseqs).isascii():
-        raise InvalidOptionException("trimmed_fasta needs ASCII sequences")
     q, t, thr, blob = _record_arrays(sequences, targets, settings, True)
-    q_seq, q_seq_off = blob(qseqs)
+    if _is_packed(sequences):
+        q_seq, q_seq_off = sequences.residues, sequences.offsets
+        if len(q_seq) and int(q_seq.max()) >= 128:
+            raise InvalidOptionException("trimmed_fasta needs ASCII sequences")
+    else:
+        qseqs = [str(r.seq) for r in sequences]
+        if not "".join(qseqs).isascii():
+            raise InvalidOptionException("trimmed_fasta needs ASCII sequences")
+        q_seq, q_seq_off = blob(qseqs)
     vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)
     head = (vp(hits) if len(hits) else None, len(hits), len(sequences), len(targets))
     tail = tuple(vp(a) for a in q) + (vp(q_seq), vp(q_seq_off)) + tuple(vp(a) for a in t) + (vp(thr),)

@@ -8,9 +8,17 @@ from .scores import make_score
 from .smith_waterman import SmithWatermanB200
 
 
+def _is_packed(records):
+    return hasattr(records, "id_blob") and hasattr(records, "residues")
+
+
 def _one_block(program, records_seqs, targets, max_length=None):
     """The driver's single target block (the engine takes every target):
-    the engine's hit records, their strings and the block."""
+    the engine's hit records, their strings and the block.  Records given as
+    packed sets (pypaswas_b200.readers.RecordSet) go to the engine as they are."""
+    if _is_packed(records_seqs) and _is_packed(targets):
+        hits, strbuf = program.smith_waterman.align_packed(records_seqs, targets)
+        return hits, strbuf, targets
     all_targets_length = sum(len(s.seq) for s in targets)
     all_sequences_length = sum(len(s.seq) for s in records_seqs)
     program.smith_waterman.set_total_work_size(all_targets_length * all_sequences_length)
@@ -47,7 +55,8 @@ class Aligner(object):
     def txt(self, records_seqs, targets):
         """The TXT output of process() + DefaultFormatter, byte for byte, with
         the HitList and the records built in native code
-        (formatters.txt_records)."""
+        (formatters.txt_records).  Records: lists of record objects, or packed
+        record sets (pypaswas_b200.readers)."""
         from .formatters import txt_records
         if len(targets) == 0:
             return ""
@@ -77,10 +86,12 @@ class Trimmer(Aligner):
         """The trimmedFasta output of process() + TrimmerFormatter, byte for
         byte, with the HitList and the records built in native code
         (formatters.trimmed_fasta).  The engine takes every target in one
-        block, so the per-block HitList merge does not arise."""
+        block, so the per-block HitList merge does not arise.  Records: lists
+        of record objects, or packed record sets (pypaswas_b200.readers)."""
         from .formatters import trimmed_fasta
         if len(targets) == 0:
             return ""
-        max_length = len(targets[0]) if getattr(self.settings, "recompile", "T") == "F" else None
+        max_length = len(targets[0]) if getattr(self.settings, "recompile", "T") == "F" and \
+            not _is_packed(targets) else None
         hits, _, block = _one_block(self, records_seqs, targets, max_length)
         return trimmed_fasta(hits, records_seqs, block, self.settings)

@@ -72,6 +72,25 @@ class RecordSet(object):
         return self._records
 
 
+def concat(sets):
+    """One RecordSet of several, in order (offsets shifted)."""
+    if len(sets) == 1:
+        return sets[0]
+    res = np.concatenate([s.residues for s in sets]) if sets else np.zeros(0, np.uint8)
+    blob = np.concatenate([s.id_blob for s in sets]) if sets else np.zeros(0, np.uint8)
+    off, id_off = [np.zeros(1, np.int64)], [np.zeros(1, np.int64)]
+    r0 = i0 = 0
+    for s in sets:
+        off.append(s.offsets[1:] + r0)
+        id_off.append(s.id_offsets[1:] + i0)
+        r0 += int(s.offsets[-1])
+        i0 += int(s.id_offsets[-1])
+    out = RecordSet(res, np.concatenate(off), blob, np.concatenate(id_off), sum(s.dropped for s in sets))
+    if all(s._ids is not None for s in sets):
+        out._ids = [i for s in sets for i in s._ids]
+    return out
+
+
 def _from_handle(lib, h):
     n, nres, nid, dropped = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
     try:

@@ -185,6 +185,22 @@ class SmithWatermanB200(object):
         self._progress(records_seqs, block, t0)
         return hits, strbuf, block
 
+    def align_packed(self, queries, targets):
+        """One engine call on packed record sets (pypaswas_b200.readers.RecordSet):
+        all queries against all targets; returns the hit records (walk order)
+        and their strings, without Python record or Hit objects."""
+        qk, tk = id_keys(queries.ids, targets.ids)
+        self.engine.set_queries_packed(queries.residues, queries.offsets, qk)
+        self.engine.set_targets_packed(targets.residues, targets.offsets, tk)
+        info = self.engine.align(start_cap=self.maximum_number_starting_points * len(queries) * len(targets))
+        self.last_info = info
+        if info.truncated:
+            self.logger.warning("Too many hits returned. Skipping the rest. Please set lower_limit_score "
+                                "higher in config.")
+        self.last_h2d_bytes = int(info.h2d_bytes)
+        self.last_d2h_bytes = int(info.d2h_bytes)
+        return self.engine.hits()
+
     def _build_hits(self, hits, strbuf, sequences, targets, hit_list):
         """Hit objects in walk order (SmithWaterman._print_alignments :822-838).
 

@@ -46,6 +46,8 @@ def test_start_end_slice_before_the_filter():
     # a slice whose records are all filtered out is not an error (Readers.py:105-114)
     rs = readers.read_records(FASTA, "fasta", 4, 5, 100, _native.PW_RECORDS_AS_READ, False)
     assert len(rs) == 0 and rs.dropped == 1
+    with pytest.raises(ReaderException):  # islice(it, 2, 1) selects nothing
+        readers.read_records(FASTA, "fasta", 2, 1, 100, _native.PW_RECORDS_AS_READ, False)
 
 
 def test_targets_get_reverse_complements_and_a_stable_length_sort():
