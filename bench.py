@@ -753,6 +753,7 @@ def run_reference(args):
         if i >= args.warmup:
             steps.append(rec)
     v = float(np.median([s["value"] for s in steps]))
+    kernels = reference_kernels(args.config, procs)
     line = {"impl": "reference", "metric": "GCUPS", "value": v, "unit": "GCUPS", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -761,9 +762,28 @@ def run_reference(args):
             "cpu_baseline": {"value": v, "unit": "GCUPS", "cores": procs, "kind": "port",
                              "sample": steps[0]["sample"]},
             "e2e": {"value": v, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "note": "CPU restatement of the reference path (oracle/paswas_oracle.c) over all host cores"}
+            "reference_kernels": kernels,
+            "note": "value: the CPU restatement of the reference path (oracle/paswas_oracle.c) over all host cores, "
+                    "the faster of the two CPU timings here; reference_kernels: the reference's own OpenCL CPU "
+                    "kernels under a work-item emulation (oracle/ref), once, on a fixed sample"}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def reference_kernels(cfg, threads):
+    """The reference's own OpenCL CPU kernels (oracle/ref/ocl_cpu_arm.py) on
+    the configuration's fixed sample, when they were built; else why not."""
+    sys.path.insert(0, os.path.join(REPO, "oracle", "ref"))
+    try:
+        import ocl_cpu_arm
+    except ImportError as exc:
+        return {"unavailable": str(exc)}
+    if not ocl_cpu_arm.available(cfg):
+        return {"unavailable": "kernels not built (built where the reference tree is present)"}
+    r = ocl_cpu_arm.time_sample(cfg, threads)
+    return {"value": r["value"], "unit": "GCUPS", "cores": r["threads"], "kind": "reference",
+            "sample": r["sample"], "seconds": r["seconds"], "starting_points": r["starting_points"],
+            "execution": "work-groups over host threads, work-items as fibers switched at barriers"}
 
 
 if __name__ == "__main__":

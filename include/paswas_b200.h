@@ -218,6 +218,11 @@ int pw_set_wave_limit(pw_engine* e, int64_t bytes);
  *                       runs out (PW_TUNE_WAIT_NS) and pw_align reports the
  *                       failure; a test of the bounded waits.  0: off */
 #define PW_TUNE_STALL_TEST 6
+/*   PW_TUNE_LANES       score sweep lane width: 32 runs it on 32-bit lanes as
+ *                       PW_FLAG_INT32 does; 0 the 16x2 sweep wherever the
+ *                       scores allow it (pairs that reach the 16-bit limit are
+ *                       recomputed on 32-bit lanes either way) */
+#define PW_TUNE_LANES 7
 int pw_set_tuning(pw_engine* e, int key, int64_t value);
 
 /* Pair maxima (the last block of the maxima chain, default_main.cu:591),

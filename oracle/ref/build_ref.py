@@ -90,6 +90,39 @@ extern "C" void emu_tracebackAffineGap(unsigned gx, unsigned gy, void* m, void* 
 """
 
 
+# The reference host driver's launch loops (SmithWaterman._calculate_score,
+# SmithWaterman.py:591-618, and _traceback_host, :626-655) over the OpenCL CPU
+# kernels, with SmithWatermanCPU's launch shapes (SmithWatermanOcl.py:459-511):
+# one call runs a whole batch.
+_OCL_CPU_LOOPS = r"""
+extern "C" void emu_run_cpu_path(void* m, void* mi, void* mj, char* s, char* t, void* gmax, void* gdir,
+        unsigned* idx_inc, void* sp, float* mps, void* sem, int affine, int nthreads) {
+    const int xd = XdivSHARED_X, yd = YdivSHARED_Y;
+    const int maxb = xd < yd ? xd : yd, dec = xd + yd - maxb;
+    int idx = 0, idy = 0;
+    for (int i = 1; i < xd + yd; ++i) {
+        const int nb = i <= maxb ? i : (i >= dec ? xd + yd - i : maxb);
+        const unsigned gx = NUMBER_SEQUENCES * WORKGROUP_X, gy = NUMBER_TARGETS * nb * WORKGROUP_Y;
+        if (affine) emu_calculateScoreAffineGap(gx, gy, m, mi, mj, idx, idy, nb, s, t, gmax, gdir, nthreads);
+        else emu_calculateScore(gx, gy, m, idx, idy, nb, s, t, gmax, gdir, nthreads);
+        if (idx == xd - 1) ++idy;
+        if (idx < xd - 1) ++idx;
+    }
+    idx = xd - 1;
+    idy = yd - 1;
+    for (int i = 1; i < xd + yd; ++i) {
+        const int nb = i <= maxb ? i : (i >= dec ? xd + yd - i : maxb);
+        const unsigned gx = NUMBER_SEQUENCES * WORKGROUP_X, gy = NUMBER_TARGETS * nb * WORKGROUP_Y;
+        if (affine) emu_tracebackAffineGap(gx, gy, m, mi, mj, idx, idy, nb, gmax, gdir, idx_inc, sp, mps, sem,
+                                           nthreads);
+        else emu_traceback(gx, gy, m, idx, idy, nb, gmax, gdir, idx_inc, sp, mps, sem, nthreads);
+        if (idy == 0) --idx;
+        if (idy > 0) --idy;
+    }
+}
+"""
+
+
 def _import_reference_codegen():
     if REFERENCE_ROOT not in sys.path:
         sys.path.insert(0, REFERENCE_ROOT)
@@ -120,8 +153,10 @@ def expand_source(score, n_sequences, n_targets, x, y, flavour="cuda"):
 def build(score, n_sequences, n_targets, x, y, flavour="cuda", out_dir=OUT_DIR):
     """Returns the path of the emulated reference kernel library for this shape."""
     src = expand_source(score, n_sequences, n_targets, x, y, flavour)
-    src += _CUDA_LAUNCHERS if flavour == "cuda" else _OCL_CPU_LAUNCHERS
-    tag = hashlib.sha1((flavour + src).encode()).hexdigest()[:16]
+    src += _CUDA_LAUNCHERS if flavour == "cuda" else _OCL_CPU_LAUNCHERS + _OCL_CPU_LOOPS
+    with open(os.path.join(HERE, "kernel_emu.hpp")) as f:
+        shim = f.read()
+    tag = hashlib.sha1((flavour + shim + src).encode()).hexdigest()[:16]
     os.makedirs(out_dir, exist_ok=True)
     so_path = os.path.join(out_dir, "ref_%s_%s.so" % (flavour, tag))
     if os.path.exists(so_path):

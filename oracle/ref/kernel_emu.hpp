@@ -21,7 +21,6 @@
 //   * __shared__ variables become function-local statics in thread_local
 //     storage: one copy per host thread, shared by the fibers of the block.
 #pragma once
-#include <ucontext.h>
 #include <stdint.h>
 #include <string.h>
 #include <math.h>
@@ -35,10 +34,41 @@
 
 struct emu_dim3 { unsigned int x, y, z; };
 
+// Fiber switch: saves the callee-saved registers of the x86-64 System V ABI
+// on the current stack, stores the stack pointer in *from and continues on
+// `to`.  Unlike swapcontext it makes no system call (no signal mask), so a
+// barrier costs a few nanoseconds, as work-item loops of an OpenCL CPU
+// runtime do.  The floating-point control state is never changed by the
+// kernels, so it is not switched.
+extern "C" void emu_ctx_switch(void** from, void* to);
+asm(R"(
+.text
+.globl emu_ctx_switch
+.hidden emu_ctx_switch
+.type emu_ctx_switch,@function
+emu_ctx_switch:
+    pushq %rbp
+    pushq %rbx
+    pushq %r12
+    pushq %r13
+    pushq %r14
+    pushq %r15
+    movq %rsp, (%rdi)
+    movq %rsi, %rsp
+    popq %r15
+    popq %r14
+    popq %r13
+    popq %r12
+    popq %rbx
+    popq %rbp
+    ret
+.size emu_ctx_switch, .-emu_ctx_switch
+)");
+
 namespace emu {
 
 struct Fiber {
-    ucontext_t ctx;
+    void* sp;
     char* stack;
     bool done;
     emu_dim3 tid;
@@ -54,7 +84,7 @@ inline char* fiber_stack(unsigned t) {
 }
 
 struct BlockRunner {
-    ucontext_t sched;
+    void* sched;
     std::vector<Fiber> fibers;
     int current;
     const std::function<void()>* body;
@@ -67,12 +97,23 @@ inline void fiber_entry() {
     BlockRunner* r = tl_runner;
     (*r->body)();
     r->fibers[r->current].done = true;
-    swapcontext(&r->fibers[r->current].ctx, &r->sched);
+    emu_ctx_switch(&r->fibers[r->current].sp, r->sched);  // never resumed
 }
 
 inline void barrier_yield() {
     BlockRunner* r = tl_runner;
-    swapcontext(&r->fibers[r->current].ctx, &r->sched);
+    emu_ctx_switch(&r->fibers[r->current].sp, r->sched);
+}
+
+// A fresh fiber's stack: switching to it "returns" into fiber_entry with the
+// stack aligned as at a function's entry (rsp + 8 a multiple of 16).
+inline void* fiber_start(char* stack) {
+    uintptr_t top = ((uintptr_t)(stack + kFiberStack)) & ~(uintptr_t)15;
+    void** sp = (void**)top;
+    *--sp = nullptr;                                   // fiber_entry's return slot (never used)
+    *--sp = (void*)(void (*)())fiber_entry;            // popped by the switch's ret
+    for (int k = 0; k < 6; ++k) *--sp = nullptr;       // r15 r14 r13 r12 rbx rbp
+    return (void*)sp;
 }
 
 // Runs one block: bdx*bdy work-items, each executing `body`.
@@ -87,11 +128,7 @@ inline void run_block(unsigned bdx, unsigned bdy, const std::function<void()>& b
         f.stack = fiber_stack(t);
         f.done = false;
         f.tid = emu_dim3{t % bdx, t / bdx, 0};
-        getcontext(&f.ctx);
-        f.ctx.uc_stack.ss_sp = f.stack;
-        f.ctx.uc_stack.ss_size = kFiberStack;
-        f.ctx.uc_link = nullptr;
-        makecontext(&f.ctx, fiber_entry, 0);
+        f.sp = fiber_start(f.stack);
     }
     BlockRunner* saved = tl_runner;
     tl_runner = &r;
@@ -102,7 +139,7 @@ inline void run_block(unsigned bdx, unsigned bdy, const std::function<void()>& b
             if (r.fibers[t].done) continue;
             r.current = (int)t;
             tl_threadIdx = r.fibers[t].tid;
-            swapcontext(&r.sched, &r.fibers[t].ctx);
+            emu_ctx_switch(&r.sched, r.fibers[t].sp);
             if (!r.fibers[t].done) any = true;
         }
     }

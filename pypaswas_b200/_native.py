@@ -37,6 +37,7 @@ PW_TUNE_DUAL = 3
 PW_TUNE_CAND_SLOT = 4
 PW_TUNE_WAIT_NS = 5
 PW_TUNE_STALL_TEST = 6
+PW_TUNE_LANES = 7
 PW_FORMAT_FASTA = 0
 PW_FORMAT_FASTQ = 1
 PW_RECORDS_AS_READ = 0

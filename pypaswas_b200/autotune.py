@@ -1,32 +1,61 @@
-"""Empirical tuning of the engine's launch shapes on the inputs it holds.
+"""Empirical tuning of the score sweep's shape on the inputs the engine holds.
 
-The score sweep's shape is mostly fixed by cost models (lane orientation,
-strip class, list-scheduling plan); what is left to measurement is the share
-of multi-strip items cut into chained one-strip entries (PW_TUNE_CHAIN_MIN):
-more chaining shortens the longest items and keeps boundary rows in L2, less
-chaining saves the pipeline fill of each chain.  `autotune` times the score
-sweep (device time of its launches, pw_run_info.score_kernel_ms) for each
-candidate on the engine's current queries and targets and keeps the fastest.
+Most of the shape comes from cost models (lane orientation, strip class,
+list-scheduling plan); what is left to measurement is tuned here, one knob
+after the other, each time keeping the fastest setting (device time of the
+score sweep's launches, pw_run_info.score_kernel_ms, best of `repeats`):
+
+  1. lane width (PW_TUNE_LANES): the 16x2 sweep -- two 16-bit cells per
+     32-bit lane, pairs that reach the 16-bit limit recomputed on 32-bit
+     lanes -- against the 32-bit sweep;
+  2. register form of the 16x2 sweep (PW_TUNE_DUAL): two strips against one
+     lane sequence, one strip against two lane sequences, or the cost model's
+     pick;
+  3. chaining (PW_TUNE_CHAIN_MIN): the share of multi-strip items cut into
+     chained one-strip entries -- more chaining shortens the longest items,
+     less saves each chain's pipeline fill.
+
 The reference has no counterpart: its shapes are template constants
 (pyPaSWAS/Core/cuda/default_main.cu:7-30).
 """
 from . import _native
 
 CHAIN_MIN_CANDIDATES = (250, 500, 1000, 2000)
+DUAL_CANDIDATES = (0, 1, 2)  # cost model, always dual lanes, always strip pairs
+LANE_CANDIDATES = (0, 32)    # 16x2 where possible, 32-bit
 
 
-def autotune(engine, candidates=CHAIN_MIN_CANDIDATES, repeats=2):
-    """Sets PW_TUNE_CHAIN_MIN on `engine` to the fastest candidate; returns
-    {"chain_min": best, "score_kernel_ms": {candidate: best time}}."""
-    times = {}
+def _time(engine, repeats):
+    engine.align(score_only=True)  # builds and caches the plan of this setting
+    best = None
+    for _ in range(max(1, repeats)):
+        info = engine.align(score_only=True)
+        best = info.score_kernel_ms if best is None else min(best, info.score_kernel_ms)
+    return best, info
+
+
+def _pick(engine, key, candidates, repeats):
+    times, infos = {}, {}
     for value in candidates:
-        engine.set_tuning(_native.PW_TUNE_CHAIN_MIN, int(value))
-        engine.align(score_only=True)  # builds and caches the plan for this value
-        best = None
-        for _ in range(max(1, repeats)):
-            ms = engine.align(score_only=True).score_kernel_ms
-            best = ms if best is None else min(best, ms)
-        times[int(value)] = best
+        engine.set_tuning(key, int(value))
+        times[int(value)], infos[int(value)] = _time(engine, repeats)
     choice = min(times, key=lambda v: (times[v], v))
-    engine.set_tuning(_native.PW_TUNE_CHAIN_MIN, choice)
-    return {"chain_min": choice, "score_kernel_ms": times}
+    engine.set_tuning(key, choice)
+    return choice, times, infos
+
+
+def autotune(engine, repeats=2, chain_candidates=CHAIN_MIN_CANDIDATES):
+    """Sets the engine's lane width, 16x2 form and chaining threshold to the
+    fastest measured values; returns the choices and the times behind them."""
+    out = {}
+    lanes, t_lanes, infos = _pick(engine, _native.PW_TUNE_LANES, LANE_CANDIDATES, repeats)
+    out["lanes"] = 16 if lanes == 0 else 32
+    out["lanes_ms"] = {("16x2" if k == 0 else "32"): v for k, v in t_lanes.items()}
+    if lanes == 0 and infos[0].score_path == 0:
+        dual, t_dual, _ = _pick(engine, _native.PW_TUNE_DUAL, DUAL_CANDIDATES, repeats)
+        out["dual"] = {0: "cost model", 1: "dual lanes", 2: "strip pairs"}[dual]
+        out["dual_ms"] = t_dual
+        chain, t_chain, _ = _pick(engine, _native.PW_TUNE_CHAIN_MIN, chain_candidates, repeats)
+        out["chain_min"] = chain
+        out["score_kernel_ms"] = t_chain
+    return out

@@ -1547,6 +1547,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         return cuda_fail(e, c, "alloc pair maxima");
     KernelArgs A = base_args(e);
     const bool plain = (flags & PW_FLAG_PLAIN) != 0;
+    if (e->tune[PW_TUNE_LANES] == 32) flags |= PW_FLAG_INT32;  // the tuned lane width
 
     // ---------------------------------------------------------- phase 1
     // All-vs-all calls too small for the inter-sequence sweeps to give every

@@ -102,12 +102,13 @@ def test_autotune_keeps_the_fastest_candidate():
     from pypaswas_b200.autotune import autotune
 
     class Info(object):
-        def __init__(self, ms):
+        def __init__(self, ms, path):
             self.score_kernel_ms = ms
+            self.score_path = path
 
     class FakeEngine(object):
-        """Score-sweep time as a function of the chaining threshold."""
-        cost = {250: 9.0, 500: 7.5, 1000: 8.0, 2000: 7.5}
+        """Score-sweep time as a function of lane width, 16x2 form and chaining."""
+        chain_cost = {250: 9.0, 500: 7.5, 1000: 8.0, 2000: 7.5}
 
         def __init__(self):
             self.tune = {}
@@ -117,13 +118,19 @@ def test_autotune_keeps_the_fastest_candidate():
 
         def align(self, score_only=False):
             assert score_only
-            return Info(self.cost[self.tune[_native.PW_TUNE_CHAIN_MIN]])
+            if self.tune.get(_native.PW_TUNE_LANES, 0) == 32:
+                return Info(20.0, 1)
+            t = self.chain_cost[self.tune.get(_native.PW_TUNE_CHAIN_MIN, 500)]
+            t += {0: 0.0, 1: 0.5, 2: -0.25}[self.tune.get(_native.PW_TUNE_DUAL, 0)]
+            return Info(t, 0)
 
     e = FakeEngine()
     r = autotune(e)
+    assert r["lanes"] == 16 and e.tune[_native.PW_TUNE_LANES] == 0
+    assert r["dual"] == "strip pairs" and e.tune[_native.PW_TUNE_DUAL] == 2
     assert r["chain_min"] == 500  # ties go to the smaller value
     assert e.tune[_native.PW_TUNE_CHAIN_MIN] == 500
-    assert r["score_kernel_ms"] == FakeEngine.cost
+    assert r["score_kernel_ms"] == {k: v - 0.25 for k, v in FakeEngine.chain_cost.items()}
 
 
 def test_fast_hit_building_matches_hitlist_append_and_checked_path():
