@@ -313,16 +313,11 @@ def _records(w):
 
 
 def _e2e_calls(w):
-    """(queries, targets) per public-API call: one call for all-vs-all; with
-    explicit pairs one call per query against its targets, as the reference
-    is run once per pair file."""
+    """(queries, targets, explicit pairs or None) per public-API call: one
+    Aligner.process call for all-vs-all, one Aligner.process_pairs call with
+    explicit pairs."""
     qs, ts = _records(w)
-    if w.pairs is None:
-        return [(qs, ts)]
-    per_q = {}
-    for qi, ti in w.pairs:
-        per_q.setdefault(qi, []).append(ts[ti])
-    return [([qs[qi]], t) for qi, t in sorted(per_q.items())]
+    return [(qs, ts, w.pairs)]
 
 
 def _fasta_bytes(w):
@@ -353,20 +348,29 @@ def e2e_leg(ws, steps, device, trimmer):
     prog = (Trimmer if trimmer else Aligner)(None, None, st, device=device)
     sw = prog.smith_waterman
     score = scores.make_score(st)
+    timing = []
 
     def step(calls):
         h2d = d2h = 0
         reuse = 0
         if trimmer:
+            t0 = time.perf_counter()
             q = readers.read_query_records(st, calls[0])
             t = readers.read_target_records(st, score, calls[1])
+            t1 = time.perf_counter()
             prog.trimmed_fasta(q, t)  # the program's output text, natively
+            timing.append({"read_ms": (t1 - t0) * 1e3, "align_and_format_ms": (time.perf_counter() - t1) * 1e3,
+                           "engine_ms": float(sw.last_info.total_ms)})
             return sw.last_h2d_bytes, sw.last_d2h_bytes, int(sw.last_info.reuse)
-        for qs, ts in calls:
-            prog.process(qs, ts, None)  # HitList of Hit objects
+        for qs, ts, pairs in calls:
+            if pairs is None:
+                prog.process(qs, ts, None)  # HitList of Hit objects
+            else:
+                prog.process_pairs(qs, ts, pairs)
             h2d += sw.last_h2d_bytes
             d2h += sw.last_d2h_bytes
             reuse |= int(sw.last_info.reuse)
+            timing.append(dict(sw.last_timing))
         return h2d, d2h, reuse
 
     try:
@@ -387,7 +391,8 @@ def e2e_leg(ws, steps, device, trimmer):
         dt = time.perf_counter() - t0
     finally:
         sw.close()
-    return cells, dt, h2d // steps, d2h // steps, reuse
+    parts = {k: float(np.median([t[k] for t in timing[-steps:]])) for k in timing[0]} if timing else {}
+    return cells, dt, h2d // steps, d2h // steps, reuse, parts
 
 
 # ------------------------------------------------------------------ plain form
@@ -665,7 +670,7 @@ def run_config(cfg, args, device, world, flush, sampler, headline):
             import torch
             torch.distributed.barrier()
         steps_e2e = args.steps if headline else max(3, min(args.steps, 5))
-        cells, dt, h2d, d2h, reuse = e2e_leg(ws, steps_e2e, device, trimmer=cfg == 4)
+        cells, dt, h2d, d2h, reuse, parts = e2e_leg(ws, steps_e2e, device, trimmer=cfg == 4)
         if headline:
             dt = reduce_max(dt)
         rec["e2e"] = {"value": whole_job_gcups(cells / steps_e2e, steps_e2e, dt, world if headline else 1),
@@ -673,8 +678,9 @@ def run_config(cfg, args, device, world, flush, sampler, headline):
                       "steps": steps_e2e, "ms_per_step": dt * 1e3 / steps_e2e,
                       "api": "FASTA text -> readers (native) -> Trimmer.trimmed_fasta -> trimmedFasta text"
                              if cfg == 4 else
-                             ("Aligner.process per query (records -> HitList)" if w.pairs is not None else
-                              "Aligner.process (records -> HitList)"),
+                             ("Aligner.process_pairs (records, explicit pairs -> HitList)" if w.pairs is not None
+                              else "Aligner.process (records -> HitList)"),
+                      "host_ms_median": parts,
                       "inputs": "two seeded input sets of the same shape, alternating: every step copies and "
                                 "prepares its inputs and rebuilds its plan (reuse bits seen: %d)" % reuse,
                       "workload": ws[0].name}
@@ -701,7 +707,7 @@ def main():
         out.update({"n_gpus": world, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                     "clocks": sampler.summary()})
         out["config"]["parallelism"] = "replica per GPU" if world > 1 else "single GPU"
-        n_plain = {1: (8, 100), 2: (8, 64), 3: (4, 0), 4: (64, 48)}
+        n_plain = {1: (8, 100), 2: (8, 64), 3: (16, 0), 4: (64, 48)}
         if not args.no_plain:
             out["plain"] = plain_leg(w if w.queries is not None else w.head(64), local, *n_plain[args.config])
         if rank == 0 and world == 1 and not args.no_cpu_baseline:

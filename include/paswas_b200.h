@@ -171,8 +171,9 @@ int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_info* info)
  * pw_get_pair_max then holds -1 for the pairs that are not listed. */
 int pw_set_pairs(pw_engine* e, const int32_t* query_idx, const int32_t* target_idx, int64_t n);
 
-/* Upper bound, in bytes, on the direction-matrix (cell code) memory of one
- * memory wave of pw_align; 0 restores the automatic choice (55% of the free
+/* Upper bound, in bytes, on the direction-matrix memory of one memory wave of
+ * pw_align (4-bit cell codes -- direction, stop flag, candidate flag -- and a
+ * 1-bit mark plane: half a byte plus one bit per traced cell); 0 restores the automatic choice (55% of the free
  * device memory with the candidate slots counted, at most 100 GiB).  Traced
  * pairs beyond the bound run in
  * further waves; a single pair larger than the bound runs alone.  Replaces

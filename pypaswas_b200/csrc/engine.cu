@@ -269,7 +269,7 @@ struct pw_engine {
         int xm_multi = 4;
         int n_chain_items = 0;
     } p1;
-    DevBuf codes, metas, cands, cands_alt, cand_base, cand_cap, n_cand, n_starts, start_off, starts, hits,
+    DevBuf codes, marks, metas, cands, cands_alt, cand_base, cand_cap, n_cand, n_starts, start_off, starts, hits,
         hit_count, ops, allowed;
     // prepared (device-resident) inputs
     Prepared pr;
@@ -840,22 +840,53 @@ static int run_phase(pw_engine* e, KernelArgs A, const WorkItem* dev_items, cons
     return PW_OK;
 }
 
-// Sorts items by strip class (stable) and returns the class boundaries.
+// Sorts items by strip class (stable; a counting sort) and returns the class
+// boundaries.
 static void order_by_class(std::vector<WorkItem>& items, std::vector<int>& cls, int (&begin)[kNumClasses + 1]) {
-    std::vector<size_t> idx(items.size());
-    std::iota(idx.begin(), idx.end(), 0);
-    std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return cls[a] < cls[b]; });
-    std::vector<WorkItem> it2(items.size());
-    std::vector<int> c2(items.size());
-    for (size_t k = 0; k < idx.size(); ++k) {
-        it2[k] = items[idx[k]];
-        c2[k] = cls[idx[k]];
-    }
-    items.swap(it2);
-    cls.swap(c2);
     for (int c = 0; c <= kNumClasses; ++c) begin[c] = 0;
     for (int c : cls) begin[c + 1]++;
     for (int c = 0; c < kNumClasses; ++c) begin[c + 1] += begin[c];
+    int pos[kNumClasses + 1];
+    for (int c = 0; c <= kNumClasses; ++c) pos[c] = begin[c];
+    std::vector<WorkItem> it2(items.size());
+    std::vector<int> c2(items.size());
+    for (size_t k = 0; k < items.size(); ++k) {
+        const int p = pos[cls[k]]++;
+        it2[p] = items[k];
+        c2[p] = cls[k];
+    }
+    items.swap(it2);
+    cls.swap(c2);
+}
+
+// Order of items by strip class ascending, then cost descending, ties in
+// their current order (what a stable sort by cost followed by a stable sort
+// by class gives): an LSD radix sort of (class, ~cost) keys, 16 bits a pass,
+// stopping once every key agrees in the digits left.  Linear in the item
+// count: millions of work items (short reads) are ordered in milliseconds.
+static std::vector<uint32_t> class_cost_order(const std::vector<int>& cls, const std::vector<int64_t>& cost) {
+    const size_t n = cls.size();
+    constexpr uint64_t kCostMask = ((uint64_t)1 << 48) - 1;
+    std::vector<uint64_t> key(n);
+    uint64_t lo = ~(uint64_t)0, hi = 0;
+    for (size_t k = 0; k < n; ++k) {
+        const uint64_t c = std::min<uint64_t>((uint64_t)std::max<int64_t>(cost[k], 0), kCostMask);
+        key[k] = ((uint64_t)cls[k] << 48) | (kCostMask - c);
+        lo = std::min(lo, key[k]);
+        hi = std::max(hi, key[k]);
+    }
+    std::vector<uint32_t> idx(n), tmp(n);
+    std::iota(idx.begin(), idx.end(), 0u);
+    std::vector<uint32_t> cnt(65537);
+    for (int shift = 0; shift < 64 && n > 0; shift += 16) {
+        if (((lo ^ hi) >> shift) == 0) break;  // every key agrees from this digit up
+        std::fill(cnt.begin(), cnt.end(), 0u);
+        for (size_t k = 0; k < n; ++k) cnt[((key[idx[k]] >> shift) & 0xffff) + 1]++;
+        for (int d = 0; d < 65536; ++d) cnt[d + 1] += cnt[d];
+        for (size_t k = 0; k < n; ++k) tmp[cnt[(key[idx[k]] >> shift) & 0xffff]++] = idx[k];
+        idx.swap(tmp);
+    }
+    return idx;
 }
 
 
@@ -1062,19 +1093,18 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uin
                 cost.push_back((int64_t)w.xmax * ls);
             }
         }
-        std::vector<size_t> idx(items.size());
-        std::iota(idx.begin(), idx.end(), 0);
-        std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return cost[a] > cost[b]; });
-        std::vector<WorkItem> it2;
-        std::vector<int> c2;
-        it2.reserve(items.size());
-        c2.reserve(items.size());
-        for (size_t k : idx) {
-            it2.push_back(items[k]);
-            c2.push_back(cls[k]);
+        // largest cost first within each strip class (dynamic scheduling tail)
+        const std::vector<uint32_t> idx = class_cost_order(cls, cost);
+        std::vector<WorkItem> it2(items.size());
+        std::vector<int> c2(items.size());
+        for (size_t k = 0; k < idx.size(); ++k) {
+            it2[k] = items[idx[k]];
+            c2[k] = cls[idx[k]];
         }
         int begin[kNumClasses + 1];
-        order_by_class(it2, c2, begin);
+        for (int k = 0; k <= kNumClasses; ++k) begin[k] = 0;
+        for (int k : c2) begin[k + 1]++;
+        for (int k = 0; k < kNumClasses; ++k) begin[k + 1] += begin[k];
         if ((c = upload(e, e->p1_items, it2)) != cudaSuccess) return cuda_fail(e, c, "upload items");
         int xm = 4;
         for (int k = begin[kS32Multi]; k < begin[kS32Multi + 1]; ++k) xm = std::max(xm, (int)align_up(it2[k].xmax, 4));
@@ -1415,8 +1445,6 @@ static int run_band_phase(pw_engine* e, KernelArgs A, std::vector<BandPair>& pai
         }
     }
     const size_t n = entries.size();
-    if ((c = upload(e, e->band_pairs, sorted)) != cudaSuccess) return cuda_fail(e, c, "upload band pairs");
-    if ((c = upload(e, e->band_entries, entries)) != cudaSuccess) return cuda_fail(e, c, "upload band queue");
     if (e->tune[PW_TUNE_STALL_TEST]) {
         // one band below another waits on the spare flag (index n) instead
         for (int4& v : entries)
@@ -1426,6 +1454,8 @@ static int run_band_phase(pw_engine* e, KernelArgs A, std::vector<BandPair>& pai
                 break;
             }
     }
+    if ((c = upload(e, e->band_pairs, sorted)) != cudaSuccess) return cuda_fail(e, c, "upload band pairs");
+    if ((c = upload(e, e->band_entries, entries)) != cudaSuccess) return cuda_fail(e, c, "upload band queue");
     if ((c = e->band_prog.reserve(e->stream, (n + 1) * sizeof(int))) != cudaSuccess ||
         (c = e->band_max.reserve(e->stream, n * sizeof(int))) != cudaSuccess ||
         (c = e->band_ring.reserve(e->stream, (size_t)std::max<int64_t>(ring_elems, 1) * sizeof(int4))) != cudaSuccess ||
@@ -1654,19 +1684,19 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
                 cls.push_back(k);
             }
         // largest work first inside each class (dynamic scheduling tail)
-        std::vector<size_t> idx(items.size());
-        std::iota(idx.begin(), idx.end(), 0);
-        std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) {
-            return (int64_t)items[a].xmax * tlen[items[a].target] > (int64_t)items[b].xmax * tlen[items[b].target];
-        });
-        std::vector<WorkItem> it2;
-        std::vector<int> c2;
-        for (size_t k : idx) {
-            it2.push_back(items[k]);
-            c2.push_back(cls[k]);
+        std::vector<int64_t> cost(items.size());
+        for (size_t k = 0; k < items.size(); ++k) cost[k] = (int64_t)items[k].xmax * tlen[items[k].target];
+        const std::vector<uint32_t> idx = class_cost_order(cls, cost);
+        std::vector<WorkItem> it2(items.size());
+        std::vector<int> c2(items.size());
+        for (size_t k = 0; k < idx.size(); ++k) {
+            it2[k] = items[idx[k]];
+            c2[k] = cls[idx[k]];
         }
         int begin[kNumClasses + 1];
-        order_by_class(it2, c2, begin);
+        for (int k = 0; k <= kNumClasses; ++k) begin[k] = 0;
+        for (int k : c2) begin[k + 1]++;
+        for (int k = 0; k < kNumClasses; ++k) begin[k + 1] += begin[k];
         int xm = 4;
         for (int k = begin[kS32Multi]; k < begin[kS32Multi + 1]; ++k) xm = std::max(xm, (int)align_up(it2[k].xmax, 4));
         if ((c = upload(e, e->items, it2)) != cudaSuccess) return cuda_fail(e, c, "upload items");
@@ -1894,7 +1924,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
                 w.S = S;
                 items2[it] = w;
                 cls2[it] = k;
-                bytes2[it] = strips * S * align_up(std::max(w.xmax, 1), 4) * kWarp;
+                bytes2[it] = strips * S * align_up(std::max(w.xmax, 1), 4) * kWarp / 2;  // 4-bit codes
             }
         }
     }, std::max<int64_t>(1, (int64_t)n_strip * ((int64_t)1 << 15) / std::max<int64_t>(s_pairs[n_strip], 1)));
@@ -1962,10 +1992,11 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         if (e->free_mem_t < 0 || now - e->free_mem_t > 1000.0) {
             size_t free_b = 0, total_b = 0;
             cudaMemGetInfo(&free_b, &total_b);
-            e->free_mem = (int64_t)free_b + (int64_t)(e->codes.bytes + e->cands.bytes + e->metas.bytes);
+            e->free_mem = (int64_t)free_b + (int64_t)(e->codes.bytes + e->marks.bytes + e->cands.bytes +
+                                                      e->metas.bytes);
             e->free_mem_t = now;
         }
-        const int64_t kept = (int64_t)(e->codes.bytes + e->cands.bytes + e->metas.bytes);
+        const int64_t kept = (int64_t)(e->codes.bytes + e->marks.bytes + e->cands.bytes + e->metas.bytes);
         budget = std::min<int64_t>((int64_t)(std::max<int64_t>(e->free_mem - kept, 0) * 0.55) + kept,
                                    (int64_t)100 << 30);
     }
@@ -1975,7 +2006,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         size_t i0 = 0;
         int64_t acc = 0;
         for (size_t i = 0; i < items2.size(); ++i) {
-            const int64_t b = bytes2[i] + items2[i].lanes * pair_bytes;
+            const int64_t b = bytes2[i] + bytes2[i] / 4 + items2[i].lanes * pair_bytes;  // codes + mark plane
             if (acc > 0 && (acc + b > budget || plain)) {
                 waves.push_back({i0, i});
                 i0 = i;
@@ -2024,6 +2055,11 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         int xm = 4;
         for (int k = begin[kS32Multi]; k < begin[kS32Multi + 1]; ++k) xm = std::max(xm, (int)align_up(wi[k].xmax, 4));
         if ((c = e->codes.reserve(e->stream, (size_t)dir_off)) != cudaSuccess) return cuda_fail(e, c, "alloc cell codes");
+        // one mark bit per cell (two cells per code byte), zeroed for the wave
+        const size_t mark_bytes = (size_t)(dir_off / 4 + 16);
+        if ((c = e->marks.reserve(e->stream, mark_bytes)) != cudaSuccess ||
+            (c = cudaMemsetAsync(e->marks.p, 0, mark_bytes, e->stream)) != cudaSuccess)
+            return cuda_fail(e, c, "alloc cell marks");
         if ((c = e->metas.reserve(e->stream, n_pairs * sizeof(PairMeta))) != cudaSuccess) return cuda_fail(e, c, "alloc metas");
         if ((c = e->n_cand.reserve(e->stream, n_pairs * sizeof(int32_t))) != cudaSuccess) return cuda_fail(e, c, "alloc");
         if ((c = e->n_starts.reserve(e->stream, n_pairs * sizeof(int32_t))) != cudaSuccess) return cuda_fail(e, c, "alloc");
@@ -2159,6 +2195,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         TA.n_pairs = (int)n_pairs;
         TA.items = e->items.as<WorkItem>();
         TA.codes = A.codes;
+        TA.marks = e->marks.as<uint8_t>();
         TA.cands = A.cands;
         TA.cand_base = A.cand_base;
         TA.n_starts = e->n_starts.as<int32_t>();

@@ -22,8 +22,9 @@
 // DIRS = false: pair maxima only (the score sweep of long pairs).
 // DIRS = true: the direction sweep of traced pairs: per cell the code byte of
 // the reference's classification (direction, stop flag, candidate flag) and
-// the pair's candidate list, exactly as the strip sweep computes them; cell
-// codes are stored [band][step][lane][8 rows] (warp_layout_offset).
+// the pair's candidate list, exactly as the strip sweep computes them; 4-bit
+// cell codes are stored [band][step][lane][8 rows] (warp_layout_offset), one
+// 4-byte word per lane and step: a warp stores 128 contiguous bytes.
 #pragma once
 #include "pw_kernels.cuh"
 #include "pw_score16.cuh"
@@ -36,9 +37,11 @@ constexpr int kBandLead = 128;                 // planning lead between bands (s
 
 static_assert(kBandRows == 256 && kWarpRows == 8, "warp_layout_offset (pw_kernels.cuh) assumes 8 x 32 rows");
 
+// Bytes of a pair's 4-bit cell codes in the band layout (8 rows of a lane per
+// 4-byte word).
 __host__ __device__ __forceinline__ int64_t warp_code_bytes(int lq, int lt) {
     const int64_t bands = lt > 0 ? (lt + kBandRows - 1) / kBandRows : 1;
-    return bands * ((int64_t)lq + kWarp - 1) * kWarp * kWarpRows;
+    return bands * ((int64_t)lq + kWarp - 1) * kWarp * kWarpRows / 2;
 }
 
 struct BandPair {
@@ -201,7 +204,7 @@ __global__ void __launch_bounds__(128) band_kernel(KernelArgs A, BandArgs B) {
                 const int a = __ldg(qg + x);
                 const uint2 pw = prof[lane * alpha1 + a];
                 const bool xin = x > 0;
-                uint32_t w0 = 0, w1 = 0;
+                uint32_t w0 = 0;  // the lane's 8 rows as 4-bit codes
                 if constexpr (!AFFINE) {
                     int up = up_h, diag = dg_h;
 #pragma unroll
@@ -231,10 +234,7 @@ __global__ void __launch_bounds__(128) band_kernel(KernelArgs A, BandArgs B) {
                                     cand[k] = cc;
                                 }
                             }
-                            if (r < 4)
-                                w0 |= code << (8 * r);
-                            else
-                                w1 |= code << (8 * (r - 4));
+                            w0 |= code << (4 * r);
                         } else {
                             mx = max(mx, h);
                         }
@@ -271,10 +271,7 @@ __global__ void __launch_bounds__(128) band_kernel(KernelArgs A, BandArgs B) {
                                     cand[k] = cc;
                                 }
                             }
-                            if (r < 4)
-                                w0 |= code << (8 * r);
-                            else
-                                w1 |= code << (8 * (r - 4));
+                            w0 |= code << (4 * r);
                         } else {
                             mx = max(mx, b);
                         }
@@ -291,7 +288,7 @@ __global__ void __launch_bounds__(128) band_kernel(KernelArgs A, BandArgs B) {
                     bt_b = Bl[kWarpRows - 1];
                 }
                 if constexpr (DIRS)
-                    *(uint2*)(codes + ((band * nsteps + s) * kWarp + lane) * kWarpRows) = make_uint2(w0, w1);
+                    *(uint32_t*)(codes + ((band * nsteps + s) * kWarp + lane) * kWarpRows / 2) = w0;
                 if (lane == kWarp - 1 && store_bnd) __stcg(&ring_out[x], make_int4(AFFINE ? bt_m : bt_h, bt_i, bt_b, 0));
             } else {
                 // not started (x < 0): hand the left-boundary values down

@@ -27,13 +27,13 @@ constexpr int kWarp = 32;
 constexpr int kCandCap = 64;          // candidates stored per pair before overflow
 constexpr int kNeg = -(1 << 28);       // stands in for AFFINE_GAP_INIT (-1e10f) in int32
 
-// direction codes of the cell code byte (bits 0-1)
+// direction codes of the 4-bit cell code (bits 0-1)
 constexpr uint8_t kNo = 0, kUL = 1, kUp = 2, kLeft = 3;
-// flag bits of the cell code byte
+// flag bits of the cell code
 constexpr uint8_t kStopFlag = 1u << 2;  // UL/MAIN cell whose diagonal predecessor is 0 (in matrix)
 constexpr uint8_t kCand = 1u << 3;      // starting-point candidate (score >= threshold)
-constexpr uint8_t kCovered = 1u << 4;   // candidate lying on another candidate's chain
-constexpr uint8_t kVisited = 1u << 5;   // IN_ALIGNMENT mark of the host walk
+// (covered candidates and the walk's IN_ALIGNMENT marks are bits of a
+// separate plane, see PairView in pw_kernels.cuh)
 
 // Scoring constants shared by all kernels.
 struct ScoreParams {
@@ -89,9 +89,10 @@ struct DevHit {
     int64_t ops_offset;
 };
 
-// Byte offset of cell (x, y) of lane `lane` inside a group's code block.
-// Layout: [strip][x][chunk of 16 rows][lane][16 bytes]; one 16-byte vector
-// store per lane and chunk makes each warp store a contiguous 512 bytes.
+// Index of cell (x, y) of lane `lane` inside a group's code block.
+// Layout: [strip][x][chunk of 16 rows][lane][16 cells]; cells are 4-bit codes,
+// so one 8-byte store per lane and chunk makes each warp store a contiguous
+// 256 bytes (the byte of cell i is i / 2).
 template <int S>
 __host__ __device__ __forceinline__ int64_t cell_offset(int x, int y, int lane, int xmax) {
     const int strip = y / S, r = y % S;

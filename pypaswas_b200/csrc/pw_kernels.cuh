@@ -215,7 +215,7 @@ template <typename T, int S, bool AFFINE, bool TRANS = false>
 __device__ __forceinline__ void sweep_dirs(const LaneCtx& c, const void* prof, int alpha1, T gap, T ext, T ge,
                                            Bnd<T>* bnd, uint8_t* codes, int lane, int xmax4, T thr, Cand* cand,
                                            int cand_cap, int& n_cand) {
-    uint4* out = (uint4*)codes;
+    uint2* out = (uint2*)codes;  // 4-bit cell codes: 16 rows of a lane in 8 bytes
     if constexpr (!AFFINE) {
         T H[S];
 #pragma unroll
@@ -231,11 +231,12 @@ __device__ __forceinline__ void sweep_dirs(const LaneCtx& c, const void* prof, i
                 T up = c.has_up ? bnd[(int64_t)x * kWarp].m : T(0);
                 T diag = hb_prev;
                 hb_prev = up;
-                uint32_t words[S / 4];
+                uint32_t words[S / 8];
+#pragma unroll
+                for (int q = 0; q < S / 8; ++q) words[q] = 0;
 #pragma unroll
                 for (int g = 0; g < S / 4; ++g) {
                     const Prof4<T> p = load_prof<T>(prof, g, alpha1, a);
-                    uint32_t w = 0;
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
                         const int r = 4 * g + k;
@@ -266,17 +267,15 @@ __device__ __forceinline__ void sweep_dirs(const LaneCtx& c, const void* prof, i
                                 ++n_cand;
                             }
                         }
-                        w |= code << (8 * k);
+                        words[r / 8] |= code << (4 * (r % 8));
                         diag = left;
                         H[r] = h;
                         up = h;
                     }
-                    words[g] = w;
                 }
 #pragma unroll
                 for (int q = 0; q < S / 16; ++q)
-                    out[((int64_t)x * (S / 16) + q) * kWarp + lane] =
-                        make_uint4(words[4 * q], words[4 * q + 1], words[4 * q + 2], words[4 * q + 3]);
+                    out[((int64_t)x * (S / 16) + q) * kWarp + lane] = make_uint2(words[2 * q], words[2 * q + 1]);
                 if (c.has_down) bnd[(int64_t)x * kWarp].m = H[S - 1];
             }
         }
@@ -307,11 +306,12 @@ __device__ __forceinline__ void sweep_dirs(const LaneCtx& c, const void* prof, i
                 T bdiag = bb_prev, mdiag = bm_prev;
                 bb_prev = bup;
                 bm_prev = mup;
-                uint32_t words[S / 4];
+                uint32_t words[S / 8];
+#pragma unroll
+                for (int q = 0; q < S / 8; ++q) words[q] = 0;
 #pragma unroll
                 for (int g = 0; g < S / 4; ++g) {
                     const Prof4<T> p = load_prof<T>(prof, g, alpha1, a);
-                    uint32_t w = 0;
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
                         const int r = 4 * g + k;
@@ -341,7 +341,7 @@ __device__ __forceinline__ void sweep_dirs(const LaneCtx& c, const void* prof, i
                                 ++n_cand;
                             }
                         }
-                        w |= code << (8 * k);
+                        words[r / 8] |= code << (4 * (r % 8));
                         bdiag = Bl[r];
                         mdiag = Ml[r];
                         Ml[r] = m;
@@ -350,12 +350,10 @@ __device__ __forceinline__ void sweep_dirs(const LaneCtx& c, const void* prof, i
                         mup = m;
                         iup = i;
                     }
-                    words[g] = w;
                 }
 #pragma unroll
                 for (int q = 0; q < S / 16; ++q)
-                    out[((int64_t)x * (S / 16) + q) * kWarp + lane] =
-                        make_uint4(words[4 * q], words[4 * q + 1], words[4 * q + 2], words[4 * q + 3]);
+                    out[((int64_t)x * (S / 16) + q) * kWarp + lane] = make_uint2(words[2 * q], words[2 * q + 1]);
                 if (c.has_down) {
                     Bnd<T> b;
                     b.m = mup;
@@ -488,7 +486,7 @@ __global__ void __launch_bounds__(128) sweep_kernel(KernelArgs A) {
                 if (PHASE == 1) {
                     sweep_score<T, S, AFFINE>(c, prof, alpha1, gap, ext, ge, bnd_slot, mx);
                 } else {
-                    uint8_t* codes = A.codes + W.dir_base + (int64_t)s * xmax4 * S * kWarp;
+                    uint8_t* codes = A.codes + W.dir_base + (int64_t)s * xmax4 * S * kWarp / 2;
                     sweep_dirs<T, S, AFFINE, TRANS>(c, prof, alpha1, gap, ext, ge, bnd_slot, codes, lane, xmax4,
                                                     thr, cand, cap, n_cand);
                 }
@@ -510,7 +508,8 @@ struct TraceArgs {
     const PairMeta* metas;
     int n_pairs;
     const WorkItem* items;
-    uint8_t* codes;
+    uint8_t* codes;          // 4-bit cell codes of the wave
+    uint8_t* marks;          // one bit per cell of the wave (zeroed per wave): covered, then visited
     Cand* cands;
     const int64_t* cand_base;
     int32_t* n_starts;       // per pair: starting points (after collect)
@@ -533,14 +532,37 @@ __host__ __device__ __forceinline__ int64_t warp_layout_offset(int x, int y, int
     return ((band * nsteps + x + l) * 32 + l) * 8 + r;
 }
 
+// A traced pair's cells.  Each cell has a 4-bit code (direction, stop flag,
+// candidate flag; two cells per byte, the even index in the low nibble) and a
+// 1-bit mark in a separate plane: collect_kernel marks covered candidates there
+// (and clears them again), walk_kernel marks the cells it visits
+// (IN_ALIGNMENT).  The cell index is the item's own: the strip or band layout.
 struct PairView {
-    uint8_t* base;
+    uint8_t* base;      // the item's codes
+    uint8_t* marks;     // the wave's mark plane
+    int64_t cell0;      // the item's first cell in the wave (2 x its code byte offset)
     int S, lane, xmax4, lq, lt;
     int layout;  // 0: strip sweep, targets as strips; 1: strip sweep, queries as strips; 2: warp sweep
     // cell (x, y) in the reference's coordinates (x: query, y: target)
-    __device__ __forceinline__ uint8_t& at(int x, int y) const {
-        if (layout == 2) return base[warp_layout_offset(x, y, lq)];
-        return base[layout == 1 ? cell_offset_rt(S, y, x, lane, xmax4) : cell_offset_rt(S, x, y, lane, xmax4)];
+    __device__ __forceinline__ int64_t index(int x, int y) const {
+        if (layout == 2) return warp_layout_offset(x, y, lq);
+        return layout == 1 ? cell_offset_rt(S, y, x, lane, xmax4) : cell_offset_rt(S, x, y, lane, xmax4);
+    }
+    __device__ __forceinline__ uint32_t code(int x, int y) const {
+        const int64_t i = index(x, y);
+        return (base[i >> 1] >> ((i & 1) * 4)) & 15u;
+    }
+    __device__ __forceinline__ bool marked(int x, int y) const {
+        const int64_t i = cell0 + index(x, y);
+        return (marks[i >> 3] >> (i & 7)) & 1u;
+    }
+    __device__ __forceinline__ void mark(int x, int y) const {
+        const int64_t i = cell0 + index(x, y);
+        marks[i >> 3] |= (uint8_t)(1u << (i & 7));
+    }
+    __device__ __forceinline__ void unmark(int x, int y) const {
+        const int64_t i = cell0 + index(x, y);
+        marks[i >> 3] &= (uint8_t)~(1u << (i & 7));
     }
 };
 
@@ -548,6 +570,8 @@ __device__ __forceinline__ PairView pair_view(const TraceArgs& A, const PairMeta
     PairView v;
     const WorkItem W = A.items[pm.item];
     v.base = A.codes + W.dir_base;
+    v.marks = A.marks;
+    v.cell0 = W.dir_base * 2;
     v.S = W.S;
     v.lane = pm.lane;
     v.xmax4 = (W.xmax + 3) & ~3;
@@ -581,10 +605,10 @@ __global__ void collect_kernel(TraceArgs A) {
     for (int k = 0; k < n; ++k) {
         int x = cl[k].x - 1, y = cl[k].y - 1;
         while (x >= 0 && y >= 0) {
-            uint8_t& cd = v.at(x, y);
+            const uint32_t cd = v.code(x, y);
             const int d = cd & 3;
             if (cd & kCand) {
-                cd |= kCovered;
+                v.mark(x, y);  // covered
                 break;
             }
             if (AFFINE) {
@@ -604,12 +628,17 @@ __global__ void collect_kernel(TraceArgs A) {
             }
         }
     }
-    // keep uncovered candidates, then order them for the walk: ascending score,
-    // then emission order (SmithWaterman.py:699 is a stable sort)
+    // keep uncovered candidates (clearing the covered marks, so that the
+    // plane holds only the walk's marks afterwards), then order them for the
+    // walk: ascending score, then emission order (SmithWaterman.py:699 is a
+    // stable sort)
     int m = 0;
     for (int k = 0; k < n; ++k) {
         const Cand cc = cl[k];
-        if (!(v.at(cc.x, cc.y) & kCovered)) cl[m++] = cc;
+        if (v.marked(cc.x, cc.y))
+            v.unmark(cc.x, cc.y);
+        else
+            cl[m++] = cc;
     }
     for (int k = 1; k < m; ++k) {
         const Cand key = cl[k];
@@ -633,7 +662,7 @@ __global__ void collect_kernel(TraceArgs A) {
 // (itself or further down-right).
 __device__ __forceinline__ bool run_has_candidate(const PairView& v, int x, int y) {
     while (x < v.lq && y < v.lt) {
-        const uint8_t cd = v.at(x, y);
+        const uint32_t cd = v.code(x, y);
         if (cd & kCand) return true;
         if ((cd & 3) != kUL) return false;
         ++x;
@@ -646,8 +675,8 @@ constexpr int kStopDir = 64, kInAlignment = 96;
 
 template <bool AFFINE>
 __device__ __forceinline__ int walk_direction(const PairView& v, int x, int y) {
-    const uint8_t cd = v.at(x, y);
-    if (cd & kVisited) return kInAlignment;
+    if (v.marked(x, y)) return kInAlignment;
+    const uint32_t cd = v.code(x, y);
     const int d = cd & 3;
     if (d == kUL && (cd & kStopFlag)) {
         if (!AFFINE || run_has_candidate(v, x, y)) return kStopDir;
@@ -690,10 +719,10 @@ __global__ void walk_kernel(TraceArgs A) {
         // after a gap move), so the run is scanned only when that is unknown.
         int run_next = -1;
         while (show && x >= 0 && y >= 0 && dir != kStopDir && dir != 32) {  // :761
-            const uint8_t cd = v.at(x, y);
+            const uint32_t cd = v.code(x, y);
             const int d = cd & 3;
             int run_here = (cd & kCand) ? 1 : (d != kUL ? 0 : run_next);
-            if (cd & kVisited) {
+            if (v.marked(x, y)) {
                 dir = kInAlignment;
             } else if (d == kUL && (cd & kStopFlag)) {
                 if (AFFINE && run_here < 0) run_here = run_has_candidate(v, x + 1, y + 1) ? 1 : 0;
@@ -702,7 +731,7 @@ __global__ void walk_kernel(TraceArgs A) {
                 dir = d;
             }
             run_next = dir == kUL ? run_here : -1;
-            v.at(x, y) |= kVisited;
+            v.mark(x, y);  // IN_ALIGNMENT
             if (dir == kInAlignment) {
                 show = false;
             } else if (dir == kUL || dir == kStopDir) {
@@ -767,7 +796,7 @@ __global__ void ops_kernel(TraceArgs A, const DevHit* hits, int n_hits) {
     int x = H.end_x, y = H.end_y;
     char* o = A.ops + H.ops_offset;
     for (int k = 0; k < H.n_cols; ++k) {
-        const int d = v.at(x, y) & 3;
+        const int d = v.code(x, y) & 3;
         char op;
         if (d == kLeft) {
             op = 'I';

@@ -52,6 +52,14 @@ class Aligner(object):
             target_index = last
         return self.hitlist
 
+    def process_pairs(self, records_seqs, targets, pairs):
+        """Explicit (query index, target index) pairs; returns the HitList that
+        process() gives for each pair on its own, merged
+        (SmithWatermanB200.align_pairs)."""
+        self.hitlist = HitList(self.logger)
+        self.hitlist.extend(self.smith_waterman.align_pairs(records_seqs, targets, pairs))
+        return self.hitlist
+
     def txt(self, records_seqs, targets):
         """The TXT output of process() + DefaultFormatter, byte for byte, with
         the HitList and the records built in native code

@@ -118,6 +118,7 @@ class SmithWatermanB200(object):
         self.last_info = None
         self.last_h2d_bytes = 0
         self.last_d2h_bytes = 0
+        self.last_timing = {}
 
     def set_total_work_size(self, size):
         self.total_work_size = size
@@ -151,18 +152,45 @@ class SmithWatermanB200(object):
             return hitlist
         t0 = time.time()
         block = self._upload(records_seqs, targets, target_index)
-        cap = self.maximum_number_starting_points * len(records_seqs) * len(block)
-        info = self.engine.align(start_cap=cap)
+        self._align_into(records_seqs, block, hitlist, len(records_seqs) * len(block), t0)
+        self._progress(records_seqs, block, t0)
+        return hitlist
+
+    def align_pairs(self, records_seqs, targets, pairs):
+        """Explicit (query index, target index) pairs instead of all against
+        all; returns a HitList.  The same hits as running align_sequences once
+        per pair (how the reference is run on pair files), in one engine call
+        whose long pairs are swept band by band across the whole GPU."""
+        hitlist = HitList(self.logger)
+        if len(pairs) == 0:
+            return hitlist
+        t0 = time.time()
+        self.number_targets = len(targets)
+        block = self._upload(records_seqs, targets, 0)
+        self.engine.set_pairs([int(p[0]) for p in pairs], [int(p[1]) for p in pairs])
+        try:
+            self._align_into(records_seqs, block, hitlist, len(pairs), t0)
+        finally:
+            self.engine.set_pairs([], [])
+        return hitlist
+
+    def _align_into(self, records_seqs, block, hitlist, n_pairs, t0):
+        """One engine call on the uploaded records; its Hits into hitlist.
+        last_timing holds the call's host wall time in three parts (ms):
+        records to the engine, the engine call, hits to Hit objects."""
+        t1 = time.time()
+        info = self.engine.align(start_cap=self.maximum_number_starting_points * n_pairs)
         self.last_info = info
         if info.truncated:
             self.logger.warning("Too many hits returned. Skipping the rest. Please set lower_limit_score "
                                 "higher in config.")
         hits, strbuf = self.engine.hits()
+        t2 = time.time()
         self.last_h2d_bytes = int(info.h2d_bytes)  # counted by the engine, copy by copy
         self.last_d2h_bytes = int(info.d2h_bytes)
         self._build_hits(hits, strbuf, records_seqs, block, hitlist)
-        self._progress(records_seqs, block, t0)
-        return hitlist
+        self.last_timing = {"records_ms": (t1 - t0) * 1e3, "engine_ms": (t2 - t1) * 1e3,
+                            "hits_ms": (time.time() - t2) * 1e3}
 
     def align_records(self, records_seqs, targets, target_index):
         """align_sequences without the Python Hit objects: the engine's hit

@@ -191,3 +191,15 @@ def test_config3_sample_pairs_bit_exact_and_driver_agrees(engine_lib, oracle_mod
         want = sorted((trec[r["target"]].id, (r["s_start"], r["s_end"]), (r["t_start"], r["t_end"]), r["score"],
                        r["sequence_match"]) for r in ref[(qi, qi)] + ref[(qi, qi + 3)])
         assert got_d == want
+    # all pairs in one call through the public pairs API
+    prog = Aligner(None, None, w.settings)
+    try:
+        hl = prog.process_pairs(qrec, trec, w.pairs)
+    finally:
+        prog.smith_waterman.close()
+    got_p = sorted((h.sequence_info.id, h.target_info.id, h.seq_location, h.target_location, h.score,
+                    h.sequence_match, h.alignment, h.target_match) for h in hl.real_hits.values())
+    want_p = sorted((qrec[r["query"]].id, trec[r["target"]].id, (r["s_start"], r["s_end"]), (r["t_start"], r["t_end"]),
+                     r["score"], r["sequence_match"], r["alignment"], r["target_match"])
+                    for v in ref.values() for r in v)
+    assert got_p == want_p

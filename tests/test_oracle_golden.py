@@ -91,3 +91,15 @@ def test_genbank_case_reproduces_reference_expected_output():
     assert h["score"] == float(exp[6]) and h["matches"] == int(exp[7]) and h["mismatches"] == int(exp[8])
     assert len(h["alignment"]) == int(exp[10])
     assert abs(h["score"] / len(h["alignment"]) - float(exp[11])) < 1e-9
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_reference_emits_starting_points_in_launch_order(name):
+    """Within a batch the reference's kernels, run one launch and one block
+    after another, emit starting points by block anti-diagonal descending,
+    block x descending, target, query, cell anti-diagonal descending, row --
+    the order pw_get_starting_points reports."""
+    fx = G.load(name)
+    for b in fx.get("batches", []):
+        keys = [(-(u[2] + u[3]), -u[2], u[1], u[0], -(u[4] + u[5]), u[5]) for u in b["starts_u32"]]
+        assert keys == sorted(keys)
