@@ -86,6 +86,11 @@ def parse():
                          "--tune chain_min=250; without chain_min the autotuner picks it during the warm-up")
     ap.add_argument("--serve-seconds", type=float, default=6.0, help="length of each arrival stream of the serving leg")
     ap.add_argument("--serve-loads", default="0.3,0.5,0.6,0.7", help="offered loads (fractions of batched peak) swept")
+    ap.add_argument("--serve-streams", type=int, default=1,
+                    help="arrival streams per offered load (different seeds); the report gives the median p99")
+    ap.add_argument("--serve-workers", type=int, default=2)
+    ap.add_argument("--serve-max-batch", type=int, default=32)
+    ap.add_argument("--serve-policy", type=int, default=0, help="0 arrival order, 1 shortest first with aging")
     return ap.parse_args()
 
 
@@ -571,7 +576,7 @@ def parity_leg(w, jobs, idx, oracle_res, device):
 
 
 # ------------------------------------------------------------------ serving
-def serve_leg(device, seconds, loads, workers=2, max_batch=32):
+def serve_leg(device, seconds, loads, workers=2, max_batch=32, policy=0, streams=1, age_ms=25):
     """Serving configuration: a resident database of 100,000 protein sequences
     (log-normal lengths, median 300, 50-1,500 aa), Poisson arrivals of single
     queries (log-normal, median 300, max 5,000 aa), 70% top-10 by pair maximum
@@ -586,25 +591,39 @@ def serve_leg(device, seconds, loads, workers=2, max_batch=32):
     sweep = []
     try:
         srv.load_db(db)
+        srv.tune(_native_const("PW_SERVE_TUNE_POLICY"), policy)
+        srv.tune(_native_const("PW_SERVE_TUNE_AGE_MS"), age_ms)
         serving.run_arrivals(srv, workloads.query_stream(seed=8, n=16, rate_hz=1e9))
         peak = serving.run_arrivals(srv, workloads.query_stream(seed=7, n=64, rate_hz=1e9))
         probe = workloads.query_stream(seed=9, n=4000, rate_hz=1.0)
         mean_cells = float(np.mean([len(q[2]) for q in probe])) * srv.db_residues
         for k, load in enumerate(loads):
             rate = load * peak["gcups"] * 1e9 / mean_cells
-            stream = workloads.query_stream(seed=60 + k, n=max(20, int(rate * seconds)), rate_hz=rate)
-            rep = serving.run_arrivals(srv, stream)
-            sweep.append({"offered_load": load, "offered_rps": rep["offered_rps"], "gcups": rep["gcups"],
-                          "fraction_of_peak": rep["gcups"] / peak["gcups"], "p50_ms": rep["p50_ms"],
-                          "p99_ms": rep["p99_ms"], "max_ms": rep["max_ms"], "p99_top_ms": rep["p99_top_ms"],
-                          "p99_traceback_ms": rep["p99_traceback_ms"], "requests": rep["requests"],
-                          "mean_batch": rep["mean_batch"], "workers_used": rep["workers_used"],
-                          "peak_reserved_bytes": rep["peak_reserved_bytes"]})
+            reps = []
+            for j in range(max(1, streams)):
+                stream = workloads.query_stream(seed=60 + k + 100 * j, n=max(20, int(rate * seconds)), rate_hz=rate)
+                reps.append(serving.run_arrivals(srv, stream))
+            med = lambda key: float(np.median([r[key] for r in reps]))
+            sweep.append({"offered_load": load, "offered_rps": med("offered_rps"), "gcups": med("gcups"),
+                          "fraction_of_peak": med("gcups") / peak["gcups"], "p50_ms": med("p50_ms"),
+                          "p99_ms": med("p99_ms"), "p99_ms_streams": [round(r["p99_ms"], 2) for r in reps],
+                          "max_ms": max(r["max_ms"] for r in reps), "p99_top_ms": med("p99_top_ms"),
+                          "p99_traceback_ms": med("p99_traceback_ms"), "p99_queue_ms": med("p99_queue_ms"),
+                          "p99_run_ms": med("p99_run_ms"), "mean_run_ms": med("mean_run_ms"),
+                          "requests": sum(r["requests"] for r in reps), "mean_batch": med("mean_batch"),
+                          "workers_used": max(r["workers_used"] for r in reps),
+                          "peak_reserved_bytes": max(r["peak_reserved_bytes"] for r in reps)})
     finally:
         srv.close()
     return {"db": "%d sequences, %d residues, resident" % (len(db), srv.db_residues),
-            "workers": workers, "max_batch": max_batch, "batched_peak_gcups": peak["gcups"],
-            "seconds_per_rate": seconds, "sweep": sweep}
+            "workers": workers, "max_batch": max_batch, "policy": ["arrival order", "shortest first"][policy],
+            "batched_peak_gcups": peak["gcups"], "seconds_per_stream": seconds, "streams_per_load": streams,
+            "sweep": sweep}
+
+
+def _native_const(name):
+    from pypaswas_b200 import _native
+    return getattr(_native, name)
 
 
 # ------------------------------------------------------------------ one config
@@ -729,7 +748,9 @@ def main():
                 out["configs"][NAMES[c]] = rec
                 del wc
         if not args.no_serve and rank == 0 and world == 1 and args.config == 2:
-            out["serve"] = serve_leg(local, args.serve_seconds, [float(x) for x in args.serve_loads.split(",")])
+            out["serve"] = serve_leg(local, args.serve_seconds, [float(x) for x in args.serve_loads.split(",")],
+                                     workers=args.serve_workers, max_batch=args.serve_max_batch,
+                                     policy=args.serve_policy, streams=args.serve_streams)
     finally:
         sampler.stop()
     if rank == 0:

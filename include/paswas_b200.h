@@ -317,7 +317,18 @@ int pw_server_wait(pw_server* s, int64_t ticket, int32_t timeout_ms, pw_request_
 int pw_server_top_hits(pw_server* s, int64_t ticket, int32_t* targets, float* scores, int32_t k);
 int pw_server_hits(pw_server* s, int64_t ticket, pw_hit* hits, int64_t max_hits, char* strbuf,
                    int64_t strbuf_bytes);
-/* pw_set_tuning on every worker engine. */
+/* pw_set_tuning on every worker engine, or, for the keys below, a setting of
+ * the server's own scheduler:
+ *   PW_SERVE_TUNE_POLICY   0: batches in arrival order (default); 1: the
+ *                          shortest waiting queries first, except that a
+ *                          request waiting longer than PW_SERVE_TUNE_AGE_MS
+ *                          goes first (no request starves)
+ *   PW_SERVE_TUNE_AGE_MS   the waiting time after which policy 1 serves a
+ *                          request in arrival order (default 25)
+ *   PW_SERVE_TUNE_MAX_BATCH  requests per batch (as at pw_server_create) */
+#define PW_SERVE_TUNE_POLICY 100
+#define PW_SERVE_TUNE_AGE_MS 101
+#define PW_SERVE_TUNE_MAX_BATCH 102
 int pw_server_tune(pw_server* s, int key, int64_t value);
 /* Frees a finished request's results. */
 int pw_server_release(pw_server* s, int64_t ticket);

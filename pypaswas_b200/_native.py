@@ -38,6 +38,9 @@ PW_TUNE_CAND_SLOT = 4
 PW_TUNE_WAIT_NS = 5
 PW_TUNE_STALL_TEST = 6
 PW_TUNE_LANES = 7
+PW_SERVE_TUNE_POLICY = 100
+PW_SERVE_TUNE_AGE_MS = 101
+PW_SERVE_TUNE_MAX_BATCH = 102
 PW_FORMAT_FASTA = 0
 PW_FORMAT_FASTQ = 1
 PW_RECORDS_AS_READ = 0

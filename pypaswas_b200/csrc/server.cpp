@@ -64,6 +64,8 @@ struct Worker {
 struct pw_server {
     int device = 0;
     int max_batch = 16;
+    int policy = 0;              // PW_SERVE_TUNE_POLICY
+    double age_ms = 25.0;        // PW_SERVE_TUNE_AGE_MS
     int64_t budget = 0;          // direction-matrix bytes shared by all traceback batches
     int64_t in_use = 0;          // reserved by running batches
     int64_t peak_in_use = 0;
@@ -100,6 +102,20 @@ std::vector<Request*> take_batch(pw_server* s, int64_t* reserve) {
     std::vector<Request*> batch;
     *reserve = 0;
     if (s->pending.empty()) return batch;
+    if (s->policy == 1) {
+        // shortest first, requests past the age limit first of all (oldest
+        // first among them): the pending queue is reordered that way, and
+        // the batch is then taken from its front as in arrival order
+        const double now = now_ms();
+        std::vector<Request*> v(s->pending.begin(), s->pending.end());
+        std::stable_sort(v.begin(), v.end(), [&](const Request* a, const Request* b) {
+            const bool oa = now - a->t_submit >= s->age_ms, ob = now - b->t_submit >= s->age_ms;
+            if (oa != ob) return oa;
+            if (oa) return a->t_submit < b->t_submit;
+            return a->residues.size() < b->residues.size();
+        });
+        s->pending.assign(v.begin(), v.end());
+    }
     int mode = s->pending.front()->mode;
     if (mode == PW_SERVE_TRACEBACK) {
         Request* r = s->pending.front();
@@ -327,6 +343,20 @@ extern "C" int pw_server_set_scoring(pw_server* s, const float* matrix, int dim,
 
 extern "C" int pw_server_tune(pw_server* s, int key, int64_t value) {
     if (!s) return PW_ERR_ARG;
+    if (key >= PW_SERVE_TUNE_POLICY) {
+        std::lock_guard<std::mutex> g(s->mu);
+        if (key == PW_SERVE_TUNE_POLICY && (value == 0 || value == 1)) {
+            s->policy = (int)value;
+        } else if (key == PW_SERVE_TUNE_AGE_MS && value >= 0) {
+            s->age_ms = (double)value;
+        } else if (key == PW_SERVE_TUNE_MAX_BATCH && value >= 1 && value <= 4096) {
+            s->max_batch = (int)value;
+        } else {
+            s->err = "unknown server setting or value out of range";
+            return PW_ERR_ARG;
+        }
+        return PW_OK;
+    }
     for (Worker& w : s->workers) {
         const int rc = pw_set_tuning(w.engine, key, value);
         if (rc != PW_OK) return server_fail(s, rc, pw_last_error(w.engine));

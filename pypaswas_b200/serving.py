@@ -191,6 +191,9 @@ def run_arrivals(server, stream, keep_results=False):
            "p99_traceback_ms": percentile(lat_tb, 99) if lat_tb else None,
            "offered_rps": len(stream) / span if span > 0 else None, "served_rps": len(stream) / wall,
            "mean_batch": float(np.mean([i["batch_queries"] for i in infos])),
+           "p99_queue_ms": percentile([i["queue_ms"] for i in infos], 99),
+           "p99_run_ms": percentile([i["run_ms"] for i in infos], 99),
+           "mean_run_ms": float(np.mean([i["run_ms"] for i in infos])),
            "workers_used": len(set(i["worker"] for i in infos)),
            "peak_reserved_bytes": server.stats()["peak_reserved_bytes"]}
     if keep_results:
