@@ -70,6 +70,9 @@ def parse():
                     help="further configurations in the same line, e.g. 1,3,4; 'auto' = the other three when the "
                          "headline is config 2, 'none' = headline only")
     ap.add_argument("--reads", type=int, default=10_000_000, help="config 4: number of reads")
+    ap.add_argument("--pairs", type=int, default=64,
+                    help="config 3: number of long pairs, each aligned with the target and its reverse complement "
+                         "(small cases for ncu captures)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="length of the headline's CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--targets", type=int, default=0,
@@ -101,7 +104,7 @@ def workload(cfg, args, seed=None):
     if cfg == 1:
         return workloads.config1(**kw)
     if cfg == 3:
-        return workloads.config3(**kw)
+        return workloads.config3(n_pairs=args.pairs, **kw)
     if cfg == 4:
         return workloads.config4(n_reads=args.reads, **kw)
     w = workloads.config2(**kw)

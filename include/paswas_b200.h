@@ -428,6 +428,13 @@ int pw_records_sizes(const pw_records* r, int64_t* n_records, int64_t* residue_b
 /* Copies the packed records into caller buffers sized from pw_records_sizes. */
 int pw_records_copy(const pw_records* r, uint8_t* residues, int64_t* offsets, char* ids, int64_t* id_offsets);
 void pw_records_free(pw_records* r);
+/* Dense ranks of n byte strings blob[off[i], off[i + 1]) in byte order (a
+ * prefix before its extensions; equal strings share a rank): Python's string
+ * order of ASCII record ids, which HitList de-duplication and the formatters'
+ * (query id, target id, score) sort compare (HitList.py:28-52,
+ * Formatters.py:34-37).  The formatters take these ranks (pw_trimmed_fasta,
+ * pw_txt_records). */
+int pw_id_ranks(const char* blob, const int64_t* off, int64_t n, int32_t* ranks);
 
 #ifdef __cplusplus
 }

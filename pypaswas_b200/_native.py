@@ -60,6 +60,7 @@ EXPORTED_SYMBOLS = (
     "pw_server_load_db", "pw_server_submit", "pw_server_wait", "pw_server_top_hits", "pw_server_hits",
     "pw_server_release", "pw_server_stats", "pw_server_tune", "pw_trimmed_fasta", "pw_txt_records",
     "pw_records_parse", "pw_records_read", "pw_records_sizes", "pw_records_copy", "pw_records_free",
+    "pw_id_ranks",
 )
 
 
@@ -171,6 +172,7 @@ def bind(lib):
                                             ctypes.POINTER(I64)]),
         "pw_records_copy": (ctypes.c_int, [P, P, P, P, P]),
         "pw_records_free": (None, [P]),
+        "pw_id_ranks": (ctypes.c_int, [P, P, I64, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

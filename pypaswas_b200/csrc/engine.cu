@@ -32,6 +32,7 @@
 #include "pw_band.cuh"
 #include "pw_plan.h"
 #include "pw_finish.cuh"
+#include "pw_host.h"
 
 using namespace pw;
 
@@ -59,19 +60,6 @@ struct HostTrace {
     }
 };
 
-template <typename F>
-static void parallel_for(int64_t n, F&& f, int64_t min_chunk = 1 << 15) {
-    const int64_t hw = std::max<int64_t>(1, (int64_t)std::thread::hardware_concurrency());
-    const int T = (int)std::min<int64_t>(std::min<int64_t>(hw, 32), std::max<int64_t>(1, n / min_chunk));
-    if (T <= 1) {
-        f((int64_t)0, n);
-        return;
-    }
-    std::vector<std::thread> th;
-    th.reserve(T);
-    for (int k = 0; k < T; ++k) th.emplace_back([&, k] { f(n * k / T, n * (k + 1) / T); });
-    for (auto& t : th) t.join();
-}
 
 // Host array in page-locked memory when the driver grants it (faster device
 // copies of large results such as the pair maxima), else in ordinary memory.
@@ -257,7 +245,7 @@ struct pw_engine {
     HostBuf<int32_t> h_ptq, h_p2order;  // phase-2 pair lists (kept across calls: no page faults, no zero fill)
     int64_t free_mem = 0;    // free device memory plus this engine's kept wave buffers, as last queried
     double free_mem_t = -1;  // wall_ms() of that query
-    DevBuf chain_items, chain_info, chain_prog, chain_max, chain_ring_off, chain_ring, chain_abort, p1_items;
+    DevBuf chain_items, chain_info, chain_prog, chain_max, chain_ring_off, chain_ring, chain_abort, p1_items, p1_grid;
     // plan of the 16-bit score phase (work items, classes, chain queue), kept
     // on the device and reused while inputs, scoring, flags and tuning stay
     struct {
@@ -268,6 +256,10 @@ struct pw_engine {
         int begin[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         int xm_multi = 4;
         int n_chain_items = 0;
+        // grid form: one-strip classes as strip-pair lists (p1_grid) x lane groups
+        bool grid = false;
+        int gbegin[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        int n_groups = 0;
     } p1;
     DevBuf codes, marks, metas, cands, cands_alt, cand_base, cand_cap, n_cand, n_starts, start_off, starts, hits,
         hit_count, ops, allowed;
@@ -280,6 +272,7 @@ struct pw_engine {
     int64_t tune[8] = {0, 0, 0, 0, 0, 0, 0, 0};      // pw_set_tuning values (0: automatic)
     // results
     HostBuf<float> h_pair_max;
+    bool pm_stale = false;  // h_pair_max lags the device maxima (copied on pw_get_pair_max)
     HostBuf<pw_hit> h_hits;
     HostBuf<char> h_strings;
     HostBuf<StartRec> h_starts;
@@ -559,6 +552,18 @@ static cudaError_t download(pw_engine* e, HostBuf<float>& v, const void* src, si
     cudaError_t c = copy_d2h(e, v.data(), src, n * sizeof(float));
     if (c != cudaSuccess) return c;
     return cudaStreamSynchronize(e->stream);
+}
+
+// Brings the host copy of the pair maxima up to date (the batched sweeps
+// leave them on the device, where pruning and the trace kernels read them).
+static int sync_pair_max(pw_engine* e, const float* dev) {
+    if (!e->pm_stale) return PW_OK;
+    cudaError_t c;
+    if ((c = download(e, e->h_pair_max, dev, e->h_pair_max.size())) != cudaSuccess ||
+        (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
+        return cuda_fail(e, c, "copy pair maxima");
+    e->pm_stale = false;
+    return PW_OK;
 }
 
 template <typename HT>
@@ -859,34 +864,23 @@ static void order_by_class(std::vector<WorkItem>& items, std::vector<int>& cls, 
     cls.swap(c2);
 }
 
+// Phase-1 work items above which the one-strip classes take the grid form
+// (strip-pair lists, items formed on the device) instead of an item list.
+constexpr int64_t kGridItems = (int64_t)1 << 18;
+
 // Order of items by strip class ascending, then cost descending, ties in
 // their current order (what a stable sort by cost followed by a stable sort
 // by class gives): an LSD radix sort of (class, ~cost) keys, 16 bits a pass,
-// stopping once every key agrees in the digits left.  Linear in the item
-// count: millions of work items (short reads) are ordered in milliseconds.
+// skipping the digits in which every key agrees.  Linear in the item count:
+// millions of work items (short reads) are ordered in milliseconds.
 static std::vector<uint32_t> class_cost_order(const std::vector<int>& cls, const std::vector<int64_t>& cost) {
-    const size_t n = cls.size();
     constexpr uint64_t kCostMask = ((uint64_t)1 << 48) - 1;
-    std::vector<uint64_t> key(n);
-    uint64_t lo = ~(uint64_t)0, hi = 0;
-    for (size_t k = 0; k < n; ++k) {
+    std::vector<uint64_t> key(cls.size());
+    for (size_t k = 0; k < key.size(); ++k) {
         const uint64_t c = std::min<uint64_t>((uint64_t)std::max<int64_t>(cost[k], 0), kCostMask);
         key[k] = ((uint64_t)cls[k] << 48) | (kCostMask - c);
-        lo = std::min(lo, key[k]);
-        hi = std::max(hi, key[k]);
     }
-    std::vector<uint32_t> idx(n), tmp(n);
-    std::iota(idx.begin(), idx.end(), 0u);
-    std::vector<uint32_t> cnt(65537);
-    for (int shift = 0; shift < 64 && n > 0; shift += 16) {
-        if (((lo ^ hi) >> shift) == 0) break;  // every key agrees from this digit up
-        std::fill(cnt.begin(), cnt.end(), 0u);
-        for (size_t k = 0; k < n; ++k) cnt[((key[idx[k]] >> shift) & 0xffff) + 1]++;
-        for (int d = 0; d < 65536; ++d) cnt[d + 1] += cnt[d];
-        for (size_t k = 0; k < n; ++k) tmp[cnt[(key[idx[k]] >> shift) & 0xffff]++] = idx[k];
-        idx.swap(tmp);
-    }
-    return idx;
+    return radix_order(std::move(key));
 }
 
 
@@ -1074,9 +1068,25 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uin
         std::vector<int> cls;
         std::vector<int64_t> cost;
         const int strip_step = dual ? 1 : 2, lane_step = dual ? 2 * kWarp : kWarp;
+        // Many items (short reads against a few targets): the one-strip
+        // classes go as strip-pair lists, their items formed on the device
+        // (grid_item), lane groups longest first; the chained class keeps its
+        // explicit queue.
+        const int64_t n_groups = (n_lane + lane_step - 1) / lane_step;
+        const int64_t n_pairs_s = (n_strip + strip_step - 1) / strip_step;
+        if (n_pairs_s * n_groups > (int64_t)INT32_MAX) return fail(e, PW_ERR_CAPACITY, "too many work items");
+        const bool grid = n_pairs_s * n_groups > kGridItems;
+        std::vector<int2> gstrips[kNumClasses];
         for (int i = 0; i < n_strip; i += strip_step) {
             const int sa = strip_order[i], sb = !dual && i + 1 < n_strip ? strip_order[i + 1] : -1;
             const int ls = std::max(strip_len[sa], sb >= 0 ? strip_len[sb] : 0);
+            if (grid) {
+                const int k = pick_class16(ls, e->affine);
+                if (k != kS32Multi) {
+                    gstrips[k].push_back(make_int2(sa, sb));
+                    continue;
+                }
+            }
             for (int g = 0; g < n_lane; g += lane_step) {
                 WorkItem w;
                 memset(&w, 0, sizeof(w));
@@ -1106,6 +1116,17 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uin
         for (int k : c2) begin[k + 1]++;
         for (int k = 0; k < kNumClasses; ++k) begin[k + 1] += begin[k];
         if ((c = upload(e, e->p1_items, it2)) != cudaSuccess) return cuda_fail(e, c, "upload items");
+        {
+            std::vector<int2> gs;
+            for (int k = 0; k < kNumClasses; ++k) {
+                P1.gbegin[k] = (int)gs.size();
+                gs.insert(gs.end(), gstrips[k].begin(), gstrips[k].end());
+            }
+            P1.gbegin[kNumClasses] = (int)gs.size();
+            if ((c = upload(e, e->p1_grid, gs)) != cudaSuccess) return cuda_fail(e, c, "upload strip pairs");
+            P1.grid = grid;
+            P1.n_groups = (int)n_groups;
+        }
         int xm = 4;
         for (int k = begin[kS32Multi]; k < begin[kS32Multi + 1]; ++k) xm = std::max(xm, (int)align_up(it2[k].xmax, 4));
         P1.chained = !(flags & PW_FLAG_NO_CHAIN) && begin[kS32Multi + 1] > begin[kS32Multi];
@@ -1230,18 +1251,26 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uin
         S.items = e->p1_items.as<WorkItem>() + begin[k];
         S.n_items = n;
         S.counter = e->counter.as<int>() + k;
+        S.grid_strips = nullptr;
+        c = dual ? launch_s16_class<true>(e, k, e->affine, S) : launch_s16_class<false>(e, k, e->affine, S);
+        if (c != cudaSuccess) return cuda_fail(e, c, "score16 launch");
+        inf.score_launches++;
+    }
+    for (int k = 0; P1.grid && k < kNumClasses; ++k) {
+        const int np_ = P1.gbegin[k + 1] - P1.gbegin[k];
+        if (np_ <= 0 || k == kS32Multi) continue;
+        S.items = nullptr;
+        S.grid_strips = e->p1_grid.as<int2>() + P1.gbegin[k];
+        S.grid_n_strips = np_;
+        S.grid_lane_step = dual ? 2 * kWarp : kWarp;
+        S.grid_n_lane = trans ? nt : nq;
+        S.n_items = (int)((int64_t)np_ * P1.n_groups);
+        S.counter = e->counter.as<int>() + k;
         c = dual ? launch_s16_class<true>(e, k, e->affine, S) : launch_s16_class<false>(e, k, e->affine, S);
         if (c != cudaSuccess) return cuda_fail(e, c, "score16 launch");
         inf.score_launches++;
     }
     cudaEventRecord(b, e->stream);
-    if ((c = download(e, e->h_pair_max, A32.pair_max, (size_t)nq * nt)) != cudaSuccess)
-        return cuda_fail(e, c, "copy pair maxima");
-    float ms = 0;
-    cudaEventElapsedTime(&ms, a, b);
-    inf.score_kernel_ms += ms;
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
     int status[2] = {0, 0};  // overflow count, chain abort flag
     if ((c = copy_d2h(e, &status[0], S.ovf_count, sizeof(int))) != cudaSuccess ||
         (chained &&
@@ -1249,7 +1278,19 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uin
              cudaSuccess) ||
         (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
         return cuda_fail(e, c, "read score status");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    inf.score_kernel_ms += ms;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
     if (status[1]) return fail(e, PW_ERR_KERNEL, "chained score sweep: a strip waited too long for its predecessor");
+    // the maxima stay on the device (pruning reads them there); the host
+    // copy is needed only to find the pairs that reached the 16-bit limit
+    e->pm_stale = true;
+    if (status[0] > 0) {
+        const int rc = sync_pair_max(e, A32.pair_max);
+        if (rc != PW_OK) return rc;
+    }
 
     // pairs that reached the 16-bit limit: the 32-bit sweep, per target
     std::vector<std::vector<int32_t>> ovf(nt);
@@ -1291,8 +1332,7 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uin
     A.q_order = e->q_order2.as<int32_t>();
     int rc = run_phase<1>(e, A, e->items.as<WorkItem>(), bg, xm, &inf.score_kernel_ms, &inf.score_launches);
     if (rc != PW_OK) return rc;
-    if ((c = download(e, e->h_pair_max, A32.pair_max, (size_t)nq * nt)) != cudaSuccess)
-        return cuda_fail(e, c, "copy pair maxima");
+    e->pm_stale = true;
     return PW_OK;
 }
 
@@ -1544,6 +1584,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     memset(&inf, 0, sizeof(inf));
     const int nq = e->Q.n, nt = e->T.n;
     if (!e->h_pair_max.resize((size_t)nq * nt)) return fail(e, PW_ERR_NOMEM, "host pair maxima");
+    e->pm_stale = false;
     inf.pairs = (int64_t)nq * nt;
     int64_t sumq = 0, sumt = 0;
     for (int i = 0; i < nq; ++i) sumq += e->Q.off[i + 1] - e->Q.off[i];
@@ -1715,8 +1756,8 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
             if (rc != PW_OK) return rc;
         }
         cudaEventRecord(e->ev[1], e->stream);
-        if ((c = download(e, e->h_pair_max, A.pair_max, (size_t)nq * nt)) != cudaSuccess)
-            return cuda_fail(e, c, "copy pair maxima");
+        if ((c = cudaEventSynchronize(e->ev[1])) != cudaSuccess) return cuda_fail(e, c, "score sweep");
+        e->pm_stale = true;
         float ms = 0;
         cudaEventElapsedTime(&ms, e->ev[0], e->ev[1]);
         inf.score_ms = ms;
@@ -1729,6 +1770,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     }
     if (pair_mode) {
         // pairs outside the list get -1: below MINIMUM_SCORE, never traced
+        if (const int r = sync_pair_max(e, A.pair_max)) return r;
         std::vector<uint8_t> listed((size_t)nq * nt, 0);
         for (size_t k = 0; k < e->pair_q.size(); ++k) listed[(size_t)e->pair_q[k] * nt + e->pair_t[k]] = 1;
         for (size_t k = 0; k < listed.size(); ++k)
@@ -2359,6 +2401,11 @@ extern "C" int pw_set_wave_limit(pw_engine* e, int64_t bytes) {
 extern "C" int pw_get_pair_max(pw_engine* e, float* out, int64_t n) {
     if (!e || !out) return PW_ERR_ARG;
     if (n < (int64_t)e->h_pair_max.size()) return fail(e, PW_ERR_ARG, "output too small");
+    if (e->pm_stale) {
+        if (cudaSetDevice(e->device) != cudaSuccess) return fail(e, PW_ERR_DEVICE, "cudaSetDevice failed");
+        const int rc = sync_pair_max(e, e->pair_max.as<float>());
+        if (rc != PW_OK) return rc;
+    }
     std::memcpy(out, e->h_pair_max.data(), e->h_pair_max.size() * sizeof(float));
     return PW_OK;
 }

@@ -10,6 +10,7 @@
 // caller (Python's string order), so ordering and de-duplication compare
 // integers; the target ids arrive with the "_RC" suffix already stripped.
 #include <algorithm>
+#include <atomic>
 #include <charconv>
 #include <cmath>
 #include <cstdint>
@@ -17,6 +18,8 @@
 #include <cstring>
 #include <string>
 #include <vector>
+
+#include "pw_host.h"
 
 #include "../../include/paswas_b200.h"
 
@@ -102,43 +105,45 @@ struct Rec {
 
 }  // namespace
 
-// The driver's HitList for these records: locations checked as the Hit
-// constructor checks them (Hit.py:16-60; any invalid one fails the call, as
-// the reference's exception does), the filter (SmithWaterman._filter_hit),
-// HitList.append in walk order, then HitList.real_hits sorted by (query id,
-// target id, score), stable (Formatters.py:34-37).  `real` keeps Python's
-// dict order: a new key goes last, a replaced one keeps its place, a deleted
-// one is gone.
-static int ordered_real_hits(const pw_hit* hits, int64_t n_hits, int32_t n_queries, int32_t n_targets,
-                             const int32_t* q_rank, const int64_t* q_orig_len, const int64_t* q_start_pos,
-                             const int32_t* t_rank, const int64_t* t_orig_len, const int64_t* t_start_pos,
-                             const double* thresholds, std::vector<Rec>& rec, std::vector<int64_t>& order) {
-    rec.resize((size_t)n_hits);
-    for (int64_t i = 0; i < n_hits; ++i) {
-        const pw_hit& h = hits[i];
-        const int q = h.query, t = h.target;
-        if (q < 0 || q >= n_queries || t < 0 || t >= n_targets) return PW_ERR_ARG;
-        const int64_t s0 = h.s_start + q_start_pos[q], s1 = h.s_end + q_start_pos[q];
-        const int64_t t0 = h.t_start + t_start_pos[t], t1 = h.t_end + t_start_pos[t];
-        if (!(0 <= s0 && s0 < s1 && s1 < q_orig_len[q] && 0 <= t0 && t0 < t1 && t1 < t_orig_len[t]))
-            return PW_ERR_ARG;
-        rec[i] = Rec{q, t, q_rank[q], t_rank[t], s0, t0, t1, (double)h.score};
+// Key -> int64 over a handful of entries: a linear scan (most (query,
+// target) groups hold one or two hits).
+struct SmallMap {
+    std::vector<std::pair<Key, int64_t>> v;
+    int64_t* find(const Key& k) {
+        for (auto& e : v)
+            if (e.first == k) return &e.second;
+        return nullptr;
     }
-    FlatMap best((size_t)n_hits * 2);   // key -> hit
-    FlatMap real_pos((size_t)n_hits);   // start key -> slot of `real`
-    std::vector<int64_t> real;          // slot -> hit (-1: deleted)
-    real.reserve((size_t)n_hits);
-    for (int64_t i = 0; i < n_hits; ++i) {
-        const pw_hit& h = hits[i];
+    void put(const Key& k, int64_t x) {
+        if (int64_t* f = find(k))
+            *f = x;
+        else
+            v.push_back({k, x});
+    }
+    void erase(const Key& k) {
+        for (size_t i = 0; i < v.size(); ++i)
+            if (v[i].first == k) {
+                v[i] = v.back();
+                v.pop_back();
+                return;
+            }
+    }
+};
+
+// HitList.append (HitList.py:28-52) over the hits of one (query id, target
+// id) group in walk order: `best` maps a start or end key to its hit,
+// `real_pos` a start key to its slot of `real` (Python's dict order: a new
+// key goes last, a replaced one keeps its place, a deleted one is gone).
+// Survivors go to `out` ordered by score, ties in slot order; returns their
+// number.
+template <typename Map>
+static int64_t append_group(const pw_hit* hits, const Rec* rec, const int64_t* q_start_pos, const uint32_t* grp,
+                            int64_t n, Map& best, Map& real_pos, std::vector<int64_t>& real, int64_t* out) {
+    real.clear();
+    for (int64_t g = 0; g < n; ++g) {
+        const int64_t i = grp[g];
         const Rec& r = rec[i];
-        const int64_t s1 = h.s_end + q_start_pos[r.q];
-        const double span = (double)(s1 - r.s0 + 1);
-        const double rel = r.score / (double)std::min(q_orig_len[r.q], t_orig_len[r.t]);
-        const double ident = (double)h.matches / span;
-        const double cov = span / (double)q_orig_len[r.q];
-        const double base = r.score / (double)h.n_cols;
-        if (!(rel >= thresholds[0] && ident >= thresholds[1] && cov >= thresholds[2] && base >= thresholds[3]))
-            continue;
+        const int64_t s1 = hits[i].s_end + q_start_pos[r.q];
         const Key k0{r.qr, r.tr, r.s0, r.t0}, k1{r.qr, r.tr, s1, r.t1};
         const int64_t* f0 = best.find(k0);
         const int64_t* f1 = best.find(k1);
@@ -162,22 +167,113 @@ static int ordered_real_hits(const pw_hit* hits, int64_t n_hits, int32_t n_queri
             }
         }
     }
-    struct SortKey {
-        int32_t qr, tr;
-        double score;
-        int64_t hit;
-    };
-    std::vector<SortKey> sk;
-    sk.reserve(real.size());
+    int64_t m = 0;
     for (int64_t i : real)
-        if (i >= 0) sk.push_back(SortKey{rec[i].qr, rec[i].tr, rec[i].score, i});
-    std::stable_sort(sk.begin(), sk.end(), [](const SortKey& x, const SortKey& y) {
-        if (x.qr != y.qr) return x.qr < y.qr;
-        if (x.tr != y.tr) return x.tr < y.tr;
-        return x.score < y.score;
-    });
-    order.resize(sk.size());
-    for (size_t k = 0; k < sk.size(); ++k) order[k] = sk[k].hit;
+        if (i >= 0) out[m++] = i;
+    std::stable_sort(out, out + m, [&](int64_t a, int64_t b) { return rec[a].score < rec[b].score; });
+    return m;
+}
+
+// The driver's HitList for these records: locations checked as the Hit
+// constructor checks them (Hit.py:16-60; any invalid one fails the call, as
+// the reference's exception does), the filter (SmithWaterman._filter_hit),
+// HitList.append in walk order, then HitList.real_hits sorted by (query id,
+// target id, score), stable (Formatters.py:34-37).  Every key that
+// HitList.append looks up carries the hit's two ids, so hits of different
+// (query id, target id) groups never meet: the passing hits are grouped by
+// their id ranks (a stable radix sort keeps walk order inside a group), the
+// groups run the append rule independently on host threads, and the
+// survivors come out in group order, by score inside a group, ties in the
+// order their keys entered the dict.
+static int ordered_real_hits(const pw_hit* hits, int64_t n_hits, int32_t n_queries, int32_t n_targets,
+                             const int32_t* q_rank, const int64_t* q_orig_len, const int64_t* q_start_pos,
+                             const int32_t* t_rank, const int64_t* t_orig_len, const int64_t* t_start_pos,
+                             const double* thresholds, std::vector<Rec>& rec, std::vector<int64_t>& order) {
+    rec.resize((size_t)n_hits);
+    std::vector<uint8_t> pass((size_t)n_hits, 0);
+    std::atomic<bool> bad{false};
+    int64_t max_tr = 0;
+    for (int32_t t = 0; t < n_targets; ++t) max_tr = std::max<int64_t>(max_tr, t_rank[t]);
+    parallel_for(n_hits, [&](int64_t i0, int64_t i1) {
+        bool ok = true;
+        for (int64_t i = i0; i < i1; ++i) {
+            const pw_hit& h = hits[i];
+            const int q = h.query, t = h.target;
+            if (q < 0 || q >= n_queries || t < 0 || t >= n_targets) {
+                ok = false;
+                break;
+            }
+            const int64_t s0 = h.s_start + q_start_pos[q], s1 = h.s_end + q_start_pos[q];
+            const int64_t t0 = h.t_start + t_start_pos[t], t1 = h.t_end + t_start_pos[t];
+            if (!(0 <= s0 && s0 < s1 && s1 < q_orig_len[q] && 0 <= t0 && t0 < t1 && t1 < t_orig_len[t])) {
+                ok = false;
+                break;
+            }
+            const Rec r{q, t, q_rank[q], t_rank[t], s0, t0, t1, (double)h.score};
+            rec[i] = r;
+            // SmithWaterman._filter_hit
+            const double span = (double)(s1 - s0 + 1);
+            const double rel = r.score / (double)std::min(q_orig_len[q], t_orig_len[t]);
+            const double ident = (double)h.matches / span;
+            const double cov = span / (double)q_orig_len[q];
+            const double base = r.score / (double)h.n_cols;
+            pass[i] = rel >= thresholds[0] && ident >= thresholds[1] && cov >= thresholds[2] && base >= thresholds[3];
+        }
+        if (!ok) bad = true;
+    }, 1 << 16);
+    if (bad) return PW_ERR_ARG;
+    std::vector<uint64_t> key;
+    std::vector<uint32_t> hit_of;
+    key.reserve((size_t)n_hits);
+    hit_of.reserve((size_t)n_hits);
+    for (int64_t i = 0; i < n_hits; ++i)
+        if (pass[i]) {
+            key.push_back((uint64_t)rec[i].qr * (uint64_t)(max_tr + 1) + (uint64_t)rec[i].tr);
+            hit_of.push_back((uint32_t)i);
+        }
+    const int64_t m = (int64_t)key.size();
+    std::vector<uint32_t> grp;  // passing hits, grouped, walk order inside a group
+    {
+        std::vector<uint64_t> k2 = key;
+        const std::vector<uint32_t> o = radix_order(std::move(k2));
+        grp.resize((size_t)m);
+        for (int64_t k = 0; k < m; ++k) grp[k] = hit_of[o[k]];
+        std::vector<uint64_t> ks((size_t)m);
+        for (int64_t k = 0; k < m; ++k) ks[k] = key[o[k]];
+        key.swap(ks);
+    }
+    std::vector<int64_t> gstart;
+    for (int64_t k = 0; k < m; ++k)
+        if (k == 0 || key[k] != key[k - 1]) gstart.push_back(k);
+    const int64_t ng = (int64_t)gstart.size();
+    gstart.push_back(m);
+    std::vector<int64_t> surv((size_t)m), nsurv((size_t)ng);
+    parallel_for(ng, [&](int64_t g0, int64_t g1) {
+        SmallMap sb, sr;
+        std::vector<int64_t> real;
+        for (int64_t g = g0; g < g1; ++g) {
+            const int64_t a = gstart[g], n = gstart[g + 1] - a;
+            if (n == 1) {  // a lone hit is appended as it is
+                surv[a] = grp[a];
+                nsurv[g] = 1;
+                continue;
+            }
+            if (n <= 32) {
+                sb.v.clear();
+                sr.v.clear();
+                nsurv[g] = append_group(hits, rec.data(), q_start_pos, grp.data() + a, n, sb, sr, real, &surv[a]);
+            } else {
+                FlatMap fb((size_t)n * 2), fr((size_t)n);
+                nsurv[g] = append_group(hits, rec.data(), q_start_pos, grp.data() + a, n, fb, fr, real, &surv[a]);
+            }
+        }
+    }, 1 << 14);
+    int64_t total = 0;
+    for (int64_t g = 0; g < ng; ++g) total += nsurv[g];
+    order.resize((size_t)total);
+    int64_t w = 0;
+    for (int64_t g = 0; g < ng; ++g)
+        for (int64_t k = 0; k < nsurv[g]; ++k) order[w++] = surv[gstart[g] + k];
     return PW_OK;
 }
 

@@ -61,6 +61,14 @@ struct Score16Args {
     int item_base;               // chained launch: first queue entry of this launch (entries [item_base, n_items))
     int* ovf_count;              // pairs reported as NaN (16-bit limit reached)
     unsigned long long wait_ns;  // bound of one chain wait
+    // grid form of a one-strip class launch (no item list): item `it` is lane
+    // group it / grid_n_strips (grid_lane_step lanes from the sorted position
+    // it / grid_n_strips * grid_lane_step) against strip pair
+    // grid_strips[it % grid_n_strips] (x: strip A, y: strip B or -1)
+    const int2* grid_strips;     // null: items come from `items`
+    int grid_n_strips;
+    int grid_lane_step;          // 32, or 64 for the dual-lane form
+    int grid_n_lane;             // lane sequences in the sorted order
 };
 
 // Profile of strip rows [y0, y0 + S): for row group g (4 rows) and lane
@@ -495,6 +503,25 @@ __device__ __forceinline__ Lanes16 item_lanes(const Score16Args& A, const WorkIt
     return L;
 }
 
+// Work item `it` of a grid-form launch (see Score16Args::grid_strips).
+template <int S, bool DL>
+__device__ __forceinline__ WorkItem grid_item(const Score16Args& A, int it) {
+    const int g = it / A.grid_n_strips, p = it - g * A.grid_n_strips;
+    const int2 sp = A.grid_strips[p];
+    WorkItem W;
+    W.target = sp.x;
+    W.index = sp.y;
+    W.first = g * A.grid_lane_step;
+    W.lanes = min(kWarp, A.grid_n_lane - W.first);
+    W.lanes_hi = DL ? max(0, min(kWarp, A.grid_n_lane - W.first - kWarp)) : 0;
+    W.xmax = A.lane_len[A.lane_order[W.first]];
+    W.S = S;
+    W.orient = 0;
+    W.dir_base = 0;
+    W.pair_base = 0;
+    return W;
+}
+
 // Writes a lane's two pair maxima (NaN where the 16-bit limit was reached).
 template <bool DL>
 __device__ __forceinline__ void store_max16(const Score16Args& A, const WorkItem& W, const Lanes16& L, uint32_t mx) {
@@ -601,7 +628,7 @@ __global__ void __launch_bounds__(128) score16_kernel(Score16Args A) {
         if (lane == 0) it = atomicAdd(A.counter, 1);
         it = __shfl_sync(0xffffffffu, it, 0);
         if (it >= A.n_items) break;
-        const WorkItem W = A.items[it];
+        const WorkItem W = A.grid_strips ? grid_item<S, DL>(A, it) : A.items[it];
         const int sa = W.target, sb = DL ? -1 : W.index;
         const int la = A.strip_len[sa];
         const int lb = sb >= 0 ? A.strip_len[sb] : 0;

@@ -21,6 +21,7 @@
 // Line ends may be "\n" or "\r\n" (the reference opens files in universal
 // newline mode).
 #include <algorithm>
+#include <thread>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -29,14 +30,7 @@
 #include <vector>
 
 #include "../../include/paswas_b200.h"
-
-struct pw_records {
-    std::vector<uint8_t> res;
-    std::vector<int64_t> off;
-    std::vector<char> ids;
-    std::vector<int64_t> id_off;
-    int64_t dropped = 0;  // records removed by the length limit
-};
+#include "pw_host.h"
 
 namespace {
 
@@ -50,11 +44,32 @@ int report(char* err, int32_t err_bytes, int code, const char* fmt, ...) {
     return code;
 }
 
-// One record as parsed: title id span in the input, sequence in `seq`.
+// One record as parsed: title id span in the input, sequence in a parser
+// buffer (seq_begin there; `s` points at it once parsing is done).
 struct Rec {
     int64_t id_begin, id_len;
-    int64_t seq_begin, seq_len;  // in the parser's sequence buffer
+    int64_t seq_begin, seq_len;
+    const uint8_t* s;
 };
+
+}  // namespace
+
+// Parsed records in their output order.  The residues are written by
+// pw_records_copy straight from the parse buffers into the caller's array
+// (upper-cased, complemented or reversed on the way); ids and offsets are
+// built at parse time.
+struct pw_records {
+    std::vector<std::vector<uint8_t>> bufs;  // parsed sequence bytes (Rec::s points here)
+    std::vector<Rec> recs;
+    std::vector<int64_t> src;                // output record -> parsed record, in output order
+    std::vector<uint8_t> kind;               // 0 as read, 1 reverse complement, 2 reversed
+    std::vector<int64_t> off;
+    std::vector<char> ids;
+    std::vector<int64_t> id_off;
+    int64_t dropped = 0;  // records removed by the length limit
+};
+
+namespace {
 
 struct Lines {
     const char* p;
@@ -96,9 +111,10 @@ inline void append_seq(std::vector<uint8_t>& seq, const char* b, const char* e) 
     }
 }
 
-int parse_fasta(const char* data, int64_t n, std::vector<Rec>& recs, std::vector<uint8_t>& seq) {
-    Lines L{data, data + n};
-    seq.reserve((size_t)n);
+// FASTA records of data[b0, b1) (ids as offsets into `data`).
+int parse_fasta_range(const char* data, int64_t b0, int64_t b1, std::vector<Rec>& recs, std::vector<uint8_t>& seq) {
+    Lines L{data + b0, data + b1};
+    seq.reserve((size_t)(b1 - b0));
     const char *b, *e;
     bool in_rec = false;
     while (L.next(b, e)) {
@@ -116,6 +132,46 @@ int parse_fasta(const char* data, int64_t n, std::vector<Rec>& recs, std::vector
         }
     }
     if (in_rec) recs.back().seq_len = (int64_t)seq.size() - recs.back().seq_begin;
+    return PW_OK;
+}
+
+// A whole FASTA input, in pieces on host threads: a piece starts at a line
+// that begins with '>' (every such line starts a record, so the pieces parse
+// independently); text before the first record is skipped as in one piece.
+int parse_fasta(const char* data, int64_t n, std::vector<Rec>& recs, std::vector<std::vector<uint8_t>>& bufs) {
+    const int64_t hw = std::max<int64_t>(1, (int64_t)std::thread::hardware_concurrency());
+    const int64_t pieces = std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(hw, 32), n >> 22));
+    std::vector<int64_t> cut{0};
+    for (int64_t k = 1; k < pieces; ++k) {
+        int64_t c = std::max(n * k / pieces, cut.back());
+        // the next "\n>" at or after c: the '>' line starts the piece
+        while (c < n) {
+            const char* nl = (const char*)memchr(data + c, '\n', (size_t)(n - c));
+            if (!nl) {
+                c = n;
+                break;
+            }
+            c = nl - data + 1;
+            if (c < n && data[c] == '>') break;
+        }
+        cut.push_back(std::min(c, n));
+    }
+    cut.push_back(n);
+    const int np = (int)cut.size() - 1;
+    std::vector<std::vector<Rec>> pr((size_t)np);
+    bufs.assign((size_t)np, {});
+    parallel_for(np, [&](int64_t k0, int64_t k1) {
+        for (int64_t k = k0; k < k1; ++k) parse_fasta_range(data, cut[k], cut[k + 1], pr[k], bufs[k]);
+    }, 1);
+    size_t total = 0;
+    for (auto& v : pr) total += v.size();
+    recs.clear();
+    recs.reserve(total);
+    for (int k = 0; k < np; ++k)
+        for (Rec r : pr[k]) {
+            r.s = bufs[k].data() + r.seq_begin;
+            recs.push_back(r);
+        }
     return PW_OK;
 }
 
@@ -194,14 +250,17 @@ int build(const char* data, int64_t n, int format, int64_t start, int64_t end, i
     if (transform < PW_RECORDS_AS_READ || transform > PW_RECORDS_APPEND_REVERSED)
         return report(err, err_bytes, PW_ERR_ARG, "unknown record transform %d", transform);
     std::vector<Rec> recs;
-    std::vector<uint8_t> seq;
+    std::vector<std::vector<uint8_t>> bufs;
     int rc;
-    if (format == PW_FORMAT_FASTA)
-        rc = parse_fasta(data, n, recs, seq);
-    else if (format == PW_FORMAT_FASTQ)
-        rc = parse_fastq(data, n, recs, seq, err, err_bytes);
-    else
+    if (format == PW_FORMAT_FASTA) {
+        rc = parse_fasta(data, n, recs, bufs);
+    } else if (format == PW_FORMAT_FASTQ) {
+        bufs.resize(1);
+        rc = parse_fastq(data, n, recs, bufs[0], err, err_bytes);
+        for (Rec& r : recs) r.s = bufs[0].data() + r.seq_begin;
+    } else {
         return report(err, err_bytes, PW_ERR_ARG, "unknown record format %d", format);
+    }
     if (rc != PW_OK) return rc;
     // islice(records, start, end)
     const int64_t total = (int64_t)recs.size();
@@ -222,7 +281,7 @@ int build(const char* data, int64_t n, int format, int64_t start, int64_t end, i
     const int64_t nk = (int64_t)keep.size();
     const int64_t nout = (transform == PW_RECORDS_APPEND_RC || transform == PW_RECORDS_APPEND_REVERSED) ? 2 * nk : nk;
     std::vector<int64_t> src(nout), lens(nout);
-    std::vector<int> kind(nout);  // 0 as read, 1 reverse complement, 2 reversed
+    std::vector<uint8_t> kind(nout);
     for (int64_t i = 0; i < nk; ++i) {
         if (transform == PW_RECORDS_RC_ONLY) {
             src[i] = keep[i];
@@ -236,46 +295,48 @@ int build(const char* data, int64_t n, int format, int64_t start, int64_t end, i
             }
         }
     }
-    for (int64_t i = 0; i < nout; ++i) lens[i] = recs[src[i]].seq_len;
-    std::vector<int64_t> order(nout);
-    std::iota(order.begin(), order.end(), 0);
-    if (sort_desc) std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return lens[a] > lens[b]; });
-    int64_t res_total = 0, id_total = 0;
+    int64_t max_len = 0;
     for (int64_t i = 0; i < nout; ++i) {
-        res_total += lens[i];
-        id_total += recs[src[i]].id_len + (kind[i] ? 3 : 0);
+        lens[i] = recs[src[i]].seq_len;
+        max_len = std::max(max_len, lens[i]);
     }
-    R->res.resize((size_t)res_total);
+    // a stable sort by length, longest first: ascending (max_len - length)
+    std::vector<uint32_t> order;
+    if (sort_desc) {
+        std::vector<uint64_t> key((size_t)nout);
+        for (int64_t i = 0; i < nout; ++i) key[i] = (uint64_t)(max_len - lens[i]);
+        order = radix_order(std::move(key));
+    } else {
+        order.resize((size_t)nout);
+        std::iota(order.begin(), order.end(), 0u);
+    }
+    R->src.resize((size_t)nout);
+    R->kind.resize((size_t)nout);
     R->off.resize((size_t)nout + 1);
-    R->ids.resize((size_t)id_total);
     R->id_off.resize((size_t)nout + 1);
     int64_t p = 0, q = 0;
     for (int64_t j = 0; j < nout; ++j) {
         const int64_t i = order[j];
-        const Rec& r = recs[src[i]];
+        R->src[j] = src[i];
+        R->kind[j] = kind[i];
         R->off[j] = p;
-        const uint8_t* s = seq.data() + r.seq_begin;
-        uint8_t* d = R->res.data() + p;
-        // SWSeqRecord upper-cases; the complement of an upper-case residue is upper case
-        auto upper = [](uint8_t v) { return (v >= 'a' && v <= 'z') ? (uint8_t)(v - 32) : v; };
-        if (kind[i] == 0) {
-            for (int64_t k = 0; k < r.seq_len; ++k) d[k] = upper(s[k]);
-        } else if (kind[i] == 1) {
-            for (int64_t k = 0; k < r.seq_len; ++k) d[k] = upper(complement(s[r.seq_len - 1 - k]));
-        } else {
-            for (int64_t k = 0; k < r.seq_len; ++k) d[k] = upper(s[r.seq_len - 1 - k]);
-        }
-        p += r.seq_len;
         R->id_off[j] = q;
-        memcpy(R->ids.data() + q, data + r.id_begin, (size_t)r.id_len);
-        q += r.id_len;
-        if (kind[i]) {
-            memcpy(R->ids.data() + q, "_RC", 3);
-            q += 3;
-        }
+        p += lens[i];
+        q += recs[src[i]].id_len + (kind[i] ? 3 : 0);
     }
     R->off[nout] = p;
     R->id_off[nout] = q;
+    R->ids.resize((size_t)q);
+    parallel_for(nout, [&](int64_t j0, int64_t j1) {
+        for (int64_t j = j0; j < j1; ++j) {
+            const Rec& r = recs[R->src[j]];
+            char* di = R->ids.data() + R->id_off[j];
+            memcpy(di, data + r.id_begin, (size_t)r.id_len);
+            if (R->kind[j]) memcpy(di + r.id_len, "_RC", 3);
+        }
+    }, 1 << 15);
+    R->recs.swap(recs);
+    R->bufs.swap(bufs);
     *out = R;
     return PW_OK;
 }
@@ -310,7 +371,7 @@ extern "C" int pw_records_sizes(const pw_records* r, int64_t* n_records, int64_t
                                 int64_t* dropped) {
     if (!r) return PW_ERR_ARG;
     if (n_records) *n_records = (int64_t)r->off.size() - 1;
-    if (residue_bytes) *residue_bytes = (int64_t)r->res.size();
+    if (residue_bytes) *residue_bytes = r->off.back();
     if (id_bytes) *id_bytes = (int64_t)r->ids.size();
     if (dropped) *dropped = r->dropped;
     return PW_OK;
@@ -319,7 +380,25 @@ extern "C" int pw_records_sizes(const pw_records* r, int64_t* n_records, int64_t
 extern "C" int pw_records_copy(const pw_records* r, uint8_t* residues, int64_t* offsets, char* ids,
                                int64_t* id_offsets) {
     if (!r) return PW_ERR_ARG;
-    if (residues && !r->res.empty()) memcpy(residues, r->res.data(), r->res.size());
+    const int64_t n = (int64_t)r->src.size();
+    if (residues)
+        parallel_for(n, [&](int64_t j0, int64_t j1) {
+            // SWSeqRecord upper-cases; the complement of an upper-case residue is upper case
+            auto upper = [](uint8_t v) { return (v >= 'a' && v <= 'z') ? (uint8_t)(v - 32) : v; };
+            for (int64_t j = j0; j < j1; ++j) {
+                const Rec& rc = r->recs[r->src[j]];
+                const uint8_t* s = rc.s;
+                const int64_t L = rc.seq_len;
+                uint8_t* d = residues + r->off[j];
+                if (r->kind[j] == 0) {
+                    for (int64_t k = 0; k < L; ++k) d[k] = upper(s[k]);
+                } else if (r->kind[j] == 1) {
+                    for (int64_t k = 0; k < L; ++k) d[k] = upper(complement(s[L - 1 - k]));
+                } else {
+                    for (int64_t k = 0; k < L; ++k) d[k] = upper(s[L - 1 - k]);
+                }
+            }
+        }, 1 << 14);
     if (offsets) memcpy(offsets, r->off.data(), r->off.size() * sizeof(int64_t));
     if (ids && !r->ids.empty()) memcpy(ids, r->ids.data(), r->ids.size());
     if (id_offsets) memcpy(id_offsets, r->id_off.data(), r->id_off.size() * sizeof(int64_t));
@@ -327,3 +406,44 @@ extern "C" int pw_records_copy(const pw_records* r, uint8_t* residues, int64_t* 
 }
 
 extern "C" void pw_records_free(pw_records* r) { delete r; }
+
+// Dense ranks of n byte strings blob[off[i], off[i + 1]) in byte order, a
+// string before every longer string it prefixes: the order of Python's str
+// comparison on ASCII text (code points).  Equal strings share a rank.
+// Sorted in pieces on host threads, then merged pairwise.
+extern "C" int pw_id_ranks(const char* blob, const int64_t* off, int64_t n, int32_t* ranks) {
+    if (n < 0 || (n > 0 && (!off || !ranks))) return PW_ERR_ARG;
+    if (n == 0) return PW_OK;
+    if (n > (int64_t)INT32_MAX) return PW_ERR_ARG;
+    auto less = [&](uint32_t a, uint32_t b) {
+        const int64_t la = off[a + 1] - off[a], lb = off[b + 1] - off[b];
+        const int c = memcmp(blob + off[a], blob + off[b], (size_t)std::min(la, lb));
+        return c < 0 || (c == 0 && la < lb);
+    };
+    std::vector<uint32_t> idx((size_t)n), tmp((size_t)n);
+    std::iota(idx.begin(), idx.end(), 0u);
+    const int64_t hw = std::max<int64_t>(1, (int64_t)std::thread::hardware_concurrency());
+    const int64_t pieces = std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(hw, 32), n >> 14));
+    std::vector<int64_t> cut((size_t)pieces + 1);
+    for (int64_t k = 0; k <= pieces; ++k) cut[k] = n * k / pieces;
+    parallel_for(pieces, [&](int64_t k0, int64_t k1) {
+        for (int64_t k = k0; k < k1; ++k) std::sort(idx.begin() + cut[k], idx.begin() + cut[k + 1], less);
+    }, 1);
+    for (int64_t width = 1; width < pieces; width *= 2) {
+        const int64_t merges = (pieces + 2 * width - 1) / (2 * width);
+        parallel_for(merges, [&](int64_t m0, int64_t m1) {
+            for (int64_t m = m0; m < m1; ++m) {
+                const int64_t a = cut[m * 2 * width], b = cut[std::min(pieces, m * 2 * width + width)],
+                              c = cut[std::min(pieces, m * 2 * width + 2 * width)];
+                std::merge(idx.begin() + a, idx.begin() + b, idx.begin() + b, idx.begin() + c, tmp.begin() + a, less);
+            }
+        }, 1);
+        idx.swap(tmp);
+    }
+    int32_t r = 0;
+    for (int64_t k = 0; k < n; ++k) {
+        if (k > 0 && less(idx[k - 1], idx[k])) ++r;
+        ranks[idx[k]] = r;
+    }
+    return PW_OK;
+}

@@ -86,6 +86,10 @@ def _record_arrays(sequences, targets, settings, strip_target_rc):
 
     def arrays(records, strip_rc):
         if _is_packed(records):  # packed records (pypaswas_b200.readers): no per-record objects
+            if not strip_rc and _ascii(records.id_blob):
+                # ASCII ids: byte order is Python's string order; ranked natively
+                return (_native_ranks(records.id_blob, records.id_offsets), records.lengths.astype(np.int64),
+                        np.zeros(len(records), dtype=np.int64), records.id_blob, records.id_offsets)
             ids = records.ids
             b = blob([_strip_rc(i) for i in ids]) if strip_rc else (records.id_blob, records.id_offsets)
             return (ranks(ids), records.lengths.astype(np.int64), np.zeros(len(ids), dtype=np.int64)) + tuple(b)
@@ -101,8 +105,30 @@ def _record_arrays(sequences, targets, settings, strip_target_rc):
     return q, t, thr, blob
 
 
-# first output buffer at most this large; a longer text takes the exact-size retry
-_ESTIMATE_CAP = 256 << 20
+def _ascii(blob):
+    return len(blob) == 0 or int(blob.max()) < 128
+
+
+def _native_ranks(blob, offsets):
+    """Dense ranks of the ids blob[offsets[i]:offsets[i + 1]] in byte order
+    (pw_id_ranks): Python's string order for ASCII ids."""
+    import ctypes
+    import numpy as np
+    from . import _native
+    n = len(offsets) - 1
+    out = np.zeros(max(n, 0), dtype=np.int32)
+    blob = np.ascontiguousarray(blob, dtype=np.uint8)
+    offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+    vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    rc = _native.load_library().pw_id_ranks(vp(blob) if len(blob) else None, vp(offsets), n, vp(out))
+    if rc != _native.PW_OK:
+        raise CudaException("pw_id_ranks failed (%d)" % rc)
+    return out
+
+
+# first output buffer at most this large (np.empty commits no pages until they
+# are written); a longer text takes the exact-size retry
+_ESTIMATE_CAP = 8 << 30
 
 
 def _per_hit_estimate(hits, q_id_off, t_id_off, body):
@@ -137,7 +163,7 @@ def _call_twice(fn, head, tail, estimate):
         raise CudaException("Invalid hit location in the engine's records")
     if rc != _native.PW_OK:
         raise CudaException("native formatter failed (%d)" % rc)
-    return out[:n.value].tobytes().decode("utf-8")
+    return str(memoryview(out[:n.value]), "utf-8")
 
 
 def txt_records(hits, strbuf, sequences, targets, settings, lib=None):

@@ -262,9 +262,10 @@ def query_stream(seed=6, n=1000, median=300.0, sigma=0.5, max_len=5000, min_len=
             for i in range(n)]
 
 
-def config3(seed=3, **kw):
-    q, t, pairs = long_dna_pairs(seed, **kw)
-    return Workload("C3 long DNA, 64 pairs of 10-50 kb (+RC), linear gap", q, t, Settings(**C3_SETTINGS), pairs)
+def config3(seed=3, n_pairs=64, **kw):
+    q, t, pairs = long_dna_pairs(seed, n_pairs=n_pairs, **kw)
+    return Workload("C3 long DNA, %d pairs of 10-50 kb (+RC), linear gap" % n_pairs, q, t, Settings(**C3_SETTINGS),
+                    pairs)
 
 
 def config4(seed=4, n_reads=10_000_000):
