@@ -114,3 +114,43 @@ def test_native_reader_interface_matches_the_packed_chain(tmp_path):
     got = [(x.id, str(x.seq)) for x in r.get_records()]
     want = readers.read_records(str(p), "fasta", 5, 45, 30, _native.PW_RECORDS_APPEND_RC, True)
     assert got == _as_list(want)
+
+
+def test_native_id_ranks_follow_python_string_order():
+    """pw_id_ranks: dense ranks in Python's str order (ASCII ids: prefixes
+    first, equal ids share a rank), across the threaded sort-and-merge."""
+    from pypaswas_b200.formatters import _native_ranks
+    rng = np.random.default_rng(5)
+    alphabet = np.array(list("ab_Z09.-"))
+    for n in (0, 1, 7, 40000):
+        ids = ["".join(rng.choice(alphabet, size=int(rng.integers(0, 6)))) for _ in range(n)]
+        blob = np.frombuffer("".join(ids).encode() or b"\0", dtype=np.uint8)[:sum(map(len, ids))]
+        off = np.zeros(n + 1, dtype=np.int64)
+        np.cumsum([len(i) for i in ids], out=off[1:])
+        got = _native_ranks(blob, off)
+        order = {v: k for k, v in enumerate(sorted(set(ids)))}
+        assert got.tolist() == [order[v] for v in ids]
+
+
+def test_parallel_fasta_pieces_equal_one_piece():
+    """A FASTA input large enough to be parsed in pieces on host threads
+    gives the records a sequential parse gives (pieces start at '>' lines;
+    junk before the first record, blank and wrapped lines, CRLF)."""
+    rng = np.random.default_rng(9)
+    parts = [b"junk line\n\n"]
+    want = []
+    letters = np.array(list("ACGTacgtN"))
+    for i in range(60000):
+        seq = "".join(letters[rng.integers(0, 9, size=int(rng.integers(1, 400)))])
+        wrapped = "\n".join(seq[k:k + 60] for k in range(0, len(seq), 60))
+        eol = "\r\n" if i % 7 == 0 else "\n"
+        parts.append((">r%d desc %d%s%s%s" % (i, i, eol, wrapped.replace("\n", eol), eol)).encode())
+        if i % 11 == 0:
+            parts.append(b"\n")
+        want.append(("r%d" % i, seq.upper()))
+    data = b"".join(parts)
+    assert len(data) > (1 << 23)  # several pieces
+    rs = readers.read_records(data, "fasta", 0, None, 0, _native.PW_RECORDS_AS_READ, False)
+    assert len(rs) == len(want)
+    assert rs.ids == [w[0] for w in want]
+    assert [rs.seq(k) for k in range(len(rs))] == [w[1] for w in want]
