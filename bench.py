@@ -302,6 +302,23 @@ def roofline(e, w, score, infos, steps):
         lanes16 = sixteen
     peak32, peak16, _ = e.measure_int_peak()
     peak = peak16 if lanes16 else peak32
+    if dom.startswith("direction") and last.get("trace_store"):
+        # the H-storing direction sweep: the score recurrence plus a 2-byte
+        # store per cell; its roof is the HBM write of those bytes
+        ops = sum(i["traced_cells"] for i in infos) * OPS_PER_CELL[(mode, "score")]
+        per_cell = OPS_PER_CELL[(mode, "score")]
+        written = sum(i["traced_cells"] for i in infos) * 2
+        peaks = load_peaks()
+        hbm = peaks.get("hbm_gbs")
+        src = "measured (MEASURED_PEAKS.json hbm_gbs)" if hbm else "fallback 6,650 GB/s (no MEASURED_PEAKS.json)"
+        hbm = float(hbm or 6650.0)
+        gbs = written / (dom_ms * 1e-3) / 1e9
+        alu = ops / (dom_ms * 1e-3) / 1e12
+        return {"bound": "hbm", "kernel": dom + ", 16-bit H stored per cell", "achieved": gbs, "peak": hbm,
+                "unit": "GB/s", "frac": gbs / hbm, "peak_source": src, "bytes_per_cell": 2,
+                "alu": {"achieved": alu, "peak": peak / 1e12, "unit": "Tops/s", "frac": alu / (peak / 1e12),
+                        "ops_per_cell": per_cell},
+                "launches": launches, "avg_launch_ms": dom_ms / max(1, launches)}
     achieved = ops / (dom_ms * 1e-3) / 1e12
     return {"bound": "int_alu", "kernel": dom, "achieved": achieved, "peak": peak / 1e12, "unit": "Tops/s",
             "frac": achieved / (peak / 1e12),
@@ -663,6 +680,7 @@ def run_config(cfg, args, device, world, flush, sampler, headline):
                       "cand_overflow_pairs": last["cand_overflow_pairs"],
                       "starting_points": last["starting_points"], "hits": last["hits"],
                       "memory_waves": last["waves"],
+                      "trace_store": "16-bit H per cell" if last.get("trace_store") else "4-bit cell codes",
                       "score_lanes": "targets" if last["orientation"] else "queries",
                       "trace_lanes": "targets" if last["trace_orientation"] else "queries",
                       "minimum_score": w.settings.minimum_score,

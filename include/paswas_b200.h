@@ -94,6 +94,8 @@ typedef struct {
                                was kept) */
     int64_t h2d_bytes;      /* bytes this call copied host -> device (sequences, encodings, work lists) */
     int64_t d2h_bytes;      /* bytes this call copied device -> host (maxima, pair lists, starts, hits) */
+    int32_t trace_store;    /* direction sweeps stored 1: each cell's 16-bit H, 0: 4-bit cell codes */
+    int32_t pad0;
 } pw_run_info;
 
 #define PW_REUSE_QUERIES 1
@@ -224,6 +226,11 @@ int pw_set_wave_limit(pw_engine* e, int64_t bytes);
  *                       scores allow it (pairs that reach the 16-bit limit are
  *                       recomputed on 32-bit lanes either way) */
 #define PW_TUNE_LANES 7
+/*   PW_TUNE_TRACE_STORE direction sweeps of linear integer scoring: 0 the
+ *                       engine's choice (16-bit H per cell when every traced
+ *                       maximum is below 2^15, cell codes derived on read),
+ *                       1 always 4-bit cell codes */
+#define PW_TUNE_TRACE_STORE 8
 int pw_set_tuning(pw_engine* e, int key, int64_t value);
 
 /* Pair maxima (the last block of the maxima chain, default_main.cu:591),

@@ -269,7 +269,7 @@ struct pw_engine {
     int64_t prep_q[2] = {0, 0}, prep_t[2] = {0, 0};  // (sequence gen, scoring gen) last prepared
     int64_t wave_limit = 0;                          // cell-code bytes per memory wave (0: automatic)
     std::vector<int32_t> pair_q, pair_t;             // pw_set_pairs: explicit (query, target) pairs
-    int64_t tune[8] = {0, 0, 0, 0, 0, 0, 0, 0};      // pw_set_tuning values (0: automatic)
+    int64_t tune[16] = {};                           // pw_set_tuning values (0: automatic)
     // results
     HostBuf<float> h_pair_max;
     bool pm_stale = false;  // h_pair_max lags the device maxima (copied on pw_get_pair_max)
@@ -505,26 +505,36 @@ cudaError_t launch_sweep(pw_engine* e, KernelArgs A, int* counter) {
 
 template <typename T, int PH, bool TR>
 cudaError_t launch_class_o(pw_engine* e, int cls, bool affine, const KernelArgs& A, int* counter) {
-    if (affine) {
+    if constexpr (PH == 3) {  // H store: linear gap, int lanes only
         switch (cls) {
-            case kS16: return launch_sweep<T, 16, true, false, PH, TR>(e, A, counter);
-            case kS32: return launch_sweep<T, 32, true, false, PH, TR>(e, A, counter);
-            default: return launch_sweep<T, 32, true, true, PH, TR>(e, A, counter);
+            case kS16: return launch_sweep<int, 16, false, false, 3, TR>(e, A, counter);
+            case kS32: return launch_sweep<int, 32, false, false, 3, TR>(e, A, counter);
+            case kS48: return launch_sweep<int, 48, false, false, 3, TR>(e, A, counter);
+            case kS64: return launch_sweep<int, 64, false, false, 3, TR>(e, A, counter);
+            default: return launch_sweep<int, 32, false, true, 3, TR>(e, A, counter);
         }
-    }
-    switch (cls) {
-        case kS16: return launch_sweep<T, 16, false, false, PH, TR>(e, A, counter);
-        case kS32: return launch_sweep<T, 32, false, false, PH, TR>(e, A, counter);
-        case kS48: return launch_sweep<T, 48, false, false, PH, TR>(e, A, counter);
-        case kS64: return launch_sweep<T, 64, false, false, PH, TR>(e, A, counter);
-        default: return launch_sweep<T, 32, false, true, PH, TR>(e, A, counter);
+    } else {
+        if (affine) {
+            switch (cls) {
+                case kS16: return launch_sweep<T, 16, true, false, PH, TR>(e, A, counter);
+                case kS32: return launch_sweep<T, 32, true, false, PH, TR>(e, A, counter);
+                default: return launch_sweep<T, 32, true, true, PH, TR>(e, A, counter);
+            }
+        }
+        switch (cls) {
+            case kS16: return launch_sweep<T, 16, false, false, PH, TR>(e, A, counter);
+            case kS32: return launch_sweep<T, 32, false, false, PH, TR>(e, A, counter);
+            case kS48: return launch_sweep<T, 48, false, false, PH, TR>(e, A, counter);
+            case kS64: return launch_sweep<T, 64, false, false, PH, TR>(e, A, counter);
+            default: return launch_sweep<T, 32, false, true, PH, TR>(e, A, counter);
+        }
     }
 }
 
 // Phase 1 never needs the transposed form (maxima are orientation-free).
 template <typename T, int PH>
 cudaError_t launch_class(pw_engine* e, int cls, bool affine, const KernelArgs& A, int* counter, bool trans) {
-    if (PH == 2 && trans) return launch_class_o<T, PH, true>(e, cls, affine, A, counter);
+    if (PH >= 2 && trans) return launch_class_o<T, PH, true>(e, cls, affine, A, counter);
     return launch_class_o<T, PH, false>(e, cls, affine, A, counter);
 }
 
@@ -827,8 +837,11 @@ static int run_phase(pw_engine* e, KernelArgs A, const WorkItem* dev_items, cons
         cudaEventCreate(&a);
         cudaEventCreate(&b);
         cudaEventRecord(a, e->stream);
-        c = e->pr.int_path ? launch_class<int, PH>(e, cls, e->affine, A, e->counter.as<int>() + cls, trans)
-                           : launch_class<float, PH>(e, cls, e->affine, A, e->counter.as<int>() + cls, trans);
+        if constexpr (PH == 3)
+            c = launch_class<int, 3>(e, cls, false, A, e->counter.as<int>() + cls, trans);
+        else
+            c = e->pr.int_path ? launch_class<int, PH>(e, cls, e->affine, A, e->counter.as<int>() + cls, trans)
+                               : launch_class<float, PH>(e, cls, e->affine, A, e->counter.as<int>() + cls, trans);
         cudaEventRecord(b, e->stream);
         evs.push_back({a, b});
         if (c != cudaSuccess) return cuda_fail(e, c, "sweep kernel launch");
@@ -1420,15 +1433,18 @@ static cudaError_t finish_hits(pw_engine* e, int64_t n, int64_t* str_bytes) {
 }
 
 // Launches band_kernel over `pairs` (one warp per band, the bands of a pair
-// chained across warps, pw_band.cuh).  DIRS: the direction sweep of traced
-// pairs; otherwise pair maxima into band_max (indexed by BandPair.slot).
-template <bool DIRS>
+// chained across warps, pw_band.cuh).  DIRS 1: the direction sweep of traced
+// pairs (cell codes), 2: the same storing H (linear gap); 0: pair maxima into
+// band_max (indexed by BandPair.slot).
+template <int DIRS>
 static int run_band_phase(pw_engine* e, KernelArgs A, std::vector<BandPair>& pairs, double* kernel_ms,
                           int* n_launch) {
     if (pairs.empty()) return PW_OK;
     const int prof_bytes = (int)align_up((int64_t)kWarp * (A.P.alpha + 1) * kWarpRows, 16);
     const int smem = 4 * prof_bytes;
-    auto kern = e->affine ? band_kernel<true, DIRS> : band_kernel<false, DIRS>;
+    auto kern = band_kernel<false, DIRS>;
+    if constexpr (DIRS != 2)
+        if (e->affine) kern = band_kernel<true, DIRS>;
     cudaError_t c;
     if (smem > 48 * 1024 &&
         (c = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
@@ -1654,7 +1670,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         if ((c = e->band_out.reserve(e->stream, np * sizeof(float))) != cudaSuccess)
             return cuda_fail(e, c, "alloc band maxima");
         cudaEventRecord(e->ev[0], e->stream);
-        rc = run_band_phase<false>(e, A, bp, &inf.score_kernel_ms, &inf.score_launches);
+        rc = run_band_phase<0>(e, A, bp, &inf.score_kernel_ms, &inf.score_launches);
         if (rc != PW_OK) return rc;
         cudaEventRecord(e->ev[1], e->stream);
         std::vector<float> bm;
@@ -1684,7 +1700,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
             bp[0].q = q;
             bp[0].t = t;
             bp[0].nbands = tlen[t] > 0 ? (tlen[t] + kBandRows - 1) / kBandRows : 1;
-            rc = run_band_phase<false>(e, A, bp, &inf.score_kernel_ms, &inf.score_launches);
+            rc = run_band_phase<0>(e, A, bp, &inf.score_kernel_ms, &inf.score_launches);
             if (rc != PW_OK) return rc;
             float m = 0.0f;
             if ((c = copy_d2h(e, &m, e->band_out.p, sizeof(float))) != cudaSuccess ||
@@ -1802,12 +1818,12 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     std::vector<int64_t> pt_off((size_t)nt + 1, 0);
     HostBuf<int32_t>& pt_q = e->h_ptq;
     pt_q.clear();
-    int64_t min_pass = 0, n_pass = 0;
+    int64_t min_pass = 0, n_pass = 0, max_pass = 0;
     {
         // the test runs on the device over the resident maxima (prune_kernel);
         // the passing pairs come back as a target-major list of pair indices
         const int64_t npairs = (int64_t)nq * nt;
-        unsigned long long cnt[2] = {0, 0};
+        unsigned long long cnt[4] = {0, 0, 0, 0};
         if ((c = e->prune_flags.reserve(e->stream, (size_t)std::max<int64_t>(npairs, 16))) != cudaSuccess ||
             (c = e->prune_cnt.reserve(e->stream, 4 * sizeof(unsigned long long))) != cudaSuccess ||
             (c = cudaMemsetAsync(e->prune_cnt.p, 0, 4 * sizeof(unsigned long long), e->stream)) != cudaSuccess)
@@ -1824,6 +1840,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
             return cuda_fail(e, c, "prune pairs");
         min_pass = (int64_t)cnt[0];
         n_pass = (int64_t)cnt[1];
+        max_pass = (int64_t)cnt[3];
         ht.mark("prune kernel + counts");
         if (n_pass > 0) {
             int64_t* d_count = e->prune_cnt.as<int64_t>() + 2;
@@ -1858,6 +1875,12 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         }
         ht.mark("passing pairs to per-target lists");
     }
+    // Linear integer scoring whose traced maxima all stay below 2^15: the
+    // direction sweeps store each cell's 16-bit H (four times the bytes of a
+    // 4-bit code, a few instructions a cell instead of the classification);
+    // collect and walk derive the codes of the cells they visit
+    const bool hstore = pr.int_path && !e->affine && max_pass < 32767 && e->tune[PW_TUNE_TRACE_STORE] != 1;
+    inf.trace_store = hstore ? 1 : 0;
     auto span_n = [&](int t) -> int64_t { return pt_off[t + 1] - pt_off[t]; };
     // Traced pairs with targets longer than one register strip go to the
     // one-warp-per-pair sweep (pw_band.cuh); the others are grouped 32 to
@@ -1966,7 +1989,8 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
                 w.S = S;
                 items2[it] = w;
                 cls2[it] = k;
-                bytes2[it] = strips * S * align_up(std::max(w.xmax, 1), 4) * kWarp / 2;  // 4-bit codes
+                const int64_t cells = strips * S * align_up(std::max(w.xmax, 1), 4) * kWarp;
+                bytes2[it] = hstore ? cells * 2 : cells / 2;  // 16-bit H or 4-bit codes
             }
         }
     }, std::max<int64_t>(1, (int64_t)n_strip * ((int64_t)1 << 15) / std::max<int64_t>(s_pairs[n_strip], 1)));
@@ -1988,7 +2012,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         w.S = kWarpRows;
         items2.push_back(w);
         cls2.push_back(kNumClasses);  // marks a warp item
-        bytes2.push_back(align_up(warp_code_bytes(qlen[wp.first], tlen[wp.second]), 16));
+        bytes2.push_back(align_up(warp_code_bytes(qlen[wp.first], tlen[wp.second], hstore), 16));
         qmax_warp = std::max(qmax_warp, qlen[wp.first]);
     }
     ht.mark("phase-2 work items");
@@ -2048,7 +2072,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         size_t i0 = 0;
         int64_t acc = 0;
         for (size_t i = 0; i < items2.size(); ++i) {
-            const int64_t b = bytes2[i] + bytes2[i] / 4 + items2[i].lanes * pair_bytes;  // codes + mark plane
+            const int64_t b = bytes2[i] + bytes2[i] / (hstore ? 16 : 4) + items2[i].lanes * pair_bytes;  // + marks
             if (acc > 0 && (acc + b > budget || plain)) {
                 waves.push_back({i0, i});
                 i0 = i;
@@ -2097,8 +2121,9 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         int xm = 4;
         for (int k = begin[kS32Multi]; k < begin[kS32Multi + 1]; ++k) xm = std::max(xm, (int)align_up(wi[k].xmax, 4));
         if ((c = e->codes.reserve(e->stream, (size_t)dir_off)) != cudaSuccess) return cuda_fail(e, c, "alloc cell codes");
-        // one mark bit per cell (two cells per code byte), zeroed for the wave
-        const size_t mark_bytes = (size_t)(dir_off / 4 + 16);
+        // one mark bit per cell (two cells per code byte, half a cell per H
+        // byte), zeroed for the wave
+        const size_t mark_bytes = (size_t)(dir_off / (hstore ? 16 : 4) + 16);
         if ((c = e->marks.reserve(e->stream, mark_bytes)) != cudaSuccess ||
             (c = cudaMemsetAsync(e->marks.p, 0, mark_bytes, e->stream)) != cudaSuccess)
             return cuda_fail(e, c, "alloc cell marks");
@@ -2138,13 +2163,16 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         if ((c = cudaMemsetAsync(A.n_cand, 0, n_pairs * sizeof(int32_t), e->stream)) != cudaSuccess)
             return cuda_fail(e, c, "reset candidate counts");
         if (!wi.empty()) {
-            rc = run_phase<2>(e, A, e->items.as<WorkItem>(), begin, xm, &inf.trace_kernel_ms, &inf.trace_launches,
-                              trans2);
+            rc = hstore ? run_phase<3>(e, A, e->items.as<WorkItem>(), begin, xm, &inf.trace_kernel_ms,
+                                       &inf.trace_launches, trans2)
+                        : run_phase<2>(e, A, e->items.as<WorkItem>(), begin, xm, &inf.trace_kernel_ms,
+                                       &inf.trace_launches, trans2);
             if (rc != PW_OK) return rc;
         }
         {
             std::vector<BandPair> bp = band_pairs_of(e, ww);
-            rc = run_band_phase<true>(e, Aw, bp, &inf.trace_kernel_ms, &inf.trace_launches);
+            rc = hstore ? run_band_phase<2>(e, Aw, bp, &inf.trace_kernel_ms, &inf.trace_launches)
+                        : run_band_phase<1>(e, Aw, bp, &inf.trace_kernel_ms, &inf.trace_launches);
             if (rc != PW_OK) return rc;
         }
         // candidate overflow: pairs with more candidates than their slot get an
@@ -2217,13 +2245,16 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
                 int rb[kNumClasses + 1];
                 order_by_class(ri, rcl, rb);
                 if ((c = upload(e, e->items_alt, ri)) != cudaSuccess) return cuda_fail(e, c, "upload items");
-                rc = run_phase<2>(e, A, e->items_alt.as<WorkItem>(), rb, xm, &inf.trace_kernel_ms,
-                                  &inf.trace_launches, trans2);
+                rc = hstore ? run_phase<3>(e, A, e->items_alt.as<WorkItem>(), rb, xm, &inf.trace_kernel_ms,
+                                           &inf.trace_launches, trans2)
+                            : run_phase<2>(e, A, e->items_alt.as<WorkItem>(), rb, xm, &inf.trace_kernel_ms,
+                                           &inf.trace_launches, trans2);
                 if (rc != PW_OK) return rc;
             }
             if (!rw.empty()) {
                 std::vector<BandPair> bp = band_pairs_of(e, rw);
-                rc = run_band_phase<true>(e, Aw, bp, &inf.trace_kernel_ms, &inf.trace_launches);
+                rc = hstore ? run_band_phase<2>(e, Aw, bp, &inf.trace_kernel_ms, &inf.trace_launches)
+                            : run_band_phase<1>(e, Aw, bp, &inf.trace_kernel_ms, &inf.trace_launches);
                 if (rc != PW_OK) return rc;
             }
         }
@@ -2237,6 +2268,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         TA.n_pairs = (int)n_pairs;
         TA.items = e->items.as<WorkItem>();
         TA.codes = A.codes;
+        TA.hstore = hstore ? 1 : 0;
         TA.marks = e->marks.as<uint8_t>();
         TA.cands = A.cands;
         TA.cand_base = A.cand_base;
@@ -2386,7 +2418,8 @@ extern "C" int pw_set_pairs(pw_engine* e, const int32_t* query_idx, const int32_
 
 extern "C" int pw_set_tuning(pw_engine* e, int key, int64_t value) {
     if (!e) return PW_ERR_ARG;
-    if (key < 0 || key >= 8 || value < 0) return fail(e, PW_ERR_ARG, "unknown tuning key or negative value");
+    if (key < 0 || key > PW_TUNE_TRACE_STORE || value < 0)
+        return fail(e, PW_ERR_ARG, "unknown tuning key or negative value");
     e->tune[key] = value;
     return PW_OK;
 }

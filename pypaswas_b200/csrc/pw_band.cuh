@@ -19,12 +19,15 @@
 // above it: band-major when there are many pairs, otherwise planned like the
 // chained strips (pw_plan.h) so that the bands of a few long pairs pipeline.
 //
-// DIRS = false: pair maxima only (the score sweep of long pairs).
-// DIRS = true: the direction sweep of traced pairs: per cell the code byte of
-// the reference's classification (direction, stop flag, candidate flag) and
-// the pair's candidate list, exactly as the strip sweep computes them; 4-bit
-// cell codes are stored [band][step][lane][8 rows] (warp_layout_offset), one
-// 4-byte word per lane and step: a warp stores 128 contiguous bytes.
+// DIRS = 0: pair maxima only (the score sweep of long pairs).
+// DIRS = 1: the direction sweep of traced pairs: per cell the code of the
+// reference's classification (direction, stop flag, candidate flag) and the
+// pair's candidate list, exactly as the strip sweep computes them; 4-bit cell
+// codes are stored [band][step][lane][8 rows] (warp_layout_offset), one 4-byte
+// word per lane and step: a warp stores 128 contiguous bytes.
+// DIRS = 2 (linear gap): the same sweep storing each cell's 16-bit H at the
+// same positions (16 bytes per lane and step, 512 contiguous bytes a warp) and
+// the candidate list; codes are derived from H on read (PairView::code).
 #pragma once
 #include "pw_kernels.cuh"
 #include "pw_score16.cuh"
@@ -38,10 +41,11 @@ constexpr int kBandLead = 128;                 // planning lead between bands (s
 static_assert(kBandRows == 256 && kWarpRows == 8, "warp_layout_offset (pw_kernels.cuh) assumes 8 x 32 rows");
 
 // Bytes of a pair's 4-bit cell codes in the band layout (8 rows of a lane per
-// 4-byte word).
-__host__ __device__ __forceinline__ int64_t warp_code_bytes(int lq, int lt) {
+// 4-byte word), or of its 16-bit H values (hstore: four times as many).
+__host__ __device__ __forceinline__ int64_t warp_code_bytes(int lq, int lt, bool hstore = false) {
     const int64_t bands = lt > 0 ? (lt + kBandRows - 1) / kBandRows : 1;
-    return bands * ((int64_t)lq + kWarp - 1) * kWarp * kWarpRows / 2;
+    const int64_t cells = bands * ((int64_t)lq + kWarp - 1) * kWarp * kWarpRows;
+    return hstore ? cells * 2 : cells / 2;
 }
 
 struct BandPair {
@@ -66,8 +70,9 @@ struct BandArgs {
     unsigned long long wait_ns;  // bound of one wait for the band above
 };
 
-template <bool AFFINE, bool DIRS>
+template <bool AFFINE, int DIRS>
 __global__ void __launch_bounds__(128) band_kernel(KernelArgs A, BandArgs B) {
+    static_assert(DIRS != 2 || !AFFINE, "H store: linear gap only");
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -93,7 +98,7 @@ __global__ void __launch_bounds__(128) band_kernel(KernelArgs A, BandArgs B) {
         int cap = 0;
         int* ncand = nullptr;
         uint8_t* codes = nullptr;
-        if constexpr (DIRS) {
+        if constexpr (DIRS != 0) {
             // threshold of the pair (default_main.cu:609, SmithWatermanCuda.py:269-275)
             const float maxf = A.pair_max[(int64_t)q * A.pm_lane + (int64_t)t * A.pm_strip];
             const int mn = lq < lt ? lq : lt;
@@ -213,7 +218,19 @@ __global__ void __launch_bounds__(128) band_kernel(KernelArgs A, BandArgs B) {
                         const int left = Hl[r];
                         int h = addmax(left, gap, diag + sc);
                         h = addmax_relu(up, gap, h);
-                        if constexpr (DIRS) {
+                        if constexpr (DIRS == 2) {
+                            if (h >= thr && r < rows_left && h > 0 && h != left + gap && h != up + gap) {
+                                const int k = atomicAdd(ncand, 1);
+                                if (k < cap) {
+                                    Cand cc;
+                                    cc.x = x;
+                                    cc.y = ymine + r;
+                                    cc.score_i = h;
+                                    cc.score_f = (float)h;
+                                    cand[k] = cc;
+                                }
+                            }
+                        } else if constexpr (DIRS == 1) {
                             const int ls = left + gap, us = up + gap;
                             uint32_t code = h == ls ? kLeft : (h == us ? kUp : kUL);
                             code = h > 0 ? code : kNo;
@@ -243,6 +260,14 @@ __global__ void __launch_bounds__(128) band_kernel(KernelArgs A, BandArgs B) {
                         up = h;
                     }
                     bt_h = up;
+                    if constexpr (DIRS == 2) {
+                        uint4 hv;
+                        hv.x = __byte_perm(Hl[0], Hl[1], 0x5410);
+                        hv.y = __byte_perm(Hl[2], Hl[3], 0x5410);
+                        hv.z = __byte_perm(Hl[4], Hl[5], 0x5410);
+                        hv.w = __byte_perm(Hl[6], Hl[7], 0x5410);
+                        *(uint4*)(codes + ((band * nsteps + s) * kWarp + lane) * kWarpRows * 2) = hv;
+                    }
                 } else {
                     int mup = up_m, iup = up_i, bdiag = dg_b, mdiag = dg_m;
 #pragma unroll
@@ -252,7 +277,7 @@ __global__ void __launch_bounds__(128) band_kernel(KernelArgs A, BandArgs B) {
                         const int i = addmax(iup, ext, mup + ge);
                         const int jj = addmax(Jl[r], ext, Ml[r] + ge);
                         const int b = max3(m, i, jj);
-                        if constexpr (DIRS) {
+                        if constexpr (DIRS != 0) {
                             uint32_t code = b == m ? kUL : (b == i ? kUp : kLeft);
                             code = b > 0 ? code : kNo;
                             const bool main_src = code == kUL;
@@ -287,7 +312,7 @@ __global__ void __launch_bounds__(128) band_kernel(KernelArgs A, BandArgs B) {
                     bt_i = iup;
                     bt_b = Bl[kWarpRows - 1];
                 }
-                if constexpr (DIRS)
+                if constexpr (DIRS == 1)
                     *(uint32_t*)(codes + ((band * nsteps + s) * kWarp + lane) * kWarpRows / 2) = w0;
                 if (lane == kWarp - 1 && store_bnd) __stcg(&ring_out[x], make_int4(AFFINE ? bt_m : bt_h, bt_i, bt_b, 0));
             } else {
@@ -304,18 +329,18 @@ __global__ void __launch_bounds__(128) band_kernel(KernelArgs A, BandArgs B) {
         if (!ok) break;
         if (store_bnd && lane == kWarp - 1) st_release_gpu(prog_out, lq);
         // pair maximum (score sweep) / candidate count (direction sweep)
-        if constexpr (!DIRS) mx = __reduce_max_sync(0xffffffffu, mx);
+        if constexpr (DIRS == 0) mx = __reduce_max_sync(0xffffffffu, mx);
         if (has_up) {
             // the band above has finished: its running maximum and its candidates are final
             if (chain_wait(prog_in, kChainDone, B.abort_flag, B.wait_ns) < 0) break;
-            if constexpr (!DIRS) mx = max(mx, __ldcg(&B.run_max[pred]));
+            if constexpr (DIRS == 0) mx = max(mx, __ldcg(&B.run_max[pred]));
         }
         if (store_bnd) {
-            if constexpr (!DIRS)
+            if constexpr (DIRS == 0)
                 if (lane == 0) __stcg(&B.run_max[it], mx);
             chain_publish(prog_out, kChainDone);
         } else if (lane == 0) {
-            if constexpr (DIRS)
+            if constexpr (DIRS != 0)
                 A.metas[BP.slot].n_cand = atomicAdd(ncand, 0);
             else
                 B.max_out[BP.slot] = (float)mx;

@@ -12,6 +12,8 @@
 //                    (SmithWaterman.py:699-838), one thread per pair
 //   ops_kernel       writes the column operations of every kept hit
 #pragma once
+#include <type_traits>
+
 #include "pw_device.cuh"
 
 namespace pw {
@@ -368,6 +370,77 @@ __device__ __forceinline__ void sweep_dirs(const LaneCtx& c, const void* prof, i
     (void)xmax4;
 }
 
+// Direction sweep of linear-gap integer pairs that stores H instead of cell
+// codes: every cell's 16-bit score (all traced maxima are below 2^15), 16 rows
+// of a lane in 32 bytes at the cells' code positions, [strip][x][r / 16][lane]
+// [16 rows], so that a warp stores 1 KB contiguous per 16 rows and column.  The
+// code of a cell (direction, stop flag, candidate flag) is derived on read
+// from the cell and its left, upper and diagonal neighbours (PairView::code):
+// the collect and walk kernels read only the cells on their paths.  The
+// candidate list is written here, as sweep_dirs writes it.
+template <int S, bool TRANS = false>
+__device__ __forceinline__ void sweep_hstore(const LaneCtx& c, const void* prof, int alpha1, int gap,
+                                             Bnd<int>* bnd, uint8_t* hs, int lane, int thr, Cand* cand,
+                                             int cand_cap, int& n_cand) {
+    uint4* out = (uint4*)hs;
+    int H[S];
+#pragma unroll
+    for (int r = 0; r < S; ++r) H[r] = 0;
+    int hb_prev = 0;
+    for (int x4 = 0; x4 < c.lq4; x4 += 4) {
+        const uint32_t cw = *(const uint32_t*)(c.qc + x4);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int x = x4 + j;
+            const int a = (cw >> (8 * j)) & 0xff;
+            int up = c.has_up ? bnd[(int64_t)x * kWarp].m : 0;
+            int diag = hb_prev;
+            hb_prev = up;
+#pragma unroll
+            for (int g = 0; g < S / 4; ++g) {
+                const Prof4<int> p = load_prof<int>(prof, g, alpha1, a);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int r = 4 * g + k;
+                    const int left = H[r];
+                    int h = addmax(left, gap, diag + p.s[k]);
+                    h = relu_addmax(up, gap, h);
+                    if (h >= thr) {
+                        // a candidate is a UL cell (neither gap source
+                        // reaches h, in either orientation) inside the matrix
+                        const bool ul = h > 0 && h != left + gap && h != up + gap;
+                        const int y = c.y0 + r;
+                        if (ul && x < c.lq && y < c.lt) {
+                            if (n_cand < cand_cap) {
+                                Cand cc;
+                                cc.x = TRANS ? y : x;
+                                cc.y = TRANS ? x : y;
+                                cc.score_i = h;
+                                cc.score_f = (float)h;
+                                cand[n_cand] = cc;
+                            }
+                            ++n_cand;
+                        }
+                    }
+                    diag = left;
+                    H[r] = h;
+                    up = h;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < S / 16; ++q) {
+                uint32_t w[8];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) w[k] = __byte_perm(H[16 * q + 2 * k], H[16 * q + 2 * k + 1], 0x5410);
+                uint4* o = out + (((int64_t)x * (S / 16) + q) * kWarp + lane) * 2;
+                o[0] = make_uint4(w[0], w[1], w[2], w[3]);
+                o[1] = make_uint4(w[4], w[5], w[6], w[7]);
+            }
+            if (c.has_down) bnd[(int64_t)x * kWarp].m = H[S - 1];
+        }
+    }
+}
+
 // Sequences on the device.
 struct SeqSet {
     const uint8_t* codes;    // query: compact codes / target: matrix residue index
@@ -410,9 +483,11 @@ __device__ __forceinline__ T from_f(float v) {
 }
 
 // Persistent kernel over work items: one warp per item, dynamic scheduling.
-// PHASE 1 writes pair maxima; PHASE 2 writes cell codes and candidates.
+// PHASE 1 writes pair maxima; PHASE 2 writes cell codes and candidates;
+// PHASE 3 writes 16-bit H values and candidates (sweep_hstore).
 template <typename T, int S, bool AFFINE, bool MULTI, int PHASE, bool TRANS = false>
 __global__ void __launch_bounds__(128) sweep_kernel(KernelArgs A) {
+    static_assert(PHASE != 3 || (std::is_same<T, int>::value && !AFFINE), "H store: linear gap, int lanes");
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -449,7 +524,7 @@ __global__ void __launch_bounds__(128) sweep_kernel(KernelArgs A) {
         Cand* cand = nullptr;
         int cap = 0;
         int64_t pslot = W.pair_base + lane;
-        if (PHASE == 2 && active) {
+        if (PHASE >= 2 && active) {
             const float maxf = A.pair_max[(int64_t)q * A.pm_lane + (int64_t)t * A.pm_strip];
             const int mn = c.lq < lt ? c.lq : lt;
             // maxPossibleScore, SmithWatermanCuda.py:269-275 (double, stored as fp32)
@@ -483,17 +558,21 @@ __global__ void __launch_bounds__(128) sweep_kernel(KernelArgs A) {
             build_profile<T, S>(prof, A.cmat_i8, A.cmat_f, tres, c.y0, lt, alpha1, A.P.dim, lane);
             __syncwarp();
             if (active) {
-                if (PHASE == 1) {
+                if constexpr (PHASE == 1) {
                     sweep_score<T, S, AFFINE>(c, prof, alpha1, gap, ext, ge, bnd_slot, mx);
-                } else {
+                } else if constexpr (PHASE == 2) {
                     uint8_t* codes = A.codes + W.dir_base + (int64_t)s * xmax4 * S * kWarp / 2;
                     sweep_dirs<T, S, AFFINE, TRANS>(c, prof, alpha1, gap, ext, ge, bnd_slot, codes, lane, xmax4,
                                                     thr, cand, cap, n_cand);
+                } else {
+                    uint8_t* hs = A.codes + W.dir_base + (int64_t)s * xmax4 * S * kWarp * 2;
+                    sweep_hstore<S, TRANS>(c, prof, alpha1, (int)gap, (Bnd<int>*)bnd_slot, hs, lane, (int)thr,
+                                           cand, cap, n_cand);
                 }
             }
         }
         if (active) {
-            if (PHASE == 1)
+            if constexpr (PHASE == 1)
                 A.pair_max[(int64_t)q * A.pm_lane + (int64_t)t * A.pm_strip] = (float)mx;
             else {
                 A.metas[pslot].n_cand = n_cand;
@@ -508,7 +587,8 @@ struct TraceArgs {
     const PairMeta* metas;
     int n_pairs;
     const WorkItem* items;
-    uint8_t* codes;          // 4-bit cell codes of the wave
+    uint8_t* codes;          // 4-bit cell codes of the wave, or 16-bit H values (hstore)
+    int hstore;              // linear integer sweeps: the wave holds H, codes are derived on read
     uint8_t* marks;          // one bit per cell of the wave (zeroed per wave): covered, then visited
     Cand* cands;
     const int64_t* cand_base;
@@ -538,19 +618,40 @@ __host__ __device__ __forceinline__ int64_t warp_layout_offset(int x, int y, int
 // (and clears them again), walk_kernel marks the cells it visits
 // (IN_ALIGNMENT).  The cell index is the item's own: the strip or band layout.
 struct PairView {
-    uint8_t* base;      // the item's codes
+    uint8_t* base;      // the item's cell codes (4 bits a cell), or its 16-bit H values (hstore)
     uint8_t* marks;     // the wave's mark plane
-    int64_t cell0;      // the item's first cell in the wave (2 x its code byte offset)
+    int64_t cell0;      // the item's first cell in the wave
     int S, lane, xmax4, lq, lt;
     int layout;  // 0: strip sweep, targets as strips; 1: strip sweep, queries as strips; 2: warp sweep
+    bool hstore;        // base holds H; codes are derived on read
+    int gap, thr;       // hstore: the linear gap and the pair's integer candidate threshold
     // cell (x, y) in the reference's coordinates (x: query, y: target)
     __device__ __forceinline__ int64_t index(int x, int y) const {
         if (layout == 2) return warp_layout_offset(x, y, lq);
         return layout == 1 ? cell_offset_rt(S, y, x, lane, xmax4) : cell_offset_rt(S, x, y, lane, xmax4);
     }
+    // H of a cell; 0 left of and above the matrix (the sweeps' boundary)
+    __device__ __forceinline__ int hval(int x, int y) const {
+        return (x < 0 || y < 0) ? 0 : (int)((const int16_t*)base)[index(x, y)];
+    }
     __device__ __forceinline__ uint32_t code(int x, int y) const {
-        const int64_t i = index(x, y);
-        return (base[i >> 1] >> ((i & 1) * 4)) & 15u;
+        if (!hstore) {
+            const int64_t i = index(x, y);
+            return (base[i >> 1] >> ((i & 1) * 4)) & 15u;
+        }
+        // the classification of sweep_dirs from the stored H values: LEFT
+        // when the left neighbour plus the gap reaches H, else UP when the
+        // upper one does, else UL; NO where H is 0; a UL cell inside the
+        // matrix with a zero diagonal neighbour carries the stop flag, one
+        // reaching the pair's threshold the candidate flag
+        const int h = hval(x, y);
+        if (h <= 0) return kNo;
+        if (h == hval(x - 1, y) + gap) return kLeft;
+        if (h == hval(x, y - 1) + gap) return kUp;
+        uint32_t cd = kUL;
+        if (x > 0 && y > 0 && hval(x - 1, y - 1) == 0) cd |= kStopFlag;
+        if (h >= thr && x < lq && y < lt) cd |= kCand;
+        return cd;
     }
     __device__ __forceinline__ bool marked(int x, int y) const {
         const int64_t i = cell0 + index(x, y);
@@ -571,7 +672,10 @@ __device__ __forceinline__ PairView pair_view(const TraceArgs& A, const PairMeta
     const WorkItem W = A.items[pm.item];
     v.base = A.codes + W.dir_base;
     v.marks = A.marks;
-    v.cell0 = W.dir_base * 2;
+    v.hstore = A.hstore != 0;
+    v.cell0 = v.hstore ? W.dir_base / 2 : W.dir_base * 2;
+    v.gap = A.P.gap_i;
+    v.thr = pm.thr_i;
     v.S = W.S;
     v.lane = pm.lane;
     v.xmax4 = (W.xmax + 3) & ~3;
@@ -952,6 +1056,7 @@ __global__ void prune_kernel(const float* pair_max, const int32_t* q_order, cons
     const int64_t n = (int64_t)nq * nt;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     unsigned long long n_min = 0, n_pass = 0;
+    unsigned pass_max = 0;  // largest maximum of a passing pair (counts[3])
     for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
         const int64_t k = base + threadIdx.x;
         bool m = false, pass = false;
@@ -965,6 +1070,7 @@ __global__ void prune_kernel(const float* pair_max, const int32_t* q_order, cons
                 const float pos = (float)(highest * (double)mn * filter_factor);
                 const float llm = __fmul_rn(lower_limit, mx);
                 pass = mx >= fmaxf(llm, pos);
+                if (pass) pass_max = max(pass_max, __float2uint_rz(fminf(fmaxf(mx, 0.0f), 4.0e9f)));
             }
             flags[k] = pass ? 1 : 0;
         }
@@ -974,9 +1080,11 @@ __global__ void prune_kernel(const float* pair_max, const int32_t* q_order, cons
             n_pass += __popc(bp);
         }
     }
+    pass_max = __reduce_max_sync(0xffffffffu, pass_max);
     if ((threadIdx.x & 31) == 0 && (n_min | n_pass)) {
         atomicAdd(&counts[0], n_min);
         atomicAdd(&counts[1], n_pass);
+        atomicMax(&counts[3], (unsigned long long)pass_max);
     }
 }
 
