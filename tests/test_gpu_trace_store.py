@@ -83,8 +83,13 @@ def test_band_sweep_forms_agree(engine_lib, oracle_mod):
 
 def test_memory_waves_forms_agree(engine_lib, oracle_mod):
     """The same hits when the cells of one call are split into waves."""
-    queries, targets, score, st = _linear(77, max_queries=40, max_tlen=260)
-    o = _oracle(oracle_mod, queries, targets, score, st)
+    seed = 77
+    while True:  # a case with several hits
+        queries, targets, score, st = _linear(seed, max_queries=40, max_tlen=260)
+        o = _oracle(oracle_mod, queries, targets, score, st)
+        if len(o["hits"]) >= 4:
+            break
+        seed += 1
     e = _native.Engine(0, lib=engine_lib)
     try:
         from engine_helpers import configure, decode_hits
