@@ -402,6 +402,20 @@ int pw_txt_records(const pw_hit* hits, int64_t n_hits, int32_t n_queries, int32_
                    const int64_t* t_start_pos, const char* t_id, const int64_t* t_id_off, const double* thresholds,
                    char* out, int64_t out_cap, int64_t* out_len);
 
+/* SAM output (SamFormatter, Formatters.py:51-106; Hit.get_sam_line and
+ * get_sam_sq, Hit.py:222-272,298-304,338-406) of the same HitList, byte for
+ * byte: "@HD", the "@SQ" lines, "@PG", one alignment line per hit (CIGAR,
+ * RC flag and mirroring, reverse-complemented SEQ, AS/RS/BS/QC/QI fields with
+ * Python's float repr).  Arguments as pw_txt_records's plus the query
+ * sequences (q_seq / q_seq_off, as pw_trimmed_fasta takes them); q_id and
+ * t_id hold the ids as they are. */
+int pw_sam_records(const pw_hit* hits, int64_t n_hits, int32_t n_queries, int32_t n_targets,
+                   const char* strbuf, int64_t strbuf_bytes, const int32_t* q_rank, const int64_t* q_orig_len,
+                   const int64_t* q_start_pos, const char* q_id, const int64_t* q_id_off, const char* q_seq,
+                   const int64_t* q_seq_off, const int32_t* t_rank, const int64_t* t_orig_len,
+                   const int64_t* t_start_pos, const char* t_id, const int64_t* t_id_off, const double* thresholds,
+                   char* out, int64_t out_cap, int64_t* out_len);
+
 /* ---------------------------------------------------------------------------
  * Sequence records read natively (host only, no device).  Replaces the
  * reference's record preparation for the engine: BioPythonReader.read_records

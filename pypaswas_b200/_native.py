@@ -60,6 +60,7 @@ EXPORTED_SYMBOLS = (
     "pw_set_wave_limit", "pw_set_tuning", "pw_set_pairs", "pw_server_create", "pw_server_destroy", "pw_server_last_error", "pw_server_set_scoring",
     "pw_server_load_db", "pw_server_submit", "pw_server_wait", "pw_server_top_hits", "pw_server_hits",
     "pw_server_release", "pw_server_stats", "pw_server_tune", "pw_trimmed_fasta", "pw_txt_records",
+    "pw_sam_records",
     "pw_records_parse", "pw_records_read", "pw_records_sizes", "pw_records_copy", "pw_records_free",
     "pw_id_ranks",
 )
@@ -166,6 +167,8 @@ def bind(lib):
                                             ctypes.POINTER(I64)]),
         "pw_txt_records": (ctypes.c_int, [P, I64, I32, I32, P, I64, P, P, P, P, P, P, P, P, P, P, P, P, I64,
                                           ctypes.POINTER(I64)]),
+        "pw_sam_records": (ctypes.c_int, [P, I64, I32, I32, P, I64, P, P, P, P, P, P, P, P, P, P, P, P, P, P,
+                                          I64, ctypes.POINTER(I64)]),
         "pw_records_parse": (ctypes.c_int, [P, I64, ctypes.c_int, I64, I64, I64, ctypes.c_int, ctypes.c_int,
                                             ctypes.POINTER(ctypes.c_void_p), ctypes.c_char_p, I32]),
         "pw_records_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, I64, I64, I64, ctypes.c_int,

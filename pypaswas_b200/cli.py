@@ -15,10 +15,10 @@ chunks (the reference re-initialises its device state per chunk).
 Two output paths give the same file:
   * objects: every chunk goes through Aligner/Trimmer.process into one HitList
     of Hit objects, which the formatter prints (the reference's path);
-  * native: when the output is TXT or trimmedFasta, ids are unique within each
+  * native: when the output is TXT, SAM or trimmedFasta, ids are unique within each
     file and per-hit log records are off (level above INFO), the engine's hit
     records of all chunks go straight to the native formatter
-    (pw_txt_records / pw_trimmed_fasta) -- no Hit objects.
+    (pw_txt_records / pw_sam_records / pw_trimmed_fasta) -- no Hit objects.
 """
 import configparser
 import logging
@@ -201,7 +201,7 @@ class Pypaswas(object):
             raise InvalidOptionException("Invalid program selected {0}".format(self.settings.program))
 
     def _native_ok(self, query_path, target_path):
-        if self.output_format not in ("TXT", "trimmedFasta"):
+        if self.output_format not in ("TXT", "SAM", "trimmedFasta"):
             return False
         if self.logger.isEnabledFor(logging.INFO):
             return False  # the object path logs every HitList append
@@ -321,22 +321,29 @@ def _ids_unique(path, filetype):
     return len(set(ids)) == len(ids)
 
 
+def formatters_hitlist():
+    from .hits import HitList
+    return HitList(None)
+
+
 def _native_text(parts, output_format, settings):
     """The output file's text from the hit records of every chunk: one native
     formatter call over all of them, with record indices and string offsets
     made global."""
     if not parts:
-        return ""
+        return "".join(line + "\n" for line in formatters.SamFormatter(None, formatters_hitlist(), None).lines()) \
+            if output_format == "SAM" else ""
     hits = np.concatenate([p[0] for p in parts])
     queries = readers.concat([p[2] for p in parts])
     targets = readers.concat([p[3] for p in parts])
-    if output_format == "TXT":
+    if output_format in ("TXT", "SAM"):
         k = shift = 0
         for h, sb, _, _ in parts:
             hits["str_offset"][k:k + len(h)] += shift
             k += len(h)
             shift += len(sb)
-        return formatters.txt_records(hits, b"".join(p[1] for p in parts), queries, targets, settings)
+        fmt = formatters.txt_records if output_format == "TXT" else formatters.sam_records
+        return fmt(hits, b"".join(p[1] for p in parts), queries, targets, settings)
     return formatters.trimmed_fasta(hits, queries, targets, settings)
 
 

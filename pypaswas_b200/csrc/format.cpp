@@ -17,6 +17,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "pw_host.h"
@@ -444,6 +445,170 @@ extern "C" int pw_txt_records(const pw_hit* hits, int64_t n_hits, int32_t n_quer
         o.append(sb + n, (size_t)n);
         o += '\n';
         o.append(sb + 2 * n, (size_t)n);
+        o += '\n';
+    }
+    *out_len = (int64_t)o.size();
+    if (!out) return PW_OK;
+    if (out_cap < (int64_t)o.size()) return PW_ERR_CAPACITY;
+    if (!o.empty()) std::memcpy(out, o.data(), o.size());
+    return PW_OK;
+}
+
+namespace {
+
+// Python's identifier[:-3] if identifier[-2:] == "RC" else identifier
+// (the formatters' RC suffix strip; Hit.py:159-164, Formatters.py:67-83)
+inline bool ends_rc(const char* s, int64_t n) { return n >= 2 && s[n - 2] == 'R' && s[n - 1] == 'C'; }
+inline int64_t stripped_len(const char* s, int64_t n) { return ends_rc(s, n) ? std::max<int64_t>(n - 3, 0) : n; }
+
+// IUPAC complement (case kept): the table the reverse-complement targets use
+struct Complement {
+    char t[256];
+    Complement() {
+        for (int i = 0; i < 256; ++i) t[i] = (char)i;
+        const char* from = "ACGTUNKMRYSWBDHVacgtunkmryswbdhv";
+        const char* to = "TGCAANMKYRSWVHDBtgcaanmkyrswvhdb";
+        for (int i = 0; from[i]; ++i) t[(uint8_t)from[i]] = to[i];
+    }
+};
+
+}  // namespace
+
+// SAM text (SamFormatter.print_results, Formatters.py:51-106) of the same
+// HitList: "@HD", one "@SQ" line per target id in order of first use (the
+// formatter's dict keyed by the id without its RC suffix, looked up by the id
+// as it is), "@PG", then Hit.get_sam_line per hit (Hit.py:222-272,338-406):
+// QNAME / RNAME without the RC suffix, FLAG 16 when either id ends in "RC",
+// POS 1-based on the target (mirrored on RC hits), MAPQ 255, the extended
+// CIGAR of the alignment string (reversed on RC hits, soft clips mirrored),
+// SEQ the query (reverse-complemented on RC hits), then AS:i / RS:f / BS:f /
+// QC:f / QI:f with Python's int() and float repr.  strbuf holds the hits'
+// strings (pw_get_hits); ids arrive as they are.
+extern "C" int pw_sam_records(const pw_hit* hits, int64_t n_hits, int32_t n_queries, int32_t n_targets,
+                              const char* strbuf, int64_t strbuf_bytes, const int32_t* q_rank,
+                              const int64_t* q_orig_len, const int64_t* q_start_pos, const char* q_id,
+                              const int64_t* q_id_off, const char* q_seq, const int64_t* q_seq_off,
+                              const int32_t* t_rank, const int64_t* t_orig_len, const int64_t* t_start_pos,
+                              const char* t_id, const int64_t* t_id_off, const double* thresholds, char* out,
+                              int64_t out_cap, int64_t* out_len) {
+    if (n_hits < 0 || (n_hits > 0 && (!hits || !strbuf || !q_rank || !q_orig_len || !q_start_pos || !q_id ||
+                                      !q_id_off || !q_seq || !q_seq_off || !t_rank || !t_orig_len ||
+                                      !t_start_pos || !t_id || !t_id_off)) ||
+        !thresholds || !out_len)
+        return PW_ERR_ARG;
+    for (int64_t i = 0; i < n_hits; ++i)
+        if (hits[i].n_cols <= 0 || hits[i].str_offset < 0 ||
+            hits[i].str_offset + 3 * (int64_t)hits[i].n_cols > strbuf_bytes)
+            return PW_ERR_ARG;
+    std::vector<Rec> rec;
+    std::vector<int64_t> order;
+    const int rc = ordered_real_hits(hits, n_hits, n_queries, n_targets, q_rank, q_orig_len, q_start_pos, t_rank,
+                                     t_orig_len, t_start_pos, thresholds, rec, order);
+    if (rc != PW_OK) return rc;
+    static const Complement comp;
+    // @SQ lines: a dict keyed by the stripped id; a hit whose id is already a
+    // key (an id without the suffix) is skipped, otherwise its stripped key is
+    // (re)assigned, keeping the key's first position
+    std::vector<std::string> sq;
+    {
+        std::unordered_map<std::string, size_t> keys;  // stripped id -> its line
+        int prev = -1;
+        for (int64_t i : order) {
+            const int t = rec[i].t;
+            if (t == prev) continue;  // the same lookup and assignment again: no change
+            prev = t;
+            const char* id = t_id + t_id_off[t];
+            const int64_t n = t_id_off[t + 1] - t_id_off[t];
+            if (keys.count(std::string(id, (size_t)n))) continue;
+            const std::string key(id, (size_t)stripped_len(id, n));
+            std::string line = "@SQ\tSN:" + key + "\tLN:" + std::to_string(t_orig_len[t]);
+            auto f = keys.find(key);
+            if (f != keys.end()) {
+                sq[f->second] = std::move(line);
+            } else {
+                keys.emplace(key, sq.size());
+                sq.push_back(std::move(line));
+            }
+        }
+    }
+    std::string o = "@HD\tVN:1.4\tSO:unknown\n";
+    for (const std::string& l : sq) {
+        o += l;
+        o += '\n';
+    }
+    o += "@PG\tID:0\tPN:paswas\tVN:3.0\n";
+    std::string aln, smatch;
+    for (int64_t i : order) {
+        const pw_hit& h = hits[i];
+        const Rec& r = rec[i];
+        const int64_t n = h.n_cols;
+        const char* qi = q_id + q_id_off[r.q];
+        const int64_t qn = q_id_off[r.q + 1] - q_id_off[r.q];
+        const char* ti = t_id + t_id_off[r.t];
+        const int64_t tn = t_id_off[r.t + 1] - t_id_off[r.t];
+        const bool is_rc = ends_rc(qi, qn) || ends_rc(ti, tn);
+        const int64_t s0 = r.s0, s1 = h.s_end + q_start_pos[r.q];
+        const int64_t ql = q_orig_len[r.q], tl = t_orig_len[r.t];
+        const char* seq = q_seq + q_seq_off[r.q];
+        const int64_t L = q_seq_off[r.q + 1] - q_seq_off[r.q];
+        const char* sb = strbuf + h.str_offset;
+        smatch.assign(sb, (size_t)n);
+        aln.assign(sb + n, (size_t)n);
+        if (is_rc) {
+            std::reverse(aln.begin(), aln.end());
+            std::reverse(smatch.begin(), smatch.end());
+        }
+        o.append(qi, (size_t)stripped_len(qi, qn));
+        o += is_rc ? "\t16\t" : "\t0\t";
+        o.append(ti, (size_t)stripped_len(ti, tn));
+        o += '\t';
+        o += std::to_string(is_rc ? tl - r.t1 : r.t0 + 1);
+        o += "\t255\t";
+        // CIGAR: soft clip, one run per stretch of equal alignment
+        // characters named by its last column, soft clip
+        if (is_rc) {
+            o += std::to_string(L - s1 - 1);
+            o += 'S';
+        } else if (s0 > 0) {
+            o += std::to_string(s0);
+            o += 'S';
+        }
+        auto cigar_char = [&](int64_t p) -> char {
+            if (aln[p] == '|') return '=';
+            if (aln[p] == '.') return 'X';
+            return smatch[p] == '-' ? 'D' : 'I';
+        };
+        int64_t run = 0;
+        for (int64_t k = 1; k < n; ++k)
+            if (aln[k] != aln[run]) {
+                o += std::to_string(k - run);
+                o += cigar_char(k - 1);
+                run = k;
+            }
+        o += std::to_string(n - run);
+        o += cigar_char(n - 1);
+        const int64_t tail = is_rc ? s0 : ql - s1 - 1;
+        if (tail > 0) {
+            o += std::to_string(tail);
+            o += 'S';
+        }
+        o += "\t*\t0\t0\t";
+        if (is_rc) {
+            for (int64_t k = L - 1; k >= 0; --k) o += comp.t[(uint8_t)seq[k]];
+        } else {
+            o.append(seq, (size_t)L);
+        }
+        o += "\t*\tAS:i:";
+        o += std::to_string((int64_t)r.score);
+        const double span = (double)(s1 - s0 + 1);
+        o += "\tRS:f:";
+        put_pyfloat(o, r.score / (double)std::min(ql, tl));
+        o += "\tBS:f:";
+        put_pyfloat(o, r.score / (double)n);
+        o += "\tQC:f:";
+        put_pyfloat(o, span / (double)ql);
+        o += "\tQI:f:";
+        put_pyfloat(o, (double)h.matches / span);
         o += '\n';
     }
     *out_len = (int64_t)o.size();

@@ -71,18 +71,7 @@ def _record_arrays(sequences, targets, settings, strip_target_rc):
         order = {v: k for k, v in enumerate(sorted(set(ids)))}
         return np.array([order[v] for v in ids], dtype=np.int32)
 
-    def blob(items):
-        text = "".join(items)
-        if text.isascii():
-            data = text.encode("ascii")
-            lens = np.fromiter(map(len, items), dtype=np.int64, count=len(items))
-        else:
-            enc = [x.encode("utf-8") for x in items]
-            data = b"".join(enc)
-            lens = np.fromiter(map(len, enc), dtype=np.int64, count=len(enc))
-        off = np.zeros(len(items) + 1, dtype=np.int64)
-        np.cumsum(lens, out=off[1:])
-        return np.frombuffer(data or b"\0", dtype=np.uint8), off
+    blob = _blob
 
     def arrays(records, strip_rc):
         if _is_packed(records):  # packed records (pypaswas_b200.readers): no per-record objects
@@ -103,6 +92,22 @@ def _record_arrays(sequences, targets, settings, strip_target_rc):
     thr = np.array([float(settings.relative_score), float(settings.query_identity),
                     float(settings.query_coverage), float(settings.base_score)], dtype=np.float64)
     return q, t, thr, blob
+
+
+def _blob(items):
+    """The UTF-8 bytes of strings concatenated, with int64 offsets."""
+    import numpy as np
+    text = "".join(items)
+    if text.isascii():
+        data = text.encode("ascii")
+        lens = np.fromiter(map(len, items), dtype=np.int64, count=len(items))
+    else:
+        enc = [x.encode("utf-8") for x in items]
+        data = b"".join(enc)
+        lens = np.fromiter(map(len, enc), dtype=np.int64, count=len(enc))
+    off = np.zeros(len(items) + 1, dtype=np.int64)
+    np.cumsum(lens, out=off[1:])
+    return np.frombuffer(data or b"\0", dtype=np.uint8), off
 
 
 def _ascii(blob):
@@ -184,6 +189,42 @@ def txt_records(hits, strbuf, sequences, targets, settings, lib=None):
     return _call_twice(lib.pw_txt_records, head, tail, est)
 
 
+def _query_residues(sequences, what):
+    """(residues, offsets) of the queries for a native formatter; ASCII only."""
+    from .exceptions import InvalidOptionException
+    if _is_packed(sequences):
+        q_seq, q_seq_off = sequences.residues, sequences.offsets
+        if len(q_seq) and int(q_seq.max()) >= 128:
+            raise InvalidOptionException("%s needs ASCII sequences" % what)
+        return q_seq, q_seq_off
+    qseqs = [str(r.seq) for r in sequences]
+    if not "".join(qseqs).isascii():
+        raise InvalidOptionException("%s needs ASCII sequences" % what)
+    return _blob(qseqs)
+
+
+def sam_records(hits, strbuf, sequences, targets, settings, lib=None):
+    """The SAM text (SamFormatter.print_results: @HD, @SQ, @PG and one line
+    per hit) of engine hit records and their strings (Engine.hits()), built
+    in native code (pw_sam_records)."""
+    import ctypes
+    import numpy as np
+    from . import _native
+    lib = lib if lib is not None else _native.load_library()
+    hits = np.ascontiguousarray(hits, dtype=_native.HIT_DTYPE)
+    q, t, thr, _ = _record_arrays(sequences, targets, settings, False)
+    q_seq, q_seq_off = _query_residues(sequences, "SAM output")
+    sb = np.frombuffer(bytes(strbuf) or b"\0", dtype=np.uint8)
+    vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    head = (vp(hits) if len(hits) else None, len(hits), len(sequences), len(targets), vp(sb), len(strbuf))
+    tail = tuple(vp(a) for a in q) + (vp(q_seq), vp(q_seq_off)) + tuple(vp(a) for a in t) + (vp(thr),)
+    q_len = np.diff(q_seq_off)
+    qi = np.clip(hits["query"].astype(np.int64), 0, max(len(q_len) - 1, 0))
+    body = (2 * hits["n_cols"].astype(np.int64) + q_len[qi] + 200) if len(hits) and len(q_len) else 0
+    est = _per_hit_estimate(hits, q[4], t[4], body) + 64 * (len(targets) + 2)
+    return _call_twice(lib.pw_sam_records, head, tail, est)
+
+
 def trimmed_fasta(hits, sequences, targets, settings, lib=None):
     """The trimmedFasta text of engine hit records (pw_get_hits order) -- the
     bytes TrimmerFormatter(...).print_results writes for the HitList that the
@@ -197,16 +238,8 @@ def trimmed_fasta(hits, sequences, targets, settings, lib=None):
     from .exceptions import InvalidOptionException
     lib = lib if lib is not None else _native.load_library()
     hits = np.ascontiguousarray(hits, dtype=_native.HIT_DTYPE)
-    q, t, thr, blob = _record_arrays(sequences, targets, settings, True)
-    if _is_packed(sequences):
-        q_seq, q_seq_off = sequences.residues, sequences.offsets
-        if len(q_seq) and int(q_seq.max()) >= 128:
-            raise InvalidOptionException("trimmed_fasta needs ASCII sequences")
-    else:
-        qseqs = [str(r.seq) for r in sequences]
-        if not "".join(qseqs).isascii():
-            raise InvalidOptionException("trimmed_fasta needs ASCII sequences")
-        q_seq, q_seq_off = blob(qseqs)
+    q, t, thr, _ = _record_arrays(sequences, targets, settings, True)
+    q_seq, q_seq_off = _query_residues(sequences, "trimmed_fasta")
     vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)
     head = (vp(hits) if len(hits) else None, len(hits), len(sequences), len(targets))
     tail = tuple(vp(a) for a in q) + (vp(q_seq), vp(q_seq_off)) + tuple(vp(a) for a in t) + (vp(thr),)

@@ -71,6 +71,17 @@ class Aligner(object):
         hits, strbuf, block = _one_block(self, records_seqs, targets)
         return txt_records(hits, strbuf, records_seqs, block, self.settings)
 
+    def sam(self, records_seqs, targets):
+        """The SAM output of process() + SamFormatter, byte for byte, with the
+        HitList and the records built in native code (formatters.sam_records)."""
+        from .formatters import sam_records
+        if len(targets) == 0:
+            import numpy as np
+            from . import _native
+            return sam_records(np.zeros(0, dtype=_native.HIT_DTYPE), b"", records_seqs, targets, self.settings)
+        hits, strbuf, block = _one_block(self, records_seqs, targets)
+        return sam_records(hits, strbuf, records_seqs, block, self.settings)
+
 
 class Trimmer(Aligner):
     """Same loop; output goes through the trimmedFasta formatter (Programs.py:95-120)."""

@@ -108,7 +108,8 @@ def test_cli_output_files_equal_the_reference(engine_lib, tmp_path, name):
             "trimmedFasta": "".join(t + "\n" for t in fx["trimmed"])}
     runs = [("TXT", ["--loglevel", "ERROR"], True),
             ("TXT", ["--loglevel", "INFO", "-L", str(tmp_path / "log")], False),
-            ("SAM", ["--loglevel", "ERROR"], False),
+            ("SAM", ["--loglevel", "ERROR"], True),
+            ("SAM", ["--loglevel", "INFO", "-L", str(tmp_path / "log_sam")], False),
             # query chunks of 3 records (the target chunk covers the whole file)
             ("TXT", ["--loglevel", "ERROR", "--query_step", "3"], True)]
     if fx["program"] == "trimmer":

@@ -221,3 +221,13 @@ def test_native_hit_builder_equals_the_interpreter_path(seed):
     sw._build_hits_python(hits, strbuf, queries, targets, python, sp, tp, ql, tl)
     assert 0 < len(native.real_hits) < n
     assert _hit_state(native) == _hit_state(python)
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_native_sam_writes_the_reference_file(name):
+    """pw_sam_records on the engine records of each fixture writes the SAM
+    file the reference wrote (SamFormatter over the reference's HitList)."""
+    from pypaswas_b200.formatters import sam_records
+    fx = G.load(name)
+    hits, strbuf, queries, targets = _engine_records(fx)
+    assert sam_records(hits, strbuf, queries, targets, G.FixtureSettings(fx)) == fx["sam_text"]

@@ -202,3 +202,45 @@ def test_native_formatter_id_ranks_follow_python_order():
         q, _, _, _ = _record_arrays(recs, recs, st, False)
         order = {v: k for k, v in enumerate(sorted(set(ids)))}
         assert q[0].tolist() == [order[v] for v in ids]
+
+
+def test_native_sam_records_match_sam_formatter(engine_lib):
+    """formatters.sam_records (pw_sam_records) writes exactly what
+    SamFormatter.print_results writes for the driver's HitList: @SQ lines in
+    the formatter's dict order (ids that strip to the same key, one without
+    the suffix), RC flags and mirrored CIGARs, reverse-complemented SEQ,
+    soft clips with start positions, mixed match / mismatch / gap runs, the
+    float fields in Python's repr."""
+    import logging
+    import numpy as np
+    import cases
+    from pypaswas_b200.formatters import SamFormatter, sam_records
+    from pypaswas_b200.hits import HitList
+    from pypaswas_b200.smith_waterman import SmithWatermanB200
+    for seed in (6, 7, 8):
+        hits, strbuf, seqs, tgts = _synthetic_trimmer_hits(seed)
+        rng = np.random.default_rng(seed)
+        seqs[5].id = "read5_RC"
+        seqs[6].id = "readRC"
+        tgts[4].id = "adapter1zRC"  # strips to the key of adapter1_RC
+        tgts[5].id = "adapter1"
+        # alignment strings with runs of matches, mismatches and both gap kinds
+        text = bytearray(strbuf)
+        for h in hits:
+            k, o = int(h["n_cols"]), int(h["str_offset"])
+            kinds = rng.integers(0, 4, size=k)
+            text[o:o + k] = b"".join(b"-" if c == 2 else b"ACGT"[int(rng.integers(0, 4))].to_bytes(1, "little")
+                                     for c in kinds)
+            text[o + k:o + 2 * k] = b"".join(b"|" if c == 0 else b"." if c == 1 else b" " for c in kinds)
+            text[o + 2 * k:o + 3 * k] = b"".join(b"-" if c == 3 else b"G" for c in kinds)
+        strbuf = bytes(text)
+        hits["score"] = hits["score"] + (seed - 6) * 0.5
+        st = cases.Settings(relative_score="0", query_identity="0", query_coverage="0", base_score="0")
+        sw = SmithWatermanB200.__new__(SmithWatermanB200)
+        sw.logger = logging.getLogger("test")
+        sw.settings = st
+        hl = HitList(sw.logger)
+        sw._build_hits(hits, strbuf, seqs, tgts, hl)
+        expect = "".join(line + "\n" for line in SamFormatter(None, hl, None).lines())
+        assert len(hl.real_hits) > 20 and "\t16\t" in expect
+        assert sam_records(hits, strbuf, seqs, tgts, st, lib=engine_lib) == expect
