@@ -243,6 +243,7 @@ struct pw_engine {
     DevBuf acc_hits, acc_ops, fk_a, fk_b, fk_c, fk_t, fk_g, fi_a, fi_b, f_len, f_soff, f_out, f_str;
     HostBuf<int64_t> h_sel;
     HostBuf<int32_t> h_ptq, h_p2order;  // phase-2 pair lists (kept across calls: no page faults, no zero fill)
+    HostBuf<uint8_t> h_qc, h_qres;      // query encodings staged for upload (page-locked, kept across calls)
     int64_t free_mem = 0;    // free device memory plus this engine's kept wave buffers, as last queried
     double free_mem_t = -1;  // wall_ms() of that query
     DevBuf chain_items, chain_info, chain_prog, chain_max, chain_ring_off, chain_ring, chain_abort, p1_items, p1_grid;
@@ -673,16 +674,42 @@ static int prepare_queries(pw_engine* e) {
     const HostSeqs& Q = e->Q;
     const int off = e->char_offset, dim = e->dim;
     Prepared& pr = e->pr;
-    // residues must index the matrix (default_main.cu:234 reads matrix[c - offset])
+    // residues must index the matrix (default_main.cu:234 reads matrix[c - offset]);
+    // the compact alphabet numbers the residues in order of first occurrence
     int map[256];
     for (int i = 0; i < 256; ++i) map[i] = -1;
     std::vector<int> alphabet;
-    for (uint8_t c : Q.raw) {
-        if (map[c] >= 0) continue;
-        if (c == 0 || (int)c < off || (int)c >= off + dim)
-            return fail(e, PW_ERR_ARG, "query residue outside the scoring matrix: code " + std::to_string(c));
-        map[c] = (int)alphabet.size();
-        alphabet.push_back(c);
+    {
+        // first occurrence of every byte value, over host threads
+        const int64_t nraw = (int64_t)Q.raw.size();
+        std::vector<std::vector<int64_t>> first_k(64);
+        std::mutex mu;
+        parallel_for(nraw, [&](int64_t b0, int64_t b1) {
+            std::vector<int64_t> f(256, INT64_MAX);
+            for (int64_t k = b0; k < b1; ++k)
+                if (f[Q.raw[k]] == INT64_MAX) f[Q.raw[k]] = k;
+            std::lock_guard<std::mutex> g(mu);
+            for (auto& v : first_k)
+                if (v.empty()) {
+                    v.swap(f);
+                    break;
+                }
+        }, (int64_t)1 << 22);
+        std::vector<std::pair<int64_t, int>> firsts;
+        for (int c = 0; c < 256; ++c) {
+            int64_t fk = INT64_MAX;
+            for (auto& v : first_k)
+                if (!v.empty()) fk = std::min(fk, v[c]);
+            if (fk != INT64_MAX) firsts.push_back({fk, c});
+        }
+        std::sort(firsts.begin(), firsts.end());
+        for (auto& fc : firsts) {
+            const int c = fc.second;
+            if (c == 0 || c < off || c >= off + dim)
+                return fail(e, PW_ERR_ARG, "query residue outside the scoring matrix: code " + std::to_string(c));
+            map[c] = (int)alphabet.size();
+            alphabet.push_back(c);
+        }
     }
     if (alphabet.size() > 250) return fail(e, PW_ERR_ARG, "too many distinct query residues");
     pr.alpha = (int)alphabet.size();
@@ -719,17 +746,38 @@ static int prepare_queries(pw_engine* e) {
         pos += align_up(std::max<int64_t>(pr.qlen[i], 1), 16);
     }
     qco[Q.n] = pos;
-    std::vector<uint8_t> qc((size_t)std::max<int64_t>(pos, 16), (uint8_t)pr.alpha);
-    for (int32_t i = 0; i < Q.n; ++i)
-        for (int32_t k = 0; k < pr.qlen[i]; ++k) qc[qco[i] + k] = (uint8_t)map[Q.raw[Q.off[i] + k]];
-    pr.order.resize(Q.n);
-    std::iota(pr.order.begin(), pr.order.end(), 0);
-    std::stable_sort(pr.order.begin(), pr.order.end(),
-                     [&](int a, int b) { return pr.qlen[a] > pr.qlen[b]; });
     // the transposed orientation: queries as strips (matrix residue indices)
-    std::vector<uint8_t> qres(qc.size(), 0);
-    for (int32_t i = 0; i < Q.n; ++i)
-        for (int32_t k = 0; k < pr.qlen[i]; ++k) qres[qco[i] + k] = (uint8_t)(Q.raw[Q.off[i] + k] - off);
+    HostBuf<uint8_t>& qc = e->h_qc;
+    HostBuf<uint8_t>& qres = e->h_qres;
+    if (!qc.resize((size_t)std::max<int64_t>(pos, 16)) || !qres.resize((size_t)std::max<int64_t>(pos, 16)))
+        return fail(e, PW_ERR_NOMEM, "host memory for the query encodings");
+    parallel_for(Q.n, [&](int64_t i0, int64_t i1) {
+        for (int64_t i = i0; i < i1; ++i) {
+            const uint8_t* r = Q.raw.data() + Q.off[i];
+            uint8_t* d = qc.data() + qco[i];
+            uint8_t* d2 = qres.data() + qco[i];
+            const int64_t L = pr.qlen[i], end = qco[i + 1] - qco[i];
+            for (int64_t k = 0; k < L; ++k) {
+                d[k] = (uint8_t)map[r[k]];
+                d2[k] = (uint8_t)(r[k] - off);
+            }
+            for (int64_t k = L; k < end; ++k) {
+                d[k] = (uint8_t)pr.alpha;
+                d2[k] = 0;
+            }
+        }
+    }, (int64_t)1 << 14);
+    for (size_t k = (size_t)pos; k < qc.size(); ++k) {
+        qc.data()[k] = (uint8_t)pr.alpha;
+        qres.data()[k] = 0;
+    }
+    // a stable sort by length, longest first
+    {
+        std::vector<uint64_t> key((size_t)Q.n);
+        for (int32_t i = 0; i < Q.n; ++i) key[i] = (uint64_t)(pr.maxlq - pr.qlen[i]);
+        const std::vector<uint32_t> o = radix_order(std::move(key));
+        pr.order.assign(o.begin(), o.end());
+    }
     cudaError_t c;
 #define UP(buf, vec)                                      \
     if ((c = upload(e, buf, vec)) != cudaSuccess) return cuda_fail(e, c, "upload " #buf);
@@ -1875,12 +1923,6 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         }
         ht.mark("passing pairs to per-target lists");
     }
-    // Linear integer scoring whose traced maxima all stay below 2^15: the
-    // direction sweeps store each cell's 16-bit H (four times the bytes of a
-    // 4-bit code, a few instructions a cell instead of the classification);
-    // collect and walk derive the codes of the cells they visit
-    const bool hstore = pr.int_path && !e->affine && max_pass < 32767 && e->tune[PW_TUNE_TRACE_STORE] != 1;
-    inf.trace_store = hstore ? 1 : 0;
     auto span_n = [&](int t) -> int64_t { return pt_off[t + 1] - pt_off[t]; };
     // Traced pairs with targets longer than one register strip go to the
     // one-warp-per-pair sweep (pw_band.cuh); the others are grouped 32 to
@@ -1906,6 +1948,19 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     }
     auto live_n = [&](int t) -> int64_t { return t_warp[t] ? 0 : span_n(t); };
     ht.mark("warp-sweep routing");
+    // Linear integer scoring whose traced maxima all stay below 2^15, with
+    // most traced cells on the strip sweep: the direction sweeps store each
+    // cell's 16-bit H (four times the bytes of a 4-bit code, a few
+    // instructions a cell instead of the classification); collect and walk
+    // derive the codes of the cells they visit.  Long pairs (the one-warp
+    // band sweep) keep the codes: their multi-kilobase walks read one code
+    // per step instead of up to four H values, and their cells fit fewer
+    // memory waves.
+    int64_t warp_cells = 0;
+    for (const auto& wp : warp_pairs) warp_cells += (int64_t)qlen[wp.first] * tlen[wp.second];
+    const bool hstore = pr.int_path && !e->affine && max_pass < 32767 && e->tune[PW_TUNE_TRACE_STORE] != 1 &&
+                        inf.traced_cells - warp_cells >= warp_cells;
+    inf.trace_store = hstore ? 1 : 0;
     const int per_item = plain ? 1 : kWarp;
     double cost_t = 0, cost_q = 0;
     for (int t = 0; t < nt; ++t)

@@ -71,14 +71,27 @@ def test_both_lane_orientations(engine_lib, oracle_mod, shape):
 
 def test_band_sweep_forms_agree(engine_lib, oracle_mod):
     """Targets longer than one register strip: one pair per warp, 256-row
-    bands chained across warps."""
+    bands chained across warps.  Alone they keep the codes (their long walks
+    read one code a step); next to a majority of strip-sweep cells they store
+    H as well, in the band layout."""
     rng = np.random.default_rng(41)
     motif = "".join(rng.choice(list("ACGT"), size=700))
     queries = [cases.mutate(rng, motif[k * 50:k * 50 + 400], "ACGT", 0.1, 3) for k in range(5)]
     targets = [motif, "".join(rng.choice(list("ACGT"), size=900))]
     st = cases.Settings(minimum_score="20", lower_limit_score="0.9")
     score = cases.scores.make_score(st)
-    _both_forms(engine_lib, oracle_mod, queries, targets, score, st, 1)
+    _both_forms(engine_lib, oracle_mod, queries, targets, score, st, 0)
+    # 600 reads against 10 short adapters (strip sweep, > 32 traced pairs per
+    # SM) and one target of two bands (band sweep, fewer cells), all pairs
+    # traced
+    ad = ["".join(rng.choice(list("ACGT"), size=int(rng.integers(24, 40)))) for _ in range(10)]
+    queries = ["".join(rng.choice(list("ACGT"), size=int(rng.integers(20, 50)))) + ad[i % 10][:20]
+               for i in range(600)]
+    targets = ad + ["".join(rng.choice(list("ACGT"), size=250)) + ad[0]]
+    st = cases.Settings(minimum_score="1", lower_limit_score="0.5", filter_factor="0.0")
+    score = cases.scores.make_score(st)
+    info = _both_forms(engine_lib, oracle_mod, queries, targets, score, st, 1)
+    assert 0 < info.warp_pairs < info.traced_pairs
 
 
 def test_memory_waves_forms_agree(engine_lib, oracle_mod):
