@@ -87,13 +87,13 @@ def parse():
     ap.add_argument("--tune", action="append", default=[], metavar="KEY=VALUE",
                     help="engine tuning knob (chain_min, grid_share, segment, dual, cand_slot), e.g. "
                          "--tune chain_min=250; without chain_min the autotuner picks it during the warm-up")
-    ap.add_argument("--serve-seconds", type=float, default=6.0, help="length of each arrival stream of the serving leg")
-    ap.add_argument("--serve-loads", default="0.3,0.5,0.6,0.7", help="offered loads (fractions of batched peak) swept")
-    ap.add_argument("--serve-streams", type=int, default=1,
+    ap.add_argument("--serve-seconds", type=float, default=20.0, help="length of each arrival stream of the serving leg")
+    ap.add_argument("--serve-loads", default="0.5,0.7", help="offered loads (fractions of batched peak) swept")
+    ap.add_argument("--serve-streams", type=int, default=3,
                     help="arrival streams per offered load (different seeds); the report gives the median p99")
     ap.add_argument("--serve-workers", type=int, default=2)
     ap.add_argument("--serve-max-batch", type=int, default=32)
-    ap.add_argument("--serve-policy", type=int, default=0, help="0 arrival order, 1 shortest first with aging")
+    ap.add_argument("--serve-policy", type=int, default=1, help="0 arrival order, 1 shortest first with aging")
     return ap.parse_args()
 
 
@@ -596,7 +596,7 @@ def parity_leg(w, jobs, idx, oracle_res, device):
 
 
 # ------------------------------------------------------------------ serving
-def serve_leg(device, seconds, loads, workers=2, max_batch=32, policy=0, streams=1, age_ms=25):
+def serve_leg(device, seconds, loads, workers=2, max_batch=32, policy=1, streams=3, age_ms=25):
     """Serving configuration: a resident database of 100,000 protein sequences
     (log-normal lengths, median 300, 50-1,500 aa), Poisson arrivals of single
     queries (log-normal, median 300, max 5,000 aa), 70% top-10 by pair maximum

@@ -239,7 +239,8 @@ int pw_get_pair_max(pw_engine* e, float* out, int64_t n);
 
 /* Hits of the last pw_align in the order the reference appends them to its
  * HitList: ascending score, then the pinned emission order of their starting
- * points.  strbuf receives the alignment strings (info->string_bytes). */
+ * points.  strbuf receives the alignment strings (info->string_bytes); a null
+ * strbuf copies the hit records only. */
 int pw_get_hits(pw_engine* e, pw_hit* hits, int64_t max_hits, char* strbuf, int64_t strbuf_bytes);
 
 /* Starting points of the last pw_align (StartingPoint layout of
@@ -326,7 +327,7 @@ int pw_server_hits(pw_server* s, int64_t ticket, pw_hit* hits, int64_t max_hits,
                    int64_t strbuf_bytes);
 /* pw_set_tuning on every worker engine, or, for the keys below, a setting of
  * the server's own scheduler:
- *   PW_SERVE_TUNE_POLICY   0: batches in arrival order (default); 1: the
+ *   PW_SERVE_TUNE_POLICY   0: batches in arrival order; 1 (default): the
  *                          shortest waiting queries first, except that a
  *                          request waiting longer than PW_SERVE_TUNE_AGE_MS
  *                          goes first (no request starves)

@@ -313,14 +313,19 @@ class Engine(object):
         _check(self.lib, self.handle, self.lib.pw_get_pair_max(self.handle, _ptr(out), out.size), "pw_get_pair_max")
         return out
 
-    def hits(self):
-        """Returns (structured array of hits in HitList order, string bytes)."""
+    def hits(self, strings=True):
+        """Returns (structured array of hits in HitList order, string bytes);
+        strings=False skips the alignment strings (b"")."""
         n = int(self.last_info.hits) if self.last_info is not None else 0
-        nb = int(self.last_info.string_bytes) if self.last_info is not None else 0
-        hits = np.zeros(n, dtype=HIT_DTYPE)
-        strbuf = np.zeros(max(nb, 1), dtype=np.uint8)
-        _check(self.lib, self.handle, self.lib.pw_get_hits(self.handle, _ptr(hits), n, _ptr(strbuf), nb),
-               "pw_get_hits")
+        nb = int(self.last_info.string_bytes) if self.last_info is not None and strings else 0
+        hits = np.empty(n, dtype=HIT_DTYPE)
+        if not strings:
+            _check(self.lib, self.handle, self.lib.pw_get_hits(self.handle, _ptr(hits) if n else None, n, None, 0),
+                   "pw_get_hits")
+            return hits, b""
+        strbuf = np.empty(max(nb, 1), dtype=np.uint8)
+        _check(self.lib, self.handle, self.lib.pw_get_hits(self.handle, _ptr(hits) if n else None, n, _ptr(strbuf),
+                                                            nb), "pw_get_hits")
         return hits, strbuf[:nb].tobytes()
 
     def starting_points(self):

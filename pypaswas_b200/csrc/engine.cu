@@ -586,6 +586,30 @@ static cudaError_t download(pw_engine* e, std::vector<HT>& v, const void* src, s
     return cudaStreamSynchronize(e->stream);
 }
 
+// The byte values present in data[0, n), in order of first occurrence
+// (chunks scanned on host threads).
+static std::vector<int> first_occurrence_order(const uint8_t* data, int64_t n) {
+    std::vector<std::vector<int64_t>> first_k;
+    std::mutex mu;
+    parallel_for(n, [&](int64_t b0, int64_t b1) {
+        std::vector<int64_t> f(256, INT64_MAX);
+        for (int64_t k = b0; k < b1; ++k)
+            if (f[data[k]] == INT64_MAX) f[data[k]] = k;
+        std::lock_guard<std::mutex> g(mu);
+        first_k.push_back(std::move(f));
+    }, (int64_t)1 << 22);
+    std::vector<std::pair<int64_t, int>> firsts;
+    for (int c = 0; c < 256; ++c) {
+        int64_t fk = INT64_MAX;
+        for (auto& v : first_k) fk = std::min(fk, v[c]);
+        if (fk != INT64_MAX) firsts.push_back({fk, c});
+    }
+    std::sort(firsts.begin(), firsts.end());
+    std::vector<int> out;
+    for (auto& fc : firsts) out.push_back(fc.second);
+    return out;
+}
+
 // Builds the device copies of the sequences, the compact query alphabet and the
 // compact substitution matrices.  Targets and queries are prepared separately
 // and cached: a target database stays resident on the device while query sets
@@ -599,9 +623,23 @@ static int prepare_targets(pw_engine* e) {
     const HostSeqs& T = e->T;
     const int off = e->char_offset, dim = e->dim;
     Prepared& pr = e->pr;
-    for (uint8_t c : T.raw)
-        if (c == 0 || (int)c < off || (int)c >= off + dim)
-            return fail(e, PW_ERR_ARG, "target residue outside the scoring matrix: code " + std::to_string(c));
+    // the byte values present, in order of first occurrence (host threads)
+    const std::vector<int> present = first_occurrence_order(T.raw.data(), (int64_t)T.raw.size());
+    {
+        // the first invalid residue of the input is reported
+        int64_t bad_at = INT64_MAX;
+        int bad = -1;
+        for (int c : present)
+            if (c == 0 || c < off || c >= off + dim) {
+                const int64_t at = (int64_t)(std::find(T.raw.begin(), T.raw.end(), (uint8_t)c) - T.raw.begin());
+                if (at < bad_at) {
+                    bad_at = at;
+                    bad = c;
+                }
+            }
+        if (bad >= 0)
+            return fail(e, PW_ERR_ARG, "target residue outside the scoring matrix: code " + std::to_string(bad));
+    }
     pr.tlen.assign(T.n, 0);
     pr.maxlt = 0;
     for (int32_t i = 0; i < T.n; ++i)
@@ -614,27 +652,33 @@ static int prepare_targets(pw_engine* e) {
         pos += align_up(std::max<int64_t>(pr.tlen[i], 1), 16);
     }
     tco[T.n] = pos;
-    std::vector<uint8_t> tc((size_t)std::max<int64_t>(pos, 16), 0);
-    for (int32_t i = 0; i < T.n; ++i)
-        for (int32_t k = 0; k < pr.tlen[i]; ++k) tc[tco[i] + k] = (uint8_t)(T.raw[T.off[i] + k] - off);
-    pr.order_t.resize(T.n);
-    std::iota(pr.order_t.begin(), pr.order_t.end(), 0);
-    std::stable_sort(pr.order_t.begin(), pr.order_t.end(),
-                     [&](int a, int b) { return pr.tlen[a] > pr.tlen[b]; });
     // the transposed orientation: targets on the lanes in a compact target
     // alphabet, with the matrix transposed to [target residue][query residue]
     int tmap[256];
     for (int i = 0; i < 256; ++i) tmap[i] = -1;
     std::vector<int> talpha;
-    for (uint8_t c : T.raw)
-        if (tmap[c] < 0) {
-            tmap[c] = (int)talpha.size();
-            talpha.push_back(c);
-        }
+    for (int c : present) {
+        tmap[c] = (int)talpha.size();
+        talpha.push_back(c);
+    }
     pr.alpha_t = (int)talpha.size();
+    std::vector<uint8_t> tc((size_t)std::max<int64_t>(pos, 16), 0);
     std::vector<uint8_t> tcc(tc.size(), (uint8_t)pr.alpha_t);
-    for (int32_t i = 0; i < T.n; ++i)
-        for (int32_t k = 0; k < pr.tlen[i]; ++k) tcc[tco[i] + k] = (uint8_t)tmap[T.raw[T.off[i] + k]];
+    parallel_for(T.n, [&](int64_t i0, int64_t i1) {
+        for (int64_t i = i0; i < i1; ++i) {
+            const uint8_t* r = T.raw.data() + T.off[i];
+            for (int32_t k = 0; k < pr.tlen[i]; ++k) {
+                tc[tco[i] + k] = (uint8_t)(r[k] - off);
+                tcc[tco[i] + k] = (uint8_t)tmap[r[k]];
+            }
+        }
+    }, (int64_t)1 << 12);
+    {
+        std::vector<uint64_t> key((size_t)T.n);
+        for (int32_t i = 0; i < T.n; ++i) key[i] = (uint64_t)(pr.maxlt - pr.tlen[i]);
+        const std::vector<uint32_t> o = radix_order(std::move(key));
+        pr.order_t.assign(o.begin(), o.end());
+    }
     std::vector<int8_t> cmt8((size_t)(pr.alpha_t + 1) * dim, (int8_t)-128);
     std::vector<float> cmtf((size_t)(pr.alpha_t + 1) * dim, -1.0e30f);
     bool t_int8 = pr.alpha_t <= 250;
@@ -679,37 +723,11 @@ static int prepare_queries(pw_engine* e) {
     int map[256];
     for (int i = 0; i < 256; ++i) map[i] = -1;
     std::vector<int> alphabet;
-    {
-        // first occurrence of every byte value, over host threads
-        const int64_t nraw = (int64_t)Q.raw.size();
-        std::vector<std::vector<int64_t>> first_k(64);
-        std::mutex mu;
-        parallel_for(nraw, [&](int64_t b0, int64_t b1) {
-            std::vector<int64_t> f(256, INT64_MAX);
-            for (int64_t k = b0; k < b1; ++k)
-                if (f[Q.raw[k]] == INT64_MAX) f[Q.raw[k]] = k;
-            std::lock_guard<std::mutex> g(mu);
-            for (auto& v : first_k)
-                if (v.empty()) {
-                    v.swap(f);
-                    break;
-                }
-        }, (int64_t)1 << 22);
-        std::vector<std::pair<int64_t, int>> firsts;
-        for (int c = 0; c < 256; ++c) {
-            int64_t fk = INT64_MAX;
-            for (auto& v : first_k)
-                if (!v.empty()) fk = std::min(fk, v[c]);
-            if (fk != INT64_MAX) firsts.push_back({fk, c});
-        }
-        std::sort(firsts.begin(), firsts.end());
-        for (auto& fc : firsts) {
-            const int c = fc.second;
-            if (c == 0 || c < off || c >= off + dim)
-                return fail(e, PW_ERR_ARG, "query residue outside the scoring matrix: code " + std::to_string(c));
-            map[c] = (int)alphabet.size();
-            alphabet.push_back(c);
-        }
+    for (int c : first_occurrence_order(Q.raw.data(), (int64_t)Q.raw.size())) {
+        if (c == 0 || c < off || c >= off + dim)
+            return fail(e, PW_ERR_ARG, "query residue outside the scoring matrix: code " + std::to_string(c));
+        map[c] = (int)alphabet.size();
+        alphabet.push_back(c);
     }
     if (alphabet.size() > 250) return fail(e, PW_ERR_ARG, "too many distinct query residues");
     pr.alpha = (int)alphabet.size();
@@ -2500,10 +2518,13 @@ extern "C" int pw_get_pair_max(pw_engine* e, float* out, int64_t n) {
 
 extern "C" int pw_get_hits(pw_engine* e, pw_hit* hits, int64_t max_hits, char* strbuf, int64_t strbuf_bytes) {
     if (!e) return PW_ERR_ARG;
-    if (max_hits < (int64_t)e->h_hits.size() || strbuf_bytes < (int64_t)e->h_strings.size())
+    if (max_hits < (int64_t)e->h_hits.size() || (strbuf && strbuf_bytes < (int64_t)e->h_strings.size()))
         return fail(e, PW_ERR_ARG, "output buffers too small");
-    if (!e->h_hits.empty()) std::memcpy(hits, e->h_hits.data(), e->h_hits.size() * sizeof(pw_hit));
-    if (!e->h_strings.empty()) std::memcpy(strbuf, e->h_strings.data(), e->h_strings.size());
+    if (!e->h_hits.empty()) {
+        if (!hits) return fail(e, PW_ERR_ARG, "no hit buffer");
+        std::memcpy(hits, e->h_hits.data(), e->h_hits.size() * sizeof(pw_hit));
+    }
+    if (strbuf && !e->h_strings.empty()) std::memcpy(strbuf, e->h_strings.data(), e->h_strings.size());
     return PW_OK;
 }
 

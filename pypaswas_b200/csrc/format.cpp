@@ -296,36 +296,42 @@ extern "C" int pw_trimmed_fasta(const pw_hit* hits, int64_t n_hits, int32_t n_qu
                                      t_orig_len, t_start_pos, thresholds, rec, order);
     if (rc != PW_OK) return rc;
     // ">" target id " " query id "\n" query[:t0] query[t1 + 1:] "\n": the
-    // query cut by the hit's TARGET coordinates, as Hit.get_trimmed_line does
-    int64_t need = 0;
-    for (int64_t i : order) {
-        const Rec& r = rec[i];
+    // query cut by the hit's TARGET coordinates, as Hit.get_trimmed_line does;
+    // record sizes, their offsets, then the records on host threads
+    const int64_t m = (int64_t)order.size();
+    std::vector<int64_t> at((size_t)m + 1, 0);
+    for (int64_t k = 0; k < m; ++k) {
+        const Rec& r = rec[order[k]];
         const int64_t L = q_seq_off[r.q + 1] - q_seq_off[r.q];
         const int64_t a = std::min(r.t0, L), b = std::min(r.t1 + 1, L);
-        need += 1 + (t_id_off[r.t + 1] - t_id_off[r.t]) + 1 + (q_id_off[r.q + 1] - q_id_off[r.q]) + 1 + a + (L - b) + 1;
+        at[k + 1] = at[k] + 1 + (t_id_off[r.t + 1] - t_id_off[r.t]) + 1 + (q_id_off[r.q + 1] - q_id_off[r.q]) + 1 +
+                    a + (L - b) + 1;
     }
+    const int64_t need = at[m];
     *out_len = need;
     if (!out) return PW_OK;
     if (out_cap < need) return PW_ERR_CAPACITY;
-    char* p = out;
-    auto put = [&](const char* s, int64_t n) {
-        if (n > 0) std::memcpy(p, s, (size_t)n);
-        p += n;
-    };
-    for (int64_t i : order) {
-        const Rec& r = rec[i];
-        const char* seq = q_seq + q_seq_off[r.q];
-        const int64_t L = q_seq_off[r.q + 1] - q_seq_off[r.q];
-        const int64_t a = std::min(r.t0, L), b = std::min(r.t1 + 1, L);
-        *p++ = '>';
-        put(t_id + t_id_off[r.t], t_id_off[r.t + 1] - t_id_off[r.t]);
-        *p++ = ' ';
-        put(q_id + q_id_off[r.q], q_id_off[r.q + 1] - q_id_off[r.q]);
-        *p++ = '\n';
-        put(seq, a);
-        put(seq + b, L - b);
-        *p++ = '\n';
-    }
+    parallel_for(m, [&](int64_t k0, int64_t k1) {
+        for (int64_t k = k0; k < k1; ++k) {
+            const Rec& r = rec[order[k]];
+            char* p = out + at[k];
+            auto put = [&](const char* s, int64_t n) {
+                if (n > 0) std::memcpy(p, s, (size_t)n);
+                p += n;
+            };
+            const char* seq = q_seq + q_seq_off[r.q];
+            const int64_t L = q_seq_off[r.q + 1] - q_seq_off[r.q];
+            const int64_t a = std::min(r.t0, L), b = std::min(r.t1 + 1, L);
+            *p++ = '>';
+            put(t_id + t_id_off[r.t], t_id_off[r.t + 1] - t_id_off[r.t]);
+            *p++ = ' ';
+            put(q_id + q_id_off[r.q], q_id_off[r.q + 1] - q_id_off[r.q]);
+            *p++ = '\n';
+            put(seq, a);
+            put(seq + b, L - b);
+            *p++ = '\n';
+        }
+    }, 1 << 15);
     return PW_OK;
 }
 

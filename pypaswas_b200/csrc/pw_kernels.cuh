@@ -644,12 +644,13 @@ struct PairView {
         // upper one does, else UL; NO where H is 0; a UL cell inside the
         // matrix with a zero diagonal neighbour carries the stop flag, one
         // reaching the pair's threshold the candidate flag
-        const int h = hval(x, y);
+        // the four loads are issued together (one memory round trip a cell)
+        const int h = hval(x, y), l = hval(x - 1, y), u = hval(x, y - 1), d = hval(x - 1, y - 1);
         if (h <= 0) return kNo;
-        if (h == hval(x - 1, y) + gap) return kLeft;
-        if (h == hval(x, y - 1) + gap) return kUp;
+        if (h == l + gap) return kLeft;
+        if (h == u + gap) return kUp;
         uint32_t cd = kUL;
-        if (x > 0 && y > 0 && hval(x - 1, y - 1) == 0) cd |= kStopFlag;
+        if (x > 0 && y > 0 && d == 0) cd |= kStopFlag;
         if (h >= thr && x < lq && y < lt) cd |= kCand;
         return cd;
     }

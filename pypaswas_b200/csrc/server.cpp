@@ -64,7 +64,7 @@ struct Worker {
 struct pw_server {
     int device = 0;
     int max_batch = 16;
-    int policy = 0;              // PW_SERVE_TUNE_POLICY
+    int policy = 1;              // PW_SERVE_TUNE_POLICY (shortest first with aging)
     double age_ms = 25.0;        // PW_SERVE_TUNE_AGE_MS
     int64_t budget = 0;          // direction-matrix bytes shared by all traceback batches
     int64_t in_use = 0;          // reserved by running batches

@@ -12,12 +12,12 @@ def _is_packed(records):
     return hasattr(records, "id_blob") and hasattr(records, "residues")
 
 
-def _one_block(program, records_seqs, targets, max_length=None):
+def _one_block(program, records_seqs, targets, max_length=None, strings=True):
     """The driver's single target block (the engine takes every target):
     the engine's hit records, their strings and the block.  Records given as
     packed sets (pypaswas_b200.readers.RecordSet) go to the engine as they are."""
     if _is_packed(records_seqs) and _is_packed(targets):
-        hits, strbuf = program.smith_waterman.align_packed(records_seqs, targets)
+        hits, strbuf = program.smith_waterman.align_packed(records_seqs, targets, strings)
         return hits, strbuf, targets
     all_targets_length = sum(len(s.seq) for s in targets)
     all_sequences_length = sum(len(s.seq) for s in records_seqs)
@@ -112,5 +112,5 @@ class Trimmer(Aligner):
             return ""
         max_length = len(targets[0]) if getattr(self.settings, "recompile", "T") == "F" and \
             not _is_packed(targets) else None
-        hits, _, block = _one_block(self, records_seqs, targets, max_length)
+        hits, _, block = _one_block(self, records_seqs, targets, max_length, strings=False)
         return trimmed_fasta(hits, records_seqs, block, self.settings)

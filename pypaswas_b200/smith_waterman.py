@@ -39,6 +39,18 @@ def id_keys(query_ids, target_ids):
     return qk, tk
 
 
+def packed_id_keys(queries, targets):
+    """id_keys of two packed record sets (pypaswas_b200.readers.RecordSet),
+    without Python strings: the dense byte-order ranks of all ids together
+    (pw_id_ranks) are equal exactly when the id bytes are, i.e. when the ids
+    are (their UTF-8 / surrogate-escape decoding is one to one)."""
+    from .formatters import _native_ranks
+    blob = np.concatenate([queries.id_blob, targets.id_blob])
+    off = np.concatenate([queries.id_offsets, targets.id_offsets[1:] + queries.id_offsets[-1]])
+    r = _native_ranks(blob, off)
+    return r[:len(queries)].astype(np.int32), r[len(queries):].astype(np.int32)
+
+
 def configure_engine(engine, score, settings):
     """Scoring model and thresholds as the reference's kernels see them.
     `score` is any scoring model with the reference Score's public attributes:
@@ -213,11 +225,12 @@ class SmithWatermanB200(object):
         self._progress(records_seqs, block, t0)
         return hits, strbuf, block
 
-    def align_packed(self, queries, targets):
+    def align_packed(self, queries, targets, strings=True):
         """One engine call on packed record sets (pypaswas_b200.readers.RecordSet):
         all queries against all targets; returns the hit records (walk order)
-        and their strings, without Python record or Hit objects."""
-        qk, tk = id_keys(queries.ids, targets.ids)
+        and their strings (b"" with strings=False), without Python record or
+        Hit objects."""
+        qk, tk = packed_id_keys(queries, targets)
         self.engine.set_queries_packed(queries.residues, queries.offsets, qk)
         self.engine.set_targets_packed(targets.residues, targets.offsets, tk)
         info = self.engine.align(start_cap=self.maximum_number_starting_points * len(queries) * len(targets))
@@ -227,7 +240,7 @@ class SmithWatermanB200(object):
                                 "higher in config.")
         self.last_h2d_bytes = int(info.h2d_bytes)
         self.last_d2h_bytes = int(info.d2h_bytes)
-        return self.engine.hits()
+        return self.engine.hits(strings)
 
     def _build_hits(self, hits, strbuf, sequences, targets, hit_list):
         """Hit objects in walk order (SmithWaterman._print_alignments :822-838).
