@@ -44,8 +44,6 @@ static double wall_ms() {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
-// Runs f(begin, end) over [0, n) split into contiguous ranges, one host
-// thread each (ranges in order: range k covers [n * k / T, n * (k + 1) / T)).
 // Host-phase timing on stderr when the environment sets PW_HOST_TRACE
 // (diagnostics of the host orchestration between kernels; off by default).
 struct HostTrace {
@@ -1690,8 +1688,10 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         if (info) *info = inf;
         return PW_OK;
     }
+    HostTrace ht0;
     int rc = prepare(e);
     if (rc != PW_OK) return rc;
+    ht0.mark("prepare (encodings, uploads)");
     const Prepared& pr = e->pr;
     const std::vector<int32_t>& qlen = pr.qlen;
     const std::vector<int32_t>& tlen = pr.tlen;
@@ -1788,6 +1788,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         float ms = 0;
         cudaEventElapsedTime(&ms, e->ev[0], e->ev[1]);
         inf.score_ms = ms;
+        ht0.mark("score phase (16-bit, wall)");
     } else {
         inf.score_path = 1;
     // items: one target against 32 consecutive queries of the length order

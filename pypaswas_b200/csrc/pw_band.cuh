@@ -13,9 +13,10 @@
 // (two rows, alternating by band parity) and publishes every 32 steps how many
 // columns are stored (st.release.gpu, by the storing thread itself); the band
 // below polls that count (ld.acquire.gpu, bounded wait) and reads the ring
-// with ld.global.cg.  A ring row is rewritten by band b + 2 only after band
-// b + 1 has published progress past those columns, which it does only after
-// its lane 0 has read them.  In the queue every band comes after the band
+// with ld.global.cg, 32 columns per coalesced warp load, one block ahead (it
+// waits for 64 columns at each 32-step block).  A ring row is rewritten by
+// band b + 2 only after band b + 1 has published progress past those columns,
+// which it does only after it has read them.  In the queue every band comes after the band
 // above it: band-major when there are many pairs, otherwise planned like the
 // chained strips (pw_plan.h) so that the bands of a few long pairs pipeline.
 //
@@ -71,7 +72,7 @@ struct BandArgs {
 };
 
 template <bool AFFINE, int DIRS>
-__global__ void __launch_bounds__(128) band_kernel(KernelArgs A, BandArgs B) {
+__global__ void __launch_bounds__(128, AFFINE ? 5 : 8) band_kernel(KernelArgs A, BandArgs B) {
     static_assert(DIRS != 2 || !AFFINE, "H store: linear gap only");
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
@@ -163,9 +164,20 @@ __global__ void __launch_bounds__(128) band_kernel(KernelArgs A, BandArgs B) {
         int mx = 0;
         int avail = 0;
         bool ok = true;
+        // the row above, 32 columns at a time: lane k holds column 32j + k of
+        // the current block (cur) and of the next one (nxt), loaded with one
+        // coalesced read a block ahead; lane 0 takes column s by a shuffle
+        // (linear gap: the H values only)
+        int4 cur = make_int4(0, 0, 0, 0), nxt = make_int4(0, 0, 0, 0);
+        auto fetch = [&](int64_t c) -> int4 {
+            if (c >= lq) return make_int4(0, 0, 0, 0);
+            if constexpr (AFFINE) return __ldcg(&ring_in[c]);
+            return make_int4(__ldcg((const int*)&ring_in[c]), 0, 0, 0);
+        };
         for (int64_t s = 0; s < nsteps; ++s) {
             if (has_up && (s & 31) == 0) {
-                const int need = (int)(s + 32 < (int64_t)lq ? s + 32 : (int64_t)lq);
+                // this block and the next one must be stored by the band above
+                const int need = (int)(s + 64 < (int64_t)lq ? s + 64 : (int64_t)lq);
                 if (avail < need) {
                     avail = chain_wait(prog_in, need, B.abort_flag, B.wait_ns);
                     if (avail < 0) {
@@ -173,10 +185,20 @@ __global__ void __launch_bounds__(128) band_kernel(KernelArgs A, BandArgs B) {
                         break;
                     }
                 }
+                cur = s == 0 ? fetch(s + lane) : nxt;
+                nxt = fetch(s + 32 + lane);
             }
             const int x = (int)s - lane;
             const bool active = x >= 0 && x < lq;
             int rh = 0, rm = 0, ri = neg, rb = 0;
+            int4 above = make_int4(0, 0, 0, 0);
+            if (has_up) {
+                above.x = __shfl_sync(0xffffffffu, cur.x, (int)(s & 31));
+                if constexpr (AFFINE) {
+                    above.y = __shfl_sync(0xffffffffu, cur.y, (int)(s & 31));
+                    above.z = __shfl_sync(0xffffffffu, cur.z, (int)(s & 31));
+                }
+            }
             if constexpr (AFFINE) {
                 rm = __shfl_up_sync(0xffffffffu, bt_m, 1);
                 ri = __shfl_up_sync(0xffffffffu, bt_i, 1);
@@ -186,7 +208,7 @@ __global__ void __launch_bounds__(128) band_kernel(KernelArgs A, BandArgs B) {
             }
             if (lane == 0) {
                 if (has_up && active) {
-                    const int4 v = __ldcg(&ring_in[x]);
+                    const int4 v = above;
                     rh = v.x;
                     rm = v.x;
                     ri = v.y;

@@ -383,60 +383,73 @@ __device__ __forceinline__ void sweep_hstore(const LaneCtx& c, const void* prof,
                                              Bnd<int>* bnd, uint8_t* hs, int lane, int thr, Cand* cand,
                                              int cand_cap, int& n_cand) {
     uint4* out = (uint4*)hs;
+    const int16_t* hv = (const int16_t*)hs;
     int H[S];
 #pragma unroll
     for (int r = 0; r < S; ++r) H[r] = 0;
     int hb_prev = 0;
-    for (int x4 = 0; x4 < c.lq4; x4 += 4) {
-        const uint32_t cw = *(const uint32_t*)(c.qc + x4);
+    uint32_t cw = 0;
+    // one column per iteration (a compact loop body: the fully unrolled
+    // four-column form stalled on instruction fetch)
+#pragma unroll 1
+    for (int x = 0; x < c.lq4; ++x) {
+        if ((x & 3) == 0) cw = *(const uint32_t*)(c.qc + x);
+        const int a = (cw >> (8 * (x & 3))) & 0xff;
+        const int up0 = c.has_up ? bnd[(int64_t)x * kWarp].m : 0;
+        int up = up0;
+        int diag = hb_prev;
+        hb_prev = up0;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int x = x4 + j;
-            const int a = (cw >> (8 * j)) & 0xff;
-            int up = c.has_up ? bnd[(int64_t)x * kWarp].m : 0;
-            int diag = hb_prev;
-            hb_prev = up;
+        for (int g = 0; g < S / 4; ++g) {
+            const Prof4<int> p = load_prof<int>(prof, g, alpha1, a);
 #pragma unroll
-            for (int g = 0; g < S / 4; ++g) {
-                const Prof4<int> p = load_prof<int>(prof, g, alpha1, a);
+            for (int k = 0; k < 4; ++k) {
+                const int r = 4 * g + k;
+                const int left = H[r];
+                int h = addmax(left, gap, diag + p.s[k]);
+                h = relu_addmax(up, gap, h);
+                diag = left;
+                H[r] = h;
+                up = h;
+            }
+        }
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const int r = 4 * g + k;
-                    const int left = H[r];
-                    int h = addmax(left, gap, diag + p.s[k]);
-                    h = relu_addmax(up, gap, h);
-                    if (h >= thr) {
-                        // a candidate is a UL cell (neither gap source
-                        // reaches h, in either orientation) inside the matrix
-                        const bool ul = h > 0 && h != left + gap && h != up + gap;
-                        const int y = c.y0 + r;
-                        if (ul && x < c.lq && y < c.lt) {
-                            if (n_cand < cand_cap) {
-                                Cand cc;
-                                cc.x = TRANS ? y : x;
-                                cc.y = TRANS ? x : y;
-                                cc.score_i = h;
-                                cc.score_f = (float)h;
-                                cand[n_cand] = cc;
-                            }
-                            ++n_cand;
-                        }
-                    }
-                    diag = left;
-                    H[r] = h;
-                    up = h;
+        for (int q = 0; q < S / 16; ++q) {
+            uint32_t w[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) w[k] = __byte_perm(H[16 * q + 2 * k], H[16 * q + 2 * k + 1], 0x5410);
+            uint4* o = out + (((int64_t)x * (S / 16) + q) * kWarp + lane) * 2;
+            o[0] = make_uint4(w[0], w[1], w[2], w[3]);
+            o[1] = make_uint4(w[4], w[5], w[6], w[7]);
+        }
+        if (c.has_down) bnd[(int64_t)x * kWarp].m = H[S - 1];
+        // candidates (rare: cells reaching the pair's threshold): a UL cell,
+        // i.e. neither gap source reaches h (in either orientation), inside
+        // the matrix; the left neighbours come back from the column stored
+        // one iteration earlier by this thread
+        int cm = 0;
+#pragma unroll
+        for (int r = 0; r < S; r += 2) cm = max3(cm, H[r], H[r + 1]);
+        if (cm >= thr) {
+#pragma unroll
+            for (int r = 0; r < S; ++r) {  // unrolled: H stays in registers
+                const int h = H[r];
+                const int y = c.y0 + r;
+                if (h < thr || h <= 0 || x >= c.lq || y >= c.lt) continue;
+                const int left = x > 0 ? (int)hv[(((int64_t)(x - 1) * (S / 16) + r / 16) * kWarp + lane) * 16 + r % 16]
+                                       : 0;
+                const int upv = r > 0 ? H[r - 1] : up0;
+                if (h == left + gap || h == upv + gap) continue;
+                if (n_cand < cand_cap) {
+                    Cand cc;
+                    cc.x = TRANS ? y : x;
+                    cc.y = TRANS ? x : y;
+                    cc.score_i = h;
+                    cc.score_f = (float)h;
+                    cand[n_cand] = cc;
                 }
+                ++n_cand;
             }
-#pragma unroll
-            for (int q = 0; q < S / 16; ++q) {
-                uint32_t w[8];
-#pragma unroll
-                for (int k = 0; k < 8; ++k) w[k] = __byte_perm(H[16 * q + 2 * k], H[16 * q + 2 * k + 1], 0x5410);
-                uint4* o = out + (((int64_t)x * (S / 16) + q) * kWarp + lane) * 2;
-                o[0] = make_uint4(w[0], w[1], w[2], w[3]);
-                o[1] = make_uint4(w[4], w[5], w[6], w[7]);
-            }
-            if (c.has_down) bnd[(int64_t)x * kWarp].m = H[S - 1];
         }
     }
 }

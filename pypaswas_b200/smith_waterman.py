@@ -188,20 +188,23 @@ class SmithWatermanB200(object):
 
     def _align_into(self, records_seqs, block, hitlist, n_pairs, t0):
         """One engine call on the uploaded records; its Hits into hitlist.
-        last_timing holds the call's host wall time in three parts (ms):
-        records to the engine, the engine call, hits to Hit objects."""
+        last_timing holds the call's host wall time in parts (ms): records to
+        the engine, the engine call with the copy of its hit records (and of
+        that, pw_align alone, and pw_align's own clock), hits to Hit objects."""
         t1 = time.time()
         info = self.engine.align(start_cap=self.maximum_number_starting_points * n_pairs)
         self.last_info = info
         if info.truncated:
             self.logger.warning("Too many hits returned. Skipping the rest. Please set lower_limit_score "
                                 "higher in config.")
+        t_align = time.time()
         hits, strbuf = self.engine.hits()
         t2 = time.time()
         self.last_h2d_bytes = int(info.h2d_bytes)  # counted by the engine, copy by copy
         self.last_d2h_bytes = int(info.d2h_bytes)
         self._build_hits(hits, strbuf, records_seqs, block, hitlist)
         self.last_timing = {"records_ms": (t1 - t0) * 1e3, "engine_ms": (t2 - t1) * 1e3,
+                            "engine_call_ms": (t_align - t1) * 1e3, "engine_info_total_ms": float(info.total_ms),
                             "hits_ms": (time.time() - t2) * 1e3}
 
     def align_records(self, records_seqs, targets, target_index):
