@@ -388,12 +388,16 @@ __device__ __forceinline__ void sweep_hstore(const LaneCtx& c, const void* prof,
 #pragma unroll
     for (int r = 0; r < S; ++r) H[r] = 0;
     int hb_prev = 0;
-    uint32_t cw = 0;
+    // the code word of the next four columns is loaded four columns ahead
+    uint32_t cw = 0, cw_next = c.lq4 > 0 ? *(const uint32_t*)c.qc : 0u;
     // one column per iteration (a compact loop body: the fully unrolled
     // four-column form stalled on instruction fetch)
 #pragma unroll 1
     for (int x = 0; x < c.lq4; ++x) {
-        if ((x & 3) == 0) cw = *(const uint32_t*)(c.qc + x);
+        if ((x & 3) == 0) {
+            cw = cw_next;
+            if (x + 4 < c.lq4) cw_next = *(const uint32_t*)(c.qc + x + 4);
+        }
         const int a = (cw >> (8 * (x & 3))) & 0xff;
         const int up0 = c.has_up ? bnd[(int64_t)x * kWarp].m : 0;
         int up = up0;
@@ -667,6 +671,18 @@ struct PairView {
         if (h >= thr && x < lq && y < lt) cd |= kCand;
         return cd;
     }
+    // Starts fetching cell (x, y)'s code (or H values) and mark into L2: the
+    // walks follow one path a dependent load at a time, mostly along the
+    // diagonal, so the cells a few steps ahead are requested early.  A hint
+    // only: cells outside the matrix are skipped.
+    __device__ __forceinline__ void prefetch(int x, int y) const {
+        if (x < 1 || y < 1) return;
+        const int64_t i = index(x, y);
+        const uint8_t* c = hstore ? base + 2 * i : base + (i >> 1);
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(c));
+        if (hstore) asm volatile("prefetch.global.L2 [%0];" ::"l"(base + 2 * index(x - 1, y)));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(marks + ((cell0 + i) >> 3)));
+    }
     __device__ __forceinline__ bool marked(int x, int y) const {
         const int64_t i = cell0 + index(x, y);
         return (marks[i >> 3] >> (i & 7)) & 1u;
@@ -680,6 +696,9 @@ struct PairView {
         marks[i >> 3] &= (uint8_t)~(1u << (i & 7));
     }
 };
+
+// Diagonal steps a path walk requests ahead (PairView::prefetch).
+constexpr int kWalkAhead = 8;
 
 __device__ __forceinline__ PairView pair_view(const TraceArgs& A, const PairMeta& pm) {
     PairView v;
@@ -723,6 +742,7 @@ __global__ void collect_kernel(TraceArgs A) {
     for (int k = 0; k < n; ++k) {
         int x = cl[k].x - 1, y = cl[k].y - 1;
         while (x >= 0 && y >= 0) {
+            v.prefetch(x - kWalkAhead, y - kWalkAhead);
             const uint32_t cd = v.code(x, y);
             const int d = cd & 3;
             if (cd & kCand) {
@@ -837,6 +857,7 @@ __global__ void walk_kernel(TraceArgs A) {
         // after a gap move), so the run is scanned only when that is unknown.
         int run_next = -1;
         while (show && x >= 0 && y >= 0 && dir != kStopDir && dir != 32) {  // :761
+            v.prefetch(x - kWalkAhead, y - kWalkAhead);
             const uint32_t cd = v.code(x, y);
             const int d = cd & 3;
             int run_here = (cd & kCand) ? 1 : (d != kUL ? 0 : run_next);
@@ -914,6 +935,7 @@ __global__ void ops_kernel(TraceArgs A, const DevHit* hits, int n_hits) {
     int x = H.end_x, y = H.end_y;
     char* o = A.ops + H.ops_offset;
     for (int k = 0; k < H.n_cols; ++k) {
+        v.prefetch(x - kWalkAhead, y - kWalkAhead);
         const int d = v.code(x, y) & 3;
         char op;
         if (d == kLeft) {

@@ -547,7 +547,7 @@ __device__ __forceinline__ void build_item_profile(void* prof, const Score16Args
 }
 
 template <int S, bool AFFINE, bool DL>
-__global__ void __launch_bounds__(128, 4) score16_chain_kernel(Score16Args A) {
+__global__ void __launch_bounds__(128, 3) score16_chain_kernel(Score16Args A) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
