@@ -227,9 +227,11 @@ int pw_set_wave_limit(pw_engine* e, int64_t bytes);
  *                       recomputed on 32-bit lanes either way) */
 #define PW_TUNE_LANES 7
 /*   PW_TUNE_TRACE_STORE direction sweeps of linear integer scoring: 0 the
- *                       engine's choice (16-bit H per cell when every traced
- *                       maximum is below 2^15, cell codes derived on read),
- *                       1 always 4-bit cell codes */
+ *                       engine's choice (16-bit H per cell, cell codes derived
+ *                       on read, when every traced maximum is below 2^15 and
+ *                       the strip sweep holds most traced cells), 1 always
+ *                       4-bit cell codes, 2 the H store wherever the maxima
+ *                       allow it (the band sweep's long pairs included) */
 #define PW_TUNE_TRACE_STORE 8
 int pw_set_tuning(pw_engine* e, int key, int64_t value);
 

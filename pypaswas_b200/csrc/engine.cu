@@ -1977,8 +1977,9 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     // memory waves.
     int64_t warp_cells = 0;
     for (const auto& wp : warp_pairs) warp_cells += (int64_t)qlen[wp.first] * tlen[wp.second];
-    const bool hstore = pr.int_path && !e->affine && max_pass < 32767 && e->tune[PW_TUNE_TRACE_STORE] != 1 &&
-                        inf.traced_cells - warp_cells >= warp_cells;
+    const int64_t store_mode = e->tune[PW_TUNE_TRACE_STORE];
+    const bool hstore = pr.int_path && !e->affine && max_pass < 32767 && store_mode != 1 &&
+                        (store_mode == 2 || inf.traced_cells - warp_cells >= warp_cells);
     inf.trace_store = hstore ? 1 : 0;
     const int per_item = plain ? 1 : kWarp;
     double cost_t = 0, cost_q = 0;

@@ -234,14 +234,44 @@ __global__ void __launch_bounds__(128, AFFINE ? 5 : 8) band_kernel(KernelArgs A,
                 uint32_t w0 = 0;  // the lane's 8 rows as 4-bit codes
                 if constexpr (!AFFINE) {
                     int up = up_h, diag = dg_h;
+                    int Hold[kWarpRows];  // the left neighbours (previous column), for the candidate test
+#pragma unroll
+                    for (int r = 0; r < kWarpRows; ++r) Hold[r] = Hl[r];
+                    // the stop flag needs a cell inside the matrix: x > 0 and y > 0
+                    const bool stop_ok0 = xin && ypos, stop_ok = xin;
 #pragma unroll
                     for (int r = 0; r < kWarpRows; ++r) {
                         const int sc = (int)(int8_t)(uint8_t)((r < 4 ? pw.x : pw.y) >> (8 * (r & 3)));
                         const int left = Hl[r];
                         int h = addmax(left, gap, diag + sc);
                         h = addmax_relu(up, gap, h);
-                        if constexpr (DIRS == 2) {
-                            if (h >= thr && r < rows_left && h > 0 && h != left + gap && h != up + gap) {
+                        if constexpr (DIRS == 1) {
+                            // the reference's classification (LEFT > UP > UL, NO at
+                            // 0), shifted into the row's nibble; the stop flag on a
+                            // UL cell inside the matrix whose diagonal is 0
+                            const uint32_t sh = 4 * r;
+                            uint32_t code = h == left + gap ? (kLeft << sh) : (h == up + gap ? (kUp << sh) : (kUL << sh));
+                            const bool stop = (r > 0 ? stop_ok : stop_ok0) && diag == 0 && code == (kUL << sh);
+                            code = stop ? code | (kStopFlag << sh) : code;
+                            w0 |= h > 0 ? code : 0u;
+                        } else if constexpr (DIRS == 0) {
+                            mx = max(mx, h);
+                        }
+                        diag = left;
+                        Hl[r] = h;
+                        up = h;
+                    }
+                    if constexpr (DIRS != 0) {
+                        // candidates: UL cells inside the matrix at or above the
+                        // threshold -- rare, so one test of the step's maximum
+                        const int smax = max(max3(Hl[0], Hl[1], Hl[2]), max3(Hl[3], Hl[4], max3(Hl[5], Hl[6], Hl[7])));
+                        if (smax >= thr) {
+#pragma unroll
+                            for (int r = 0; r < kWarpRows; ++r) {
+                                const int h = Hl[r], upv = r > 0 ? Hl[r - 1] : up_h;
+                                if (h < thr || h <= 0 || r >= rows_left || h == Hold[r] + gap || h == upv + gap)
+                                    continue;
+                                if constexpr (DIRS == 1) w0 |= kCand << (4 * r);
                                 const int k = atomicAdd(ncand, 1);
                                 if (k < cap) {
                                     Cand cc;
@@ -252,34 +282,7 @@ __global__ void __launch_bounds__(128, AFFINE ? 5 : 8) band_kernel(KernelArgs A,
                                     cand[k] = cc;
                                 }
                             }
-                        } else if constexpr (DIRS == 1) {
-                            const int ls = left + gap, us = up + gap;
-                            uint32_t code = h == ls ? kLeft : (h == us ? kUp : kUL);
-                            code = h > 0 ? code : kNo;
-                            const bool ul = code == kUL;
-                            // y = ymine + r > 0 unless r == 0 and the lane's first row is row 0
-                            const bool stop = ul && xin && (r > 0 || ypos) && diag == 0;
-                            code |= stop ? kStopFlag : 0u;
-                            if (ul && h >= thr && r < rows_left) {
-                                const int y = ymine + r;
-                                code |= kCand;
-                                const int k = atomicAdd(ncand, 1);
-                                if (k < cap) {
-                                    Cand cc;
-                                    cc.x = x;
-                                    cc.y = y;
-                                    cc.score_i = h;
-                                    cc.score_f = (float)h;
-                                    cand[k] = cc;
-                                }
-                            }
-                            w0 |= code << (4 * r);
-                        } else {
-                            mx = max(mx, h);
                         }
-                        diag = left;
-                        Hl[r] = h;
-                        up = h;
                     }
                     bt_h = up;
                     if constexpr (DIRS == 2) {

@@ -83,6 +83,13 @@ def test_band_sweep_forms_agree(engine_lib, oracle_mod):
     st = cases.Settings(minimum_score="20", lower_limit_score="0.9")
     score = cases.scores.make_score(st)
     _both_forms(engine_lib, oracle_mod, queries, targets, score, st, 0)
+    # the H store forced on the band sweep (PW_TUNE_TRACE_STORE = 2)
+    o = _oracle(oracle_mod, queries, targets, score, st)
+    pm, hits, info, _ = run_engine(engine_lib, queries, targets, score, st,
+                                   tuning={_native.PW_TUNE_TRACE_STORE: 2})
+    assert info.trace_store == 1 and info.warp_pairs == info.traced_pairs
+    np.testing.assert_array_equal(pm, o["pair_max"])
+    assert hits == o["hits"]
     # 600 reads against 10 short adapters (strip sweep, > 32 traced pairs per
     # SM) and one target of two bands (band sweep, fewer cells), all pairs
     # traced
