@@ -242,6 +242,7 @@ struct pw_engine {
     HostBuf<int64_t> h_sel;
     HostBuf<int32_t> h_ptq, h_p2order;  // phase-2 pair lists (kept across calls: no page faults, no zero fill)
     HostBuf<uint8_t> h_qc, h_qres;      // query encodings staged for upload (page-locked, kept across calls)
+    HostBuf<uint8_t> h_stage;           // page-locked staging of the other per-set uploads (Staged)
     int64_t free_mem = 0;    // free device memory plus this engine's kept wave buffers, as last queried
     double free_mem_t = -1;  // wall_ms() of that query
     DevBuf chain_items, chain_info, chain_prog, chain_max, chain_ring_off, chain_ring, chain_abort, p1_items, p1_grid;
@@ -584,6 +585,39 @@ static cudaError_t download(pw_engine* e, std::vector<HT>& v, const void* src, s
     return cudaStreamSynchronize(e->stream);
 }
 
+// The uploads of one sequence set, gathered into the engine's page-locked
+// staging buffer and copied asynchronously (a pageable source makes every
+// cudaMemcpyAsync a synchronous staged copy of its own); the caller
+// synchronises the stream before the staging buffer is reused.
+struct Staged {
+    struct Item {
+        DevBuf* dst;
+        const void* src;
+        size_t bytes;
+    };
+    std::vector<Item> items;
+    template <typename V>
+    void add(DevBuf& b, const V& v) {
+        items.push_back({&b, v.data(), v.size() * sizeof(v[0])});
+    }
+    cudaError_t run(pw_engine* e) {
+        size_t total = 0;
+        for (const Item& it : items) total += (it.bytes + 15) & ~(size_t)15;
+        if (!e->h_stage.resize(std::max<size_t>(total, 16))) return cudaErrorMemoryAllocation;
+        size_t off = 0;
+        for (const Item& it : items) {
+            cudaError_t c = it.dst->reserve(e->stream, std::max<size_t>(it.bytes, 16));
+            if (c != cudaSuccess) return c;
+            if (it.bytes) {
+                std::memcpy(e->h_stage.data() + off, it.src, it.bytes);
+                if ((c = copy_h2d(e, it.dst->p, e->h_stage.data() + off, it.bytes)) != cudaSuccess) return c;
+            }
+            off += (it.bytes + 15) & ~(size_t)15;
+        }
+        return cudaSuccess;
+    }
+};
+
 // The byte values present in data[0, n), in order of first occurrence
 // (chunks scanned on host threads).
 static std::vector<int> first_occurrence_order(const uint8_t* data, int64_t n) {
@@ -689,20 +723,19 @@ static int prepare_targets(pw_engine* e) {
         }
     pr.t_int8 = t_int8;
     cudaError_t c;
-#define UP(buf, vec)                                      \
-    if ((c = upload(e, buf, vec)) != cudaSuccess) return cuda_fail(e, c, "upload " #buf);
-    UP(e->t_codes, tc);
-    UP(e->t_code_off, tco);
-    UP(e->t_raw, T.raw);
-    UP(e->t_raw_off, T.off);
-    UP(e->t_len, pr.tlen);
-    UP(e->t_key, T.key);
-    UP(e->t_ccodes, tcc);
-    UP(e->t_order, pr.order_t);
-    UP(e->cmat_t8, cmt8);
-    UP(e->cmat_tf, cmtf);
-#undef UP
-    if ((c = cudaStreamSynchronize(e->stream)) != cudaSuccess) return cuda_fail(e, c, "upload targets");
+    Staged st;
+    st.add(e->t_codes, tc);
+    st.add(e->t_code_off, tco);
+    st.add(e->t_raw, T.raw);
+    st.add(e->t_raw_off, T.off);
+    st.add(e->t_len, pr.tlen);
+    st.add(e->t_key, T.key);
+    st.add(e->t_ccodes, tcc);
+    st.add(e->t_order, pr.order_t);
+    st.add(e->cmat_t8, cmt8);
+    st.add(e->cmat_tf, cmtf);
+    if ((c = st.run(e)) != cudaSuccess || (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
+        return cuda_fail(e, c, "upload targets");
     e->prep_t[0] = e->t_gen;
     e->prep_t[1] = e->s_gen;
     return PW_OK;
@@ -795,20 +828,20 @@ static int prepare_queries(pw_engine* e) {
         pr.order.assign(o.begin(), o.end());
     }
     cudaError_t c;
-#define UP(buf, vec)                                      \
-    if ((c = upload(e, buf, vec)) != cudaSuccess) return cuda_fail(e, c, "upload " #buf);
-    UP(e->q_codes, qc);
-    UP(e->q_code_off, qco);
-    UP(e->q_raw, Q.raw);
-    UP(e->q_raw_off, Q.off);
-    UP(e->q_len, pr.qlen);
-    UP(e->q_key, Q.key);
-    UP(e->q_order, pr.order);
-    UP(e->cmat_i8, cm8);
-    UP(e->cmat_f, cmf);
-    UP(e->q_res, qres);
-#undef UP
-    if ((c = cudaStreamSynchronize(e->stream)) != cudaSuccess) return cuda_fail(e, c, "upload queries");
+    // the encodings are page-locked already; the rest goes through the staging buffer
+    if ((c = upload(e, e->q_codes, qc)) != cudaSuccess || (c = upload(e, e->q_res, qres)) != cudaSuccess)
+        return cuda_fail(e, c, "upload query encodings");
+    Staged st;
+    st.add(e->q_code_off, qco);
+    st.add(e->q_raw, Q.raw);
+    st.add(e->q_raw_off, Q.off);
+    st.add(e->q_len, pr.qlen);
+    st.add(e->q_key, Q.key);
+    st.add(e->q_order, pr.order);
+    st.add(e->cmat_i8, cm8);
+    st.add(e->cmat_f, cmf);
+    if ((c = st.run(e)) != cudaSuccess || (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
+        return cuda_fail(e, c, "upload queries");
     e->prep_q[0] = e->q_gen;
     e->prep_q[1] = e->s_gen;
     return PW_OK;

@@ -308,19 +308,6 @@ __global__ void __launch_bounds__(128, AFFINE ? 5 : 8) band_kernel(KernelArgs A,
                             const bool main_src = code == kUL;
                             const bool stop = main_src && xin && (r > 0 || ypos) && mdiag == 0;
                             code |= stop ? kStopFlag : 0u;
-                            if (main_src && m >= thr && r < rows_left) {
-                                const int y = ymine + r;
-                                code |= kCand;
-                                const int k = atomicAdd(ncand, 1);
-                                if (k < cap) {
-                                    Cand cc;
-                                    cc.x = x;
-                                    cc.y = y;
-                                    cc.score_i = m;
-                                    cc.score_f = (float)m;
-                                    cand[k] = cc;
-                                }
-                            }
                             w0 |= code << (4 * r);
                         } else {
                             mx = max(mx, b);
@@ -336,6 +323,29 @@ __global__ void __launch_bounds__(128, AFFINE ? 5 : 8) band_kernel(KernelArgs A,
                     bt_m = mup;
                     bt_i = iup;
                     bt_b = Bl[kWarpRows - 1];
+                    if constexpr (DIRS != 0) {
+                        // candidates: MAIN-source cells (b == m > 0) inside the
+                        // matrix with m at or above the threshold -- rare, so one
+                        // test of the step's maximum of m
+                        const int smax = max(max3(Ml[0], Ml[1], Ml[2]), max3(Ml[3], Ml[4], max3(Ml[5], Ml[6], Ml[7])));
+                        if (smax >= thr) {
+#pragma unroll
+                            for (int r = 0; r < kWarpRows; ++r) {
+                                const int m = Ml[r];
+                                if (m < thr || Bl[r] != m || m <= 0 || r >= rows_left) continue;
+                                w0 |= kCand << (4 * r);
+                                const int k = atomicAdd(ncand, 1);
+                                if (k < cap) {
+                                    Cand cc;
+                                    cc.x = x;
+                                    cc.y = ymine + r;
+                                    cc.score_i = m;
+                                    cc.score_f = (float)m;
+                                    cand[k] = cc;
+                                }
+                            }
+                        }
+                    }
                 }
                 if constexpr (DIRS == 1)
                     *(uint32_t*)(codes + ((band * nsteps + s) * kWarp + lane) * kWarpRows / 2) = w0;
