@@ -618,27 +618,24 @@ struct Staged {
     }
 };
 
-// The byte values present in data[0, n), in order of first occurrence
-// (chunks scanned on host threads).
-static std::vector<int> first_occurrence_order(const uint8_t* data, int64_t n) {
-    std::vector<std::vector<int64_t>> first_k;
+// The byte values present in data[0, n), ascending (chunks marked on host
+// threads, without branches).  The compact alphabets number them in this
+// order; any numbering gives the same scores.
+static std::vector<int> present_bytes(const uint8_t* data, int64_t n) {
+    std::vector<std::vector<uint8_t>> marks;
     std::mutex mu;
     parallel_for(n, [&](int64_t b0, int64_t b1) {
-        std::vector<int64_t> f(256, INT64_MAX);
-        for (int64_t k = b0; k < b1; ++k)
-            if (f[data[k]] == INT64_MAX) f[data[k]] = k;
+        std::vector<uint8_t> m(256, 0);
+        for (int64_t k = b0; k < b1; ++k) m[data[k]] = 1;
         std::lock_guard<std::mutex> g(mu);
-        first_k.push_back(std::move(f));
-    }, (int64_t)1 << 22);
-    std::vector<std::pair<int64_t, int>> firsts;
-    for (int c = 0; c < 256; ++c) {
-        int64_t fk = INT64_MAX;
-        for (auto& v : first_k) fk = std::min(fk, v[c]);
-        if (fk != INT64_MAX) firsts.push_back({fk, c});
-    }
-    std::sort(firsts.begin(), firsts.end());
+        marks.push_back(std::move(m));
+    }, (int64_t)1 << 20);
     std::vector<int> out;
-    for (auto& fc : firsts) out.push_back(fc.second);
+    for (int c = 0; c < 256; ++c) {
+        bool any = false;
+        for (auto& m : marks) any = any || m[c];
+        if (any) out.push_back(c);
+    }
     return out;
 }
 
@@ -655,8 +652,8 @@ static int prepare_targets(pw_engine* e) {
     const HostSeqs& T = e->T;
     const int off = e->char_offset, dim = e->dim;
     Prepared& pr = e->pr;
-    // the byte values present, in order of first occurrence (host threads)
-    const std::vector<int> present = first_occurrence_order(T.raw.data(), (int64_t)T.raw.size());
+    // the byte values present (host threads)
+    const std::vector<int> present = present_bytes(T.raw.data(), (int64_t)T.raw.size());
     {
         // the first invalid residue of the input is reported
         int64_t bad_at = INT64_MAX;
@@ -704,7 +701,7 @@ static int prepare_targets(pw_engine* e) {
                 tcc[tco[i] + k] = (uint8_t)tmap[r[k]];
             }
         }
-    }, (int64_t)1 << 12);
+    }, (int64_t)64);
     {
         std::vector<uint64_t> key((size_t)T.n);
         for (int32_t i = 0; i < T.n; ++i) key[i] = (uint64_t)(pr.maxlt - pr.tlen[i]);
@@ -749,14 +746,28 @@ static int prepare_queries(pw_engine* e) {
     const HostSeqs& Q = e->Q;
     const int off = e->char_offset, dim = e->dim;
     Prepared& pr = e->pr;
-    // residues must index the matrix (default_main.cu:234 reads matrix[c - offset]);
-    // the compact alphabet numbers the residues in order of first occurrence
+    // residues must index the matrix (default_main.cu:234 reads matrix[c - offset];
+    // the first invalid one of the input is reported); the compact alphabet
+    // numbers the residues present in byte order
     int map[256];
     for (int i = 0; i < 256; ++i) map[i] = -1;
     std::vector<int> alphabet;
-    for (int c : first_occurrence_order(Q.raw.data(), (int64_t)Q.raw.size())) {
-        if (c == 0 || c < off || c >= off + dim)
-            return fail(e, PW_ERR_ARG, "query residue outside the scoring matrix: code " + std::to_string(c));
+    const std::vector<int> present = present_bytes(Q.raw.data(), (int64_t)Q.raw.size());
+    {
+        int64_t bad_at = INT64_MAX;
+        int bad = -1;
+        for (int c : present)
+            if (c == 0 || c < off || c >= off + dim) {
+                const int64_t at = (int64_t)(std::find(Q.raw.begin(), Q.raw.end(), (uint8_t)c) - Q.raw.begin());
+                if (at < bad_at) {
+                    bad_at = at;
+                    bad = c;
+                }
+            }
+        if (bad >= 0)
+            return fail(e, PW_ERR_ARG, "query residue outside the scoring matrix: code " + std::to_string(bad));
+    }
+    for (int c : present) {
         map[c] = (int)alphabet.size();
         alphabet.push_back(c);
     }
@@ -1085,7 +1096,8 @@ static int setup_chains(pw_engine* e, const std::vector<WorkItem>& items, int i0
 template <int S, bool AFF, bool DL>
 static cudaError_t launch_s16_chain(pw_engine* e, Score16Args A) {
     auto kern = score16_chain_kernel<S, AFF, DL>;
-    const int smem = 4 * (S / 4) * A.alpha1 * prof_entry_bytes<DL>();
+    // the four warps' profiles, then (affine) their prefetch rings of the row above
+    const int smem = chain_profile_bytes<S, DL>(A.alpha1) + (AFF ? 4 * kPre * kWarp * (int)sizeof(uint4) : 0);
     if (smem > 48 * 1024) {
         cudaError_t c = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (c != cudaSuccess) return c;
@@ -1243,7 +1255,9 @@ static int phase1_s16(pw_engine* e, const KernelArgs& A32, pw_run_info& inf, uin
         P1.n_chain_items = 0;
         if (P1.chained) {
             int per_sm = 0;
-            const int smem = 4 * 8 * ((trans ? pr.alpha_t : pr.alpha) + 1) * (dual ? 8 : 16);
+            const int a1 = (trans ? pr.alpha_t : pr.alpha) + 1;
+            const int smem = (dual ? chain_profile_bytes<32, true>(a1) : chain_profile_bytes<32, false>(a1)) +
+                             (e->affine ? 4 * kPre * kWarp * (int)sizeof(uint4) : 0);
             auto kern = e->affine ? (dual ? score16_chain_kernel<32, true, true> : score16_chain_kernel<32, true, false>)
                                   : (dual ? score16_chain_kernel<32, false, true> : score16_chain_kernel<32, false, false>);
             if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);

@@ -137,6 +137,12 @@ __device__ __forceinline__ void fetch16(const void* prof, int ia, int ib, uint32
 template <bool DL>
 __host__ __device__ constexpr int prof_entry_bytes() { return DL ? (int)sizeof(uint2) : (int)sizeof(uint4); }
 
+// Bytes of the four warps' profiles of a 128-thread block, rounded to 16.
+template <int S, bool DL>
+__host__ __device__ constexpr int chain_profile_bytes(int alpha1) {
+    return (4 * (S / 4) * alpha1 * prof_entry_bytes<DL>() + 15) & ~15;
+}
+
 // This warp's profile in shared memory (typed offsets keep the address a
 // 32-bit shared-window computation).
 template <int S, bool DL>
@@ -308,6 +314,22 @@ constexpr int kChainLead = 64;
 constexpr int kChainNeed = 40;
 // Default bound of one wait (PW_TUNE_WAIT_NS overrides it per launch).
 constexpr unsigned long long kChainWaitNs = 2000000000ull;
+// Columns of the ring row above that the affine chained sweep keeps in
+// flight: each lane copies its own 16-byte entry into a per-warp shared-memory
+// ring with cp.async, kPre - 1 columns ahead of the column it computes (within
+// the kChainNeed columns the chain wait guarantees).
+constexpr int kPre = 8;
+static_assert(kPre - 1 < kChainNeed - 4, "prefetched columns must be published");
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
 __device__ __forceinline__ int ld_acquire_gpu(const int* p) {
     int v;
@@ -361,7 +383,7 @@ __device__ __forceinline__ bool sweep16_chain(const uint8_t* qc, int lq4, const 
                                               uint32_t pad4, const void* prof, int alpha1, int gap, int ext, int ge,
                                               bool has_up, bool has_down, const uint4* ring_in, uint4* ring_out,
                                               const int* prog_in, int* prog_out, int* abort_flag,
-                                              unsigned long long wait_ns, uint32_t& mx) {
+                                              unsigned long long wait_ns, uint4* pre, uint32_t& mx) {
     const uint32_t g2 = pack16(gap), e2 = pack16(ext), ge2 = pack16(ge), nge2 = pack16(-ge);
     int avail = 0;  // columns of the predecessor known to be published
     auto need_cols = [&](int upto) -> bool {  // columns [0, upto) of ring_in readable
@@ -428,10 +450,20 @@ __device__ __forceinline__ bool sweep16_chain(const uint8_t* qc, int lq4, const 
         uint32_t bb_prev = 0;
         uint32_t cw_next = xm4 > 0 ? code_word(0) : pad4;
         uint32_t cw2_next = DL && xm4 > 0 ? code_word2(0) : pad4;
-        uint4 v_next = has_up && xm4 > 0 ? __ldcg(&ring_in[0]) : make_uint4(ge2, kNeg16x2, 0u, 0u);
-        uint4 v_next2 = has_up && xm4 > 1 ? __ldcg(&ring_in[kWarp]) : make_uint4(ge2, kNeg16x2, 0u, 0u);
+        // this lane's entries of the ring row above: slot k % kPre holds column k
+        uint4* my = pre + (threadIdx.x & 31);
+        if (has_up) {
+#pragma unroll
+            for (int k = 0; k < kPre - 1; ++k) {
+                if (k < xm4) cp_async16(&my[k * kWarp], &ring_in[(int64_t)k * kWarp]);
+                cp_async_commit();
+            }
+        }
         for (int x4 = 0; x4 < xm4; x4 += 4) {
-            if (!need_cols(min(x4 + kChainNeed, xm4))) return false;
+            if (!need_cols(min(x4 + kChainNeed, xm4))) {
+                cp_async_wait<0>();  // no copy outlives the sweep
+                return false;
+            }
             const uint32_t cw = cw_next, cw2 = cw2_next;
             if (x4 + 4 < xm4) {
                 cw_next = code_word(x4 + 4);
@@ -442,9 +474,14 @@ __device__ __forceinline__ bool sweep16_chain(const uint8_t* qc, int lq4, const 
                 const int x = x4 + j;
                 const int a = (cw >> (8 * j)) & 0xff;
                 const int a2 = DL ? (cw2 >> (8 * j)) & 0xff : 0;
-                const uint4 v = v_next;
-                v_next = v_next2;
-                if (has_up && x + 2 < xm4) v_next2 = __ldcg(&ring_in[(int64_t)(x + 2) * kWarp]);
+                uint4 v = make_uint4(ge2, kNeg16x2, 0u, 0u);
+                if (has_up) {
+                    const int xn = x + kPre - 1;  // its slot held column x - 1, already read
+                    if (xn < xm4) cp_async16(&my[(xn % kPre) * kWarp], &ring_in[(int64_t)xn * kWarp]);
+                    cp_async_commit();
+                    cp_async_wait<kPre - 1>();  // column x's copy has landed
+                    v = my[(x % kPre) * kWarp];
+                }
                 uint32_t mgup = v.x, yup = v.y, bup = v.z;
                 uint32_t bdiag = bb_prev;
                 bb_prev = bup;
@@ -472,6 +509,7 @@ __device__ __forceinline__ bool sweep16_chain(const uint8_t* qc, int lq4, const 
             }
             if (has_down && (((x4 + 4) % kChainPublish) == 0 || x4 + 4 >= xm4)) chain_publish(prog_out, x4 + 4);
         }
+        cp_async_wait<0>();
     }
     return true;
 }
@@ -552,6 +590,8 @@ __global__ void __launch_bounds__(128, 3) score16_chain_kernel(Score16Args A) {
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     void* prof = warp_profile<S, DL>(smem, wib, A.alpha1);
+    // after the four warps' profiles: each warp's prefetch ring (affine)
+    uint4* pre = (uint4*)(smem + chain_profile_bytes<S, DL>(A.alpha1)) + wib * kPre * kWarp;
     const int shift = AFFINE ? A.ge : 0;
     const uint32_t pad4 = (uint32_t)A.pad_code * 0x01010101u;
     const int64_t warp_global = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
@@ -596,7 +636,7 @@ __global__ void __launch_bounds__(128, 3) score16_chain_kernel(Score16Args A) {
             if (!sweep16_chain<S, AFFINE, DL>(L.qc, L.lq4, L.qc2, L.lq42, xm4, pad4, prof, A.alpha1, A.gap, A.ext,
                                               A.ge, s > 0, has_down, ring_in, ring_out,
                                               s > 0 ? A.progress + pred : nullptr, A.progress + it, A.abort_flag,
-                                              A.wait_ns, mx))
+                                              A.wait_ns, pre, mx))
                 break;
             if (s > 0) {
                 // the predecessor's running maximum is final once it has finished
