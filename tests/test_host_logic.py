@@ -103,11 +103,11 @@ def test_autotune_keeps_the_fastest_candidate():
 
     class Info(object):
         def __init__(self, ms, path):
-            self.score_kernel_ms = ms
+            self.total_ms = ms
             self.score_path = path
 
     class FakeEngine(object):
-        """Score-sweep time as a function of lane width, 16x2 form and chaining."""
+        """Score-phase time (plan and sweep) as a function of lane width, 16x2 form and chaining."""
         chain_cost = {250: 9.0, 500: 7.5, 1000: 8.0, 2000: 7.5}
 
         def __init__(self):
@@ -116,8 +116,8 @@ def test_autotune_keeps_the_fastest_candidate():
         def set_tuning(self, key, value):
             self.tune[key] = value
 
-        def align(self, score_only=False):
-            assert score_only
+        def align(self, score_only=False, replan=False):
+            assert score_only and replan
             if self.tune.get(_native.PW_TUNE_LANES, 0) == 32:
                 return Info(20.0, 1)
             t = self.chain_cost[self.tune.get(_native.PW_TUNE_CHAIN_MIN, 500)]
@@ -130,7 +130,7 @@ def test_autotune_keeps_the_fastest_candidate():
     assert r["dual"] == "strip pairs" and e.tune[_native.PW_TUNE_DUAL] == 2
     assert r["chain_min"] == 500  # ties go to the smaller value
     assert e.tune[_native.PW_TUNE_CHAIN_MIN] == 500
-    assert r["score_kernel_ms"] == {k: v - 0.25 for k, v in FakeEngine.chain_cost.items()}
+    assert r["score_phase_ms"] == {k: v - 0.25 for k, v in FakeEngine.chain_cost.items()}
 
 
 def test_fast_hit_building_matches_hitlist_append_and_checked_path():
