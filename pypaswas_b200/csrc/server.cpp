@@ -9,7 +9,8 @@
 // Structure: W worker threads, each owning one engine (its own CUDA stream and
 // device buffers) with the database loaded once.  A free worker takes the
 // requests that are waiting -- those that arrived while the other workers' batches
-// were on the GPU -- up to `max_batch` of one mode, and runs them as one batch;
+// were on the GPU -- up to `max_batch` of either mode, and runs them as one batch
+// (the full path when one of them wants its hits);
 // batches of different workers overlap on the device.  Traceback requests are
 // admitted by direction-matrix memory: each reserves an estimate of its cell-code
 // bytes from a shared budget (query length x database residues x the traced
@@ -94,10 +95,14 @@ int server_fail(pw_server* s, int code, const std::string& msg) {
     return code;
 }
 
-// Takes the next batch: the oldest waiting request decides the mode; requests
-// of that mode follow in arrival order up to max_batch; traceback requests
-// only while their reservations fit the free budget (the first one alone may
-// take the whole budget when nothing else is reserved).  Called with s->mu held.
+// Takes the next batch: requests in queue order (arrival order, or shortest
+// first under policy 1) up to max_batch, of either mode.  A batch with a
+// traceback request runs the full path for all its queries (a top-k request
+// reads its row of pair maxima either way), so every request of such a batch
+// reserves its direction-memory estimate from the shared budget; a request
+// joins only while the reservations fit the free budget (the first one alone
+// may take the whole budget when nothing else is reserved).  Called with
+// s->mu held.
 std::vector<Request*> take_batch(pw_server* s, int64_t* reserve) {
     std::vector<Request*> batch;
     *reserve = 0;
@@ -105,7 +110,7 @@ std::vector<Request*> take_batch(pw_server* s, int64_t* reserve) {
     if (s->policy == 1) {
         // shortest first, requests past the age limit first of all (oldest
         // first among them): the pending queue is reordered that way, and
-        // the batch is then taken from its front as in arrival order
+        // the batch is then taken from its front
         const double now = now_ms();
         std::vector<Request*> v(s->pending.begin(), s->pending.end());
         std::stable_sort(v.begin(), v.end(), [&](const Request* a, const Request* b) {
@@ -116,38 +121,40 @@ std::vector<Request*> take_batch(pw_server* s, int64_t* reserve) {
         });
         s->pending.assign(v.begin(), v.end());
     }
-    int mode = s->pending.front()->mode;
-    if (mode == PW_SERVE_TRACEBACK) {
-        Request* r = s->pending.front();
-        const int64_t need = std::min(r->est_bytes, s->budget);
-        if (s->in_use + need > s->budget && s->in_use > 0) {
-            // no room for the oldest traceback request: serve score-only work
-            // meanwhile if there is any
-            mode = PW_SERVE_TOP;
-        }
-    }
-    int64_t free_b = s->budget - s->in_use;
+    const int64_t free_b = s->budget - s->in_use;
+    bool traceback = false;
+    int64_t need_all = 0;  // reservations of every request taken so far
     for (auto it = s->pending.begin(); it != s->pending.end() && (int)batch.size() < s->max_batch;) {
         Request* r = *it;
-        if (r->mode != mode) {
-            ++it;
-            continue;
+        const int64_t need = std::min(r->est_bytes, s->budget);
+        const bool tb = traceback || r->mode == PW_SERVE_TRACEBACK;
+        if (tb) {
+            // the batch would run the full path: all its requests reserve
+            const int64_t total = need_all + need;
+            const bool alone = batch.empty() && s->in_use == 0;
+            if (!alone && total > free_b) {
+                if (r->mode == PW_SERVE_TRACEBACK && !traceback) {
+                    ++it;  // no room for it now: score-only requests may still go
+                    continue;
+                }
+                break;
+            }
+            traceback = true;
         }
-        if (mode == PW_SERVE_TRACEBACK) {
-            const int64_t need = std::min(r->est_bytes, s->budget);
-            if (!batch.empty() && *reserve + need > free_b) break;
-            *reserve += need;
-        }
+        need_all += need;
         batch.push_back(r);
         it = s->pending.erase(it);
     }
-    if (mode == PW_SERVE_TRACEBACK) *reserve = std::max<int64_t>(std::min(*reserve, s->budget), 1);
+    *reserve = traceback ? std::max<int64_t>(std::min(need_all, s->budget), 1) : 0;
     return batch;
 }
 
 void run_batch(pw_server* s, int w, pw_engine* e, std::vector<Request*>& batch, int64_t reserve) {
     const int n = (int)batch.size();
-    const int mode = batch[0]->mode;
+    // the full path when any request wants its hits, else score only
+    int mode = PW_SERVE_TOP;
+    for (const Request* r : batch)
+        if (r->mode == PW_SERVE_TRACEBACK) mode = PW_SERVE_TRACEBACK;
     std::vector<int64_t> off(n + 1, 0);
     for (int i = 0; i < n; ++i) off[i + 1] = off[i] + (int64_t)batch[i]->residues.size();
     std::vector<uint8_t> res((size_t)std::max<int64_t>(off[n], 1));
@@ -163,7 +170,9 @@ void run_batch(pw_server* s, int w, pw_engine* e, std::vector<Request*>& batch, 
     std::vector<float> pmax;
     std::vector<pw_hit> hits;
     std::vector<char> strings;
-    if (rc == PW_OK && mode == PW_SERVE_TOP) {
+    bool any_top = false;
+    for (const Request* r : batch) any_top = any_top || r->mode == PW_SERVE_TOP;
+    if (rc == PW_OK && any_top) {
         pmax.resize((size_t)n * s->db_n);
         rc = pw_get_pair_max(e, pmax.data(), (int64_t)pmax.size());
     }
@@ -174,9 +183,10 @@ void run_batch(pw_server* s, int w, pw_engine* e, std::vector<Request*>& batch, 
     }
     const std::string msg = rc == PW_OK ? std::string() : std::string(pw_last_error(e));
     // top hits of the score-only requests: one host thread per request
-    if (rc == PW_OK && mode == PW_SERVE_TOP) {
+    if (rc == PW_OK && any_top) {
         auto top = [&](int i) {
             Request* r = batch[i];
+            if (r->mode != PW_SERVE_TOP) return;
             const float* row = pmax.data() + (size_t)i * s->db_n;
             std::vector<int32_t> idx(s->db_n);
             for (int32_t t = 0; t < s->db_n; ++t) idx[t] = t;
@@ -209,7 +219,7 @@ void run_batch(pw_server* s, int w, pw_engine* e, std::vector<Request*>& batch, 
         r->setup_ms = info.setup_ms;
         r->call_ms = info.total_ms;
         if (rc != PW_OK) continue;
-        if (mode == PW_SERVE_TOP) {
+        if (r->mode == PW_SERVE_TOP) {
             // filled above
         } else {
             for (const pw_hit& h : hits) {
@@ -225,7 +235,7 @@ void run_batch(pw_server* s, int w, pw_engine* e, std::vector<Request*>& batch, 
     }
     const double t = now_ms();
     std::lock_guard<std::mutex> g(s->mu);
-    if (mode == PW_SERVE_TRACEBACK) {
+    if (reserve > 0) {
         s->in_use -= reserve;
         if (rc == PW_OK && info.cells > 0) {
             const double f = (double)info.traced_cells / (double)info.cells;
@@ -260,7 +270,7 @@ void worker_loop(pw_server* s, int w) {
             }
             const double t = now_ms();
             for (Request* r : batch) r->t_admit = t;
-            if (batch[0]->mode == PW_SERVE_TRACEBACK) {
+            if (reserve > 0) {
                 s->in_use += reserve;
                 s->peak_in_use = std::max(s->peak_in_use, s->in_use);
             }
