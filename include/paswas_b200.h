@@ -173,6 +173,15 @@ int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_info* info)
  * pw_get_pair_max then holds -1 for the pairs that are not listed. */
 int pw_set_pairs(pw_engine* e, const int32_t* query_idx, const int32_t* target_idx, int64_t n);
 
+/* Queries whose hits are wanted: mask[q] != 0 traces query q's pairs as
+ * usual; a 0 leaves its pairs at their maxima (pw_get_pair_max) and gives
+ * them no starting points or hits, as if no cell reached the threshold.  n is
+ * the number of queries of the last pw_set_queries, or 0 for no mask (every
+ * query traced).  pw_set_queries clears the mask.  No counterpart in the
+ * reference: the serving loop batches score-only and traceback requests in
+ * one pw_align with it. */
+int pw_set_query_trace(pw_engine* e, const uint8_t* mask, int32_t n);
+
 /* Upper bound, in bytes, on the direction-matrix memory of one memory wave of
  * pw_align (4-bit cell codes -- direction, stop flag, candidate flag -- and a
  * 1-bit mark plane: half a byte plus one bit per traced cell); 0 restores the automatic choice (55% of the free

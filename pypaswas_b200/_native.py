@@ -62,7 +62,7 @@ EXPORTED_SYMBOLS = (
     "pw_server_release", "pw_server_stats", "pw_server_tune", "pw_trimmed_fasta", "pw_txt_records",
     "pw_sam_records",
     "pw_records_parse", "pw_records_read", "pw_records_sizes", "pw_records_copy", "pw_records_free",
-    "pw_id_ranks",
+    "pw_id_ranks", "pw_set_query_trace",
 )
 
 
@@ -178,6 +178,7 @@ def bind(lib):
         "pw_records_copy": (ctypes.c_int, [P, P, P, P, P]),
         "pw_records_free": (None, [P]),
         "pw_id_ranks": (ctypes.c_int, [P, P, I64, P]),
+        "pw_set_query_trace": (ctypes.c_int, [P, P, I32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -357,6 +358,14 @@ class Engine(object):
 
     def set_tuning(self, key, value):
         _check(self.lib, self.handle, self.lib.pw_set_tuning(self.handle, int(key), int(value)), "pw_set_tuning")
+
+    def set_query_trace(self, mask):
+        """Per query: traced (nonzero) or maxima only (0); None clears the mask."""
+        if mask is None:
+            _check(self.lib, self.handle, self.lib.pw_set_query_trace(self.handle, None, 0), "pw_set_query_trace")
+            return
+        m = np.ascontiguousarray(np.asarray(mask) != 0, dtype=np.uint8)
+        _check(self.lib, self.handle, self.lib.pw_set_query_trace(self.handle, _ptr(m), len(m)), "pw_set_query_trace")
 
     def set_wave_limit(self, nbytes):
         _check(self.lib, self.handle, self.lib.pw_set_wave_limit(self.handle, int(nbytes)), "pw_set_wave_limit")

@@ -269,6 +269,8 @@ struct pw_engine {
     int64_t prep_q[2] = {0, 0}, prep_t[2] = {0, 0};  // (sequence gen, scoring gen) last prepared
     int64_t wave_limit = 0;                          // cell-code bytes per memory wave (0: automatic)
     std::vector<int32_t> pair_q, pair_t;             // pw_set_pairs: explicit (query, target) pairs
+    bool q_trace_set = false;                        // pw_set_query_trace: a mask is on the device
+    DevBuf q_trace;                                  // per query: 1 traced, 0 maxima only
     int64_t tune[16] = {};                           // pw_set_tuning values (0: automatic)
     // results
     HostBuf<float> h_pair_max;
@@ -434,6 +436,7 @@ static int set_seqs(pw_engine* e, HostSeqs& S, const uint8_t* residues, const in
 
 extern "C" int pw_set_queries(pw_engine* e, const uint8_t* residues, const int64_t* offsets, int32_t n,
                               const int32_t* id_keys) {
+    if (e) e->q_trace_set = false;  // a trace mask belongs to one pw_set_queries
     return set_seqs(e, e->Q, residues, offsets, n, id_keys);
 }
 
@@ -1945,8 +1948,9 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((npairs + 255) / 256, (int64_t)e->sm_count * 16));
         PW_LAUNCH(prune_kernel, grid, 256, 0, e->stream, (const float*)A.pair_max, e->q_order.as<int32_t>(),
                   e->q_len.as<int32_t>(), e->t_len.as<int32_t>(), nq, nt, e->minimum_score, e->highest,
-                  e->filter_factor, e->lower_limit, e->prune_flags.as<uint8_t>(),
-                  e->prune_cnt.as<unsigned long long>());
+                  e->filter_factor, e->lower_limit,
+                  e->q_trace_set ? (const uint8_t*)e->q_trace.as<uint8_t>() : (const uint8_t*)nullptr,
+                  e->prune_flags.as<uint8_t>(), e->prune_cnt.as<unsigned long long>());
         e->launches++;
         if ((c = cudaGetLastError()) != cudaSuccess ||
             (c = copy_d2h(e, cnt, e->prune_cnt.p, sizeof(cnt))) != cudaSuccess ||
@@ -2527,6 +2531,23 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     inf.d2h_bytes = e->d2h;
     inf.reuse = e->reuse;
     if (info) *info = inf;
+    return PW_OK;
+}
+
+extern "C" int pw_set_query_trace(pw_engine* e, const uint8_t* mask, int32_t n) {
+    if (!e) return PW_ERR_ARG;
+    if (n == 0) {
+        e->q_trace_set = false;
+        return PW_OK;
+    }
+    if (!mask || n != e->Q.n) return fail(e, PW_ERR_ARG, "the trace mask needs one byte per query");
+    if (cudaSetDevice(e->device) != cudaSuccess) return fail(e, PW_ERR_DEVICE, "cudaSetDevice failed");
+    cudaError_t c;
+    if ((c = e->q_trace.reserve(e->stream, (size_t)std::max(n, 16))) != cudaSuccess ||
+        (c = copy_h2d(e, e->q_trace.p, mask, (size_t)n)) != cudaSuccess ||
+        (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
+        return cuda_fail(e, c, "upload trace mask");
+    e->q_trace_set = true;
     return PW_OK;
 }
 

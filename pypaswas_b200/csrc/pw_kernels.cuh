@@ -1087,7 +1087,7 @@ __global__ void cand_overflow_kernel(const int32_t* n_cand, const int32_t* cand_
 // reaching MINIMUM_SCORE, counts[1] += passing pairs.
 __global__ void prune_kernel(const float* pair_max, const int32_t* q_order, const int32_t* q_len,
                              const int32_t* t_len, int nq, int nt, float minimum, double highest,
-                             double filter_factor, float lower_limit, uint8_t* flags,
+                             double filter_factor, float lower_limit, const uint8_t* q_trace, uint8_t* flags,
                              unsigned long long* counts) {
     const int64_t n = (int64_t)nq * nt;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -1105,7 +1105,8 @@ __global__ void prune_kernel(const float* pair_max, const int32_t* q_order, cons
                 const int mn = min(q_len[q], t_len[t]);
                 const float pos = (float)(highest * (double)mn * filter_factor);
                 const float llm = __fmul_rn(lower_limit, mx);
-                pass = mx >= fmaxf(llm, pos);
+                // q_trace (null: every query): queries whose hits are wanted
+                pass = mx >= fmaxf(llm, pos) && (q_trace == nullptr || q_trace[q] != 0);
                 if (pass) pass_max = max(pass_max, __float2uint_rz(fminf(fmaxf(mx, 0.0f), 4.0e9f)));
             }
             flags[k] = pass ? 1 : 0;

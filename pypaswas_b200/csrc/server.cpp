@@ -97,12 +97,13 @@ int server_fail(pw_server* s, int code, const std::string& msg) {
 
 // Takes the next batch: requests in queue order (arrival order, or shortest
 // first under policy 1) up to max_batch, of either mode.  A batch with a
-// traceback request runs the full path for all its queries (a top-k request
-// reads its row of pair maxima either way), so every request of such a batch
-// reserves its direction-memory estimate from the shared budget; a request
-// joins only while the reservations fit the free budget (the first one alone
-// may take the whole budget when nothing else is reserved).  Called with
-// s->mu held.
+// traceback request runs the full path with a trace mask that leaves the
+// top-k requests' pairs at their maxima (pw_set_query_trace), so only
+// traceback requests reserve their direction-memory estimate from the shared
+// budget; one joins only while the reservations fit the free budget (the
+// first one alone may take the whole budget when nothing else is reserved),
+// and one that does not fit leaves the batch to the requests behind it.
+// Called with s->mu held.
 std::vector<Request*> take_batch(pw_server* s, int64_t* reserve) {
     std::vector<Request*> batch;
     *reserve = 0;
@@ -123,29 +124,22 @@ std::vector<Request*> take_batch(pw_server* s, int64_t* reserve) {
     }
     const int64_t free_b = s->budget - s->in_use;
     bool traceback = false;
-    int64_t need_all = 0;  // reservations of every request taken so far
     for (auto it = s->pending.begin(); it != s->pending.end() && (int)batch.size() < s->max_batch;) {
         Request* r = *it;
-        const int64_t need = std::min(r->est_bytes, s->budget);
-        const bool tb = traceback || r->mode == PW_SERVE_TRACEBACK;
-        if (tb) {
-            // the batch would run the full path: all its requests reserve
-            const int64_t total = need_all + need;
-            const bool alone = batch.empty() && s->in_use == 0;
-            if (!alone && total > free_b) {
-                if (r->mode == PW_SERVE_TRACEBACK && !traceback) {
-                    ++it;  // no room for it now: score-only requests may still go
-                    continue;
-                }
-                break;
+        if (r->mode == PW_SERVE_TRACEBACK) {
+            const int64_t need = std::min(r->est_bytes, s->budget);
+            const bool alone = *reserve == 0 && s->in_use == 0;
+            if (!alone && *reserve + need > free_b) {
+                ++it;  // no room for it now
+                continue;
             }
+            *reserve += need;
             traceback = true;
         }
-        need_all += need;
         batch.push_back(r);
         it = s->pending.erase(it);
     }
-    *reserve = traceback ? std::max<int64_t>(std::min(need_all, s->budget), 1) : 0;
+    *reserve = traceback ? std::max<int64_t>(std::min(*reserve, s->budget), 1) : 0;
     return batch;
 }
 
@@ -165,7 +159,17 @@ void run_batch(pw_server* s, int w, pw_engine* e, std::vector<Request*>& batch, 
     pw_run_info info;
     std::memset(&info, 0, sizeof(info));
     int rc = pw_set_queries(e, res.data(), off.data(), n, keys.data());
-    if (rc == PW_OK && mode == PW_SERVE_TRACEBACK) rc = pw_set_wave_limit(e, reserve);
+    if (rc == PW_OK && mode == PW_SERVE_TRACEBACK) {
+        // only the traceback requests' pairs are traced
+        std::vector<uint8_t> mask(n);
+        bool all = true;
+        for (int i = 0; i < n; ++i) {
+            mask[i] = batch[i]->mode == PW_SERVE_TRACEBACK ? 1 : 0;
+            all = all && mask[i];
+        }
+        if (!all) rc = pw_set_query_trace(e, mask.data(), n);
+        if (rc == PW_OK) rc = pw_set_wave_limit(e, reserve);
+    }
     if (rc == PW_OK) rc = pw_align(e, mode == PW_SERVE_TOP ? PW_FLAG_SCORE_ONLY : 0u, -1, &info);
     std::vector<float> pmax;
     std::vector<pw_hit> hits;

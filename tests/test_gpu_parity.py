@@ -312,3 +312,29 @@ def test_pair_list_long_pairs_bands_chained(engine_lib, oracle_mod, affine):
         by_pair.setdefault((h["query"], h["target"]), []).append(h)
     assert {k: v for k, v in by_pair.items()} == {k: v for k, v in ref_hits.items() if v}
     assert sum(len(v) for v in ref_hits.values()) >= 4
+
+
+@pytest.mark.parametrize("seed", range(3))
+def test_query_trace_mask_keeps_the_traced_queries_hits(engine_lib, oracle_mod, seed):
+    """pw_set_query_trace: masked-out queries keep their pair maxima and give
+    no hits; the others give exactly their hits of the unmasked run, in the
+    same order.  pw_set_queries clears the mask."""
+    from engine_helpers import configure, decode_hits
+    from pypaswas_b200 import _native
+    queries, targets, score, st = cases.make_case(500 + seed, ["dna", "protein", "dna"][seed])
+    o = _oracle(oracle_mod, queries, targets, score, st)
+    mask = np.arange(len(queries)) % 2 == 0
+    e = _native.Engine(0, lib=engine_lib)
+    try:
+        configure(e, score, st)
+        e.set_queries([q.encode() for q in queries], np.arange(len(queries)))
+        e.set_targets([t.encode() for t in targets], np.arange(len(targets)) + len(queries))
+        e.set_query_trace(mask)
+        e.align()
+        np.testing.assert_array_equal(e.pair_max(), o["pair_max"])
+        assert decode_hits(*e.hits()) == [h for h in o["hits"] if mask[h["query"]]]
+        e.set_queries([q.encode() for q in queries], np.arange(len(queries)))
+        e.align()
+        assert decode_hits(*e.hits()) == o["hits"]
+    finally:
+        e.close()
