@@ -131,9 +131,10 @@ def _native_ranks(blob, offsets):
     return out
 
 
-# first output buffer at most this large (np.empty commits no pages until they
-# are written); a longer text takes the exact-size retry
-_ESTIMATE_CAP = 8 << 30
+# first output buffer at most this large; a longer text takes the exact-size
+# retry (the estimate is per hit, so it is near the real size unless the score
+# filter drops most hits)
+_ESTIMATE_CAP = 1 << 30
 
 
 def _per_hit_estimate(hits, q_id_off, t_id_off, body):
@@ -159,8 +160,13 @@ def _call_twice(fn, head, tail, estimate):
     import numpy as np
     from . import _native
     n = ctypes.c_int64()
-    out = np.empty(max(int(estimate), 1), dtype=np.uint8)
-    rc = fn(*head, *tail, out.ctypes.data_as(ctypes.c_void_p), len(out), ctypes.byref(n))
+    try:
+        out = np.empty(max(int(estimate), 1), dtype=np.uint8)
+        rc = fn(*head, *tail, out.ctypes.data_as(ctypes.c_void_p), len(out), ctypes.byref(n))
+    except MemoryError:
+        # no room for the estimate: a size pass (null buffer), then the exact size
+        rc = fn(*head, *tail, None, 0, ctypes.byref(n))
+        rc = _native.PW_ERR_CAPACITY if rc == _native.PW_OK else rc
     if rc == _native.PW_ERR_CAPACITY:
         out = np.empty(max(n.value, 1), dtype=np.uint8)
         rc = fn(*head, *tail, out.ctypes.data_as(ctypes.c_void_p), len(out), ctypes.byref(n))

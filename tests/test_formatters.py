@@ -188,6 +188,34 @@ def test_native_formatter_retries_with_the_exact_size(engine_lib, monkeypatch):
     assert formatters.txt_records(hits, strbuf, seqs, tgts, st, lib=engine_lib)
 
 
+def test_native_formatter_sizes_first_when_the_estimate_cannot_be_allocated(engine_lib, monkeypatch):
+    """An estimate the host cannot allocate turns into a size pass (null
+    buffer) and one call at the exact size."""
+    import cases
+    import numpy as np
+    from pypaswas_b200 import formatters
+    hits, strbuf, seqs, tgts = _synthetic_trimmer_hits(9, n=50)
+    st = cases.Settings(relative_score="0", query_identity="0", query_coverage="0", base_score="0")
+    full = formatters.trimmed_fasta(hits, seqs, tgts, st, lib=engine_lib)
+    real_empty, real_call, sizes = np.empty, formatters._call_twice, []
+
+    def empty(n, dtype=None):
+        sizes.append(n)
+        if len(sizes) == 1:
+            raise MemoryError("planted")
+        return real_empty(n, dtype=dtype)
+
+    def call(*a):  # the plant covers the formatter call alone
+        monkeypatch.setattr(np, "empty", empty)
+        try:
+            return real_call(*a)
+        finally:
+            monkeypatch.setattr(np, "empty", real_empty)
+    monkeypatch.setattr(formatters, "_call_twice", call)
+    assert formatters.trimmed_fasta(hits, seqs, tgts, st, lib=engine_lib) == full
+    assert len(sizes) == 2 and sizes[1] == len(full.encode())
+
+
 def test_native_formatter_id_ranks_follow_python_order():
     """The id ranks given to the native formatters order ids as Python's
     sorted() does: mixed case, digits, non-ASCII, prefixes, whitespace, and
