@@ -212,6 +212,12 @@ def _check(lib, handle, rc, what):
     raise CudaException(msg)
 
 
+# a new bytes object of n bytes, its contents not yet written
+_new_bytes = ctypes.pythonapi.PyBytes_FromStringAndSize
+_new_bytes.restype = ctypes.py_object
+_new_bytes.argtypes = (ctypes.c_void_p, ctypes.c_ssize_t)
+
+
 def _ptr(a):
     return ctypes.c_void_p(a.ctypes.data) if a is not None and a.size else ctypes.c_void_p(0)
 
@@ -324,10 +330,17 @@ class Engine(object):
             _check(self.lib, self.handle, self.lib.pw_get_hits(self.handle, _ptr(hits) if n else None, n, None, 0),
                    "pw_get_hits")
             return hits, b""
-        strbuf = np.empty(max(nb, 1), dtype=np.uint8)
-        _check(self.lib, self.handle, self.lib.pw_get_hits(self.handle, _ptr(hits) if n else None, n, _ptr(strbuf),
+        if nb < 2:
+            strbuf = np.empty(max(nb, 1), dtype=np.uint8)
+            _check(self.lib, self.handle, self.lib.pw_get_hits(self.handle, _ptr(hits) if n else None, n,
+                                                                _ptr(strbuf), nb), "pw_get_hits")
+            return hits, strbuf[:nb].tobytes()
+        # the strings go straight into a new, unshared bytes object (one copy)
+        text = _new_bytes(None, nb)
+        _check(self.lib, self.handle, self.lib.pw_get_hits(self.handle, _ptr(hits) if n else None, n,
+                                                            ctypes.cast(ctypes.c_char_p(text), ctypes.c_void_p),
                                                             nb), "pw_get_hits")
-        return hits, strbuf[:nb].tobytes()
+        return hits, text
 
     def starting_points(self):
         n = ctypes.c_int64()

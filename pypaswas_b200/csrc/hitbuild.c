@@ -49,6 +49,7 @@ static const char* kKeyNames[K_COUNT] = {
 static PyObject* kKeys[K_COUNT];
 static PyObject* kStrDistance;
 static PyObject* kStrKeys;
+static PyObject* kEmpty; /* () */
 
 static int get_i64(Py_buffer* b, Py_ssize_t n, const char* what) {
     if (b->len != n * (Py_ssize_t)sizeof(int64_t)) {
@@ -72,6 +73,19 @@ static PyObject* pair_of(int64_t a, int64_t b) {
     PyTuple_SET_ITEM(t, 0, x);
     PyTuple_SET_ITEM(t, 1, y);
     return t;
+}
+
+/* A tuple of exact str / int / float items cannot be part of a reference
+ * cycle; the cyclic collector untracks such tuples on its first pass over
+ * them.  Untracking them here, when they are made, spares that pass over the
+ * four tuples of every hit. */
+static void untrack_atoms(PyObject* t) {
+    const Py_ssize_t n = PyTuple_GET_SIZE(t);
+    for (Py_ssize_t i = 0; i < n; ++i) {
+        PyObject* x = PyTuple_GET_ITEM(t, i);
+        if (!(PyUnicode_CheckExact(x) || PyLong_CheckExact(x) || PyFloat_CheckExact(x))) return;
+    }
+    if (PyObject_GC_IsTracked(t)) PyObject_GC_UnTrack(t);
 }
 
 /* HitList.append's replacement rule for a new hit h with score sc and keys
@@ -239,8 +253,10 @@ static PyObject* build(PyObject* self, PyObject* args) {
             for (int i = 0; i < K_COUNT; ++i)
                 if (!v[i]) ok = 0;
             if (ok) {
-                /* attributes in Hit.__init__'s order (the class's shared key order) */
-                h = ((PyTypeObject*)hit_type)->tp_alloc((PyTypeObject*)hit_type, 0);
+                /* the class's __new__ (object_new) readies the instance's
+                   inline attribute values; the attributes follow in
+                   Hit.__init__'s order (the class's shared key order) */
+                h = ((PyTypeObject*)hit_type)->tp_new((PyTypeObject*)hit_type, kEmpty, NULL);
                 ok = h != NULL;
                 for (int i = 0; ok && i < K_COUNT; ++i) ok = PyObject_GenericSetAttr(h, kKeys[i], v[i]) == 0;
             }
@@ -254,6 +270,10 @@ static PyObject* build(PyObject* self, PyObject* args) {
                 b1 = PyTuple_GET_ITEM(v[K_TGT_LOC], 1);
                 k0 = PyTuple_Pack(4, qid, tid, a0, b0);
                 k1 = PyTuple_Pack(4, qid, tid, a1, b1);
+                untrack_atoms(v[K_SEQ_LOC]);
+                untrack_atoms(v[K_TGT_LOC]);
+                if (k0) untrack_atoms(k0);
+                if (k1) untrack_atoms(k1);
                 ok = k0 && k1 && hitlist_append(hits_d, real_d, h, v[K_SCORE], k0, k1) == 0;
             }
             Py_XDECREF(k0);
@@ -288,6 +308,8 @@ PyMODINIT_FUNC PyInit__hitbuild(void) {
     }
     kStrDistance = PyUnicode_InternFromString("distance");
     kStrKeys = PyUnicode_InternFromString("keys");
+    kEmpty = PyTuple_New(0);
+    if (!kEmpty) return NULL;
     if (!kStrDistance || !kStrKeys) return NULL;
     return PyModule_Create(&kModule);
 }
