@@ -95,7 +95,7 @@ typedef struct {
     int64_t h2d_bytes;      /* bytes this call copied host -> device (sequences, encodings, work lists) */
     int64_t d2h_bytes;      /* bytes this call copied device -> host (maxima, pair lists, starts, hits) */
     int32_t trace_store;    /* direction sweeps stored 1: each cell's 16-bit H, 0: 4-bit cell codes */
-    int32_t pad0;
+    int32_t tile_pairs;     /* traced long pairs in the tile form (checkpoints, tiles recomputed on the walk) */
 } pw_run_info;
 
 #define PW_REUSE_QUERIES 1
@@ -242,6 +242,13 @@ int pw_set_wave_limit(pw_engine* e, int64_t bytes);
  *                       4-bit cell codes, 2 the H store wherever the maxima
  *                       allow it (the band sweep's long pairs included) */
 #define PW_TUNE_TRACE_STORE 8
+/*   PW_TUNE_TILE_TRACE  long pairs (the band sweep) of linear integer scoring:
+ *                       0 the engine's choice (the tile form: a checkpoint
+ *                       sweep, then 256 x 128-cell tiles of codes recomputed
+ *                       where the walks need them), 1 the direction sweep's
+ *                       stored cell codes (or H, PW_TUNE_TRACE_STORE), 2 the
+ *                       tile form */
+#define PW_TUNE_TILE_TRACE 9
 int pw_set_tuning(pw_engine* e, int key, int64_t value);
 
 /* Pair maxima (the last block of the maxima chain, default_main.cu:591),

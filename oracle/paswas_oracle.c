@@ -331,6 +331,22 @@ static void traceback_pair(const orc_params* p, pair_mats* P, float pos, uint32_
     }
 }
 
+/* emission order alone (the order of the reference's starting-point buffer) */
+static int emit_cmp(const void* a, const void* b) {
+    const start_key* x = (const start_key*)a;
+    const start_key* y = (const start_key*)b;
+#define CMPF(f) if (x->f != y->f) return x->f < y->f ? -1 : 1
+    CMPF(neg_diag);
+    CMPF(neg_bx);
+    CMPF(target);
+    CMPF(query);
+    CMPF(neg_i);
+    CMPF(ty);
+    CMPF(src);
+#undef CMPF
+    return 0;
+}
+
 static int key_cmp(const void* a, const void* b) {
     const start_key* x = (const start_key*)a;
     const start_key* y = (const start_key*)b;
@@ -428,9 +444,15 @@ int orc_run(const orc_params* p, int nq, const uint8_t* q_res, const int64_t* q_
     *n_starts = sink.n;
     for (int64_t s = 0; s < sink.n && s < max_starts; ++s) starts_out[s] = sink.starts[s];
     if (sink.n > max_starts) rc = -1;
-    qsort(sink.keys, sink.n, sizeof(start_key), key_cmp);
+    /* the host reads the first start_cap starting points of the device
+     * buffer (emission order) when there are at least that many
+     * (SmithWaterman.py:683-687), then sorts those by score (:699) */
     int64_t walk_n = sink.n;
-    if (start_cap >= 0 && walk_n >= start_cap) walk_n = start_cap; /* :683-685 */
+    if (start_cap >= 0 && walk_n >= start_cap) {
+        qsort(sink.keys, sink.n, sizeof(start_key), emit_cmp);
+        walk_n = start_cap;
+    }
+    qsort(sink.keys, walk_n, sizeof(start_key), key_cmp);
 
     int64_t nh = 0, used = 0;
     for (int64_t s = 0; s < walk_n; ++s) {

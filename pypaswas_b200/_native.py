@@ -39,6 +39,7 @@ PW_TUNE_WAIT_NS = 5
 PW_TUNE_STALL_TEST = 6
 PW_TUNE_LANES = 7
 PW_TUNE_TRACE_STORE = 8
+PW_TUNE_TILE_TRACE = 9
 PW_SERVE_TUNE_POLICY = 100
 PW_SERVE_TUNE_AGE_MS = 101
 PW_SERVE_TUNE_MAX_BATCH = 102
@@ -98,7 +99,7 @@ class PwRunInfo(ctypes.Structure):
                 ("score_path", ctypes.c_int32), ("dual_lanes", ctypes.c_int32),
                 ("waves", ctypes.c_int32), ("reuse", ctypes.c_int32),
                 ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64),
-                ("trace_store", ctypes.c_int32), ("pad0", ctypes.c_int32)]
+                ("trace_store", ctypes.c_int32), ("tile_pairs", ctypes.c_int32)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

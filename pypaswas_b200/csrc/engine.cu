@@ -30,6 +30,7 @@
 #include "pw_kernels.cuh"
 #include "pw_score16.cuh"
 #include "pw_band.cuh"
+#include "pw_tiles.cuh"
 #include "pw_plan.h"
 #include "pw_finish.cuh"
 #include "pw_host.h"
@@ -235,6 +236,7 @@ struct pw_engine {
     DevBuf q_res, t_ccodes, t_order, cmat_t8, cmat_tf;  // the other orientation's encodings
     DevBuf cmat_i8, cmat_f, pair_max, items, items_alt, counter, bnd_pool, q_order2;
     DevBuf band_pairs, band_entries, band_prog, band_max, band_ring, band_out;  // band sweep (pw_band.cuh)
+    DevBuf tile_ck, tile_marks, tile_pairs, slot_tile;                        // tile form (pw_tiles.cuh)
     DevBuf scan_tmp;  // CUB scan / select scratch
     DevBuf prune_flags, prune_cnt, prune_sel, t_skip, q_count;  // phase-2 pruning on the device
     // hits and column operations of all memory waves, then their order and strings
@@ -1548,8 +1550,9 @@ static cudaError_t finish_hits(pw_engine* e, int64_t n, int64_t* str_bytes) {
 
 // Launches band_kernel over `pairs` (one warp per band, the bands of a pair
 // chained across warps, pw_band.cuh).  DIRS 1: the direction sweep of traced
-// pairs (cell codes), 2: the same storing H (linear gap); 0: pair maxima into
-// band_max (indexed by BandPair.slot).
+// pairs (cell codes), 2: the same storing H (linear gap), 3: the checkpoint
+// sweep of the tile form (linear gap, checkpoints into tile_ck); 0: pair
+// maxima into band_max (indexed by BandPair.slot).
 template <int DIRS>
 static int run_band_phase(pw_engine* e, KernelArgs A, std::vector<BandPair>& pairs, double* kernel_ms,
                           int* n_launch) {
@@ -1557,7 +1560,7 @@ static int run_band_phase(pw_engine* e, KernelArgs A, std::vector<BandPair>& pai
     const int prof_bytes = (int)align_up((int64_t)kWarp * (A.P.alpha + 1) * kWarpRows, 16);
     const int smem = 4 * prof_bytes;
     auto kern = band_kernel<false, DIRS>;
-    if constexpr (DIRS != 2)
+    if constexpr (DIRS != 2 && DIRS != 3)
         if (e->affine) kern = band_kernel<true, DIRS>;
     cudaError_t c;
     if (smem > 48 * 1024 &&
@@ -1588,7 +1591,7 @@ static int run_band_phase(pw_engine* e, KernelArgs A, std::vector<BandPair>& pai
         nstr[k] = sorted[k].nbands;
         xm[k] = steps[order[k]];
         sorted[k].ring_off = ring_elems;
-        if (sorted[k].nbands > 1) ring_elems += 2 * (int64_t)e->pr.qlen[sorted[k].q];
+        if (sorted[k].nbands > 1 && DIRS != 3) ring_elems += 2 * (int64_t)e->pr.qlen[sorted[k].q];
     }
     std::vector<int4> entries;
     if ((int64_t)sorted.size() * 2 >= warps) {
@@ -1646,6 +1649,7 @@ static int run_band_phase(pw_engine* e, KernelArgs A, std::vector<BandPair>& pai
     B.run_max = e->band_max.as<int>();
     B.abort_flag = e->chain_abort.as<int>();
     B.max_out = e->band_out.as<float>();
+    B.ck = DIRS == 3 ? e->tile_ck.as<int>() : nullptr;
     B.wait_ns = wait_limit(e);
     const int grid = std::max(1, std::min(grid_cap(e, per_sm), (int)((n + 3) / 4)));
     cudaEvent_t a, b;
@@ -2028,10 +2032,15 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     // memory waves.
     int64_t warp_cells = 0;
     for (const auto& wp : warp_pairs) warp_cells += (int64_t)qlen[wp.first] * tlen[wp.second];
+    // Long pairs of linear integer scoring take the tile form (pw_tiles.cuh):
+    // no cell codes at all, so the strip sweep's items decide the store alone.
     const int64_t store_mode = e->tune[PW_TUNE_TRACE_STORE];
+    const bool tile_form = pr.int_path && !e->affine && e->tune[PW_TUNE_TILE_TRACE] != 1 && !warp_pairs.empty();
     const bool hstore = pr.int_path && !e->affine && max_pass < 32767 && store_mode != 1 &&
-                        (store_mode == 2 || inf.traced_cells - warp_cells >= warp_cells);
+                        (store_mode == 2 || (tile_form ? inf.traced_cells > warp_cells
+                                                       : inf.traced_cells - warp_cells >= warp_cells));
     inf.trace_store = hstore ? 1 : 0;
+    inf.tile_pairs = tile_form ? (int32_t)warp_pairs.size() : 0;
     const int per_item = plain ? 1 : kWarp;
     double cost_t = 0, cost_q = 0;
     for (int t = 0; t < nt; ++t)
@@ -2138,7 +2147,10 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         w.S = kWarpRows;
         items2.push_back(w);
         cls2.push_back(kNumClasses);  // marks a warp item
-        bytes2.push_back(align_up(warp_code_bytes(qlen[wp.first], tlen[wp.second], hstore), 16));
+        // tile form: checkpoints and the mark plane; else cell codes (or H)
+        bytes2.push_back(tile_form ? tile_checkpoint_ints(qlen[wp.first], tlen[wp.second]) * 4 +
+                                         align_up(((int64_t)qlen[wp.first] * tlen[wp.second] + 31) / 32 * 4, 16)
+                                   : align_up(warp_code_bytes(qlen[wp.first], tlen[wp.second], hstore), 16));
         qmax_warp = std::max(qmax_warp, qlen[wp.first]);
     }
     ht.mark("phase-2 work items");
@@ -2198,7 +2210,8 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         size_t i0 = 0;
         int64_t acc = 0;
         for (size_t i = 0; i < items2.size(); ++i) {
-            const int64_t b = bytes2[i] + bytes2[i] / (hstore ? 16 : 4) + items2[i].lanes * pair_bytes;  // + marks
+            const bool tile_item = tile_form && cls2[i] == kNumClasses;  // its marks are in bytes2
+            const int64_t b = bytes2[i] + (tile_item ? 0 : bytes2[i] / (hstore ? 16 : 4)) + items2[i].lanes * pair_bytes;
             if (acc > 0 && (acc + b > budget || plain)) {
                 waves.push_back({i0, i});
                 i0 = i;
@@ -2219,11 +2232,28 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         std::vector<WorkItem> wi(items2.begin() + i0, items2.begin() + i1);
         std::vector<int> wc(cls2.begin() + i0, cls2.begin() + i1);
         int64_t dir_off = 0, n_pairs = 0;
+        int64_t ck_ints = 0, mark_words = 0;  // tile form: checkpoints, mark planes
+        std::vector<TilePair> tps;
         for (size_t k = 0; k < wi.size(); ++k) {
             wi[k].index = (int32_t)k;
-            wi[k].dir_base = dir_off;
             wi[k].pair_base = n_pairs;
-            dir_off += bytes2[i0 + k];
+            if (tile_form && wc[k] == kNumClasses) {
+                TilePair tp;
+                memset(&tp, 0, sizeof(tp));
+                const int lq_ = qlen[wi[k].first], lt_ = tlen[wi[k].target];
+                tp.q = wi[k].first;
+                tp.t = wi[k].target;
+                tp.slot = (int32_t)n_pairs;
+                tp.ck = ck_ints;
+                tp.marks = mark_words;
+                tps.push_back(tp);
+                wi[k].dir_base = ck_ints;  // band_kernel<false, 3>: the pair's checkpoints
+                ck_ints += tile_checkpoint_ints(lq_, lt_);
+                mark_words += align_up(((int64_t)lq_ * lt_ + 31) / 32, 4);
+            } else {
+                wi[k].dir_base = dir_off;
+                dir_off += bytes2[i0 + k];
+            }
             n_pairs += wi[k].lanes;
         }
         std::vector<WorkItem> by_index = wi;  // trace kernels index items by wave position
@@ -2253,6 +2283,31 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         if ((c = e->marks.reserve(e->stream, mark_bytes)) != cudaSuccess ||
             (c = cudaMemsetAsync(e->marks.p, 0, mark_bytes, e->stream)) != cudaSuccess)
             return cuda_fail(e, c, "alloc cell marks");
+        const int n_tile = (int)tps.size();
+        if (n_tile > 0) {
+            std::vector<int32_t> slot_tile((size_t)n_pairs, -1);
+            for (int k = 0; k < n_tile; ++k) slot_tile[tps[k].slot] = k;
+            if ((c = e->tile_ck.reserve(e->stream, (size_t)ck_ints * sizeof(int))) != cudaSuccess ||
+                (c = e->tile_marks.reserve(e->stream, (size_t)mark_words * 4)) != cudaSuccess ||
+                (c = cudaMemsetAsync(e->tile_marks.p, 0, (size_t)mark_words * 4, e->stream)) != cudaSuccess)
+                return cuda_fail(e, c, "alloc tile-form checkpoints");
+            if ((c = upload(e, e->tile_pairs, tps)) != cudaSuccess || (c = upload(e, e->slot_tile, slot_tile)) != cudaSuccess)
+                return cuda_fail(e, c, "upload tile pairs");
+        }
+        TileArgs TT;
+        memset(&TT, 0, sizeof(TT));
+        TT.pairs = n_tile > 0 ? e->tile_pairs.as<TilePair>() : nullptr;
+        TT.n_pairs = n_tile;
+        TT.ck = n_tile > 0 ? e->tile_ck.as<int>() : nullptr;
+        TT.marks = n_tile > 0 ? e->tile_marks.as<uint32_t>() : nullptr;
+        TT.slot_tile = n_tile > 0 ? e->slot_tile.as<int32_t>() : nullptr;
+        const int tsmem = tile_smem_bytes(Aref.P.alpha + 1);
+        if (n_tile > 0 && tsmem > 48 * 1024) {
+            if ((c = cudaFuncSetAttribute(tile_collect_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tsmem)) != cudaSuccess ||
+                (c = cudaFuncSetAttribute(tile_walk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tsmem)) != cudaSuccess ||
+                (c = cudaFuncSetAttribute(tile_ops_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tsmem)) != cudaSuccess)
+                return cuda_fail(e, c, "tile kernels smem");
+        }
         if ((c = e->metas.reserve(e->stream, n_pairs * sizeof(PairMeta))) != cudaSuccess) return cuda_fail(e, c, "alloc metas");
         if ((c = e->n_cand.reserve(e->stream, n_pairs * sizeof(int32_t))) != cudaSuccess) return cuda_fail(e, c, "alloc");
         if ((c = e->n_starts.reserve(e->stream, n_pairs * sizeof(int32_t))) != cudaSuccess) return cuda_fail(e, c, "alloc");
@@ -2297,8 +2352,9 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         }
         {
             std::vector<BandPair> bp = band_pairs_of(e, ww);
-            rc = hstore ? run_band_phase<2>(e, Aw, bp, &inf.trace_kernel_ms, &inf.trace_launches)
-                        : run_band_phase<1>(e, Aw, bp, &inf.trace_kernel_ms, &inf.trace_launches);
+            rc = tile_form ? run_band_phase<3>(e, Aw, bp, &inf.trace_kernel_ms, &inf.trace_launches)
+                 : hstore  ? run_band_phase<2>(e, Aw, bp, &inf.trace_kernel_ms, &inf.trace_launches)
+                           : run_band_phase<1>(e, Aw, bp, &inf.trace_kernel_ms, &inf.trace_launches);
             if (rc != PW_OK) return rc;
         }
         // candidate overflow: pairs with more candidates than their slot get an
@@ -2379,8 +2435,9 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
             }
             if (!rw.empty()) {
                 std::vector<BandPair> bp = band_pairs_of(e, rw);
-                rc = hstore ? run_band_phase<2>(e, Aw, bp, &inf.trace_kernel_ms, &inf.trace_launches)
-                            : run_band_phase<1>(e, Aw, bp, &inf.trace_kernel_ms, &inf.trace_launches);
+                rc = tile_form ? run_band_phase<3>(e, Aw, bp, &inf.trace_kernel_ms, &inf.trace_launches)
+                     : hstore  ? run_band_phase<2>(e, Aw, bp, &inf.trace_kernel_ms, &inf.trace_launches)
+                               : run_band_phase<1>(e, Aw, bp, &inf.trace_kernel_ms, &inf.trace_launches);
                 if (rc != PW_OK) return rc;
             }
         }
@@ -2402,6 +2459,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         TA.q = Aref.q;
         TA.t = Aref.t;
         TA.P = Aref.P;
+        TA.slot_tile = TT.slot_tile;
         const int tb = 128;
         const int gb = (int)((n_pairs + tb - 1) / tb);
         if (e->affine)
@@ -2409,6 +2467,10 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         else
             PW_LAUNCH(collect_kernel<false>, gb, tb, 0, e->stream, TA);
         e->launches++;
+        if (n_tile > 0) {
+            PW_LAUNCH(tile_collect_kernel, n_tile, kWarp, tsmem, e->stream, Aw, TA, TT);
+            e->launches++;
+        }
         if ((c = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, c, "collect launch");
         // packed start offsets: exclusive scan of the per-pair counts on the device
         {
@@ -2485,6 +2547,10 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
             else
                 PW_LAUNCH(walk_kernel<false>, gb, tb, 0, e->stream, TA);
             e->launches++;
+            if (n_tile > 0) {
+                PW_LAUNCH(tile_walk_kernel, n_tile, kWarp, tsmem, e->stream, Aw, TA, TT);
+                e->launches++;
+            }
             if ((c = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, c, "walk launch");
             std::vector<int64_t> cnt;
             if ((c = download(e, cnt, TA.hit_count, 2)) != cudaSuccess) return cuda_fail(e, c, "walk");
@@ -2498,6 +2564,10 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
                 TA.ops = e->acc_ops.as<char>();
                 PW_LAUNCH(ops_kernel, (nh + 127) / 128, 128, 0, e->stream, TA, TA.hits, nh);
                 e->launches++;
+                if (n_tile > 0) {
+                    PW_LAUNCH(tile_ops_kernel, nh, kWarp, tsmem, e->stream, Aw, TA, TT, (const DevHit*)TA.hits);
+                    e->launches++;
+                }
                 if ((c = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, c, "ops launch");
                 acc_n += nh;
                 acc_ops = ops_end;
@@ -2561,7 +2631,7 @@ extern "C" int pw_set_pairs(pw_engine* e, const int32_t* query_idx, const int32_
 
 extern "C" int pw_set_tuning(pw_engine* e, int key, int64_t value) {
     if (!e) return PW_ERR_ARG;
-    if (key < 0 || key > PW_TUNE_TRACE_STORE || value < 0)
+    if (key < 0 || key > PW_TUNE_TILE_TRACE || value < 0)
         return fail(e, PW_ERR_ARG, "unknown tuning key or negative value");
     e->tune[key] = value;
     return PW_OK;

@@ -29,6 +29,11 @@
 // DIRS = 2 (linear gap): the same sweep storing each cell's 16-bit H at the
 // same positions (16 bytes per lane and step, 512 contiguous bytes a warp) and
 // the candidate list; codes are derived from H on read (PairView::code).
+// DIRS = 3 (linear gap): the checkpoint sweep of the tile form (pw_tiles.cuh):
+// the candidate list as DIRS 1 finds it, no cell codes; instead every band's
+// bottom row is kept (in place of the two-row ring) and every lane stores its
+// 8 rows' H at the last column of each kTileW-column tile, from which any
+// 256 x kTileW tile's codes are recomputed later.
 #pragma once
 #include "pw_kernels.cuh"
 #include "pw_score16.cuh"
@@ -38,6 +43,7 @@ namespace pw {
 constexpr int kWarpRows = 8;                   // rows per lane
 constexpr int kBandRows = kWarpRows * kWarp;   // 256 rows per band
 constexpr int kBandLead = 128;                 // planning lead between bands (steps)
+constexpr int kTileW = 128;                    // tile form: columns of a checkpointed tile
 
 static_assert(kBandRows == 256 && kWarpRows == 8, "warp_layout_offset (pw_kernels.cuh) assumes 8 x 32 rows");
 
@@ -49,12 +55,25 @@ __host__ __device__ __forceinline__ int64_t warp_code_bytes(int lq, int lt, bool
     return hstore ? cells * 2 : cells / 2;
 }
 
+// Tile form: ints of a pair's checkpoints -- the bottom rows of its bands but
+// the last ((nbands - 1) x lq), then per band and tile the 256 H values of the
+// tile's last column (nbands x ntiles x 256; tile ntiles - 1's are not read).
+__host__ __device__ __forceinline__ int tile_count(int lq) { return lq > 0 ? (lq + kTileW - 1) / kTileW : 1; }
+__host__ __device__ __forceinline__ int64_t tile_col_offset(int lq, int lt) {  // 4-int aligned
+    const int64_t bands = lt > 0 ? (lt + kBandRows - 1) / kBandRows : 1;
+    return ((bands - 1) * (int64_t)lq + 3) & ~(int64_t)3;
+}
+__host__ __device__ __forceinline__ int64_t tile_checkpoint_ints(int lq, int lt) {  // a multiple of 4
+    const int64_t bands = lt > 0 ? (lt + kBandRows - 1) / kBandRows : 1;
+    return tile_col_offset(lq, lt) + bands * tile_count(lq) * (int64_t)kBandRows;
+}
+
 struct BandPair {
     int32_t q, t;        // query / target index (reference orientation)
     int32_t nbands;
     int32_t meta_item;   // DIRS: value for PairMeta.item (the pair's work item in the wave)
     int64_t ring_off;    // int4 offset of the pair's two boundary rows (2 x lq)
-    int64_t dir_base;    // DIRS: byte offset of the pair's cell codes
+    int64_t dir_base;    // DIRS 1, 2: byte offset of the pair's cell codes; 3: int offset of its checkpoints
     int64_t slot;        // DIRS: pair slot (metas, candidates); score sweep: pair_max index
 };
 
@@ -68,12 +87,13 @@ struct BandArgs {
     int* run_max;         // per entry: running maximum of the pair's bands so far
     int* abort_flag;
     float* max_out;       // score sweep: pair maxima, indexed by BandPair.slot
+    int* ck;              // DIRS 3: checkpoints (tile_checkpoint_ints per pair, at BandPair.dir_base)
     unsigned long long wait_ns;  // bound of one wait for the band above
 };
 
 template <bool AFFINE, int DIRS>
 __global__ void __launch_bounds__(128, AFFINE ? 5 : 8) band_kernel(KernelArgs A, BandArgs B) {
-    static_assert(DIRS != 2 || !AFFINE, "H store: linear gap only");
+    static_assert((DIRS != 2 && DIRS != 3) || !AFFINE, "H store and tile form: linear gap only");
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -119,7 +139,7 @@ __global__ void __launch_bounds__(128, AFFINE ? 5 : 8) band_kernel(KernelArgs A,
             cand = A.cands + A.cand_base[BP.slot];
             cap = A.cand_cap[BP.slot];
             ncand = A.n_cand + BP.slot;
-            codes = A.codes + BP.dir_base;
+            if constexpr (DIRS != 3) codes = A.codes + BP.dir_base;
         }
         const uint8_t* qg = A.q.codes + A.q.code_off[q];
         const uint8_t* tres = A.t.codes + A.t.code_off[t];
@@ -143,8 +163,20 @@ __global__ void __launch_bounds__(128, AFFINE ? 5 : 8) band_kernel(KernelArgs A,
         __syncwarp();
         const bool has_up = band > 0;
         const bool store_bnd = band + 1 < nbands;
-        const int4* ring_in = B.ring + BP.ring_off + (int64_t)((band + 1) & 1) * lq;
-        int4* ring_out = B.ring + BP.ring_off + (int64_t)(band & 1) * lq;
+        const int4* ring_in = nullptr;
+        int4* ring_out = nullptr;
+        const int* ck_in = nullptr;  // DIRS 3: the bottom row of the band above, this band's, its tile columns
+        int* ck_out = nullptr;
+        int* ck_col = nullptr;
+        if constexpr (DIRS == 3) {
+            int* ckp = B.ck + BP.dir_base;
+            if (has_up) ck_in = ckp + (int64_t)(band - 1) * lq;
+            if (store_bnd) ck_out = ckp + (int64_t)band * lq;
+            ck_col = ckp + tile_col_offset(lq, lt) + ((int64_t)band * tile_count(lq)) * kBandRows + lane * kWarpRows;
+        } else {
+            ring_in = B.ring + BP.ring_off + (int64_t)((band + 1) & 1) * lq;
+            ring_out = B.ring + BP.ring_off + (int64_t)(band & 1) * lq;
+        }
         const int* prog_in = B.progress + pred;
         int* prog_out = B.progress + it;
         const int ymine = yb + lane * kWarpRows;
@@ -171,6 +203,7 @@ __global__ void __launch_bounds__(128, AFFINE ? 5 : 8) band_kernel(KernelArgs A,
         int4 cur = make_int4(0, 0, 0, 0), nxt = make_int4(0, 0, 0, 0);
         auto fetch = [&](int64_t c) -> int4 {
             if (c >= lq) return make_int4(0, 0, 0, 0);
+            if constexpr (DIRS == 3) return make_int4(__ldcg(ck_in + c), 0, 0, 0);
             if constexpr (AFFINE) return __ldcg(&ring_in[c]);
             return make_int4(__ldcg((const int*)&ring_in[c]), 0, 0, 0);
         };
@@ -285,6 +318,14 @@ __global__ void __launch_bounds__(128, AFFINE ? 5 : 8) band_kernel(KernelArgs A,
                         }
                     }
                     bt_h = up;
+                    if constexpr (DIRS == 3) {
+                        // the lane's rows at the last column of a tile: the next tile's left boundary
+                        if (((x + 1) & (kTileW - 1)) == 0 && x + 1 < lq) {
+                            int4* d = (int4*)(ck_col + (int64_t)((x + 1) / kTileW) * kBandRows);
+                            __stcg(d, make_int4(Hl[0], Hl[1], Hl[2], Hl[3]));
+                            __stcg(d + 1, make_int4(Hl[4], Hl[5], Hl[6], Hl[7]));
+                        }
+                    }
                     if constexpr (DIRS == 2) {
                         uint4 hv;
                         hv.x = __byte_perm(Hl[0], Hl[1], 0x5410);
@@ -349,7 +390,12 @@ __global__ void __launch_bounds__(128, AFFINE ? 5 : 8) band_kernel(KernelArgs A,
                 }
                 if constexpr (DIRS == 1)
                     *(uint32_t*)(codes + ((band * nsteps + s) * kWarp + lane) * kWarpRows / 2) = w0;
-                if (lane == kWarp - 1 && store_bnd) __stcg(&ring_out[x], make_int4(AFFINE ? bt_m : bt_h, bt_i, bt_b, 0));
+                if (lane == kWarp - 1 && store_bnd) {
+                    if constexpr (DIRS == 3)
+                        __stcg(ck_out + x, bt_h);
+                    else
+                        __stcg(&ring_out[x], make_int4(AFFINE ? bt_m : bt_h, bt_i, bt_b, 0));
+                }
             } else {
                 // not started (x < 0): hand the left-boundary values down
                 bt_h = 0;

@@ -619,6 +619,8 @@ struct TraceArgs {
     int max_hits;
     char* ops;
     unsigned long long* ops_total;  // column operations reserved so far (walk_kernel assigns ops offsets)
+    const int32_t* slot_tile;       // per pair slot: >= 0 for pairs of the tile form (pw_tiles.cuh), which
+                                    // these kernels leave to the tile kernels; null: none
 };
 
 // Offset of cell (x, y) in the layout of the band direction sweep
@@ -734,6 +736,7 @@ template <bool AFFINE>
 __global__ void collect_kernel(TraceArgs A) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= A.n_pairs) return;
+    if (A.slot_tile && A.slot_tile[p] >= 0) return;
     const PairMeta pm = A.metas[p];
     Cand* cl = A.cands + A.cand_base[p];
     const int n = pm.n_cand;
@@ -832,6 +835,7 @@ template <bool AFFINE>
 __global__ void walk_kernel(TraceArgs A) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= A.n_pairs) return;
+    if (A.slot_tile && A.slot_tile[p] >= 0) return;
     const PairMeta pm = A.metas[p];
     const Cand* cl = A.cands + A.cand_base[p];
     const int m = A.n_starts[p];
@@ -930,6 +934,7 @@ __global__ void ops_kernel(TraceArgs A, const DevHit* hits, int n_hits) {
     const int h = blockIdx.x * blockDim.x + threadIdx.x;
     if (h >= n_hits) return;
     const DevHit H = hits[h];
+    if (A.slot_tile && A.slot_tile[H.pair] >= 0) return;
     const PairMeta pm = A.metas[H.pair];
     PairView v = pair_view(A, pm);
     int x = H.end_x, y = H.end_y;

@@ -1,0 +1,423 @@
+// pw_tiles.cuh -- the tile form of the long-pair traceback (linear gap).
+//
+// The band direction sweep of a long pair stores a 4-bit code for every cell
+// (a 30 kb x 30 kb pair: 450 MB), and the walks then follow their paths one
+// dependent global load a step.  The tile form stores no cell codes: the
+// checkpoint sweep (band_kernel<false, 3>) finds the candidates and keeps
+// every band's bottom row and, per band, the H column at every kTileW-th
+// column.  From those, one warp recomputes the codes of any 256 x kTileW tile
+// into shared memory -- the same codes, bit for bit, as the direction sweep
+// (same recurrence, same boundary values, same classification) -- and the
+// covering chains, the walks and the column operations read them there.
+//
+// One warp per pair (collect, walk) or per hit (operations); every lane runs
+// the same path in step, so a tile miss is recomputed by the whole warp.  The
+// walk follows up to 32 steps by the codes alone and then checks the cells'
+// marks (one load per lane): a walk never revisits its own cells, so the
+// first marked cell of the batch is where the reference's walk stops.  Marks
+// are one bit per cell, bit y * lq + x of the pair's plane.
+#pragma once
+#include "pw_band.cuh"
+
+namespace pw {
+
+// A traced long pair in the tile form.
+struct TilePair {
+    int32_t q, t;     // query / target index (reference orientation)
+    int32_t slot;     // pair slot of the wave (metas, candidates, starting points)
+    int32_t pad;
+    int64_t ck;       // int offset of the pair's checkpoints (tile_checkpoint_ints)
+    int64_t marks;    // uint32 offset of the pair's mark plane
+};
+
+struct TileArgs {
+    const TilePair* pairs;
+    int n_pairs;
+    const int* ck;
+    uint32_t* marks;
+    const int32_t* slot_tile;  // per pair slot: index into pairs, -1 for the other pairs
+};
+
+// Words of one tile's codes: [column of the tile][lane] -> the lane's 8 rows,
+// 4 bits each (the band sweep's word of that lane and column).
+constexpr int kTileWords = kTileW * kWarp;
+
+__host__ __device__ __forceinline__ int tile_smem_bytes(int alpha1) {
+    return kTileWords * 4 + ((kWarp * alpha1 * kWarpRows + 15) & ~15) + (((kTileW + 1) * 4 + 15) & ~15) + kTileW;
+}
+
+// One warp's view of a pair in the tile form, with its one cached tile.
+struct TileView {
+    const int* ckp;         // the pair's checkpoints
+    int64_t col_off;        // tile columns' offset in ckp
+    int ntiles, lq, lt, thr, gap, alpha1, dim;
+    const uint8_t* qg;      // query codes (compact)
+    const uint8_t* tres;    // target residues (matrix index)
+    const int8_t* cmat;
+    uint32_t* words;        // shared: the cached tile's codes
+    uint2* prof;            // shared: [lane][alpha1] scores of the lane's 8 rows in the cached band
+    int* top;               // shared: the row above the tile, columns x0 - 1 .. x0 + kTileW - 1
+    uint8_t* qc;            // shared: the query codes of the tile's columns
+    int band, tile, prof_band;
+    uint32_t* mark_plane;   // the pair's mark bits
+
+    __device__ __forceinline__ uint32_t* mark_word(int x, int y) const {
+        return mark_plane + (((int64_t)y * lq + x) >> 5);
+    }
+    __device__ __forceinline__ uint32_t mark_bit(int x, int y) const {
+        return 1u << ((((int64_t)y * lq + x)) & 31);
+    }
+    __device__ __forceinline__ bool marked(int x, int y) const { return (__ldcg(mark_word(x, y)) & mark_bit(x, y)) != 0; }
+    __device__ __forceinline__ void mark(int x, int y) const { atomicOr(mark_word(x, y), mark_bit(x, y)); }
+    __device__ __forceinline__ void unmark(int x, int y) const { atomicAnd(mark_word(x, y), ~mark_bit(x, y)); }
+
+    // Recomputes tile (band b, tile j); every lane of the warp calls it.
+    __device__ void load(int b, int j) {
+        const int lane = threadIdx.x & 31;
+        __syncwarp();
+        const int yb = b * kBandRows;
+        if (prof_band != b) {
+            for (int idx = lane; idx < kWarp * alpha1; idx += kWarp) {
+                const int ll = idx / alpha1, a = idx % alpha1;
+                uint32_t w0 = 0, w1 = 0;
+#pragma unroll
+                for (int r = 0; r < kWarpRows; ++r) {
+                    const int y = yb + ll * kWarpRows + r;
+                    const int8_t sc = y < lt ? cmat[a * dim + tres[y]] : (int8_t)-128;
+                    if (r < 4)
+                        w0 |= (uint32_t)(uint8_t)sc << (8 * r);
+                    else
+                        w1 |= (uint32_t)(uint8_t)sc << (8 * (r - 4));
+                }
+                prof[idx] = make_uint2(w0, w1);
+            }
+            prof_band = b;
+        }
+        const int x0 = j * kTileW;
+        const int ncol = min(kTileW, lq - x0);
+        for (int k = lane; k <= ncol; k += kWarp) {
+            const int xx = x0 - 1 + k;
+            top[k] = (b > 0 && xx >= 0) ? __ldcg(ckp + (int64_t)(b - 1) * lq + xx) : 0;
+        }
+        for (int k = lane; k < ncol; k += kWarp) qc[k] = qg[x0 + k];
+        int Hl[kWarpRows];
+        if (j > 0) {
+            const int4* src = (const int4*)(ckp + col_off + ((int64_t)b * ntiles + j) * kBandRows + lane * kWarpRows);
+            const int4 v0 = __ldcg(src), v1 = __ldcg(src + 1);
+            Hl[0] = v0.x; Hl[1] = v0.y; Hl[2] = v0.z; Hl[3] = v0.w;
+            Hl[4] = v1.x; Hl[5] = v1.y; Hl[6] = v1.z; Hl[7] = v1.w;
+        } else {
+#pragma unroll
+            for (int r = 0; r < kWarpRows; ++r) Hl[r] = 0;
+        }
+        __syncwarp();
+        const int ymine = yb + lane * kWarpRows;
+        const bool ypos = ymine > 0;
+        const int rows_left = lt - ymine;
+        // the skewed wavefront of band_kernel over the tile's columns; a lane
+        // that has not started hands down its left boundary's bottom value
+        int bt_h = Hl[kWarpRows - 1];
+        int up_h = lane == 0 ? top[0] : 0;  // lane 0: the corner, its first cell's diagonal
+        const int nsteps = ncol + kWarp - 1;
+        for (int s = 0; s < nsteps; ++s) {
+            const int xl = s - lane;
+            const int x = x0 + xl;
+            const bool active = xl >= 0 && xl < ncol;
+            int rh = __shfl_up_sync(0xffffffffu, bt_h, 1);
+            if (lane == 0) rh = (b > 0 && active) ? top[xl + 1] : 0;
+            const int dg_h = x == 0 ? 0 : up_h;
+            up_h = rh;
+            if (active) {
+                const uint2 pw = prof[lane * alpha1 + qc[xl]];
+                const bool xin = x > 0;
+                uint32_t w0 = 0;
+                int up = up_h, diag = dg_h;
+                int Hold[kWarpRows];
+#pragma unroll
+                for (int r = 0; r < kWarpRows; ++r) Hold[r] = Hl[r];
+                const bool stop_ok0 = xin && ypos, stop_ok = xin;
+#pragma unroll
+                for (int r = 0; r < kWarpRows; ++r) {
+                    const int sc = (int)(int8_t)(uint8_t)((r < 4 ? pw.x : pw.y) >> (8 * (r & 3)));
+                    const int left = Hl[r];
+                    int h = addmax(left, gap, diag + sc);
+                    h = addmax_relu(up, gap, h);
+                    const uint32_t sh = 4 * r;
+                    uint32_t code = h == left + gap ? (kLeft << sh) : (h == up + gap ? (kUp << sh) : (kUL << sh));
+                    const bool stop = (r > 0 ? stop_ok : stop_ok0) && diag == 0 && code == (kUL << sh);
+                    code = stop ? code | (kStopFlag << sh) : code;
+                    w0 |= h > 0 ? code : 0u;
+                    diag = left;
+                    Hl[r] = h;
+                    up = h;
+                }
+                const int smax = max(max3(Hl[0], Hl[1], Hl[2]), max3(Hl[3], Hl[4], max3(Hl[5], Hl[6], Hl[7])));
+                if (smax >= thr) {
+#pragma unroll
+                    for (int r = 0; r < kWarpRows; ++r) {
+                        const int h = Hl[r], upv = r > 0 ? Hl[r - 1] : up_h;
+                        if (h < thr || h <= 0 || r >= rows_left || h == Hold[r] + gap || h == upv + gap) continue;
+                        w0 |= kCand << (4 * r);
+                    }
+                }
+                bt_h = up;
+                words[xl * kWarp + lane] = w0;
+            } else if (xl < 0) {
+                bt_h = Hl[kWarpRows - 1];
+            }
+        }
+        band = b;
+        tile = j;
+        __syncwarp();
+    }
+
+    // The 4-bit code of cell (x, y); kNo outside the matrix.  Uniform across the warp.
+    __device__ __forceinline__ uint32_t code(int x, int y) {
+        if (x < 0 || y < 0 || x >= lq || y >= lt) return kNo;
+        const int b = y >> 8, j = x / kTileW;
+        if (b != band || j != tile) load(b, j);
+        const uint32_t w = words[(x - j * kTileW) * kWarp + ((y & (kBandRows - 1)) >> 3)];
+        return (w >> (4 * (y & 7))) & 15u;
+    }
+};
+
+__device__ __forceinline__ TileView tile_view(const KernelArgs& A, const TileArgs& T, const TilePair& tp, int thr,
+                                              unsigned char* smem) {
+    TileView v;
+    v.lq = A.q.len[tp.q];
+    v.lt = A.t.len[tp.t];
+    v.ckp = T.ck + tp.ck;
+    v.col_off = tile_col_offset(v.lq, v.lt);
+    v.ntiles = tile_count(v.lq);
+    v.thr = thr;
+    v.gap = A.P.gap_i;
+    v.alpha1 = A.P.alpha + 1;
+    v.dim = A.P.dim;
+    v.qg = A.q.codes + A.q.code_off[tp.q];
+    v.tres = A.t.codes + A.t.code_off[tp.t];
+    v.cmat = A.cmat_i8;
+    v.words = (uint32_t*)smem;
+    v.prof = (uint2*)(smem + kTileWords * 4);
+    v.top = (int*)(smem + kTileWords * 4 + ((kWarp * v.alpha1 * kWarpRows + 15) & ~15));
+    v.qc = (uint8_t*)v.top + (((kTileW + 1) * 4 + 15) & ~15);
+    v.band = -1;
+    v.tile = -1;
+    v.prof_band = -1;
+    v.mark_plane = T.marks + tp.marks;
+    return v;
+}
+
+// collect_kernel for the pairs of the tile form: the covering chains, the
+// uncovered candidates in walk order, their count.  One warp per pair.
+__global__ void __launch_bounds__(32) tile_collect_kernel(KernelArgs A, TraceArgs TA, TileArgs T) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x;
+    const TilePair tp = T.pairs[blockIdx.x];
+    const int p = tp.slot;
+    const PairMeta pm = TA.metas[p];
+    Cand* cl = TA.cands + TA.cand_base[p];
+    const int n = pm.n_cand;
+    TileView v = tile_view(A, T, tp, pm.thr_i, smem);
+    // marking chains: the nearest candidate up a candidate's chain is covered
+    for (int k = 0; k < n; ++k) {
+        int x = cl[k].x - 1, y = cl[k].y - 1;
+        while (x >= 0 && y >= 0) {
+            const uint32_t cd = v.code(x, y);
+            const int d = cd & 3;
+            if (cd & kCand) {
+                if (lane == 0) v.mark(x, y);  // covered
+                break;
+            }
+            if (d == kNo) break;
+            if (d == kUL) {
+                --x;
+                --y;
+            } else if (d == kUp) {
+                --y;
+            } else {
+                --x;
+            }
+        }
+    }
+    __syncwarp();
+    if (lane != 0) return;
+    // the uncovered candidates (covered marks cleared again), ordered for the
+    // walk: ascending score, then emission order (a stable sort)
+    int m = 0;
+    for (int k = 0; k < n; ++k) {
+        const Cand cc = cl[k];
+        if (v.marked(cc.x, cc.y))
+            v.unmark(cc.x, cc.y);
+        else
+            cl[m++] = cc;
+    }
+    for (int k = 1; k < m; ++k) {
+        const Cand key = cl[k];
+        const uint64_t ek = emission_key(key.x, key.y);
+        int j = k - 1;
+        while (j >= 0) {
+            const Cand o = cl[j];
+            const bool after = o.score_f > key.score_f || (o.score_f == key.score_f && emission_key(o.x, o.y) > ek);
+            if (!after) break;
+            cl[j + 1] = o;
+            --j;
+        }
+        cl[j + 1] = key;
+    }
+    TA.n_starts[p] = m;
+}
+
+// walk_kernel for the pairs of the tile form.  One warp per pair; the walks
+// of a pair run in order, as the reference's (their marks stop later walks).
+__global__ void __launch_bounds__(32) tile_walk_kernel(KernelArgs A, TraceArgs TA, TileArgs T) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x;
+    const TilePair tp = T.pairs[blockIdx.x];
+    const int p = tp.slot;
+    const PairMeta pm = TA.metas[p];
+    const Cand* cl = TA.cands + TA.cand_base[p];
+    const int m = TA.n_starts[p];
+    TileView v = tile_view(A, T, tp, pm.thr_i, smem);
+    const uint8_t* qs = TA.q.raw + TA.q.raw_off[pm.query];
+    const uint8_t* ts = TA.t.raw + TA.t.raw_off[pm.target];
+    const bool same_id = TA.q.key[pm.query] == TA.t.key[pm.target];
+    for (int k = 0; k < m; ++k) {
+        if (TA.allowed && !TA.allowed[TA.start_off[p] + k]) continue;
+        const Cand st = cl[k];
+        int x = st.x, y = st.y;
+        // walk_direction of the starting cell
+        int dir;
+        {
+            const bool mk = v.marked(x, y);
+            const uint32_t cd = v.code(x, y);
+            const int d = cd & 3;
+            dir = mk ? kInAlignment : ((d == kUL && (cd & kStopFlag)) ? kStopDir : d);
+        }
+        bool show = true;
+        if (same_id) {  // SmithWaterman.py:752-755
+            dir = kStopDir;
+            show = false;
+        }
+        if ((double)st.score_f < A.P.host_minimum) show = false;  // :758-759
+        int s_start = x + 1, t_start = y + 1, ncols = 0, mt = 0, mm = 0;
+        bool go = show && x >= 0 && y >= 0 && dir != kStopDir && dir != 32;  // :761
+        while (go) {
+            // up to 32 steps by the codes alone; lane i keeps step i
+            int sx = 0, sy = 0, sd = kNo, n = 0;
+            bool end = false;
+            int cx = x, cy = y;
+            for (int i = 0; i < kWarp; ++i) {
+                if (cx < 0 || cy < 0) {
+                    end = true;
+                    break;
+                }
+                const uint32_t cd = v.code(cx, cy);
+                const int d = cd & 3;
+                const int dd = (d == kUL && (cd & kStopFlag)) ? kStopDir : d;
+                if (lane == i) {
+                    sx = cx;
+                    sy = cy;
+                    sd = dd;
+                }
+                ++n;
+                if (dd == kStopDir || dd == kNo) {  // the walk ends at this cell
+                    end = true;
+                    break;
+                }
+                if (dd == kUL) {
+                    --cx;
+                    --cy;
+                } else if (dd == kLeft) {
+                    --cx;
+                } else {
+                    --cy;
+                }
+            }
+            // the first marked cell of the batch ends the walk there (IN_ALIGNMENT)
+            const unsigned hit_mark = __ballot_sync(0xffffffffu, lane < n && v.marked(sx, sy));
+            const int f = hit_mark ? __ffs(hit_mark) - 1 : n;
+            if (lane < (hit_mark ? f + 1 : n)) v.mark(sx, sy);
+            const bool proc = lane < f;
+            const bool dg = proc && (sd == kUL || sd == kStopDir);
+            const unsigned n_dg = __popc(__ballot_sync(0xffffffffu, dg));
+            const unsigned n_mt = __popc(__ballot_sync(0xffffffffu, dg && same_residue(ts[sy], qs[sx])));
+            const unsigned n_l = __popc(__ballot_sync(0xffffffffu, proc && sd == kLeft));
+            const unsigned n_u = __popc(__ballot_sync(0xffffffffu, proc && sd == kUp));
+            mt += (int)n_mt;
+            mm += (int)(n_dg - n_mt);
+            ncols += (int)(n_dg + n_l + n_u);
+            s_start -= (int)(n_dg + n_l);
+            t_start -= (int)(n_dg + n_u);
+            __syncwarp();
+            if (hit_mark) {
+                show = false;
+                go = false;
+            } else if (end) {
+                go = false;
+            } else {
+                x = cx;
+                y = cy;
+            }
+        }
+        if (show && lane == 0) {
+            const int h = atomicAdd(TA.hit_count, 1);
+            if (h < TA.max_hits) {
+                DevHit o;
+                o.pair = p;
+                o.query = pm.query;
+                o.target = pm.target;
+                o.s_start = s_start;
+                o.s_end = st.x;
+                o.t_start = t_start;
+                o.t_end = st.y;
+                o.score = st.score_f;
+                o.matches = mt;
+                o.mismatches = mm;
+                o.n_cols = ncols;
+                o.end_x = st.x;
+                o.end_y = st.y;
+                o.ops_offset = (int64_t)atomicAdd(TA.ops_total, (unsigned long long)ncols);
+                TA.hits[h] = o;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// ops_kernel for the hits of tile-form pairs: one warp per hit of the wave
+// (hits of the other pairs return at once).
+__global__ void __launch_bounds__(32) tile_ops_kernel(KernelArgs A, TraceArgs TA, TileArgs T, const DevHit* hits) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x;
+    const DevHit H = hits[blockIdx.x];
+    const int ti = T.slot_tile[H.pair];
+    if (ti < 0) return;
+    const TilePair tp = T.pairs[ti];
+    TileView v = tile_view(A, T, tp, TA.metas[H.pair].thr_i, smem);
+    int x = H.end_x, y = H.end_y;
+    char* o = TA.ops + H.ops_offset;
+    char mine = 0;
+    for (int k = 0; k < H.n_cols; ++k) {
+        const int d = v.code(x, y) & 3;
+        char op;
+        if (d == kLeft) {
+            op = 'I';
+            --x;
+        } else if (d == kUp) {
+            op = 'D';
+            --y;
+        } else {
+            op = 'M';
+            --x;
+            --y;
+        }
+        if (lane == (k & 31)) mine = op;
+        if ((k & 31) == 31 || k + 1 == H.n_cols) {
+            // the batch of up to 32 operations, one byte a lane
+            if (lane <= (k & 31)) o[H.n_cols - 1 - (k - (k & 31) + lane)] = mine;
+            __syncwarp();
+        }
+    }
+}
+
+}  // namespace pw

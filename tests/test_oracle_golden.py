@@ -103,3 +103,34 @@ def test_reference_emits_starting_points_in_launch_order(name):
     for b in fx.get("batches", []):
         keys = [(-(u[2] + u[3]), -u[2], u[1], u[0], -(u[4] + u[5]), u[5]) for u in b["starts_u32"]]
         assert keys == sorted(keys)
+
+
+def test_oracle_start_cap_walks_the_first_starts_in_emission_order(oracle_mod):
+    """With more starting points than the cap, the host reads the first cap of
+    the device buffer (emission order, SmithWaterman.py:683-687) and walks
+    those by ascending score: every capped hit ends on one of them, and a cap
+    at the full count changes nothing."""
+    rng = np.random.default_rng(3)
+    seqs = ["".join("ACGT"[i] for i in rng.integers(0, 4, int(rng.integers(60, 200)))) for _ in range(6)]
+    queries = seqs[:3] + [s[10:90] for s in seqs[3:]]
+    targets = seqs[3:] + [s[5:80] for s in seqs[:3]]
+    st = cases.Settings(minimum_score="6", lower_limit_score="0.3", filter_factor="0.05")
+    score = scores.make_score(st)
+    p = cases.oracle_params(oracle_mod, score)
+    pos = cases.pos_scores(score, st, queries, targets)
+    full = oracle_mod.run(p, queries, targets, pos, float(st.minimum_score))
+    starts = full["starts"]
+    assert len(starts) > 20
+    emit = sorted(range(len(starts)), key=lambda k: (
+        -(int(starts[k]["block_x"]) + int(starts[k]["block_y"])), -int(starts[k]["block_x"]),
+        int(starts[k]["target"]), int(starts[k]["sequence"]),
+        -(int(starts[k]["value_x"]) + int(starts[k]["value_y"])), int(starts[k]["value_y"])))
+    assert oracle_mod.run(p, queries, targets, pos, float(st.minimum_score), start_cap=len(starts))["hits"] == \
+        full["hits"]
+    for cap in (1, len(starts) // 4, len(starts) // 2):
+        first = {(int(starts[k]["sequence"]), int(starts[k]["target"]),
+                  int(starts[k]["block_x"]) * 8 + int(starts[k]["value_x"]),
+                  int(starts[k]["block_y"]) * 8 + int(starts[k]["value_y"])) for k in emit[:cap]}
+        got = oracle_mod.run(p, queries, targets, pos, float(st.minimum_score), start_cap=cap)["hits"]
+        assert all((h["query"], h["target"], h["s_end"], h["t_end"]) in first for h in got)
+        assert len(got) <= cap
