@@ -38,12 +38,14 @@ struct TileArgs {
     const int32_t* slot_tile;  // per pair slot: index into pairs, -1 for the other pairs
 };
 
-// Words of one tile's codes: [column of the tile][lane] -> the lane's 8 rows,
-// 4 bits each (the band sweep's word of that lane and column).
-constexpr int kTileWords = kTileW * kWarp;
+// The cached tile holds H, int32, column-major with a one-cell border:
+// column c = x - x0 + 1 (c = 0: the left boundary, column x0 - 1), row
+// r = y - yb + 1 (r = 0: the row above the band); kTileRows values a column.
+constexpr int kTileRows = kBandRows + 1;
+constexpr int kTileCells = (kTileW + 1) * kTileRows;
 
 __host__ __device__ __forceinline__ int tile_smem_bytes(int alpha1) {
-    return kTileWords * 4 + ((kWarp * alpha1 * kWarpRows + 15) & ~15) + (((kTileW + 1) * 4 + 15) & ~15) + kTileW;
+    return ((kTileCells * 4 + 15) & ~15) + ((kWarp * alpha1 * kWarpRows + 15) & ~15) + kTileW;
 }
 
 // One warp's view of a pair in the tile form, with its one cached tile.
@@ -54,11 +56,10 @@ struct TileView {
     const uint8_t* qg;      // query codes (compact)
     const uint8_t* tres;    // target residues (matrix index)
     const int8_t* cmat;
-    uint32_t* words;        // shared: the cached tile's codes
+    int* hs;                // shared: the cached tile's H with its border
     uint2* prof;            // shared: [lane][alpha1] scores of the lane's 8 rows in the cached band
-    int* top;               // shared: the row above the tile, columns x0 - 1 .. x0 + kTileW - 1
     uint8_t* qc;            // shared: the query codes of the tile's columns
-    int band, tile, prof_band;
+    int band, tile, prof_band, x0, yb;
     uint32_t* mark_plane;   // the pair's mark bits
 
     __device__ __forceinline__ uint32_t* mark_word(int x, int y) const {
@@ -71,11 +72,13 @@ struct TileView {
     __device__ __forceinline__ void mark(int x, int y) const { atomicOr(mark_word(x, y), mark_bit(x, y)); }
     __device__ __forceinline__ void unmark(int x, int y) const { atomicAnd(mark_word(x, y), ~mark_bit(x, y)); }
 
-    // Recomputes tile (band b, tile j); every lane of the warp calls it.
+    // Recomputes the H values of tile (band b, tile j) and its border; every
+    // lane of the warp calls it.
     __device__ void load(int b, int j) {
         const int lane = threadIdx.x & 31;
         __syncwarp();
-        const int yb = b * kBandRows;
+        yb = b * kBandRows;
+        x0 = j * kTileW;
         if (prof_band != b) {
             for (int idx = lane; idx < kWarp * alpha1; idx += kWarp) {
                 const int ll = idx / alpha1, a = idx % alpha1;
@@ -93,13 +96,14 @@ struct TileView {
             }
             prof_band = b;
         }
-        const int x0 = j * kTileW;
         const int ncol = min(kTileW, lq - x0);
+        // border row (r = 0): the row above, columns x0 - 1 .. x0 + ncol - 1; 0 above band 0 and left of column 0
         for (int k = lane; k <= ncol; k += kWarp) {
             const int xx = x0 - 1 + k;
-            top[k] = (b > 0 && xx >= 0) ? __ldcg(ckp + (int64_t)(b - 1) * lq + xx) : 0;
+            hs[k * kTileRows] = (b > 0 && xx >= 0) ? __ldcg(ckp + (int64_t)(b - 1) * lq + xx) : 0;
         }
         for (int k = lane; k < ncol; k += kWarp) qc[k] = qg[x0 + k];
+        // border column (c = 0): the checkpointed last column of tile j - 1
         int Hl[kWarpRows];
         if (j > 0) {
             const int4* src = (const int4*)(ckp + col_off + ((int64_t)b * ntiles + j) * kBandRows + lane * kWarpRows);
@@ -110,58 +114,39 @@ struct TileView {
 #pragma unroll
             for (int r = 0; r < kWarpRows; ++r) Hl[r] = 0;
         }
+#pragma unroll
+        for (int r = 0; r < kWarpRows; ++r) hs[1 + lane * kWarpRows + r] = Hl[r];
         __syncwarp();
-        const int ymine = yb + lane * kWarpRows;
-        const bool ypos = ymine > 0;
-        const int rows_left = lt - ymine;
         // the skewed wavefront of band_kernel over the tile's columns; a lane
         // that has not started hands down its left boundary's bottom value
         int bt_h = Hl[kWarpRows - 1];
-        int up_h = lane == 0 ? top[0] : 0;  // lane 0: the corner, its first cell's diagonal
+        int up_h = lane == 0 ? hs[0] : 0;  // lane 0: the corner, its first cell's diagonal
         const int nsteps = ncol + kWarp - 1;
         for (int s = 0; s < nsteps; ++s) {
             const int xl = s - lane;
             const int x = x0 + xl;
             const bool active = xl >= 0 && xl < ncol;
             int rh = __shfl_up_sync(0xffffffffu, bt_h, 1);
-            if (lane == 0) rh = (b > 0 && active) ? top[xl + 1] : 0;
+            if (lane == 0) rh = (b > 0 && active) ? hs[(xl + 1) * kTileRows] : 0;
             const int dg_h = x == 0 ? 0 : up_h;
             up_h = rh;
             if (active) {
                 const uint2 pw = prof[lane * alpha1 + qc[xl]];
-                const bool xin = x > 0;
-                uint32_t w0 = 0;
                 int up = up_h, diag = dg_h;
-                int Hold[kWarpRows];
-#pragma unroll
-                for (int r = 0; r < kWarpRows; ++r) Hold[r] = Hl[r];
-                const bool stop_ok0 = xin && ypos, stop_ok = xin;
 #pragma unroll
                 for (int r = 0; r < kWarpRows; ++r) {
                     const int sc = (int)(int8_t)(uint8_t)((r < 4 ? pw.x : pw.y) >> (8 * (r & 3)));
                     const int left = Hl[r];
                     int h = addmax(left, gap, diag + sc);
                     h = addmax_relu(up, gap, h);
-                    const uint32_t sh = 4 * r;
-                    uint32_t code = h == left + gap ? (kLeft << sh) : (h == up + gap ? (kUp << sh) : (kUL << sh));
-                    const bool stop = (r > 0 ? stop_ok : stop_ok0) && diag == 0 && code == (kUL << sh);
-                    code = stop ? code | (kStopFlag << sh) : code;
-                    w0 |= h > 0 ? code : 0u;
                     diag = left;
                     Hl[r] = h;
                     up = h;
                 }
-                const int smax = max(max3(Hl[0], Hl[1], Hl[2]), max3(Hl[3], Hl[4], max3(Hl[5], Hl[6], Hl[7])));
-                if (smax >= thr) {
-#pragma unroll
-                    for (int r = 0; r < kWarpRows; ++r) {
-                        const int h = Hl[r], upv = r > 0 ? Hl[r - 1] : up_h;
-                        if (h < thr || h <= 0 || r >= rows_left || h == Hold[r] + gap || h == upv + gap) continue;
-                        w0 |= kCand << (4 * r);
-                    }
-                }
                 bt_h = up;
-                words[xl * kWarp + lane] = w0;
+                int* dst = hs + (xl + 1) * kTileRows + 1 + lane * kWarpRows;
+#pragma unroll
+                for (int r = 0; r < kWarpRows; ++r) dst[r] = Hl[r];
             } else if (xl < 0) {
                 bt_h = Hl[kWarpRows - 1];
             }
@@ -171,13 +156,25 @@ struct TileView {
         __syncwarp();
     }
 
-    // The 4-bit code of cell (x, y); kNo outside the matrix.  Uniform across the warp.
+    // The 4-bit code of cell (x, y), derived from the cached H values exactly
+    // as the direction sweep classifies it (LEFT when the left neighbour plus
+    // the gap reaches H, else UP, else UL; NO where H is 0; the stop flag on a
+    // UL cell inside the matrix with a zero diagonal neighbour, the candidate
+    // flag on a UL cell at or above the pair's threshold); kNo outside the
+    // matrix.  Uniform across the warp.
     __device__ __forceinline__ uint32_t code(int x, int y) {
         if (x < 0 || y < 0 || x >= lq || y >= lt) return kNo;
         const int b = y >> 8, j = x / kTileW;
         if (b != band || j != tile) load(b, j);
-        const uint32_t w = words[(x - j * kTileW) * kWarp + ((y & (kBandRows - 1)) >> 3)];
-        return (w >> (4 * (y & 7))) & 15u;
+        const int* c = hs + (x - x0 + 1) * kTileRows + (y - yb + 1);
+        const int h = c[0], l = c[-kTileRows], u = c[-1], d = c[-kTileRows - 1];
+        if (h <= 0) return kNo;
+        if (h == l + gap) return kLeft;
+        if (h == u + gap) return kUp;
+        uint32_t cd = kUL;
+        if (x > 0 && y > 0 && d == 0) cd |= kStopFlag;
+        if (h >= thr) cd |= kCand;
+        return cd;
     }
 };
 
@@ -196,10 +193,11 @@ __device__ __forceinline__ TileView tile_view(const KernelArgs& A, const TileArg
     v.qg = A.q.codes + A.q.code_off[tp.q];
     v.tres = A.t.codes + A.t.code_off[tp.t];
     v.cmat = A.cmat_i8;
-    v.words = (uint32_t*)smem;
-    v.prof = (uint2*)(smem + kTileWords * 4);
-    v.top = (int*)(smem + kTileWords * 4 + ((kWarp * v.alpha1 * kWarpRows + 15) & ~15));
-    v.qc = (uint8_t*)v.top + (((kTileW + 1) * 4 + 15) & ~15);
+    v.hs = (int*)smem;
+    v.prof = (uint2*)(smem + ((kTileCells * 4 + 15) & ~15));
+    v.qc = (uint8_t*)v.prof + ((kWarp * v.alpha1 * kWarpRows + 15) & ~15);
+    v.x0 = 0;
+    v.yb = 0;
     v.band = -1;
     v.tile = -1;
     v.prof_band = -1;

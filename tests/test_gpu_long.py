@@ -3,8 +3,8 @@ long-DNA workload (64 pairs of 10-50 kb with a shared 2-20 kb region at 85%
 identity, each query against its target and the target's reverse complement;
 here 14.9 x 14.2 kb and 11.3 x 21.2 kb), through explicit pairs on the band
 sweep, against the oracle pair by pair: pair maxima, every hit with its
-strings.  The direction memory is capped so that the traced pairs run in
-separate memory waves."""
+strings, in the tile form and with stored cell codes.  The trace memory is
+capped so that the traced pairs run in separate memory waves."""
 import multiprocessing as mp
 
 import numpy as np
@@ -42,27 +42,32 @@ def test_long_dna_pairs_at_full_length_bit_exact_over_memory_waves(engine_lib, o
     # the oracle in fresh processes (spawned: this process already uses the GPU)
     with mp.get_context("spawn").Pool(len(jobs)) as pool:
         ref = pool.map(_oracle_pair, jobs)
-    e = _native.Engine(0, lib=engine_lib)
-    try:
-        configure(e, score, w.settings)
-        e.set_queries([s.encode() for s in q], np.arange(len(q)))
-        e.set_targets([s.encode() for s in t], np.arange(len(t)) + len(q))
-        e.set_pairs([a for a, _ in pairs], [b for _, b in pairs])
-        e.set_wave_limit(250 << 20)  # one traced pair's cell codes per wave
-        info = e.align()
-        pm = e.pair_max()
-        got = decode_hits(*e.hits())
-    finally:
-        e.close()
-    assert info.score_path == 2
     traced = [k for k, (m, _) in enumerate(ref) if m >= float(w.settings.minimum_score)]
-    assert len(traced) >= 2 and info.waves >= 2
-    by_pair = {}
-    for h in got:
-        by_pair.setdefault((h["query"], h["target"]), []).append(h)
-    for (a, b), (m, hits) in zip(pairs, ref):
-        assert pm[a, b] == m
-        want = [dict(h, query=a, target=b) for h in hits]
-        assert by_pair.get((a, b), []) == want
-    # the planted regions are found, 2 kb or longer
-    assert all(max(h["s_end"] - h["s_start"] for h in by_pair[(a, a)]) >= 1500 for a in (0, 1))
+    # the tile form (checkpoints and mark bits, ~0.17 bytes a cell) and the
+    # stored cell codes (~0.63 bytes a cell), one traced pair per wave each
+    for tile, limit in ((0, 48 << 20), (1, 250 << 20)):
+        e = _native.Engine(0, lib=engine_lib)
+        try:
+            configure(e, score, w.settings)
+            e.set_queries([s.encode() for s in q], np.arange(len(q)))
+            e.set_targets([s.encode() for s in t], np.arange(len(t)) + len(q))
+            e.set_pairs([a for a, _ in pairs], [b for _, b in pairs])
+            e.set_tuning(_native.PW_TUNE_TILE_TRACE, tile)
+            e.set_wave_limit(limit)
+            info = e.align()
+            pm = e.pair_max()
+            got = decode_hits(*e.hits())
+        finally:
+            e.close()
+        assert info.score_path == 2
+        assert len(traced) >= 2 and info.waves >= 2
+        assert (info.tile_pairs > 0) == (tile == 0)
+        by_pair = {}
+        for h in got:
+            by_pair.setdefault((h["query"], h["target"]), []).append(h)
+        for (a, b), (m, hits) in zip(pairs, ref):
+            assert pm[a, b] == m
+            want = [dict(h, query=a, target=b) for h in hits]
+            assert by_pair.get((a, b), []) == want
+        # the planted regions are found, 2 kb or longer
+        assert all(max(h["s_end"] - h["s_start"] for h in by_pair[(a, a)]) >= 1500 for a in (0, 1))

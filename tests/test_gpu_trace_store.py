@@ -112,18 +112,21 @@ def test_memory_waves_forms_agree(engine_lib, oracle_mod):
         if len(o["hits"]) >= 4:
             break
         seed += 1
-    e = _native.Engine(0, lib=engine_lib)
-    try:
-        from engine_helpers import configure, decode_hits
-        configure(e, score, st)
-        e.set_queries([q.encode() for q in queries], np.arange(len(queries)))
-        e.set_targets([t.encode() for t in targets], np.arange(len(targets)) + len(queries))
-        e.set_wave_limit(64 << 10)
-        info = e.align()
-        assert info.waves > 1
-        assert decode_hits(*e.hits()) == o["hits"]
-    finally:
-        e.close()
+    from engine_helpers import configure, decode_hits
+    # long pairs in the tile form (a few KB each) and with stored codes
+    for tile, limit in ((0, 8 << 10), (1, 64 << 10)):
+        e = _native.Engine(0, lib=engine_lib)
+        try:
+            configure(e, score, st)
+            e.set_queries([q.encode() for q in queries], np.arange(len(queries)))
+            e.set_targets([t.encode() for t in targets], np.arange(len(targets)) + len(queries))
+            e.set_tuning(_native.PW_TUNE_TILE_TRACE, tile)
+            e.set_wave_limit(limit)
+            info = e.align()
+            assert info.waves > 1
+            assert decode_hits(*e.hits()) == o["hits"]
+        finally:
+            e.close()
 
 
 def test_affine_and_large_maxima_keep_codes(engine_lib, oracle_mod):
