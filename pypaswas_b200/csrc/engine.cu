@@ -19,6 +19,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <unordered_map>
 #include <numeric>
 #include <queue>
 #include <string>
@@ -237,6 +238,12 @@ struct pw_engine {
     DevBuf cmat_i8, cmat_f, pair_max, items, items_alt, counter, bnd_pool, q_order2;
     DevBuf band_pairs, band_entries, band_prog, band_max, band_ring, band_out;  // band sweep (pw_band.cuh)
     DevBuf tile_ck, tile_marks, tile_pairs, slot_tile;                        // tile form (pw_tiles.cuh)
+    DevBuf tile_pairs_alt, tile_sel, tile_cnt;
+    // explicit pairs: the score sweep's tile-form checkpoints (band_kernel<false, 4>)
+    DevBuf p1_ck;
+    bool p1_tiles = false;
+    std::vector<int64_t> p1_ck_off, p1_tm_off;           // per listed pair
+    std::unordered_map<int64_t, int32_t> p1_index;        // query * nt + target -> listed pair
     DevBuf scan_tmp;  // CUB scan / select scratch
     DevBuf prune_flags, prune_cnt, prune_sel, t_skip, q_count;  // phase-2 pruning on the device
     // hits and column operations of all memory waves, then their order and strings
@@ -1560,7 +1567,7 @@ static int run_band_phase(pw_engine* e, KernelArgs A, std::vector<BandPair>& pai
     const int prof_bytes = (int)align_up((int64_t)kWarp * (A.P.alpha + 1) * kWarpRows, 16);
     const int smem = 4 * prof_bytes;
     auto kern = band_kernel<false, DIRS>;
-    if constexpr (DIRS != 2 && DIRS != 3)
+    if constexpr (DIRS < 2)
         if (e->affine) kern = band_kernel<true, DIRS>;
     cudaError_t c;
     if (smem > 48 * 1024 &&
@@ -1590,8 +1597,10 @@ static int run_band_phase(pw_engine* e, KernelArgs A, std::vector<BandPair>& pai
         sorted[k] = pairs[order[k]];
         nstr[k] = sorted[k].nbands;
         xm[k] = steps[order[k]];
-        sorted[k].ring_off = ring_elems;
-        if (sorted[k].nbands > 1 && DIRS != 3) ring_elems += 2 * (int64_t)e->pr.qlen[sorted[k].q];
+        if constexpr (DIRS < 3) {  // DIRS 4 keeps its tile-maxima offset there
+            sorted[k].ring_off = ring_elems;
+            if (sorted[k].nbands > 1) ring_elems += 2 * (int64_t)e->pr.qlen[sorted[k].q];
+        }
     }
     std::vector<int4> entries;
     if ((int64_t)sorted.size() * 2 >= warps) {
@@ -1649,7 +1658,7 @@ static int run_band_phase(pw_engine* e, KernelArgs A, std::vector<BandPair>& pai
     B.run_max = e->band_max.as<int>();
     B.abort_flag = e->chain_abort.as<int>();
     B.max_out = e->band_out.as<float>();
-    B.ck = DIRS == 3 ? e->tile_ck.as<int>() : nullptr;
+    B.ck = DIRS == 3 ? e->tile_ck.as<int>() : DIRS == 4 ? e->p1_ck.as<int>() : nullptr;
     B.wait_ns = wait_limit(e);
     const int grid = std::max(1, std::min(grid_cap(e, per_sm), (int)((n + 3) / 4)));
     cudaEvent_t a, b;
@@ -1671,6 +1680,51 @@ static int run_band_phase(pw_engine* e, KernelArgs A, std::vector<BandPair>& pai
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     if (aborted) return fail(e, PW_ERR_KERNEL, "band sweep: a band waited too long for the band above");
+    return PW_OK;
+}
+
+// Candidates of tile-form pairs whose checkpoints the score sweep kept
+// (band_kernel<false, 4>): the pairs' records and the tiles that reach their
+// thresholds (tile_select_kernel), those tiles recomputed with the
+// candidate test (tile_cand_kernel), the counts into the records.
+static int run_tile_cands(pw_engine* e, KernelArgs A, TileArgs T, const TilePair* dev_list,
+                          const std::vector<TilePair>& list, double* kernel_ms, int* n_launch) {
+    if (list.empty()) return PW_OK;
+    int64_t tiles = 0;
+    for (const TilePair& tp : list) {
+        const int lq = e->pr.qlen[tp.q], lt = e->pr.tlen[tp.t];
+        tiles += (int64_t)(lt > 0 ? (lt + kBandRows - 1) / kBandRows : 1) * tile_count(lq);
+    }
+    if (tiles > INT32_MAX) return fail(e, PW_ERR_CAPACITY, "tile form: too many tiles in one wave");
+    cudaError_t c;
+    const int tsmem = tile_smem_bytes(A.P.alpha + 1);
+    if ((c = e->tile_sel.reserve(e->stream, (size_t)std::max<int64_t>(tiles, 1) * sizeof(int2))) != cudaSuccess ||
+        (c = e->tile_cnt.reserve(e->stream, 4 * sizeof(int))) != cudaSuccess ||
+        (c = cudaMemsetAsync(e->tile_cnt.p, 0, 4 * sizeof(int), e->stream)) != cudaSuccess)
+        return cuda_fail(e, c, "tile selection");
+    if (tsmem > 48 * 1024 &&
+        (c = cudaFuncSetAttribute(tile_cand_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tsmem)) != cudaSuccess)
+        return cuda_fail(e, c, "tile kernels smem");
+    int* cnt = e->tile_cnt.as<int>();
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, e->stream);
+    const int n = (int)list.size();
+    PW_LAUNCH(tile_select_kernel, n, 256, 0, e->stream, A, T, dev_list, e->tile_sel.as<int2>(), cnt, (int)tiles);
+    PW_LAUNCH(tile_cand_kernel, e->sm_count, kWarp, tsmem, e->stream, A, T, dev_list,
+              (const int2*)e->tile_sel.as<int2>(), (const int*)cnt, cnt + 1);
+    PW_LAUNCH(tile_cand_count_kernel, (n + 127) / 128, 128, 0, e->stream, A, dev_list, n);
+    e->launches += 3;
+    cudaEventRecord(b, e->stream);
+    if ((c = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, c, "tile candidates launch");
+    if ((c = cudaEventSynchronize(b)) != cudaSuccess) return cuda_fail(e, c, "tile candidates");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    if (kernel_ms) *kernel_ms += ms;
+    if (n_launch) *n_launch += 3;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
     return PW_OK;
 }
 
@@ -1719,6 +1773,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     const int nq = e->Q.n, nt = e->T.n;
     if (!e->h_pair_max.resize((size_t)nq * nt)) return fail(e, PW_ERR_NOMEM, "host pair maxima");
     e->pm_stale = false;
+    e->p1_tiles = false;
     inf.pairs = (int64_t)nq * nt;
     int64_t sumq = 0, sumt = 0;
     for (int i = 0; i < nq; ++i) sumq += e->Q.off[i + 1] - e->Q.off[i];
@@ -1789,9 +1844,44 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         }
         if ((c = e->band_out.reserve(e->stream, np * sizeof(float))) != cudaSuccess)
             return cuda_fail(e, c, "alloc band maxima");
+        // linear integer scoring: the sweep also keeps the tile form's
+        // checkpoints and tile maxima (band_kernel<false, 4>), so that the
+        // traced pairs need no second sweep -- when they take at most 35% of
+        // the free device memory
+        bool p1ck = !e->affine && e->tune[PW_TUNE_TILE_TRACE] != 1;
+        if (p1ck) {
+            e->p1_ck_off.assign(np, 0);
+            e->p1_tm_off.assign(np, 0);
+            int64_t ck = 0, tm = 0;
+            for (size_t k = 0; k < np; ++k) {
+                const int lq = qlen[bp[k].q], lt = tlen[bp[k].t];
+                e->p1_ck_off[k] = ck;
+                ck += tile_checkpoint_ints(lq, lt);
+                e->p1_tm_off[k] = tm;
+                tm += (int64_t)bp[k].nbands * tile_count(lq);
+            }
+            size_t free_b = 0, total_b = 0;
+            cudaMemGetInfo(&free_b, &total_b);
+            const int64_t bytes = (ck + tm) * (int64_t)sizeof(int);
+            p1ck = (double)bytes <= 0.35 * (double)(free_b + e->p1_ck.bytes);
+            if (p1ck) {
+                if ((c = e->p1_ck.reserve(e->stream, (size_t)bytes)) != cudaSuccess ||
+                    (c = cudaMemsetAsync(e->p1_ck.as<int>() + ck, 0, (size_t)tm * sizeof(int), e->stream)) != cudaSuccess)
+                    return cuda_fail(e, c, "alloc score-sweep checkpoints");
+                e->p1_index.clear();
+                for (size_t k = 0; k < np; ++k) {
+                    e->p1_tm_off[k] += ck;
+                    bp[k].dir_base = e->p1_ck_off[k];
+                    bp[k].ring_off = e->p1_tm_off[k];
+                    e->p1_index.emplace((int64_t)bp[k].q * nt + bp[k].t, (int32_t)k);
+                }
+            }
+        }
         cudaEventRecord(e->ev[0], e->stream);
-        rc = run_band_phase<0>(e, A, bp, &inf.score_kernel_ms, &inf.score_launches);
+        rc = p1ck ? run_band_phase<4>(e, A, bp, &inf.score_kernel_ms, &inf.score_launches)
+                  : run_band_phase<0>(e, A, bp, &inf.score_kernel_ms, &inf.score_launches);
         if (rc != PW_OK) return rc;
+        e->p1_tiles = p1ck;
         cudaEventRecord(e->ev[1], e->stream);
         std::vector<float> bm;
         if ((c = download(e, bm, e->band_out.p, np)) != cudaSuccess) return cuda_fail(e, c, "copy pair maxima");
@@ -2041,6 +2131,8 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
                                                        : inf.traced_cells - warp_cells >= warp_cells));
     inf.trace_store = hstore ? 1 : 0;
     inf.tile_pairs = tile_form ? (int32_t)warp_pairs.size() : 0;
+    // the traced long pairs' checkpoints and tile maxima from the score sweep
+    const bool p1ck = tile_form && e->p1_tiles;
     const int per_item = plain ? 1 : kWarp;
     double cost_t = 0, cost_q = 0;
     for (int t = 0; t < nt; ++t)
@@ -2148,7 +2240,8 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         items2.push_back(w);
         cls2.push_back(kNumClasses);  // marks a warp item
         // tile form: checkpoints and the mark plane; else cell codes (or H)
-        bytes2.push_back(tile_form ? tile_checkpoint_ints(qlen[wp.first], tlen[wp.second]) * 4 +
+        // (the score sweep's checkpoints, when it kept them, are not the wave's)
+        bytes2.push_back(tile_form ? (p1ck ? 0 : tile_checkpoint_ints(qlen[wp.first], tlen[wp.second]) * 4) +
                                          align_up(((int64_t)qlen[wp.first] * tlen[wp.second] + 31) / 32 * 4, 16)
                                    : align_up(warp_code_bytes(qlen[wp.first], tlen[wp.second], hstore), 16));
         qmax_warp = std::max(qmax_warp, qlen[wp.first]);
@@ -2244,11 +2337,18 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
                 tp.q = wi[k].first;
                 tp.t = wi[k].target;
                 tp.slot = (int32_t)n_pairs;
-                tp.ck = ck_ints;
                 tp.marks = mark_words;
+                if (p1ck) {
+                    const auto f = e->p1_index.find((int64_t)tp.q * nt + tp.t);
+                    if (f == e->p1_index.end()) return fail(e, PW_ERR_STATE, "traced pair without checkpoints");
+                    tp.ck = e->p1_ck_off[f->second];
+                    tp.tm = e->p1_tm_off[f->second];
+                } else {
+                    tp.ck = ck_ints;
+                    wi[k].dir_base = ck_ints;  // band_kernel<false, 3>: the pair's checkpoints
+                    ck_ints += tile_checkpoint_ints(lq_, lt_);
+                }
                 tps.push_back(tp);
-                wi[k].dir_base = ck_ints;  // band_kernel<false, 3>: the pair's checkpoints
-                ck_ints += tile_checkpoint_ints(lq_, lt_);
                 mark_words += align_up(((int64_t)lq_ * lt_ + 31) / 32, 4);
             } else {
                 wi[k].dir_base = dir_off;
@@ -2287,7 +2387,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         if (n_tile > 0) {
             std::vector<int32_t> slot_tile((size_t)n_pairs, -1);
             for (int k = 0; k < n_tile; ++k) slot_tile[tps[k].slot] = k;
-            if ((c = e->tile_ck.reserve(e->stream, (size_t)ck_ints * sizeof(int))) != cudaSuccess ||
+            if ((!p1ck && (c = e->tile_ck.reserve(e->stream, (size_t)ck_ints * sizeof(int))) != cudaSuccess) ||
                 (c = e->tile_marks.reserve(e->stream, (size_t)mark_words * 4)) != cudaSuccess ||
                 (c = cudaMemsetAsync(e->tile_marks.p, 0, (size_t)mark_words * 4, e->stream)) != cudaSuccess)
                 return cuda_fail(e, c, "alloc tile-form checkpoints");
@@ -2298,7 +2398,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         memset(&TT, 0, sizeof(TT));
         TT.pairs = n_tile > 0 ? e->tile_pairs.as<TilePair>() : nullptr;
         TT.n_pairs = n_tile;
-        TT.ck = n_tile > 0 ? e->tile_ck.as<int>() : nullptr;
+        TT.ck = n_tile == 0 ? nullptr : p1ck ? e->p1_ck.as<int>() : e->tile_ck.as<int>();
         TT.marks = n_tile > 0 ? e->tile_marks.as<uint32_t>() : nullptr;
         TT.slot_tile = n_tile > 0 ? e->slot_tile.as<int32_t>() : nullptr;
         const int tsmem = tile_smem_bytes(Aref.P.alpha + 1);
@@ -2352,7 +2452,8 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         }
         {
             std::vector<BandPair> bp = band_pairs_of(e, ww);
-            rc = tile_form ? run_band_phase<3>(e, Aw, bp, &inf.trace_kernel_ms, &inf.trace_launches)
+            rc = p1ck ? run_tile_cands(e, Aw, TT, TT.pairs, tps, &inf.trace_kernel_ms, &inf.trace_launches)
+                 : tile_form ? run_band_phase<3>(e, Aw, bp, &inf.trace_kernel_ms, &inf.trace_launches)
                  : hstore  ? run_band_phase<2>(e, Aw, bp, &inf.trace_kernel_ms, &inf.trace_launches)
                            : run_band_phase<1>(e, Aw, bp, &inf.trace_kernel_ms, &inf.trace_launches);
             if (rc != PW_OK) return rc;
@@ -2435,7 +2536,15 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
             }
             if (!rw.empty()) {
                 std::vector<BandPair> bp = band_pairs_of(e, rw);
-                rc = tile_form ? run_band_phase<3>(e, Aw, bp, &inf.trace_kernel_ms, &inf.trace_launches)
+                std::vector<TilePair> rt;  // the overflowing tile-form pairs
+                if (p1ck) {
+                    for (const TilePair& tp : tps)
+                        if (over[tp.slot]) rt.push_back(tp);
+                    if ((c = upload(e, e->tile_pairs_alt, rt)) != cudaSuccess) return cuda_fail(e, c, "upload tile pairs");
+                }
+                rc = p1ck ? run_tile_cands(e, Aw, TT, e->tile_pairs_alt.as<TilePair>(), rt, &inf.trace_kernel_ms,
+                                           &inf.trace_launches)
+                     : tile_form ? run_band_phase<3>(e, Aw, bp, &inf.trace_kernel_ms, &inf.trace_launches)
                      : hstore  ? run_band_phase<2>(e, Aw, bp, &inf.trace_kernel_ms, &inf.trace_launches)
                                : run_band_phase<1>(e, Aw, bp, &inf.trace_kernel_ms, &inf.trace_launches);
                 if (rc != PW_OK) return rc;

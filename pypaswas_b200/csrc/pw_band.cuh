@@ -34,6 +34,10 @@
 // bottom row is kept (in place of the two-row ring) and every lane stores its
 // 8 rows' H at the last column of each kTileW-column tile, from which any
 // 256 x kTileW tile's codes are recomputed later.
+// DIRS = 4 (linear gap): the score sweep of DIRS 0 that also keeps the tile
+// form's checkpoints (as DIRS 3) and each tile's maximum H, so that traced
+// pairs need no second sweep: only the tiles that reach a pair's threshold
+// are recomputed for its candidates (pw_tiles.cuh).
 #pragma once
 #include "pw_kernels.cuh"
 #include "pw_score16.cuh"
@@ -87,13 +91,16 @@ struct BandArgs {
     int* run_max;         // per entry: running maximum of the pair's bands so far
     int* abort_flag;
     float* max_out;       // score sweep: pair maxima, indexed by BandPair.slot
-    int* ck;              // DIRS 3: checkpoints (tile_checkpoint_ints per pair, at BandPair.dir_base)
+    int* ck;              // DIRS 3, 4: checkpoints (tile_checkpoint_ints per pair, at BandPair.dir_base);
+                          // DIRS 4: tile maxima (bands x tiles per pair, at BandPair.ring_off)
     unsigned long long wait_ns;  // bound of one wait for the band above
 };
 
 template <bool AFFINE, int DIRS>
 __global__ void __launch_bounds__(128, AFFINE ? 5 : 8) band_kernel(KernelArgs A, BandArgs B) {
-    static_assert((DIRS != 2 && DIRS != 3) || !AFFINE, "H store and tile form: linear gap only");
+    static_assert(DIRS < 2 || !AFFINE, "H store and tile form: linear gap only");
+    constexpr bool MAXIMA = DIRS == 0 || DIRS == 4;  // pair maxima, no trace
+    constexpr bool CKPT = DIRS == 3 || DIRS == 4;    // tile-form checkpoints
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -119,7 +126,7 @@ __global__ void __launch_bounds__(128, AFFINE ? 5 : 8) band_kernel(KernelArgs A,
         int cap = 0;
         int* ncand = nullptr;
         uint8_t* codes = nullptr;
-        if constexpr (DIRS != 0) {
+        if constexpr (!MAXIMA) {
             // threshold of the pair (default_main.cu:609, SmithWatermanCuda.py:269-275)
             const float maxf = A.pair_max[(int64_t)q * A.pm_lane + (int64_t)t * A.pm_strip];
             const int mn = lq < lt ? lq : lt;
@@ -165,11 +172,13 @@ __global__ void __launch_bounds__(128, AFFINE ? 5 : 8) band_kernel(KernelArgs A,
         const bool store_bnd = band + 1 < nbands;
         const int4* ring_in = nullptr;
         int4* ring_out = nullptr;
-        const int* ck_in = nullptr;  // DIRS 3: the bottom row of the band above, this band's, its tile columns
+        const int* ck_in = nullptr;  // DIRS 3, 4: the bottom row of the band above, this band's, its tile columns
         int* ck_out = nullptr;
         int* ck_col = nullptr;
-        if constexpr (DIRS == 3) {
+        int* tmax = nullptr;  // DIRS 4: this band's tile maxima
+        if constexpr (CKPT) {
             int* ckp = B.ck + BP.dir_base;
+            if constexpr (DIRS == 4) tmax = B.ck + BP.ring_off + (int64_t)band * tile_count(lq);
             if (has_up) ck_in = ckp + (int64_t)(band - 1) * lq;
             if (store_bnd) ck_out = ckp + (int64_t)band * lq;
             ck_col = ckp + tile_col_offset(lq, lt) + ((int64_t)band * tile_count(lq)) * kBandRows + lane * kWarpRows;
@@ -194,6 +203,7 @@ __global__ void __launch_bounds__(128, AFFINE ? 5 : 8) band_kernel(KernelArgs A,
         int dg_h = 0, dg_m = 0, dg_b = 0;
         int bt_h = 0, bt_m = 0, bt_i = neg, bt_b = 0;
         int mx = 0;
+        int tm = 0;  // DIRS 4: the lane's maximum in its current tile
         int avail = 0;
         bool ok = true;
         // the row above, 32 columns at a time: lane k holds column 32j + k of
@@ -203,7 +213,7 @@ __global__ void __launch_bounds__(128, AFFINE ? 5 : 8) band_kernel(KernelArgs A,
         int4 cur = make_int4(0, 0, 0, 0), nxt = make_int4(0, 0, 0, 0);
         auto fetch = [&](int64_t c) -> int4 {
             if (c >= lq) return make_int4(0, 0, 0, 0);
-            if constexpr (DIRS == 3) return make_int4(__ldcg(ck_in + c), 0, 0, 0);
+            if constexpr (CKPT) return make_int4(__ldcg(ck_in + c), 0, 0, 0);
             if constexpr (AFFINE) return __ldcg(&ring_in[c]);
             return make_int4(__ldcg((const int*)&ring_in[c]), 0, 0, 0);
         };
@@ -287,14 +297,16 @@ __global__ void __launch_bounds__(128, AFFINE ? 5 : 8) band_kernel(KernelArgs A,
                             const bool stop = (r > 0 ? stop_ok : stop_ok0) && diag == 0 && code == (kUL << sh);
                             code = stop ? code | (kStopFlag << sh) : code;
                             w0 |= h > 0 ? code : 0u;
-                        } else if constexpr (DIRS == 0) {
+                        } else if constexpr (DIRS == 4) {
+                            tm = max(tm, h);
+                        } else if constexpr (MAXIMA) {
                             mx = max(mx, h);
                         }
                         diag = left;
                         Hl[r] = h;
                         up = h;
                     }
-                    if constexpr (DIRS != 0) {
+                    if constexpr (!MAXIMA) {
                         // candidates: UL cells inside the matrix at or above the
                         // threshold -- rare, so one test of the step's maximum
                         const int smax = max(max3(Hl[0], Hl[1], Hl[2]), max3(Hl[3], Hl[4], max3(Hl[5], Hl[6], Hl[7])));
@@ -318,7 +330,15 @@ __global__ void __launch_bounds__(128, AFFINE ? 5 : 8) band_kernel(KernelArgs A,
                         }
                     }
                     bt_h = up;
-                    if constexpr (DIRS == 3) {
+                    if constexpr (DIRS == 4) {
+                        // the lane's maximum over a tile's columns, into the tile's maximum
+                        if (((x + 1) & (kTileW - 1)) == 0 || x + 1 == lq) {
+                            atomicMax(tmax + x / kTileW, tm);
+                            mx = max(mx, tm);
+                            tm = 0;
+                        }
+                    }
+                    if constexpr (CKPT) {
                         // the lane's rows at the last column of a tile: the next tile's left boundary
                         if (((x + 1) & (kTileW - 1)) == 0 && x + 1 < lq) {
                             int4* d = (int4*)(ck_col + (int64_t)((x + 1) / kTileW) * kBandRows);
@@ -343,7 +363,7 @@ __global__ void __launch_bounds__(128, AFFINE ? 5 : 8) band_kernel(KernelArgs A,
                         const int i = addmax(iup, ext, mup + ge);
                         const int jj = addmax(Jl[r], ext, Ml[r] + ge);
                         const int b = max3(m, i, jj);
-                        if constexpr (DIRS != 0) {
+                        if constexpr (!MAXIMA) {
                             uint32_t code = b == m ? kUL : (b == i ? kUp : kLeft);
                             code = b > 0 ? code : kNo;
                             const bool main_src = code == kUL;
@@ -364,7 +384,7 @@ __global__ void __launch_bounds__(128, AFFINE ? 5 : 8) band_kernel(KernelArgs A,
                     bt_m = mup;
                     bt_i = iup;
                     bt_b = Bl[kWarpRows - 1];
-                    if constexpr (DIRS != 0) {
+                    if constexpr (!MAXIMA) {
                         // candidates: MAIN-source cells (b == m > 0) inside the
                         // matrix with m at or above the threshold -- rare, so one
                         // test of the step's maximum of m
@@ -391,7 +411,7 @@ __global__ void __launch_bounds__(128, AFFINE ? 5 : 8) band_kernel(KernelArgs A,
                 if constexpr (DIRS == 1)
                     *(uint32_t*)(codes + ((band * nsteps + s) * kWarp + lane) * kWarpRows / 2) = w0;
                 if (lane == kWarp - 1 && store_bnd) {
-                    if constexpr (DIRS == 3)
+                    if constexpr (CKPT)
                         __stcg(ck_out + x, bt_h);
                     else
                         __stcg(&ring_out[x], make_int4(AFFINE ? bt_m : bt_h, bt_i, bt_b, 0));
@@ -410,18 +430,18 @@ __global__ void __launch_bounds__(128, AFFINE ? 5 : 8) band_kernel(KernelArgs A,
         if (!ok) break;
         if (store_bnd && lane == kWarp - 1) st_release_gpu(prog_out, lq);
         // pair maximum (score sweep) / candidate count (direction sweep)
-        if constexpr (DIRS == 0) mx = __reduce_max_sync(0xffffffffu, mx);
+        if constexpr (MAXIMA) mx = __reduce_max_sync(0xffffffffu, mx);
         if (has_up) {
             // the band above has finished: its running maximum and its candidates are final
             if (chain_wait(prog_in, kChainDone, B.abort_flag, B.wait_ns) < 0) break;
-            if constexpr (DIRS == 0) mx = max(mx, __ldcg(&B.run_max[pred]));
+            if constexpr (MAXIMA) mx = max(mx, __ldcg(&B.run_max[pred]));
         }
         if (store_bnd) {
-            if constexpr (DIRS == 0)
+            if constexpr (MAXIMA)
                 if (lane == 0) __stcg(&B.run_max[it], mx);
             chain_publish(prog_out, kChainDone);
         } else if (lane == 0) {
-            if constexpr (DIRS != 0)
+            if constexpr (!MAXIMA)
                 A.metas[BP.slot].n_cand = atomicAdd(ncand, 0);
             else
                 B.max_out[BP.slot] = (float)mx;

@@ -28,6 +28,14 @@ struct TilePair {
     int32_t pad;
     int64_t ck;       // int offset of the pair's checkpoints (tile_checkpoint_ints)
     int64_t marks;    // uint32 offset of the pair's mark plane
+    int64_t tm;       // checkpoints of the score sweep (band_kernel<false, 4>): int offset of the tile maxima
+};
+
+// Where a tile sweep puts the candidates it finds (the pair's slot).
+struct CandSink {
+    Cand* cand;
+    int cap;
+    int* n;
 };
 
 struct TileArgs {
@@ -72,9 +80,14 @@ struct TileView {
     __device__ __forceinline__ void mark(int x, int y) const { atomicOr(mark_word(x, y), mark_bit(x, y)); }
     __device__ __forceinline__ void unmark(int x, int y) const { atomicAnd(mark_word(x, y), ~mark_bit(x, y)); }
 
+    __device__ void load(int b, int j) { load_h<false>(b, j, CandSink{nullptr, 0, nullptr}); }
+
     // Recomputes the H values of tile (band b, tile j) and its border; every
-    // lane of the warp calls it.
-    __device__ void load(int b, int j) {
+    // lane of the warp calls it.  CANDS: also the tile's candidates into the
+    // sink, with the band sweep's test (UL cells inside the matrix at or above
+    // the threshold).
+    template <bool CANDS>
+    __device__ void load_h(int b, int j, CandSink sink) {
         const int lane = threadIdx.x & 31;
         __syncwarp();
         yb = b * kBandRows;
@@ -119,6 +132,8 @@ struct TileView {
         __syncwarp();
         // the skewed wavefront of band_kernel over the tile's columns; a lane
         // that has not started hands down its left boundary's bottom value
+        const int ymine = yb + lane * kWarpRows;
+        const int rows_left = lt - ymine;
         int bt_h = Hl[kWarpRows - 1];
         int up_h = lane == 0 ? hs[0] : 0;  // lane 0: the corner, its first cell's diagonal
         const int nsteps = ncol + kWarp - 1;
@@ -133,6 +148,11 @@ struct TileView {
             if (active) {
                 const uint2 pw = prof[lane * alpha1 + qc[xl]];
                 int up = up_h, diag = dg_h;
+                int Hold[kWarpRows];
+                if constexpr (CANDS) {
+#pragma unroll
+                    for (int r = 0; r < kWarpRows; ++r) Hold[r] = Hl[r];
+                }
 #pragma unroll
                 for (int r = 0; r < kWarpRows; ++r) {
                     const int sc = (int)(int8_t)(uint8_t)((r < 4 ? pw.x : pw.y) >> (8 * (r & 3)));
@@ -142,6 +162,25 @@ struct TileView {
                     diag = left;
                     Hl[r] = h;
                     up = h;
+                }
+                if constexpr (CANDS) {
+                    const int smax = max(max3(Hl[0], Hl[1], Hl[2]), max3(Hl[3], Hl[4], max3(Hl[5], Hl[6], Hl[7])));
+                    if (smax >= thr) {
+#pragma unroll
+                        for (int r = 0; r < kWarpRows; ++r) {
+                            const int h = Hl[r], upv = r > 0 ? Hl[r - 1] : up_h;
+                            if (h < thr || h <= 0 || r >= rows_left || h == Hold[r] + gap || h == upv + gap) continue;
+                            const int k = atomicAdd(sink.n, 1);
+                            if (k < sink.cap) {
+                                Cand cc;
+                                cc.x = x;
+                                cc.y = ymine + r;
+                                cc.score_i = h;
+                                cc.score_f = (float)h;
+                                sink.cand[k] = cc;
+                            }
+                        }
+                    }
                 }
                 bt_h = up;
                 int* dst = hs + (xl + 1) * kTileRows + 1 + lane * kWarpRows;
@@ -217,7 +256,8 @@ __global__ void __launch_bounds__(32) tile_collect_kernel(KernelArgs A, TraceArg
     const int n = pm.n_cand;
     TileView v = tile_view(A, T, tp, pm.thr_i, smem);
     // marking chains: the nearest candidate up a candidate's chain is covered
-    for (int k = 0; k < n; ++k) {
+    // (a lone candidate has no other candidate to cover)
+    for (int k = 0; k < n && n > 1; ++k) {
         int x = cl[k].x - 1, y = cl[k].y - 1;
         while (x >= 0 && y >= 0) {
             const uint32_t cd = v.code(x, y);
@@ -416,6 +456,77 @@ __global__ void __launch_bounds__(32) tile_ops_kernel(KernelArgs A, TraceArgs TA
             __syncwarp();
         }
     }
+}
+
+// ---- candidates from the score sweep's checkpoints (band_kernel<false, 4>)
+
+// The candidate threshold of a pair (default_main.cu:609,
+// SmithWatermanCuda.py:269-275), as band_kernel computes it.
+__device__ __forceinline__ float tile_pair_threshold(const KernelArgs& A, int q, int t, int lq, int lt, float* maxf) {
+    *maxf = A.pair_max[(int64_t)q * A.pm_lane + (int64_t)t * A.pm_strip];
+    const int mn = lq < lt ? lq : lt;
+    const float pos = (float)(A.P.highest * (double)mn * A.P.filter_factor);
+    return fmaxf(__fmul_rn(A.P.lower_limit, *maxf), pos);
+}
+
+// One block per pair of `list`: the pair's record (threshold, maximum) and
+// the tiles whose maximum reaches the threshold, appended to sel as
+// (list index, band * tiles + tile).
+__global__ void tile_select_kernel(KernelArgs A, TileArgs T, const TilePair* list, int2* sel, int* sel_count,
+                                   int sel_cap) {
+    const TilePair tp = list[blockIdx.x];
+    const int lq = A.q.len[tp.q], lt = A.t.len[tp.t];
+    float maxf;
+    const float thf = tile_pair_threshold(A, tp.q, tp.t, lq, lt, &maxf);
+    const int thr = (int)fminf(fmaxf(ceilf(thf), -1.0e9f), 1.0e9f);
+    if (threadIdx.x == 0) {
+        PairMeta pm;
+        pm.query = tp.q;
+        pm.target = tp.t;
+        pm.item = 0;
+        pm.lane = 0;
+        pm.n_cand = 0;
+        pm.thr_i = thr;
+        pm.thr_f = thf;
+        pm.max_f = maxf;
+        A.metas[tp.slot] = pm;
+    }
+    const int nbands = lt > 0 ? (lt + kBandRows - 1) / kBandRows : 1;
+    const int n = nbands * tile_count(lq);
+    const int* tmx = T.ck + tp.tm;
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        if (tmx[i] >= thr) {
+            const int k = atomicAdd(sel_count, 1);
+            if (k < sel_cap) sel[k] = make_int2((int)blockIdx.x, i);
+        }
+}
+
+// One warp a block, persistent: each selected tile recomputed from the
+// checkpoints, its candidates into the pair's slot.
+__global__ void __launch_bounds__(32) tile_cand_kernel(KernelArgs A, TileArgs T, const TilePair* list,
+                                                       const int2* sel, const int* sel_count, int* counter) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x;
+    const int total = *sel_count;
+    for (;;) {
+        int it = 0;
+        if (lane == 0) it = atomicAdd(counter, 1);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it >= total) break;
+        const int2 en = sel[it];
+        const TilePair tp = list[en.x];
+        TileView v = tile_view(A, T, tp, A.metas[tp.slot].thr_i, smem);
+        const int b = en.y / v.ntiles, j = en.y % v.ntiles;
+        v.load_h<true>(b, j, CandSink{A.cands + A.cand_base[tp.slot], A.cand_cap[tp.slot], A.n_cand + tp.slot});
+    }
+}
+
+// The candidate counts of `list`'s pairs into their records.
+__global__ void tile_cand_count_kernel(KernelArgs A, const TilePair* list, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int p = list[i].slot;
+    A.metas[p].n_cand = A.n_cand[p];
 }
 
 }  // namespace pw
