@@ -238,7 +238,7 @@ struct pw_engine {
     DevBuf cmat_i8, cmat_f, pair_max, items, items_alt, counter, bnd_pool, q_order2;
     DevBuf band_pairs, band_entries, band_prog, band_max, band_ring, band_out;  // band sweep (pw_band.cuh)
     DevBuf tile_ck, tile_marks, tile_pairs, slot_tile;                        // tile form (pw_tiles.cuh)
-    DevBuf tile_pairs_alt, tile_sel, tile_cnt;
+    DevBuf tile_pairs_alt, tile_sel, tile_cnt, tile_acc, tile_scratch, tile_ops;
     // explicit pairs: the score sweep's tile-form checkpoints (band_kernel<false, 4>)
     DevBuf p1_ck;
     bool p1_tiles = false;
@@ -2325,7 +2325,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         std::vector<WorkItem> wi(items2.begin() + i0, items2.begin() + i1);
         std::vector<int> wc(cls2.begin() + i0, cls2.begin() + i1);
         int64_t dir_off = 0, n_pairs = 0;
-        int64_t ck_ints = 0, mark_words = 0;  // tile form: checkpoints, mark planes
+        int64_t ck_ints = 0, mark_words = 0, scratch_bytes = 0;  // tile form: checkpoints, mark planes, walk scratch
         std::vector<TilePair> tps;
         for (size_t k = 0; k < wi.size(); ++k) {
             wi[k].index = (int32_t)k;
@@ -2338,6 +2338,8 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
                 tp.t = wi[k].target;
                 tp.slot = (int32_t)n_pairs;
                 tp.marks = mark_words;
+                tp.scratch = scratch_bytes;
+                scratch_bytes += align_up((int64_t)lq_ + lt_ + 32, 16);
                 if (p1ck) {
                     const auto f = e->p1_index.find((int64_t)tp.q * nt + tp.t);
                     if (f == e->p1_index.end()) return fail(e, PW_ERR_STATE, "traced pair without checkpoints");
@@ -2388,6 +2390,9 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
             std::vector<int32_t> slot_tile((size_t)n_pairs, -1);
             for (int k = 0; k < n_tile; ++k) slot_tile[tps[k].slot] = k;
             if ((!p1ck && (c = e->tile_ck.reserve(e->stream, (size_t)ck_ints * sizeof(int))) != cudaSuccess) ||
+                (c = e->tile_scratch.reserve(e->stream, (size_t)scratch_bytes)) != cudaSuccess ||
+                (c = e->tile_acc.reserve(e->stream, 4 * sizeof(unsigned long long))) != cudaSuccess ||
+                (c = cudaMemsetAsync(e->tile_acc.p, 0, 4 * sizeof(unsigned long long), e->stream)) != cudaSuccess ||
                 (c = e->tile_marks.reserve(e->stream, (size_t)mark_words * 4)) != cudaSuccess ||
                 (c = cudaMemsetAsync(e->tile_marks.p, 0, (size_t)mark_words * 4, e->stream)) != cudaSuccess)
                 return cuda_fail(e, c, "alloc tile-form checkpoints");
@@ -2401,6 +2406,9 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         TT.ck = n_tile == 0 ? nullptr : p1ck ? e->p1_ck.as<int>() : e->tile_ck.as<int>();
         TT.marks = n_tile > 0 ? e->tile_marks.as<uint32_t>() : nullptr;
         TT.slot_tile = n_tile > 0 ? e->slot_tile.as<int32_t>() : nullptr;
+        TT.scratch = n_tile > 0 ? e->tile_scratch.as<char>() : nullptr;
+        TT.ops_bound = n_tile > 0 ? e->tile_acc.as<unsigned long long>() : nullptr;
+        TT.ops_total = n_tile > 0 ? e->tile_acc.as<unsigned long long>() + 1 : nullptr;
         const int tsmem = tile_smem_bytes(Aref.P.alpha + 1);
         if (n_tile > 0 && tsmem > 48 * 1024) {
             if ((c = cudaFuncSetAttribute(tile_collect_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tsmem)) != cudaSuccess ||
@@ -2597,10 +2605,21 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
         cudaEventRecord(e->ev[2], e->stream);
         int64_t last_off = 0;
         int32_t last_n = 0;
+        unsigned long long tile_bound = 0;  // tile form: bytes of operations its walks can reserve at most
         if ((c = copy_d2h(e, &last_off, e->start_off.as<int64_t>() + n_pairs - 1, sizeof(int64_t))) != cudaSuccess ||
             (c = copy_d2h(e, &last_n, TA.n_starts + n_pairs - 1, sizeof(int32_t))) != cudaSuccess ||
+            (n_tile > 0 && (c = copy_d2h(e, &tile_bound, TT.ops_bound, sizeof(tile_bound))) != cudaSuccess) ||
             (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
             return cuda_fail(e, c, "collect");
+        // the tile walks spell their hits' operations themselves unless that
+        // bound is large (more than 1 GiB); else tile_ops_kernel walks the
+        // hits again
+        TT.ops = nullptr;
+        if (n_tile > 0 && tile_bound <= (1ull << 30)) {
+            if ((c = e->tile_ops.reserve(e->stream, (size_t)std::max<unsigned long long>(tile_bound, 16))) != cudaSuccess)
+                return cuda_fail(e, c, "alloc tile operations");
+            TT.ops = e->tile_ops.as<char>();
+        }
         const int64_t wave_starts = last_off + last_n;
         TA.start_off = e->start_off.as<int64_t>();
         const size_t first_rec = e->h_starts.size();
@@ -2664,7 +2683,12 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
             std::vector<int64_t> cnt;
             if ((c = download(e, cnt, TA.hit_count, 2)) != cudaSuccess) return cuda_fail(e, c, "walk");
             const int nh = (int)std::min<int64_t>((int32_t)(cnt[0] & 0xffffffff), wave_starts);
-            const int64_t ops_end = cnt[1];
+            unsigned long long tile_ops_n = 0;
+            if (TT.ops && (c = copy_d2h(e, &tile_ops_n, TT.ops_total, sizeof(tile_ops_n))) != cudaSuccess)
+                return cuda_fail(e, c, "walk");
+            if (TT.ops && (c = cudaStreamSynchronize(e->stream)) != cudaSuccess) return cuda_fail(e, c, "walk");
+            const int64_t strip_end = cnt[1];
+            const int64_t ops_end = strip_end + (int64_t)tile_ops_n;
             if (nh) {
                 // column operations of the kept hits
                 if ((c = e->acc_ops.grow_keep(e->stream, (size_t)acc_ops, (size_t)std::max<int64_t>(ops_end, 16))) !=
@@ -2673,7 +2697,15 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
                 TA.ops = e->acc_ops.as<char>();
                 PW_LAUNCH(ops_kernel, (nh + 127) / 128, 128, 0, e->stream, TA, TA.hits, nh);
                 e->launches++;
-                if (n_tile > 0) {
+                if (n_tile > 0 && TT.ops) {
+                    // the tile walks' operations go after the others
+                    PW_LAUNCH(tile_ops_rebase_kernel, (nh + 127) / 128, 128, 0, e->stream, TT, TA.hits, nh, strip_end);
+                    e->launches++;
+                    if (tile_ops_n > 0 &&
+                        (c = cudaMemcpyAsync(e->acc_ops.as<char>() + strip_end, TT.ops, (size_t)tile_ops_n,
+                                             cudaMemcpyDeviceToDevice, e->stream)) != cudaSuccess)
+                        return cuda_fail(e, c, "copy tile operations");
+                } else if (n_tile > 0) {
                     PW_LAUNCH(tile_ops_kernel, nh, kWarp, tsmem, e->stream, Aw, TA, TT, (const DevHit*)TA.hits);
                     e->launches++;
                 }

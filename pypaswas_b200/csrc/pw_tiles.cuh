@@ -29,6 +29,7 @@ struct TilePair {
     int64_t ck;       // int offset of the pair's checkpoints (tile_checkpoint_ints)
     int64_t marks;    // uint32 offset of the pair's mark plane
     int64_t tm;       // checkpoints of the score sweep (band_kernel<false, 4>): int offset of the tile maxima
+    int64_t scratch;  // byte offset of the pair's walk scratch (lq + lt bytes)
 };
 
 // Where a tile sweep puts the candidates it finds (the pair's slot).
@@ -44,6 +45,13 @@ struct TileArgs {
     const int* ck;
     uint32_t* marks;
     const int32_t* slot_tile;  // per pair slot: index into pairs, -1 for the other pairs
+    // the walk writes its hits' column operations itself when ops is set:
+    // reserved from ops_total in ops (offsets relative to ops, the host adds
+    // the base), spelled in walk order into the pair's scratch first
+    char* scratch;
+    char* ops;
+    unsigned long long* ops_total;
+    unsigned long long* ops_bound;  // tile_collect_kernel: sum of starts x (lq + lt) over the pairs
 };
 
 // The cached tile holds H, int32, column-major with a one-cell border:
@@ -137,16 +145,27 @@ struct TileView {
         int bt_h = Hl[kWarpRows - 1];
         int up_h = lane == 0 ? hs[0] : 0;  // lane 0: the corner, its first cell's diagonal
         const int nsteps = ncol + kWarp - 1;
+        // the shared-memory reads of a step (its scores; lane 0: the row
+        // above) are issued one step ahead, off the recurrence's path
+        auto fetch_pw = [&](int c) -> uint2 {
+            return (c >= 0 && c < ncol) ? prof[lane * alpha1 + qc[c]] : make_uint2(0u, 0u);
+        };
+        auto fetch_top = [&](int c) -> int { return (b > 0 && c >= 0 && c < ncol) ? hs[(c + 1) * kTileRows] : 0; };
+        uint2 pw_n = fetch_pw(-lane);
+        int top_n = lane == 0 ? fetch_top(0) : 0;
         for (int s = 0; s < nsteps; ++s) {
             const int xl = s - lane;
             const int x = x0 + xl;
             const bool active = xl >= 0 && xl < ncol;
+            const uint2 pw = pw_n;
+            const int top = top_n;
+            pw_n = fetch_pw(xl + 1);
+            if (lane == 0) top_n = fetch_top(xl + 1);
             int rh = __shfl_up_sync(0xffffffffu, bt_h, 1);
-            if (lane == 0) rh = (b > 0 && active) ? hs[(xl + 1) * kTileRows] : 0;
+            if (lane == 0) rh = top;
             const int dg_h = x == 0 ? 0 : up_h;
             up_h = rh;
             if (active) {
-                const uint2 pw = prof[lane * alpha1 + qc[xl]];
                 int up = up_h, diag = dg_h;
                 int Hold[kWarpRows];
                 if constexpr (CANDS) {
@@ -303,6 +322,7 @@ __global__ void __launch_bounds__(32) tile_collect_kernel(KernelArgs A, TraceArg
         cl[j + 1] = key;
     }
     TA.n_starts[p] = m;
+    if (T.ops_bound) atomicAdd(T.ops_bound, (unsigned long long)m * (unsigned long long)(v.lq + v.lt));
 }
 
 // walk_kernel for the pairs of the tile form.  One warp per pair; the walks
@@ -319,6 +339,7 @@ __global__ void __launch_bounds__(32) tile_walk_kernel(KernelArgs A, TraceArgs T
     const uint8_t* qs = TA.q.raw + TA.q.raw_off[pm.query];
     const uint8_t* ts = TA.t.raw + TA.t.raw_off[pm.target];
     const bool same_id = TA.q.key[pm.query] == TA.t.key[pm.target];
+    char* scr = T.ops ? T.scratch + tp.scratch : nullptr;
     for (int k = 0; k < m; ++k) {
         if (TA.allowed && !TA.allowed[TA.start_off[p] + k]) continue;
         const Cand st = cl[k];
@@ -377,6 +398,10 @@ __global__ void __launch_bounds__(32) tile_walk_kernel(KernelArgs A, TraceArgs T
             if (lane < (hit_mark ? f + 1 : n)) v.mark(sx, sy);
             const bool proc = lane < f;
             const bool dg = proc && (sd == kUL || sd == kStopDir);
+            if (T.ops) {  // the batch's columns in walk order (a prefix of the lanes)
+                const bool col = proc && sd != kNo;
+                if (col) scr[ncols + lane] = dg ? 'M' : (sd == kLeft ? 'I' : 'D');
+            }
             const unsigned n_dg = __popc(__ballot_sync(0xffffffffu, dg));
             const unsigned n_mt = __popc(__ballot_sync(0xffffffffu, dg && same_residue(ts[sy], qs[sx])));
             const unsigned n_l = __popc(__ballot_sync(0xffffffffu, proc && sd == kLeft));
@@ -397,8 +422,23 @@ __global__ void __launch_bounds__(32) tile_walk_kernel(KernelArgs A, TraceArgs T
                 y = cy;
             }
         }
+        __syncwarp();
+        int h = 0;
+        int64_t ops_off = 0;
         if (show && lane == 0) {
-            const int h = atomicAdd(TA.hit_count, 1);
+            h = atomicAdd(TA.hit_count, 1);
+            if (h < TA.max_hits)
+                ops_off = T.ops ? (int64_t)atomicAdd(T.ops_total, (unsigned long long)ncols)
+                                : (int64_t)atomicAdd(TA.ops_total, (unsigned long long)ncols);
+        }
+        if (show && T.ops) {
+            // the operations in alignment order: the scratch reversed
+            h = __shfl_sync(0xffffffffu, h, 0);
+            ops_off = __shfl_sync(0xffffffffu, ops_off, 0);
+            if (h < TA.max_hits)
+                for (int i = lane; i < ncols; i += kWarp) T.ops[ops_off + ncols - 1 - i] = scr[i];
+        }
+        if (show && lane == 0) {
             if (h < TA.max_hits) {
                 DevHit o;
                 o.pair = p;
@@ -414,7 +454,7 @@ __global__ void __launch_bounds__(32) tile_walk_kernel(KernelArgs A, TraceArgs T
                 o.n_cols = ncols;
                 o.end_x = st.x;
                 o.end_y = st.y;
-                o.ops_offset = (int64_t)atomicAdd(TA.ops_total, (unsigned long long)ncols);
+                o.ops_offset = ops_off;
                 TA.hits[h] = o;
             }
         }
@@ -527,6 +567,14 @@ __global__ void tile_cand_count_kernel(KernelArgs A, const TilePair* list, int n
     if (i >= n) return;
     const int p = list[i].slot;
     A.metas[p].n_cand = A.n_cand[p];
+}
+
+// After a walk that wrote the tile-form hits' operations into their own
+// buffer: those hits' offsets move past the other hits' operations (base).
+__global__ void tile_ops_rebase_kernel(TileArgs T, DevHit* hits, int n_hits, int64_t base) {
+    const int h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= n_hits) return;
+    if (T.slot_tile[hits[h].pair] >= 0) hits[h].ops_offset += base;
 }
 
 }  // namespace pw
