@@ -242,6 +242,8 @@ struct pw_engine {
     // explicit pairs: the score sweep's tile-form checkpoints (band_kernel<false, 4>)
     DevBuf p1_ck;
     bool p1_tiles = false;
+    int64_t p1_free = 0;
+    double p1_free_t = -1.0;
     std::vector<int64_t> p1_ck_off, p1_tm_off;           // per listed pair
     std::unordered_map<int64_t, int32_t> p1_index;        // query * nt + target -> listed pair
     DevBuf scan_tmp;  // CUB scan / select scratch
@@ -1860,14 +1862,24 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
                 e->p1_tm_off[k] = tm;
                 tm += (int64_t)bp[k].nbands * tile_count(lq);
             }
-            size_t free_b = 0, total_b = 0;
-            cudaMemGetInfo(&free_b, &total_b);
+            // the driver's free-memory query can be held for tens of
+            // milliseconds by tools polling the GPU: read at most once a second
+            const double now = wall_ms();
+            if (e->p1_free_t < 0 || now - e->p1_free_t > 1000.0) {
+                size_t free_b = 0, total_b = 0;
+                cudaMemGetInfo(&free_b, &total_b);
+                e->p1_free = (int64_t)free_b + (int64_t)e->p1_ck.bytes;
+                e->p1_free_t = now;
+            }
             const int64_t bytes = (ck + tm) * (int64_t)sizeof(int);
-            p1ck = (double)bytes <= 0.35 * (double)(free_b + e->p1_ck.bytes);
+            p1ck = (double)bytes <= 0.35 * (double)e->p1_free;
+            if (p1ck && e->p1_ck.reserve(e->stream, (size_t)bytes) != cudaSuccess) {
+                cudaGetLastError();  // no room after all: the traced pairs get the checkpoint sweep
+                p1ck = false;
+            }
             if (p1ck) {
-                if ((c = e->p1_ck.reserve(e->stream, (size_t)bytes)) != cudaSuccess ||
-                    (c = cudaMemsetAsync(e->p1_ck.as<int>() + ck, 0, (size_t)tm * sizeof(int), e->stream)) != cudaSuccess)
-                    return cuda_fail(e, c, "alloc score-sweep checkpoints");
+                if ((c = cudaMemsetAsync(e->p1_ck.as<int>() + ck, 0, (size_t)tm * sizeof(int), e->stream)) != cudaSuccess)
+                    return cuda_fail(e, c, "reset tile maxima");
                 e->p1_index.clear();
                 for (size_t k = 0; k < np; ++k) {
                     e->p1_tm_off[k] += ck;
