@@ -96,6 +96,32 @@ struct BandArgs {
     unsigned long long wait_ns;  // bound of one wait for the band above
 };
 
+// Byte k of w as a signed int: one prmt whose selector copies byte k into the
+// low byte and replicates its sign bit over the three others (PTX prmt.b32,
+// default mode: the msb of a selector nibble replicates the byte's sign).
+template <int K>
+__device__ __forceinline__ int sbyte(uint32_t w) {
+    constexpr uint32_t sel = K | ((8u | K) << 4) | ((8u | K) << 8) | ((8u | K) << 12);
+    int d;
+    asm("prmt.b32 %0, %1, 0, %2;" : "=r"(d) : "r"(w), "n"(sel));
+    return d;
+}
+
+// Score of row r (0..7) of a lane's profile word pair (r a constant once the
+// row loop is unrolled).
+__device__ __forceinline__ int prof_score(uint2 pw, int r) {
+    switch (r) {
+        case 0: return sbyte<0>(pw.x);
+        case 1: return sbyte<1>(pw.x);
+        case 2: return sbyte<2>(pw.x);
+        case 3: return sbyte<3>(pw.x);
+        case 4: return sbyte<0>(pw.y);
+        case 5: return sbyte<1>(pw.y);
+        case 6: return sbyte<2>(pw.y);
+        default: return sbyte<3>(pw.y);
+    }
+}
+
 template <bool AFFINE, int DIRS>
 __global__ void __launch_bounds__(128, AFFINE ? 5 : 8) band_kernel(KernelArgs A, BandArgs B) {
     static_assert(DIRS < 2 || !AFFINE, "H store and tile form: linear gap only");
@@ -284,7 +310,7 @@ __global__ void __launch_bounds__(128, AFFINE ? 5 : 8) band_kernel(KernelArgs A,
                     const bool stop_ok0 = xin && ypos, stop_ok = xin;
 #pragma unroll
                     for (int r = 0; r < kWarpRows; ++r) {
-                        const int sc = (int)(int8_t)(uint8_t)((r < 4 ? pw.x : pw.y) >> (8 * (r & 3)));
+                        const int sc = prof_score(pw, r);
                         const int left = Hl[r];
                         int h = addmax(left, gap, diag + sc);
                         h = addmax_relu(up, gap, h);
@@ -297,15 +323,15 @@ __global__ void __launch_bounds__(128, AFFINE ? 5 : 8) band_kernel(KernelArgs A,
                             const bool stop = (r > 0 ? stop_ok : stop_ok0) && diag == 0 && code == (kUL << sh);
                             code = stop ? code | (kStopFlag << sh) : code;
                             w0 |= h > 0 ? code : 0u;
-                        } else if constexpr (DIRS == 4) {
-                            tm = max(tm, h);
-                        } else if constexpr (MAXIMA) {
-                            mx = max(mx, h);
                         }
                         diag = left;
                         Hl[r] = h;
                         up = h;
                     }
+                    if constexpr (DIRS == 4)
+                        tm = max3(tm, max3(Hl[0], Hl[1], Hl[2]), max3(Hl[3], Hl[4], max3(Hl[5], Hl[6], Hl[7])));
+                    else if constexpr (DIRS == 0)
+                        mx = max3(mx, max3(Hl[0], Hl[1], Hl[2]), max3(Hl[3], Hl[4], max3(Hl[5], Hl[6], Hl[7])));
                     if constexpr (!MAXIMA) {
                         // candidates: UL cells inside the matrix at or above the
                         // threshold -- rare, so one test of the step's maximum
@@ -358,7 +384,7 @@ __global__ void __launch_bounds__(128, AFFINE ? 5 : 8) band_kernel(KernelArgs A,
                     int mup = up_m, iup = up_i, bdiag = dg_b, mdiag = dg_m;
 #pragma unroll
                     for (int r = 0; r < kWarpRows; ++r) {
-                        const int sc = (int)(int8_t)(uint8_t)((r < 4 ? pw.x : pw.y) >> (8 * (r & 3)));
+                        const int sc = prof_score(pw, r);
                         const int m = addmax_relu(bdiag, sc, neg);
                         const int i = addmax(iup, ext, mup + ge);
                         const int jj = addmax(Jl[r], ext, Ml[r] + ge);

@@ -174,7 +174,7 @@ struct TileView {
                 }
 #pragma unroll
                 for (int r = 0; r < kWarpRows; ++r) {
-                    const int sc = (int)(int8_t)(uint8_t)((r < 4 ? pw.x : pw.y) >> (8 * (r & 3)));
+                    const int sc = prof_score(pw, r);
                     const int left = Hl[r];
                     int h = addmax(left, gap, diag + sc);
                     h = addmax_relu(up, gap, h);
