@@ -296,6 +296,8 @@ def roofline(e, w, score, infos, steps):
         dom = {0: "score sweep (score16_chain_kernel / score16_kernel, 16x2 lanes)",
                1: "score sweep (sweep_kernel phase 1, 32-bit lanes)",
                2: "score sweep (band_kernel, bands chained across warps)"}.get(last["score_path"], "score sweep")
+        if last["score_path"] == 2 and last.get("tile_pairs"):
+            dom = "score sweep (band_kernel, bands chained across warps, keeping the tile form's checkpoints)"
         dom_ms, launches = score_ms, sum(i["score_launches"] for i in infos)
         ops = w.cells * OPS_PER_CELL[(mode, "score")] * steps
         per_cell = OPS_PER_CELL[(mode, "score")]
@@ -682,6 +684,7 @@ def run_config(cfg, args, device, world, flush, sampler, headline):
                       "starting_points": last["starting_points"], "hits": last["hits"],
                       "memory_waves": last["waves"],
                       "trace_store": "16-bit H per cell" if last.get("trace_store") else "4-bit cell codes",
+                      "tile_form_pairs": int(last.get("tile_pairs", 0)),
                       "score_lanes": "targets" if last["orientation"] else "queries",
                       "trace_lanes": "targets" if last["trace_orientation"] else "queries",
                       "minimum_score": w.settings.minimum_score,
