@@ -139,8 +139,9 @@ int pw_set_scoring(pw_engine* e, const float* matrix, int dim, int char_offset, 
                    double filter_factor);
 
 /* Query sequences (the x axis; records_seqs of SmithWaterman.align_sequences,
- * SmithWaterman.py:441).  residues: all sequences concatenated, upper-cased,
- * unpadded; offsets: n + 1 entries.  id_keys: one int per record, equal for
+ * SmithWaterman.py:441).  residues: all sequences concatenated, unpadded,
+ * upper-cased (the engine upper-cases ASCII letters itself; other bytes are
+ * kept as given); offsets: n + 1 entries.  id_keys: one int per record, equal for
  * records whose ids are equal (same-id pairs are skipped,
  * SmithWaterman.py:752-755).  Replaces the query half of copy_sequences
  * (SmithWatermanCuda.py:176-184). */
@@ -260,6 +261,11 @@ int pw_get_pair_max(pw_engine* e, float* out, int64_t n);
  * points.  strbuf receives the alignment strings (info->string_bytes); a null
  * strbuf copies the hit records only. */
 int pw_get_hits(pw_engine* e, pw_hit* hits, int64_t max_hits, char* strbuf, int64_t strbuf_bytes);
+
+/* The same records and strings without a copy: pointers into the engine's own
+ * host copies, valid until the next pw_align, pw_set_* or pw_destroy on this
+ * engine (the driver turns them into its Hit objects at once). */
+int pw_get_hits_view(pw_engine* e, const pw_hit** hits, int64_t* n_hits, const char** strbuf, int64_t* strbuf_bytes);
 
 /* Starting points of the last pw_align (StartingPoint layout of
  * default_main.cu:66-76, 36 bytes each) in emission order; `sequence` and

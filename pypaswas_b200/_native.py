@@ -56,7 +56,7 @@ PW_REUSE_PLAN = 4
 # symbols the header declares, checked by the CPU test-suite
 EXPORTED_SYMBOLS = (
     "pw_create", "pw_destroy", "pw_last_error", "pw_device_free_memory", "pw_set_scoring",
-    "pw_set_queries", "pw_set_targets", "pw_align", "pw_get_pair_max", "pw_get_hits",
+    "pw_set_queries", "pw_set_targets", "pw_align", "pw_get_pair_max", "pw_get_hits", "pw_get_hits_view",
     "pw_get_starting_points", "pw_last_launch_count", "pw_measure_int_peak", "pw_score_max_noalloc",
     "pw_set_wave_limit", "pw_set_tuning", "pw_set_pairs", "pw_server_create", "pw_server_destroy", "pw_server_last_error", "pw_server_set_scoring",
     "pw_server_load_db", "pw_server_submit", "pw_server_wait", "pw_server_top_hits", "pw_server_hits",
@@ -142,6 +142,7 @@ def bind(lib):
         "pw_align": (ctypes.c_int, [P, U32, I64, ctypes.POINTER(PwRunInfo)]),
         "pw_get_pair_max": (ctypes.c_int, [P, P, I64]),
         "pw_get_hits": (ctypes.c_int, [P, P, I64, P, I64]),
+        "pw_get_hits_view": (ctypes.c_int, [P, P, P, P, P]),
         "pw_get_starting_points": (ctypes.c_int, [P, P, I64, ctypes.POINTER(I64)]),
         "pw_last_launch_count": (ctypes.c_int, [P, ctypes.POINTER(I64)]),
         "pw_measure_int_peak": (ctypes.c_int, [P, ctypes.POINTER(D), ctypes.POINTER(D), ctypes.POINTER(D)]),
@@ -342,6 +343,23 @@ class Engine(object):
                                                             ctypes.cast(ctypes.c_char_p(text), ctypes.c_void_p),
                                                             nb), "pw_get_hits")
         return hits, text
+
+    def hits_view(self):
+        """(hit records, strings) of the last align without a copy: a numpy
+        view and a memoryview of the engine's own host copies, valid until the
+        next align or set_* call on this engine."""
+        hp, n, sp, nb = ctypes.c_void_p(), ctypes.c_int64(), ctypes.c_void_p(), ctypes.c_int64()
+        _check(self.lib, self.handle, self.lib.pw_get_hits_view(self.handle, ctypes.byref(hp), ctypes.byref(n),
+                                                                 ctypes.byref(sp), ctypes.byref(nb)),
+               "pw_get_hits_view")
+        if n.value == 0:
+            hits = np.zeros(0, dtype=HIT_DTYPE)
+        else:
+            raw = (ctypes.c_char * (n.value * HIT_DTYPE.itemsize)).from_address(hp.value)
+            hits = np.frombuffer(raw, dtype=HIT_DTYPE)
+        strings = memoryview((ctypes.c_char * nb.value).from_address(sp.value)).cast("B") if nb.value else \
+            memoryview(b"")
+        return hits, strings
 
     def starting_points(self):
         n = ctypes.c_int64()

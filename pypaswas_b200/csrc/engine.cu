@@ -20,6 +20,7 @@
 #include <cstdio>
 #include <cstring>
 #include <unordered_map>
+#include <atomic>
 #include <numeric>
 #include <queue>
 #include <string>
@@ -416,6 +417,27 @@ extern "C" int pw_set_scoring(pw_engine* e, const float* matrix, int dim, int ch
     return PW_OK;
 }
 
+// The residues as the engine keeps them: ASCII letters upper-cased (the
+// reference upper-cases every sequence before its kernels see it), on host
+// threads.  Returns whether dst already held exactly that.
+static bool copy_upper(std::vector<uint8_t>& dst, const uint8_t* src, int64_t n) {
+    const bool same_size = (int64_t)dst.size() == n;
+    std::atomic<bool> differ{!same_size};
+    if (!same_size) dst.resize((size_t)n);
+    parallel_for(n, [&](int64_t i0, int64_t i1) {
+        uint8_t* d = dst.data();
+        bool diff = false;
+        for (int64_t i = i0; i < i1; ++i) {
+            const uint8_t c = src[i];
+            const uint8_t u = (uint8_t)(c - (((uint8_t)(c - 'a') < 26u) ? 32 : 0));
+            diff |= d[i] != u;
+            d[i] = u;
+        }
+        if (diff) differ.store(true, std::memory_order_relaxed);
+    }, (int64_t)1 << 22);
+    return !differ.load();
+}
+
 static int set_seqs(pw_engine* e, HostSeqs& S, const uint8_t* residues, const int64_t* offsets, int32_t n,
                     const int32_t* id_keys) {
     if (!e) return PW_ERR_ARG;
@@ -430,12 +452,11 @@ static int set_seqs(pw_engine* e, HostSeqs& S, const uint8_t* residues, const in
     if (total > 0 && !residues) return fail(e, PW_ERR_ARG, "residues missing");
     // the same set again (a resident database handed in once more): keep the
     // device copy
-    if (S.set && S.n == n && (int64_t)S.raw.size() == total && S.off.size() == (size_t)(n > 0 ? n + 1 : 1) &&
-        (total == 0 || std::memcmp(S.raw.data(), residues, (size_t)total) == 0) &&
+    const bool same_raw = copy_upper(S.raw, residues, total);
+    if (S.set && S.n == n && same_raw && S.off.size() == (size_t)(n > 0 ? n + 1 : 1) &&
         (n == 0 || (std::memcmp(S.off.data(), offsets, (size_t)(n + 1) * sizeof(int64_t)) == 0 &&
                     std::memcmp(S.key.data(), id_keys, (size_t)n * sizeof(int32_t)) == 0)))
         return PW_OK;
-    S.raw.assign(residues, residues + total);
     S.off.assign(offsets, offsets + (n > 0 ? n + 1 : 0));
     if (n == 0) S.off.assign(1, 0);
     S.key.assign(id_keys, id_keys + n);
@@ -2806,6 +2827,16 @@ extern "C" int pw_get_pair_max(pw_engine* e, float* out, int64_t n) {
         if (rc != PW_OK) return rc;
     }
     std::memcpy(out, e->h_pair_max.data(), e->h_pair_max.size() * sizeof(float));
+    return PW_OK;
+}
+
+extern "C" int pw_get_hits_view(pw_engine* e, const pw_hit** hits, int64_t* n_hits, const char** strbuf,
+                                int64_t* strbuf_bytes) {
+    if (!e || !hits || !n_hits || !strbuf || !strbuf_bytes) return PW_ERR_ARG;
+    *hits = e->h_hits.empty() ? nullptr : e->h_hits.data();
+    *n_hits = (int64_t)e->h_hits.size();
+    *strbuf = e->h_strings.empty() ? nullptr : (const char*)e->h_strings.data();
+    *strbuf_bytes = (int64_t)e->h_strings.size();
     return PW_OK;
 }
 

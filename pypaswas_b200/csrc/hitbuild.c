@@ -13,7 +13,7 @@
  * build(hits, strbuf, sequences, targets, q_ids, t_ids, q_len, t_len, q_pos,
  *       t_pos, thresholds, hit_type, logger, hits_dict, real_dict)
  *   hits        buffer of pw_hit records (48 bytes each)
- *   strbuf      bytes: the alignment strings, n_cols bytes each at str_offset
+ *   strbuf      a bytes-like buffer: the alignment strings, n_cols bytes each at str_offset
  *   sequences, targets   the record lists the hit indices refer to
  *   q_ids, t_ids         lists of their ids
  *   q_len, t_len         buffers of int64 original lengths
@@ -137,7 +137,7 @@ static PyObject* build(PyObject* self, PyObject* args) {
     PyObject *hits_obj, *strbuf, *seqs, *tgts, *q_ids, *t_ids, *qlen_obj, *tlen_obj, *qpos_obj, *tpos_obj;
     PyObject *thr, *hit_type, *logger, *hits_d, *real_d;
     (void)self;
-    if (!PyArg_ParseTuple(args, "OSO!O!O!O!OOOOOOOO!O!", &hits_obj, &strbuf, &PyList_Type, &seqs, &PyList_Type,
+    if (!PyArg_ParseTuple(args, "OOO!O!O!O!OOOOOOOO!O!", &hits_obj, &strbuf, &PyList_Type, &seqs, &PyList_Type,
                           &tgts, &PyList_Type, &q_ids, &PyList_Type, &t_ids, &qlen_obj, &tlen_obj, &qpos_obj,
                           &tpos_obj, &thr, &hit_type, &logger, &PyDict_Type, &hits_d, &PyDict_Type, &real_d))
         return NULL;
@@ -152,8 +152,12 @@ static PyObject* build(PyObject* self, PyObject* args) {
         PyErr_SetString(PyExc_ValueError, "id lists do not match the record lists");
         return NULL;
     }
-    Py_buffer hb, qlb, tlb, qpb, tpb;
-    if (PyObject_GetBuffer(hits_obj, &hb, PyBUF_C_CONTIGUOUS) < 0) return NULL;
+    Py_buffer hb, qlb, tlb, qpb, tpb, sb;
+    if (PyObject_GetBuffer(strbuf, &sb, PyBUF_SIMPLE) < 0) return NULL;
+    if (PyObject_GetBuffer(hits_obj, &hb, PyBUF_C_CONTIGUOUS) < 0) {
+        PyBuffer_Release(&sb);
+        return NULL;
+    }
     int have[4] = {0, 0, 0, 0};
     int gc_was_on = 0;
     PyObject* result = NULL;
@@ -177,8 +181,8 @@ static PyObject* build(PyObject* self, PyObject* args) {
         const Py_ssize_t n = hb.len / (Py_ssize_t)sizeof(HitRec);
         const int64_t *ql = (const int64_t*)qlb.buf, *tl = (const int64_t*)tlb.buf;
         const int64_t *qp = (const int64_t*)qpb.buf, *tp = (const int64_t*)tpb.buf;
-        const char* text = PyBytes_AS_STRING(strbuf);
-        const Py_ssize_t text_len = PyBytes_GET_SIZE(strbuf);
+        const char* text = (const char*)sb.buf;
+        const Py_ssize_t text_len = sb.len;
         /* every location valid (Hit._is_a_valid_location), else the caller's path */
         for (Py_ssize_t k = 0; k < n; ++k) {
             const HitRec* r = &H[k];
@@ -287,6 +291,7 @@ static PyObject* build(PyObject* self, PyObject* args) {
     }
 done:
     if (gc_was_on) PyGC_Enable();
+    PyBuffer_Release(&sb);
     PyBuffer_Release(&hb);
     if (have[0]) PyBuffer_Release(&qlb);
     if (have[1]) PyBuffer_Release(&tlb);

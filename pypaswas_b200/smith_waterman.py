@@ -70,12 +70,20 @@ def _filter_factor(settings):
 
 
 def _packed(records):
-    """(residues uint8, offsets int64) of the records' upper-cased sequences."""
-    seqs = [str(r.seq) for r in records]
+    """(residues uint8, offsets int64) of the records' upper-cased sequences.
+    ASCII text goes as it is (the engine upper-cases ASCII letters in its own
+    copy); other text is upper-cased here, per record where a character's
+    upper case is longer."""
+    seqs = [r.seq if isinstance(r.seq, str) else str(r.seq) for r in records]
     lens = np.fromiter(map(len, seqs), dtype=np.int64, count=len(seqs))
     off = np.zeros(len(seqs) + 1, dtype=np.int64)
     np.cumsum(lens, out=off[1:])
-    text = "".join(seqs).upper()
+    text = "".join(seqs)
+    if text.isascii():
+        data = text.encode("ascii")
+        return np.frombuffer(data, dtype=np.uint8) if data else np.zeros(0, np.uint8), off
+    seqs = [str(s) for s in seqs]
+    text = text.upper()
     if len(text) != off[-1]:  # a character whose upper case is longer: per record
         text = "".join(s.upper() for s in seqs)
         lens = np.fromiter((len(s.upper()) for s in seqs), dtype=np.int64, count=len(seqs))
@@ -198,7 +206,8 @@ class SmithWatermanB200(object):
             self.logger.warning("Too many hits returned. Skipping the rest. Please set lower_limit_score "
                                 "higher in config.")
         t_align = time.time()
-        hits, strbuf = self.engine.hits()
+        # the engine's own host copies, turned into Hit objects before its next call
+        hits, strbuf = self.engine.hits_view()
         t2 = time.time()
         self.last_h2d_bytes = int(info.h2d_bytes)  # counted by the engine, copy by copy
         self.last_d2h_bytes = int(info.d2h_bytes)
@@ -263,7 +272,7 @@ class SmithWatermanB200(object):
         if type(hit_list) is HitList and not _logs_hits(hit_list):
             # the same objects, built in native code (csrc/hitbuild.c); None
             # means an invalid location, reported below by the checked path
-            kept = _hitbuild().build(np.ascontiguousarray(hits, dtype=_native.HIT_DTYPE), bytes(strbuf),
+            kept = _hitbuild().build(np.ascontiguousarray(hits, dtype=_native.HIT_DTYPE), strbuf,
                                      list(sequences), list(targets), [r.id for r in sequences],
                                      [r.id for r in targets], qlen, tlen, sp, tp, self._filter_thresholds(), Hit,
                                      self.logger, hit_list.hits, hit_list.real_hits)
@@ -281,7 +290,7 @@ class SmithWatermanB200(object):
         t1 = hits["t_end"].astype(np.int64) + tp[t_col]
         ql, tl = qlen[q_col], tlen[t_col]
         valid = ((0 <= s0) & (s0 < s1) & (s1 < ql) & (0 <= t0) & (t0 < t1) & (t1 < tl)).all()
-        text = strbuf.decode("latin-1")
+        text = bytes(strbuf).decode("latin-1")
         if not valid:
             self._build_hits_checked(hits, text, sequences, targets, hit_list, s0, s1, t0, t1)
             return
