@@ -92,7 +92,9 @@ def parse():
     ap.add_argument("--serve-streams", type=int, default=3,
                     help="arrival streams per offered load (different seeds); the report gives the median p99")
     ap.add_argument("--serve-workers", type=int, default=2)
-    ap.add_argument("--serve-max-batch", type=int, default=32)
+    ap.add_argument("--serve-max-batch", type=int, default=6)
+    ap.add_argument("--serve-max-residues", type=int, default=0,
+                    help="query residues per serving batch (0: no limit)")
     ap.add_argument("--serve-policy", type=int, default=1, help="0 arrival order, 1 shortest first with aging")
     return ap.parse_args()
 
@@ -598,7 +600,7 @@ def parity_leg(w, jobs, idx, oracle_res, device):
 
 
 # ------------------------------------------------------------------ serving
-def serve_leg(device, seconds, loads, workers=2, max_batch=32, policy=1, streams=3, age_ms=25):
+def serve_leg(device, seconds, loads, workers=2, max_batch=32, policy=1, streams=3, age_ms=25, max_residues=0):
     """Serving configuration: a resident database of 100,000 protein sequences
     (log-normal lengths, median 300, 50-1,500 aa), Poisson arrivals of single
     queries (log-normal, median 300, max 5,000 aa), 70% top-10 by pair maximum
@@ -615,6 +617,7 @@ def serve_leg(device, seconds, loads, workers=2, max_batch=32, policy=1, streams
         srv.load_db(db)
         srv.tune(_native_const("PW_SERVE_TUNE_POLICY"), policy)
         srv.tune(_native_const("PW_SERVE_TUNE_AGE_MS"), age_ms)
+        srv.tune(_native_const("PW_SERVE_TUNE_MAX_RESIDUES"), max_residues)
         serving.run_arrivals(srv, workloads.query_stream(seed=8, n=16, rate_hz=1e9))
         peak = serving.run_arrivals(srv, workloads.query_stream(seed=7, n=64, rate_hz=1e9))
         probe = workloads.query_stream(seed=9, n=4000, rate_hz=1.0)
@@ -638,7 +641,8 @@ def serve_leg(device, seconds, loads, workers=2, max_batch=32, policy=1, streams
     finally:
         srv.close()
     return {"db": "%d sequences, %d residues, resident" % (len(db), srv.db_residues),
-            "workers": workers, "max_batch": max_batch, "policy": ["arrival order", "shortest first"][policy],
+            "workers": workers, "max_batch": max_batch, "max_residues": max_residues,
+            "policy": ["arrival order", "shortest first"][policy],
             "batched_peak_gcups": peak["gcups"], "seconds_per_stream": seconds, "streams_per_load": streams,
             "sweep": sweep}
 
@@ -775,7 +779,8 @@ def main():
         if not args.no_serve and rank == 0 and world == 1 and args.config == 2:
             out["serve"] = serve_leg(local, args.serve_seconds, [float(x) for x in args.serve_loads.split(",")],
                                      workers=args.serve_workers, max_batch=args.serve_max_batch,
-                                     policy=args.serve_policy, streams=args.serve_streams)
+                                     policy=args.serve_policy, streams=args.serve_streams,
+                                     max_residues=args.serve_max_residues)
     finally:
         sampler.stop()
     if rank == 0:

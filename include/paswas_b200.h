@@ -357,10 +357,15 @@ int pw_server_hits(pw_server* s, int64_t ticket, pw_hit* hits, int64_t max_hits,
  *                          goes first (no request starves)
  *   PW_SERVE_TUNE_AGE_MS   the waiting time after which policy 1 serves a
  *                          request in arrival order (default 25)
- *   PW_SERVE_TUNE_MAX_BATCH  requests per batch (as at pw_server_create) */
+ *   PW_SERVE_TUNE_MAX_BATCH  requests per batch (as at pw_server_create)
+ *   PW_SERVE_TUNE_MAX_RESIDUES  query residues per batch (0: no limit): a
+ *                          batch's requests all finish when it does, so this
+ *                          bounds the run time a request can wait for; the
+ *                          first request of a batch always joins */
 #define PW_SERVE_TUNE_POLICY 100
 #define PW_SERVE_TUNE_AGE_MS 101
 #define PW_SERVE_TUNE_MAX_BATCH 102
+#define PW_SERVE_TUNE_MAX_RESIDUES 103
 int pw_server_tune(pw_server* s, int key, int64_t value);
 /* Frees a finished request's results. */
 int pw_server_release(pw_server* s, int64_t ticket);

@@ -43,6 +43,7 @@ PW_TUNE_TILE_TRACE = 9
 PW_SERVE_TUNE_POLICY = 100
 PW_SERVE_TUNE_AGE_MS = 101
 PW_SERVE_TUNE_MAX_BATCH = 102
+PW_SERVE_TUNE_MAX_RESIDUES = 103
 PW_FORMAT_FASTA = 0
 PW_FORMAT_FASTQ = 1
 PW_RECORDS_AS_READ = 0

@@ -67,6 +67,7 @@ struct pw_server {
     int max_batch = 16;
     int policy = 1;              // PW_SERVE_TUNE_POLICY (shortest first with aging)
     double age_ms = 25.0;        // PW_SERVE_TUNE_AGE_MS
+    int64_t max_residues = 0;    // PW_SERVE_TUNE_MAX_RESIDUES (0: no limit)
     int64_t budget = 0;          // direction-matrix bytes shared by all traceback batches
     int64_t in_use = 0;          // reserved by running batches
     int64_t peak_in_use = 0;
@@ -124,8 +125,13 @@ std::vector<Request*> take_batch(pw_server* s, int64_t* reserve) {
     }
     const int64_t free_b = s->budget - s->in_use;
     bool traceback = false;
+    int64_t residues = 0;
     for (auto it = s->pending.begin(); it != s->pending.end() && (int)batch.size() < s->max_batch;) {
         Request* r = *it;
+        if (s->max_residues > 0 && !batch.empty() && residues + (int64_t)r->residues.size() > s->max_residues) {
+            ++it;  // would make the batch too long a run for the requests in it
+            continue;
+        }
         if (r->mode == PW_SERVE_TRACEBACK) {
             const int64_t need = std::min(r->est_bytes, s->budget);
             const bool alone = *reserve == 0 && s->in_use == 0;
@@ -137,6 +143,7 @@ std::vector<Request*> take_batch(pw_server* s, int64_t* reserve) {
             traceback = true;
         }
         batch.push_back(r);
+        residues += (int64_t)r->residues.size();
         it = s->pending.erase(it);
     }
     *reserve = traceback ? std::max<int64_t>(std::min(*reserve, s->budget), 1) : 0;
@@ -365,6 +372,8 @@ extern "C" int pw_server_tune(pw_server* s, int key, int64_t value) {
             s->age_ms = (double)value;
         } else if (key == PW_SERVE_TUNE_MAX_BATCH && value >= 1 && value <= 4096) {
             s->max_batch = (int)value;
+        } else if (key == PW_SERVE_TUNE_MAX_RESIDUES && value >= 0) {
+            s->max_residues = value;
         } else {
             s->err = "unknown server setting or value out of range";
             return PW_ERR_ARG;
