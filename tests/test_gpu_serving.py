@@ -102,6 +102,30 @@ def test_direction_memory_admission_keeps_reservations_within_budget():
     assert [_strip(r) for r in res] == [_direct(db, st, r) for r in reqs]
 
 
+def test_residue_cap_limits_batches_and_keeps_results():
+    """PW_SERVE_TUNE_MAX_RESIDUES: a burst of requests is batched only while
+    the batch's query residues stay within the cap (a longer request runs
+    alone); results equal lone runs."""
+    db = workloads.protein_database(seed=26, n_seqs=1200)
+    st = workloads.Settings(**SETTINGS)
+    reqs = _requests(db, 16, seed=27)
+    cap = 500
+    srv = serving.Server(st, workers=1, max_batch=16)
+    try:
+        srv.load_db(db)
+        srv.tune(_native.PW_SERVE_TUNE_MAX_RESIDUES, cap)
+        tickets = [srv.submit(r[2], traceback=r[3]) for r in reqs]
+        res = [srv.result(t) for t in tickets]
+    finally:
+        srv.close()
+    assert [_strip(r) for r in res] == [_direct(db, st, r) for r in reqs]
+    lens = [len(r[2]) for r in reqs]
+    # a request longer than the cap always runs alone; batches of several existed
+    assert all(r["info"]["batch_queries"] == 1 for r, n in zip(res, lens) if n > cap)
+    assert max(r["info"]["batch_queries"] for r in res) > 1
+    assert max(r["info"]["batch_queries"] for r in res) <= cap // min(lens)
+
+
 def test_arrival_stream_report():
     db = workloads.protein_database(seed=25, n_seqs=2000)
     st = workloads.Settings(**SETTINGS)
