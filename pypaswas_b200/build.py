@@ -12,7 +12,7 @@ REPO_DIR = os.path.dirname(PACKAGE_DIR)
 CSRC = os.path.join(PACKAGE_DIR, "csrc")
 SOURCES = [os.path.join(CSRC, "engine.cu"), os.path.join(CSRC, "noalloc.cu"), os.path.join(CSRC, "server.cpp"),
            os.path.join(CSRC, "format.cpp"), os.path.join(CSRC, "reader.cpp")]
-DEPENDS = SOURCES + [os.path.join(CSRC, f) for f in ("pw_device.cuh", "pw_kernels.cuh", "pw_score16.cuh", "pw_band.cuh", "pw_tiles.cuh", "pw_plan.h", "pw_finish.cuh", "pw_host.h", "server.cpp")] + [
+DEPENDS = SOURCES + [os.path.join(CSRC, f) for f in ("pw_device.cuh", "pw_kernels.cuh", "pw_score16.cuh", "pw_band.cuh", "pw_band16.cuh", "pw_tiles.cuh", "pw_plan.h", "pw_finish.cuh", "pw_host.h", "server.cpp")] + [
     os.path.join(REPO_DIR, "include", "paswas_b200.h")]
 LIBRARY = os.path.join(PACKAGE_DIR, "libpaswas_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

@@ -20,6 +20,7 @@
 #include <cstdio>
 #include <cstring>
 #include <unordered_map>
+#include <map>
 #include <atomic>
 #include <numeric>
 #include <queue>
@@ -33,6 +34,7 @@
 #include "pw_score16.cuh"
 #include "pw_band.cuh"
 #include "pw_tiles.cuh"
+#include "pw_band16.cuh"
 #include "pw_plan.h"
 #include "pw_finish.cuh"
 #include "pw_host.h"
@@ -240,6 +242,7 @@ struct pw_engine {
     DevBuf band_pairs, band_entries, band_prog, band_max, band_ring, band_out;  // band sweep (pw_band.cuh)
     DevBuf tile_ck, tile_marks, tile_pairs, slot_tile;                        // tile form (pw_tiles.cuh)
     DevBuf tile_pairs_alt, tile_sel, tile_cnt, tile_acc, tile_scratch, tile_ops;
+    DevBuf band_over;                                                         // band16_kernel: pairs past 16 bits
     // explicit pairs: the score sweep's tile-form checkpoints (band_kernel<false, 4>)
     DevBuf p1_ck;
     bool p1_tiles = false;
@@ -1578,6 +1581,36 @@ static cudaError_t finish_hits(pw_engine* e, int64_t n, int64_t* str_bytes) {
     return cudaSuccess;
 }
 
+// Queue entries (pair, band, queue index of the band above) of band chains:
+// pair k has nbands[k] bands of steps[k] steps, pairs in priority order.
+static std::vector<int4> band_queue(const std::vector<int>& nbands, const std::vector<int64_t>& steps, int warps) {
+    std::vector<int4> entries;
+    if ((int64_t)nbands.size() * 2 >= warps) {
+        // many pairs: band-major order (every band 0, then every band 1, ...,
+        // longest pairs first within a band); a band's predecessor was handed
+        // out at least a whole band generation earlier, so nobody waits long
+        int maxb = 0;
+        for (int nb : nbands) maxb = std::max(maxb, nb);
+        std::vector<int32_t> last(nbands.size(), -1);
+        for (int b = 0; b < maxb; ++b)
+            for (size_t k = 0; k < nbands.size(); ++k)
+                if (b < nbands[k]) {
+                    entries.push_back(make_int4((int)k, b, last[k], 0));
+                    last[k] = (int32_t)entries.size() - 1;
+                }
+    } else {
+        // few (long) pairs: a list-scheduling plan pipelines each pair's bands
+        ChainPlan plan;
+        plan_chain_queue(nbands, steps, warps, 1, kBandLead, plan);
+        entries.resize(plan.queue.size());
+        for (size_t k = 0; k < plan.queue.size(); ++k) {
+            const PlanEntry& p = plan.queue[k];
+            entries[k] = make_int4(p.item, p.chain >= 0 ? p.strip : 0, p.pred, 0);
+        }
+    }
+    return entries;
+}
+
 // Launches band_kernel over `pairs` (one warp per band, the bands of a pair
 // chained across warps, pw_band.cuh).  DIRS 1: the direction sweep of traced
 // pairs (cell codes), 2: the same storing H (linear gap), 3: the checkpoint
@@ -1625,30 +1658,7 @@ static int run_band_phase(pw_engine* e, KernelArgs A, std::vector<BandPair>& pai
             if (sorted[k].nbands > 1) ring_elems += 2 * (int64_t)e->pr.qlen[sorted[k].q];
         }
     }
-    std::vector<int4> entries;
-    if ((int64_t)sorted.size() * 2 >= warps) {
-        // many pairs: band-major order (every band 0, then every band 1, ...,
-        // longest pairs first within a band); a band's predecessor was handed
-        // out at least a whole band generation earlier, so nobody waits long
-        int maxb = 0;
-        for (const BandPair& bp : sorted) maxb = std::max(maxb, bp.nbands);
-        std::vector<int32_t> last(sorted.size(), -1);
-        for (int b = 0; b < maxb; ++b)
-            for (size_t k = 0; k < sorted.size(); ++k)
-                if (b < sorted[k].nbands) {
-                    entries.push_back(make_int4((int)k, b, last[k], 0));
-                    last[k] = (int32_t)entries.size() - 1;
-                }
-    } else {
-        // few (long) pairs: a list-scheduling plan pipelines each pair's bands
-        ChainPlan plan;
-        plan_chain_queue(nstr, xm, warps, 1, kBandLead, plan);
-        entries.resize(plan.queue.size());
-        for (size_t k = 0; k < plan.queue.size(); ++k) {
-            const PlanEntry& p = plan.queue[k];
-            entries[k] = make_int4(p.item, p.chain >= 0 ? p.strip : 0, p.pred, 0);
-        }
-    }
+    std::vector<int4> entries = band_queue(nstr, xm, warps);
     const size_t n = entries.size();
     if (e->tune[PW_TUNE_STALL_TEST]) {
         // one band below another waits on the spare flag (index n) instead
@@ -1689,6 +1699,86 @@ static int run_band_phase(pw_engine* e, KernelArgs A, std::vector<BandPair>& pai
     cudaEventCreate(&b);
     cudaEventRecord(a, e->stream);
     PW_LAUNCH(kern, grid, 128, smem, e->stream, A, B);
+    e->launches++;
+    cudaEventRecord(b, e->stream);
+    if ((c = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, c, "band sweep launch");
+    int aborted = 0;
+    if ((c = copy_d2h(e, &aborted, e->chain_abort.p, sizeof(int))) != cudaSuccess ||
+        (c = cudaStreamSynchronize(e->stream)) != cudaSuccess)
+        return cuda_fail(e, c, "band sweep");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    if (kernel_ms) *kernel_ms += ms;
+    if (n_launch) ++*n_launch;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (aborted) return fail(e, PW_ERR_KERNEL, "band sweep: a band waited too long for the band above");
+    return PW_OK;
+}
+
+// Launches band16_kernel over `pairs` (two explicit pairs a chain, 16x2;
+// pw_band16.cuh): maxima into band_out by pair-list index, the pairs past the
+// 16-bit limit flagged in band_over, checkpoints and tile maxima into p1_ck.
+static int run_band16_phase(pw_engine* e, KernelArgs A, const std::vector<BandPair2>& pairs, int limit,
+                            double* kernel_ms, int* n_launch) {
+    if (pairs.empty()) return PW_OK;
+    const int smem = 4 * kWarp * (A.P.alpha + 1) * kWarpRows * 4;
+    cudaError_t c;
+    if (smem > 48 * 1024 &&
+        (c = cudaFuncSetAttribute(band16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
+        return cuda_fail(e, c, "band sweep smem");
+    int per_sm = 0;
+    if ((c = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, band16_kernel, 128, smem)) != cudaSuccess)
+        return cuda_fail(e, c, "occupancy");
+    per_sm = std::max(1, std::min(per_sm, 16));
+    const int warps = grid_cap(e, per_sm) * 4;
+    std::vector<int> order(pairs.size());
+    std::iota(order.begin(), order.end(), 0);
+    std::vector<int64_t> steps(pairs.size());
+    for (size_t k = 0; k < pairs.size(); ++k) steps[k] = (int64_t)e->pr.qlen[pairs[k].q] + kWarp - 1;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        return steps[x] * pairs[x].nbands > steps[y] * pairs[y].nbands;
+    });
+    std::vector<BandPair2> sorted(pairs.size());
+    std::vector<int> nstr(pairs.size());
+    std::vector<int64_t> xm(pairs.size());
+    for (size_t k = 0; k < order.size(); ++k) {
+        sorted[k] = pairs[order[k]];
+        nstr[k] = std::max(1, sorted[k].nbands);
+        xm[k] = steps[order[k]];
+    }
+    const std::vector<int4> entries = band_queue(nstr, xm, warps);
+    const size_t n = entries.size();
+    if ((c = upload(e, e->band_pairs, sorted)) != cudaSuccess) return cuda_fail(e, c, "upload band pairs");
+    if ((c = upload(e, e->band_entries, entries)) != cudaSuccess) return cuda_fail(e, c, "upload band queue");
+    if ((c = e->band_prog.reserve(e->stream, (n + 1) * sizeof(int))) != cudaSuccess ||
+        (c = e->band_max.reserve(e->stream, n * sizeof(int2))) != cudaSuccess ||
+        (c = e->chain_abort.reserve(e->stream, sizeof(int))) != cudaSuccess)
+        return cuda_fail(e, c, "alloc band state");
+    if ((c = cudaMemsetAsync(e->band_prog.p, 0, (n + 1) * sizeof(int), e->stream)) != cudaSuccess ||
+        (c = cudaMemsetAsync(e->chain_abort.p, 0, sizeof(int), e->stream)) != cudaSuccess ||
+        (c = cudaMemsetAsync(e->counter.as<int>() + kNumClasses, 0, sizeof(int), e->stream)) != cudaSuccess)
+        return cuda_fail(e, c, "reset band state");
+    BandArgs2 B;
+    memset(&B, 0, sizeof(B));
+    B.entries = e->band_entries.as<int4>();
+    B.pairs = e->band_pairs.as<BandPair2>();
+    B.n_entries = (int)n;
+    B.counter = e->counter.as<int>() + kNumClasses;
+    B.progress = e->band_prog.as<int>();
+    B.run_max = e->band_max.as<int2>();
+    B.abort_flag = e->chain_abort.as<int>();
+    B.max_out = e->band_out.as<float>();
+    B.over = e->band_over.as<int>();
+    B.ck = e->p1_ck.as<int>();
+    B.limit = limit;
+    B.wait_ns = wait_limit(e);
+    const int grid = std::max(1, std::min(grid_cap(e, per_sm), (int)((n + 3) / 4)));
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, e->stream);
+    PW_LAUNCH(band16_kernel, grid, 128, smem, e->stream, A, B);
     e->launches++;
     cudaEventRecord(b, e->stream);
     if ((c = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, c, "band sweep launch");
@@ -1911,8 +2001,67 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
             }
         }
         cudaEventRecord(e->ev[0], e->stream);
-        rc = p1ck ? run_band_phase<4>(e, A, bp, &inf.score_kernel_ms, &inf.score_launches)
-                  : run_band_phase<0>(e, A, bp, &inf.score_kernel_ms, &inf.score_launches);
+        if (p1ck) {
+            // pairs that share their query and their target's length go two to
+            // a 16x2 sweep (pw_band16.cuh); the others, and pairs whose maximum
+            // passes the 16-bit limit, run on 32-bit lanes
+            const int limit = 32767 - (int)std::ceil(A.P.highest);
+            std::vector<BandPair2> bp2;
+            std::vector<BandPair> bp1;
+            if (!(flags & PW_FLAG_INT32) && limit > 0) {
+                std::map<std::pair<int32_t, int32_t>, size_t> open;
+                std::vector<char> paired(np, 0);
+                for (size_t k = 0; k < np; ++k) {
+                    const auto key = std::make_pair(bp[k].q, tlen[bp[k].t]);
+                    const auto f = open.find(key);
+                    if (f == open.end()) {
+                        open.emplace(key, k);
+                        continue;
+                    }
+                    const size_t j = f->second;
+                    open.erase(f);
+                    BandPair2 p2;
+                    memset(&p2, 0, sizeof(p2));
+                    p2.q = bp[j].q;
+                    p2.t[0] = bp[j].t;
+                    p2.t[1] = bp[k].t;
+                    p2.nbands = bp[j].nbands;
+                    p2.slot[0] = (int64_t)j;
+                    p2.slot[1] = (int64_t)k;
+                    p2.ck[0] = bp[j].dir_base;
+                    p2.ck[1] = bp[k].dir_base;
+                    p2.tm[0] = bp[j].ring_off;
+                    p2.tm[1] = bp[k].ring_off;
+                    bp2.push_back(p2);
+                    paired[j] = paired[k] = 1;
+                }
+                for (size_t k = 0; k < np; ++k)
+                    if (!paired[k]) bp1.push_back(bp[k]);
+            } else {
+                bp1 = bp;
+            }
+            if (!bp2.empty()) {
+                if ((c = e->band_over.reserve(e->stream, np * sizeof(int))) != cudaSuccess ||
+                    (c = cudaMemsetAsync(e->band_over.p, 0, np * sizeof(int), e->stream)) != cudaSuccess)
+                    return cuda_fail(e, c, "alloc band flags");
+                rc = run_band16_phase(e, A, bp2, limit, &inf.score_kernel_ms, &inf.score_launches);
+                if (rc != PW_OK) return rc;
+                std::vector<int32_t> over;
+                if ((c = download(e, over, e->band_over.p, np)) != cudaSuccess) return cuda_fail(e, c, "copy band flags");
+                for (size_t k = 0; k < np; ++k) {
+                    if (!over[k]) continue;
+                    const int lq = qlen[bp[k].q];
+                    if ((c = cudaMemsetAsync(e->p1_ck.as<int>() + bp[k].ring_off, 0,
+                                             (size_t)bp[k].nbands * tile_count(lq) * sizeof(int), e->stream)) != cudaSuccess)
+                        return cuda_fail(e, c, "reset tile maxima");
+                    bp1.push_back(bp[k]);
+                    inf.overflow_pairs++;
+                }
+            }
+            rc = run_band_phase<4>(e, A, bp1, &inf.score_kernel_ms, &inf.score_launches);
+        } else {
+            rc = run_band_phase<0>(e, A, bp, &inf.score_kernel_ms, &inf.score_launches);
+        }
         if (rc != PW_OK) return rc;
         e->p1_tiles = p1ck;
         cudaEventRecord(e->ev[1], e->stream);

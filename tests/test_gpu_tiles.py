@@ -129,3 +129,72 @@ def test_tile_form_next_to_strip_pairs(engine_lib, oracle_mod):
     st = cases.Settings(minimum_score="6", lower_limit_score="0.5", filter_factor="0.05")
     o, info = _both(engine_lib, oracle_mod, queries, targets, st)
     assert 0 < info.warp_pairs < info.traced_pairs
+
+
+def _pairs_run(engine_lib, queries, targets, pairs, st, tuning=None):
+    score = scores.make_score(st)
+    e = _native.Engine(0, lib=engine_lib)
+    try:
+        configure(e, score, st)
+        e.set_queries([q.encode() for q in queries], np.arange(len(queries)))
+        e.set_targets([t.encode() for t in targets], np.arange(len(targets)) + len(queries))
+        for k, v in (tuning or {}).items():
+            e.set_tuning(k, v)
+        e.set_pairs([a for a, _ in pairs], [b for _, b in pairs])
+        info = e.align()
+        return e.pair_max(), decode_hits(*e.hits()), info
+    finally:
+        e.close()
+
+
+def _oracle_pairs(oracle_mod, queries, targets, pairs, st):
+    score = scores.make_score(st)
+    p = cases.oracle_params(oracle_mod, score)
+    hits, maxima = [], {}
+    for qi, ti in pairs:
+        pos = cases.pos_scores(score, st, [queries[qi]], [targets[ti]])
+        o = oracle_mod.run(p, [queries[qi]], [targets[ti]], pos, float(st.minimum_score))
+        maxima[(qi, ti)] = float(o["pair_max"][0, 0])
+        hits += [dict(h, query=qi, target=ti) for h in o["hits"]]
+    return maxima, hits
+
+
+@pytest.mark.parametrize("big", [False, True])
+def test_pairs_two_at_a_time_on_16x2_lanes(engine_lib, oracle_mod, big):
+    """Explicit pairs that share their query and their target's length (a pair
+    and its reverse-complement target) are swept two at a time in 16-bit
+    halves; with scores whose maxima pass 32767 - highest, those pairs are
+    swept again on 32-bit lanes (pw_run_info.overflow_pairs).  Maxima and hits
+    equal the oracle's pair by pair, and the 32-bit form's."""
+    rng = np.random.default_rng(61 + big)
+    comp = {"A": "T", "C": "G", "G": "C", "T": "A"}
+    queries, targets, pairs = [], [], []
+    for k in range(3):
+        lq, lt = int(rng.integers(800, 1200)), int(rng.integers(800, 1200))
+        q = "".join(rng.choice(list("ACGT"), size=lq))
+        t = "".join(rng.choice(list("ACGT"), size=lt))
+        n = min(lq, lt) // 2
+        a, b = int(rng.integers(0, lq - n)), int(rng.integers(0, lt - n))
+        # big scores: exact copies of 400-600 residues reach 40,000-60,000
+        seg = q[a:a + n] if big else cases.mutate(rng, q[a:a + n], "ACGT", 0.05, 1)
+        t = t[:b] + seg + t[b + n:]
+        t = t[:lt]
+        queries.append(q)
+        targets += [t, "".join(comp[c] for c in reversed(t))]
+        pairs += [(k, 2 * k), (k, 2 * k + 1)]
+    pairs.append((0, 3))  # a pair without a partner of its target length
+    if big:
+        st = cases.Settings(match_score="100", mismatch_score="-300", gap_score="-500", minimum_score="10",
+                            lower_limit_score="0.5", filter_factor="0.01")
+    else:
+        st = cases.Settings(minimum_score="20", lower_limit_score="0.5", filter_factor="0.01")
+    maxima, hits = _oracle_pairs(oracle_mod, queries, targets, pairs, st)
+    pm, got, info = _pairs_run(engine_lib, queries, targets, pairs, st)
+    pm32, got32, info32 = _pairs_run(engine_lib, queries, targets, pairs, st, {_native.PW_TUNE_LANES: 32})
+    for (qi, ti), m in maxima.items():
+        assert pm[qi, ti] == m and pm32[qi, ti] == m
+    key = lambda h: (h["query"], h["target"], h["s_end"], h["t_end"])
+    assert sorted(got, key=key) == sorted(hits, key=key)
+    assert got == got32
+    assert len(hits) >= 3
+    assert (info.overflow_pairs > 0) == big
