@@ -184,7 +184,8 @@ def test_pairs_two_at_a_time_on_16x2_lanes(engine_lib, oracle_mod, big):
         pairs += [(k, 2 * k), (k, 2 * k + 1)]
     pairs.append((0, 3))  # a pair without a partner of its target length
     if big:
-        st = cases.Settings(match_score="100", mismatch_score="-300", gap_score="-500", minimum_score="10",
+        # int8 scores (the integer sweeps' range) whose maxima pass 2^15
+        st = cases.Settings(match_score="100", mismatch_score="-100", gap_score="-120", minimum_score="10",
                             lower_limit_score="0.5", filter_factor="0.01")
     else:
         st = cases.Settings(minimum_score="20", lower_limit_score="0.5", filter_factor="0.01")
