@@ -85,7 +85,7 @@ def parse():
     ap.add_argument("--plan-cached", action="store_true",
                     help="keep the score sweep's work list between steps (inputs unchanged)")
     ap.add_argument("--tune", action="append", default=[], metavar="KEY=VALUE",
-                    help="engine tuning knob (chain_min, grid_share, segment, dual, cand_slot, lanes, trace_store), e.g. "
+                    help="engine tuning knob (chain_min, grid_share, segment, dual, cand_slot, lanes, trace_store, tile_trace, wait_ns), e.g. "
                          "--tune chain_min=250; without chain_min the autotuner picks it during the warm-up")
     ap.add_argument("--serve-seconds", type=float, default=20.0, help="length of each arrival stream of the serving leg")
     ap.add_argument("--serve-loads", default="0.5,0.7", help="offered loads (fractions of batched peak) swept")
@@ -661,7 +661,8 @@ def run_config(cfg, args, device, world, flush, sampler, headline):
     chain = not args.no_chain
     knobs = {"chain_min": _native.PW_TUNE_CHAIN_MIN, "grid_share": _native.PW_TUNE_GRID_SHARE,
              "segment": _native.PW_TUNE_SEGMENT, "dual": _native.PW_TUNE_DUAL, "cand_slot": _native.PW_TUNE_CAND_SLOT,
-             "lanes": _native.PW_TUNE_LANES, "trace_store": _native.PW_TUNE_TRACE_STORE}
+             "lanes": _native.PW_TUNE_LANES, "trace_store": _native.PW_TUNE_TRACE_STORE,
+             "tile_trace": _native.PW_TUNE_TILE_TRACE, "wait_ns": _native.PW_TUNE_WAIT_NS}
     tuning = {}
     for kv in args.tune:
         key, val = kv.split("=")
