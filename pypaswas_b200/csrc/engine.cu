@@ -1974,9 +1974,9 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
                 tm += (int64_t)bp[k].nbands * tile_count(lq);
             }
             // the driver's free-memory query can be held for tens of
-            // milliseconds by tools polling the GPU: read at most once a second
+            // milliseconds by tools polling the GPU: read at most every 10 s
             const double now = wall_ms();
-            if (e->p1_free_t < 0 || now - e->p1_free_t > 1000.0) {
+            if (e->p1_free_t < 0 || now - e->p1_free_t > 10000.0) {
                 size_t free_b = 0, total_b = 0;
                 cudaMemGetInfo(&free_b, &total_b);
                 e->p1_free = (int64_t)free_b + (int64_t)e->p1_ck.bytes;
@@ -2466,9 +2466,10 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
     if (auto_budget) {
         // the free-memory query goes to the driver, which tools polling the
         // GPU (nvidia-smi) can hold for tens of milliseconds: it is refreshed
-        // at most once a second
+        // at most every 10 s (the budget is a fraction of it, and an allocation
+        // that still fails is reported)
         const double now = wall_ms();
-        if (e->free_mem_t < 0 || now - e->free_mem_t > 1000.0) {
+        if (e->free_mem_t < 0 || now - e->free_mem_t > 10000.0) {
             size_t free_b = 0, total_b = 0;
             cudaMemGetInfo(&free_b, &total_b);
             e->free_mem = (int64_t)free_b + (int64_t)(e->codes.bytes + e->marks.bytes + e->cands.bytes +
