@@ -300,6 +300,11 @@ def roofline(e, w, score, infos, steps):
                2: "score sweep (band_kernel, bands chained across warps)"}.get(last["score_path"], "score sweep")
         if last["score_path"] == 2 and last.get("tile_pairs"):
             dom = "score sweep (band_kernel, bands chained across warps, keeping the tile form's checkpoints)"
+        if last["score_path"] == 2 and 2 * last.get("paired_cells", 0) >= last["cells"]:
+            # most cells on the 16x2 band sweep: its DPX issue peak is the 16x2 one
+            dom = ("score sweep (band16_kernel: a pair and its reverse-complement pair in 16-bit halves, bands "
+                   "chained across warps, keeping the tile form's checkpoints)")
+            sixteen = True
         dom_ms, launches = score_ms, sum(i["score_launches"] for i in infos)
         ops = w.cells * OPS_PER_CELL[(mode, "score")] * steps
         per_cell = OPS_PER_CELL[(mode, "score")]

@@ -96,6 +96,7 @@ typedef struct {
     int64_t d2h_bytes;      /* bytes this call copied device -> host (maxima, pair lists, starts, hits) */
     int32_t trace_store;    /* direction sweeps stored 1: each cell's 16-bit H, 0: 4-bit cell codes */
     int32_t tile_pairs;     /* traced long pairs in the tile form (checkpoints, tiles recomputed on the walk) */
+    int64_t paired_cells;   /* cells of explicit pairs swept two to a warp in 16-bit halves (band16) */
 } pw_run_info;
 
 #define PW_REUSE_QUERIES 1

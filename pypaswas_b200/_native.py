@@ -100,7 +100,8 @@ class PwRunInfo(ctypes.Structure):
                 ("score_path", ctypes.c_int32), ("dual_lanes", ctypes.c_int32),
                 ("waves", ctypes.c_int32), ("reuse", ctypes.c_int32),
                 ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64),
-                ("trace_store", ctypes.c_int32), ("tile_pairs", ctypes.c_int32)]
+                ("trace_store", ctypes.c_int32), ("tile_pairs", ctypes.c_int32),
+                ("paired_cells", ctypes.c_int64)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

@@ -2034,6 +2034,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
                     p2.tm[1] = bp[k].ring_off;
                     bp2.push_back(p2);
                     paired[j] = paired[k] = 1;
+                    inf.paired_cells += 2 * (int64_t)qlen[bp[j].q] * tlen[bp[j].t];
                 }
                 for (size_t k = 0; k < np; ++k)
                     if (!paired[k]) bp1.push_back(bp[k]);
@@ -2056,6 +2057,7 @@ extern "C" int pw_align(pw_engine* e, uint32_t flags, int64_t start_cap, pw_run_
                         return cuda_fail(e, c, "reset tile maxima");
                     bp1.push_back(bp[k]);
                     inf.overflow_pairs++;
+                    inf.paired_cells -= (int64_t)qlen[bp[k].q] * tlen[bp[k].t];
                 }
             }
             rc = run_band_phase<4>(e, A, bp1, &inf.score_kernel_ms, &inf.score_launches);
