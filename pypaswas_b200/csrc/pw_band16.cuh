@@ -8,7 +8,10 @@
 // targets' scores, and every DPX add-max (__viaddmax_s16x2) advances both
 // pairs.  Everything else is band_kernel<false, 4>: 256-row bands chained
 // across warps, the pair maxima, and per pair the tile form's checkpoints and
-// tile maxima, written as int32 for each pair separately.
+// tile maxima, written as int32 for each pair separately -- except that a band
+// lags the band above by one 32-column block, with progress published every
+// 16 steps (half as many chains run as in the 32-bit form, so the chains'
+// length bounds the sweep).
 //
 // 16-bit halves hold H exactly while every value stays at or below
 // 32767 - highest (no add can then wrap); a pair whose maximum passes that
@@ -106,14 +109,17 @@ __global__ void __launch_bounds__(128, 6) band16_kernel(KernelArgs A, BandArgs2 
         int avail = 0;
         bool ok = true;
         // the row above, 32 columns at a time (both pairs' values packed)
-        uint32_t cur = 0u, nxt = 0u;
+        uint32_t cur = 0u;
         auto fetch = [&](int64_t c) -> uint32_t {
             if (c >= lq) return 0u;
             return pack16(__ldcg(ck0 + (int64_t)(band - 1) * lq + c), __ldcg(ck1 + (int64_t)(band - 1) * lq + c));
         };
         for (int64_t s = 0; s < nsteps; ++s) {
             if (has_up && (s & 31) == 0) {
-                const int need = (int)(s + 64 < (int64_t)lq ? s + 64 : (int64_t)lq);
+                // only this block of the row above is waited for (one block
+                // of lag between bands; fetching the next block too would
+                // double it, and the chains' length is what bounds this sweep)
+                const int need = (int)(s + 32 < (int64_t)lq ? s + 32 : (int64_t)lq);
                 if (avail < need) {
                     avail = chain_wait(prog_in, need, B.abort_flag, B.wait_ns);
                     if (avail < 0) {
@@ -121,8 +127,7 @@ __global__ void __launch_bounds__(128, 6) band16_kernel(KernelArgs A, BandArgs2 
                         break;
                     }
                 }
-                cur = s == 0 ? fetch(s + lane) : nxt;
-                nxt = fetch(s + 32 + lane);
+                cur = fetch(s + lane);
             }
             const int x = (int)s - lane;
             const bool active = x >= 0 && x < lq;
@@ -170,7 +175,8 @@ __global__ void __launch_bounds__(128, 6) band16_kernel(KernelArgs A, BandArgs2 
             } else {
                 bt_h = 0u;  // not started (x < 0): the left boundary
             }
-            if (store_bnd && lane == kWarp - 1 && ((s + 1) & 31) == 0 && s >= kWarp - 1)
+            // progress every 16 steps
+            if (store_bnd && lane == kWarp - 1 && ((s + 1) & 15) == 0 && s >= kWarp - 1)
                 st_release_gpu(prog_out, (int)(s - (kWarp - 2)));
         }
         if (!ok) break;
