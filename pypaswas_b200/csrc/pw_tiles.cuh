@@ -76,6 +76,7 @@ struct TileView {
     uint2* prof;            // shared: [lane][alpha1] scores of the lane's 8 rows in the cached band
     uint8_t* qc;            // shared: the query codes of the tile's columns
     int band, tile, prof_band, x0, yb;
+    int xmax_c, ymax_c;     // the cached tile's computed extent (its cells up to these coordinates)
     uint32_t* mark_plane;   // the pair's mark bits
 
     __device__ __forceinline__ uint32_t* mark_word(int x, int y) const {
@@ -88,14 +89,18 @@ struct TileView {
     __device__ __forceinline__ void mark(int x, int y) const { atomicOr(mark_word(x, y), mark_bit(x, y)); }
     __device__ __forceinline__ void unmark(int x, int y) const { atomicAnd(mark_word(x, y), ~mark_bit(x, y)); }
 
-    __device__ void load(int b, int j) { load_h<false>(b, j, CandSink{nullptr, 0, nullptr}); }
+    __device__ void load(int b, int j, int xneed, int yneed) {
+        load_h<false>(b, j, CandSink{nullptr, 0, nullptr}, xneed, yneed);
+    }
 
-    // Recomputes the H values of tile (band b, tile j) and its border; every
-    // lane of the warp calls it.  CANDS: also the tile's candidates into the
-    // sink, with the band sweep's test (UL cells inside the matrix at or above
-    // the threshold).
+    // Recomputes the H values of tile (band b, tile j) and its border, as far
+    // as cell (xneed, yneed): the columns up to xneed and the lanes up to
+    // yneed's (a walk only moves up and left, so it needs no more of the
+    // tile); every lane of the warp calls it.  CANDS: the whole tile, and its
+    // candidates into the sink, with the band sweep's test (UL cells inside
+    // the matrix at or above the threshold).
     template <bool CANDS>
-    __device__ void load_h(int b, int j, CandSink sink) {
+    __device__ void load_h(int b, int j, CandSink sink, int xneed, int yneed) {
         const int lane = threadIdx.x & 31;
         __syncwarp();
         yb = b * kBandRows;
@@ -117,7 +122,8 @@ struct TileView {
             }
             prof_band = b;
         }
-        const int ncol = min(kTileW, lq - x0);
+        const int ncol = min(min(kTileW, lq - x0), xneed - x0 + 1);
+        const int lanes_need = min(kWarp - 1, (yneed - yb) >> 3);
         // border row (r = 0): the row above, columns x0 - 1 .. x0 + ncol - 1; 0 above band 0 and left of column 0
         for (int k = lane; k <= ncol; k += kWarp) {
             const int xx = x0 - 1 + k;
@@ -144,7 +150,7 @@ struct TileView {
         const int rows_left = lt - ymine;
         int bt_h = Hl[kWarpRows - 1];
         int up_h = lane == 0 ? hs[0] : 0;  // lane 0: the corner, its first cell's diagonal
-        const int nsteps = ncol + kWarp - 1;
+        const int nsteps = ncol + lanes_need;
         // the shared-memory reads of a step (its scores; lane 0: the row
         // above) are issued one step ahead, off the recurrence's path
         auto fetch_pw = [&](int c) -> uint2 {
@@ -211,6 +217,8 @@ struct TileView {
         }
         band = b;
         tile = j;
+        xmax_c = x0 + ncol - 1;
+        ymax_c = yb + (lanes_need + 1) * kWarpRows - 1;
         __syncwarp();
     }
 
@@ -223,7 +231,12 @@ struct TileView {
     __device__ __forceinline__ uint32_t code(int x, int y) {
         if (x < 0 || y < 0 || x >= lq || y >= lt) return kNo;
         const int b = y >> 8, j = x / kTileW;
-        if (b != band || j != tile) load(b, j);
+        if (b != band || j != tile || x > xmax_c || y > ymax_c) {
+            // a miss, or a cell past the cached extent (the covering chains of
+            // several candidates reuse a tile): recompute far enough for both
+            const bool same = b == band && j == tile;
+            load(b, j, same ? max(x, xmax_c) : x, same ? max(y, ymax_c) : y);
+        }
         const int* c = hs + (x - x0 + 1) * kTileRows + (y - yb + 1);
         const int h = c[0], l = c[-kTileRows], u = c[-1], d = c[-kTileRows - 1];
         if (h <= 0) return kNo;
@@ -257,6 +270,8 @@ __device__ __forceinline__ TileView tile_view(const KernelArgs& A, const TileArg
     v.x0 = 0;
     v.yb = 0;
     v.band = -1;
+    v.xmax_c = -1;
+    v.ymax_c = -1;
     v.tile = -1;
     v.prof_band = -1;
     v.mark_plane = T.marks + tp.marks;
@@ -557,7 +572,8 @@ __global__ void __launch_bounds__(32) tile_cand_kernel(KernelArgs A, TileArgs T,
         const TilePair tp = list[en.x];
         TileView v = tile_view(A, T, tp, A.metas[tp.slot].thr_i, smem);
         const int b = en.y / v.ntiles, j = en.y % v.ntiles;
-        v.load_h<true>(b, j, CandSink{A.cands + A.cand_base[tp.slot], A.cand_cap[tp.slot], A.n_cand + tp.slot});
+        v.load_h<true>(b, j, CandSink{A.cands + A.cand_base[tp.slot], A.cand_cap[tp.slot], A.n_cand + tp.slot},
+                       v.lq - 1, b * kBandRows + kBandRows - 1);
     }
 }
 
